@@ -1,0 +1,1018 @@
+// abi.cu -- the C ABI declared in include/fresnel_b200.h.
+//
+// Object model (mirrors fresnel/gpu/{Device,Scene,Geometry,Tracer}.cc):
+//   fr_device    one CUDA device and one stream; shared BVH-build scratch; an error status word
+//   fr_scene     ordered list of geometries (index = geometry id of the hit records) and the
+//                device table of their GeomDev records
+//   fr_geometry  device copies of the user arrays + the BVH (rebuilt lazily when a geometric
+//                array changed, like OptiX's markDirty, fresnel/gpu/Scene.h:64-83)
+//   fr_tracer    output buffers (linear RGBA f32, sRGB RGBA8) and the path tracer's per-pixel
+//                wavefront state (allocated on first path render)
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+#include "bvh.hpp"
+#include "fresnel_b200.h"
+#include "render.hpp"
+
+using namespace fr;
+
+namespace {
+
+thread_local std::string g_error;
+
+fr_status fail(fr_status s, const std::string& msg)
+{
+    g_error = msg;
+    return s;
+}
+
+fr_status cuda_fail(cudaError_t e, const char* what)
+{
+    fr_status s = (e == cudaErrorMemoryAllocation) ? FR_ERR_OUT_OF_MEMORY : FR_ERR_CUDA;
+    return fail(s, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define FR_CUDA(expr, what)                    \
+    do {                                       \
+        cudaError_t e_ = (expr);               \
+        if (e_ != cudaSuccess)                 \
+            return cuda_fail(e_, what);        \
+    } while (0)
+
+#define FR_CHECK_NULL(p)                                        \
+    do {                                                        \
+        if (!(p))                                               \
+            return fail(FR_ERR_INVALID, #p " must not be null"); \
+    } while (0)
+
+Mat to_mat(const fr_material& m)
+{
+    Mat r;
+    r.solid = m.solid;
+    r.color = c3(m.color[0], m.color[1], m.color[2]);
+    r.primitive_color_mix = m.primitive_color_mix;
+    r.roughness = m.roughness;
+    r.specular = m.specular;
+    r.metal = m.metal;
+    r.spec_trans = m.spec_trans;
+    return r;
+}
+
+// fresnel::Material(color, solid) defaults (fresnel/common/Material.h:59-64)
+fr_material default_material(float r, float g, float b, float solid)
+{
+    fr_material m;
+    m.solid = solid;
+    m.color[0] = r;
+    m.color[1] = g;
+    m.color[2] = b;
+    m.primitive_color_mix = 0.0f;
+    m.roughness = 0.1f;
+    m.specular = 0.5f;
+    m.metal = 0.0f;
+    m.spec_trans = 0.0f;
+    return m;
+}
+
+}  // namespace
+
+struct fr_device {
+    int ordinal = 0;
+    cudaStream_t stream = nullptr;
+    int num_sms = 0;
+    cudaDeviceProp prop{};
+    Scratch scratch;
+    BuildParams build;
+    LaunchShape shape{};
+    DevArray<uint32_t> status;  // traversal error bits
+};
+
+struct fr_geometry {
+    fr_scene* scene = nullptr;
+    int type = 0;
+    uint32_t n = 0;        // user primitives (mesh: instances)
+    uint32_t n_faces = 0;  // mesh
+    uint32_t n_vertices = 0;
+    uint32_t n_planes = 0;
+    float poly_radius = 0.0f;
+    float color_by_face = 0.0f;
+    bool enabled = true;
+    bool removed = false;
+    fr_material material{}, outline{};
+    float outline_width = 0.0f;
+    DevArray<float> position, radius, color, points, orientation, vertices, planes;
+    BvhBuffers bvh;
+    bool bvh_dirty = true;
+    double last_build_ms = 0.0;
+
+    uint32_t bvh_prims() const { return type == FR_GEOM_MESH ? n * n_faces : n; }
+    DevArray<float>* field(int f, size_t& count)
+    {
+        count = 0;
+        switch (f) {
+        case FR_FIELD_POSITION:
+            if (type == FR_GEOM_CYLINDER)
+                return nullptr;
+            count = size_t(n) * 3;
+            return &position;
+        case FR_FIELD_RADIUS:
+            if (type != FR_GEOM_SPHERE && type != FR_GEOM_CYLINDER)
+                return nullptr;
+            count = n;
+            return &radius;
+        case FR_FIELD_COLOR:
+            count = type == FR_GEOM_CYLINDER ? size_t(n) * 6
+                    : type == FR_GEOM_MESH   ? size_t(n_vertices) * 3
+                                             : size_t(n) * 3;
+            return &color;
+        case FR_FIELD_POINTS:
+            if (type != FR_GEOM_CYLINDER)
+                return nullptr;
+            count = size_t(n) * 6;
+            return &points;
+        case FR_FIELD_ORIENTATION:
+            if (type != FR_GEOM_POLYHEDRON && type != FR_GEOM_MESH)
+                return nullptr;
+            count = size_t(n) * 4;
+            return &orientation;
+        }
+        return nullptr;
+    }
+};
+
+struct fr_scene {
+    fr_device* dev = nullptr;
+    std::vector<fr_geometry*> geoms;
+    DevArray<GeomDev> table;
+    bool table_dirty = true;
+};
+
+struct fr_tracer {
+    fr_device* dev = nullptr;
+    uint32_t w = 0, h = 0;
+    DevArray<float4> linear;
+    DevArray<uint32_t> srgb;
+    // path tracer state
+    DevArray<float4> prim_o, prim_d, ray_o, ray_d, att, result;
+    DevArray<uint2> prim_hit, ls_depth, hit;
+    DevArray<uint32_t> q0, q1, ctr;
+    DevArray<uint2> preview_hits;
+    DevArray<unsigned long long> stats;
+    uint32_t* h_count = nullptr;  // pinned
+    uint64_t launches = 0;
+    uint64_t builds = 0;
+    double build_ms = 0.0;
+};
+
+namespace {
+
+fr_status use_device(const fr_device* d)
+{
+    FR_CUDA(cudaSetDevice(d->ordinal), "cudaSetDevice");
+    return FR_OK;
+}
+
+fr_status alloc_field(fr_geometry* g, int f)
+{
+    size_t count;
+    DevArray<float>* a = g->field(f, count);
+    if (!a || count == 0)
+        return FR_OK;
+    FR_CUDA(a->reserve(count), "allocating a geometry array");
+    FR_CUDA(cudaMemsetAsync(a->ptr, 0, count * sizeof(float), g->scene->dev->stream),
+            "clearing a geometry array");
+    return FR_OK;
+}
+
+fr_status new_geometry(fr_scene* scene, int type, uint32_t n, fr_geometry** out,
+                       fr_geometry** made)
+{
+    FR_CHECK_NULL(scene);
+    FR_CHECK_NULL(out);
+    fr_geometry* g = new (std::nothrow) fr_geometry();
+    if (!g)
+        return fail(FR_ERR_OUT_OF_MEMORY, "out of host memory");
+    g->scene = scene;
+    g->type = type;
+    g->n = n;
+    g->material = default_material(1, 0, 1, 0);
+    g->outline = default_material(0, 0, 0, 1);
+    *made = g;
+    return FR_OK;
+}
+
+fr_status finish_geometry(fr_geometry* g, fr_geometry** out)
+{
+    fr_status s = use_device(g->scene->dev);
+    if (s != FR_OK) {
+        delete g;
+        return s;
+    }
+    for (int f = 0; f <= FR_FIELD_ORIENTATION; ++f) {
+        if ((s = alloc_field(g, f)) != FR_OK) {
+            delete g;
+            return s;
+        }
+    }
+    g->scene->geoms.push_back(g);
+    g->scene->table_dirty = true;
+    *out = g;
+    return FR_OK;
+}
+
+// Build stale BVHs and refresh the device geometry table.
+fr_status prepare_scene(fr_scene* sc, fr_tracer* tr)
+{
+    fr_device* dev = sc->dev;
+    for (fr_geometry* g : sc->geoms) {
+        if (g->removed || !g->bvh_dirty)
+            continue;
+        BuildInput in;
+        in.type = g->type;
+        in.position = g->position.ptr;
+        in.radius = g->radius.ptr;
+        in.points = g->points.ptr;
+        in.orientation = g->orientation.ptr;
+        in.vertices = g->vertices.ptr;
+        in.n_faces = g->n_faces;
+        in.poly_radius = g->poly_radius;
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, dev->stream);
+        cudaError_t e = build_bvh(in, g->bvh_prims(), dev->build, g->bvh, dev->scratch, dev->stream);
+        cudaEventRecord(e1, dev->stream);
+        cudaEventSynchronize(e1);
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (e != cudaSuccess)
+            return cuda_fail(e, "building a BVH");
+        g->last_build_ms = ms;
+        if (tr) {
+            tr->builds++;
+            tr->build_ms = ms;
+        }
+        g->bvh_dirty = false;
+        sc->table_dirty = true;
+    }
+    if (sc->table_dirty) {
+        std::vector<GeomDev> host(sc->geoms.size());
+        for (size_t i = 0; i < sc->geoms.size(); ++i) {
+            fr_geometry* g = sc->geoms[i];
+            GeomDev& d = host[i];
+            std::memset(&d, 0, sizeof(d));
+            d.type = g->type;
+            d.enabled = (g->enabled && !g->removed) ? 1 : 0;
+            d.n_prims = g->bvh_prims();
+            d.n_nodes = g->bvh.n_nodes;
+            d.nodes = g->bvh.nodes.ptr;
+            d.leaf_data = g->bvh.leaf_data.ptr;
+            d.order = g->bvh.order.ptr;
+            d.position = g->position.ptr;
+            d.radius = g->radius.ptr;
+            d.color = g->color.ptr;
+            d.points = g->points.ptr;
+            d.orientation = g->orientation.ptr;
+            d.vertices = g->vertices.ptr;
+            d.planes = g->planes.ptr;
+            d.n_faces = g->n_faces;
+            d.n_planes = g->n_planes;
+            d.color_by_face = g->color_by_face;
+            d.outline_width = g->outline_width;
+            d.material = to_mat(g->material);
+            d.outline = to_mat(g->outline);
+        }
+        if (!host.empty()) {
+            FR_CUDA(sc->table.reserve(host.size()), "allocating the geometry table");
+            FR_CUDA(cudaMemcpyAsync(sc->table.ptr, host.data(), host.size() * sizeof(GeomDev),
+                                    cudaMemcpyHostToDevice, dev->stream),
+                    "uploading the geometry table");
+            FR_CUDA(cudaStreamSynchronize(dev->stream), "uploading the geometry table");
+        }
+        sc->table_dirty = false;
+    }
+    return FR_OK;
+}
+
+FrameParams frame_params(fr_tracer* tr, fr_scene* sc, const fr_render_params* p, bool preview,
+                         uint32_t aa_n)
+{
+    FrameParams P;
+    std::memset(&P, 0, sizeof(P));
+    P.scene.geoms = sc->table.ptr;
+    P.scene.n_geoms = uint32_t(sc->geoms.size());
+    P.scene.status = sc->dev->status.ptr;
+    const fr_user_camera& c = p->camera;
+    float f_stop = preview ? std::numeric_limits<float>::infinity() : c.f_stop;  // no depth of field in preview
+    bool sample_aa = preview ? (aa_n != 1) : true;
+    P.cam = make_camera(v3(c.position[0], c.position[1], c.position[2]),
+                        v3(c.look_at[0], c.look_at[1], c.look_at[2]),
+                        v3(c.up[0], c.up[1], c.up[2]), c.h, c.f, f_stop, c.focus_distance, c.model,
+                        tr->w, tr->h, p->seed, sample_aa);
+    V3 dirs[4];
+    C3 cols[4];
+    float th[4];
+    uint32_t n = p->lights.n > 4 ? 4 : p->lights.n;
+    for (uint32_t i = 0; i < 4; ++i) {
+        dirs[i] = v3(p->lights.direction[i][0], p->lights.direction[i][1], p->lights.direction[i][2]);
+        cols[i] = c3(p->lights.color[i][0], p->lights.color[i][1], p->lights.color[i][2]);
+        th[i] = p->lights.theta[i];
+    }
+    P.lights = lights_to_world(dirs, cols, th, n, P.cam);
+    P.bg = c3(p->background_color[0], p->background_color[1], p->background_color[2]);
+    P.bg_alpha = p->background_alpha;
+    P.w = tr->w;
+    P.h = tr->h;
+    P.highlight = p->highlight_warning;
+    P.hl_color = c3(p->highlight_color[0], p->highlight_color[1], p->highlight_color[2]);
+    P.linear = tr->linear.ptr;
+    P.srgb = tr->srgb.ptr;
+    P.stats = tr->stats.ptr;
+    return P;
+}
+
+fr_status check_status(fr_device* dev)
+{
+    uint32_t st = 0;
+    FR_CUDA(cudaMemcpyAsync(&st, dev->status.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                            dev->stream),
+            "reading the device status");
+    FR_CUDA(cudaStreamSynchronize(dev->stream), "render");
+    if (st) {
+        FR_CUDA(cudaMemsetAsync(dev->status.ptr, 0, sizeof(uint32_t), dev->stream), "status reset");
+        return fail(FR_ERR_DEVICE_LIMIT, (st & ERR_STACK_OVERFLOW)
+                                             ? "BVH traversal stack overflow (tree too deep)"
+                                             : "BVH traversal iteration cap reached");
+    }
+    return FR_OK;
+}
+
+fr_status alloc_outputs(fr_tracer* tr, uint32_t w, uint32_t h)
+{
+    size_t n = size_t(w) * h;
+    FR_CUDA(tr->linear.reserve(n), "allocating the linear output");
+    FR_CUDA(tr->srgb.reserve(n), "allocating the sRGB output");
+    FR_CUDA(cudaMemsetAsync(tr->linear.ptr, 0, n * sizeof(float4), tr->dev->stream), "clear");
+    FR_CUDA(cudaMemsetAsync(tr->srgb.ptr, 0, n * sizeof(uint32_t), tr->dev->stream), "clear");
+    tr->w = w;
+    tr->h = h;
+    return FR_OK;
+}
+
+fr_status alloc_path_state(fr_tracer* tr)
+{
+    size_t n = size_t(tr->w) * tr->h;
+    FR_CUDA(tr->prim_o.reserve(n), "path state");
+    FR_CUDA(tr->prim_d.reserve(n), "path state");
+    FR_CUDA(tr->ray_o.reserve(n), "path state");
+    FR_CUDA(tr->ray_d.reserve(n), "path state");
+    FR_CUDA(tr->att.reserve(n), "path state");
+    FR_CUDA(tr->result.reserve(n), "path state");
+    FR_CUDA(tr->prim_hit.reserve(n), "path state");
+    FR_CUDA(tr->ls_depth.reserve(n), "path state");
+    FR_CUDA(tr->hit.reserve(n), "path state");
+    FR_CUDA(tr->q0.reserve(n), "path state");
+    FR_CUDA(tr->q1.reserve(n), "path state");
+    FR_CUDA(tr->ctr.reserve(4), "path state");
+    return FR_OK;
+}
+
+PathState path_state(fr_tracer* tr)
+{
+    PathState S;
+    S.prim_o = tr->prim_o.ptr;
+    S.prim_d = tr->prim_d.ptr;
+    S.prim_hit = tr->prim_hit.ptr;
+    S.ray_o = tr->ray_o.ptr;
+    S.ray_d = tr->ray_d.ptr;
+    S.att = tr->att.ptr;
+    S.result = tr->result.ptr;
+    S.ls_depth = tr->ls_depth.ptr;
+    S.hit = tr->hit.ptr;
+    S.queue[0] = tr->q0.ptr;
+    S.queue[1] = tr->q1.ptr;
+    S.ctr = tr->ctr.ptr;
+    return S;
+}
+
+fr_status check_params(const fr_tracer* tr, const fr_scene* sc, const fr_render_params* p)
+{
+    FR_CHECK_NULL(tr);
+    FR_CHECK_NULL(sc);
+    FR_CHECK_NULL(p);
+    if (sc->dev != tr->dev)
+        return fail(FR_ERR_INVALID, "Scene and Tracer devices do not match");
+    return FR_OK;
+}
+
+}  // namespace
+
+// =============================================================================================
+extern "C" {
+
+const char* fr_last_error(void) { return g_error.c_str(); }
+int fr_abi_version(void) { return FR_ABI_VERSION; }
+
+fr_status fr_get_num_available_devices(int* n)
+{
+    FR_CHECK_NULL(n);
+    *n = 0;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess) {
+        cudaGetLastError();
+        return FR_OK;  // no driver or no device: zero GPUs
+    }
+    for (int i = 0; i < count; ++i) {
+        cudaDeviceProp prop;
+        if (cudaGetDeviceProperties(&prop, i) == cudaSuccess && prop.major == 10)
+            ++*n;
+    }
+    return FR_OK;
+}
+
+fr_status fr_get_all_gpus(char* buf, size_t cap)
+{
+    FR_CHECK_NULL(buf);
+    std::string s;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess) {
+        cudaGetLastError();
+        count = 0;
+    }
+    for (int i = 0; i < count; ++i) {
+        cudaDeviceProp prop;
+        if (cudaGetDeviceProperties(&prop, i) == cudaSuccess && prop.major == 10) {
+            s += "[" + std::to_string(i) + "]: " + prop.name + " " +
+                 std::to_string(prop.multiProcessorCount) + " SM_" + std::to_string(prop.major) +
+                 "." + std::to_string(prop.minor) + "\n";
+        }
+    }
+    if (cap == 0)
+        return fail(FR_ERR_INVALID, "buffer capacity is zero");
+    std::snprintf(buf, cap, "%s", s.c_str());
+    return FR_OK;
+}
+
+fr_status fr_device_create(int n, fr_device** out)
+{
+    FR_CHECK_NULL(out);
+    *out = nullptr;
+    int avail = 0;
+    fr_get_num_available_devices(&avail);
+    if (avail == 0)
+        return fail(FR_ERR_UNSUPPORTED, "No GPUs are available (an sm_100 device is required)");
+    if (n == 0 || n < -1)
+        return fail(FR_ERR_INVALID, "the number of GPUs must be positive or -1");
+    int count = 0;
+    FR_CUDA(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
+    int ordinal = -1;
+    for (int i = 0; i < count && ordinal < 0; ++i) {
+        cudaDeviceProp prop;
+        if (cudaGetDeviceProperties(&prop, i) == cudaSuccess && prop.major == 10)
+            ordinal = i;
+    }
+    fr_device* d = new (std::nothrow) fr_device();
+    if (!d)
+        return fail(FR_ERR_OUT_OF_MEMORY, "out of host memory");
+    d->ordinal = ordinal;
+    cudaError_t e = cudaSetDevice(ordinal);
+    if (e == cudaSuccess)
+        e = cudaGetDeviceProperties(&d->prop, ordinal);
+    if (e == cudaSuccess)
+        e = cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess)
+        e = d->status.reserve(1);
+    if (e == cudaSuccess)
+        e = cudaMemset(d->status.ptr, 0, sizeof(uint32_t));
+    if (e != cudaSuccess) {
+        delete d;
+        return cuda_fail(e, "creating the device");
+    }
+    d->num_sms = d->prop.multiProcessorCount;
+    d->shape = path_launch_shape(d->num_sms);
+    *out = d;
+    return FR_OK;
+}
+
+fr_status fr_device_destroy(fr_device* d)
+{
+    if (!d)
+        return FR_OK;
+    cudaSetDevice(d->ordinal);
+    if (d->stream) {
+        cudaStreamSynchronize(d->stream);
+        cudaStreamDestroy(d->stream);
+    }
+    delete d;
+    return FR_OK;
+}
+
+fr_status fr_device_describe(const fr_device* d, char* buf, size_t cap)
+{
+    FR_CHECK_NULL(d);
+    FR_CHECK_NULL(buf);
+    if (cap == 0)
+        return fail(FR_ERR_INVALID, "buffer capacity is zero");
+    std::snprintf(buf, cap, "Enabled GPUs:\n[%d]: %s %d SM_%d.%d\n", d->ordinal, d->prop.name,
+                  d->num_sms, d->prop.major, d->prop.minor);
+    return FR_OK;
+}
+
+fr_status fr_device_synchronize(fr_device* d)
+{
+    FR_CHECK_NULL(d);
+    FR_CUDA(cudaStreamSynchronize(d->stream), "cudaStreamSynchronize");
+    return FR_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+fr_status fr_scene_create(fr_device* dev, fr_scene** out)
+{
+    FR_CHECK_NULL(dev);
+    FR_CHECK_NULL(out);
+    fr_scene* s = new (std::nothrow) fr_scene();
+    if (!s)
+        return fail(FR_ERR_OUT_OF_MEMORY, "out of host memory");
+    s->dev = dev;
+    *out = s;
+    return FR_OK;
+}
+
+fr_status fr_scene_destroy(fr_scene* s)
+{
+    if (!s)
+        return FR_OK;
+    cudaSetDevice(s->dev->ordinal);
+    cudaStreamSynchronize(s->dev->stream);
+    for (fr_geometry* g : s->geoms)
+        g->scene = nullptr;  // geometries outlive nothing: the owner destroys them explicitly
+    delete s;
+    return FR_OK;
+}
+
+fr_status fr_scene_build(fr_scene* s)
+{
+    FR_CHECK_NULL(s);
+    fr_status st = use_device(s->dev);
+    if (st != FR_OK)
+        return st;
+    return prepare_scene(s, nullptr);
+}
+
+// ---------------------------------------------------------------------------------------------
+fr_status fr_geometry_create_sphere(fr_scene* scene, uint32_t n, fr_geometry** out)
+{
+    fr_geometry* g = nullptr;
+    fr_status s = new_geometry(scene, FR_GEOM_SPHERE, n, out, &g);
+    return s != FR_OK ? s : finish_geometry(g, out);
+}
+
+fr_status fr_geometry_create_cylinder(fr_scene* scene, uint32_t n, fr_geometry** out)
+{
+    fr_geometry* g = nullptr;
+    fr_status s = new_geometry(scene, FR_GEOM_CYLINDER, n, out, &g);
+    return s != FR_OK ? s : finish_geometry(g, out);
+}
+
+fr_status fr_geometry_create_polyhedron(fr_scene* scene, const float* origins, const float* normals,
+                                        const float* colors, uint32_t n_planes, uint32_t n,
+                                        float radius, fr_geometry** out)
+{
+    FR_CHECK_NULL(origins);
+    FR_CHECK_NULL(normals);
+    FR_CHECK_NULL(colors);
+    if (n_planes == 0)
+        return fail(FR_ERR_INVALID, "a convex polyhedron needs at least one plane");
+    fr_geometry* g = nullptr;
+    fr_status s = new_geometry(scene, FR_GEOM_POLYHEDRON, n, out, &g);
+    if (s != FR_OK)
+        return s;
+    g->n_planes = n_planes;
+    g->poly_radius = radius;
+    // [origin, unit normal, colour] per plane; normals scaled by 1/|n|
+    // (fresnel/cpu/GeometryConvexPolyhedron.cc:81-91)
+    std::vector<float> pl(size_t(n_planes) * 9);
+    for (uint32_t i = 0; i < n_planes; ++i) {
+        V3 nn = v3(normals[3 * i], normals[3 * i + 1], normals[3 * i + 2]);
+        nn = div_recip(nn, sqrtf(dot(nn, nn)));
+        float* q = pl.data() + 9 * i;
+        q[0] = origins[3 * i];
+        q[1] = origins[3 * i + 1];
+        q[2] = origins[3 * i + 2];
+        q[3] = nn.x;
+        q[4] = nn.y;
+        q[5] = nn.z;
+        q[6] = colors[3 * i];
+        q[7] = colors[3 * i + 1];
+        q[8] = colors[3 * i + 2];
+    }
+    cudaError_t e = use_device(scene->dev) == FR_OK ? g->planes.reserve(pl.size()) : cudaErrorUnknown;
+    if (e == cudaSuccess)
+        e = cudaMemcpy(g->planes.ptr, pl.data(), pl.size() * sizeof(float), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        delete g;
+        return cuda_fail(e, "uploading polyhedron planes");
+    }
+    return finish_geometry(g, out);
+}
+
+fr_status fr_geometry_create_mesh(fr_scene* scene, const float* vertices, uint32_t n_vertices,
+                                  uint32_t n, fr_geometry** out)
+{
+    FR_CHECK_NULL(vertices);
+    if (n_vertices % 3 != 0)
+        return fail(FR_ERR_INVALID, "the number of triangle vertices must be a multiple of three.");
+    fr_geometry* g = nullptr;
+    fr_status s = new_geometry(scene, FR_GEOM_MESH, n, out, &g);
+    if (s != FR_OK)
+        return s;
+    g->n_vertices = n_vertices;
+    g->n_faces = n_vertices / 3;
+    cudaError_t e = use_device(scene->dev) == FR_OK ? g->vertices.reserve(size_t(n_vertices) * 3)
+                                                    : cudaErrorUnknown;
+    if (e == cudaSuccess && n_vertices)
+        e = cudaMemcpy(g->vertices.ptr, vertices, size_t(n_vertices) * 3 * sizeof(float),
+                       cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        delete g;
+        return cuda_fail(e, "uploading mesh vertices");
+    }
+    return finish_geometry(g, out);
+}
+
+fr_status fr_geometry_destroy(fr_geometry* g)
+{
+    if (!g)
+        return FR_OK;
+    if (g->scene) {
+        cudaSetDevice(g->scene->dev->ordinal);
+        cudaStreamSynchronize(g->scene->dev->stream);
+        auto& v = g->scene->geoms;
+        for (size_t i = 0; i < v.size(); ++i)
+            if (v[i] == g) {
+                v.erase(v.begin() + long(i));
+                break;
+            }
+        g->scene->table_dirty = true;
+    }
+    delete g;
+    return FR_OK;
+}
+
+fr_status fr_geometry_field_size(const fr_geometry* g, int field, size_t* nbytes)
+{
+    FR_CHECK_NULL(g);
+    FR_CHECK_NULL(nbytes);
+    size_t count = 0;
+    const_cast<fr_geometry*>(g)->field(field, count);
+    *nbytes = count * sizeof(float);
+    return FR_OK;
+}
+
+fr_status fr_geometry_write(fr_geometry* g, int field, const void* host, size_t offset,
+                            size_t nbytes)
+{
+    FR_CHECK_NULL(g);
+    FR_CHECK_NULL(host);
+    if (!g->scene)
+        return fail(FR_ERR_STATE, "the geometry's scene was destroyed");
+    size_t count = 0;
+    DevArray<float>* a = g->field(field, count);
+    if (!a)
+        return fail(FR_ERR_INVALID, "this geometry has no such array");
+    if (offset + nbytes > count * sizeof(float))
+        return fail(FR_ERR_INVALID, "write past the end of the array");
+    if (nbytes == 0)
+        return FR_OK;
+    fr_status s = use_device(g->scene->dev);
+    if (s != FR_OK)
+        return s;
+    FR_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(a->ptr) + offset, host, nbytes,
+                            cudaMemcpyHostToDevice, g->scene->dev->stream),
+            "uploading a geometry array");
+    FR_CUDA(cudaStreamSynchronize(g->scene->dev->stream), "uploading a geometry array");
+    if (field != FR_FIELD_COLOR)
+        g->bvh_dirty = true;  // colours do not move primitives
+    return FR_OK;
+}
+
+fr_status fr_geometry_read(fr_geometry* g, int field, void* host, size_t offset, size_t nbytes)
+{
+    FR_CHECK_NULL(g);
+    FR_CHECK_NULL(host);
+    if (!g->scene)
+        return fail(FR_ERR_STATE, "the geometry's scene was destroyed");
+    size_t count = 0;
+    DevArray<float>* a = g->field(field, count);
+    if (!a)
+        return fail(FR_ERR_INVALID, "this geometry has no such array");
+    if (offset + nbytes > count * sizeof(float))
+        return fail(FR_ERR_INVALID, "read past the end of the array");
+    if (nbytes == 0)
+        return FR_OK;
+    fr_status s = use_device(g->scene->dev);
+    if (s != FR_OK)
+        return s;
+    FR_CUDA(cudaMemcpyAsync(host, reinterpret_cast<const char*>(a->ptr) + offset, nbytes,
+                            cudaMemcpyDeviceToHost, g->scene->dev->stream),
+            "downloading a geometry array");
+    FR_CUDA(cudaStreamSynchronize(g->scene->dev->stream), "downloading a geometry array");
+    return FR_OK;
+}
+
+fr_status fr_geometry_set_enabled(fr_geometry* g, int enabled)
+{
+    FR_CHECK_NULL(g);
+    if (g->removed || !g->scene)
+        return fail(FR_ERR_STATE, enabled ? "Cannot enable inactive Geometry"
+                                          : "Cannot disable inactive Geometry");
+    g->enabled = enabled != 0;
+    g->scene->table_dirty = true;
+    return FR_OK;
+}
+
+fr_status fr_geometry_remove(fr_geometry* g)
+{
+    FR_CHECK_NULL(g);
+    if (!g->removed && g->scene) {
+        g->removed = true;
+        g->scene->table_dirty = true;
+    }
+    return FR_OK;
+}
+
+fr_status fr_geometry_set_material(fr_geometry* g, const fr_material* m, const fr_material* outline,
+                                   float outline_width)
+{
+    FR_CHECK_NULL(g);
+    if (m)
+        g->material = *m;
+    if (outline)
+        g->outline = *outline;
+    g->outline_width = outline_width;
+    if (g->scene)
+        g->scene->table_dirty = true;
+    return FR_OK;
+}
+
+fr_status fr_geometry_set_color_by_face(fr_geometry* g, float f)
+{
+    FR_CHECK_NULL(g);
+    g->color_by_face = f;
+    if (g->scene)
+        g->scene->table_dirty = true;
+    return FR_OK;
+}
+
+fr_status fr_geometry_update(fr_geometry* g)
+{
+    FR_CHECK_NULL(g);
+    g->bvh_dirty = true;
+    return FR_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+fr_status fr_tracer_create(fr_device* dev, uint32_t w, uint32_t h, fr_tracer** out)
+{
+    FR_CHECK_NULL(dev);
+    FR_CHECK_NULL(out);
+    *out = nullptr;
+    if (w == 0 || h == 0)
+        return fail(FR_ERR_INVALID, "Invalid dimensions");
+    fr_status s = use_device(dev);
+    if (s != FR_OK)
+        return s;
+    fr_tracer* t = new (std::nothrow) fr_tracer();
+    if (!t)
+        return fail(FR_ERR_OUT_OF_MEMORY, "out of host memory");
+    t->dev = dev;
+    cudaError_t e = t->stats.reserve(4);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(t->stats.ptr, 0, 4 * sizeof(unsigned long long), dev->stream);
+    if (e == cudaSuccess)
+        e = cudaMallocHost((void**)&t->h_count, 4 * sizeof(uint32_t));
+    if (e != cudaSuccess) {
+        delete t;
+        return cuda_fail(e, "creating a tracer");
+    }
+    if ((s = alloc_outputs(t, w, h)) != FR_OK) {
+        cudaFreeHost(t->h_count);
+        delete t;
+        return s;
+    }
+    *out = t;
+    return FR_OK;
+}
+
+fr_status fr_tracer_destroy(fr_tracer* t)
+{
+    if (!t)
+        return FR_OK;
+    cudaSetDevice(t->dev->ordinal);
+    cudaStreamSynchronize(t->dev->stream);
+    if (t->h_count)
+        cudaFreeHost(t->h_count);
+    delete t;
+    return FR_OK;
+}
+
+fr_status fr_tracer_resize(fr_tracer* t, uint32_t w, uint32_t h)
+{
+    FR_CHECK_NULL(t);
+    if (w == 0 || h == 0)
+        return fail(FR_ERR_INVALID, "Invalid dimensions");
+    fr_status s = use_device(t->dev);
+    if (s != FR_OK)
+        return s;
+    s = alloc_outputs(t, w, h);
+    if (s != FR_OK)
+        return s;
+    FR_CUDA(cudaStreamSynchronize(t->dev->stream), "resize");
+    return FR_OK;
+}
+
+fr_status fr_tracer_clear(fr_tracer* t)
+{
+    FR_CHECK_NULL(t);
+    fr_status s = use_device(t->dev);
+    if (s != FR_OK)
+        return s;
+    size_t n = size_t(t->w) * t->h;
+    FR_CUDA(cudaMemsetAsync(t->linear.ptr, 0, n * sizeof(float4), t->dev->stream), "clear");
+    FR_CUDA(cudaMemsetAsync(t->srgb.ptr, 0, n * sizeof(uint32_t), t->dev->stream), "clear");
+    FR_CUDA(cudaStreamSynchronize(t->dev->stream), "clear");
+    return FR_OK;
+}
+
+fr_status fr_tracer_render_path(fr_tracer* t, fr_scene* sc, const fr_render_params* p,
+                                uint32_t first_sample, uint32_t n_render, uint32_t light_samples)
+{
+    fr_status s = check_params(t, sc, p);
+    if (s != FR_OK)
+        return s;
+    if (light_samples == 0)
+        return fail(FR_ERR_INVALID, "light_samples must be positive");
+    if (first_sample == 0)
+        return fail(FR_ERR_INVALID, "sample numbers start at 1");
+    if ((s = use_device(t->dev)) != FR_OK)
+        return s;
+    if ((s = prepare_scene(sc, t)) != FR_OK)
+        return s;
+    if ((s = alloc_path_state(t)) != FR_OK)
+        return s;
+    FrameParams P = frame_params(t, sc, p, false, 1);
+    P.light_samples = light_samples;
+    PathState S = path_state(t);
+    cudaStream_t st = t->dev->stream;
+    const int CHECK_EVERY = 4;
+    const int MAX_ITER = 1 << 20;
+    for (uint32_t k = 0; k < n_render; ++k) {
+        P.n_samples = first_sample + k;
+        launch_path_primary(P, S, st);
+        t->launches++;
+        int it = 0;
+        while (true) {
+            for (int b = 0; b < CHECK_EVERY; ++b, ++it) {
+                launch_path_iteration(P, S, it, t->dev->shape, st);
+                t->launches += 2;
+            }
+            FR_CUDA(cudaGetLastError(), "launching the path tracer");
+            FR_CUDA(cudaMemcpyAsync(t->h_count, t->ctr.ptr + ((it - 1) & 1), sizeof(uint32_t),
+                                    cudaMemcpyDeviceToHost, st),
+                    "reading the queue length");
+            FR_CUDA(cudaStreamSynchronize(st), "path tracer");
+            if (*t->h_count == 0)
+                break;
+            if (it >= MAX_ITER)
+                return fail(FR_ERR_DEVICE_LIMIT, "path tracer exceeded the bounce iteration cap");
+        }
+    }
+    return check_status(t->dev);
+}
+
+fr_status fr_tracer_render_preview(fr_tracer* t, fr_scene* sc, const fr_render_params* p,
+                                   uint32_t aa_n, uint32_t* hit_ids)
+{
+    fr_status s = check_params(t, sc, p);
+    if (s != FR_OK)
+        return s;
+    if (aa_n == 0)
+        return fail(FR_ERR_INVALID, "the anti-aliasing level must be positive");
+    if ((s = use_device(t->dev)) != FR_OK)
+        return s;
+    if ((s = prepare_scene(sc, t)) != FR_OK)
+        return s;
+    FrameParams P = frame_params(t, sc, p, true, aa_n);
+    size_t nh = size_t(t->w) * t->h * aa_n * aa_n;
+    uint2* hits = nullptr;
+    if (hit_ids) {
+        FR_CUDA(t->preview_hits.reserve(nh), "allocating the hit-id buffer");
+        hits = t->preview_hits.ptr;
+    }
+    launch_preview(P, aa_n, hits, t->dev->stream);
+    t->launches++;
+    FR_CUDA(cudaGetLastError(), "launching the preview tracer");
+    if (hit_ids)
+        FR_CUDA(cudaMemcpyAsync(hit_ids, hits, nh * sizeof(uint2), cudaMemcpyDeviceToHost,
+                                t->dev->stream),
+                "downloading hit ids");
+    return check_status(t->dev);
+}
+
+fr_status fr_tracer_read_linear(fr_tracer* t, float* host, size_t nbytes)
+{
+    FR_CHECK_NULL(t);
+    FR_CHECK_NULL(host);
+    if (nbytes != size_t(t->w) * t->h * sizeof(float4))
+        return fail(FR_ERR_INVALID, "linear output size mismatch");
+    fr_status s = use_device(t->dev);
+    if (s != FR_OK)
+        return s;
+    FR_CUDA(cudaMemcpyAsync(host, t->linear.ptr, nbytes, cudaMemcpyDeviceToHost, t->dev->stream),
+            "downloading the linear output");
+    FR_CUDA(cudaStreamSynchronize(t->dev->stream), "downloading the linear output");
+    return FR_OK;
+}
+
+fr_status fr_tracer_read_srgb(fr_tracer* t, uint8_t* host, size_t nbytes)
+{
+    FR_CHECK_NULL(t);
+    FR_CHECK_NULL(host);
+    if (nbytes != size_t(t->w) * t->h * 4)
+        return fail(FR_ERR_INVALID, "sRGB output size mismatch");
+    fr_status s = use_device(t->dev);
+    if (s != FR_OK)
+        return s;
+    FR_CUDA(cudaMemcpyAsync(host, t->srgb.ptr, nbytes, cudaMemcpyDeviceToHost, t->dev->stream),
+            "downloading the sRGB output");
+    FR_CUDA(cudaStreamSynchronize(t->dev->stream), "downloading the sRGB output");
+    return FR_OK;
+}
+
+fr_status fr_tracer_write_linear(fr_tracer* t, const float* host, size_t nbytes)
+{
+    FR_CHECK_NULL(t);
+    FR_CHECK_NULL(host);
+    if (nbytes != size_t(t->w) * t->h * sizeof(float4))
+        return fail(FR_ERR_INVALID, "linear output size mismatch");
+    fr_status s = use_device(t->dev);
+    if (s != FR_OK)
+        return s;
+    FR_CUDA(cudaMemcpyAsync(t->linear.ptr, host, nbytes, cudaMemcpyHostToDevice, t->dev->stream),
+            "uploading the linear output");
+    FR_CUDA(cudaStreamSynchronize(t->dev->stream), "uploading the linear output");
+    return FR_OK;
+}
+
+fr_status fr_tracer_write_srgb(fr_tracer* t, const uint8_t* host, size_t nbytes)
+{
+    FR_CHECK_NULL(t);
+    FR_CHECK_NULL(host);
+    if (nbytes != size_t(t->w) * t->h * 4)
+        return fail(FR_ERR_INVALID, "sRGB output size mismatch");
+    fr_status s = use_device(t->dev);
+    if (s != FR_OK)
+        return s;
+    FR_CUDA(cudaMemcpyAsync(t->srgb.ptr, host, nbytes, cudaMemcpyHostToDevice, t->dev->stream),
+            "uploading the sRGB output");
+    FR_CUDA(cudaStreamSynchronize(t->dev->stream), "uploading the sRGB output");
+    return FR_OK;
+}
+
+fr_status fr_tracer_get_stats(const fr_tracer* t, fr_stats* out)
+{
+    FR_CHECK_NULL(t);
+    FR_CHECK_NULL(out);
+    unsigned long long v[4] = {0, 0, 0, 0};
+    FR_CUDA(cudaSetDevice(t->dev->ordinal), "cudaSetDevice");
+    FR_CUDA(cudaMemcpyAsync(v, t->stats.ptr, sizeof(v), cudaMemcpyDeviceToHost, t->dev->stream),
+            "reading tracer counters");
+    FR_CUDA(cudaStreamSynchronize(t->dev->stream), "reading tracer counters");
+    out->rays = v[0];
+    out->paths = v[1];
+    out->dropped = v[2];
+    out->kernel_launches = t->launches;
+    out->bvh_builds = t->builds;
+    out->bvh_build_ms = t->build_ms;
+    return FR_OK;
+}
+
+fr_status fr_tracer_reset_stats(fr_tracer* t)
+{
+    FR_CHECK_NULL(t);
+    FR_CUDA(cudaSetDevice(t->dev->ordinal), "cudaSetDevice");
+    FR_CUDA(cudaMemsetAsync(t->stats.ptr, 0, 4 * sizeof(unsigned long long), t->dev->stream),
+            "clearing tracer counters");
+    FR_CUDA(cudaStreamSynchronize(t->dev->stream), "clearing tracer counters");
+    t->launches = 0;
+    t->builds = 0;
+    return FR_OK;
+}
+
+}  // extern "C"

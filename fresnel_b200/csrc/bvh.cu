@@ -1,0 +1,542 @@
+// bvh.cu -- GPU LBVH construction for one geometry.
+//
+// Replaces the acceleration structure the reference gets from OptiX ("Trbvh",
+// fresnel/gpu/Scene.cc:19) or Embree (RTC_BUILD_QUALITY_LOW, fresnel/cpu/Scene.cc:18-19),
+// built over the per-primitive bounds of fresnel/gpu/Geometry*.cu / fresnel/cpu/Geometry*.cc.
+// Method (published): Karras, "Maximizing parallelism in the construction of BVHs, octrees,
+// and k-d trees", HPG 2012 -- 63-bit Morton codes of the box centroids, radix sort (CUB),
+// one thread per internal node to find its key range and split, then a bottom-up pass with
+// per-node arrival counters that unions child boxes and evaluates the surface-area cost of
+// turning each subtree into a leaf (collapse when count <= leaf_max and the leaf is cheaper).
+// The surviving interior nodes are compacted so that the two children of every interior node
+// are adjacent (one 64-byte load per traversal step).
+#include <cub/cub.cuh>
+
+#include "bvh.hpp"
+#include "engine.cuh"
+
+namespace fr {
+
+namespace {
+
+struct Box {
+    float3 lo, hi;
+};
+
+__device__ __forceinline__ float3 f3min(float3 a, float3 b)
+{
+    return make_float3(fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z));
+}
+__device__ __forceinline__ float3 f3max(float3 a, float3 b)
+{
+    return make_float3(fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z));
+}
+
+__device__ __forceinline__ bool finite3(float3 a)
+{
+    return isfinite(a.x) && isfinite(a.y) && isfinite(a.z);
+}
+
+// Pad a box outward so that rounding in the traversal's slab test (one fused multiply-add per
+// plane) can never reject a ray that the exact intersector would accept.
+__device__ __forceinline__ Box inflate(Box b)
+{
+    float scale = fmaxf(fmaxf(fmaxf(fabsf(b.lo.x), fabsf(b.hi.x)), fmaxf(fabsf(b.lo.y), fabsf(b.hi.y))),
+                        fmaxf(fabsf(b.lo.z), fabsf(b.hi.z)));
+    float ext = (b.hi.x - b.lo.x) + (b.hi.y - b.lo.y) + (b.hi.z - b.lo.z);
+    float pad = 1e-5f * scale + 1e-6f * ext + 1e-30f;
+    b.lo = make_float3(b.lo.x - pad, b.lo.y - pad, b.lo.z - pad);
+    b.hi = make_float3(b.hi.x + pad, b.hi.y + pad, b.hi.z + pad);
+    return b;
+}
+
+__device__ __forceinline__ void grow(Box& b, V3 p)
+{
+    b.lo = f3min(b.lo, make_float3(p.x, p.y, p.z));
+    b.hi = f3max(b.hi, make_float3(p.x, p.y, p.z));
+}
+
+__device__ __forceinline__ Box empty_box()
+{
+    const float inf = __int_as_float(0x7f800000);
+    return Box{make_float3(inf, inf, inf), make_float3(-inf, -inf, -inf)};
+}
+
+// Bounds of one primitive (fresnel/cpu/GeometrySphere.cc:60-73, GeometryCylinder.cc:55-70,
+// GeometryConvexPolyhedron.cc:119-132, GeometryMesh.cc:81-113).  Non-finite bounds (e.g. an
+// infinite radius) give an empty box, which no ray enters.
+__device__ Box prim_bounds(const BuildInput& in, uint32_t i)
+{
+    Box b = empty_box();
+    switch (in.type) {
+    case FR_GEOM_SPHERE: {
+        V3 p = load3(in.position, i);
+        float r = in.radius[i];
+        grow(b, v3(p.x - r, p.y - r, p.z - r));
+        grow(b, v3(p.x + r, p.y + r, p.z + r));
+        break;
+    }
+    case FR_GEOM_CYLINDER: {
+        V3 A = load3(in.points, 2 * i), B = load3(in.points, 2 * i + 1);
+        float r = in.radius[i];
+        grow(b, v3(A.x - r, A.y - r, A.z - r));
+        grow(b, v3(A.x + r, A.y + r, A.z + r));
+        grow(b, v3(B.x - r, B.y - r, B.z - r));
+        grow(b, v3(B.x + r, B.y + r, B.z + r));
+        break;
+    }
+    case FR_GEOM_POLYHEDRON: {
+        V3 p = load3(in.position, i);
+        float r = in.poly_radius;
+        grow(b, v3(p.x - r, p.y - r, p.z - r));
+        grow(b, v3(p.x + r, p.y + r, p.z + r));
+        break;
+    }
+    default: {
+        uint32_t inst = i / in.n_faces, face = i - inst * in.n_faces;
+        V3 p = load3(in.position, inst);
+        Qt q = loadq(in.orientation, inst);
+        for (int k = 0; k < 3; ++k)
+            grow(b, rotate(q, load3(in.vertices, 3 * face + k)) + p);
+        break;
+    }
+    }
+    if (!finite3(b.lo) || !finite3(b.hi) || b.lo.x > b.hi.x || b.lo.y > b.hi.y || b.lo.z > b.hi.z)
+        return empty_box();
+    return inflate(b);
+}
+
+// float <-> order-preserving uint32 for atomic min/max of the centroid bounds
+__device__ __forceinline__ uint32_t f2o(float f)
+{
+    uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float o2f(uint32_t u)
+{
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+__global__ void k_bounds(BuildInput in, uint32_t n, float4* box_lo, float4* box_hi,
+                         uint32_t* cbounds)
+{
+    uint32_t lmin[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, lmax[3] = {0u, 0u, 0u};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        Box b = prim_bounds(in, i);
+        box_lo[i] = make_float4(b.lo.x, b.lo.y, b.lo.z, 0.0f);
+        box_hi[i] = make_float4(b.hi.x, b.hi.y, b.hi.z, 0.0f);
+        if (b.lo.x <= b.hi.x) {
+            float c[3] = {0.5f * (b.lo.x + b.hi.x), 0.5f * (b.lo.y + b.hi.y), 0.5f * (b.lo.z + b.hi.z)};
+            for (int k = 0; k < 3; ++k) {
+                lmin[k] = min(lmin[k], f2o(c[k]));
+                lmax[k] = max(lmax[k], f2o(c[k]));
+            }
+        }
+    }
+    for (int k = 0; k < 3; ++k) {
+        for (int off = 16; off > 0; off >>= 1) {
+            lmin[k] = min(lmin[k], __shfl_xor_sync(0xffffffffu, lmin[k], off));
+            lmax[k] = max(lmax[k], __shfl_xor_sync(0xffffffffu, lmax[k], off));
+        }
+    }
+    if ((threadIdx.x & 31) == 0) {
+        for (int k = 0; k < 3; ++k) {
+            atomicMin(cbounds + k, lmin[k]);
+            atomicMax(cbounds + 3 + k, lmax[k]);
+        }
+    }
+}
+
+__device__ __forceinline__ uint64_t spread21(uint32_t x)
+{
+    uint64_t v = x & 0x1fffffu;
+    v = (v | (v << 32)) & 0x1f00000000ffffull;
+    v = (v | (v << 16)) & 0x1f0000ff0000ffull;
+    v = (v | (v << 8)) & 0x100f00f00f00f00full;
+    v = (v | (v << 4)) & 0x10c30c30c30c30c3ull;
+    v = (v | (v << 2)) & 0x1249249249249249ull;
+    return v;
+}
+
+__global__ void k_morton(uint32_t n, const float4* box_lo, const float4* box_hi,
+                         const uint32_t* cbounds, uint64_t* keys, uint32_t* vals)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    float4 lo = box_lo[i], hi = box_hi[i];
+    uint64_t key = ~0ull;
+    if (lo.x <= hi.x) {
+        float c[3] = {0.5f * (lo.x + hi.x), 0.5f * (lo.y + hi.y), 0.5f * (lo.z + hi.z)};
+        uint32_t q[3];
+        for (int k = 0; k < 3; ++k) {
+            float mn = o2f(cbounds[k]), mx = o2f(cbounds[3 + k]);
+            float ext = mx - mn;
+            float u = ext > 0.0f ? (c[k] - mn) / ext : 0.5f;
+            u = fminf(fmaxf(u, 0.0f), 1.0f);
+            q[k] = min(uint32_t(u * 2097152.0f), 2097151u);
+        }
+        key = (spread21(q[0]) << 2) | (spread21(q[1]) << 1) | spread21(q[2]);
+    }
+    keys[i] = key;
+    vals[i] = i;
+}
+
+// common-prefix length of sorted keys i and j, with the index breaking ties (Karras 2012 sec 4)
+__device__ __forceinline__ int delta(const uint64_t* keys, uint32_t n, int i, int j)
+{
+    if (j < 0 || j >= int(n))
+        return -1;
+    uint64_t a = keys[i], b = keys[j];
+    if (a == b)
+        return 64 + __clz(uint32_t(i) ^ uint32_t(j));
+    return __clzll(a ^ b);
+}
+
+__global__ void k_karras(uint32_t n, const uint64_t* keys, int2* range, uint32_t* split,
+                         uint32_t* parent_int, uint32_t* parent_leaf)
+{
+    int i = int(blockIdx.x * blockDim.x + threadIdx.x);
+    if (i >= int(n) - 1)
+        return;
+    int d = (delta(keys, n, i, i + 1) - delta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
+    int dmin = delta(keys, n, i, i - d);
+    int lmax = 2;
+    while (delta(keys, n, i, i + lmax * d) > dmin)
+        lmax <<= 1;
+    int l = 0;
+    for (int t = lmax >> 1; t >= 1; t >>= 1)
+        if (delta(keys, n, i, i + (l + t) * d) > dmin)
+            l += t;
+    int j = i + l * d;
+    int dnode = delta(keys, n, i, j);
+    int s = 0;
+    for (int div = 2;; div <<= 1) {
+        int t = (l + div - 1) / div;
+        if (delta(keys, n, i, i + (s + t) * d) > dnode)
+            s += t;
+        if (t == 1)
+            break;
+    }
+    int gamma = i + s * d + min(d, 0);
+    int first = min(i, j), last = max(i, j);
+    range[i] = make_int2(first, last);
+    split[i] = uint32_t(gamma);
+    // children: gamma (leaf if first == gamma) and gamma + 1 (leaf if last == gamma + 1)
+    if (first == gamma)
+        parent_leaf[gamma] = uint32_t(i);
+    else
+        parent_int[gamma] = uint32_t(i);
+    if (last == gamma + 1)
+        parent_leaf[gamma + 1] = uint32_t(i);
+    else
+        parent_int[gamma + 1] = uint32_t(i);
+}
+
+__device__ __forceinline__ float half_area(float3 lo, float3 hi)
+{
+    float dx = hi.x - lo.x, dy = hi.y - lo.y, dz = hi.z - lo.z;
+    if (!(dx >= 0.0f) || !(dy >= 0.0f) || !(dz >= 0.0f))
+        return 0.0f;
+    return dx * dy + dy * dz + dz * dx;
+}
+
+struct NodeInfo {  // per internal node, written by the refit pass
+    float4 lo, hi;  // lo.w = SAH cost, hi.w = primitive count (as float)
+};
+
+// Bottom-up: one thread per leaf; the second thread to arrive at a node unions its children.
+__global__ void k_refit(uint32_t n, const uint32_t* sorted_vals, const float4* box_lo,
+                        const float4* box_hi, const int2* range, const uint32_t* split,
+                        const uint32_t* parent_int, const uint32_t* parent_leaf, uint32_t* arrive,
+                        NodeInfo* info, uint8_t* collapse, int leaf_max, float c_trav,
+                        float c_isect)
+{
+    uint32_t leaf = blockIdx.x * blockDim.x + threadIdx.x;
+    if (leaf >= n || n < 2)
+        return;
+    uint32_t node = parent_leaf[leaf];
+    while (true) {
+        __threadfence();
+        if (atomicAdd(arrive + node, 1u) == 0u)
+            return;
+        __threadfence();
+        uint32_t g = split[node];
+        int2 rg = range[node];
+        float4 lo[2], hi[2];
+        float cost[2];
+        float cnt[2];
+        for (int c = 0; c < 2; ++c) {
+            uint32_t idx = g + uint32_t(c);
+            bool is_leaf = (c == 0) ? (uint32_t(rg.x) == g) : (uint32_t(rg.y) == g + 1);
+            if (is_leaf) {
+                uint32_t p = sorted_vals[idx];
+                lo[c] = box_lo[p];
+                hi[c] = box_hi[p];
+                float a = half_area(make_float3(lo[c].x, lo[c].y, lo[c].z),
+                                    make_float3(hi[c].x, hi[c].y, hi[c].z));
+                cost[c] = c_isect * a;
+                cnt[c] = 1.0f;
+            } else {
+                NodeInfo ci;
+                ci.lo = __ldcg(&info[idx].lo);
+                ci.hi = __ldcg(&info[idx].hi);
+                lo[c] = ci.lo;
+                hi[c] = ci.hi;
+                cost[c] = ci.lo.w;
+                cnt[c] = ci.hi.w;
+            }
+        }
+        float3 ulo = f3min(make_float3(lo[0].x, lo[0].y, lo[0].z), make_float3(lo[1].x, lo[1].y, lo[1].z));
+        float3 uhi = f3max(make_float3(hi[0].x, hi[0].y, hi[0].z), make_float3(hi[1].x, hi[1].y, hi[1].z));
+        float a = half_area(ulo, uhi);
+        float count = cnt[0] + cnt[1];
+        float split_cost = c_trav * a + cost[0] + cost[1];
+        float leaf_cost = c_isect * a * count;
+        bool col = (count <= float(leaf_max)) && (leaf_cost <= split_cost);
+        NodeInfo out;
+        out.lo = make_float4(ulo.x, ulo.y, ulo.z, col ? leaf_cost : split_cost);
+        out.hi = make_float4(uhi.x, uhi.y, uhi.z, count);
+        __stcg(&info[node].lo, out.lo);
+        __stcg(&info[node].hi, out.hi);
+        collapse[node] = col ? 1 : 0;
+        if (node == 0)
+            return;
+        node = parent_int[node];
+    }
+}
+
+// An internal node survives as an interior node of the output tree iff it is not collapsed
+// and no ancestor is collapsed.  keep[gamma] marks the child pair owned by that node.
+__global__ void k_mark(uint32_t n, const uint32_t* split, const uint32_t* parent_int,
+                       const uint8_t* collapse, uint32_t* keep, uint32_t* removed)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1)
+        return;
+    bool rem = false;
+    uint32_t a = i;
+    for (int guard = 0; a != 0 && guard < 4096; ++guard) {
+        a = parent_int[a];
+        if (collapse[a]) {
+            rem = true;
+            break;
+        }
+    }
+    removed[i] = rem ? 1u : 0u;
+    keep[split[i]] = (!rem && !collapse[i]) ? 1u : 0u;
+}
+
+__device__ __forceinline__ void write_node(float4* nodes, uint32_t slot, float4 lo, float4 hi,
+                                           uint32_t a, uint32_t b)
+{
+    nodes[2 * size_t(slot)] = make_float4(lo.x, lo.y, lo.z, __uint_as_float(a));
+    nodes[2 * size_t(slot) + 1] = make_float4(hi.x, hi.y, hi.z, __uint_as_float(b));
+}
+
+__global__ void k_emit(uint32_t n, const int2* range, const uint32_t* split,
+                       const uint8_t* collapse, const uint32_t* removed, const uint32_t* pair_index,
+                       const NodeInfo* info, const uint32_t* sorted_vals, const float4* box_lo,
+                       const float4* box_hi, float4* nodes)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1 || removed[i])
+        return;
+    if (i == 0) {  // root
+        int2 rg = range[0];
+        if (collapse[0])
+            write_node(nodes, 0, info[0].lo, info[0].hi, uint32_t(rg.x), uint32_t(rg.y - rg.x + 1));
+        else
+            write_node(nodes, 0, info[0].lo, info[0].hi, 1u + 2u * pair_index[split[0]], 0u);
+    }
+    if (collapse[i])
+        return;
+    uint32_t g = split[i];
+    int2 rg = range[i];
+    uint32_t base = 1u + 2u * pair_index[g];
+    for (int c = 0; c < 2; ++c) {
+        uint32_t idx = g + uint32_t(c);
+        bool is_leaf = (c == 0) ? (uint32_t(rg.x) == g) : (uint32_t(rg.y) == g + 1);
+        if (is_leaf) {
+            uint32_t p = sorted_vals[idx];
+            write_node(nodes, base + c, box_lo[p], box_hi[p], idx, 1u);
+        } else if (collapse[idx]) {
+            int2 cr = range[idx];
+            write_node(nodes, base + c, info[idx].lo, info[idx].hi, uint32_t(cr.x),
+                       uint32_t(cr.y - cr.x + 1));
+        } else {
+            write_node(nodes, base + c, info[idx].lo, info[idx].hi, 1u + 2u * pair_index[split[idx]],
+                       0u);
+        }
+    }
+}
+
+__global__ void k_single_leaf(const float4* box_lo, const float4* box_hi, float4* nodes)
+{
+    write_node(nodes, 0, box_lo[0], box_hi[0], 0u, 1u);
+}
+
+// Leaf-ordered copies of the primitive data the intersection loop reads.
+__global__ void k_gather(BuildInput in, uint32_t n, const uint32_t* sorted_vals, float4* leaf_data,
+                         uint32_t* order)
+{
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n)
+        return;
+    uint32_t p = sorted_vals[s];
+    order[s] = p;
+    switch (in.type) {
+    case FR_GEOM_SPHERE: {
+        V3 c = load3(in.position, p);
+        leaf_data[s] = make_float4(c.x, c.y, c.z, in.radius[p]);
+        break;
+    }
+    case FR_GEOM_CYLINDER: {
+        V3 A = load3(in.points, 2 * p), B = load3(in.points, 2 * p + 1);
+        leaf_data[2 * s] = make_float4(A.x, A.y, A.z, in.radius[p]);
+        leaf_data[2 * s + 1] = make_float4(B.x, B.y, B.z, 0.0f);
+        break;
+    }
+    case FR_GEOM_POLYHEDRON: {
+        V3 c = load3(in.position, p);
+        Qt q = loadq(in.orientation, p);
+        leaf_data[2 * s] = make_float4(c.x, c.y, c.z, 0.0f);
+        leaf_data[2 * s + 1] = make_float4(q.s, q.v.x, q.v.y, q.v.z);
+        break;
+    }
+    default: {
+        uint32_t inst = p / in.n_faces, face = p - inst * in.n_faces;
+        V3 c = load3(in.position, inst);
+        Qt q = loadq(in.orientation, inst);
+        leaf_data[2 * s] = make_float4(c.x, c.y, c.z, __uint_as_float(face));
+        leaf_data[2 * s + 1] = make_float4(q.s, q.v.x, q.v.y, q.v.z);
+        break;
+    }
+    }
+}
+
+inline uint32_t blocks_for(size_t n, int threads) { return uint32_t((n + threads - 1) / threads); }
+
+}  // namespace
+
+size_t leaf_record_float4s(int type) { return type == FR_GEOM_SPHERE ? 1 : 2; }
+
+cudaError_t build_bvh(const BuildInput& in, uint32_t n, const BuildParams& bp, BvhBuffers& out,
+                      Scratch& scratch, cudaStream_t st)
+{
+    out.n_nodes = 0;
+    if (n == 0)
+        return cudaSuccess;
+    const int T = 256;
+    const size_t rec = leaf_record_float4s(in.type);
+    // persistent outputs
+    cudaError_t e;
+    if ((e = out.nodes.reserve(size_t(2) * (2 * size_t(n) - 1))) != cudaSuccess)
+        return e;
+    if ((e = out.leaf_data.reserve(rec * n)) != cudaSuccess)
+        return e;
+    if ((e = out.order.reserve(n)) != cudaSuccess)
+        return e;
+
+    // scratch carve-up
+    size_t sort_bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (uint64_t*)nullptr, (uint64_t*)nullptr,
+                                    (uint32_t*)nullptr, (uint32_t*)nullptr, int(n), 0, 63, st);
+    size_t scan_bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (uint32_t*)nullptr, (uint32_t*)nullptr,
+                                  int(n), st);
+    ScratchLayout L;
+    float4* box_lo = L.take<float4>(n);
+    float4* box_hi = L.take<float4>(n);
+    uint64_t* keys = L.take<uint64_t>(n);
+    uint64_t* keys_sorted = L.take<uint64_t>(n);
+    uint32_t* vals = L.take<uint32_t>(n);
+    uint32_t* vals_sorted = L.take<uint32_t>(n);
+    int2* range = L.take<int2>(n);
+    uint32_t* split = L.take<uint32_t>(n);
+    uint32_t* parent_int = L.take<uint32_t>(n);
+    uint32_t* parent_leaf = L.take<uint32_t>(n);
+    uint32_t* arrive = L.take<uint32_t>(n);
+    NodeInfo* info = L.take<NodeInfo>(n);
+    uint8_t* collapse = L.take<uint8_t>(n);
+    uint32_t* keep = L.take<uint32_t>(n);
+    uint32_t* removed = L.take<uint32_t>(n);
+    uint32_t* pair_index = L.take<uint32_t>(n);
+    uint32_t* cbounds = L.take<uint32_t>(8);
+    uint8_t* cub_tmp = L.take<uint8_t>(sort_bytes > scan_bytes ? sort_bytes : scan_bytes);
+    if ((e = scratch.reserve(L.bytes)) != cudaSuccess)
+        return e;
+    L.bind(scratch.ptr);
+#define FR_RELOC(p) p = L.at(p)
+    FR_RELOC(box_lo);
+    FR_RELOC(box_hi);
+    FR_RELOC(keys);
+    FR_RELOC(keys_sorted);
+    FR_RELOC(vals);
+    FR_RELOC(vals_sorted);
+    FR_RELOC(range);
+    FR_RELOC(split);
+    FR_RELOC(parent_int);
+    FR_RELOC(parent_leaf);
+    FR_RELOC(arrive);
+    FR_RELOC(info);
+    FR_RELOC(collapse);
+    FR_RELOC(keep);
+    FR_RELOC(removed);
+    FR_RELOC(pair_index);
+    FR_RELOC(cbounds);
+    FR_RELOC(cub_tmp);
+#undef FR_RELOC
+
+    // centroid bounds: min slots start at 0xff.., max slots at 0
+    if ((e = cudaMemsetAsync(cbounds, 0xff, 3 * sizeof(uint32_t), st)) != cudaSuccess)
+        return e;
+    if ((e = cudaMemsetAsync(cbounds + 3, 0, 3 * sizeof(uint32_t), st)) != cudaSuccess)
+        return e;
+    uint32_t gb = blocks_for(n, T);
+    if (gb > 4096)
+        gb = 4096;
+    k_bounds<<<gb, T, 0, st>>>(in, n, box_lo, box_hi, cbounds);
+    k_morton<<<blocks_for(n, T), T, 0, st>>>(n, box_lo, box_hi, cbounds, keys, vals);
+    size_t tmp_bytes = sort_bytes;
+    if ((e = cub::DeviceRadixSort::SortPairs(cub_tmp, tmp_bytes, keys, keys_sorted, vals,
+                                             vals_sorted, int(n), 0, 63, st)) != cudaSuccess)
+        return e;
+    if (n == 1) {
+        k_single_leaf<<<1, 1, 0, st>>>(box_lo, box_hi, out.nodes.ptr);
+        out.n_nodes = 1;
+    } else {
+        k_karras<<<blocks_for(n - 1, T), T, 0, st>>>(n, keys_sorted, range, split, parent_int,
+                                                    parent_leaf);
+        if ((e = cudaMemsetAsync(arrive, 0, n * sizeof(uint32_t), st)) != cudaSuccess)
+            return e;
+        k_refit<<<blocks_for(n, T), T, 0, st>>>(n, vals_sorted, box_lo, box_hi, range, split,
+                                                parent_int, parent_leaf, arrive, info, collapse,
+                                                bp.leaf_max, bp.c_trav, bp.c_isect);
+        if ((e = cudaMemsetAsync(keep, 0, n * sizeof(uint32_t), st)) != cudaSuccess)
+            return e;
+        k_mark<<<blocks_for(n - 1, T), T, 0, st>>>(n, split, parent_int, collapse, keep, removed);
+        tmp_bytes = scan_bytes;
+        if ((e = cub::DeviceScan::ExclusiveSum(cub_tmp, tmp_bytes, keep, pair_index, int(n),
+                                               st)) != cudaSuccess)
+            return e;
+        k_emit<<<blocks_for(n - 1, T), T, 0, st>>>(n, range, split, collapse, removed, pair_index,
+                                                   info, vals_sorted, box_lo, box_hi,
+                                                   out.nodes.ptr);
+        // node count = 1 + 2 * (number of kept pairs) = 1 + 2 * (pair_index[n-1] + keep[n-1])
+        uint32_t tail[2];
+        if ((e = cudaMemcpyAsync(tail, pair_index + (n - 1), sizeof(uint32_t),
+                                 cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+            return e;
+        if ((e = cudaMemcpyAsync(tail + 1, keep + (n - 1), sizeof(uint32_t),
+                                 cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+            return e;
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess)
+            return e;
+        out.n_nodes = 1u + 2u * (tail[0] + tail[1]);
+    }
+    k_gather<<<blocks_for(n, T), T, 0, st>>>(in, n, vals_sorted, out.leaf_data.ptr, out.order.ptr);
+    return cudaGetLastError();
+}
+
+}  // namespace fr

@@ -1,0 +1,109 @@
+// bvh.hpp -- device buffers and the LBVH builder's host interface.
+#ifndef FR_BVH_HPP
+#define FR_BVH_HPP
+
+#include <cstddef>
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace fr {
+
+// A growable device allocation: reserve() only reallocates when the request exceeds capacity.
+template <class T> struct DevArray {
+    T* ptr = nullptr;
+    size_t cap = 0;  // elements
+    cudaError_t reserve(size_t n)
+    {
+        if (n <= cap)
+            return cudaSuccess;
+        release();
+        if (n == 0)
+            return cudaSuccess;
+        cudaError_t e = cudaMalloc((void**)&ptr, n * sizeof(T));
+        if (e != cudaSuccess) {
+            ptr = nullptr;
+            cap = 0;
+            return e;
+        }
+        cap = n;
+        return cudaSuccess;
+    }
+    void release()
+    {
+        if (ptr)
+            cudaFree(ptr);
+        ptr = nullptr;
+        cap = 0;
+    }
+    DevArray() = default;
+    DevArray(const DevArray&) = delete;
+    DevArray& operator=(const DevArray&) = delete;
+    ~DevArray() { release(); }
+};
+
+// Byte scratch shared by the builds of one device.
+struct Scratch {
+    DevArray<unsigned char> buf;
+    void* ptr = nullptr;
+    cudaError_t reserve(size_t bytes)
+    {
+        cudaError_t e = buf.reserve(bytes);
+        ptr = buf.ptr;
+        return e;
+    }
+};
+
+// Carves typed, 256-byte aligned sub-arrays out of one scratch block: take() records offsets
+// (returned as pointers relative to address 0), bind() sets the base, at() relocates.
+struct ScratchLayout {
+    size_t bytes = 0;
+    char* base = nullptr;
+    template <class T> T* take(size_t n)
+    {
+        bytes = (bytes + 255) & ~size_t(255);
+        T* off = reinterpret_cast<T*>(bytes);
+        bytes += n * sizeof(T);
+        return off;
+    }
+    void bind(void* b) { base = static_cast<char*>(b); }
+    template <class T> T* at(T* off) const
+    {
+        return reinterpret_cast<T*>(base + reinterpret_cast<size_t>(off));
+    }
+};
+
+struct BuildInput {
+    int type;  // FR_GEOM_*
+    const float* position;
+    const float* radius;
+    const float* points;
+    const float* orientation;
+    const float* vertices;
+    uint32_t n_faces;
+    float poly_radius;
+};
+
+struct BuildParams {
+    int leaf_max = 4;      // largest leaf the SAH collapse may form
+    float c_trav = 1.0f;   // cost of one child-pair visit, in units of one primitive test
+    float c_isect = 1.0f;
+};
+
+struct BvhBuffers {
+    DevArray<float4> nodes;      // 2 float4 per node
+    DevArray<float4> leaf_data;  // leaf_record_float4s(type) per primitive
+    DevArray<uint32_t> order;    // leaf slot -> primitive index
+    uint32_t n_nodes = 0;
+};
+
+size_t leaf_record_float4s(int type);
+
+// Build the BVH of n primitives (n == 0 leaves an empty tree).  Synchronises the stream once
+// to read back the node count.
+cudaError_t build_bvh(const BuildInput& in, uint32_t n, const BuildParams& bp, BvhBuffers& out,
+                      Scratch& scratch, cudaStream_t st);
+
+}  // namespace fr
+
+#endif

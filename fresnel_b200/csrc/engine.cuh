@@ -1,0 +1,479 @@
+// engine.cuh -- device-side scene layout and closest-hit traversal.
+//
+// Layout in HBM, per geometry:
+//   nodes      BVH2 nodes of 32 bytes, two float4 each: (lo.xyz, a) and (hi.xyz, b).
+//              Interior nodes have b == 0 and their two children at a and a+1, so one 64-byte
+//              load fetches both child boxes; leaves have b == primitive count and a == first
+//              slot.  Node 0 is the root.
+//   leaf_data  primitives in BVH leaf order, packed for the intersection loop
+//              (sphere: 1 float4 (x,y,z,r); cylinder: (A,r),(B,-); polyhedron: (p,-),(quat);
+//              mesh: (p, face bits),(quat)).
+//   order      leaf slot -> primitive index of the user's arrays.
+//   position/radius/color/... the user's arrays (read only when shading a hit).
+// A scene is an array of GeomDev records; every ray traverses the BVH of each enabled
+// geometry in turn, carrying its closest t so far (the reference puts all geometries in one
+// Embree/OptiX acceleration structure; the closest hit is the same).
+#ifndef FR_ENGINE_CUH
+#define FR_ENGINE_CUH
+
+#include <cstdint>
+
+#include "fresnel_b200.h"
+#include "frmath.cuh"
+
+namespace fr {
+
+constexpr int TRAVERSAL_STACK = 64;
+constexpr uint32_t MISS = 0xFFFFFFFFu;
+
+// error bits reported through the device status word
+constexpr uint32_t ERR_STACK_OVERFLOW = 1u;
+constexpr uint32_t ERR_ITERATION_CAP = 2u;
+
+struct GeomDev {
+    int32_t type;
+    int32_t enabled;
+    uint32_t n_prims;  // BVH primitives (mesh: instances * faces)
+    uint32_t n_nodes;
+    const float4* nodes;
+    const float4* leaf_data;
+    const uint32_t* order;
+    const float* position;
+    const float* radius;
+    const float* color;
+    const float* points;
+    const float* orientation;
+    const float* vertices;
+    const float* planes;  // [n_planes][9]: origin, unit normal, colour
+    uint32_t n_faces;
+    uint32_t n_planes;
+    float color_by_face;
+    float outline_width;
+    Mat material;
+    Mat outline;
+};
+
+struct SceneDev {
+    const GeomDev* geoms;
+    uint32_t n_geoms;
+    uint32_t* status;  // error bits (device)
+};
+
+// --------------------------------------------------------------------------------------------
+// loads
+// --------------------------------------------------------------------------------------------
+__device__ __forceinline__ float4 ldg4(const float4* p) { return __ldg(p); }
+
+__device__ __forceinline__ V3 load3(const float* a, uint32_t i)
+{
+    return v3(__ldg(a + 3 * i), __ldg(a + 3 * i + 1), __ldg(a + 3 * i + 2));
+}
+
+__device__ __forceinline__ C3 loadc3(const float* a, uint32_t i)
+{
+    return c3(__ldg(a + 3 * i), __ldg(a + 3 * i + 1), __ldg(a + 3 * i + 2));
+}
+
+__device__ __forceinline__ Qt loadq(const float* a, uint32_t i)
+{
+    return Qt{__ldg(a + 4 * i), v3(__ldg(a + 4 * i + 1), __ldg(a + 4 * i + 2), __ldg(a + 4 * i + 3))};
+}
+
+// --------------------------------------------------------------------------------------------
+// ray/box slab test with precomputed reciprocal direction (boxes are inflated at build time,
+// so the single rounding of each fused multiply-add cannot cull a primitive that the exact
+// intersector accepts)
+// --------------------------------------------------------------------------------------------
+struct RayK {
+    V3 o, d;
+    V3 inv, oinv;  // 1/d and -o/d
+};
+
+__device__ __forceinline__ RayK make_rayk(V3 o, V3 d)
+{
+    RayK r;
+    r.o = o;
+    r.d = d;
+    auto safe_inv = [](float x) {
+        float ax = fabsf(x);
+        return 1.0f / (ax < 1e-30f ? copysignf(1e-30f, x) : x);
+    };
+    r.inv = v3(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
+    r.oinv = v3(-o.x * r.inv.x, -o.y * r.inv.y, -o.z * r.inv.z);
+    return r;
+}
+
+__device__ __forceinline__ bool slab(const RayK& r, float4 lo, float4 hi, float tmax, float& tentry)
+{
+    float tx0 = fmaf(lo.x, r.inv.x, r.oinv.x), tx1 = fmaf(hi.x, r.inv.x, r.oinv.x);
+    float ty0 = fmaf(lo.y, r.inv.y, r.oinv.y), ty1 = fmaf(hi.y, r.inv.y, r.oinv.y);
+    float tz0 = fmaf(lo.z, r.inv.z, r.oinv.z), tz1 = fmaf(hi.z, r.inv.z, r.oinv.z);
+    float t0 = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), 0.0f));
+    float t1 = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tmax));
+    tentry = t0;
+    return t0 <= t1;
+}
+
+// --------------------------------------------------------------------------------------------
+// per-type leaf tests: update (tmax, hit) when a primitive is accepted with tnear < t < tmax
+// (the acceptance rule of fresnel/cpu/Geometry*.cc).  Only t is computed here; the shading
+// quantities are recomputed for the one closest hit (hit_surface below).
+// --------------------------------------------------------------------------------------------
+struct PolyHit {
+    bool hit;
+    float t;
+    int plane;
+    V3 n, p;  // local-frame normal and origin of the hit plane
+    V3 ol, dl;
+};
+
+// slab test over the face planes (fresnel/cpu/GeometryConvexPolyhedron.cc:146-224)
+__device__ __forceinline__ PolyHit poly_planes(const GeomDev& g, V3 o, V3 d, V3 pos, Qt q,
+                                               float tnear, float tfar)
+{
+    PolyHit r;
+    r.hit = false;
+    float t0 = -3.402823466e+38f, t1 = 3.402823466e+38f;
+    V3 dl = rotate(conj(q), d);
+    V3 ol = rotate(conj(q), o - pos);
+    r.ol = ol;
+    r.dl = dl;
+    V3 t0n = v3(0, 0, 0), t0p = v3(0, 0, 0), t1n = v3(0, 0, 0), t1p = v3(0, 0, 0);
+    int t0_plane = 0, t1_plane = 0;
+    for (uint32_t i = 0; i < g.n_planes && t0 < t1; ++i) {
+        const float* pl = g.planes + 9 * i;
+        V3 p = v3(__ldg(pl), __ldg(pl + 1), __ldg(pl + 2));
+        V3 n = v3(__ldg(pl + 3), __ldg(pl + 4), __ldg(pl + 5));
+        float dd = -dot(n, p);
+        float denom = dot(n, dl);
+        float t = -(dd + dot(n, ol)) / denom;
+        if (double(fabsf(denom)) < 1e-5) {
+            if (dot(ol - p, n) > 0)
+                return r;
+        } else if (denom < 0) {
+            if (t > t0) {
+                t0 = t;
+                t0n = n;
+                t0p = p;
+                t0_plane = int(i);
+            }
+        } else {
+            if (t < t1) {
+                t1 = t;
+                t1n = n;
+                t1p = p;
+                t1_plane = int(i);
+            }
+        }
+    }
+    if (t0 > t1)
+        return r;
+    if ((tnear < t0) & (t0 < tfar)) {
+        r.hit = true;
+        r.t = tfar = t0;
+        r.n = t0n;
+        r.p = t0p;
+        r.plane = t0_plane;
+    }
+    if ((tnear < t1) & (t1 < tfar)) {
+        r.hit = true;
+        r.t = tfar = t1;
+        r.n = t1n;
+        r.p = t1p;
+        r.plane = t1_plane;
+    }
+    return r;
+}
+
+// double-sided instanced triangle (fresnel/cpu/GeometryMesh.cc:115-166)
+struct TriHit {
+    bool hit;
+    float u, v, w, t, d;
+    V3 n;
+};
+
+__device__ __forceinline__ TriHit mesh_triangle(const GeomDev& g, uint32_t face, V3 o, V3 d, V3 pos,
+                                                Qt q)
+{
+    TriHit r;
+    V3 dl = rotate(conj(q), d);
+    V3 ol = rotate(conj(q), o - pos);
+    V3 v0 = load3(g.vertices, 3 * face), v1 = load3(g.vertices, 3 * face + 1),
+       v2 = load3(g.vertices, 3 * face + 2);
+    r.u = r.v = r.w = r.t = r.d = 0.0f;
+    r.n = v3(0, 0, 0);
+    V3 q2 = ol + dl;
+    r.hit = isect_triangle(r.u, r.v, r.w, r.t, r.d, r.n, ol, q2, v0, v1, v2)
+            || isect_triangle(r.v, r.u, r.w, r.t, r.d, r.n, ol, q2, v1, v0, v2);
+    return r;
+}
+
+template <int TYPE>
+__device__ __forceinline__ void leaf_test(const GeomDev& g, uint32_t gi, const RayK& ray,
+                                          uint32_t first, uint32_t count, float tnear,
+                                          float& tmax, uint32_t& hit_geom, uint32_t& hit_slot)
+{
+    for (uint32_t s = first; s < first + count; ++s) {
+        float t = 0.0f;
+        bool ok;
+        if (TYPE == FR_GEOM_SPHERE) {
+            float4 q = ldg4(g.leaf_data + s);
+            ok = sphere_t(ray.o, ray.d, v3(q.x, q.y, q.z), q.w, t);
+        } else if (TYPE == FR_GEOM_CYLINDER) {
+            float4 a = ldg4(g.leaf_data + 2 * s), b = ldg4(g.leaf_data + 2 * s + 1);
+            float de;
+            V3 N;
+            uint32_t ci;
+            ok = isect_spherocylinder(t, de, N, ci, ray.o, ray.d, v3(a.x, a.y, a.z),
+                                      v3(b.x, b.y, b.z), a.w);
+        } else if (TYPE == FR_GEOM_POLYHEDRON) {
+            float4 a = ldg4(g.leaf_data + 2 * s), b = ldg4(g.leaf_data + 2 * s + 1);
+            PolyHit ph = poly_planes(g, ray.o, ray.d, v3(a.x, a.y, a.z), Qt{b.x, v3(b.y, b.z, b.w)},
+                                     tnear, tmax);
+            ok = ph.hit;
+            t = ph.t;
+        } else {
+            float4 a = ldg4(g.leaf_data + 2 * s), b = ldg4(g.leaf_data + 2 * s + 1);
+            TriHit th = mesh_triangle(g, __float_as_uint(a.w), ray.o, ray.d, v3(a.x, a.y, a.z),
+                                      Qt{b.x, v3(b.y, b.z, b.w)});
+            ok = th.hit;
+            t = th.t;
+        }
+        if (ok && (tnear < t) && (t < tmax)) {
+            tmax = t;
+            hit_geom = gi;
+            hit_slot = s;
+        }
+    }
+}
+
+// Closest hit in one geometry's BVH (stack-light: a 64-entry per-thread stack of child pairs
+// with their entry distances, near child first, leaves tested as soon as their box is hit).
+template <int TYPE>
+__device__ __forceinline__ void traverse(const GeomDev& g, uint32_t gi, const RayK& ray, float tnear,
+                                         float& tmax, uint32_t& hit_geom, uint32_t& hit_slot,
+                                         uint32_t* status)
+{
+    if (g.n_nodes == 0)
+        return;
+    float te;
+    float4 rlo = ldg4(g.nodes), rhi = ldg4(g.nodes + 1);
+    if (!slab(ray, rlo, rhi, tmax, te))
+        return;
+    uint32_t rb = __float_as_uint(rhi.w);
+    if (rb != 0) {
+        leaf_test<TYPE>(g, gi, ray, __float_as_uint(rlo.w), rb, tnear, tmax, hit_geom, hit_slot);
+        return;
+    }
+    uint32_t stack_node[TRAVERSAL_STACK];
+    float stack_t[TRAVERSAL_STACK];
+    int sp = 0;
+    uint32_t cur = __float_as_uint(rlo.w);
+    uint32_t guard = 2u * g.n_nodes + 8u;
+    while (true) {
+        if (--guard == 0u) {
+            atomicOr(status, ERR_ITERATION_CAP);
+            return;
+        }
+        const float4* np = g.nodes + 2 * size_t(cur);
+        float4 alo = ldg4(np), ahi = ldg4(np + 1), blo = ldg4(np + 2), bhi = ldg4(np + 3);
+        float ta, tb;
+        bool ha = slab(ray, alo, ahi, tmax, ta);
+        bool hb = slab(ray, blo, bhi, tmax, tb);
+        uint32_t ca = __float_as_uint(ahi.w), cb = __float_as_uint(bhi.w);
+        if (ha && ca != 0) {
+            leaf_test<TYPE>(g, gi, ray, __float_as_uint(alo.w), ca, tnear, tmax, hit_geom, hit_slot);
+            ha = false;
+        }
+        if (hb && cb != 0) {
+            if (tb <= tmax)
+                leaf_test<TYPE>(g, gi, ray, __float_as_uint(blo.w), cb, tnear, tmax, hit_geom,
+                                hit_slot);
+            hb = false;
+        }
+        if (ha && hb) {
+            uint32_t near_n = __float_as_uint(alo.w), far_n = __float_as_uint(blo.w);
+            float far_t = tb;
+            if (tb < ta) {
+                near_n = __float_as_uint(blo.w);
+                far_n = __float_as_uint(alo.w);
+                far_t = ta;
+            }
+            if (sp < TRAVERSAL_STACK) {
+                stack_node[sp] = far_n;
+                stack_t[sp] = far_t;
+                ++sp;
+            } else {
+                atomicOr(status, ERR_STACK_OVERFLOW);
+            }
+            cur = near_n;
+            continue;
+        }
+        if (ha) {
+            cur = __float_as_uint(alo.w);
+            continue;
+        }
+        if (hb) {
+            cur = __float_as_uint(blo.w);
+            continue;
+        }
+        bool found = false;
+        while (sp > 0) {
+            --sp;
+            if (stack_t[sp] <= tmax) {
+                cur = stack_node[sp];
+                found = true;
+                break;
+            }
+        }
+        if (!found)
+            return;
+    }
+}
+
+struct Hit {
+    uint32_t geom;  // MISS if none
+    uint32_t prim;  // index into the geometry's user arrays
+};
+
+// Closest hit over all enabled geometries of the scene.
+__device__ __forceinline__ Hit trace_closest(const SceneDev& sc, V3 o, V3 d, float tnear)
+{
+    RayK ray = make_rayk(o, d);
+    float tmax = __int_as_float(0x7f800000);  // +inf
+    uint32_t hg = MISS, hs = 0;
+    for (uint32_t gi = 0; gi < sc.n_geoms; ++gi) {
+        const GeomDev& g = sc.geoms[gi];
+        if (!g.enabled)
+            continue;
+        switch (g.type) {
+        case FR_GEOM_SPHERE:
+            traverse<FR_GEOM_SPHERE>(g, gi, ray, tnear, tmax, hg, hs, sc.status);
+            break;
+        case FR_GEOM_CYLINDER:
+            traverse<FR_GEOM_CYLINDER>(g, gi, ray, tnear, tmax, hg, hs, sc.status);
+            break;
+        case FR_GEOM_POLYHEDRON:
+            traverse<FR_GEOM_POLYHEDRON>(g, gi, ray, tnear, tmax, hg, hs, sc.status);
+            break;
+        default:
+            traverse<FR_GEOM_MESH>(g, gi, ray, tnear, tmax, hg, hs, sc.status);
+            break;
+        }
+    }
+    Hit h;
+    h.geom = hg;
+    h.prim = (hg == MISS) ? 0u : __ldg(sc.geoms[hg].order + hs);
+    return h;
+}
+
+// --------------------------------------------------------------------------------------------
+// shading quantities of the closest hit (what the reference's intersect callbacks leave in
+// RTCHit::Ng, FresnelRTCIntersectContext::shading_color and ::d)
+// --------------------------------------------------------------------------------------------
+struct Surface {
+    float t;
+    V3 Ng;
+    C3 color;
+    float d_edge;
+};
+
+__device__ __forceinline__ Surface hit_surface(const GeomDev& g, uint32_t prim, V3 o, V3 d,
+                                               float tnear)
+{
+    Surface s;
+    s.t = 0.0f;
+    s.Ng = v3(0, 0, 1);
+    s.color = c3(0, 0, 0);
+    s.d_edge = 0.0f;
+    switch (g.type) {
+    case FR_GEOM_SPHERE: {  // fresnel/cpu/GeometrySphere.cc:81-118
+        V3 p = load3(g.position, prim);
+        float r = __ldg(g.radius + prim);
+        V3 N;
+        isect_sphere(s.t, s.d_edge, N, o, d, p, r);
+        s.Ng = v3(o.x + s.t * d.x - p.x, o.y + s.t * d.y - p.y, o.z + s.t * d.z - p.z);
+        s.color = loadc3(g.color, prim);
+        break;
+    }
+    case FR_GEOM_CYLINDER: {  // fresnel/cpu/GeometryCylinder.cc:76-120
+        V3 A = load3(g.points, 2 * prim), B = load3(g.points, 2 * prim + 1);
+        float r = __ldg(g.radius + prim);
+        uint32_t ci = 0;
+        float t = HUGE_VALF, de = HUGE_VALF;
+        V3 N = v3(0, 0, 0);
+        isect_spherocylinder(t, de, N, ci, o, d, A, B, r);
+        s.t = t;
+        s.d_edge = de;
+        s.Ng = N;
+        s.color = loadc3(g.color, 2 * prim + ci);
+        break;
+    }
+    case FR_GEOM_POLYHEDRON: {  // fresnel/cpu/GeometryConvexPolyhedron.cc:226-335
+        V3 pos = load3(g.position, prim);
+        Qt q = loadq(g.orientation, prim);
+        PolyHit ph = poly_planes(g, o, d, pos, q, tnear, __int_as_float(0x7f800000));
+        s.t = ph.t;
+        s.Ng = rotate(q, ph.n);
+        const float* pl = g.planes + 9 * ph.plane;
+        s.color = lerp(g.color_by_face, loadc3(g.color, prim),
+                       c3(__ldg(pl + 6), __ldg(pl + 7), __ldg(pl + 8)));
+        float min_d = 3.402823466e+38f;
+        V3 r_hit = ph.ol + ph.t * ph.dl;
+        for (uint32_t i = 0; i < g.n_planes; ++i) {
+            const float* pi = g.planes + 9 * i;
+            V3 p = v3(__ldg(pi), __ldg(pi + 1), __ldg(pi + 2));
+            V3 n = v3(__ldg(pi + 3), __ldg(pi + 4), __ldg(pi + 5));
+            V3 u = cross(n, ph.n);
+            if (double(fabsf(dot(u, u))) >= 1e-5) {
+                int maxc;
+                if (fabsf(u.x) > fabsf(u.y))
+                    maxc = (fabsf(u.x) > fabsf(u.z)) ? 1 : 3;
+                else
+                    maxc = (fabsf(u.y) > fabsf(u.z)) ? 2 : 3;
+                V3 x0 = v3(0, 0, 0);
+                float d1 = -dot(n, p);
+                float d2 = -dot(ph.n, ph.p);
+                if (maxc == 1) {
+                    x0.y = (d2 * n.z - d1 * ph.n.z) / u.x;
+                    x0.z = (d1 * ph.n.y - d2 * n.y) / u.x;
+                } else if (maxc == 2) {
+                    x0.x = (d1 * ph.n.z - d2 * n.z) / u.y;
+                    x0.z = (d2 * n.x - d1 * ph.n.x) / u.y;
+                } else {
+                    x0.x = (d2 * n.y - d1 * ph.n.y) / u.z;
+                    x0.y = (d1 * ph.n.x - d2 * n.x) / u.z;
+                }
+                V3 view = div_recip(-ph.dl, sqrtf(dot(ph.dl, ph.dl)));
+                u = u - dot(u, view) * view;
+                V3 w = x0 - r_hit;
+                V3 w_perp = w - dot(w, view) * view;
+                x0 = r_hit + w_perp;
+                V3 vv = cross(u, x0 - r_hit);
+                float dist = sqrtf(dot(vv, vv) / dot(u, u));
+                if (dist < min_d)
+                    min_d = dist;
+            }
+        }
+        s.d_edge = min_d;
+        break;
+    }
+    default: {  // mesh, fresnel/cpu/GeometryMesh.cc:115-193
+        uint32_t inst = prim / g.n_faces, face = prim - inst * g.n_faces;
+        V3 pos = load3(g.position, inst);
+        Qt q = loadq(g.orientation, inst);
+        TriHit th = mesh_triangle(g, face, o, d, pos, q);
+        s.t = th.t;
+        s.d_edge = th.d;
+        s.Ng = rotate(q, th.n);
+        s.color = loadc3(g.color, 3 * face + 0) * th.u + loadc3(g.color, 3 * face + 1) * th.v
+                  + loadc3(g.color, 3 * face + 2) * th.w;
+        break;
+    }
+    }
+    return s;
+}
+
+}  // namespace fr
+
+#endif

@@ -1,0 +1,606 @@
+// py_gpu.cpp -- the `_gpu` extension module: fresnel's GPU backend classes over the C ABI.
+//
+// Class and method names follow fresnel's `_gpu` module (fresnel/gpu/module-gpu.cc:27-43):
+// Device, Scene, Geometry, GeometrySphere, GeometryCylinder, GeometryConvexPolyhedron,
+// GeometryMesh, Tracer, TracerDirect, TracerPath and the Array* buffer classes.  Everything
+// below is host bookkeeping; all rendering work happens in libfrb200 (include/fresnel_b200.h).
+//
+// Arrays: geometry arrays keep an authoritative host copy; unmap() marks the array stale and
+// the next render uploads stale arrays (a BVH rebuild follows only when a geometric array
+// changed).  Output arrays are authoritative on the device; map() downloads them.
+#include <pybind11/numpy.h>
+#include <pybind11/pybind11.h>
+
+#include <cstring>
+#include <memory>
+#include <set>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "fresnel_b200.h"
+#include "host_types.hpp"
+
+namespace py = pybind11;
+using namespace frh;
+
+namespace {
+
+void check(fr_status s)
+{
+    if (s != FR_OK)
+        throw std::runtime_error(fr_last_error());
+}
+
+// ---------------------------------------------------------------------------------------------
+// arrays
+// ---------------------------------------------------------------------------------------------
+struct ArrayBase {
+    std::vector<unsigned char> data;
+    std::vector<py::ssize_t> shape;
+    size_t item = 4;        // bytes per scalar
+    std::string format;     // python struct format of one scalar
+    bool mapped = false;
+    bool stale = false;     // host copy newer than the device copy (geometry arrays)
+    // owner: a geometry field or a tracer output
+    fr_geometry* geom = nullptr;
+    int field = -1;
+    fr_tracer* tracer = nullptr;
+    int output = -1;  // 0 linear, 1 srgb
+
+    size_t count() const
+    {
+        size_t n = 1;
+        for (auto s : shape)
+            n *= size_t(s);
+        return n;
+    }
+    void map()
+    {
+        if (tracer) {
+            if (output == 0)
+                check(fr_tracer_read_linear(tracer, reinterpret_cast<float*>(data.data()),
+                                            data.size()));
+            else
+                check(fr_tracer_read_srgb(tracer, data.data(), data.size()));
+        }
+        mapped = true;
+    }
+    void unmap()
+    {
+        mapped = false;
+        if (geom)
+            stale = true;
+    }
+    // push a stale geometry array to the device
+    void sync()
+    {
+        if (geom && stale && !data.empty()) {
+            check(fr_geometry_write(geom, field, data.data(), 0, data.size()));
+            stale = false;
+        }
+    }
+    py::buffer_info buffer()
+    {
+        if (!mapped)
+            throw std::runtime_error("Array must be mapped before it can be accessed");
+        std::vector<py::ssize_t> strides(shape.size());
+        py::ssize_t s = py::ssize_t(item);
+        for (size_t k = shape.size(); k-- > 0;) {
+            strides[k] = s;
+            s *= shape[k];
+        }
+        return py::buffer_info(data.data(), py::ssize_t(item), format, py::ssize_t(shape.size()),
+                               shape, strides);
+    }
+};
+
+// one C++ type per Python class name (fresnel/cpu/Array.cc:12-78)
+template <int K> struct ArrayK : ArrayBase {};
+using ArrayRGBAf = ArrayK<0>;
+using ArrayRGBAc = ArrayK<1>;
+using ArrayRGBf = ArrayK<2>;
+using ArrayVec3f = ArrayK<3>;
+using ArrayQuat3f = ArrayK<4>;
+using Array_f = ArrayK<5>;
+
+template <class A>
+std::shared_ptr<A> make_array(std::vector<py::ssize_t> shape, bool byte_scalar = false)
+{
+    auto a = std::make_shared<A>();
+    a->shape = std::move(shape);
+    a->item = byte_scalar ? 1 : 4;
+    a->format = byte_scalar ? py::format_descriptor<unsigned char>::format()
+                            : py::format_descriptor<float>::format();
+    a->data.assign(a->count() * a->item, 0);
+    return a;
+}
+
+// ---------------------------------------------------------------------------------------------
+// device / scene
+// ---------------------------------------------------------------------------------------------
+struct DeviceH {
+    fr_device* dev = nullptr;
+    DeviceH(const std::string& /*ptx_root*/, int n) { check(fr_device_create(n, &dev)); }
+    ~DeviceH() { fr_device_destroy(dev); }
+    std::string describe() const
+    {
+        char buf[512];
+        check(fr_device_describe(dev, buf, sizeof(buf)));
+        return buf;
+    }
+    static std::string all_gpus()
+    {
+        char buf[4096];
+        check(fr_get_all_gpus(buf, sizeof(buf)));
+        return buf;
+    }
+};
+
+struct GeometryH;
+
+struct SceneH {
+    std::shared_ptr<DeviceH> device;
+    fr_scene* scene = nullptr;
+    UserCamera camera;
+    RGBf background{0, 0, 0};
+    float background_alpha = 0.0f;
+    Lights lights;
+    std::set<GeometryH*> geoms;
+
+    explicit SceneH(std::shared_ptr<DeviceH> d) : device(std::move(d))
+    {
+        check(fr_scene_create(device->dev, &scene));
+        // default lights (fresnel/gpu/Scene.cc:15-28)
+        lights.N = 2;
+        lights.direction[0] = vec3f(-1, 0.3f, 1);
+        lights.color[0] = RGBf(1, 1, 1);
+        lights.direction[1] = vec3f(1, 0, 1);
+        lights.color[1] = RGBf(0.1f, 0.1f, 0.1f);
+    }
+    ~SceneH() { fr_scene_destroy(scene); }
+    void sync();
+};
+
+struct GeometryH {
+    std::shared_ptr<SceneH> scene;
+    fr_geometry* geom = nullptr;
+    bool valid = false;
+    Material material, outline;
+    float outline_width = 0.0f;
+    std::vector<std::shared_ptr<ArrayBase>> arrays;
+
+    explicit GeometryH(std::shared_ptr<SceneH> s) : scene(std::move(s))
+    {
+        // defaults of the reference's geometry constructors (fresnel/cpu/GeometrySphere.cc:31-33)
+        material.solid = 0;
+        material.color = RGBf(1, 0, 1);
+        material.roughness = 0.1f;
+        material.specular = 0.5f;
+        outline.solid = 1;
+        outline.color = RGBf(0, 0, 0);
+        outline.roughness = 0.1f;
+        outline.specular = 0.5f;
+    }
+    virtual ~GeometryH()
+    {
+        scene->geoms.erase(this);
+        fr_geometry_destroy(geom);
+    }
+    void attach()
+    {
+        valid = true;
+        scene->geoms.insert(this);
+        push_material();
+    }
+    template <class A> std::shared_ptr<A> add_array(int field, std::vector<py::ssize_t> shape)
+    {
+        auto a = make_array<A>(std::move(shape));
+        a->geom = geom;
+        a->field = field;
+        arrays.push_back(a);
+        return a;
+    }
+    void push_material()
+    {
+        fr_material m = to_abi(material), o = to_abi(outline);
+        check(fr_geometry_set_material(geom, &m, &o, outline_width));
+    }
+    Material getMaterial() const { return material; }
+    void setMaterial(const Material& m)
+    {
+        material = m;
+        push_material();
+    }
+    Material getOutlineMaterial() const { return outline; }
+    void setOutlineMaterial(const Material& m)
+    {
+        outline = m;
+        push_material();
+    }
+    float getOutlineWidth() const { return outline_width; }
+    void setOutlineWidth(float w)
+    {
+        outline_width = w;
+        push_material();
+    }
+    void enable()
+    {
+        if (!valid)
+            throw std::runtime_error("Cannot enable inactive Geometry");
+        check(fr_geometry_set_enabled(geom, 1));
+    }
+    void disable()
+    {
+        if (!valid)
+            throw std::runtime_error("Cannot disable inactive Geometry");
+        check(fr_geometry_set_enabled(geom, 0));
+    }
+    void remove()
+    {
+        if (valid) {
+            check(fr_geometry_remove(geom));
+            valid = false;
+        }
+    }
+    // Array writes are tracked per array (see ArrayBase::unmap); nothing else to record.
+    void update() {}
+    void sync()
+    {
+        for (auto& a : arrays)
+            a->sync();
+    }
+};
+
+void SceneH::sync()
+{
+    for (GeometryH* g : geoms)
+        g->sync();
+}
+
+struct GeometrySphereH : GeometryH {
+    std::shared_ptr<ArrayVec3f> position;
+    std::shared_ptr<Array_f> radius;
+    std::shared_ptr<ArrayRGBf> color;
+    GeometrySphereH(std::shared_ptr<SceneH> s, unsigned n) : GeometryH(std::move(s))
+    {
+        check(fr_geometry_create_sphere(scene->scene, n, &geom));
+        position = add_array<ArrayVec3f>(FR_FIELD_POSITION, {py::ssize_t(n), 3});
+        radius = add_array<Array_f>(FR_FIELD_RADIUS, {py::ssize_t(n)});
+        color = add_array<ArrayRGBf>(FR_FIELD_COLOR, {py::ssize_t(n), 3});
+        attach();
+    }
+};
+
+struct GeometryCylinderH : GeometryH {
+    std::shared_ptr<ArrayVec3f> points;
+    std::shared_ptr<Array_f> radius;
+    std::shared_ptr<ArrayRGBf> color;
+    GeometryCylinderH(std::shared_ptr<SceneH> s, unsigned n) : GeometryH(std::move(s))
+    {
+        check(fr_geometry_create_cylinder(scene->scene, n, &geom));
+        points = add_array<ArrayVec3f>(FR_FIELD_POINTS, {py::ssize_t(n), 2, 3});
+        radius = add_array<Array_f>(FR_FIELD_RADIUS, {py::ssize_t(n)});
+        color = add_array<ArrayRGBf>(FR_FIELD_COLOR, {py::ssize_t(n), 2, 3});
+        attach();
+    }
+};
+
+using farray = py::array_t<float, py::array::c_style | py::array::forcecast>;
+
+void require_nx3(const farray& a, const char* name, const char* what)
+{
+    if (a.ndim() != 2)
+        throw std::runtime_error(std::string(name) + " must be a 2-dimensional array");
+    if (a.shape(1) != 3)
+        throw std::runtime_error(std::string(name) + " must be a " + what + " by 3 array");
+}
+
+struct GeometryConvexPolyhedronH : GeometryH {
+    std::shared_ptr<ArrayVec3f> position;
+    std::shared_ptr<ArrayQuat3f> orientation;
+    std::shared_ptr<ArrayRGBf> color;
+    float color_by_face = 0.0f;
+    // argument checks of fresnel/cpu/GeometryConvexPolyhedron.cc:47-78
+    GeometryConvexPolyhedronH(std::shared_ptr<SceneH> s, farray origins, farray normals,
+                              farray colors, unsigned n, float r)
+        : GeometryH(std::move(s))
+    {
+        require_nx3(origins, "plane_origins", "Nvert");
+        require_nx3(normals, "plane_normals", "Nvert");
+        if (normals.shape(0) != origins.shape(0))
+            throw std::runtime_error("Number of vertices must match in origin and normal arrays");
+        require_nx3(colors, "plane_colors", "Nvert");
+        if (colors.shape(0) != origins.shape(0))
+            throw std::runtime_error("Number of vertices must match in origin and color arrays");
+        check(fr_geometry_create_polyhedron(scene->scene, origins.data(), normals.data(),
+                                            colors.data(), unsigned(origins.shape(0)), n, r,
+                                            &geom));
+        position = add_array<ArrayVec3f>(FR_FIELD_POSITION, {py::ssize_t(n), 3});
+        orientation = add_array<ArrayQuat3f>(FR_FIELD_ORIENTATION, {py::ssize_t(n), 4});
+        color = add_array<ArrayRGBf>(FR_FIELD_COLOR, {py::ssize_t(n), 3});
+        attach();
+    }
+    void setColorByFace(float f)
+    {
+        color_by_face = f;
+        check(fr_geometry_set_color_by_face(geom, f));
+    }
+    float getColorByFace() const { return color_by_face; }
+};
+
+struct GeometryMeshH : GeometryH {
+    std::shared_ptr<ArrayVec3f> position;
+    std::shared_ptr<ArrayQuat3f> orientation;
+    std::shared_ptr<ArrayRGBf> color;
+    // argument checks of fresnel/cpu/GeometryMesh.cc:27-34
+    GeometryMeshH(std::shared_ptr<SceneH> s, farray vertices, unsigned n) : GeometryH(std::move(s))
+    {
+        if (vertices.ndim() != 2)
+            throw std::runtime_error("vertices must be a 2-dimensional array");
+        if (vertices.shape(1) != 3)
+            throw std::runtime_error("vertices must be a Nvert by 3 array");
+        if (vertices.shape(0) % 3 != 0)
+            throw std::runtime_error("the number of triangle vertices must be a multiple of three.");
+        unsigned nv = unsigned(vertices.shape(0));
+        check(fr_geometry_create_mesh(scene->scene, vertices.data(), nv, n, &geom));
+        position = add_array<ArrayVec3f>(FR_FIELD_POSITION, {py::ssize_t(n), 3});
+        orientation = add_array<ArrayQuat3f>(FR_FIELD_ORIENTATION, {py::ssize_t(n), 4});
+        color = add_array<ArrayRGBf>(FR_FIELD_COLOR, {py::ssize_t(nv), 3});
+        attach();
+    }
+};
+
+// ---------------------------------------------------------------------------------------------
+// tracers
+// ---------------------------------------------------------------------------------------------
+struct TracerH {
+    std::shared_ptr<DeviceH> device;
+    fr_tracer* tracer = nullptr;
+    unsigned w = 0, h = 0;
+    unsigned seed = 0;
+    bool highlight = false;
+    RGBf highlight_color{1, 0, 1};
+    std::shared_ptr<ArrayRGBAf> linear;
+    std::shared_ptr<ArrayRGBAc> srgb;
+
+    TracerH(std::shared_ptr<DeviceH> d, unsigned w_, unsigned h_) : device(std::move(d))
+    {
+        check(fr_tracer_create(device->dev, w_, h_, &tracer));
+        make_outputs(w_, h_);
+    }
+    virtual ~TracerH() { fr_tracer_destroy(tracer); }
+    void make_outputs(unsigned w_, unsigned h_)
+    {
+        w = w_;
+        h = h_;
+        linear = make_array<ArrayRGBAf>({py::ssize_t(h), py::ssize_t(w), 4});
+        linear->tracer = tracer;
+        linear->output = 0;
+        srgb = make_array<ArrayRGBAc>({py::ssize_t(h), py::ssize_t(w), 4}, true);
+        srgb->tracer = tracer;
+        srgb->output = 1;
+    }
+    virtual void resize(unsigned w_, unsigned h_)
+    {
+        if (w_ == 0 || h_ == 0)
+            throw std::runtime_error("Invalid dimensions");
+        check(fr_tracer_resize(tracer, w_, h_));
+        make_outputs(w_, h_);
+    }
+    fr_render_params params(const SceneH& s) const
+    {
+        fr_render_params p;
+        std::memset(&p, 0, sizeof(p));
+        p.camera = to_abi(s.camera);
+        p.lights = to_abi(s.lights);
+        p.background_color[0] = s.background.r;
+        p.background_color[1] = s.background.g;
+        p.background_color[2] = s.background.b;
+        p.background_alpha = s.background_alpha;
+        p.seed = seed;
+        p.highlight_warning = highlight ? 1 : 0;
+        p.highlight_color[0] = highlight_color.r;
+        p.highlight_color[1] = highlight_color.g;
+        p.highlight_color[2] = highlight_color.b;
+        return p;
+    }
+    void check_scene(const std::shared_ptr<SceneH>& s) const
+    {
+        if (s->device != device)
+            throw std::runtime_error("Scene and Tracer devices do not match");
+    }
+    virtual void render(std::shared_ptr<SceneH> s) { check_scene(s); }
+    py::dict stats() const
+    {
+        fr_stats st;
+        check(fr_tracer_get_stats(tracer, &st));
+        py::dict d;
+        d["rays"] = st.rays;
+        d["paths"] = st.paths;
+        d["dropped"] = st.dropped;
+        d["kernel_launches"] = st.kernel_launches;
+        d["bvh_builds"] = st.bvh_builds;
+        d["bvh_build_ms"] = st.bvh_build_ms;
+        return d;
+    }
+};
+
+struct TracerDirectH : TracerH {
+    unsigned aa_n = 8;
+    using TracerH::TracerH;
+    void render(std::shared_ptr<SceneH> s) override
+    {
+        check_scene(s);
+        s->sync();
+        fr_render_params p = params(*s);
+        check(fr_tracer_render_preview(tracer, s->scene, &p, aa_n, nullptr));
+    }
+    // Preview render that also returns the closest-hit ids of every primary sample as a
+    // [h, w, aa_n^2, 2] uint32 array of (geometry index + 1, primitive index); (0, 0) = miss.
+    py::array_t<uint32_t> render_hit_ids(std::shared_ptr<SceneH> s)
+    {
+        check_scene(s);
+        s->sync();
+        fr_render_params p = params(*s);
+        py::array_t<uint32_t> out({py::ssize_t(h), py::ssize_t(w), py::ssize_t(aa_n * aa_n),
+                                   py::ssize_t(2)});
+        check(fr_tracer_render_preview(tracer, s->scene, &p, aa_n, out.mutable_data()));
+        return out;
+    }
+};
+
+struct TracerPathH : TracerH {
+    unsigned n_samples = 0;
+    unsigned light_samples = 1;
+    TracerPathH(std::shared_ptr<DeviceH> d, unsigned w_, unsigned h_, unsigned ls)
+        : TracerH(std::move(d), w_, h_), light_samples(ls)
+    {
+        reset();
+    }
+    // TracerPath::reset (fresnel/cpu/TracerPath.cc:31-47)
+    void reset()
+    {
+        n_samples = 0;
+        seed++;
+        check(fr_tracer_clear(tracer));
+    }
+    // TracerPath::resize (fresnel/cpu/TracerPath.h:48-53)
+    void resize(unsigned w_, unsigned h_) override
+    {
+        TracerH::resize(w_, h_);
+        n_samples = 0;
+        seed++;
+    }
+    void render(std::shared_ptr<SceneH> s) override { render_samples(s, 1); }
+    // `k` consecutive render() calls in one engine call (the sample loop stays on the device).
+    void render_samples(std::shared_ptr<SceneH> s, unsigned k)
+    {
+        check_scene(s);
+        if (k == 0)
+            return;
+        s->sync();
+        fr_render_params p = params(*s);
+        check(fr_tracer_render_path(tracer, s->scene, &p, n_samples + 1, k, light_samples));
+        n_samples += k;
+    }
+};
+
+template <class A> void export_array(py::module_& m, const char* name)
+{
+    py::class_<A, std::shared_ptr<A>>(m, name, py::buffer_protocol())
+        .def_buffer([](A& a) { return a.buffer(); })
+        .def("map", &A::map)
+        .def("unmap", &A::unmap);
+}
+
+}  // namespace
+
+PYBIND11_MODULE(_gpu, m)
+{
+    m.doc() = "fresnel_b200 GPU backend (mirror of fresnel._gpu) over libfrb200";
+    py::module_::import("fresnel_b200._common");
+
+    m.def("get_num_available_devices", []() {
+        int n = 0;
+        check(fr_get_num_available_devices(&n));
+        return n;
+    });
+
+    py::class_<DeviceH, std::shared_ptr<DeviceH>>(m, "Device")
+        .def(py::init<const std::string&, int>())
+        .def("describe", &DeviceH::describe)
+        .def_static("getAllGPUs", &DeviceH::all_gpus);
+
+    py::class_<SceneH, std::shared_ptr<SceneH>>(m, "Scene")
+        .def(py::init<std::shared_ptr<DeviceH>>())
+        .def("setCamera", [](SceneH& s, const UserCamera& c) { s.camera = c; })
+        .def("getCamera", [](SceneH& s) -> UserCamera& { return s.camera; },
+             py::return_value_policy::reference_internal)
+        .def("getBackgroundColor", [](SceneH& s) { return s.background; })
+        .def("setBackgroundColor", [](SceneH& s, const RGBf& c) { s.background = c; })
+        .def("getBackgroundAlpha", [](SceneH& s) { return s.background_alpha; })
+        .def("setBackgroundAlpha", [](SceneH& s, float a) { s.background_alpha = a; })
+        .def("getLights", [](SceneH& s) -> Lights& { return s.lights; },
+             py::return_value_policy::reference_internal)
+        .def("setLights", [](SceneH& s, const Lights& l) { s.lights = l; })
+        .def("build", [](SceneH& s) {
+            s.sync();
+            check(fr_scene_build(s.scene));
+        });
+
+    py::class_<GeometryH, std::shared_ptr<GeometryH>>(m, "Geometry")
+        .def("getMaterial", &GeometryH::getMaterial)
+        .def("setMaterial", &GeometryH::setMaterial)
+        .def("getOutlineMaterial", &GeometryH::getOutlineMaterial)
+        .def("setOutlineMaterial", &GeometryH::setOutlineMaterial)
+        .def("getOutlineWidth", &GeometryH::getOutlineWidth)
+        .def("setOutlineWidth", &GeometryH::setOutlineWidth)
+        .def("disable", &GeometryH::disable)
+        .def("enable", &GeometryH::enable)
+        .def("remove", &GeometryH::remove)
+        .def("update", &GeometryH::update);
+
+    py::class_<GeometrySphereH, GeometryH, std::shared_ptr<GeometrySphereH>>(m, "GeometrySphere")
+        .def(py::init<std::shared_ptr<SceneH>, unsigned>())
+        .def("getPositionBuffer", [](GeometrySphereH& g) { return g.position; })
+        .def("getRadiusBuffer", [](GeometrySphereH& g) { return g.radius; })
+        .def("getColorBuffer", [](GeometrySphereH& g) { return g.color; });
+
+    py::class_<GeometryCylinderH, GeometryH, std::shared_ptr<GeometryCylinderH>>(m,
+                                                                                "GeometryCylinder")
+        .def(py::init<std::shared_ptr<SceneH>, unsigned>())
+        .def("getPointsBuffer", [](GeometryCylinderH& g) { return g.points; })
+        .def("getRadiusBuffer", [](GeometryCylinderH& g) { return g.radius; })
+        .def("getColorBuffer", [](GeometryCylinderH& g) { return g.color; });
+
+    py::class_<GeometryConvexPolyhedronH, GeometryH, std::shared_ptr<GeometryConvexPolyhedronH>>(
+        m, "GeometryConvexPolyhedron")
+        .def(py::init<std::shared_ptr<SceneH>, farray, farray, farray, unsigned, float>())
+        .def("getPositionBuffer", [](GeometryConvexPolyhedronH& g) { return g.position; })
+        .def("getOrientationBuffer", [](GeometryConvexPolyhedronH& g) { return g.orientation; })
+        .def("getColorBuffer", [](GeometryConvexPolyhedronH& g) { return g.color; })
+        .def("setColorByFace", &GeometryConvexPolyhedronH::setColorByFace)
+        .def("getColorByFace", &GeometryConvexPolyhedronH::getColorByFace);
+
+    py::class_<GeometryMeshH, GeometryH, std::shared_ptr<GeometryMeshH>>(m, "GeometryMesh")
+        .def(py::init<std::shared_ptr<SceneH>, farray, unsigned>())
+        .def("getPositionBuffer", [](GeometryMeshH& g) { return g.position; })
+        .def("getOrientationBuffer", [](GeometryMeshH& g) { return g.orientation; })
+        .def("getColorBuffer", [](GeometryMeshH& g) { return g.color; });
+
+    py::class_<TracerH, std::shared_ptr<TracerH>>(m, "Tracer")
+        .def("render", &TracerH::render)
+        .def("resize", &TracerH::resize)
+        .def("getSRGBOutputBuffer", [](TracerH& t) { return t.srgb; })
+        .def("getLinearOutputBuffer", [](TracerH& t) { return t.linear; })
+        .def("enableHighlightWarning", [](TracerH& t, const RGBf& c) {
+            t.highlight = true;
+            t.highlight_color = c;
+        })
+        .def("disableHighlightWarning", [](TracerH& t) { t.highlight = false; })
+        .def("getSeed", [](TracerH& t) { return t.seed; })
+        .def("setSeed", [](TracerH& t, unsigned s) { t.seed = s; })
+        .def("getStats", &TracerH::stats)
+        .def("resetStats", [](TracerH& t) { check(fr_tracer_reset_stats(t.tracer)); });
+
+    py::class_<TracerDirectH, TracerH, std::shared_ptr<TracerDirectH>>(m, "TracerDirect")
+        .def(py::init<std::shared_ptr<DeviceH>, unsigned, unsigned>())
+        .def("setAntialiasingN", [](TracerDirectH& t, unsigned n) { t.aa_n = n; })
+        .def("getAntialiasingN", [](TracerDirectH& t) { return t.aa_n; })
+        .def("renderHitIds", &TracerDirectH::render_hit_ids);
+
+    py::class_<TracerPathH, TracerH, std::shared_ptr<TracerPathH>>(m, "TracerPath")
+        .def(py::init<std::shared_ptr<DeviceH>, unsigned, unsigned, unsigned>())
+        .def("getNumSamples", [](TracerPathH& t) { return t.n_samples; })
+        .def("reset", &TracerPathH::reset)
+        .def("setLightSamples", [](TracerPathH& t, unsigned n) { t.light_samples = n; })
+        .def("renderSamples", &TracerPathH::render_samples);
+
+    export_array<ArrayRGBAf>(m, "ArrayRGBAf");
+    export_array<ArrayRGBAc>(m, "ArrayRGBAc");
+    export_array<ArrayRGBf>(m, "ArrayRGBf");
+    export_array<ArrayVec3f>(m, "ArrayVec3f");
+    export_array<ArrayQuat3f>(m, "ArrayQuat3f");
+    export_array<Array_f>(m, "Array_f");
+}

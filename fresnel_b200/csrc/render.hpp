@@ -1,0 +1,63 @@
+// render.hpp -- host interface of the path-tracing and preview kernels.
+#ifndef FR_RENDER_HPP
+#define FR_RENDER_HPP
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "engine.cuh"
+
+namespace fr {
+
+// Everything one render reads, passed by value to every kernel of that render.
+struct FrameParams {
+    SceneDev scene;
+    CamK cam;
+    LightsK lights;
+    C3 bg;
+    float bg_alpha;
+    uint32_t w, h;
+    uint32_t n_samples;      // 1-based sample number of this render (TracerPath::m_n_samples)
+    uint32_t light_samples;  // light paths per primary ray
+    int highlight;
+    C3 hl_color;
+    float4* linear;     // [h][w] running mean, linear RGBA
+    uint32_t* srgb;     // [h][w] RGBA8
+    unsigned long long* stats;  // [0] rays, [1] paths, [2] dropped non-finite samples
+};
+
+// Per-pixel wavefront state of the path tracer (structure of arrays, w*h entries each).
+struct PathState {
+    float4* prim_o;     // primary ray, shared by the light samples of a pixel sample
+    float4* prim_d;
+    uint2* prim_hit;    // (geometry or MISS, primitive)
+    float4* ray_o;      // next extension ray
+    float4* ray_d;
+    float4* att;        // path throughput
+    float4* result;     // radiance summed over the pixel's light samples so far
+    uint2* ls_depth;    // (light sample, depth)
+    uint2* hit;         // closest hit of the last extension ray
+    uint32_t* queue[2];
+    uint32_t* ctr;      // [0], [1] queue lengths, [2] extend work counter
+};
+
+struct LaunchShape {
+    int shade_grid;
+    int extend_grid;
+};
+
+LaunchShape path_launch_shape(int num_sms);
+
+// one TracerPath::render sample: primary rays (all pixels) ...
+void launch_path_primary(const FrameParams& P, const PathState& S, cudaStream_t st);
+// ... then iteration i of shade (queue in = i == 0 ? every pixel : q[(i-1)&1], out = q[i&1])
+// and extend (q[i&1]) until the output queue is empty.
+void launch_path_iteration(const FrameParams& P, const PathState& S, int iteration,
+                           const LaunchShape& shape, cudaStream_t st);
+// TracerDirect::render
+void launch_preview(const FrameParams& P, uint32_t aa_n, uint2* hits, cudaStream_t st);
+
+}  // namespace fr
+
+#endif

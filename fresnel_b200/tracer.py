@@ -1,0 +1,115 @@
+"""Ray tracers (fresnel/tracer.py).
+
+`Preview` renders a quick direct-lighting image; `Path` is the progressive Monte Carlo path
+tracer.  Both keep their output on the device and copy it to the host when read.
+"""
+
+import numpy
+
+from . import _common
+from . import util
+
+
+class Tracer:
+    """Base class (fresnel/tracer.py:20-154)."""
+
+    def __init__(self):
+        raise RuntimeError("Use a specific tracer class")
+
+    def resize(self, w, h):
+        """Resize (and clear) the output buffer."""
+        self._tracer.resize(w, h)
+
+    def render(self, scene):
+        """Render ``scene`` into the output buffer and return `output`."""
+        self._tracer.render(scene._scene)
+        return self.output
+
+    def enable_highlight_warning(self, color=(1, 0, 1)):
+        """Paint pixels brighter than 1 in any channel with ``color``."""
+        self._tracer.enableHighlightWarning(_common.RGBf(*color))
+
+    def disable_highlight_warning(self):
+        self._tracer.disableHighlightWarning()
+
+    def histogram(self):
+        """Lightness and R, G, B histograms (512 bins, gamma 2.2) of the visible pixels
+        (fresnel/tracer.py:79-108).  Returns ``(hist[512, 4], bin_upper_edges)``."""
+        a = numpy.array(self.linear_output[:])
+        img = a[a[:, :, 3] > 0]
+        r, g, b = img[:, 0], img[:, 1], img[:, 2]
+        lum = 0.21 * r + 0.72 * g + 0.07 * b
+        n = 512
+        cols = []
+        bins = None
+        for ch in (lum, r, g, b):
+            h, bins = numpy.histogram(ch**(1 / 2.2), bins=n, range=[0, 1])
+            cols.append(h)
+        return numpy.stack(cols, axis=1), bins[1:]
+
+    @property
+    def output(self):
+        """util.ImageArray: sRGB RGBA uint8 output (H, W, 4)."""
+        return util.ImageArray(self._tracer.getSRGBOutputBuffer(), geom=None)
+
+    @property
+    def linear_output(self):
+        """util.Array: linear RGBA float32 output (H, W, 4)."""
+        return util.Array(self._tracer.getLinearOutputBuffer(), geom=None)
+
+    @property
+    def seed(self):
+        return self._tracer.getSeed()
+
+    @seed.setter
+    def seed(self, value):
+        self._tracer.setSeed(value)
+
+
+class Preview(Tracer):
+    """Direct-lighting preview tracer (fresnel/tracer.py:157-181).
+
+    ``anti_alias=True`` takes 8 x 8 tent-filtered samples per pixel.
+    """
+
+    def __init__(self, device, w, h, anti_alias=True):
+        self.device = device
+        self._tracer = device.module.TracerDirect(device._device, w, h)
+        self.anti_alias = anti_alias
+
+    @property
+    def anti_alias(self):
+        return self._tracer.getAntialiasingN() > 1
+
+    @anti_alias.setter
+    def anti_alias(self, value):
+        self._tracer.setAntialiasingN(8 if value else 1)
+
+
+class Path(Tracer):
+    """Progressive path tracer (fresnel/tracer.py:184-261).
+
+    Each `render` adds one sample per pixel to the running mean.  `sample` takes many samples
+    in one call; its result is identical to calling `render` that many times.
+    """
+
+    def __init__(self, device, w, h):
+        self.device = device
+        self._tracer = device.module.TracerPath(device._device, w, h, 1)
+
+    def reset(self):
+        """Clear the output and advance the seed (a statistically independent new image)."""
+        self._tracer.reset()
+
+    def sample(self, scene, samples, reset=True, light_samples=1):
+        """Take ``samples`` samples per pixel, each with ``light_samples`` light paths."""
+        if reset:
+            self.reset()
+        self._tracer.setLightSamples(light_samples)
+        try:
+            if samples > 0:
+                self._tracer.renderSamples(scene._scene, samples)
+        finally:
+            # keep later render() calls at one light sample (fresnel/tracer.py:257-259)
+            self._tracer.setLightSamples(1)
+        return self.output

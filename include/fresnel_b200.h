@@ -1,0 +1,228 @@
+/*
+ * fresnel_b200.h -- C ABI of the B200 (sm_100a) path-tracing engine.
+ *
+ * Every entry point takes plain pointers, sizes and opaque handles, returns an
+ * fr_status, and never lets a C++ exception cross the boundary.  The text of
+ * the last error on the calling thread is available from fr_last_error().
+ *
+ * The entry points replace the backend classes that fresnel's Python layer
+ * binds through its `_gpu` pybind11 module (fresnel/gpu/module-gpu.cc:27-43).
+ * Each declaration names the reference method it stands in for.  Geometry
+ * buffers live in device memory owned by the library; the host side copies
+ * whole arrays (or byte ranges of them) in and out, which is what the
+ * reference's Array map()/unmap() pair does (fresnel/gpu/Array.h:190-215).
+ *
+ * All work of one fr_device is ordered on one CUDA stream owned by that device.
+ */
+#ifndef FRESNEL_B200_H
+#define FRESNEL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FR_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define FR_API __attribute__((visibility("default")))
+#else
+#define FR_API
+#endif
+
+typedef enum fr_status {
+    FR_OK = 0,
+    FR_ERR_INVALID = 1,      /* bad argument (shape, size, null handle ...) */
+    FR_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+    FR_ERR_OUT_OF_MEMORY = 3,
+    FR_ERR_STATE = 4,        /* operation not allowed in the object's state */
+    FR_ERR_DEVICE_LIMIT = 5, /* a kernel hit a bounded limit (stack, iteration cap) */
+    FR_ERR_UNSUPPORTED = 6
+} fr_status;
+
+/* ------------------------------------------------------------------------ */
+/* Plain data shared with the host layer (layouts follow the reference's    */
+/* POD structs so they can be filled field by field from Python).           */
+/* ------------------------------------------------------------------------ */
+
+enum { FR_CAMERA_ORTHOGRAPHIC = 0, FR_CAMERA_PERSPECTIVE = 1 };
+
+/* fresnel::UserCamera (fresnel/common/Camera.h:55-77). */
+typedef struct fr_user_camera {
+    float position[3];
+    float look_at[3];
+    float up[3];
+    float h;
+    float f;
+    float f_stop;
+    float focus_distance;
+    int32_t model; /* FR_CAMERA_* */
+} fr_user_camera;
+
+/* fresnel::Lights (fresnel/common/Light.h:36-40): up to 4 area lights given in camera space. */
+typedef struct fr_lights {
+    float direction[4][3];
+    float color[4][3];
+    float theta[4];
+    uint32_t n;
+} fr_lights;
+
+/* fresnel::Material (fresnel/common/Material.h:47-55). */
+typedef struct fr_material {
+    float solid;
+    float color[3];
+    float primitive_color_mix;
+    float roughness;
+    float specular;
+    float metal;
+    float spec_trans;
+} fr_material;
+
+/* Per-render scene-wide inputs (fresnel/gpu/TracerPath.cc:60-101 uploads the same values as
+ * OptiX variables before each launch). */
+typedef struct fr_render_params {
+    fr_user_camera camera;
+    fr_lights lights;
+    float background_color[3];
+    float background_alpha;
+    uint32_t seed;
+    int32_t highlight_warning;
+    float highlight_color[3];
+} fr_render_params;
+
+/* Geometry kinds (fresnel/gpu/module-gpu.cc:33-38). */
+enum {
+    FR_GEOM_SPHERE = 0,
+    FR_GEOM_CYLINDER = 1,
+    FR_GEOM_POLYHEDRON = 2,
+    FR_GEOM_MESH = 3
+};
+
+/* Per-geometry arrays exposed through the Python Array proxy. */
+enum {
+    FR_FIELD_POSITION = 0,    /* sphere/polyhedron/mesh: [N][3] f32 */
+    FR_FIELD_RADIUS = 1,      /* sphere/cylinder: [N] f32 */
+    FR_FIELD_COLOR = 2,       /* sphere/polyhedron: [N][3]; cylinder: [N][2][3]; mesh: [n_verts][3] */
+    FR_FIELD_POINTS = 3,      /* cylinder: [N][2][3] f32 */
+    FR_FIELD_ORIENTATION = 4  /* polyhedron/mesh: [N][4] f32 quaternion (s, x, y, z) */
+};
+
+/* Counters accumulated by a tracer since creation (or the last fr_tracer_reset_stats). */
+typedef struct fr_stats {
+    uint64_t rays;          /* closest-hit queries (primary rays shared across light samples) */
+    uint64_t paths;         /* pixel samples x light samples */
+    uint64_t dropped;       /* non-finite pixel samples not folded into the mean */
+    uint64_t kernel_launches;
+    uint64_t bvh_builds;
+    double bvh_build_ms;    /* device time of the last BVH build of any geometry */
+} fr_stats;
+
+typedef struct fr_device fr_device;
+typedef struct fr_scene fr_scene;
+typedef struct fr_geometry fr_geometry;
+typedef struct fr_tracer fr_tracer;
+
+/* Text of the last failed call on this thread ("" if none). */
+FR_API const char* fr_last_error(void);
+FR_API int fr_abi_version(void);
+
+/* ---------------- device: fresnel/gpu/Device.cc ---------------- */
+
+/* get_num_available_devices (fresnel/gpu/module-gpu.cc:22-25): number of sm_100 devices. */
+FR_API fr_status fr_get_num_available_devices(int* n);
+/* Device::getAllGPUs (fresnel/gpu/Device.cc:186-192): one line per GPU, each ending in '\n'. */
+FR_API fr_status fr_get_all_gpus(char* buf, size_t cap);
+/* Device::Device(ptx_root, n) (fresnel/gpu/Device.cc:29-54).  n = -1 selects all; the engine
+ * renders on the first selected GPU. */
+FR_API fr_status fr_device_create(int n, fr_device** out);
+FR_API fr_status fr_device_destroy(fr_device* dev);
+/* Device::describe (fresnel/gpu/Device.cc:114-128). */
+FR_API fr_status fr_device_describe(const fr_device* dev, char* buf, size_t cap);
+FR_API fr_status fr_device_synchronize(fr_device* dev);
+
+/* ---------------- scene: fresnel/gpu/Scene.cc ---------------- */
+
+/* Scene::Scene (fresnel/gpu/Scene.cc:15-28). */
+FR_API fr_status fr_scene_create(fr_device* dev, fr_scene** out);
+FR_API fr_status fr_scene_destroy(fr_scene* scene);
+
+/* ---------------- geometry: fresnel/gpu/Geometry*.cc ---------------- */
+
+/* GeometrySphere(Scene, N) (fresnel/gpu/GeometrySphere.cc:17-49). */
+FR_API fr_status fr_geometry_create_sphere(fr_scene* scene, uint32_t n, fr_geometry** out);
+/* GeometryCylinder(Scene, N) (fresnel/gpu/GeometryCylinder.cc). */
+FR_API fr_status fr_geometry_create_cylinder(fr_scene* scene, uint32_t n, fr_geometry** out);
+/* GeometryConvexPolyhedron(Scene, origins, normals, colors, N, r)
+ * (fresnel/cpu/GeometryConvexPolyhedron.cc:22-103; normals are normalised on ingest). */
+FR_API fr_status fr_geometry_create_polyhedron(fr_scene* scene, const float* plane_origins,
+                                        const float* plane_normals, const float* plane_colors,
+                                        uint32_t n_planes, uint32_t n, float radius,
+                                        fr_geometry** out);
+/* GeometryMesh(Scene, vertices[nv][3], N) (fresnel/cpu/GeometryMesh.cc:20-72; nv % 3 == 0). */
+FR_API fr_status fr_geometry_create_mesh(fr_scene* scene, const float* vertices, uint32_t n_vertices,
+                                  uint32_t n, fr_geometry** out);
+/* ~Geometry / Geometry::remove (fresnel/gpu/Geometry.cc:18-58). */
+FR_API fr_status fr_geometry_destroy(fr_geometry* geom);
+/* Geometry::remove (fresnel/gpu/Geometry.cc:47-58): detach for good; enable/disable then fail. */
+FR_API fr_status fr_geometry_remove(fr_geometry* geom);
+/* Array<T>::unmap of a geometry buffer: copy host bytes into the device array and mark the
+ * geometry's BVH stale (fresnel/util.py:54-62, fresnel/gpu/Geometry.h:85-89). */
+FR_API fr_status fr_geometry_write(fr_geometry* geom, int field, const void* host, size_t offset_bytes,
+                            size_t nbytes);
+/* Array<T>::map of a geometry buffer: copy device bytes to the host. */
+FR_API fr_status fr_geometry_read(fr_geometry* geom, int field, void* host, size_t offset_bytes,
+                           size_t nbytes);
+/* Byte size of a field (0 if the geometry kind has no such field). */
+FR_API fr_status fr_geometry_field_size(const fr_geometry* geom, int field, size_t* nbytes);
+/* Geometry::enable / disable (fresnel/gpu/Geometry.cc:24-45). */
+FR_API fr_status fr_geometry_set_enabled(fr_geometry* geom, int enabled);
+/* Geometry::setMaterial / setOutlineMaterial / setOutlineWidth (fresnel/gpu/Geometry.h:43-80). */
+FR_API fr_status fr_geometry_set_material(fr_geometry* geom, const fr_material* material,
+                                   const fr_material* outline_material, float outline_width);
+/* GeometryConvexPolyhedron::setColorByFace (fresnel/cpu/GeometryConvexPolyhedron.h:69-72). */
+FR_API fr_status fr_geometry_set_color_by_face(fr_geometry* geom, float f);
+/* Geometry::update (fresnel/gpu/Geometry.h:85-89): mark the BVH stale. */
+FR_API fr_status fr_geometry_update(fr_geometry* geom);
+/* Build (or rebuild) every stale BVH of the scene now instead of at the next render. */
+FR_API fr_status fr_scene_build(fr_scene* scene);
+
+/* ---------------- tracers: fresnel/gpu/Tracer*.cc ---------------- */
+
+/* Tracer::Tracer(device, w, h) (fresnel/gpu/Tracer.cc:14-22). */
+FR_API fr_status fr_tracer_create(fr_device* dev, uint32_t w, uint32_t h, fr_tracer** out);
+FR_API fr_status fr_tracer_destroy(fr_tracer* tr);
+/* Tracer::resize (fresnel/gpu/Tracer.cc:26-51); w or h == 0 is an error. Clears both outputs. */
+FR_API fr_status fr_tracer_resize(fr_tracer* tr, uint32_t w, uint32_t h);
+/* TracerPath::reset's buffer clear (fresnel/cpu/TracerPath.cc:31-47). */
+FR_API fr_status fr_tracer_clear(fr_tracer* tr);
+
+/* TracerPath::render (fresnel/gpu/TracerPath.cc:60-102), called n_render times in a row:
+ * render k (k = 0..n_render-1) takes pixel sample number first_sample + k (1-based, the
+ * value of m_n_samples after its increment) and folds it into the running mean. */
+FR_API fr_status fr_tracer_render_path(fr_tracer* tr, fr_scene* scene, const fr_render_params* params,
+                                uint32_t first_sample, uint32_t n_render,
+                                uint32_t light_samples);
+
+/* TracerDirect::render (fresnel/gpu/TracerDirect.cc): aa_n x aa_n primary samples per pixel.
+ * If hit_ids is not NULL it receives, for each pixel and AA sample, the pair
+ * (geometry index + 1, primitive index) of the closest hit ((0, 0) on a miss), laid out
+ * [h][w][aa_n*aa_n][2] (host memory, 8 bytes per sample). */
+FR_API fr_status fr_tracer_render_preview(fr_tracer* tr, fr_scene* scene, const fr_render_params* params,
+                                   uint32_t aa_n, uint32_t* hit_ids);
+
+/* Output buffers: linear RGBA f32 [h][w][4] and sRGB RGBA u8 [h][w][4]
+ * (fresnel/gpu/Tracer.cc:26-51, the reference's getLinearOutputBuffer/getSRGBOutputBuffer). */
+FR_API fr_status fr_tracer_read_linear(fr_tracer* tr, float* host, size_t nbytes);
+FR_API fr_status fr_tracer_read_srgb(fr_tracer* tr, uint8_t* host, size_t nbytes);
+FR_API fr_status fr_tracer_write_linear(fr_tracer* tr, const float* host, size_t nbytes);
+FR_API fr_status fr_tracer_write_srgb(fr_tracer* tr, const uint8_t* host, size_t nbytes);
+FR_API fr_status fr_tracer_get_stats(const fr_tracer* tr, fr_stats* out);
+FR_API fr_status fr_tracer_reset_stats(fr_tracer* tr);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FRESNEL_B200_H */

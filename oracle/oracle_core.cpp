@@ -1,0 +1,1068 @@
+// oracle_core.cpp -- TEST INFRASTRUCTURE (CPU oracle), not part of the product.
+//
+// A CPU restatement of fresnel's Embree backend: per-geometry closest-hit glue restated from
+// fresnel/cpu/Geometry{Sphere,Cylinder,ConvexPolyhedron,Mesh}.cc, the tile loops of
+// fresnel/cpu/TracerPath.cc and fresnel/cpu/TracerDirect.cc, and a binned-SAH BVH2 standing in
+// for Embree's scene BVH (closest-hit results do not depend on the BVH except for exact ties
+// in t).  The shading/intersection arithmetic comes from namespace M, which is either the
+// restatement (restated_math.hpp) or the reference's own headers (ref_math_adapter.hpp,
+// selected with -DFR_ORACLE_REFERENCE_MATH).
+//
+// Build: oracle/build_oracle.py (g++ -O3 -ffp-contract=off, so no FMA contraction changes a
+// rounding the reference does not make).
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <new>
+#include <thread>
+#include <vector>
+
+#include "oracle.h"
+#include "restated_math.hpp"
+
+#ifdef FR_ORACLE_REFERENCE_MATH
+#include "ref_math_adapter.hpp"
+namespace M = frref;
+static const char* k_math_kind = "reference-headers";
+#else
+namespace M = frm;
+static const char* k_math_kind = "restated";
+#endif
+
+using frm::F3;
+using frm::Mat;
+using frm::PathState;
+using frm::Quat;
+using frm::RGB3;
+
+namespace {
+
+// ---------------------------------------------------------------------------------------------
+// scene
+// ---------------------------------------------------------------------------------------------
+struct Geom {
+    int type = 0;
+    uint32_t n = 0;        // user primitives (mesh: instances)
+    uint32_t n_faces = 0;  // mesh only
+    std::vector<F3> position;
+    std::vector<float> radius;
+    std::vector<RGB3> color;
+    std::vector<F3> points;  // cylinder: 2 per primitive
+    std::vector<Quat> orientation;
+    std::vector<F3> vertices;
+    std::vector<F3> plane_origin, plane_normal;
+    std::vector<RGB3> plane_color;
+    float poly_radius = 0, color_by_face = 0;
+    Mat material{}, outline{};
+    float outline_width = 0;
+    uint32_t prim_count() const { return type == FR_GEOM_MESH ? n * n_faces : n; }
+};
+
+struct Box {
+    float lo[3], hi[3];
+};
+
+struct Node {  // 32 bytes
+    float lo[3];
+    uint32_t a;  // interior: right child; leaf: first reference
+    float hi[3];
+    uint32_t count;  // 0 = interior (left child is this index + 1)
+};
+
+struct PrimRef {
+    uint32_t geom, prim;
+};
+
+}  // namespace
+
+struct or_scene {
+    std::vector<Geom> geoms;  // indexed like the caller's array (disabled ones kept, unused)
+    std::vector<Node> nodes;
+    std::vector<PrimRef> refs;
+};
+
+namespace {
+
+Mat to_mat(const fr_material& m)
+{
+    Mat r;
+    r.solid = m.solid;
+    r.color = RGB3{m.color[0], m.color[1], m.color[2]};
+    r.primitive_color_mix = m.primitive_color_mix;
+    r.roughness = m.roughness;
+    r.specular = m.specular;
+    r.metal = m.metal;
+    r.spec_trans = m.spec_trans;
+    return r;
+}
+
+inline void box_grow(Box& b, float x, float y, float z)
+{
+    b.lo[0] = std::min(b.lo[0], x);
+    b.lo[1] = std::min(b.lo[1], y);
+    b.lo[2] = std::min(b.lo[2], z);
+    b.hi[0] = std::max(b.hi[0], x);
+    b.hi[1] = std::max(b.hi[1], y);
+    b.hi[2] = std::max(b.hi[2], z);
+}
+
+inline Box box_empty()
+{
+    const float inf = std::numeric_limits<float>::infinity();
+    return Box{{inf, inf, inf}, {-inf, -inf, -inf}};
+}
+
+inline void box_union(Box& a, const Box& b)
+{
+    for (int k = 0; k < 3; ++k) {
+        a.lo[k] = std::min(a.lo[k], b.lo[k]);
+        a.hi[k] = std::max(a.hi[k], b.hi[k]);
+    }
+}
+
+inline float box_area(const Box& b)
+{
+    float dx = b.hi[0] - b.lo[0], dy = b.hi[1] - b.lo[1], dz = b.hi[2] - b.lo[2];
+    if (!(dx >= 0) || !(dy >= 0) || !(dz >= 0))
+        return 0.0f;
+    return 2.0f * (dx * dy + dy * dz + dz * dx);
+}
+
+// Primitive bounds (fresnel/cpu/GeometrySphere.cc:60-73, GeometryCylinder.cc:55-70,
+// GeometryConvexPolyhedron.cc:119-132, GeometryMesh.cc:81-113), inflated by a small relative
+// margin so that rounding in the box test can never cull a primitive the intersector accepts.
+Box prim_box(const Geom& g, uint32_t prim)
+{
+    Box b = box_empty();
+    switch (g.type) {
+    case FR_GEOM_SPHERE: {
+        F3 p = g.position[prim];
+        float r = g.radius[prim];
+        box_grow(b, p.x - r, p.y - r, p.z - r);
+        box_grow(b, p.x + r, p.y + r, p.z + r);
+        break;
+    }
+    case FR_GEOM_CYLINDER: {
+        F3 A = g.points[2 * prim], B = g.points[2 * prim + 1];
+        float r = g.radius[prim];
+        box_grow(b, A.x - r, A.y - r, A.z - r);
+        box_grow(b, A.x + r, A.y + r, A.z + r);
+        box_grow(b, B.x - r, B.y - r, B.z - r);
+        box_grow(b, B.x + r, B.y + r, B.z + r);
+        break;
+    }
+    case FR_GEOM_POLYHEDRON: {
+        F3 p = g.position[prim];
+        float r = g.poly_radius;
+        box_grow(b, p.x - r, p.y - r, p.z - r);
+        box_grow(b, p.x + r, p.y + r, p.z + r);
+        break;
+    }
+    case FR_GEOM_MESH: {
+        uint32_t inst = prim / g.n_faces, face = prim % g.n_faces;
+        F3 p = g.position[inst];
+        Quat q = g.orientation[inst];
+        for (int k = 0; k < 3; ++k) {
+            F3 v = M::rotate(q, g.vertices[3 * face + k]) + p;
+            box_grow(b, v.x, v.y, v.z);
+        }
+        break;
+    }
+    }
+    float scale = 0;
+    for (int k = 0; k < 3; ++k)
+        scale = std::max(scale, std::max(std::fabs(b.lo[k]), std::fabs(b.hi[k])));
+    float pad = 1e-5f * scale + 1e-6f * (b.hi[0] - b.lo[0] + b.hi[1] - b.lo[1] + b.hi[2] - b.lo[2])
+                + 1e-30f;
+    for (int k = 0; k < 3; ++k) {
+        b.lo[k] -= pad;
+        b.hi[k] += pad;
+    }
+    return b;
+}
+
+// ---------------------------------------------------------------------------------------------
+// binned SAH BVH2
+// ---------------------------------------------------------------------------------------------
+struct Builder {
+    std::vector<Box> boxes;
+    std::vector<F3> cent;
+    std::vector<uint32_t> idx;
+    std::vector<Node>& nodes;
+    int leaf_max;
+    explicit Builder(std::vector<Node>& n, int lm) : nodes(n), leaf_max(lm) {}
+
+    uint32_t build(uint32_t begin, uint32_t end)
+    {
+        Box bb = box_empty(), cb = box_empty();
+        for (uint32_t i = begin; i < end; ++i) {
+            box_union(bb, boxes[idx[i]]);
+            box_grow(cb, cent[idx[i]].x, cent[idx[i]].y, cent[idx[i]].z);
+        }
+        uint32_t me = uint32_t(nodes.size());
+        nodes.push_back(Node{});
+        Node nd{};
+        for (int k = 0; k < 3; ++k) {
+            nd.lo[k] = bb.lo[k];
+            nd.hi[k] = bb.hi[k];
+        }
+        uint32_t n = end - begin;
+        auto make_leaf = [&]() {
+            nd.a = begin;
+            nd.count = n;
+            nodes[me] = nd;
+            return me;
+        };
+        if (n <= 1)
+            return make_leaf();
+        // best split over 32 bins per axis
+        const int NB = 32;
+        float best_cost = std::numeric_limits<float>::infinity();
+        int best_axis = -1, best_bin = -1;
+        for (int axis = 0; axis < 3; ++axis) {
+            float lo = (&cb.lo[0])[axis], hi = (&cb.hi[0])[axis];
+            if (!(hi > lo))
+                continue;
+            Box bin_box[NB];
+            uint32_t bin_cnt[NB];
+            for (int b = 0; b < NB; ++b) {
+                bin_box[b] = box_empty();
+                bin_cnt[b] = 0;
+            }
+            float scale = NB / (hi - lo);
+            for (uint32_t i = begin; i < end; ++i) {
+                float c = (&cent[idx[i]].x)[axis];
+                int b = std::min(NB - 1, std::max(0, int((c - lo) * scale)));
+                bin_cnt[b]++;
+                box_union(bin_box[b], boxes[idx[i]]);
+            }
+            float right_area[NB];
+            uint32_t right_cnt[NB];
+            Box acc = box_empty();
+            uint32_t cnt = 0;
+            for (int b = NB - 1; b > 0; --b) {
+                box_union(acc, bin_box[b]);
+                cnt += bin_cnt[b];
+                right_area[b] = box_area(acc);
+                right_cnt[b] = cnt;
+            }
+            acc = box_empty();
+            cnt = 0;
+            for (int b = 0; b < NB - 1; ++b) {
+                box_union(acc, bin_box[b]);
+                cnt += bin_cnt[b];
+                if (cnt == 0 || right_cnt[b + 1] == 0)
+                    continue;
+                float cost = box_area(acc) * cnt + right_area[b + 1] * right_cnt[b + 1];
+                if (cost < best_cost) {
+                    best_cost = cost;
+                    best_axis = axis;
+                    best_bin = b;
+                }
+            }
+        }
+        if (best_axis < 0) {
+            // all centroids coincide
+            if (int(n) <= leaf_max)
+                return make_leaf();
+            uint32_t mid = begin + n / 2;
+            build(begin, mid);
+            nd.a = build(mid, end);
+            nd.count = 0;
+            nodes[me] = nd;
+            return me;
+        }
+        // SAH with unit traversal and intersection costs
+        float leaf_cost = box_area(bb) * float(n);
+        float split_cost = box_area(bb) + best_cost;
+        if (int(n) <= leaf_max && leaf_cost <= split_cost)
+            return make_leaf();
+        float lo = (&cb.lo[0])[best_axis], hi = (&cb.hi[0])[best_axis];
+        float scale = NB / (hi - lo);
+        uint32_t* first = idx.data() + begin;
+        uint32_t* last = idx.data() + end;
+        uint32_t* mid = std::partition(first, last, [&](uint32_t p) {
+            float c = (&cent[p].x)[best_axis];
+            int b = std::min(NB - 1, std::max(0, int((c - lo) * scale)));
+            return b <= best_bin;
+        });
+        uint32_t m = uint32_t(mid - idx.data());
+        if (m == begin || m == end)
+            m = begin + n / 2;
+        build(begin, m);
+        uint32_t r = build(m, end);
+        nd.a = r;
+        nd.count = 0;
+        nodes[me] = nd;
+        return me;
+    }
+};
+
+// ---------------------------------------------------------------------------------------------
+// closest-hit glue (Embree user-geometry intersect callbacks)
+// ---------------------------------------------------------------------------------------------
+struct Hit {
+    float t;       // ray.tfar
+    uint32_t geom;  // UINT32_MAX = miss
+    uint32_t prim;
+    F3 Ng;
+    RGB3 color;
+    float d;
+};
+
+// fresnel/cpu/GeometrySphere.cc:81-118
+inline void glue_sphere(const Geom& g, uint32_t gi, uint32_t prim, F3 o, F3 dir, float tnear,
+                        Hit& h)
+{
+    const F3 p = g.position[prim];
+    const float r = g.radius[prim];
+    float t = 0, d = 0;
+    F3 N;
+    bool hit = M::isect_sphere(t, d, N, o, dir, p, r);
+    if (hit && (tnear < t) && (t < h.t)) {
+        h.t = t;
+        h.geom = gi;
+        h.prim = prim;
+        h.Ng = F3{o.x + t * dir.x - p.x, o.y + t * dir.y - p.y, o.z + t * dir.z - p.z};
+        h.color = g.color[prim];
+        h.d = d;
+    }
+}
+
+// fresnel/cpu/GeometryCylinder.cc:76-120
+inline void glue_cylinder(const Geom& g, uint32_t gi, uint32_t prim, F3 o, F3 dir, float tnear,
+                          Hit& h)
+{
+    const F3 A = g.points[2 * prim], B = g.points[2 * prim + 1];
+    const float r = g.radius[prim];
+    float t = HUGE_VALF, d = HUGE_VALF;
+    F3 N{0, 0, 0};
+    unsigned ci = 0;
+    bool hit = M::isect_spherocylinder(t, d, N, ci, o, dir, A, B, r);
+    if (hit && (tnear < t) && (t < h.t)) {
+        h.t = t;
+        h.geom = gi;
+        h.prim = prim;
+        h.Ng = N;
+        h.color = g.color[2 * prim + ci];
+        h.d = d;
+    }
+}
+
+// fresnel/cpu/GeometryConvexPolyhedron.cc:140-335
+inline void glue_polyhedron(const Geom& g, uint32_t gi, uint32_t prim, F3 o, F3 dir, float tnear,
+                            Hit& h)
+{
+    using frm::cross;
+    using frm::dot;
+    const int n_planes = int(g.plane_normal.size());
+    float t0 = -std::numeric_limits<float>::max();
+    float t1 = std::numeric_limits<float>::max();
+    const F3 pos = g.position[prim];
+    const Quat q = g.orientation[prim];
+    F3 dl = M::rotate(M::conj(q), dir);
+    F3 ol = M::rotate(M::conj(q), o - pos);
+    F3 t0n{0, 0, 0}, t0p{0, 0, 0}, t1n{0, 0, 0}, t1p{0, 0, 0};
+    int t0_plane = 0, t1_plane = 0;
+    for (int i = 0; i < n_planes && t0 < t1; ++i) {
+        F3 n = g.plane_normal[i];
+        F3 p = g.plane_origin[i];
+        float dd = -dot(n, p);
+        float denom = dot(n, dl);
+        float t = -(dd + dot(n, ol)) / denom;
+        if (double(std::fabs(denom)) < 1e-5) {
+            if (dot(ol - p, n) > 0)
+                return;
+        } else if (denom < 0) {
+            if (t > t0) {
+                t0 = t;
+                t0n = n;
+                t0p = p;
+                t0_plane = i;
+            }
+        } else {
+            if (t < t1) {
+                t1 = t;
+                t1n = n;
+                t1p = p;
+                t1_plane = i;
+            }
+        }
+    }
+    if (t0 > t1)
+        return;
+    float t_hit = 0;
+    bool hit = false;
+    F3 n_hit{0, 0, 0}, p_hit{0, 0, 0};
+    float tfar = h.t;
+    Hit cand = h;
+    if ((tnear < t0) & (t0 < tfar)) {
+        t_hit = tfar = t0;
+        cand.Ng = M::rotate(q, t0n);
+        n_hit = t0n;
+        p_hit = t0p;
+        cand.color = frm::lerp(g.color_by_face, g.color[prim], g.plane_color[t0_plane]);
+        hit = true;
+    }
+    if ((tnear < t1) & (t1 < tfar)) {
+        t_hit = tfar = t1;
+        cand.Ng = M::rotate(q, t1n);
+        n_hit = t1n;
+        p_hit = t1p;
+        cand.color = frm::lerp(g.color_by_face, g.color[prim], g.plane_color[t1_plane]);
+        hit = true;
+    }
+    if (!hit)
+        return;
+    float min_d = std::numeric_limits<float>::max();
+    F3 r_hit = ol + t_hit * dl;
+    for (int i = 0; i < n_planes; ++i) {
+        F3 n = g.plane_normal[i];
+        F3 p = g.plane_origin[i];
+        F3 u = cross(n, n_hit);
+        if (double(std::fabs(dot(u, u))) >= 1e-5) {
+            int maxc;
+            if (std::fabs(u.x) > std::fabs(u.y))
+                maxc = (std::fabs(u.x) > std::fabs(u.z)) ? 1 : 3;
+            else
+                maxc = (std::fabs(u.y) > std::fabs(u.z)) ? 2 : 3;
+            F3 x0{0, 0, 0};
+            float d1 = -dot(n, p);
+            float d2 = -dot(n_hit, p_hit);
+            switch (maxc) {
+            case 1:
+                x0.x = 0;
+                x0.y = (d2 * n.z - d1 * n_hit.z) / u.x;
+                x0.z = (d1 * n_hit.y - d2 * n.y) / u.x;
+                break;
+            case 2:
+                x0.x = (d1 * n_hit.z - d2 * n.z) / u.y;
+                x0.y = 0;
+                x0.z = (d2 * n.x - d1 * n_hit.x) / u.y;
+                break;
+            default:
+                x0.x = (d2 * n.y - d1 * n_hit.y) / u.z;
+                x0.y = (d1 * n_hit.x - d2 * n.x) / u.z;
+                x0.z = 0;
+            }
+            F3 view = frm::div_recip(-dl, sqrtf(dot(dl, dl)));
+            u = u - dot(u, view) * view;
+            F3 w = x0 - r_hit;
+            F3 w_perp = w - dot(w, view) * view;
+            x0 = r_hit + w_perp;
+            F3 v = cross(u, x0 - r_hit);
+            float dsq = dot(v, v) / dot(u, u);
+            float dist = sqrtf(dsq);
+            if (dist < min_d)
+                min_d = dist;
+        }
+    }
+    cand.t = t_hit;
+    cand.geom = gi;
+    cand.prim = prim;
+    cand.d = min_d;
+    h = cand;
+}
+
+// fresnel/cpu/GeometryMesh.cc:115-193 (double-sided: second test with v0/v1 swapped)
+inline void glue_mesh(const Geom& g, uint32_t gi, uint32_t item, F3 o, F3 dir, float tnear, Hit& h)
+{
+    uint32_t inst = item / g.n_faces, face = item % g.n_faces;
+    const F3 p3 = g.position[inst];
+    const Quat q = g.orientation[inst];
+    F3 dl = M::rotate(M::conj(q), dir);
+    F3 ol = M::rotate(M::conj(q), o - p3);
+    F3 v0 = g.vertices[3 * face], v1 = g.vertices[3 * face + 1], v2 = g.vertices[3 * face + 2];
+    float u = 0, v = 0, w = 0, t = 0, d = 0;
+    F3 n{0, 0, 0};
+    if (!M::isect_triangle(u, v, w, t, d, n, ol, ol + dl, v0, v1, v2)
+        && !M::isect_triangle(v, u, w, t, d, n, ol, ol + dl, v1, v0, v2))
+        return;
+    if ((tnear < t) & (t < h.t)) {
+        h.t = t;
+        h.geom = gi;
+        h.prim = item;
+        h.Ng = M::rotate(q, n);
+        h.color = g.color[3 * face + 0] * u + g.color[3 * face + 1] * v + g.color[3 * face + 2] * w;
+        h.d = d;
+    }
+}
+
+struct Counters {
+    uint64_t rays = 0, box = 0, prim = 0, paths = 0, nonfinite = 0;
+};
+
+inline bool slab(const Node& nd, const float o[3], const float inv[3], float tmax, float& tentry)
+{
+    float t0 = 0.0f, t1 = tmax;
+    for (int k = 0; k < 3; ++k) {
+        float a = (nd.lo[k] - o[k]) * inv[k];
+        float b = (nd.hi[k] - o[k]) * inv[k];
+        if (a > b)
+            std::swap(a, b);
+        t0 = a > t0 ? a : t0;
+        t1 = b < t1 ? b : t1;
+    }
+    tentry = t0;
+    return t0 <= t1;
+}
+
+// Closest hit in (tnear, inf): Embree's rtcIntersect1 with fresnel's user geometries.
+Hit trace(const or_scene& s, F3 o, F3 d, float tnear, Counters& c)
+{
+    Hit h;
+    h.t = std::numeric_limits<float>::infinity();
+    h.geom = UINT32_MAX;
+    h.prim = 0;
+    c.rays++;
+    if (s.nodes.empty())
+        return h;
+    float of[3] = {o.x, o.y, o.z};
+    float df[3] = {d.x, d.y, d.z};
+    float inv[3];
+    for (int k = 0; k < 3; ++k) {
+        float dk = df[k];
+        if (std::fabs(dk) < 1e-30f)
+            dk = std::copysign(1e-30f, dk);
+        inv[k] = 1.0f / dk;
+    }
+    uint32_t stack[128];
+    int sp = 0;
+    uint32_t cur = 0;
+    float te;
+    c.box++;
+    if (!slab(s.nodes[0], of, inv, h.t, te))
+        return h;
+    while (true) {
+        const Node& nd = s.nodes[cur];
+        if (nd.count > 0) {
+            for (uint32_t k = 0; k < nd.count; ++k) {
+                const PrimRef& r = s.refs[nd.a + k];
+                const Geom& g = s.geoms[r.geom];
+                c.prim++;
+                switch (g.type) {
+                case FR_GEOM_SPHERE:
+                    glue_sphere(g, r.geom, r.prim, o, d, tnear, h);
+                    break;
+                case FR_GEOM_CYLINDER:
+                    glue_cylinder(g, r.geom, r.prim, o, d, tnear, h);
+                    break;
+                case FR_GEOM_POLYHEDRON:
+                    glue_polyhedron(g, r.geom, r.prim, o, d, tnear, h);
+                    break;
+                case FR_GEOM_MESH:
+                    glue_mesh(g, r.geom, r.prim, o, d, tnear, h);
+                    break;
+                }
+            }
+        } else {
+            uint32_t l = cur + 1, r = nd.a;
+            float tl, tr;
+            c.box += 2;
+            bool hl = slab(s.nodes[l], of, inv, h.t, tl);
+            bool hr = slab(s.nodes[r], of, inv, h.t, tr);
+            if (hl && hr) {
+                if (tr < tl)
+                    std::swap(l, r);
+                if (sp < 128)
+                    stack[sp++] = r;
+                cur = l;
+                continue;
+            }
+            if (hl) {
+                cur = l;
+                continue;
+            }
+            if (hr) {
+                cur = r;
+                continue;
+            }
+        }
+        // pop (re-test against the shrunken tmax)
+        bool found = false;
+        while (sp > 0) {
+            uint32_t nxt = stack[--sp];
+            c.box++;
+            if (slab(s.nodes[nxt], of, inv, h.t, te)) {
+                cur = nxt;
+                found = true;
+                break;
+            }
+        }
+        if (!found)
+            break;
+    }
+    return h;
+}
+
+// ---------------------------------------------------------------------------------------------
+// tile loops
+// ---------------------------------------------------------------------------------------------
+template <class F> void parallel_tiles(uint32_t n_items, int nthreads, F&& body)
+{
+    if (nthreads <= 0)
+        nthreads = int(std::max(1u, std::thread::hardware_concurrency()));
+    nthreads = std::max(1, std::min<int>(nthreads, int(n_items)));
+    std::atomic<uint32_t> next(0);
+    auto worker = [&](int tid) {
+        while (true) {
+            uint32_t it = next.fetch_add(1);
+            if (it >= n_items)
+                break;
+            body(it, tid);
+        }
+    };
+    if (nthreads == 1) {
+        worker(0);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (int t = 0; t < nthreads; ++t)
+        th.emplace_back(worker, t);
+    for (auto& t : th)
+        t.join();
+}
+
+frm::CameraIn to_camera(const fr_user_camera& c)
+{
+    frm::CameraIn k;
+    k.position = F3{c.position[0], c.position[1], c.position[2]};
+    k.look_at = F3{c.look_at[0], c.look_at[1], c.look_at[2]};
+    k.up = F3{c.up[0], c.up[1], c.up[2]};
+    k.h = c.h;
+    k.f = c.f;
+    k.f_stop = c.f_stop;
+    k.focus_distance = c.focus_distance;
+    k.model = c.model;
+    return k;
+}
+
+frm::LightsW world_lights(const fr_lights& in, const M::Cam& cam)
+{
+    F3 dir[4];
+    RGB3 col[4];
+    float th[4];
+    unsigned n = std::min<unsigned>(in.n, 4);
+    for (unsigned i = 0; i < n; ++i) {
+        dir[i] = F3{in.direction[i][0], in.direction[i][1], in.direction[i][2]};
+        col[i] = RGB3{in.color[i][0], in.color[i][1], in.color[i][2]};
+        th[i] = in.theta[i];
+    }
+    return M::lights_to_world(dir, col, th, n, cam);
+}
+
+void write_srgb(const fr_render_params& p, const float px[4], uint8_t* out)
+{
+    if (!p.highlight_warning || (px[0] <= 1.0f && px[1] <= 1.0f && px[2] <= 1.0f)) {
+        M::srgb_encode(px, out);
+    } else {
+        float c[4] = {p.highlight_color[0], p.highlight_color[1], p.highlight_color[2], px[3]};
+        M::srgb_encode(c, out);
+    }
+}
+
+inline bool finite3(RGB3 c) { return std::isfinite(c.r) && std::isfinite(c.g) && std::isfinite(c.b); }
+
+}  // namespace
+
+// =============================================================================================
+// C interface
+// =============================================================================================
+extern "C" {
+
+const char* or_math_kind(void) { return k_math_kind; }
+
+or_scene* or_scene_create(const or_geometry_desc* gd, uint32_t n_geoms, int leaf_max)
+{
+    or_scene* s = new (std::nothrow) or_scene();
+    if (!s)
+        return nullptr;
+    if (leaf_max < 1)
+        leaf_max = 4;
+    s->geoms.resize(n_geoms);
+    Builder b(s->nodes, leaf_max);
+    for (uint32_t gi = 0; gi < n_geoms; ++gi) {
+        const or_geometry_desc& d = gd[gi];
+        Geom& g = s->geoms[gi];
+        g.type = d.type;
+        g.n = d.n;
+        g.material = to_mat(d.material);
+        g.outline = to_mat(d.outline_material);
+        g.outline_width = d.outline_width;
+        g.poly_radius = d.poly_radius;
+        g.color_by_face = d.color_by_face;
+        auto f3 = [](const float* a, size_t n) {
+            std::vector<F3> v(n);
+            for (size_t i = 0; i < n; ++i)
+                v[i] = F3{a[3 * i], a[3 * i + 1], a[3 * i + 2]};
+            return v;
+        };
+        auto c3 = [](const float* a, size_t n) {
+            std::vector<RGB3> v(n);
+            for (size_t i = 0; i < n; ++i)
+                v[i] = RGB3{a[3 * i], a[3 * i + 1], a[3 * i + 2]};
+            return v;
+        };
+        auto q4 = [](const float* a, size_t n) {
+            std::vector<Quat> v(n);
+            for (size_t i = 0; i < n; ++i)
+                v[i] = Quat{a[4 * i], F3{a[4 * i + 1], a[4 * i + 2], a[4 * i + 3]}};
+            return v;
+        };
+        switch (d.type) {
+        case FR_GEOM_SPHERE:
+            g.position = f3(d.position, d.n);
+            g.radius.assign(d.radius, d.radius + d.n);
+            g.color = c3(d.color, d.n);
+            break;
+        case FR_GEOM_CYLINDER:
+            g.points = f3(d.points, size_t(d.n) * 2);
+            g.radius.assign(d.radius, d.radius + d.n);
+            g.color = c3(d.color, size_t(d.n) * 2);
+            break;
+        case FR_GEOM_POLYHEDRON:
+            g.position = f3(d.position, d.n);
+            g.orientation = q4(d.orientation, d.n);
+            g.color = c3(d.color, d.n);
+            g.plane_origin = f3(d.plane_origin, d.n_planes);
+            g.plane_normal = f3(d.plane_normal, d.n_planes);
+            g.plane_color = c3(d.plane_color, d.n_planes);
+            break;
+        case FR_GEOM_MESH:
+            if (d.n_vertices % 3 != 0) {
+                delete s;
+                return nullptr;
+            }
+            g.n_faces = d.n_vertices / 3;
+            g.position = f3(d.position, d.n);
+            g.orientation = q4(d.orientation, d.n);
+            g.vertices = f3(d.vertices, d.n_vertices);
+            g.color = c3(d.color, d.n_vertices);
+            break;
+        default:
+            delete s;
+            return nullptr;
+        }
+        if (!d.enabled)
+            continue;
+        uint32_t np = g.prim_count();
+        for (uint32_t p = 0; p < np; ++p) {
+            Box bx = prim_box(g, p);
+            bool ok = true;
+            for (int k = 0; k < 3; ++k)
+                ok = ok && std::isfinite(bx.lo[k]) && std::isfinite(bx.hi[k]) && bx.lo[k] <= bx.hi[k];
+            if (!ok)
+                continue;  // invalid primitive (e.g. infinite radius) is never hit
+            s->refs.push_back(PrimRef{gi, p});
+            b.boxes.push_back(bx);
+        }
+    }
+    size_t n = s->refs.size();
+    if (n > 0) {
+        b.cent.resize(n);
+        b.idx.resize(n);
+        for (size_t i = 0; i < n; ++i) {
+            const Box& bx = b.boxes[i];
+            b.cent[i] = F3{0.5f * (bx.lo[0] + bx.hi[0]), 0.5f * (bx.lo[1] + bx.hi[1]),
+                           0.5f * (bx.lo[2] + bx.hi[2])};
+            b.idx[i] = uint32_t(i);
+        }
+        s->nodes.reserve(2 * n);
+        b.build(0, uint32_t(n));
+        std::vector<PrimRef> sorted(n);
+        for (size_t i = 0; i < n; ++i)
+            sorted[i] = s->refs[b.idx[i]];
+        s->refs.swap(sorted);
+    }
+    return s;
+}
+
+void or_scene_destroy(or_scene* s) { delete s; }
+
+void or_scene_info(const or_scene* s, uint64_t* nodes, uint64_t* prims)
+{
+    if (nodes)
+        *nodes = s->nodes.size();
+    if (prims)
+        *prims = s->refs.size();
+}
+
+int or_trace(const or_scene* s, const float o[3], const float d[3], float tnear, float* t,
+             uint32_t* geom, uint32_t* prim)
+{
+    Counters c;
+    Hit h = trace(*s, F3{o[0], o[1], o[2]}, F3{d[0], d[1], d[2]}, tnear, c);
+    if (h.geom == UINT32_MAX)
+        return 0;
+    *t = h.t;
+    *geom = h.geom;
+    *prim = h.prim;
+    return 1;
+}
+
+int or_render_path(const or_scene* s, const fr_render_params* p, uint32_t w, uint32_t h,
+                   uint32_t first_sample, uint32_t n_render, uint32_t light_samples, float* linear,
+                   uint8_t* srgb, float* m2, const uint32_t* pixels, uint32_t n_pixels,
+                   int nan_guard, int nthreads, or_stats* stats)
+{
+    if (!s || !p || w == 0 || h == 0 || light_samples == 0 || !linear || !srgb)
+        return 1;
+    const uint32_t seed = p->seed;
+    const M::Cam cam = M::make_camera(to_camera(p->camera), w, h, seed, true);
+    const frm::LightsW lights = world_lights(p->lights, cam);
+    const RGB3 bg{p->background_color[0], p->background_color[1], p->background_color[2]};
+    const float bg_alpha = p->background_alpha;
+
+    const uint32_t TS = 4;  // 4x4 tiles (fresnel/cpu/TracerPath.cc:78-83)
+    const uint32_t ntx = (w + TS - 1) / TS, nty = (h + TS - 1) / TS;
+    const uint32_t n_items = pixels ? (n_pixels + 15) / 16 : ntx * nty;
+    int nt = nthreads <= 0 ? int(std::max(1u, std::thread::hardware_concurrency())) : nthreads;
+    std::vector<Counters> cnt(size_t(std::max(1, nt)));
+
+    auto shade_pixel = [&](uint32_t i, uint32_t j, uint32_t slot, Counters& c) {
+        const uint32_t key0 = j * w + i;
+        for (uint32_t k = 0; k < n_render; ++k) {
+            const uint32_t n_samples = first_sample + k;
+            PathState st;
+            st.result = RGB3{0, 0, 0};
+            st.a = 1.0f;
+            st.origin = F3{0, 0, 0};
+            st.dir = F3{0, 0, 0};
+            F3 o0, d0;
+            M::camera_ray(cam, i, j, n_samples, o0, d0);
+            Hit h0 = trace(*s, o0, d0, 1e-3f, c);
+            for (st.light_sample = 0; st.light_sample < light_samples; st.light_sample++) {
+                st.att = RGB3{1.0f, 1.0f, 1.0f};
+                st.done = false;
+                c.paths++;
+                for (st.depth = 0;; st.depth++) {
+                    Hit hh;
+                    F3 ro, rd;
+                    if (st.depth == 0) {
+                        hh = h0;
+                        ro = o0;
+                        rd = d0;
+                    } else {
+                        ro = st.origin;
+                        rd = st.dir;
+                        hh = trace(*s, ro, rd, 1e-3f, c);
+                    }
+                    if (hh.geom != UINT32_MAX) {
+                        const Geom& g = s->geoms[hh.geom];
+                        M::path_hit(st, g.material, g.outline, hh.d, g.outline_width, hh.color,
+                                    hh.Ng, ro, rd, hh.t, key0, seed, n_samples, light_samples);
+                    } else {
+                        M::path_miss(st, bg, bg_alpha, light_samples, lights, rd);
+                    }
+                    if (st.done)
+                        break;
+                }
+            }
+            // Welford running mean (fresnel/cpu/TracerPath.cc:228-239)
+            RGB3 out = frm::rgb_div_recip(st.result, float(light_samples));
+            float* px = linear + size_t(slot) * 4;
+            float q = 1.0f / float(n_samples);
+            float nm[4] = {px[0] + (out.r - px[0]) * q, px[1] + (out.g - px[1]) * q,
+                           px[2] + (out.b - px[2]) * q, px[3] + (st.a - px[3]) * q};
+            bool fin = std::isfinite(nm[0]) && std::isfinite(nm[1]) && std::isfinite(nm[2]);
+            if (!fin)
+                c.nonfinite++;
+            if (!fin && nan_guard) {
+                // keep the previous mean (fresnel/gpu/path.cu:111-113)
+            } else {
+                if (m2) {
+                    float* mm = m2 + size_t(slot) * 3;
+                    float xs[3] = {out.r, out.g, out.b};
+                    for (int kk = 0; kk < 3; ++kk)
+                        mm[kk] += (xs[kk] - px[kk]) * (xs[kk] - nm[kk]);
+                }
+                px[0] = nm[0];
+                px[1] = nm[1];
+                px[2] = nm[2];
+                px[3] = nm[3];
+            }
+            write_srgb(*p, px, srgb + size_t(slot) * 4);
+        }
+    };
+
+    parallel_tiles(n_items, nt, [&](uint32_t item, int tid) {
+        Counters& c = cnt[size_t(tid)];
+        if (pixels) {
+            uint32_t b0 = item * 16, b1 = std::min(n_pixels, b0 + 16);
+            for (uint32_t k = b0; k < b1; ++k) {
+                uint32_t pix = pixels[k];
+                shade_pixel(pix % w, pix / w, k, c);
+            }
+            return;
+        }
+        uint32_t ty = item / ntx, tx = item - ty * ntx;
+        uint32_t x0 = tx * TS, x1 = std::min(x0 + TS, w);
+        uint32_t y0 = ty * TS, y1 = std::min(y0 + TS, h);
+        for (uint32_t j = y0; j < y1; ++j)
+            for (uint32_t i = x0; i < x1; ++i)
+                shade_pixel(i, j, j * w + i, c);
+    });
+    if (stats) {
+        for (auto& c : cnt) {
+            stats->rays += c.rays;
+            stats->box_tests += c.box;
+            stats->prim_tests += c.prim;
+            stats->paths += c.paths;
+            stats->nonfinite += c.nonfinite;
+        }
+    }
+    return 0;
+}
+
+int or_render_preview(const or_scene* s, const fr_render_params* p, uint32_t w, uint32_t h,
+                      uint32_t aa_n, float* linear, uint8_t* srgb, uint32_t* hit_ids,
+                      int nthreads, or_stats* stats)
+{
+    if (!s || !p || w == 0 || h == 0 || aa_n == 0 || !linear || !srgb)
+        return 1;
+    fr_user_camera uc = p->camera;
+    uc.f_stop = std::numeric_limits<float>::infinity();  // no depth of field in preview
+    const bool sample_aa = (aa_n != 1);
+    const M::Cam cam = M::make_camera(to_camera(uc), w, h, p->seed, sample_aa);
+    const frm::LightsW lights = world_lights(p->lights, cam);
+    const RGB3 bg{p->background_color[0], p->background_color[1], p->background_color[2]};
+    const float bg_alpha = p->background_alpha;
+    const uint32_t TS = 4;
+    const uint32_t ntx = (w + TS - 1) / TS, nty = (h + TS - 1) / TS;
+    int nt = nthreads <= 0 ? int(std::max(1u, std::thread::hardware_concurrency())) : nthreads;
+    std::vector<Counters> cnt(size_t(std::max(1, nt)));
+    const uint32_t ns = aa_n * aa_n;
+
+    parallel_tiles(ntx * nty, nt, [&](uint32_t item, int tid) {
+        Counters& c = cnt[size_t(tid)];
+        uint32_t ty = item / ntx, tx = item - ty * ntx;
+        uint32_t x0 = tx * TS, x1 = std::min(x0 + TS, w);
+        uint32_t y0 = ty * TS, y1 = std::min(y0 + TS, h);
+        for (uint32_t j = y0; j < y1; ++j)
+            for (uint32_t i = x0; i < x1; ++i) {
+                float avg[4] = {0, 0, 0, 0};
+                for (uint32_t sample = 0; sample < ns; ++sample) {
+                    F3 org, dir;
+                    M::camera_ray(cam, i, j, sample, org, dir);
+                    Hit hh = trace(*s, org, dir, 0.0f, c);
+                    c.paths++;
+                    RGB3 col = bg;
+                    float a = bg_alpha;
+                    if (hit_ids) {
+                        uint32_t* hp = hit_ids + ((size_t(j) * w + i) * ns + sample) * 2;
+                        hp[0] = hh.geom == UINT32_MAX ? 0u : hh.geom + 1u;
+                        hp[1] = hh.geom == UINT32_MAX ? 0u : hh.prim;
+                    }
+                    if (hh.geom != UINT32_MAX) {
+                        using frm::dot;
+                        const Geom& g = s->geoms[hh.geom];
+                        F3 n = frm::div_each(hh.Ng, std::sqrt(dot(hh.Ng, hh.Ng)));
+                        F3 v = frm::div_recip(-dir, std::sqrt(dot(dir, dir)));
+                        const Mat& m = (hh.d >= g.outline_width) ? g.material : g.outline;
+                        if (M::is_solid(m)) {
+                            col = M::base_color(m, hh.color);
+                        } else {
+                            col = RGB3{0, 0, 0};
+                            for (unsigned li = 0; li < lights.n; ++li) {
+                                F3 l = lights.dir[li];
+                                F3 r = -v + (2.0f * n * dot(n, v));
+                                float half = lights.theta[li];
+                                float cos_half = cosf(half);
+                                float ldotr = dot(l, r);
+                                if (ldotr < cos_half) {
+                                    F3 ax = frm::cross(l, r);
+                                    ax = frm::div_recip(ax, sqrtf(dot(ax, ax)));
+                                    Quat q = M::from_axis_angle(ax, -acosf(ldotr) + half);
+                                    r = M::rotate(q, r);
+                                }
+                                RGB3 f_d{0, 0, 0}, f_s{0, 0, 0};
+                                float ndotl = dot(n, l);
+                                if (ndotl >= 0.0f)
+                                    f_d = M::brdf_diffuse(m, l, v, n, hh.color) * ndotl;
+                                if (dot(n, r) >= 0.0f)
+                                    f_s = M::brdf_specular(m, r, v, n, hh.color, half) * dot(n, r);
+                                col = col + (f_d + f_s) * float(M_PI) * lights.color[li];
+                            }
+                        }
+                        a = 1.0f;
+                    }
+                    avg[0] += col.r;
+                    avg[1] += col.g;
+                    avg[2] += col.b;
+                    avg[3] += a;
+                }
+                float q = 1.0f / float(ns);
+                float* px = linear + (size_t(j) * w + i) * 4;
+                px[0] = avg[0] * q;
+                px[1] = avg[1] * q;
+                px[2] = avg[2] * q;
+                px[3] = avg[3] * q;
+                write_srgb(*p, px, srgb + (size_t(j) * w + i) * 4);
+            }
+    });
+    if (stats) {
+        for (auto& c : cnt) {
+            stats->rays += c.rays;
+            stats->box_tests += c.box;
+            stats->prim_tests += c.prim;
+            stats->paths += c.paths;
+        }
+    }
+    return 0;
+}
+
+void or_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4])
+{
+    frm::Ctr4 c{{ctr[0], ctr[1], ctr[2], ctr[3]}};
+    frm::Ctr4 r = frm::philox4x32_10(c, key[0], key[1]);
+    for (int k = 0; k < 4; ++k)
+        out[k] = r.v[k];
+}
+
+float or_u01(uint32_t x) { return frm::u01(x); }
+
+void or_srgb(const float rgba[4], uint8_t out[4]) { M::srgb_encode(rgba, out); }
+
+void or_camera_ray(const fr_user_camera* c, uint32_t w, uint32_t h, uint32_t seed, int sample_aa,
+                   uint32_t i, uint32_t j, uint32_t sample, float o[3], float d[3])
+{
+    M::Cam cam = M::make_camera(to_camera(*c), w, h, seed, sample_aa != 0);
+    F3 oo, dd;
+    M::camera_ray(cam, i, j, sample, oo, dd);
+    o[0] = oo.x;
+    o[1] = oo.y;
+    o[2] = oo.z;
+    d[0] = dd.x;
+    d[1] = dd.y;
+    d[2] = dd.z;
+}
+
+void or_mis_sample(const fr_material* m, const float v[3], const float n[3], uint32_t depth,
+                   uint32_t sample, uint32_t key0, uint32_t key1, float out[5])
+{
+    float factor = 1.0f;
+    bool transmit = false;
+    F3 l = M::mis_direction(factor, transmit, F3{v[0], v[1], v[2]}, F3{n[0], n[1], n[2]}, depth,
+                            sample, key0, key1, to_mat(*m));
+    out[0] = l.x;
+    out[1] = l.y;
+    out[2] = l.z;
+    out[3] = factor;
+    out[4] = transmit ? 1.0f : 0.0f;
+}
+
+void or_brdf(const fr_material* m, const float l[3], const float v[3], const float n[3],
+             const float sc[3], float out[3])
+{
+    RGB3 r = M::brdf(to_mat(*m), F3{l[0], l[1], l[2]}, F3{v[0], v[1], v[2]}, F3{n[0], n[1], n[2]},
+                     RGB3{sc[0], sc[1], sc[2]});
+    out[0] = r.r;
+    out[1] = r.g;
+    out[2] = r.b;
+}
+
+}  // extern "C"
