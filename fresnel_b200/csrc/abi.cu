@@ -89,6 +89,8 @@ struct fr_device {
     BuildParams build;
     LaunchShape shape{};
     DevArray<uint32_t> status;  // traversal error bits
+    cudaEvent_t timer[2] = {nullptr, nullptr};
+    bool profiling = false;
 };
 
 struct fr_geometry {
@@ -166,6 +168,49 @@ struct fr_tracer {
     uint64_t launches = 0;
     uint64_t builds = 0;
     double build_ms = 0.0;
+    // per-kernel timing while profiling: event pairs pending readback, by kernel kind
+    std::vector<cudaEvent_t> event_pool;
+    struct Pending {
+        cudaEvent_t a, b;
+        int kind;  // 0 primary, 1 shade, 2 extend
+    };
+    std::vector<Pending> pending;
+    double kernel_ms[3] = {0, 0, 0};
+    uint64_t kernel_launches[3] = {0, 0, 0};
+    ~fr_tracer()
+    {
+        for (cudaEvent_t e : event_pool)
+            cudaEventDestroy(e);
+        for (auto& p : pending) {
+            cudaEventDestroy(p.a);
+            cudaEventDestroy(p.b);
+        }
+    }
+    cudaEvent_t take_event()
+    {
+        if (!event_pool.empty()) {
+            cudaEvent_t e = event_pool.back();
+            event_pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+    // call after the stream has been synchronised
+    void collect()
+    {
+        for (auto& p : pending) {
+            float ms = 0.0f;
+            if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+                kernel_ms[p.kind] += ms;
+                kernel_launches[p.kind]++;
+            }
+            event_pool.push_back(p.a);
+            event_pool.push_back(p.b);
+        }
+        pending.clear();
+    }
 };
 
 namespace {
@@ -244,7 +289,8 @@ fr_status prepare_scene(fr_scene* sc, fr_tracer* tr)
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
         cudaEventRecord(e0, dev->stream);
-        cudaError_t e = build_bvh(in, g->bvh_prims(), dev->build, g->bvh, dev->scratch, dev->stream);
+        cudaError_t e = build_bvh(in, g->bvh_prims(), dev->build, g->bvh, dev->scratch,
+                                  dev->status.ptr, dev->stream);
         cudaEventRecord(e1, dev->stream);
         cudaEventSynchronize(e1);
         float ms = 0.0f;
@@ -254,6 +300,16 @@ fr_status prepare_scene(fr_scene* sc, fr_tracer* tr)
         if (e != cudaSuccess)
             return cuda_fail(e, "building a BVH");
         g->last_build_ms = ms;
+        {
+            uint32_t stw = 0;
+            FR_CUDA(cudaMemcpy(&stw, dev->status.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost),
+                    "reading the build status");
+            if (stw & ERR_BUILD) {
+                cudaMemset(dev->status.ptr, 0, sizeof(uint32_t));
+                g->bvh.n_nodes = 0;
+                return fail(FR_ERR_DEVICE_LIMIT, "BVH construction produced an inconsistent tree");
+            }
+        }
         if (tr) {
             tr->builds++;
             tr->build_ms = ms;
@@ -346,9 +402,10 @@ fr_status check_status(fr_device* dev)
     FR_CUDA(cudaStreamSynchronize(dev->stream), "render");
     if (st) {
         FR_CUDA(cudaMemsetAsync(dev->status.ptr, 0, sizeof(uint32_t), dev->stream), "status reset");
-        return fail(FR_ERR_DEVICE_LIMIT, (st & ERR_STACK_OVERFLOW)
-                                             ? "BVH traversal stack overflow (tree too deep)"
-                                             : "BVH traversal iteration cap reached");
+        return fail(FR_ERR_DEVICE_LIMIT,
+                    (st & ERR_STACK_OVERFLOW) ? "BVH traversal stack overflow (tree too deep)"
+                    : (st & ERR_BAD_NODE)     ? "BVH traversal met an out-of-range node"
+                                              : "BVH traversal iteration cap reached");
     }
     return FR_OK;
 }
@@ -509,6 +566,9 @@ fr_status fr_device_destroy(fr_device* d)
         cudaStreamSynchronize(d->stream);
         cudaStreamDestroy(d->stream);
     }
+    for (int k = 0; k < 2; ++k)
+        if (d->timer[k])
+            cudaEventDestroy(d->timer[k]);
     delete d;
     return FR_OK;
 }
@@ -527,7 +587,39 @@ fr_status fr_device_describe(const fr_device* d, char* buf, size_t cap)
 fr_status fr_device_synchronize(fr_device* d)
 {
     FR_CHECK_NULL(d);
+    FR_CUDA(cudaSetDevice(d->ordinal), "cudaSetDevice");
     FR_CUDA(cudaStreamSynchronize(d->stream), "cudaStreamSynchronize");
+    return FR_OK;
+}
+
+fr_status fr_device_timer_start(fr_device* d)
+{
+    FR_CHECK_NULL(d);
+    FR_CUDA(cudaSetDevice(d->ordinal), "cudaSetDevice");
+    for (int k = 0; k < 2; ++k)
+        if (!d->timer[k])
+            FR_CUDA(cudaEventCreate(&d->timer[k]), "creating a timer event");
+    FR_CUDA(cudaEventRecord(d->timer[0], d->stream), "recording the timer start");
+    return FR_OK;
+}
+
+fr_status fr_device_timer_stop(fr_device* d, float* ms)
+{
+    FR_CHECK_NULL(d);
+    FR_CHECK_NULL(ms);
+    if (!d->timer[0] || !d->timer[1])
+        return fail(FR_ERR_STATE, "the timer was not started");
+    FR_CUDA(cudaSetDevice(d->ordinal), "cudaSetDevice");
+    FR_CUDA(cudaEventRecord(d->timer[1], d->stream), "recording the timer stop");
+    FR_CUDA(cudaEventSynchronize(d->timer[1]), "waiting for the timer stop");
+    FR_CUDA(cudaEventElapsedTime(ms, d->timer[0], d->timer[1]), "reading the timer");
+    return FR_OK;
+}
+
+fr_status fr_device_set_profiling(fr_device* d, int enable)
+{
+    FR_CHECK_NULL(d);
+    d->profiling = enable != 0;
     return FR_OK;
 }
 
@@ -872,14 +964,27 @@ fr_status fr_tracer_render_path(fr_tracer* t, fr_scene* sc, const fr_render_para
     cudaStream_t st = t->dev->stream;
     const int CHECK_EVERY = 4;
     const int MAX_ITER = 1 << 20;
+    const bool prof = t->dev->profiling;
+    auto timed = [&](int kind, auto&& launch) {
+        if (!prof) {
+            launch();
+            return;
+        }
+        cudaEvent_t a = t->take_event(), b = t->take_event();
+        cudaEventRecord(a, st);
+        launch();
+        cudaEventRecord(b, st);
+        t->pending.push_back({a, b, kind});
+    };
     for (uint32_t k = 0; k < n_render; ++k) {
         P.n_samples = first_sample + k;
-        launch_path_primary(P, S, st);
+        timed(0, [&] { launch_path_primary(P, S, st); });
         t->launches++;
         int it = 0;
         while (true) {
             for (int b = 0; b < CHECK_EVERY; ++b, ++it) {
-                launch_path_iteration(P, S, it, t->dev->shape, st);
+                timed(1, [&] { launch_path_shade(P, S, it, t->dev->shape, st); });
+                timed(2, [&] { launch_path_extend(P, S, it, t->dev->shape, st); });
                 t->launches += 2;
             }
             FR_CUDA(cudaGetLastError(), "launching the path tracer");
@@ -887,6 +992,7 @@ fr_status fr_tracer_render_path(fr_tracer* t, fr_scene* sc, const fr_render_para
                                     cudaMemcpyDeviceToHost, st),
                     "reading the queue length");
             FR_CUDA(cudaStreamSynchronize(st), "path tracer");
+            t->collect();
             if (*t->h_count == 0)
                 break;
             if (it >= MAX_ITER)
@@ -1000,6 +1106,12 @@ fr_status fr_tracer_get_stats(const fr_tracer* t, fr_stats* out)
     out->kernel_launches = t->launches;
     out->bvh_builds = t->builds;
     out->bvh_build_ms = t->build_ms;
+    out->primary_ms = t->kernel_ms[0];
+    out->shade_ms = t->kernel_ms[1];
+    out->extend_ms = t->kernel_ms[2];
+    out->primary_launches = t->kernel_launches[0];
+    out->shade_launches = t->kernel_launches[1];
+    out->extend_launches = t->kernel_launches[2];
     return FR_OK;
 }
 
@@ -1012,6 +1124,10 @@ fr_status fr_tracer_reset_stats(fr_tracer* t)
     FR_CUDA(cudaStreamSynchronize(t->dev->stream), "clearing tracer counters");
     t->launches = 0;
     t->builds = 0;
+    for (int k = 0; k < 3; ++k) {
+        t->kernel_ms[k] = 0.0;
+        t->kernel_launches[k] = 0;
+    }
     return FR_OK;
 }
 

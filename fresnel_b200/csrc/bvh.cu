@@ -250,19 +250,27 @@ __global__ void k_refit(uint32_t n, const uint32_t* sorted_vals, const float4* b
                         const float4* box_hi, const int2* range, const uint32_t* split,
                         const uint32_t* parent_int, const uint32_t* parent_leaf, uint32_t* arrive,
                         NodeInfo* info, uint8_t* collapse, int leaf_max, float c_trav,
-                        float c_isect)
+                        float c_isect, uint32_t* status)
 {
     uint32_t leaf = blockIdx.x * blockDim.x + threadIdx.x;
     if (leaf >= n || n < 2)
         return;
     uint32_t node = parent_leaf[leaf];
-    while (true) {
+    for (int guard = 0;; ++guard) {
+        if (node >= n - 1 || guard > 200) {  // unset parent or a cycle: report, never follow
+            atomicOr(status, ERR_BUILD);
+            return;
+        }
         __threadfence();
         if (atomicAdd(arrive + node, 1u) == 0u)
             return;
         __threadfence();
         uint32_t g = split[node];
         int2 rg = range[node];
+        if (g + 1u >= n) {
+            atomicOr(status, ERR_BUILD);
+            return;
+        }
         float4 lo[2], hi[2];
         float cost[2];
         float cnt[2];
@@ -318,6 +326,8 @@ __global__ void k_mark(uint32_t n, const uint32_t* split, const uint32_t* parent
     uint32_t a = i;
     for (int guard = 0; a != 0 && guard < 4096; ++guard) {
         a = parent_int[a];
+        if (a >= n - 1)
+            break;  // unset parent: reported by the refit pass
         if (collapse[a]) {
             rem = true;
             break;
@@ -354,6 +364,8 @@ __global__ void k_emit(uint32_t n, const int2* range, const uint32_t* split,
     uint32_t g = split[i];
     int2 rg = range[i];
     uint32_t base = 1u + 2u * pair_index[g];
+    if (base + 1u >= 2u * n - 1u)  // both children must fit in the 2n-1 node slots
+        return;
     for (int c = 0; c < 2; ++c) {
         uint32_t idx = g + uint32_t(c);
         bool is_leaf = (c == 0) ? (uint32_t(rg.x) == g) : (uint32_t(rg.y) == g + 1);
@@ -422,7 +434,7 @@ inline uint32_t blocks_for(size_t n, int threads) { return uint32_t((n + threads
 size_t leaf_record_float4s(int type) { return type == FR_GEOM_SPHERE ? 1 : 2; }
 
 cudaError_t build_bvh(const BuildInput& in, uint32_t n, const BuildParams& bp, BvhBuffers& out,
-                      Scratch& scratch, cudaStream_t st)
+                      Scratch& scratch, uint32_t* status, cudaStream_t st)
 {
     out.n_nodes = 0;
     if (n == 0)
@@ -506,13 +518,18 @@ cudaError_t build_bvh(const BuildInput& in, uint32_t n, const BuildParams& bp, B
         k_single_leaf<<<1, 1, 0, st>>>(box_lo, box_hi, out.nodes.ptr);
         out.n_nodes = 1;
     } else {
+        // unset parents read as 0xffffffff (out of range) and are reported, never followed
+        if ((e = cudaMemsetAsync(parent_int, 0xff, n * sizeof(uint32_t), st)) != cudaSuccess)
+            return e;
+        if ((e = cudaMemsetAsync(parent_leaf, 0xff, n * sizeof(uint32_t), st)) != cudaSuccess)
+            return e;
         k_karras<<<blocks_for(n - 1, T), T, 0, st>>>(n, keys_sorted, range, split, parent_int,
                                                     parent_leaf);
         if ((e = cudaMemsetAsync(arrive, 0, n * sizeof(uint32_t), st)) != cudaSuccess)
             return e;
         k_refit<<<blocks_for(n, T), T, 0, st>>>(n, vals_sorted, box_lo, box_hi, range, split,
                                                 parent_int, parent_leaf, arrive, info, collapse,
-                                                bp.leaf_max, bp.c_trav, bp.c_isect);
+                                                bp.leaf_max, bp.c_trav, bp.c_isect, status);
         if ((e = cudaMemsetAsync(keep, 0, n * sizeof(uint32_t), st)) != cudaSuccess)
             return e;
         k_mark<<<blocks_for(n - 1, T), T, 0, st>>>(n, split, parent_int, collapse, keep, removed);

@@ -101,8 +101,10 @@ size_t leaf_record_float4s(int type);
 
 // Build the BVH of n primitives (n == 0 leaves an empty tree).  Synchronises the stream once
 // to read back the node count.
+// Construction errors (an inconsistent hierarchy) are reported by or-ing ERR_BUILD into
+// *status; no kernel follows an out-of-range index.
 cudaError_t build_bvh(const BuildInput& in, uint32_t n, const BuildParams& bp, BvhBuffers& out,
-                      Scratch& scratch, cudaStream_t st);
+                      Scratch& scratch, uint32_t* status, cudaStream_t st);
 
 }  // namespace fr
 

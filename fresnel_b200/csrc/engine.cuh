@@ -29,6 +29,8 @@ constexpr uint32_t MISS = 0xFFFFFFFFu;
 // error bits reported through the device status word
 constexpr uint32_t ERR_STACK_OVERFLOW = 1u;
 constexpr uint32_t ERR_ITERATION_CAP = 2u;
+constexpr uint32_t ERR_BAD_NODE = 4u;    // a BVH index out of range (never followed)
+constexpr uint32_t ERR_BUILD = 8u;       // BVH construction found an inconsistent hierarchy
 
 struct GeomDev {
     int32_t type;
@@ -133,6 +135,10 @@ __device__ __forceinline__ PolyHit poly_planes(const GeomDev& g, V3 o, V3 d, V3 
 {
     PolyHit r;
     r.hit = false;
+    r.t = 0.0f;
+    r.plane = 0;
+    r.n = v3(0, 0, 1);
+    r.p = v3(0, 0, 0);
     float t0 = -3.402823466e+38f, t1 = 3.402823466e+38f;
     V3 dl = rotate(conj(q), d);
     V3 ol = rotate(conj(q), o - pos);
@@ -262,7 +268,12 @@ __device__ __forceinline__ void traverse(const GeomDev& g, uint32_t gi, const Ra
         return;
     uint32_t rb = __float_as_uint(rhi.w);
     if (rb != 0) {
-        leaf_test<TYPE>(g, gi, ray, __float_as_uint(rlo.w), rb, tnear, tmax, hit_geom, hit_slot);
+        uint32_t first = __float_as_uint(rlo.w);
+        if (first > g.n_prims || rb > g.n_prims - first) {
+            atomicOr(status, ERR_BAD_NODE);
+            return;
+        }
+        leaf_test<TYPE>(g, gi, ray, first, rb, tnear, tmax, hit_geom, hit_slot);
         return;
     }
     uint32_t stack_node[TRAVERSAL_STACK];
@@ -275,12 +286,23 @@ __device__ __forceinline__ void traverse(const GeomDev& g, uint32_t gi, const Ra
             atomicOr(status, ERR_ITERATION_CAP);
             return;
         }
+        if (cur + 1u >= g.n_nodes) {  // the child pair must lie inside the node array
+            atomicOr(status, ERR_BAD_NODE);
+            return;
+        }
         const float4* np = g.nodes + 2 * size_t(cur);
         float4 alo = ldg4(np), ahi = ldg4(np + 1), blo = ldg4(np + 2), bhi = ldg4(np + 3);
         float ta, tb;
         bool ha = slab(ray, alo, ahi, tmax, ta);
         bool hb = slab(ray, blo, bhi, tmax, tb);
         uint32_t ca = __float_as_uint(ahi.w), cb = __float_as_uint(bhi.w);
+        if ((ca != 0 && (__float_as_uint(alo.w) > g.n_prims ||
+                         ca > g.n_prims - __float_as_uint(alo.w))) ||
+            (cb != 0 && (__float_as_uint(blo.w) > g.n_prims ||
+                         cb > g.n_prims - __float_as_uint(blo.w)))) {
+            atomicOr(status, ERR_BAD_NODE);
+            return;
+        }
         if (ha && ca != 0) {
             leaf_test<TYPE>(g, gi, ray, __float_as_uint(alo.w), ca, tnear, tmax, hit_geom, hit_slot);
             ha = false;

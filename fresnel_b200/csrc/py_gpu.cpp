@@ -422,6 +422,12 @@ struct TracerH {
         d["kernel_launches"] = st.kernel_launches;
         d["bvh_builds"] = st.bvh_builds;
         d["bvh_build_ms"] = st.bvh_build_ms;
+        d["primary_ms"] = st.primary_ms;
+        d["shade_ms"] = st.shade_ms;
+        d["extend_ms"] = st.extend_ms;
+        d["primary_launches"] = st.primary_launches;
+        d["shade_launches"] = st.shade_launches;
+        d["extend_launches"] = st.extend_launches;
         return d;
     }
 };
@@ -510,6 +516,14 @@ PYBIND11_MODULE(_gpu, m)
     py::class_<DeviceH, std::shared_ptr<DeviceH>>(m, "Device")
         .def(py::init<const std::string&, int>())
         .def("describe", &DeviceH::describe)
+        .def("synchronize", [](DeviceH& d) { check(fr_device_synchronize(d.dev)); })
+        .def("timerStart", [](DeviceH& d) { check(fr_device_timer_start(d.dev)); })
+        .def("timerStop", [](DeviceH& d) {
+            float ms = 0.0f;
+            check(fr_device_timer_stop(d.dev, &ms));
+            return ms;
+        })
+        .def("setProfiling", [](DeviceH& d, bool on) { check(fr_device_set_profiling(d.dev, on)); })
         .def_static("getAllGPUs", &DeviceH::all_gpus);
 
     py::class_<SceneH, std::shared_ptr<SceneH>>(m, "Scene")

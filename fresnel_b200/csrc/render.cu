@@ -299,13 +299,17 @@ void launch_path_primary(const FrameParams& P, const PathState& S, cudaStream_t 
     k_path_primary<<<grid, block, 0, st>>>(P, S);
 }
 
-void launch_path_iteration(const FrameParams& P, const PathState& S, int iteration,
-                           const LaunchShape& shape, cudaStream_t st)
+void launch_path_shade(const FrameParams& P, const PathState& S, int iteration,
+                       const LaunchShape& shape, cudaStream_t st)
 {
     int in_q = iteration == 0 ? -1 : ((iteration - 1) & 1);
-    int out_q = iteration & 1;
-    k_path_shade<<<shape.shade_grid, 256, 0, st>>>(P, S, in_q, out_q);
-    k_path_extend<<<shape.extend_grid, 256, 0, st>>>(P, S, out_q);
+    k_path_shade<<<shape.shade_grid, 256, 0, st>>>(P, S, in_q, iteration & 1);
+}
+
+void launch_path_extend(const FrameParams& P, const PathState& S, int iteration,
+                        const LaunchShape& shape, cudaStream_t st)
+{
+    k_path_extend<<<shape.extend_grid, 256, 0, st>>>(P, S, iteration & 1);
 }
 
 void launch_preview(const FrameParams& P, uint32_t aa_n, uint2* hits, cudaStream_t st)

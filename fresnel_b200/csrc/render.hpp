@@ -53,8 +53,10 @@ LaunchShape path_launch_shape(int num_sms);
 void launch_path_primary(const FrameParams& P, const PathState& S, cudaStream_t st);
 // ... then iteration i of shade (queue in = i == 0 ? every pixel : q[(i-1)&1], out = q[i&1])
 // and extend (q[i&1]) until the output queue is empty.
-void launch_path_iteration(const FrameParams& P, const PathState& S, int iteration,
-                           const LaunchShape& shape, cudaStream_t st);
+void launch_path_shade(const FrameParams& P, const PathState& S, int iteration,
+                       const LaunchShape& shape, cudaStream_t st);
+void launch_path_extend(const FrameParams& P, const PathState& S, int iteration,
+                        const LaunchShape& shape, cudaStream_t st);
 // TracerDirect::render
 void launch_preview(const FrameParams& P, uint32_t aa_n, uint2* hits, cudaStream_t st);
 

@@ -1,0 +1,161 @@
+"""Synthetic scenes for the benchmark configurations and the parity tests.
+
+The reference publishes no benchmark data; these seeded generators stand in for the scenes its
+benchmark configurations describe (uniformly placed spheres at a given density, bonds between
+neighbours, randomly oriented cubes, icosahedron instances).  Every builder takes a fresnel-API
+``device`` so the same scene can be built on the GPU engine and on the CPU oracle.
+"""
+
+import math
+
+import numpy
+
+from . import Scene, camera, color, geometry, light, material
+
+
+def perspective_fit(scene, focal_length=0.5):
+    """Perspective camera framing the scene like ``Orthographic.fit``: same position, look_at
+    and up; the image-plane height at the focus distance equals the orthographic height."""
+    ortho = camera.Orthographic.fit(scene)
+    d = float(numpy.linalg.norm(ortho.position - ortho.look_at))
+    return camera.Perspective(position=ortho.position, look_at=ortho.look_at, up=ortho.up,
+                              focal_length=focal_length, focus_distance=d, f_stop=math.inf,
+                              height=focal_length * ortho.height / d)
+
+
+def hex_spheres(device):
+    """Six spheres on a hexagon with outlines (the reference test fixture scene)."""
+    lights = [light.Light(direction=(math.sin(70 * math.pi / 180) * math.sin(45 * math.pi / 180),
+                                     math.cos(70 * math.pi / 180),
+                                     math.sin(70 * math.pi / 180) * math.cos(45 * math.pi / 180)),
+                          color=(0.75, 0.75, 0.75), theta=math.pi / 8),
+              light.Light(direction=(math.sin(math.pi / 2) * math.sin(-math.pi / 4),
+                                     math.cos(math.pi / 2),
+                                     math.sin(math.pi / 2) * math.cos(-math.pi / 4)),
+                          color=(0.1, 0.1, 0.1), theta=math.pi / 2)]
+    scene = Scene(device, lights=lights)
+    pos = [[2 * math.cos(i * 2 * math.pi / 6), 2 * math.sin(i * 2 * math.pi / 6), 0]
+           for i in range(6)]
+    g = geometry.Sphere(scene, position=pos, radius=1.0)
+    g.material = material.Material(solid=0.0, color=color.linear([1, 0.874, 0.169]))
+    g.outline_width = 0.12
+    scene.camera = camera.Orthographic(position=(0, 0, 10), look_at=(0, 0, 0), up=(0, 1, 0),
+                                       height=6)
+    return scene
+
+
+def random_spheres(device, n, box, radius=0.5, seed=0, colors=False, outline_width=0.0,
+                   mat=None, lights=None, perspective=True):
+    """n spheres uniform in a cube of side ``box`` (float32, numpy default_rng(seed))."""
+    rng = numpy.random.default_rng(seed)
+    pos = rng.uniform(-box / 2, box / 2, (n, 3)).astype(numpy.float32)
+    scene = Scene(device, lights=lights if lights is not None else light.cloudy())
+    g = geometry.Sphere(scene, position=pos, radius=radius, outline_width=outline_width)
+    if colors:
+        g.color[:] = rng.uniform(0, 1, (n, 3)).astype(numpy.float32)
+    g.material = mat if mat is not None else material.Material(
+        color=color.linear((0.1, 0.8, 0.1)), roughness=0.8, specular=0.2)
+    scene.camera = perspective_fit(scene) if perspective else camera.Orthographic.fit(scene)
+    return scene
+
+
+def config1(device):
+    """1000 spheres r=0.5 in a cube of side 20, outline 0.1, cloudy lights (580x580, 64 spp,
+    32 light samples in the benchmark)."""
+    return random_spheres(device, 1000, 20.0, 0.5, seed=0, outline_width=0.1,
+                          mat=material.Material(color=color.linear((0.1, 0.8, 0.1)),
+                                                roughness=0.8, specular=0.2))
+
+
+def config2(device, n=1_000_000, box=140.0):
+    """1M spheres r=0.5 in a cube of side 140 with per-particle colours, lightbox
+    (1920x1080, 256 spp, 1 light sample in the benchmark).  ``n``/``box`` scale it down at the
+    same density for tests."""
+    return random_spheres(device, n, box, 0.5, seed=1, colors=True,
+                          mat=material.Material(roughness=0.4, metal=0.0, specular=0.5,
+                                                primitive_color_mix=1.0),
+                          lights=light.lightbox())
+
+
+def icosahedron(circumradius=0.5):
+    """20 triangles (60 vertices, counter-clockwise seen from outside) of a regular icosahedron."""
+    p = (1 + math.sqrt(5)) / 2
+    v = numpy.array([[-1, p, 0], [1, p, 0], [-1, -p, 0], [1, -p, 0], [0, -1, p], [0, 1, p],
+                     [0, -1, -p], [0, 1, -p], [p, 0, -1], [p, 0, 1], [-p, 0, -1], [-p, 0, 1]],
+                    dtype=numpy.float64)
+    v *= circumradius / numpy.linalg.norm(v[0])
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4),
+             (11, 10, 2), (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8),
+             (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    tri = numpy.array([[v[a], v[b], v[c]] for a, b, c in faces])
+    # orient every face counter-clockwise seen from outside
+    for t in tri:
+        n = numpy.cross(t[1] - t[0], t[2] - t[0])
+        if numpy.dot(n, t.mean(axis=0)) < 0:
+            t[[1, 2]] = t[[2, 1]]
+    return tri.reshape(-1, 3).astype(numpy.float32)
+
+
+def unit_cube_planes():
+    """Face planes of a unit cube centred at the origin (radius sqrt(3)/2)."""
+    origins, normals = [], []
+    for k in range(3):
+        for s in (-1, 1):
+            n = [0, 0, 0]
+            n[k] = s
+            o = [0, 0, 0]
+            o[k] = 0.5 * s
+            origins.append(o)
+            normals.append(n)
+    return {'face_origin': numpy.array(origins, numpy.float32),
+            'face_normal': numpy.array(normals, numpy.float32),
+            'face_color': numpy.full((6, 3), 0.9, numpy.float32),
+            'radius': math.sqrt(3) / 2}
+
+
+def random_quaternions(rng, n):
+    q = rng.normal(size=(n, 4))
+    q /= numpy.linalg.norm(q, axis=1, keepdims=True)
+    return q.astype(numpy.float32)
+
+
+def bonds(rng, pos, n_bonds, cutoff=1.5):
+    """Pairs (i, j) with |p_i - p_j| < cutoff, i drawn uniformly (scipy cKDTree)."""
+    from scipy.spatial import cKDTree
+    tree = cKDTree(pos)
+    out = []
+    tries = 0
+    while len(out) < n_bonds and tries < 50 * n_bonds:
+        tries += 1
+        i = int(rng.integers(len(pos)))
+        nb = [j for j in tree.query_ball_point(pos[i], cutoff) if j != i]
+        if nb:
+            out.append((i, nb[int(rng.integers(len(nb)))]))
+    return numpy.array(out, dtype=numpy.int64).reshape(-1, 2)
+
+
+def config3(device, scale=1.0, box=100.0):
+    """Mixed scene: 200k spheres (r log-uniform in [0.3, 0.7]), 50k bonds (r = 0.1), 20k unit
+    cubes and 10k icosahedra in a cube of side 100 (1280x720, 128 spp in the benchmark).
+    ``scale`` shrinks every count (and the box at constant density) for tests."""
+    rng = numpy.random.default_rng(2)
+    L = box * scale**(1 / 3)
+    ns, nb, nc, nm = (max(1, int(round(x * scale))) for x in (200_000, 50_000, 20_000, 10_000))
+    scene = Scene(device, lights=light.rembrandt())
+    pos = rng.uniform(-L / 2, L / 2, (ns, 3)).astype(numpy.float32)
+    rad = numpy.exp(rng.uniform(math.log(0.3), math.log(0.7), ns)).astype(numpy.float32)
+    geometry.Sphere(scene, position=pos, radius=rad, color=(0.6, 0.6, 0.6))
+    pairs = bonds(rng, pos, nb)
+    if len(pairs):
+        pts = numpy.stack([pos[pairs[:, 0]], pos[pairs[:, 1]]], axis=1)
+        geometry.Cylinder(scene, points=pts, radius=0.1, color=(0.3, 0.3, 0.8))
+    cpos = rng.uniform(-L / 2, L / 2, (nc, 3)).astype(numpy.float32)
+    poly = geometry.ConvexPolyhedron(scene, unit_cube_planes(), position=cpos,
+                                     orientation=random_quaternions(rng, nc), color=(0.8, 0.3, 0.2))
+    poly.material = material.Material(color=(0.8, 0.3, 0.2), metal=0.5, roughness=0.3)
+    mpos = rng.uniform(-L / 2, L / 2, (nm, 3)).astype(numpy.float32)
+    verts = icosahedron(0.5)
+    geometry.Mesh(scene, verts, position=mpos, orientation=random_quaternions(rng, nm),
+                  color=numpy.full((len(verts), 3), 0.7, numpy.float32))
+    scene.camera = perspective_fit(scene)
+    return scene

@@ -117,6 +117,9 @@ typedef struct fr_stats {
     uint64_t kernel_launches;
     uint64_t bvh_builds;
     double bvh_build_ms;    /* device time of the last BVH build of any geometry */
+    /* per-kernel device time, accumulated only while profiling is on (fr_device_set_profiling) */
+    double primary_ms, shade_ms, extend_ms;
+    uint64_t primary_launches, shade_launches, extend_launches;
 } fr_stats;
 
 typedef struct fr_device fr_device;
@@ -141,6 +144,14 @@ FR_API fr_status fr_device_destroy(fr_device* dev);
 /* Device::describe (fresnel/gpu/Device.cc:114-128). */
 FR_API fr_status fr_device_describe(const fr_device* dev, char* buf, size_t cap);
 FR_API fr_status fr_device_synchronize(fr_device* dev);
+/* Device time between two points of the engine's stream: start records a CUDA event, stop
+ * records another, waits for it and returns the elapsed milliseconds.  No counterpart in the
+ * reference (its OptiX launches are synchronous); used to time renders on the device. */
+FR_API fr_status fr_device_timer_start(fr_device* dev);
+FR_API fr_status fr_device_timer_stop(fr_device* dev, float* ms);
+/* When enabled, every kernel launch of the path tracer is bracketed by CUDA events and its
+ * device time is accumulated in fr_stats (primary/shade/extend).  Off by default. */
+FR_API fr_status fr_device_set_profiling(fr_device* dev, int enable);
 
 /* ---------------- scene: fresnel/gpu/Scene.cc ---------------- */
 
@@ -220,6 +231,15 @@ FR_API fr_status fr_tracer_write_linear(fr_tracer* tr, const float* host, size_t
 FR_API fr_status fr_tracer_write_srgb(fr_tracer* tr, const uint8_t* host, size_t nbytes);
 FR_API fr_status fr_tracer_get_stats(const fr_tracer* tr, fr_stats* out);
 FR_API fr_status fr_tracer_reset_stats(fr_tracer* tr);
+
+/* ---------------- self-tests ---------------- */
+
+/* Runs the engine's device Philox4x32-10 and cuRAND's curand_Philox4x32_10 on n inputs
+ * in[i] = (ctr0, ctr1, ctr2, ctr3, key0, key1) (host arrays; outputs n x 4 words each).
+ * No counterpart in the reference: Random123's known-answer vectors are not in its tree, and
+ * this is how the generator behind fresnel/common/RayGen.h:49-61 is checked on the device. */
+FR_API fr_status fr_selftest_philox(const uint32_t* in, uint32_t n, uint32_t* engine_out,
+                                    uint32_t* curand_out);
 
 #ifdef __cplusplus
 }

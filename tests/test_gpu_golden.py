@@ -1,0 +1,26 @@
+"""The GPU engine against the committed golden fixtures (oracle outputs frozen after the oracle
+was pinned to the reference).  Runs on machines without the reference tree."""
+
+import os
+
+import numpy
+import pytest
+
+from golden import make_golden
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+@pytest.mark.parametrize("name", list(make_golden.CASES))
+def test_engine_matches_golden(name, gpu_device):
+    out = make_golden.render(name, gpu_device)
+    ref = numpy.load(os.path.join(HERE, "golden", name + ".npz"))
+    if "hits" in out:
+        mism = numpy.any(out["hits"] != ref["hits"], axis=-1).mean()
+        assert mism <= 1e-4
+        assert numpy.abs(out["linear"] - ref["linear"]).max() <= 1e-3
+    else:
+        close = numpy.all(numpy.abs(out["linear"] - ref["linear"]) <= 1e-3, axis=-1).mean()
+        assert close >= 0.99, f"{close:.4%} of pixels within 1e-3"
+        numpy.testing.assert_array_equal(out["srgb"][..., 3], ref["srgb"][..., 3])
