@@ -159,7 +159,7 @@ struct fr_tracer {
     DevArray<float4> linear;
     DevArray<uint32_t> srgb;
     // path tracer state
-    DevArray<float4> prim_o, prim_d, ray_o, ray_d, att, result;
+    DevArray<float4> prim_o, prim_d, ray_o, ray_d, att, result, sample;
     DevArray<uint2> prim_hit, ls_depth, hit;
     DevArray<uint32_t> q0, q1, ctr;
     DevArray<uint2> preview_hits;
@@ -422,15 +422,32 @@ fr_status alloc_outputs(fr_tracer* tr, uint32_t w, uint32_t h)
     return FR_OK;
 }
 
-fr_status alloc_path_state(fr_tracer* tr)
+// Path slots traced together: a batch of K samples of every pixel (about 144 bytes each).
+constexpr size_t PATH_SLOT_BUDGET = size_t(32) << 20;
+
+uint32_t batch_size(const fr_tracer* tr, uint32_t remaining)
 {
-    size_t n = size_t(tr->w) * tr->h;
+    size_t wh = size_t(tr->w) * tr->h;
+    size_t k = PATH_SLOT_BUDGET / (wh ? wh : 1);
+    if (k < 1)
+        k = 1;
+    if (k > 4096)
+        k = 4096;  // the primary kernel's grid z dimension
+    if (k > remaining)
+        k = remaining;
+    return uint32_t(k);
+}
+
+fr_status alloc_path_state(fr_tracer* tr, uint32_t batch)
+{
+    size_t n = size_t(tr->w) * tr->h * batch;
     FR_CUDA(tr->prim_o.reserve(n), "path state");
     FR_CUDA(tr->prim_d.reserve(n), "path state");
     FR_CUDA(tr->ray_o.reserve(n), "path state");
     FR_CUDA(tr->ray_d.reserve(n), "path state");
     FR_CUDA(tr->att.reserve(n), "path state");
     FR_CUDA(tr->result.reserve(n), "path state");
+    FR_CUDA(tr->sample.reserve(n), "path state");
     FR_CUDA(tr->prim_hit.reserve(n), "path state");
     FR_CUDA(tr->ls_depth.reserve(n), "path state");
     FR_CUDA(tr->hit.reserve(n), "path state");
@@ -452,6 +469,7 @@ PathState path_state(fr_tracer* tr)
     S.result = tr->result.ptr;
     S.ls_depth = tr->ls_depth.ptr;
     S.hit = tr->hit.ptr;
+    S.sample = tr->sample.ptr;
     S.queue[0] = tr->q0.ptr;
     S.queue[1] = tr->q1.ptr;
     S.ctr = tr->ctr.ptr;
@@ -884,9 +902,9 @@ fr_status fr_tracer_create(fr_device* dev, uint32_t w, uint32_t h, fr_tracer** o
     if (!t)
         return fail(FR_ERR_OUT_OF_MEMORY, "out of host memory");
     t->dev = dev;
-    cudaError_t e = t->stats.reserve(4);
+    cudaError_t e = t->stats.reserve(8);
     if (e == cudaSuccess)
-        e = cudaMemsetAsync(t->stats.ptr, 0, 4 * sizeof(unsigned long long), dev->stream);
+        e = cudaMemsetAsync(t->stats.ptr, 0, 8 * sizeof(unsigned long long), dev->stream);
     if (e == cudaSuccess)
         e = cudaMallocHost((void**)&t->h_count, 4 * sizeof(uint32_t));
     if (e != cudaSuccess) {
@@ -956,13 +974,14 @@ fr_status fr_tracer_render_path(fr_tracer* t, fr_scene* sc, const fr_render_para
         return s;
     if ((s = prepare_scene(sc, t)) != FR_OK)
         return s;
-    if ((s = alloc_path_state(t)) != FR_OK)
+    uint32_t batch = batch_size(t, n_render);
+    if ((s = alloc_path_state(t, batch)) != FR_OK)
         return s;
     FrameParams P = frame_params(t, sc, p, false, 1);
     P.light_samples = light_samples;
     PathState S = path_state(t);
     cudaStream_t st = t->dev->stream;
-    const int CHECK_EVERY = 4;
+    const int CHECK_EVERY = 8;
     const int MAX_ITER = 1 << 20;
     const bool prof = t->dev->profiling;
     auto timed = [&](int kind, auto&& launch) {
@@ -976,8 +995,9 @@ fr_status fr_tracer_render_path(fr_tracer* t, fr_scene* sc, const fr_render_para
         cudaEventRecord(b, st);
         t->pending.push_back({a, b, kind});
     };
-    for (uint32_t k = 0; k < n_render; ++k) {
-        P.n_samples = first_sample + k;
+    for (uint32_t done = 0; done < n_render;) {
+        P.n_samples = first_sample + done;
+        P.batch = batch < n_render - done ? batch : n_render - done;
         timed(0, [&] { launch_path_primary(P, S, st); });
         t->launches++;
         int it = 0;
@@ -998,6 +1018,9 @@ fr_status fr_tracer_render_path(fr_tracer* t, fr_scene* sc, const fr_render_para
             if (it >= MAX_ITER)
                 return fail(FR_ERR_DEVICE_LIMIT, "path tracer exceeded the bounce iteration cap");
         }
+        launch_path_fold(P, S, st);
+        t->launches++;
+        done += P.batch;
     }
     return check_status(t->dev);
 }
@@ -1095,7 +1118,7 @@ fr_status fr_tracer_get_stats(const fr_tracer* t, fr_stats* out)
 {
     FR_CHECK_NULL(t);
     FR_CHECK_NULL(out);
-    unsigned long long v[4] = {0, 0, 0, 0};
+    unsigned long long v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     FR_CUDA(cudaSetDevice(t->dev->ordinal), "cudaSetDevice");
     FR_CUDA(cudaMemcpyAsync(v, t->stats.ptr, sizeof(v), cudaMemcpyDeviceToHost, t->dev->stream),
             "reading tracer counters");
@@ -1103,6 +1126,8 @@ fr_status fr_tracer_get_stats(const fr_tracer* t, fr_stats* out)
     out->rays = v[0];
     out->paths = v[1];
     out->dropped = v[2];
+    out->box_tests = v[3];
+    out->prim_tests = v[4];
     out->kernel_launches = t->launches;
     out->bvh_builds = t->builds;
     out->bvh_build_ms = t->build_ms;
@@ -1119,7 +1144,7 @@ fr_status fr_tracer_reset_stats(fr_tracer* t)
 {
     FR_CHECK_NULL(t);
     FR_CUDA(cudaSetDevice(t->dev->ordinal), "cudaSetDevice");
-    FR_CUDA(cudaMemsetAsync(t->stats.ptr, 0, 4 * sizeof(unsigned long long), t->dev->stream),
+    FR_CUDA(cudaMemsetAsync(t->stats.ptr, 0, 8 * sizeof(unsigned long long), t->dev->stream),
             "clearing tracer counters");
     FR_CUDA(cudaStreamSynchronize(t->dev->stream), "clearing tracer counters");
     t->launches = 0;

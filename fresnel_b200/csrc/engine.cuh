@@ -214,11 +214,19 @@ __device__ __forceinline__ TriHit mesh_triangle(const GeomDev& g, uint32_t face,
     return r;
 }
 
+// box and primitive tests of one thread (summed into the tracer's counters per warp)
+struct TraceCount {
+    uint32_t box = 0;
+    uint32_t prim = 0;
+};
+
 template <int TYPE>
 __device__ __forceinline__ void leaf_test(const GeomDev& g, uint32_t gi, const RayK& ray,
                                           uint32_t first, uint32_t count, float tnear,
-                                          float& tmax, uint32_t& hit_geom, uint32_t& hit_slot)
+                                          float& tmax, uint32_t& hit_geom, uint32_t& hit_slot,
+                                          TraceCount& tc)
 {
+    tc.prim += count;
     for (uint32_t s = first; s < first + count; ++s) {
         float t = 0.0f;
         bool ok;
@@ -258,11 +266,12 @@ __device__ __forceinline__ void leaf_test(const GeomDev& g, uint32_t gi, const R
 template <int TYPE>
 __device__ __forceinline__ void traverse(const GeomDev& g, uint32_t gi, const RayK& ray, float tnear,
                                          float& tmax, uint32_t& hit_geom, uint32_t& hit_slot,
-                                         uint32_t* status)
+                                         uint32_t* status, TraceCount& tc)
 {
     if (g.n_nodes == 0)
         return;
     float te;
+    tc.box += 1;
     float4 rlo = ldg4(g.nodes), rhi = ldg4(g.nodes + 1);
     if (!slab(ray, rlo, rhi, tmax, te))
         return;
@@ -273,7 +282,7 @@ __device__ __forceinline__ void traverse(const GeomDev& g, uint32_t gi, const Ra
             atomicOr(status, ERR_BAD_NODE);
             return;
         }
-        leaf_test<TYPE>(g, gi, ray, first, rb, tnear, tmax, hit_geom, hit_slot);
+        leaf_test<TYPE>(g, gi, ray, first, rb, tnear, tmax, hit_geom, hit_slot, tc);
         return;
     }
     uint32_t stack_node[TRAVERSAL_STACK];
@@ -293,6 +302,7 @@ __device__ __forceinline__ void traverse(const GeomDev& g, uint32_t gi, const Ra
         const float4* np = g.nodes + 2 * size_t(cur);
         float4 alo = ldg4(np), ahi = ldg4(np + 1), blo = ldg4(np + 2), bhi = ldg4(np + 3);
         float ta, tb;
+        tc.box += 2;
         bool ha = slab(ray, alo, ahi, tmax, ta);
         bool hb = slab(ray, blo, bhi, tmax, tb);
         uint32_t ca = __float_as_uint(ahi.w), cb = __float_as_uint(bhi.w);
@@ -304,13 +314,14 @@ __device__ __forceinline__ void traverse(const GeomDev& g, uint32_t gi, const Ra
             return;
         }
         if (ha && ca != 0) {
-            leaf_test<TYPE>(g, gi, ray, __float_as_uint(alo.w), ca, tnear, tmax, hit_geom, hit_slot);
+            leaf_test<TYPE>(g, gi, ray, __float_as_uint(alo.w), ca, tnear, tmax, hit_geom, hit_slot,
+                            tc);
             ha = false;
         }
         if (hb && cb != 0) {
             if (tb <= tmax)
                 leaf_test<TYPE>(g, gi, ray, __float_as_uint(blo.w), cb, tnear, tmax, hit_geom,
-                                hit_slot);
+                                hit_slot, tc);
             hb = false;
         }
         if (ha && hb) {
@@ -359,7 +370,8 @@ struct Hit {
 };
 
 // Closest hit over all enabled geometries of the scene.
-__device__ __forceinline__ Hit trace_closest(const SceneDev& sc, V3 o, V3 d, float tnear)
+__device__ __forceinline__ Hit trace_closest(const SceneDev& sc, V3 o, V3 d, float tnear,
+                                             TraceCount& tc)
 {
     RayK ray = make_rayk(o, d);
     float tmax = __int_as_float(0x7f800000);  // +inf
@@ -370,16 +382,16 @@ __device__ __forceinline__ Hit trace_closest(const SceneDev& sc, V3 o, V3 d, flo
             continue;
         switch (g.type) {
         case FR_GEOM_SPHERE:
-            traverse<FR_GEOM_SPHERE>(g, gi, ray, tnear, tmax, hg, hs, sc.status);
+            traverse<FR_GEOM_SPHERE>(g, gi, ray, tnear, tmax, hg, hs, sc.status, tc);
             break;
         case FR_GEOM_CYLINDER:
-            traverse<FR_GEOM_CYLINDER>(g, gi, ray, tnear, tmax, hg, hs, sc.status);
+            traverse<FR_GEOM_CYLINDER>(g, gi, ray, tnear, tmax, hg, hs, sc.status, tc);
             break;
         case FR_GEOM_POLYHEDRON:
-            traverse<FR_GEOM_POLYHEDRON>(g, gi, ray, tnear, tmax, hg, hs, sc.status);
+            traverse<FR_GEOM_POLYHEDRON>(g, gi, ray, tnear, tmax, hg, hs, sc.status, tc);
             break;
         default:
-            traverse<FR_GEOM_MESH>(g, gi, ray, tnear, tmax, hg, hs, sc.status);
+            traverse<FR_GEOM_MESH>(g, gi, ray, tnear, tmax, hg, hs, sc.status, tc);
             break;
         }
     }
@@ -387,6 +399,20 @@ __device__ __forceinline__ Hit trace_closest(const SceneDev& sc, V3 o, V3 d, flo
     h.geom = hg;
     h.prim = (hg == MISS) ? 0u : __ldg(sc.geoms[hg].order + hs);
     return h;
+}
+
+// Add the warp's traversal counts to counters[0] (box tests) and counters[1] (primitive tests).
+__device__ __forceinline__ void flush_counts(const TraceCount& tc, unsigned long long* counters)
+{
+    unsigned long long b = tc.box, p = tc.prim;
+    for (int off = 16; off > 0; off >>= 1) {
+        b += __shfl_xor_sync(0xffffffffu, b, off);
+        p += __shfl_xor_sync(0xffffffffu, p, off);
+    }
+    if ((threadIdx.x & 31u) == 0u && (b | p)) {
+        atomicAdd(counters, b);
+        atomicAdd(counters + 1, p);
+    }
 }
 
 // --------------------------------------------------------------------------------------------

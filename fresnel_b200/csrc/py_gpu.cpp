@@ -33,6 +33,25 @@ void check(fr_status s)
 }
 
 // ---------------------------------------------------------------------------------------------
+// engine objects with shared ownership: an Array keeps the object whose buffer it exposes
+// alive (the reference's Array holds its OptiX buffer the same way, fresnel/gpu/Array.h:98-223)
+// ---------------------------------------------------------------------------------------------
+struct DeviceH;
+struct SceneH;
+
+struct TracerCore {
+    std::shared_ptr<DeviceH> device;
+    fr_tracer* tracer = nullptr;
+    ~TracerCore() { fr_tracer_destroy(tracer); }
+};
+
+struct GeometryCore {
+    std::shared_ptr<SceneH> scene;
+    fr_geometry* geom = nullptr;
+    ~GeometryCore() { fr_geometry_destroy(geom); }
+};
+
+// ---------------------------------------------------------------------------------------------
 // arrays
 // ---------------------------------------------------------------------------------------------
 struct ArrayBase {
@@ -43,8 +62,10 @@ struct ArrayBase {
     bool mapped = false;
     bool stale = false;     // host copy newer than the device copy (geometry arrays)
     // owner: a geometry field or a tracer output
+    std::shared_ptr<GeometryCore> gcore;
     fr_geometry* geom = nullptr;
     int field = -1;
+    std::shared_ptr<TracerCore> tcore;
     fr_tracer* tracer = nullptr;
     int output = -1;  // 0 linear, 1 srgb
 
@@ -164,6 +185,7 @@ struct SceneH {
 
 struct GeometryH {
     std::shared_ptr<SceneH> scene;
+    std::shared_ptr<GeometryCore> core;
     fr_geometry* geom = nullptr;
     bool valid = false;
     Material material, outline;
@@ -182,10 +204,21 @@ struct GeometryH {
         outline.roughness = 0.1f;
         outline.specular = 0.5f;
     }
+    // ~Geometry removes the geometry from its scene (fresnel/cpu/Geometry.cc:18-21); its
+    // buffers live on while an Array still refers to them.
     virtual ~GeometryH()
     {
         scene->geoms.erase(this);
-        fr_geometry_destroy(geom);
+        if (geom)
+            fr_geometry_remove(geom);
+    }
+    // take ownership of a geometry just created by the engine
+    void own(fr_geometry* g)
+    {
+        geom = g;
+        core = std::make_shared<GeometryCore>();
+        core->scene = scene;
+        core->geom = g;
     }
     void attach()
     {
@@ -196,6 +229,7 @@ struct GeometryH {
     template <class A> std::shared_ptr<A> add_array(int field, std::vector<py::ssize_t> shape)
     {
         auto a = make_array<A>(std::move(shape));
+        a->gcore = core;
         a->geom = geom;
         a->field = field;
         arrays.push_back(a);
@@ -264,7 +298,11 @@ struct GeometrySphereH : GeometryH {
     std::shared_ptr<ArrayRGBf> color;
     GeometrySphereH(std::shared_ptr<SceneH> s, unsigned n) : GeometryH(std::move(s))
     {
-        check(fr_geometry_create_sphere(scene->scene, n, &geom));
+        {
+            fr_geometry* g = nullptr;
+            check(fr_geometry_create_sphere(scene->scene, n, &g));
+            own(g);
+        }
         position = add_array<ArrayVec3f>(FR_FIELD_POSITION, {py::ssize_t(n), 3});
         radius = add_array<Array_f>(FR_FIELD_RADIUS, {py::ssize_t(n)});
         color = add_array<ArrayRGBf>(FR_FIELD_COLOR, {py::ssize_t(n), 3});
@@ -278,7 +316,11 @@ struct GeometryCylinderH : GeometryH {
     std::shared_ptr<ArrayRGBf> color;
     GeometryCylinderH(std::shared_ptr<SceneH> s, unsigned n) : GeometryH(std::move(s))
     {
-        check(fr_geometry_create_cylinder(scene->scene, n, &geom));
+        {
+            fr_geometry* g = nullptr;
+            check(fr_geometry_create_cylinder(scene->scene, n, &g));
+            own(g);
+        }
         points = add_array<ArrayVec3f>(FR_FIELD_POINTS, {py::ssize_t(n), 2, 3});
         radius = add_array<Array_f>(FR_FIELD_RADIUS, {py::ssize_t(n)});
         color = add_array<ArrayRGBf>(FR_FIELD_COLOR, {py::ssize_t(n), 2, 3});
@@ -313,9 +355,10 @@ struct GeometryConvexPolyhedronH : GeometryH {
         require_nx3(colors, "plane_colors", "Nvert");
         if (colors.shape(0) != origins.shape(0))
             throw std::runtime_error("Number of vertices must match in origin and color arrays");
+        fr_geometry* g = nullptr;
         check(fr_geometry_create_polyhedron(scene->scene, origins.data(), normals.data(),
-                                            colors.data(), unsigned(origins.shape(0)), n, r,
-                                            &geom));
+                                            colors.data(), unsigned(origins.shape(0)), n, r, &g));
+        own(g);
         position = add_array<ArrayVec3f>(FR_FIELD_POSITION, {py::ssize_t(n), 3});
         orientation = add_array<ArrayQuat3f>(FR_FIELD_ORIENTATION, {py::ssize_t(n), 4});
         color = add_array<ArrayRGBf>(FR_FIELD_COLOR, {py::ssize_t(n), 3});
@@ -343,7 +386,9 @@ struct GeometryMeshH : GeometryH {
         if (vertices.shape(0) % 3 != 0)
             throw std::runtime_error("the number of triangle vertices must be a multiple of three.");
         unsigned nv = unsigned(vertices.shape(0));
-        check(fr_geometry_create_mesh(scene->scene, vertices.data(), nv, n, &geom));
+        fr_geometry* g = nullptr;
+        check(fr_geometry_create_mesh(scene->scene, vertices.data(), nv, n, &g));
+        own(g);
         position = add_array<ArrayVec3f>(FR_FIELD_POSITION, {py::ssize_t(n), 3});
         orientation = add_array<ArrayQuat3f>(FR_FIELD_ORIENTATION, {py::ssize_t(n), 4});
         color = add_array<ArrayRGBf>(FR_FIELD_COLOR, {py::ssize_t(nv), 3});
@@ -356,6 +401,7 @@ struct GeometryMeshH : GeometryH {
 // ---------------------------------------------------------------------------------------------
 struct TracerH {
     std::shared_ptr<DeviceH> device;
+    std::shared_ptr<TracerCore> core;
     fr_tracer* tracer = nullptr;
     unsigned w = 0, h = 0;
     unsigned seed = 0;
@@ -366,18 +412,23 @@ struct TracerH {
 
     TracerH(std::shared_ptr<DeviceH> d, unsigned w_, unsigned h_) : device(std::move(d))
     {
-        check(fr_tracer_create(device->dev, w_, h_, &tracer));
+        core = std::make_shared<TracerCore>();
+        core->device = device;
+        check(fr_tracer_create(device->dev, w_, h_, &core->tracer));
+        tracer = core->tracer;
         make_outputs(w_, h_);
     }
-    virtual ~TracerH() { fr_tracer_destroy(tracer); }
+    virtual ~TracerH() = default;
     void make_outputs(unsigned w_, unsigned h_)
     {
         w = w_;
         h = h_;
         linear = make_array<ArrayRGBAf>({py::ssize_t(h), py::ssize_t(w), 4});
+        linear->tcore = core;
         linear->tracer = tracer;
         linear->output = 0;
         srgb = make_array<ArrayRGBAc>({py::ssize_t(h), py::ssize_t(w), 4}, true);
+        srgb->tcore = core;
         srgb->tracer = tracer;
         srgb->output = 1;
     }
@@ -419,6 +470,8 @@ struct TracerH {
         d["rays"] = st.rays;
         d["paths"] = st.paths;
         d["dropped"] = st.dropped;
+        d["box_tests"] = st.box_tests;
+        d["prim_tests"] = st.prim_tests;
         d["kernel_launches"] = st.kernel_launches;
         d["bvh_builds"] = st.bvh_builds;
         d["bvh_build_ms"] = st.bvh_build_ms;

@@ -37,51 +37,49 @@ __device__ __forceinline__ void write_pixel(const FrameParams& P, uint32_t p, fl
         P.srgb[p] = srgb_pack(P.hl_color.r, P.hl_color.g, P.hl_color.b, a);
 }
 
-// Welford update of one pixel (fresnel/cpu/TracerPath.cc:228-250), dropping non-finite
-// samples as the GPU backend does (fresnel/gpu/path.cu:111-113).
-__device__ __forceinline__ void finish_pixel(const FrameParams& P, uint32_t p, C3 result,
-                                             bool primary_miss)
+// Welford update of one pixel with one sample (fresnel/cpu/TracerPath.cc:228-250), dropping
+// non-finite samples as the GPU backend does (fresnel/gpu/path.cu:111-113).
+__device__ __forceinline__ float4 welford(const FrameParams& P, float4 old, float4 x, uint32_t n)
 {
-    float4 old = P.linear[p];
-    C3 out = c_div_recip(result, float(P.light_samples));
-    float a = primary_miss ? P.bg_alpha : 1.0f;
-    float q = 1.0f / float(P.n_samples);
-    float nr = old.x + (out.r - old.x) * q;
-    float ng = old.y + (out.g - old.y) * q;
-    float nb = old.z + (out.b - old.z) * q;
-    float na = old.w + (a - old.w) * q;
+    float q = 1.0f / float(n);
+    float nr = old.x + (x.x - old.x) * q;
+    float ng = old.y + (x.y - old.y) * q;
+    float nb = old.z + (x.z - old.z) * q;
+    float na = old.w + (x.w - old.w) * q;
     if (!(isfinite(nr) && isfinite(ng) && isfinite(nb))) {
         atomicAdd(P.stats + 2, 1ull);
-        nr = old.x;
-        ng = old.y;
-        nb = old.z;
-        na = old.w;
+        return old;
     }
-    write_pixel(P, p, nr, ng, nb, na);
+    return make_float4(nr, ng, nb, na);
 }
 
 __global__ void __launch_bounds__(256) k_path_primary(FrameParams P, PathState S)
 {
-    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && threadIdx.y == 0) {
+    if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0 &&
+        threadIdx.y == 0) {
         S.ctr[0] = 0;
         S.ctr[1] = 0;
         S.ctr[2] = 0;
     }
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t j = blockIdx.y * blockDim.y + threadIdx.y;
+    uint32_t k = blockIdx.z;
     bool valid = (i < P.w) && (j < P.h);
+    TraceCount tc;
     if (valid) {
         uint32_t p = j * P.w + i;
+        size_t slot = size_t(k) * P.w * P.h + p;
         V3 o, d;
-        camera_ray(P.cam, i, j, P.n_samples, o, d);
-        Hit h = trace_closest(P.scene, o, d, PATH_TNEAR);
-        S.prim_o[p] = f4(o);
-        S.prim_d[p] = f4(d);
-        S.prim_hit[p] = make_uint2(h.geom, h.prim);
-        S.ls_depth[p] = make_uint2(0u, 0u);
-        S.att[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-        S.result[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        camera_ray(P.cam, i, j, P.n_samples + k, o, d);
+        Hit h = trace_closest(P.scene, o, d, PATH_TNEAR, tc);
+        S.prim_o[slot] = f4(o);
+        S.prim_d[slot] = f4(d);
+        S.prim_hit[slot] = make_uint2(h.geom, h.prim);
+        S.ls_depth[slot] = make_uint2(0u, 0u);
+        S.att[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+        S.result[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     }
+    flush_counts(tc, P.stats + 3);
     uint32_t m = __ballot_sync(0xffffffffu, valid);
     if ((threadIdx.x + threadIdx.y * blockDim.x) % 32 == 0 && m) {
         atomicAdd(P.stats + 0, (unsigned long long)__popc(m));
@@ -89,9 +87,27 @@ __global__ void __launch_bounds__(256) k_path_primary(FrameParams P, PathState S
     }
 }
 
-// Shade one pixel's current path vertex; returns true if the path needs another closest hit.
+// Fold the batch's samples into the running mean of each pixel, in sample order, then write
+// the sRGB output once.
+__global__ void __launch_bounds__(256) k_path_fold(FrameParams P, PathState S)
+{
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t wh = P.w * P.h;
+    if (p >= wh)
+        return;
+    float4 mean = P.linear[p];
+    for (uint32_t k = 0; k < P.batch; ++k)
+        mean = welford(P, mean, S.sample[size_t(k) * wh + p], P.n_samples + k);
+    write_pixel(P, p, mean.x, mean.y, mean.z, mean.w);
+}
+
+// Shade the current path vertex of one slot; returns true if the path needs another closest hit.
 __device__ __forceinline__ bool shade_pixel(const FrameParams& P, const PathState& S, uint32_t p)
 {
+    const uint32_t wh = P.w * P.h;
+    const uint32_t k = p / wh;
+    const uint32_t pixel = p - k * wh;
+    const uint32_t n_samples = P.n_samples + k;
     uint2 ld = S.ls_depth[p];
     uint32_t ls = ld.x;
     PathS s;
@@ -118,9 +134,9 @@ __device__ __forceinline__ bool shade_pixel(const FrameParams& P, const PathStat
         if (h.x != MISS) {
             const GeomDev& g = P.scene.geoms[h.x];
             Surface sf = hit_surface(g, h.y, ro, rd, PATH_TNEAR);
-            uint32_t sample = (P.n_samples - 1u) * P.light_samples + ls;
+            uint32_t sample = (n_samples - 1u) * P.light_samples + ls;
             path_hit(s, g.material, g.outline, sf.d_edge, g.outline_width, sf.color, sf.Ng, ro, rd,
-                     sf.t, p, key1, sample);
+                     sf.t, pixel, key1, sample);
         } else if (s.depth == 0) {
             // a primary miss shows the background (fresnel/common/TracerPathMethods.h:44-50)
             s.result = P.bg * float(P.light_samples);
@@ -143,7 +159,9 @@ __device__ __forceinline__ bool shade_pixel(const FrameParams& P, const PathStat
             s.att = c3(1.0f, 1.0f, 1.0f);
             continue;
         }
-        finish_pixel(P, p, s.result, ph.x == MISS);
+        // the pixel sample (fresnel/cpu/TracerPath.cc:228): radiance / L, alpha
+        C3 out = c_div_recip(s.result, float(P.light_samples));
+        S.sample[p] = make_float4(out.r, out.g, out.b, ph.x == MISS ? P.bg_alpha : 1.0f);
         return false;
     }
 }
@@ -152,7 +170,7 @@ __global__ void __launch_bounds__(256) k_path_shade(FrameParams P, PathState S, 
 {
     if (blockIdx.x == 0 && threadIdx.x == 0)
         S.ctr[2] = 0;  // work counter of the extend kernel that follows
-    const uint32_t count = (in_q < 0) ? P.w * P.h : S.ctr[in_q];
+    const uint32_t count = (in_q < 0) ? P.w * P.h * P.batch : S.ctr[in_q];
     const uint32_t* inq = (in_q < 0) ? nullptr : S.queue[in_q];
     uint32_t* outq = S.queue[out_q];
     uint32_t* outc = S.ctr + out_q;
@@ -186,6 +204,7 @@ __global__ void __launch_bounds__(256) k_path_extend(FrameParams P, PathState S,
     const uint32_t count = S.ctr[q];
     const uint32_t* queue = S.queue[q];
     const uint32_t lane = threadIdx.x & 31u;
+    TraceCount tc;
     while (true) {
         uint32_t base = 0;
         if (lane == 0)
@@ -198,12 +217,13 @@ __global__ void __launch_bounds__(256) k_path_extend(FrameParams P, PathState S,
             uint32_t p = queue[idx];
             V3 o = xyz(S.ray_o[p]);
             V3 d = xyz(S.ray_d[p]);
-            Hit h = trace_closest(P.scene, o, d, PATH_TNEAR);
+            Hit h = trace_closest(P.scene, o, d, PATH_TNEAR, tc);
             S.hit[p] = make_uint2(h.geom, h.prim);
         }
         if (lane == 0)
             atomicAdd(P.stats + 0, (unsigned long long)min(32u, count - base));
     }
+    flush_counts(tc, P.stats + 3);
 }
 
 // Representative-point area-light shading of one preview sample
@@ -246,13 +266,14 @@ __global__ void __launch_bounds__(256) k_preview(FrameParams P, uint32_t aa_n, u
     uint32_t j = blockIdx.y * blockDim.y + threadIdx.y;
     bool valid = (i < P.w) && (j < P.h);
     const uint32_t ns = aa_n * aa_n;
+    TraceCount tc;
     if (valid) {
         uint32_t p = j * P.w + i;
         float avg[4] = {0.0f, 0.0f, 0.0f, 0.0f};
         for (uint32_t sample = 0; sample < ns; ++sample) {
             V3 o, d;
             camera_ray(P.cam, i, j, sample, o, d);
-            Hit h = trace_closest(P.scene, o, d, 0.0f);  // preview tnear is 0 on the CPU path
+            Hit h = trace_closest(P.scene, o, d, 0.0f, tc);  // preview tnear is 0 on the CPU path
             C3 c = P.bg;
             float a = P.bg_alpha;
             if (h.geom != MISS) {
@@ -272,6 +293,7 @@ __global__ void __launch_bounds__(256) k_preview(FrameParams P, uint32_t aa_n, u
         float q = 1.0f / float(ns);
         write_pixel(P, p, avg[0] * q, avg[1] * q, avg[2] * q, avg[3] * q);
     }
+    flush_counts(tc, P.stats + 3);
     uint32_t m = __ballot_sync(0xffffffffu, valid);
     if ((threadIdx.x + threadIdx.y * blockDim.x) % 32 == 0 && m) {
         atomicAdd(P.stats + 0, (unsigned long long)__popc(m) * ns);
@@ -295,8 +317,13 @@ LaunchShape path_launch_shape(int num_sms)
 void launch_path_primary(const FrameParams& P, const PathState& S, cudaStream_t st)
 {
     dim3 block(16, 16);
-    dim3 grid((P.w + 15) / 16, (P.h + 15) / 16);
+    dim3 grid((P.w + 15) / 16, (P.h + 15) / 16, P.batch);
     k_path_primary<<<grid, block, 0, st>>>(P, S);
+}
+
+void launch_path_fold(const FrameParams& P, const PathState& S, cudaStream_t st)
+{
+    k_path_fold<<<(P.w * P.h + 255) / 256, 256, 0, st>>>(P, S);
 }
 
 void launch_path_shade(const FrameParams& P, const PathState& S, int iteration,

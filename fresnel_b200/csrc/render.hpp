@@ -18,16 +18,18 @@ struct FrameParams {
     C3 bg;
     float bg_alpha;
     uint32_t w, h;
-    uint32_t n_samples;      // 1-based sample number of this render (TracerPath::m_n_samples)
+    uint32_t n_samples;      // 1-based sample number of the batch's first render
+    uint32_t batch;          // samples traced together (slot = k * w * h + pixel)
     uint32_t light_samples;  // light paths per primary ray
     int highlight;
     C3 hl_color;
     float4* linear;     // [h][w] running mean, linear RGBA
     uint32_t* srgb;     // [h][w] RGBA8
-    unsigned long long* stats;  // [0] rays, [1] paths, [2] dropped non-finite samples
+    unsigned long long* stats;  // [0] rays, [1] paths, [2] dropped, [3] box tests, [4] prim tests
 };
 
-// Per-pixel wavefront state of the path tracer (structure of arrays, w*h entries each).
+// Wavefront state of the path tracer (structure of arrays, one entry per path slot; a batch of
+// K samples uses K * w * h slots, slot = k * w * h + pixel).
 struct PathState {
     float4* prim_o;     // primary ray, shared by the light samples of a pixel sample
     float4* prim_d;
@@ -38,6 +40,7 @@ struct PathState {
     float4* result;     // radiance summed over the pixel's light samples so far
     uint2* ls_depth;    // (light sample, depth)
     uint2* hit;         // closest hit of the last extension ray
+    float4* sample;     // the finished pixel sample of each slot (folded in order at the end)
     uint32_t* queue[2];
     uint32_t* ctr;      // [0], [1] queue lengths, [2] extend work counter
 };
@@ -49,14 +52,16 @@ struct LaunchShape {
 
 LaunchShape path_launch_shape(int num_sms);
 
-// one TracerPath::render sample: primary rays (all pixels) ...
+// One batch of P.batch TracerPath::render samples: primary rays for every slot ...
 void launch_path_primary(const FrameParams& P, const PathState& S, cudaStream_t st);
-// ... then iteration i of shade (queue in = i == 0 ? every pixel : q[(i-1)&1], out = q[i&1])
-// and extend (q[i&1]) until the output queue is empty.
+// ... then iteration i of shade (queue in = i == 0 ? every slot : q[(i-1)&1], out = q[i&1])
+// and extend (q[i&1]) until the output queue is empty ...
 void launch_path_shade(const FrameParams& P, const PathState& S, int iteration,
                        const LaunchShape& shape, cudaStream_t st);
 void launch_path_extend(const FrameParams& P, const PathState& S, int iteration,
                         const LaunchShape& shape, cudaStream_t st);
+// ... then fold the batch's samples into each pixel's running mean, in sample order.
+void launch_path_fold(const FrameParams& P, const PathState& S, cudaStream_t st);
 // TracerDirect::render
 void launch_preview(const FrameParams& P, uint32_t aa_n, uint2* hits, cudaStream_t st);
 

@@ -114,6 +114,8 @@ typedef struct fr_stats {
     uint64_t rays;          /* closest-hit queries (primary rays shared across light samples) */
     uint64_t paths;         /* pixel samples x light samples */
     uint64_t dropped;       /* non-finite pixel samples not folded into the mean */
+    uint64_t box_tests;     /* ray/AABB tests of the BVH traversals */
+    uint64_t prim_tests;    /* ray/primitive intersection tests */
     uint64_t kernel_launches;
     uint64_t bvh_builds;
     double bvh_build_ms;    /* device time of the last BVH build of any geometry */
