@@ -97,6 +97,8 @@ def load(kind="restated"):
                                       ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _fp, _bp,
                                       _up, ctypes.c_int, ctypes.POINTER(OrStats)]
     lib.or_trace.argtypes = [ctypes.c_void_p, _fp, _fp, ctypes.c_float, _fp, _up, _up]
+    lib.or_prim_hit.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, _fp, _fp,
+                                ctypes.c_float, _fp]
     lib.or_philox4x32_10.argtypes = [_up, _up, _up]
     lib.or_u01.restype = ctypes.c_float
     lib.or_u01.argtypes = [ctypes.c_uint32]

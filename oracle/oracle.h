@@ -82,6 +82,11 @@ int or_render_preview(const or_scene* s, const fr_render_params* p, uint32_t w, 
 int or_trace(const or_scene* s, const float o[3], const float d[3], float tnear, float* t,
              uint32_t* geom, uint32_t* prim);
 
+/* Closest-hit glue of one primitive alone (tests): 1 if the ray hits it in (tnear, inf), with
+ * out[0] = t and out[1] = the outline distance d. */
+int or_prim_hit(const or_scene* s, uint32_t geom, uint32_t prim, const float o[3],
+                const float d[3], float tnear, float out[3]);
+
 /* Raw building blocks exposed for unit tests. */
 void or_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 float or_u01(uint32_t x);

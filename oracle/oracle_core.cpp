@@ -1015,6 +1015,42 @@ int or_render_preview(const or_scene* s, const fr_render_params* p, uint32_t w, 
     return 0;
 }
 
+int or_prim_hit(const or_scene* s, uint32_t geom, uint32_t prim, const float o[3],
+                const float d[3], float tnear, float out[3])
+{
+    if (!s || geom >= s->geoms.size())
+        return 0;
+    const Geom& g = s->geoms[geom];
+    if (prim >= g.prim_count())
+        return 0;
+    Hit h;
+    h.t = std::numeric_limits<float>::infinity();
+    h.geom = UINT32_MAX;
+    h.prim = 0;
+    h.d = 0;
+    F3 oo{o[0], o[1], o[2]}, dd{d[0], d[1], d[2]};
+    switch (g.type) {
+    case FR_GEOM_SPHERE:
+        glue_sphere(g, geom, prim, oo, dd, tnear, h);
+        break;
+    case FR_GEOM_CYLINDER:
+        glue_cylinder(g, geom, prim, oo, dd, tnear, h);
+        break;
+    case FR_GEOM_POLYHEDRON:
+        glue_polyhedron(g, geom, prim, oo, dd, tnear, h);
+        break;
+    default:
+        glue_mesh(g, geom, prim, oo, dd, tnear, h);
+        break;
+    }
+    if (h.geom == UINT32_MAX)
+        return 0;
+    out[0] = h.t;
+    out[1] = h.d;
+    out[2] = 0.0f;
+    return 1;
+}
+
 void or_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4])
 {
     frm::Ctr4 c{{ctr[0], ctr[1], ctr[2], ctr[3]}};

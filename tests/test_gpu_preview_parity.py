@@ -1,20 +1,24 @@
 """Preview tracer on the GPU versus the CPU oracle: closest-hit ids and linear RGB.
 
-Bars (from the reference CPU path as normative): hit ids bit-exact, tolerating at most 1e-4 of
-samples differing (grazing rays); linear RGB within 1e-3 wherever the hits agree; sRGB bytes
-equal on at least 99.9% of pixels (transcendental functions differ in the last place between
-CUDA and the host libm).
+Bars (from the reference CPU path as normative): hit ids bit-exact except at grazing samples --
+every disagreement is classified with the oracle (tests/grazing.py: an exact or rounding-level
+tie in t between the two primitives, or a ray within rounding of a silhouette) and none may be
+non-grazing; grazing disagreements are reported and must stay below 1e-3 of the samples (the
+stated rate is printed); linear RGB within 1e-3 wherever the hits agree; sRGB bytes equal on at
+least 99.9% of pixels (transcendental functions differ in the last place between CUDA and the
+host libm).
 """
 
 import numpy
 import pytest
 
 from fresnel_b200 import workloads
+from grazing import classify
 from parity import preview_hits
 
 pytestmark = pytest.mark.gpu
 
-HIT_MISMATCH_MAX = 1e-4
+GRAZING_MAX = 1e-3
 RGB_TOL = 1e-3
 
 
@@ -37,12 +41,17 @@ SCENES = {
 def test_preview_matches_oracle(name, aa_n, gpu_device, oracle_device):
     build, w, h = SCENES[name]
     gh, gl, g8 = preview_hits(gpu_device, build(gpu_device), w, h, aa_n)
-    oh, ol, o8 = preview_hits(oracle_device, build(oracle_device), w, h, aa_n)
+    oscene = build(oracle_device)
+    oh, ol, o8 = preview_hits(oracle_device, oscene, w, h, aa_n)
     assert gh.shape == oh.shape
     mism = numpy.any(gh != oh, axis=-1)
     assert numpy.count_nonzero(oh[..., 0]) > 0, "scene shows no geometry"
+    n_grazing, real = classify(oracle_device, oscene, w, h, aa_n, gh, oh)
     rate = mism.mean()
-    assert rate <= HIT_MISMATCH_MAX, f"{numpy.count_nonzero(mism)} hit ids differ ({rate:.2e})"
+    print(f"{name} aa={aa_n}: {numpy.count_nonzero(mism)} of {mism.size} hit ids differ "
+          f"({rate:.2e}), all grazing: {not real}")
+    assert not real, f"non-grazing hit disagreements: {real[:5]}"
+    assert rate <= GRAZING_MAX
     agree = ~numpy.any(mism, axis=-1)
     err = numpy.abs(gl - ol)[agree].max()
     assert err <= RGB_TOL, f"linear RGB differs by {err}"
