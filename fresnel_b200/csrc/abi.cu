@@ -91,6 +91,9 @@ struct fr_device {
     DevArray<uint32_t> status;  // traversal error bits
     cudaEvent_t timer[2] = {nullptr, nullptr};
     bool profiling = false;
+    size_t path_slots = size_t(32) << 20;  // path slots traced together
+    int persistent = 0;                    // persistent traversal kernels for 4-wide trees
+    std::vector<fr_scene*> scenes;         // to mark BVHs stale when a build option changes
 };
 
 struct fr_geometry {
@@ -307,6 +310,7 @@ fr_status prepare_scene(fr_scene* sc, fr_tracer* tr)
             if (stw & ERR_BUILD) {
                 cudaMemset(dev->status.ptr, 0, sizeof(uint32_t));
                 g->bvh.n_nodes = 0;
+                g->bvh.n_nodes4 = 0;
                 return fail(FR_ERR_DEVICE_LIMIT, "BVH construction produced an inconsistent tree");
             }
         }
@@ -327,7 +331,9 @@ fr_status prepare_scene(fr_scene* sc, fr_tracer* tr)
             d.enabled = (g->enabled && !g->removed) ? 1 : 0;
             d.n_prims = g->bvh_prims();
             d.n_nodes = g->bvh.n_nodes;
+            d.n_nodes4 = g->bvh.n_nodes4;
             d.nodes = g->bvh.nodes.ptr;
+            d.nodes4 = g->bvh.nodes4.ptr;
             d.leaf_data = g->bvh.leaf_data.ptr;
             d.order = g->bvh.order.ptr;
             d.position = g->position.ptr;
@@ -364,6 +370,18 @@ FrameParams frame_params(fr_tracer* tr, fr_scene* sc, const fr_render_params* p,
     P.scene.geoms = sc->table.ptr;
     P.scene.n_geoms = uint32_t(sc->geoms.size());
     P.scene.status = sc->dev->status.ptr;
+    P.type_mask = 0;
+    P.bvh_width = 2;
+    bool all4 = true;
+    for (fr_geometry* g : sc->geoms) {
+        if (!g->enabled || g->removed || g->bvh.n_nodes == 0)
+            continue;
+        P.type_mask |= 1u << g->type;
+        all4 = all4 && g->bvh.n_nodes4 > 0;
+    }
+    if (P.type_mask != 0 && all4)
+        P.bvh_width = 4;
+    P.persistent = sc->dev->persistent;
     const fr_user_camera& c = p->camera;
     float f_stop = preview ? std::numeric_limits<float>::infinity() : c.f_stop;  // no depth of field in preview
     bool sample_aa = preview ? (aa_n != 1) : true;
@@ -422,13 +440,12 @@ fr_status alloc_outputs(fr_tracer* tr, uint32_t w, uint32_t h)
     return FR_OK;
 }
 
-// Path slots traced together: a batch of K samples of every pixel (about 144 bytes each).
-constexpr size_t PATH_SLOT_BUDGET = size_t(32) << 20;
-
+// Samples traced together: a batch of K samples of every pixel fills about
+// dev->path_slots slots (about 144 bytes each).
 uint32_t batch_size(const fr_tracer* tr, uint32_t remaining)
 {
     size_t wh = size_t(tr->w) * tr->h;
-    size_t k = PATH_SLOT_BUDGET / (wh ? wh : 1);
+    size_t k = tr->dev->path_slots / (wh ? wh : 1);
     if (k < 1)
         k = 1;
     if (k > 4096)
@@ -634,6 +651,66 @@ fr_status fr_device_timer_stop(fr_device* d, float* ms)
     return FR_OK;
 }
 
+fr_status fr_device_set_option(fr_device* d, const char* name, double value)
+{
+    FR_CHECK_NULL(d);
+    FR_CHECK_NULL(name);
+    std::string n(name);
+    bool tree = false;
+    if (n == "bvh_width") {
+        if (value != 2.0 && value != 4.0)
+            return fail(FR_ERR_INVALID, "bvh_width must be 2 or 4");
+        tree = d->build.width != int(value);
+        d->build.width = int(value);
+    } else if (n == "leaf_max") {
+        if (!(value >= 1.0 && value <= 16.0))
+            return fail(FR_ERR_INVALID, "leaf_max must be in [1, 16]");
+        tree = d->build.leaf_max != int(value);
+        d->build.leaf_max = int(value);
+    } else if (n == "c_trav") {
+        if (!(value > 0.0 && value < 100.0))
+            return fail(FR_ERR_INVALID, "c_trav must be in (0, 100)");
+        tree = d->build.c_trav != float(value);
+        d->build.c_trav = float(value);
+    } else if (n == "persistent") {
+        if (value != 0.0 && value != 1.0)
+            return fail(FR_ERR_INVALID, "persistent must be 0 or 1");
+        d->persistent = int(value);
+    } else if (n == "path_slots") {
+        if (!(value >= 1.0 && value <= 1e9))
+            return fail(FR_ERR_INVALID, "path_slots must be in [1, 1e9]");
+        d->path_slots = size_t(value);
+    } else {
+        return fail(FR_ERR_INVALID, "unknown option " + n);
+    }
+    if (tree)
+        for (fr_scene* sc : d->scenes)
+            for (fr_geometry* g : sc->geoms)
+                g->bvh_dirty = true;
+    return FR_OK;
+}
+
+fr_status fr_device_get_option(const fr_device* d, const char* name, double* value)
+{
+    FR_CHECK_NULL(d);
+    FR_CHECK_NULL(name);
+    FR_CHECK_NULL(value);
+    std::string n(name);
+    if (n == "bvh_width")
+        *value = d->build.width;
+    else if (n == "leaf_max")
+        *value = d->build.leaf_max;
+    else if (n == "c_trav")
+        *value = d->build.c_trav;
+    else if (n == "path_slots")
+        *value = double(d->path_slots);
+    else if (n == "persistent")
+        *value = d->persistent;
+    else
+        return fail(FR_ERR_INVALID, "unknown option " + n);
+    return FR_OK;
+}
+
 fr_status fr_device_set_profiling(fr_device* d, int enable)
 {
     FR_CHECK_NULL(d);
@@ -650,6 +727,7 @@ fr_status fr_scene_create(fr_device* dev, fr_scene** out)
     if (!s)
         return fail(FR_ERR_OUT_OF_MEMORY, "out of host memory");
     s->dev = dev;
+    dev->scenes.push_back(s);
     *out = s;
     return FR_OK;
 }
@@ -658,6 +736,12 @@ fr_status fr_scene_destroy(fr_scene* s)
 {
     if (!s)
         return FR_OK;
+    auto& v = s->dev->scenes;
+    for (size_t i = 0; i < v.size(); ++i)
+        if (v[i] == s) {
+            v.erase(v.begin() + long(i));
+            break;
+        }
     cudaSetDevice(s->dev->ordinal);
     cudaStreamSynchronize(s->dev->stream);
     for (fr_geometry* g : s->geoms)
@@ -981,6 +1065,7 @@ fr_status fr_tracer_render_path(fr_tracer* t, fr_scene* sc, const fr_render_para
     P.light_samples = light_samples;
     PathState S = path_state(t);
     cudaStream_t st = t->dev->stream;
+    FR_CUDA(cudaMemsetAsync(t->ctr.ptr, 0, 4 * sizeof(uint32_t), st), "clearing queue lengths");
     const int CHECK_EVERY = 8;
     const int MAX_ITER = 1 << 20;
     const bool prof = t->dev->profiling;
@@ -998,7 +1083,8 @@ fr_status fr_tracer_render_path(fr_tracer* t, fr_scene* sc, const fr_render_para
     for (uint32_t done = 0; done < n_render;) {
         P.n_samples = first_sample + done;
         P.batch = batch < n_render - done ? batch : n_render - done;
-        timed(0, [&] { launch_path_primary(P, S, st); });
+        FR_CUDA(cudaMemsetAsync(t->ctr.ptr + 3, 0, sizeof(uint32_t), st), "clearing a counter");
+        timed(0, [&] { launch_path_primary(P, S, t->dev->shape, st); });
         t->launches++;
         int it = 0;
         while (true) {
@@ -1137,6 +1223,48 @@ fr_status fr_tracer_get_stats(const fr_tracer* t, fr_stats* out)
     out->primary_launches = t->kernel_launches[0];
     out->shade_launches = t->kernel_launches[1];
     out->extend_launches = t->kernel_launches[2];
+    return FR_OK;
+}
+
+fr_status fr_tracer_read_primary_hits(fr_tracer* t, uint32_t* host, size_t nbytes)
+{
+    FR_CHECK_NULL(t);
+    FR_CHECK_NULL(host);
+    size_t n = size_t(t->w) * t->h;
+    if (nbytes != n * sizeof(uint2))
+        return fail(FR_ERR_INVALID, "primary hit buffer size mismatch");
+    if (t->prim_hit.cap < n)
+        return fail(FR_ERR_STATE, "no path render yet");
+    fr_status s = use_device(t->dev);
+    if (s != FR_OK)
+        return s;
+    FR_CUDA(cudaMemcpyAsync(host, t->prim_hit.ptr, nbytes, cudaMemcpyDeviceToHost,
+                            t->dev->stream),
+            "downloading primary hits");
+    FR_CUDA(cudaStreamSynchronize(t->dev->stream), "downloading primary hits");
+    return FR_OK;
+}
+
+fr_status fr_debug_traversal_compare(fr_scene* sc, const float* rays, uint32_t n, uint32_t* out)
+{
+    FR_CHECK_NULL(sc);
+    FR_CHECK_NULL(rays);
+    FR_CHECK_NULL(out);
+    fr_status s = use_device(sc->dev);
+    if (s != FR_OK || (s = prepare_scene(sc, nullptr)) != FR_OK)
+        return s;
+    DevArray<float> d_rays;
+    DevArray<uint32_t> d_out;
+    FR_CUDA(d_rays.reserve(size_t(n) * 6), "alloc");
+    FR_CUDA(d_out.reserve(size_t(n) * 6), "alloc");
+    FR_CUDA(cudaMemcpy(d_rays.ptr, rays, size_t(n) * 6 * 4, cudaMemcpyHostToDevice), "copy");
+    SceneDev sd;
+    sd.geoms = sc->table.ptr;
+    sd.n_geoms = uint32_t(sc->geoms.size());
+    sd.status = sc->dev->status.ptr;
+    launch_traversal_compare(sd, d_rays.ptr, n, d_out.ptr, sc->dev->stream);
+    FR_CUDA(cudaStreamSynchronize(sc->dev->stream), "compare");
+    FR_CUDA(cudaMemcpy(out, d_out.ptr, size_t(n) * 6 * 4, cudaMemcpyDeviceToHost), "copy");
     return FR_OK;
 }
 

@@ -427,11 +427,177 @@ __global__ void k_gather(BuildInput in, uint32_t n, const uint32_t* sorted_vals,
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// 4-wide collapse: every 4-wide node takes the two children of a binary interior node and keeps
+// opening its largest-area interior child until it has four children (a leaf of the binary tree
+// stays a leaf).  Processed top-down, one level of 4-wide nodes per launch.
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ float node2_area(float4 lo, float4 hi)
+{
+    return half_area(make_float3(lo.x, lo.y, lo.z), make_float3(hi.x, hi.y, hi.z));
+}
+
+__global__ void k_collapse4(const float4* nodes2, uint32_t n_nodes2, const uint2* in_q,
+                            const uint32_t* in_count, uint2* out_q, uint32_t* out_count,
+                            uint32_t* node4_count, uint32_t node4_cap, float4* nodes4,
+                            uint32_t* status)
+{
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= *in_count)
+        return;
+    uint2 job = in_q[t];  // (binary node, 4-wide node)
+    if (job.x >= n_nodes2 || job.y >= node4_cap) {
+        atomicOr(status, ERR_BUILD);
+        return;
+    }
+    uint32_t child[4];
+    int nc = 0;
+    float4 root_hi = nodes2[2 * size_t(job.x) + 1];
+    if (__float_as_uint(root_hi.w) != 0) {  // the binary root is itself a leaf
+        child[nc++] = job.x;
+    } else {
+        uint32_t a = __float_as_uint(nodes2[2 * size_t(job.x)].w);
+        if (a + 1u >= n_nodes2) {
+            atomicOr(status, ERR_BUILD);
+            return;
+        }
+        child[nc++] = a;
+        child[nc++] = a + 1;
+        while (nc < 4) {
+            int best = -1;
+            float best_area = -1.0f;
+            for (int k = 0; k < nc; ++k) {
+                float4 lo = nodes2[2 * size_t(child[k])], hi = nodes2[2 * size_t(child[k]) + 1];
+                if (__float_as_uint(hi.w) == 0) {
+                    float ar = node2_area(lo, hi);
+                    if (ar > best_area) {
+                        best_area = ar;
+                        best = k;
+                    }
+                }
+            }
+            if (best < 0)
+                break;
+            uint32_t a2 = __float_as_uint(nodes2[2 * size_t(child[best])].w);
+            if (a2 + 1u >= n_nodes2) {
+                atomicOr(status, ERR_BUILD);
+                return;
+            }
+            child[best] = a2;
+            child[nc++] = a2 + 1;
+        }
+    }
+    float lo[3][4], hi[3][4];
+    uint32_t idx[4], cnt[4];
+    for (int k = 0; k < 4; ++k) {
+        if (k >= nc || child[k] >= n_nodes2) {
+            for (int ax = 0; ax < 3; ++ax) {
+                lo[ax][k] = 0.0f;
+                hi[ax][k] = 0.0f;
+            }
+            idx[k] = 0;
+            cnt[k] = EMPTY_CHILD;
+            if (k < nc)
+                atomicOr(status, ERR_BUILD);
+            continue;
+        }
+        float4 l = nodes2[2 * size_t(child[k])], h = nodes2[2 * size_t(child[k]) + 1];
+        lo[0][k] = l.x;
+        lo[1][k] = l.y;
+        lo[2][k] = l.z;
+        hi[0][k] = h.x;
+        hi[1][k] = h.y;
+        hi[2][k] = h.z;
+        uint32_t b = __float_as_uint(h.w);
+        if (b != 0) {  // leaf
+            idx[k] = __float_as_uint(l.w);
+            cnt[k] = b;
+        } else {
+            uint32_t q = atomicAdd(node4_count, 1u);
+            if (q >= node4_cap) {
+                atomicOr(status, ERR_BUILD);
+                idx[k] = 0;
+                cnt[k] = EMPTY_CHILD;
+                continue;
+            }
+            idx[k] = q;
+            cnt[k] = 0;
+            uint32_t slot = atomicAdd(out_count, 1u);
+            out_q[slot] = make_uint2(child[k], q);
+        }
+    }
+    float4* o = nodes4 + 8 * size_t(job.y);
+    o[0] = make_float4(lo[0][0], lo[0][1], lo[0][2], lo[0][3]);
+    o[1] = make_float4(hi[0][0], hi[0][1], hi[0][2], hi[0][3]);
+    o[2] = make_float4(lo[1][0], lo[1][1], lo[1][2], lo[1][3]);
+    o[3] = make_float4(hi[1][0], hi[1][1], hi[1][2], hi[1][3]);
+    o[4] = make_float4(lo[2][0], lo[2][1], lo[2][2], lo[2][3]);
+    o[5] = make_float4(hi[2][0], hi[2][1], hi[2][2], hi[2][3]);
+    o[6] = make_float4(__uint_as_float(idx[0]), __uint_as_float(idx[1]), __uint_as_float(idx[2]),
+                       __uint_as_float(idx[3]));
+    o[7] = make_float4(__uint_as_float(cnt[0]), __uint_as_float(cnt[1]), __uint_as_float(cnt[2]),
+                       __uint_as_float(cnt[3]));
+}
+
 inline uint32_t blocks_for(size_t n, int threads) { return uint32_t((n + threads - 1) / threads); }
 
 }  // namespace
 
 size_t leaf_record_float4s(int type) { return type == FR_GEOM_SPHERE ? 1 : 2; }
+
+// Collapse the binary tree in out.nodes into out.nodes4 (top-down, one launch per level).
+cudaError_t collapse4(BvhBuffers& out, Scratch& scratch, uint32_t* status, cudaStream_t st)
+{
+    out.n_nodes4 = 0;
+    if (out.n_nodes == 0)
+        return cudaSuccess;
+    const uint32_t cap = (out.n_nodes + 1) / 2 + 1;  // at most one per binary interior node
+    cudaError_t e;
+    if ((e = out.nodes4.reserve(size_t(8) * cap)) != cudaSuccess)
+        return e;
+    ScratchLayout L;
+    uint2* qa = L.take<uint2>(cap);
+    uint2* qb = L.take<uint2>(cap);
+    uint32_t* cnt = L.take<uint32_t>(4);
+    if ((e = scratch.reserve(L.bytes)) != cudaSuccess)
+        return e;
+    L.bind(scratch.ptr);
+    qa = L.at(qa);
+    qb = L.at(qb);
+    cnt = L.at(cnt);
+    // cnt[0]: jobs in qa, cnt[1]: jobs in qb, cnt[2]: 4-wide nodes allocated
+    uint32_t init[3] = {1u, 0u, 1u};
+    uint2 root = make_uint2(0u, 0u);
+    if ((e = cudaMemcpyAsync(cnt, init, sizeof(init), cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        return e;
+    if ((e = cudaMemcpyAsync(qa, &root, sizeof(root), cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        return e;
+    uint32_t jobs = 1;
+    for (int level = 0; jobs > 0 && level < 256; ++level) {
+        uint32_t* cin = cnt + (level & 1);
+        uint32_t* cout = cnt + ((level + 1) & 1);
+        uint2* qin = (level & 1) ? qb : qa;
+        uint2* qout = (level & 1) ? qa : qb;
+        if ((e = cudaMemsetAsync(cout, 0, sizeof(uint32_t), st)) != cudaSuccess)
+            return e;
+        k_collapse4<<<blocks_for(jobs, 256), 256, 0, st>>>(out.nodes.ptr, out.n_nodes, qin, cin,
+                                                           qout, cout, cnt + 2, cap,
+                                                           out.nodes4.ptr, status);
+        if ((e = cudaMemcpyAsync(&jobs, cout, sizeof(uint32_t), cudaMemcpyDeviceToHost, st)) !=
+            cudaSuccess)
+            return e;
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess)
+            return e;
+    }
+    uint32_t n4 = 0;
+    if ((e = cudaMemcpyAsync(&n4, cnt + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, st)) !=
+        cudaSuccess)
+        return e;
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return e;
+    out.n_nodes4 = n4 < cap ? n4 : cap;
+    return cudaGetLastError();
+}
 
 cudaError_t build_bvh(const BuildInput& in, uint32_t n, const BuildParams& bp, BvhBuffers& out,
                       Scratch& scratch, uint32_t* status, cudaStream_t st)
@@ -553,7 +719,13 @@ cudaError_t build_bvh(const BuildInput& in, uint32_t n, const BuildParams& bp, B
         out.n_nodes = 1u + 2u * (tail[0] + tail[1]);
     }
     k_gather<<<blocks_for(n, T), T, 0, st>>>(in, n, vals_sorted, out.leaf_data.ptr, out.order.ptr);
-    return cudaGetLastError();
+    if ((e = cudaGetLastError()) != cudaSuccess)
+        return e;
+    if (bp.width != 4) {
+        out.n_nodes4 = 0;
+        return cudaSuccess;
+    }
+    return collapse4(out, scratch, status, st);
 }
 
 }  // namespace fr

@@ -85,19 +85,25 @@ struct BuildInput {
 };
 
 struct BuildParams {
-    int leaf_max = 4;      // largest leaf the SAH collapse may form
+    int width = 4;         // 2: binary tree only; 4: also collapse to the 4-wide tree
+    int leaf_max = 2;      // largest leaf the SAH collapse may form
     float c_trav = 1.0f;   // cost of one child-pair visit, in units of one primitive test
     float c_isect = 1.0f;
 };
 
 struct BvhBuffers {
-    DevArray<float4> nodes;      // 2 float4 per node
+    DevArray<float4> nodes;      // binary tree, 2 float4 per node
+    DevArray<float4> nodes4;     // 4-wide tree traversed by the renderers, 8 float4 per node
+    uint32_t n_nodes4 = 0;
     DevArray<float4> leaf_data;  // leaf_record_float4s(type) per primitive
     DevArray<uint32_t> order;    // leaf slot -> primitive index
     uint32_t n_nodes = 0;
 };
 
 size_t leaf_record_float4s(int type);
+
+// Collapse the binary tree of `out` into its 4-wide tree (called by build_bvh).
+cudaError_t collapse4(BvhBuffers& out, Scratch& scratch, uint32_t* status, cudaStream_t st);
 
 // Build the BVH of n primitives (n == 0 leaves an empty tree).  Synchronises the stream once
 // to read back the node count.

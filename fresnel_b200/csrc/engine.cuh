@@ -1,10 +1,14 @@
 // engine.cuh -- device-side scene layout and closest-hit traversal.
 //
 // Layout in HBM, per geometry:
-//   nodes      BVH2 nodes of 32 bytes, two float4 each: (lo.xyz, a) and (hi.xyz, b).
-//              Interior nodes have b == 0 and their two children at a and a+1, so one 64-byte
-//              load fetches both child boxes; leaves have b == primitive count and a == first
-//              slot.  Node 0 is the root.
+//   nodes4     4-wide BVH nodes of 128 bytes (one cache line), eight float4: lo.x, hi.x, lo.y,
+//              hi.y, lo.z, hi.z of the four children (one child per float4 lane), then the
+//              child references and counts (count 0: interior child, its node index; count
+//              n > 0: leaf of n primitives starting at that slot; EMPTY_CHILD: unused slot).
+//              Node 0 is the root.  The renderers traverse this tree.
+//   nodes      the binary LBVH it is collapsed from, 32-byte nodes of two float4:
+//              (lo.xyz, a) and (hi.xyz, b); interior b == 0 with children at a and a+1, leaves
+//              b == primitive count and a == first slot.
 //   leaf_data  primitives in BVH leaf order, packed for the intersection loop
 //              (sphere: 1 float4 (x,y,z,r); cylinder: (A,r),(B,-); polyhedron: (p,-),(quat);
 //              mesh: (p, face bits),(quat)).
@@ -25,6 +29,7 @@ namespace fr {
 
 constexpr int TRAVERSAL_STACK = 64;
 constexpr uint32_t MISS = 0xFFFFFFFFu;
+constexpr uint32_t EMPTY_CHILD = 0xFFFFFFFFu;  // count of an unused 4-wide child slot
 
 // error bits reported through the device status word
 constexpr uint32_t ERR_STACK_OVERFLOW = 1u;
@@ -37,7 +42,9 @@ struct GeomDev {
     int32_t enabled;
     uint32_t n_prims;  // BVH primitives (mesh: instances * faces)
     uint32_t n_nodes;
+    uint32_t n_nodes4;
     const float4* nodes;
+    const float4* nodes4;
     const float4* leaf_data;
     const uint32_t* order;
     const float* position;
@@ -364,12 +371,137 @@ __device__ __forceinline__ void traverse(const GeomDev& g, uint32_t gi, const Ra
     }
 }
 
+__device__ __forceinline__ uint32_t pick4(uint32_t a, uint32_t b, uint32_t c, uint32_t d, uint32_t k)
+{
+    return k == 0 ? a : (k == 1 ? b : (k == 2 ? c : d));
+}
+
+__device__ __forceinline__ void cswap(uint32_t& a, uint32_t& b)
+{
+    uint32_t lo = min(a, b), hi = max(a, b);
+    a = lo;
+    b = hi;
+}
+
+// Closest hit in one geometry's 4-wide BVH: per step one 128-byte node and four slab tests;
+// hit leaves are tested at once; hit interior children are ordered by entry distance with a
+// five-comparator sorting network on keys (distance bits | child slot), the nearest is visited
+// next and the others are pushed far to near on a 64-entry per-thread stack.  Everything stays
+// in registers (no dynamically indexed arrays besides the stack).
+template <int TYPE>
+__device__ __forceinline__ void traverse4(const GeomDev& g, uint32_t gi, const RayK& ray,
+                                          float tnear, float& tmax, uint32_t& hit_geom,
+                                          uint32_t& hit_slot, uint32_t* status, TraceCount& tc)
+{
+    if (g.n_nodes4 == 0)
+        return;
+    uint32_t stack_node[TRAVERSAL_STACK];
+    float stack_t[TRAVERSAL_STACK];
+    int sp = 0;
+    uint32_t cur = 0;
+    uint32_t guard = g.n_nodes4 + 8u;
+    while (true) {
+        if (--guard == 0u) {
+            atomicOr(status, ERR_ITERATION_CAP);
+            return;
+        }
+        const float4* np = g.nodes4 + 8 * size_t(cur);
+        const float4 lx = ldg4(np), hx = ldg4(np + 1), ly = ldg4(np + 2), hy = ldg4(np + 3),
+                     lz = ldg4(np + 4), hz = ldg4(np + 5);
+        const uint4 ci = __ldg(reinterpret_cast<const uint4*>(np + 6));
+        const uint4 cc = __ldg(reinterpret_cast<const uint4*>(np + 7));
+        tc.box += 4;
+        float te0, te1, te2, te3;
+        bool h0, h1, h2, h3;
+        auto test = [&](float lxk, float hxk, float lyk, float hyk, float lzk, float hzk,
+                        uint32_t cck, float& te) {
+            float tx0 = fmaf(lxk, ray.inv.x, ray.oinv.x), tx1 = fmaf(hxk, ray.inv.x, ray.oinv.x);
+            float ty0 = fmaf(lyk, ray.inv.y, ray.oinv.y), ty1 = fmaf(hyk, ray.inv.y, ray.oinv.y);
+            float tz0 = fmaf(lzk, ray.inv.z, ray.oinv.z), tz1 = fmaf(hzk, ray.inv.z, ray.oinv.z);
+            float t0 = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), 0.0f));
+            float t1 = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tmax));
+            te = t0;
+            return t0 <= t1 && cck != EMPTY_CHILD;
+        };
+        h0 = test(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, cc.x, te0);
+        h1 = test(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, cc.y, te1);
+        h2 = test(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, cc.z, te2);
+        h3 = test(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, cc.w, te3);
+        // leaves: one shared copy of the primitive loop, iterated over a bit mask
+        uint32_t leaves = (h0 && cc.x != 0u ? 1u : 0u) | (h1 && cc.y != 0u ? 2u : 0u) |
+                          (h2 && cc.z != 0u ? 4u : 0u) | (h3 && cc.w != 0u ? 8u : 0u);
+        while (leaves) {
+            uint32_t k = uint32_t(__ffs(leaves) - 1);
+            leaves &= leaves - 1u;
+            uint32_t first = pick4(ci.x, ci.y, ci.z, ci.w, k);
+            uint32_t count = pick4(cc.x, cc.y, cc.z, cc.w, k);
+            if (first > g.n_prims || count > g.n_prims - first) {
+                atomicOr(status, ERR_BAD_NODE);
+                return;
+            }
+            leaf_test<TYPE>(g, gi, ray, first, count, tnear, tmax, hit_geom, hit_slot, tc);
+        }
+        // interior children: key = entry distance bits (non-negative float) | child slot
+        auto key = [&](bool h, uint32_t cck, float te, uint32_t k) {
+            return (h && cck == 0u && te <= tmax) ? ((__float_as_uint(te) & ~3u) | k) : 0xFFFFFFFFu;
+        };
+        uint32_t k0 = key(h0, cc.x, te0, 0), k1 = key(h1, cc.y, te1, 1);
+        uint32_t k2 = key(h2, cc.z, te2, 2), k3 = key(h3, cc.w, te3, 3);
+        cswap(k0, k1);
+        cswap(k2, k3);
+        cswap(k0, k2);
+        cswap(k1, k3);
+        cswap(k1, k2);
+        if (k0 != 0xFFFFFFFFu) {
+            // push the farther ones (far to near), descend into the nearest
+            uint32_t ks[3] = {k3, k2, k1};
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                if (ks[a] != 0xFFFFFFFFu) {
+                    uint32_t node = pick4(ci.x, ci.y, ci.z, ci.w, ks[a] & 3u);
+                    if (sp < TRAVERSAL_STACK) {
+                        stack_node[sp] = node;
+                        stack_t[sp] = __uint_as_float(ks[a] & ~3u);
+                        ++sp;
+                    } else {
+                        atomicOr(status, ERR_STACK_OVERFLOW);
+                    }
+                }
+            }
+            cur = pick4(ci.x, ci.y, ci.z, ci.w, k0 & 3u);
+            if (cur >= g.n_nodes4) {
+                atomicOr(status, ERR_BAD_NODE);
+                return;
+            }
+            continue;
+        }
+        bool found = false;
+        while (sp > 0) {
+            --sp;
+            if (stack_t[sp] <= tmax) {
+                cur = stack_node[sp];
+                found = cur < g.n_nodes4;
+                break;
+            }
+        }
+        if (!found)
+            return;
+    }
+}
+
 struct Hit {
     uint32_t geom;  // MISS if none
     uint32_t prim;  // index into the geometry's user arrays
 };
 
-// Closest hit over all enabled geometries of the scene.
+// Geometry-type masks a kernel is specialised for (bit FR_GEOM_* set = type handled).
+constexpr uint32_t MASK_SPHERES = 1u << FR_GEOM_SPHERE;
+constexpr uint32_t MASK_ALL = 0xFu;
+
+// Closest hit over all enabled geometries of the scene.  WIDTH selects the binary (2) or
+// 4-wide (4) tree; MASK the geometry types compiled in (the host only launches a MASK that
+// covers every enabled geometry of the scene).
+template <int WIDTH, uint32_t MASK>
 __device__ __forceinline__ Hit trace_closest(const SceneDev& sc, V3 o, V3 d, float tnear,
                                              TraceCount& tc)
 {
@@ -380,25 +512,183 @@ __device__ __forceinline__ Hit trace_closest(const SceneDev& sc, V3 o, V3 d, flo
         const GeomDev& g = sc.geoms[gi];
         if (!g.enabled)
             continue;
-        switch (g.type) {
-        case FR_GEOM_SPHERE:
-            traverse<FR_GEOM_SPHERE>(g, gi, ray, tnear, tmax, hg, hs, sc.status, tc);
-            break;
-        case FR_GEOM_CYLINDER:
-            traverse<FR_GEOM_CYLINDER>(g, gi, ray, tnear, tmax, hg, hs, sc.status, tc);
-            break;
-        case FR_GEOM_POLYHEDRON:
-            traverse<FR_GEOM_POLYHEDRON>(g, gi, ray, tnear, tmax, hg, hs, sc.status, tc);
-            break;
-        default:
-            traverse<FR_GEOM_MESH>(g, gi, ray, tnear, tmax, hg, hs, sc.status, tc);
-            break;
-        }
+#define FR_TRAVERSE(T)                                                            \
+    if ((MASK & (1u << T)) && g.type == T) {                                      \
+        if (WIDTH == 4)                                                           \
+            traverse4<T>(g, gi, ray, tnear, tmax, hg, hs, sc.status, tc);        \
+        else                                                                      \
+            traverse<T>(g, gi, ray, tnear, tmax, hg, hs, sc.status, tc);         \
+        continue;                                                                 \
+    }
+        FR_TRAVERSE(FR_GEOM_SPHERE)
+        FR_TRAVERSE(FR_GEOM_CYLINDER)
+        FR_TRAVERSE(FR_GEOM_POLYHEDRON)
+        FR_TRAVERSE(FR_GEOM_MESH)
+#undef FR_TRAVERSE
     }
     Hit h;
     h.geom = hg;
     h.prim = (hg == MISS) ? 0u : __ldg(sc.geoms[hg].order + hs);
     return h;
+}
+
+// --------------------------------------------------------------------------------------------
+// Step-wise 4-wide traversal for persistent warps (Aila & Laine, "Understanding the efficiency
+// of ray traversal on GPUs", HPG 2009): each call visits one node of the current geometry's
+// tree; a lane whose ray is finished fetches a new one, so lanes stay busy although rays need
+// very different numbers of steps.
+// --------------------------------------------------------------------------------------------
+constexpr uint32_t NEED_GEOM = 0xFFFFFFFFu;  // cur: start the next geometry's tree
+
+struct LaneRay {
+    RayK ray;
+    float tnear, tmax;
+    uint32_t hit_geom, hit_slot;
+    uint32_t gi;   // geometry being traversed
+    uint32_t cur;  // node to visit, or NEED_GEOM
+    int sp;
+    uint32_t guard;
+};
+
+__device__ __forceinline__ void lane_begin(LaneRay& L, V3 o, V3 d, float tnear)
+{
+    L.ray = make_rayk(o, d);
+    L.tnear = tnear;
+    L.tmax = __int_as_float(0x7f800000);
+    L.hit_geom = MISS;
+    L.hit_slot = 0;
+    L.gi = 0;
+    L.cur = NEED_GEOM;
+    L.sp = 0;
+    L.guard = 0;
+}
+
+template <uint32_t MASK>
+__device__ __forceinline__ void leaf_dispatch(const GeomDev& g, LaneRay& L, uint32_t first,
+                                              uint32_t count, TraceCount& tc)
+{
+    if ((MASK & MASK_SPHERES) && (MASK == MASK_SPHERES || g.type == FR_GEOM_SPHERE))
+        leaf_test<FR_GEOM_SPHERE>(g, L.gi, L.ray, first, count, L.tnear, L.tmax, L.hit_geom,
+                                  L.hit_slot, tc);
+    else if ((MASK & (1u << FR_GEOM_CYLINDER)) && g.type == FR_GEOM_CYLINDER)
+        leaf_test<FR_GEOM_CYLINDER>(g, L.gi, L.ray, first, count, L.tnear, L.tmax, L.hit_geom,
+                                    L.hit_slot, tc);
+    else if ((MASK & (1u << FR_GEOM_POLYHEDRON)) && g.type == FR_GEOM_POLYHEDRON)
+        leaf_test<FR_GEOM_POLYHEDRON>(g, L.gi, L.ray, first, count, L.tnear, L.tmax, L.hit_geom,
+                                      L.hit_slot, tc);
+    else if ((MASK & (1u << FR_GEOM_MESH)) && g.type == FR_GEOM_MESH)
+        leaf_test<FR_GEOM_MESH>(g, L.gi, L.ray, first, count, L.tnear, L.tmax, L.hit_geom,
+                                L.hit_slot, tc);
+}
+
+// One step of the lane's traversal; returns false once the ray is finished (every enabled
+// geometry's tree traversed).  Indices are checked before use; a bad one ends the ray and sets
+// an error bit.
+template <uint32_t MASK>
+__device__ __forceinline__ bool step4(const SceneDev& sc, LaneRay& L, uint32_t* stack_node,
+                                      float* stack_t, TraceCount& tc)
+{
+    if (L.cur == NEED_GEOM) {
+        while (L.gi < sc.n_geoms) {
+            const GeomDev& gg = sc.geoms[L.gi];
+            if (gg.enabled && gg.n_nodes4 && (MASK & (1u << gg.type)))
+                break;
+            ++L.gi;
+        }
+        if (L.gi >= sc.n_geoms)
+            return false;
+        L.cur = 0;
+        L.sp = 0;
+        L.guard = sc.geoms[L.gi].n_nodes4 + 8u;
+    }
+    const GeomDev& g = sc.geoms[L.gi];
+    if (L.guard-- == 0u || L.cur >= g.n_nodes4) {
+        atomicOr(sc.status, L.cur >= g.n_nodes4 ? ERR_BAD_NODE : ERR_ITERATION_CAP);
+        return false;
+    }
+    const float4* np = g.nodes4 + 8 * size_t(L.cur);
+    const float4 lx = ldg4(np), hx = ldg4(np + 1), ly = ldg4(np + 2), hy = ldg4(np + 3),
+                 lz = ldg4(np + 4), hz = ldg4(np + 5);
+    const uint4 ci = __ldg(reinterpret_cast<const uint4*>(np + 6));
+    const uint4 cc = __ldg(reinterpret_cast<const uint4*>(np + 7));
+    tc.box += 4;
+    const RayK& ray = L.ray;
+    const float tmax0 = L.tmax;
+    auto test = [&](float lxk, float hxk, float lyk, float hyk, float lzk, float hzk,
+                    uint32_t cck, float& te) {
+        float tx0 = fmaf(lxk, ray.inv.x, ray.oinv.x), tx1 = fmaf(hxk, ray.inv.x, ray.oinv.x);
+        float ty0 = fmaf(lyk, ray.inv.y, ray.oinv.y), ty1 = fmaf(hyk, ray.inv.y, ray.oinv.y);
+        float tz0 = fmaf(lzk, ray.inv.z, ray.oinv.z), tz1 = fmaf(hzk, ray.inv.z, ray.oinv.z);
+        float t0 = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), 0.0f));
+        float t1 = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tmax0));
+        te = t0;
+        return t0 <= t1 && cck != EMPTY_CHILD;
+    };
+    float te0, te1, te2, te3;
+    bool h0 = test(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, cc.x, te0);
+    bool h1 = test(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, cc.y, te1);
+    bool h2 = test(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, cc.z, te2);
+    bool h3 = test(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, cc.w, te3);
+    uint32_t leaves = (h0 && cc.x != 0u ? 1u : 0u) | (h1 && cc.y != 0u ? 2u : 0u) |
+                      (h2 && cc.z != 0u ? 4u : 0u) | (h3 && cc.w != 0u ? 8u : 0u);
+    while (leaves) {
+        uint32_t k = uint32_t(__ffs(leaves) - 1);
+        leaves &= leaves - 1u;
+        uint32_t first = pick4(ci.x, ci.y, ci.z, ci.w, k);
+        uint32_t count = pick4(cc.x, cc.y, cc.z, cc.w, k);
+        if (first > g.n_prims || count > g.n_prims - first) {
+            atomicOr(sc.status, ERR_BAD_NODE);
+            return false;
+        }
+        leaf_dispatch<MASK>(g, L, first, count, tc);
+    }
+    const float tmax = L.tmax;
+    auto key = [&](bool h, uint32_t cck, float te, uint32_t k) {
+        return (h && cck == 0u && te <= tmax) ? ((__float_as_uint(te) & ~3u) | k) : 0xFFFFFFFFu;
+    };
+    uint32_t k0 = key(h0, cc.x, te0, 0), k1 = key(h1, cc.y, te1, 1);
+    uint32_t k2 = key(h2, cc.z, te2, 2), k3 = key(h3, cc.w, te3, 3);
+    cswap(k0, k1);
+    cswap(k2, k3);
+    cswap(k0, k2);
+    cswap(k1, k3);
+    cswap(k1, k2);
+    if (k0 != 0xFFFFFFFFu) {
+        uint32_t ks[3] = {k3, k2, k1};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            if (ks[a] != 0xFFFFFFFFu) {
+                if (L.sp < TRAVERSAL_STACK) {
+                    stack_node[L.sp] = pick4(ci.x, ci.y, ci.z, ci.w, ks[a] & 3u);
+                    stack_t[L.sp] = __uint_as_float(ks[a] & ~3u);
+                    ++L.sp;
+                } else {
+                    atomicOr(sc.status, ERR_STACK_OVERFLOW);
+                }
+            }
+        }
+        L.cur = pick4(ci.x, ci.y, ci.z, ci.w, k0 & 3u);
+        return true;
+    }
+    while (L.sp > 0) {
+        --L.sp;
+        if (stack_t[L.sp] <= tmax) {
+            L.cur = stack_node[L.sp];
+            return true;
+        }
+    }
+    // this geometry's tree is done: continue with the next geometry
+    ++L.gi;
+    L.cur = NEED_GEOM;
+    return true;
+}
+
+// Lane index within the warp (independent of the block's shape).
+__device__ __forceinline__ uint32_t lane_id()
+{
+    uint32_t l;
+    asm volatile("mov.u32 %0, %%laneid;" : "=r"(l));
+    return l;
 }
 
 // Add the warp's traversal counts to counters[0] (box tests) and counters[1] (primitive tests).
@@ -409,7 +699,7 @@ __device__ __forceinline__ void flush_counts(const TraceCount& tc, unsigned long
         b += __shfl_xor_sync(0xffffffffu, b, off);
         p += __shfl_xor_sync(0xffffffffu, p, off);
     }
-    if ((threadIdx.x & 31u) == 0u && (b | p)) {
+    if (lane_id() == 0u && (b | p)) {
         atomicAdd(counters, b);
         atomicAdd(counters + 1, p);
     }

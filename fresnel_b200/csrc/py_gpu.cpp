@@ -21,6 +21,9 @@
 #include "fresnel_b200.h"
 #include "host_types.hpp"
 
+extern "C" fr_status fr_debug_traversal_compare(fr_scene* sc, const float* rays, uint32_t n,
+                                                uint32_t* out);
+
 namespace py = pybind11;
 using namespace frh;
 
@@ -577,6 +580,14 @@ PYBIND11_MODULE(_gpu, m)
             return ms;
         })
         .def("setProfiling", [](DeviceH& d, bool on) { check(fr_device_set_profiling(d.dev, on)); })
+        .def("setOption", [](DeviceH& d, const std::string& name, double v) {
+            check(fr_device_set_option(d.dev, name.c_str(), v));
+        })
+        .def("getOption", [](DeviceH& d, const std::string& name) {
+            double v = 0.0;
+            check(fr_device_get_option(d.dev, name.c_str(), &v));
+            return v;
+        })
         .def_static("getAllGPUs", &DeviceH::all_gpus);
 
     py::class_<SceneH, std::shared_ptr<SceneH>>(m, "Scene")
@@ -591,6 +602,13 @@ PYBIND11_MODULE(_gpu, m)
         .def("getLights", [](SceneH& s) -> Lights& { return s.lights; },
              py::return_value_policy::reference_internal)
         .def("setLights", [](SceneH& s, const Lights& l) { s.lights = l; })
+        .def("debugTraversalCompare", [](SceneH& s, py::array_t<float, py::array::c_style | py::array::forcecast> rays) {
+            s.sync();
+            uint32_t n = uint32_t(rays.shape(0));
+            py::array_t<uint32_t> out({py::ssize_t(n), py::ssize_t(6)});
+            check(fr_debug_traversal_compare(s.scene, rays.data(), n, out.mutable_data()));
+            return out;
+        })
         .def("build", [](SceneH& s) {
             s.sync();
             check(fr_scene_build(s.scene));
@@ -662,7 +680,12 @@ PYBIND11_MODULE(_gpu, m)
         .def("getNumSamples", [](TracerPathH& t) { return t.n_samples; })
         .def("reset", &TracerPathH::reset)
         .def("setLightSamples", [](TracerPathH& t, unsigned n) { t.light_samples = n; })
-        .def("renderSamples", &TracerPathH::render_samples);
+        .def("renderSamples", &TracerPathH::render_samples)
+        .def("primaryHits", [](TracerPathH& t) {
+            py::array_t<uint32_t> out({py::ssize_t(t.h), py::ssize_t(t.w), py::ssize_t(2)});
+            check(fr_tracer_read_primary_hits(t.tracer, out.mutable_data(), size_t(t.w) * t.h * 8));
+            return out;
+        });
 
     export_array<ArrayRGBAf>(m, "ArrayRGBAf");
     export_array<ArrayRGBAc>(m, "ArrayRGBAc");

@@ -53,38 +53,219 @@ __device__ __forceinline__ float4 welford(const FrameParams& P, float4 old, floa
     return make_float4(nr, ng, nb, na);
 }
 
+// Primary rays of every slot.  A primary miss finishes its pixel sample here (every light
+// sample sees the background: radiance bg * L, fresnel/common/TracerPathMethods.h:44-50); a hit
+// is queued in queue 1 for the first shade pass.
+template <int WIDTH, uint32_t MASK>
 __global__ void __launch_bounds__(256) k_path_primary(FrameParams P, PathState S)
 {
-    if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0 &&
-        threadIdx.y == 0) {
-        S.ctr[0] = 0;
-        S.ctr[1] = 0;
-        S.ctr[2] = 0;
-    }
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t j = blockIdx.y * blockDim.y + threadIdx.y;
     uint32_t k = blockIdx.z;
     bool valid = (i < P.w) && (j < P.h);
+    bool push = false;
+    uint32_t slot = 0;
     TraceCount tc;
     if (valid) {
         uint32_t p = j * P.w + i;
-        size_t slot = size_t(k) * P.w * P.h + p;
+        slot = k * P.w * P.h + p;
         V3 o, d;
         camera_ray(P.cam, i, j, P.n_samples + k, o, d);
-        Hit h = trace_closest(P.scene, o, d, PATH_TNEAR, tc);
-        S.prim_o[slot] = f4(o);
-        S.prim_d[slot] = f4(d);
+        Hit h = trace_closest<WIDTH, MASK>(P.scene, o, d, PATH_TNEAR, tc);
         S.prim_hit[slot] = make_uint2(h.geom, h.prim);
-        S.ls_depth[slot] = make_uint2(0u, 0u);
-        S.att[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-        S.result[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (h.geom == MISS) {
+            C3 res = P.bg * float(P.light_samples);
+            C3 out = c_div_recip(res, float(P.light_samples));
+            S.sample[slot] = make_float4(out.r, out.g, out.b, P.bg_alpha);
+        } else {
+            S.prim_o[slot] = f4(o);
+            S.prim_d[slot] = f4(d);
+            S.ls_depth[slot] = make_uint2(0u, 0u);
+            S.att[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+            S.result[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            push = true;
+        }
     }
     flush_counts(tc, P.stats + 3);
-    uint32_t m = __ballot_sync(0xffffffffu, valid);
-    if ((threadIdx.x + threadIdx.y * blockDim.x) % 32 == 0 && m) {
-        atomicAdd(P.stats + 0, (unsigned long long)__popc(m));
-        atomicAdd(P.stats + 1, (unsigned long long)__popc(m) * P.light_samples);
+    const uint32_t lane = (threadIdx.x + threadIdx.y * blockDim.x) & 31u;
+    uint32_t m = __ballot_sync(0xffffffffu, push);
+    if (m) {
+        uint32_t at = 0;
+        if (lane == 0)
+            at = atomicAdd(S.ctr + 1, uint32_t(__popc(m)));
+        at = __shfl_sync(0xffffffffu, at, 0);
+        if (push)
+            S.queue[1][at + __popc(m & ((1u << lane) - 1u))] = slot;
     }
+    uint32_t mv = __ballot_sync(0xffffffffu, valid);
+    if (lane == 0 && mv) {
+        atomicAdd(P.stats + 0, (unsigned long long)__popc(mv));
+        atomicAdd(P.stats + 1, (unsigned long long)__popc(mv) * P.light_samples);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Persistent traversal with per-lane refill (4-wide trees): a warp steps one node visit at a
+// time; whenever at least REFILL lanes are idle, they claim new work items with one atomic, so
+// lanes stay busy although rays need very different numbers of steps.
+// ---------------------------------------------------------------------------------------------
+constexpr uint32_t REFILL = 8;
+
+template <uint32_t MASK, class Src>
+__device__ __forceinline__ void persistent_trace(const FrameParams& P, Src& src, uint32_t count,
+                                                 uint32_t* work, TraceCount& tc, uint32_t& n_rays)
+{
+    uint32_t stack_node[TRAVERSAL_STACK];
+    float stack_t[TRAVERSAL_STACK];
+    LaneRay L;
+    L.gi = 0;
+    L.cur = NEED_GEOM;
+    bool active = false;
+    uint32_t item = 0;
+    bool exhausted = false;  // warp-uniform
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lt = (1u << lane) - 1u;
+    while (true) {
+        uint32_t idle = __ballot_sync(0xffffffffu, !active);
+        if (!exhausted && (__popc(idle) >= REFILL || idle == 0xffffffffu)) {
+            uint32_t n = uint32_t(__popc(idle));
+            uint32_t base = 0;
+            if (lane == 0)
+                base = atomicAdd(work, n);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (base >= count || count - base <= n)
+                exhausted = true;
+            if (!active) {
+                item = base + uint32_t(__popc(idle & lt));
+                if (item < count && src.begin(item, L)) {
+                    active = true;
+                    ++n_rays;
+                }
+            }
+        }
+        if (__ballot_sync(0xffffffffu, active) == 0u) {
+            if (exhausted)
+                break;
+            continue;
+        }
+        bool done = false;
+        if (active && !step4<MASK>(P.scene, L, stack_node, stack_t, tc)) {
+            done = true;
+            active = false;
+        }
+        if (__any_sync(0xffffffffu, done))
+            src.finish(done, item, L);
+    }
+}
+
+struct PrimarySource {
+    const FrameParams& P;
+    const PathState& S;
+    uint32_t ntx, tiles;  // 16x16 pixel tiles per row, per image
+    uint32_t slot;
+    __device__ bool begin(uint32_t item, LaneRay& L)
+    {
+        uint32_t per = tiles * 256u;
+        uint32_t k = item / per, r = item - k * per;
+        uint32_t tile = r >> 8, within = r & 255u;
+        uint32_t ty = tile / ntx, tx = tile - ty * ntx;
+        uint32_t i = tx * 16u + (within & 15u), j = ty * 16u + (within >> 4);
+        if (i >= P.w || j >= P.h)
+            return false;
+        slot = k * P.w * P.h + j * P.w + i;
+        V3 o, d;
+        camera_ray(P.cam, i, j, P.n_samples + k, o, d);
+        lane_begin(L, o, d, PATH_TNEAR);
+        return true;
+    }
+    // warp-collective: every lane calls it after each step, `done` marks finished rays
+    __device__ void finish(bool done, uint32_t, const LaneRay& L)
+    {
+        bool push = false;
+        if (done) {
+            uint32_t prim = L.hit_geom == MISS ? 0u : __ldg(P.scene.geoms[L.hit_geom].order + L.hit_slot);
+            S.prim_hit[slot] = make_uint2(L.hit_geom, prim);
+            if (L.hit_geom == MISS) {
+                C3 res = P.bg * float(P.light_samples);
+                C3 out = c_div_recip(res, float(P.light_samples));
+                S.sample[slot] = make_float4(out.r, out.g, out.b, P.bg_alpha);
+            } else {
+                S.prim_o[slot] = f4(L.ray.o);
+                S.prim_d[slot] = f4(L.ray.d);
+                S.ls_depth[slot] = make_uint2(0u, 0u);
+                S.att[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+                S.result[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                push = true;
+            }
+        }
+        uint32_t m = __ballot_sync(0xffffffffu, push);
+        if (m) {
+            const uint32_t lane = threadIdx.x & 31u;
+            uint32_t at = 0;
+            if (lane == 0)
+                at = atomicAdd(S.ctr + 1, uint32_t(__popc(m)));
+            at = __shfl_sync(0xffffffffu, at, 0);
+            if (push)
+                S.queue[1][at + __popc(m & ((1u << lane) - 1u))] = slot;
+        }
+    }
+};
+
+struct ExtendSource {
+    const FrameParams& P;
+    const PathState& S;
+    const uint32_t* queue;
+    uint32_t slot;
+    __device__ bool begin(uint32_t item, LaneRay& L)
+    {
+        slot = queue[item];
+        lane_begin(L, xyz(S.ray_o[slot]), xyz(S.ray_d[slot]), PATH_TNEAR);
+        return true;
+    }
+    __device__ void finish(bool done, uint32_t, const LaneRay& L)
+    {
+        if (done) {
+            uint32_t prim = L.hit_geom == MISS ? 0u : __ldg(P.scene.geoms[L.hit_geom].order + L.hit_slot);
+            S.hit[slot] = make_uint2(L.hit_geom, prim);
+        }
+    }
+};
+
+__device__ __forceinline__ void flush_rays(const FrameParams& P, uint32_t n_rays, bool paths)
+{
+    unsigned long long r = n_rays;
+    for (int off = 16; off > 0; off >>= 1)
+        r += __shfl_xor_sync(0xffffffffu, r, off);
+    if (lane_id() == 0u && r) {
+        atomicAdd(P.stats + 0, r);
+        if (paths)
+            atomicAdd(P.stats + 1, r * P.light_samples);
+    }
+}
+
+template <uint32_t MASK>
+__global__ void __launch_bounds__(256) k_path_primary_persistent(FrameParams P, PathState S)
+{
+    uint32_t ntx = (P.w + 15u) / 16u, nty = (P.h + 15u) / 16u;
+    PrimarySource src{P, S, ntx, ntx * nty, 0u};
+    TraceCount tc;
+    uint32_t n_rays = 0;
+    persistent_trace<MASK>(P, src, P.batch * ntx * nty * 256u, S.ctr + 3, tc, n_rays);
+    flush_counts(tc, P.stats + 3);
+    flush_rays(P, n_rays, true);
+}
+
+template <uint32_t MASK>
+__global__ void __launch_bounds__(256) k_path_extend_persistent(FrameParams P, PathState S, int q)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        S.ctr[q ^ 1] = 0;  // the other queue was consumed by the shade pass that produced q
+    ExtendSource src{P, S, S.queue[q], 0u};
+    TraceCount tc;
+    uint32_t n_rays = 0;
+    persistent_trace<MASK>(P, src, S.ctr[q], S.ctr + 2, tc, n_rays);
+    flush_counts(tc, P.stats + 3);
+    flush_rays(P, n_rays, false);
 }
 
 // Fold the batch's samples into the running mean of each pixel, in sample order, then write
@@ -170,8 +351,8 @@ __global__ void __launch_bounds__(256) k_path_shade(FrameParams P, PathState S, 
 {
     if (blockIdx.x == 0 && threadIdx.x == 0)
         S.ctr[2] = 0;  // work counter of the extend kernel that follows
-    const uint32_t count = (in_q < 0) ? P.w * P.h * P.batch : S.ctr[in_q];
-    const uint32_t* inq = (in_q < 0) ? nullptr : S.queue[in_q];
+    const uint32_t count = S.ctr[in_q];
+    const uint32_t* inq = S.queue[in_q];
     uint32_t* outq = S.queue[out_q];
     uint32_t* outc = S.ctr + out_q;
     const uint32_t lane = threadIdx.x & 31u;
@@ -182,7 +363,7 @@ __global__ void __launch_bounds__(256) k_path_shade(FrameParams P, PathState S, 
         bool push = false;
         uint32_t p = 0;
         if (idx < count) {
-            p = inq ? inq[idx] : idx;
+            p = inq[idx];
             push = shade_pixel(P, S, p);
         }
         uint32_t m = __ballot_sync(0xffffffffu, push);
@@ -197,6 +378,7 @@ __global__ void __launch_bounds__(256) k_path_shade(FrameParams P, PathState S, 
     }
 }
 
+template <int WIDTH, uint32_t MASK>
 __global__ void __launch_bounds__(256) k_path_extend(FrameParams P, PathState S, int q)
 {
     if (blockIdx.x == 0 && threadIdx.x == 0)
@@ -204,24 +386,27 @@ __global__ void __launch_bounds__(256) k_path_extend(FrameParams P, PathState S,
     const uint32_t count = S.ctr[q];
     const uint32_t* queue = S.queue[q];
     const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t CHUNK = 32;  // rays claimed per atomic: one per lane keeps every warp busy
     TraceCount tc;
     while (true) {
         uint32_t base = 0;
         if (lane == 0)
-            base = atomicAdd(S.ctr + 2, 32u);
+            base = atomicAdd(S.ctr + 2, CHUNK);
         base = __shfl_sync(0xffffffffu, base, 0);
         if (base >= count)
             break;
-        uint32_t idx = base + lane;
-        if (idx < count) {
-            uint32_t p = queue[idx];
-            V3 o = xyz(S.ray_o[p]);
-            V3 d = xyz(S.ray_d[p]);
-            Hit h = trace_closest(P.scene, o, d, PATH_TNEAR, tc);
-            S.hit[p] = make_uint2(h.geom, h.prim);
+        for (uint32_t sub = 0; sub < CHUNK; sub += 32) {
+            uint32_t idx = base + sub + lane;
+            if (idx < count) {
+                uint32_t p = queue[idx];
+                V3 o = xyz(S.ray_o[p]);
+                V3 d = xyz(S.ray_d[p]);
+                Hit h = trace_closest<WIDTH, MASK>(P.scene, o, d, PATH_TNEAR, tc);
+                S.hit[p] = make_uint2(h.geom, h.prim);
+            }
         }
         if (lane == 0)
-            atomicAdd(P.stats + 0, (unsigned long long)min(32u, count - base));
+            atomicAdd(P.stats + 0, (unsigned long long)min(CHUNK, count - base));
     }
     flush_counts(tc, P.stats + 3);
 }
@@ -260,6 +445,7 @@ __device__ __forceinline__ C3 preview_shade(const FrameParams& P, const GeomDev&
     return c;
 }
 
+template <int WIDTH, uint32_t MASK>
 __global__ void __launch_bounds__(256) k_preview(FrameParams P, uint32_t aa_n, uint2* hits)
 {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -273,7 +459,7 @@ __global__ void __launch_bounds__(256) k_preview(FrameParams P, uint32_t aa_n, u
         for (uint32_t sample = 0; sample < ns; ++sample) {
             V3 o, d;
             camera_ray(P.cam, i, j, sample, o, d);
-            Hit h = trace_closest(P.scene, o, d, 0.0f, tc);  // preview tnear is 0 on the CPU path
+            Hit h = trace_closest<WIDTH, MASK>(P.scene, o, d, 0.0f, tc);  // CPU preview: tnear 0
             C3 c = P.bg;
             float a = P.bg_alpha;
             if (h.geom != MISS) {
@@ -301,24 +487,90 @@ __global__ void __launch_bounds__(256) k_preview(FrameParams P, uint32_t aa_n, u
     }
 }
 
+// Diagnostic: trace rays[i] = (o, d) with both 4-wide traversal forms (one ray per thread, and
+// the step-wise form stepped to completion by one lane); out[i] = (geom, prim, box tests) of
+// each, six words per ray.
+__global__ void k_traversal_compare(SceneDev sc, const float* rays, uint32_t n, uint32_t* out)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    V3 o = v3(rays[6 * i], rays[6 * i + 1], rays[6 * i + 2]);
+    V3 d = v3(rays[6 * i + 3], rays[6 * i + 4], rays[6 * i + 5]);
+    TraceCount a;
+    Hit h = trace_closest<4, MASK_SPHERES>(sc, o, d, PATH_TNEAR, a);
+    LaneRay L;
+    lane_begin(L, o, d, PATH_TNEAR);
+    uint32_t stack_node[TRAVERSAL_STACK];
+    float stack_t[TRAVERSAL_STACK];
+    TraceCount b;
+    for (int guard = 0; guard < 100000 && step4<MASK_SPHERES>(sc, L, stack_node, stack_t, b); ++guard) {
+    }
+    uint32_t prim = L.hit_geom == MISS ? 0u : __ldg(sc.geoms[L.hit_geom].order + L.hit_slot);
+    uint32_t* r = out + 6 * size_t(i);
+    r[0] = h.geom;
+    r[1] = h.prim;
+    r[2] = a.box;
+    r[3] = L.hit_geom;
+    r[4] = prim;
+    r[5] = b.box;
+}
+
 }  // namespace
+
+void launch_traversal_compare(const SceneDev& sc, const float* rays, uint32_t n, uint32_t* out,
+                              cudaStream_t st)
+{
+    k_traversal_compare<<<(n + 127) / 128, 128, 0, st>>>(sc, rays, n, out);
+}
+
+// Pick the kernel instantiation for the frame's BVH width and geometry mix.
+template <class F> F pick(const FrameParams& P, F w2s, F w2a, F w4s, F w4a)
+{
+    bool spheres_only = (P.type_mask & ~MASK_SPHERES) == 0u;
+    if (P.bvh_width == 4)
+        return spheres_only ? w4s : w4a;
+    return spheres_only ? w2s : w2a;
+}
+
+template <class K> int blocks_per_sm(K kernel)
+{
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, 256, 0);
+    return n > 0 ? n : 1;
+}
 
 LaunchShape path_launch_shape(int num_sms)
 {
-    int per_sm_shade = 0, per_sm_extend = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_shade, k_path_shade, 256, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_extend, k_path_extend, 256, 0);
     LaunchShape s;
-    s.shade_grid = num_sms * (per_sm_shade > 0 ? per_sm_shade : 1);
-    s.extend_grid = num_sms * (per_sm_extend > 0 ? per_sm_extend : 1);
+    s.shade_grid = num_sms * blocks_per_sm(k_path_shade);
+    s.extend_grid[0] = num_sms * blocks_per_sm(k_path_extend<2, MASK_SPHERES>);
+    s.extend_grid[1] = num_sms * blocks_per_sm(k_path_extend<2, MASK_ALL>);
+    s.extend_grid[2] = num_sms * blocks_per_sm(k_path_extend<4, MASK_SPHERES>);
+    s.extend_grid[3] = num_sms * blocks_per_sm(k_path_extend<4, MASK_ALL>);
+    s.persistent_grid[0] = num_sms * blocks_per_sm(k_path_extend_persistent<MASK_SPHERES>);
+    s.persistent_grid[1] = num_sms * blocks_per_sm(k_path_extend_persistent<MASK_ALL>);
+    s.primary_grid[0] = num_sms * blocks_per_sm(k_path_primary_persistent<MASK_SPHERES>);
+    s.primary_grid[1] = num_sms * blocks_per_sm(k_path_primary_persistent<MASK_ALL>);
     return s;
 }
 
-void launch_path_primary(const FrameParams& P, const PathState& S, cudaStream_t st)
+void launch_path_primary(const FrameParams& P, const PathState& S, const LaunchShape& shape,
+                         cudaStream_t st)
 {
+    bool spheres_only = (P.type_mask & ~MASK_SPHERES) == 0u;
+    if (P.bvh_width == 4 && P.persistent) {
+        if (spheres_only)
+            k_path_primary_persistent<MASK_SPHERES><<<shape.primary_grid[0], 256, 0, st>>>(P, S);
+        else
+            k_path_primary_persistent<MASK_ALL><<<shape.primary_grid[1], 256, 0, st>>>(P, S);
+        return;
+    }
     dim3 block(16, 16);
     dim3 grid((P.w + 15) / 16, (P.h + 15) / 16, P.batch);
-    k_path_primary<<<grid, block, 0, st>>>(P, S);
+    auto k = pick(P, k_path_primary<2, MASK_SPHERES>, k_path_primary<2, MASK_ALL>,
+                  k_path_primary<4, MASK_SPHERES>, k_path_primary<4, MASK_ALL>);
+    k<<<grid, block, 0, st>>>(P, S);
 }
 
 void launch_path_fold(const FrameParams& P, const PathState& S, cudaStream_t st)
@@ -329,21 +581,35 @@ void launch_path_fold(const FrameParams& P, const PathState& S, cudaStream_t st)
 void launch_path_shade(const FrameParams& P, const PathState& S, int iteration,
                        const LaunchShape& shape, cudaStream_t st)
 {
-    int in_q = iteration == 0 ? -1 : ((iteration - 1) & 1);
-    k_path_shade<<<shape.shade_grid, 256, 0, st>>>(P, S, in_q, iteration & 1);
+    // iteration 0 reads the primary hits (queue 1); then the queues alternate
+    k_path_shade<<<shape.shade_grid, 256, 0, st>>>(P, S, (iteration + 1) & 1, iteration & 1);
 }
 
 void launch_path_extend(const FrameParams& P, const PathState& S, int iteration,
                         const LaunchShape& shape, cudaStream_t st)
 {
-    k_path_extend<<<shape.extend_grid, 256, 0, st>>>(P, S, iteration & 1);
+    bool spheres_only = (P.type_mask & ~MASK_SPHERES) == 0u;
+    int q = iteration & 1;
+    if (P.bvh_width == 4 && P.persistent) {
+        if (spheres_only)
+            k_path_extend_persistent<MASK_SPHERES><<<shape.persistent_grid[0], 256, 0, st>>>(P, S, q);
+        else
+            k_path_extend_persistent<MASK_ALL><<<shape.persistent_grid[1], 256, 0, st>>>(P, S, q);
+        return;
+    }
+    int grid = shape.extend_grid[(P.bvh_width == 4 ? 2 : 0) + (spheres_only ? 0 : 1)];
+    auto k = pick(P, k_path_extend<2, MASK_SPHERES>, k_path_extend<2, MASK_ALL>,
+                  k_path_extend<4, MASK_SPHERES>, k_path_extend<4, MASK_ALL>);
+    k<<<grid, 256, 0, st>>>(P, S, q);
 }
 
 void launch_preview(const FrameParams& P, uint32_t aa_n, uint2* hits, cudaStream_t st)
 {
     dim3 block(16, 16);
     dim3 grid((P.w + 15) / 16, (P.h + 15) / 16);
-    k_preview<<<grid, block, 0, st>>>(P, aa_n, hits);
+    auto k = pick(P, k_preview<2, MASK_SPHERES>, k_preview<2, MASK_ALL>,
+                  k_preview<4, MASK_SPHERES>, k_preview<4, MASK_ALL>);
+    k<<<grid, block, 0, st>>>(P, aa_n, hits);
 }
 
 }  // namespace fr

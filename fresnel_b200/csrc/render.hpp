@@ -13,6 +13,9 @@ namespace fr {
 // Everything one render reads, passed by value to every kernel of that render.
 struct FrameParams {
     SceneDev scene;
+    int bvh_width;       // 2 or 4 (selects the kernel instantiation)
+    int persistent;      // 4-wide trees: persistent warps with per-lane refill (1) or not (0)
+    uint32_t type_mask;  // geometry types enabled in the scene (selects the instantiation)
     CamK cam;
     LightsK lights;
     C3 bg;
@@ -42,26 +45,33 @@ struct PathState {
     uint2* hit;         // closest hit of the last extension ray
     float4* sample;     // the finished pixel sample of each slot (folded in order at the end)
     uint32_t* queue[2];
-    uint32_t* ctr;      // [0], [1] queue lengths, [2] extend work counter
+    uint32_t* ctr;      // [0], [1] queue lengths, [2] extend and [3] primary work counters
 };
 
 struct LaunchShape {
     int shade_grid;
-    int extend_grid;
+    int extend_grid[4];      // [width 2|4][spheres only|all types]
+    int persistent_grid[2];  // 4-wide persistent extend kernel [spheres only|all types]
+    int primary_grid[2];     // 4-wide persistent primary kernel [spheres only|all types]
 };
 
 LaunchShape path_launch_shape(int num_sms);
 
 // One batch of P.batch TracerPath::render samples: primary rays for every slot ...
-void launch_path_primary(const FrameParams& P, const PathState& S, cudaStream_t st);
-// ... then iteration i of shade (queue in = i == 0 ? every slot : q[(i-1)&1], out = q[i&1])
-// and extend (q[i&1]) until the output queue is empty ...
+void launch_path_primary(const FrameParams& P, const PathState& S, const LaunchShape& shape,
+                         cudaStream_t st);
+// ... then iteration i of shade (queue in = q[(i+1)&1], out = q[i&1]; the primary kernel fills
+// q[1] with the slots whose primary ray hit) and extend (q[i&1]) until the output queue is
+// empty; both queue lengths are zero between batches ...
 void launch_path_shade(const FrameParams& P, const PathState& S, int iteration,
                        const LaunchShape& shape, cudaStream_t st);
 void launch_path_extend(const FrameParams& P, const PathState& S, int iteration,
                         const LaunchShape& shape, cudaStream_t st);
 // ... then fold the batch's samples into each pixel's running mean, in sample order.
 void launch_path_fold(const FrameParams& P, const PathState& S, cudaStream_t st);
+// Diagnostic comparison of the two 4-wide traversal forms (sphere scenes).
+void launch_traversal_compare(const SceneDev& sc, const float* rays, uint32_t n, uint32_t* out,
+                              cudaStream_t st);
 // TracerDirect::render
 void launch_preview(const FrameParams& P, uint32_t aa_n, uint2* hits, cudaStream_t st);
 

@@ -151,6 +151,16 @@ FR_API fr_status fr_device_synchronize(fr_device* dev);
  * reference (its OptiX launches are synchronous); used to time renders on the device. */
 FR_API fr_status fr_device_timer_start(fr_device* dev);
 FR_API fr_status fr_device_timer_stop(fr_device* dev, float* ms);
+/* Engine tuning options of a device (no counterpart in the reference, whose OptiX and Embree
+ * backends tune themselves); they apply to BVHs built and renders started afterwards:
+ *   "bvh_width"     2 or 4: binary or 4-wide tree traversed by the renderers (default 2)
+ *   "leaf_max"      largest leaf the SAH collapse may form (1..16, default 4)
+ *   "c_trav"        SAH cost of one node visit relative to one primitive test (default 1)
+ *   "path_slots"    path slots traced together by the path tracer (default 33554432)
+ * Setting an option marks every BVH of the device's scenes for rebuild when it changes the
+ * tree.  Unknown names or out-of-range values return FR_ERR_INVALID. */
+FR_API fr_status fr_device_set_option(fr_device* dev, const char* name, double value);
+FR_API fr_status fr_device_get_option(const fr_device* dev, const char* name, double* value);
 /* When enabled, every kernel launch of the path tracer is bracketed by CUDA events and its
  * device time is accumulated in fr_stats (primary/shade/extend).  Off by default. */
 FR_API fr_status fr_device_set_profiling(fr_device* dev, int enable);
@@ -232,9 +242,20 @@ FR_API fr_status fr_tracer_read_srgb(fr_tracer* tr, uint8_t* host, size_t nbytes
 FR_API fr_status fr_tracer_write_linear(fr_tracer* tr, const float* host, size_t nbytes);
 FR_API fr_status fr_tracer_write_srgb(fr_tracer* tr, const uint8_t* host, size_t nbytes);
 FR_API fr_status fr_tracer_get_stats(const fr_tracer* tr, fr_stats* out);
+/* Parity hook (no counterpart in the reference): the closest hits of the primary rays of the
+ * first sample of the last path-render batch, [h][w][2] = (geometry index or 0xFFFFFFFF,
+ * primitive index), for comparing traversal variants and the CPU oracle. */
+FR_API fr_status fr_tracer_read_primary_hits(fr_tracer* tr, uint32_t* host, size_t nbytes);
 FR_API fr_status fr_tracer_reset_stats(fr_tracer* tr);
 
 /* ---------------- self-tests ---------------- */
+
+/* Diagnostic (no counterpart in the reference): trace n rays (o.xyz, d.xyz, 6 floats each,
+ * host) through a sphere scene's 4-wide trees with the one-ray-per-thread traversal and with
+ * the step-wise traversal of the persistent kernels; out (host, 6 words per ray) receives
+ * (geometry, primitive, box tests) of each. */
+FR_API fr_status fr_debug_traversal_compare(fr_scene* scene, const float* rays, uint32_t n,
+                                            uint32_t* out);
 
 /* Runs the engine's device Philox4x32-10 and cuRAND's curand_Philox4x32_10 on n inputs
  * in[i] = (ctr0, ctr1, ctr2, ctr3, key0, key1) (host arrays; outputs n x 4 words each).
