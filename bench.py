@@ -50,9 +50,14 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="engine", choices=["engine", "reference"])
     p.add_argument("--spp", type=int, default=SPP, help="samples per pixel of one frame")
+    p.add_argument("--width", type=int, default=WIDTH,
+                   help="image width (smaller frames only for profiler captures)")
+    p.add_argument("--height", type=int, default=HEIGHT)
     p.add_argument("--cpu-seconds", type=float, default=15.0,
                    help="target duration of the CPU baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--trace-only", action="store_true",
+                   help="skip the end-to-end leg and the CPU baseline (profiler captures)")
     p.add_argument("--profile-kernels", action="store_true", default=True)
     return p.parse_args()
 
@@ -248,7 +253,7 @@ def main():
 
     device = fresnel.Device(mode="gpu", n=1)
     scene = build_scene(fresnel, device)
-    tracer = fresnel.tracer.Path(device, w=WIDTH, h=HEIGHT)
+    tracer = fresnel.tracer.Path(device, w=args.width, h=args.height)
     tracer.seed = 1000 * rank
     dd = device._device
 
@@ -279,7 +284,7 @@ def main():
 
     # roofline of the dominant traversal kernel (primary rays or extension rays)
     hbm, peak_kind = peaks()
-    primary_rays = float(WIDTH * HEIGHT * args.spp * args.steps)
+    primary_rays = float(args.width * args.height * args.spp * args.steps)
     ext_rays = max(0.0, rays - primary_rays)
     kern = {"k_path_primary": (primary_rays, st["primary_ms"]),
             "k_path_extend": (ext_rays, st["extend_ms"])}
@@ -296,14 +301,15 @@ def main():
             traffic = None
 
     # ---- end to end through the public API with host buffers ----------------------------------
+    e2e_ms = []
+    out = None
+    rays_per_frame = rays / args.steps
     rng = numpy.random.default_rng(1)
     h_pos = rng.uniform(-BOX / 2, BOX / 2, (N_SPHERES, 3)).astype(numpy.float32)
     h_col = rng.uniform(0, 1, (N_SPHERES, 3)).astype(numpy.float32)
     h_rad = numpy.full(N_SPHERES, 0.5, numpy.float32)
     geom = scene.geometry[0]
-    e2e_ms = []
-    out = None
-    for step in range(args.warmup + args.steps):
+    for step in range(0 if args.trace_only else args.warmup + args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         geom.position[:] = h_pos
@@ -314,13 +320,17 @@ def main():
         dt = (time.perf_counter() - t0) * 1e3
         if step >= args.warmup:
             e2e_ms.append(dt)
-    e2e_step = barrier_max(statistics.mean(e2e_ms))
-    rays_per_frame = rays / args.steps
-    e2e_value = barrier_sum(rays_per_frame) / (e2e_step / 1e3) / 1e6
-    assert out is not None and out.shape == (HEIGHT, WIDTH, 4)
+    e2e = None
+    if e2e_ms:
+        e2e_step = barrier_max(statistics.mean(e2e_ms))
+        e2e_value = barrier_sum(rays_per_frame) / (e2e_step / 1e3) / 1e6
+        assert out is not None and out.shape == (args.height, args.width, 4)
+        e2e = {"value": e2e_value, "unit": "Mrays/s",
+               "h2d_bytes_per_step": int(h_pos.nbytes + h_col.nbytes + h_rad.nbytes),
+               "d2h_bytes_per_step": int(out.nbytes), "ms_per_step": e2e_step}
 
     cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and not args.no_cpu_baseline and not args.trace_only:
         try:
             cpu = cpu_baseline("restated", args.cpu_seconds)
         except Exception as e:  # the baseline must not hide the GPU result
@@ -332,14 +342,14 @@ def main():
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded uniform spheres)",
-            "config": {"workload": "config2: 1M spheres r=0.5, box 140, 1920x1080, "
+            "config": {"workload": f"config2: 1M spheres r=0.5, box 140, {args.width}x{args.height}, "
                                    f"{args.spp} spp, 1 light sample, lightbox",
-                       "spheres": N_SPHERES, "width": WIDTH, "height": HEIGHT, "spp": args.spp,
+                       "spheres": N_SPHERES, "width": args.width, "height": args.height, "spp": args.spp,
                        "light_samples": LIGHT_SAMPLES,
                        "l2": "inputs larger than L2 (200 MB path state + 115 MB scene)",
                        "parallelism": f"replicas{world}"},
             "rays_per_frame": rays_per_frame,
-            "mpaths_per_s": WIDTH * HEIGHT * args.spp * args.steps * world / (ms_max / 1e3) / 1e6,
+            "mpaths_per_s": args.width * args.height * args.spp * args.steps * world / (ms_max / 1e3) / 1e6,
             "gpu_launches": int(st["kernel_launches"]),
             "kernels": {"primary_ms": st["primary_ms"], "shade_ms": st["shade_ms"],
                         "extend_ms": st["extend_ms"], "primary_launches": st["primary_launches"],
@@ -352,9 +362,7 @@ def main():
                          "rays": dom_rays, "kernel_ms": dom_ms,
                          "bytes_per_ray": BYTES_PER_RAY},
             "clocks": clk.summary(),
-            "e2e": {"value": e2e_value, "unit": "Mrays/s",
-                    "h2d_bytes_per_step": int(h_pos.nbytes + h_col.nbytes + h_rad.nbytes),
-                    "d2h_bytes_per_step": int(out.nbytes), "ms_per_step": e2e_step},
+            "e2e": e2e,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line))
