@@ -291,12 +291,18 @@ def main():
     dom = max(kern, key=lambda k: kern[k][1])
     dom_rays, dom_ms = kern[dom]
     achieved = (dom_rays * BYTES_PER_RAY) / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else None
+    # DRAM bytes per launch: the per-ray DRAM traffic of this kernel from an ncu capture
+    # (dram__bytes_read.sum + dram__bytes_write.sum over every launch of one frame, divided by
+    # that frame's rays) times the mean rays per launch here.
     traffic = None
     prof = os.path.join(REPO, "profiles", "traversal_traffic.json")
-    if os.path.exists(prof):
+    launches = st["primary_launches"] if dom == "k_path_primary" else st["extend_launches"]
+    if os.path.exists(prof) and launches:
         try:
             with open(prof) as f:
-                traffic = json.load(f).get(dom, {}).get("dram_bytes_per_ray")
+                per_ray = json.load(f).get(dom, {}).get("dram_bytes_per_ray")
+            if per_ray is not None:
+                traffic = per_ray * dom_rays / launches
         except Exception:
             traffic = None
 
@@ -309,7 +315,10 @@ def main():
     h_col = rng.uniform(0, 1, (N_SPHERES, 3)).astype(numpy.float32)
     h_rad = numpy.full(N_SPHERES, 0.5, numpy.float32)
     geom = scene.geometry[0]
+    builds = 0
     for step in range(0 if args.trace_only else args.warmup + args.steps):
+        if step == args.warmup:
+            tracer._tracer.resetStats()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         geom.position[:] = h_pos
@@ -322,12 +331,14 @@ def main():
             e2e_ms.append(dt)
     e2e = None
     if e2e_ms:
+        builds = int(tracer._tracer.getStats()["bvh_builds"])
         e2e_step = barrier_max(statistics.mean(e2e_ms))
         e2e_value = barrier_sum(rays_per_frame) / (e2e_step / 1e3) / 1e6
         assert out is not None and out.shape == (args.height, args.width, 4)
         e2e = {"value": e2e_value, "unit": "Mrays/s",
                "h2d_bytes_per_step": int(h_pos.nbytes + h_col.nbytes + h_rad.nbytes),
-               "d2h_bytes_per_step": int(out.nbytes), "ms_per_step": e2e_step}
+               "d2h_bytes_per_step": int(out.nbytes), "ms_per_step": e2e_step,
+               "bvh_builds": builds}
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline and not args.trace_only:
@@ -359,7 +370,7 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
                          "peak_source": peak_kind, "kernel": dom,
-                         "rays": dom_rays, "kernel_ms": dom_ms,
+                         "rays": dom_rays, "kernel_ms": dom_ms, "launches": launches,
                          "bytes_per_ray": BYTES_PER_RAY},
             "clocks": clk.summary(),
             "e2e": e2e,
