@@ -94,6 +94,7 @@ struct fr_device {
     size_t path_slots = size_t(32) << 20;  // path slots traced together
     int persistent = 0;                    // persistent traversal kernels for 4-wide trees
     std::vector<fr_scene*> scenes;         // to mark BVHs stale when a build option changes
+    void* static_path = nullptr;           // this device's copy of g_static_path (looked up once)
 };
 
 struct fr_geometry {
@@ -1099,6 +1100,139 @@ fr_status fr_tracer_render_path(fr_tracer* t, fr_scene* sc, const fr_render_para
                     "reading the queue length");
             FR_CUDA(cudaStreamSynchronize(st), "path tracer");
             t->collect();
+            if (*t->h_count == 0)
+                break;
+            if (it >= MAX_ITER)
+                return fail(FR_ERR_DEVICE_LIMIT, "path tracer exceeded the bounce iteration cap");
+        }
+        launch_path_fold(P, S, st);
+        t->launches++;
+        done += P.batch;
+    }
+    return check_status(t->dev);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Allocation-free path render.  The wavefront state of fr_tracer_render_path_static lives in
+// g_static_path: 16 bytes of queue/work counters, then each per-slot array sized for
+// FR_STATIC_PATH_SLOTS slots at a 256-byte aligned offset.  A __device__ array is created with
+// the module (one copy per GPU), so the call allocates nothing.
+}  // extern "C"
+
+namespace {
+
+constexpr size_t kStaticSlots = FR_STATIC_PATH_SLOTS;
+constexpr size_t kStaticBytes = 256 + kStaticSlots * (7 * sizeof(float4) + 3 * sizeof(uint2) +
+                                                      2 * sizeof(uint32_t));
+
+__device__ __align__(256) unsigned char g_static_path[kStaticBytes];
+
+// Carves the per-slot arrays out of the static block; false if they would not fit.
+bool static_path_state(void* base, PathState& S)
+{
+    ScratchLayout L;
+    uint32_t* ctr = L.take<uint32_t>(4);
+    S.prim_o = L.take<float4>(kStaticSlots);
+    S.prim_d = L.take<float4>(kStaticSlots);
+    S.ray_o = L.take<float4>(kStaticSlots);
+    S.ray_d = L.take<float4>(kStaticSlots);
+    S.att = L.take<float4>(kStaticSlots);
+    S.result = L.take<float4>(kStaticSlots);
+    S.sample = L.take<float4>(kStaticSlots);
+    S.prim_hit = L.take<uint2>(kStaticSlots);
+    S.ls_depth = L.take<uint2>(kStaticSlots);
+    S.hit = L.take<uint2>(kStaticSlots);
+    S.queue[0] = L.take<uint32_t>(kStaticSlots);
+    S.queue[1] = L.take<uint32_t>(kStaticSlots);
+    L.bind(base);
+    S.ctr = L.at(ctr);
+    S.prim_o = L.at(S.prim_o);
+    S.prim_d = L.at(S.prim_d);
+    S.ray_o = L.at(S.ray_o);
+    S.ray_d = L.at(S.ray_d);
+    S.att = L.at(S.att);
+    S.result = L.at(S.result);
+    S.sample = L.at(S.sample);
+    S.prim_hit = L.at(S.prim_hit);
+    S.ls_depth = L.at(S.ls_depth);
+    S.hit = L.at(S.hit);
+    S.queue[0] = L.at(S.queue[0]);
+    S.queue[1] = L.at(S.queue[1]);
+    return L.bytes <= kStaticBytes;
+}
+
+// With a multiple of 64 slots every per-slot array ends on a 256-byte boundary, so the only
+// padding is the 240 bytes after the counters and the layout is exactly kStaticBytes.
+static_assert(kStaticSlots % 64 == 0, "static path layout");
+
+}  // namespace
+
+extern "C" {
+
+fr_status fr_tracer_render_path_static(fr_tracer* t, fr_scene* sc, const fr_render_params* p,
+                                       uint32_t first_sample, uint32_t n_render,
+                                       uint32_t light_samples)
+{
+    fr_status s = check_params(t, sc, p);
+    if (s != FR_OK)
+        return s;
+    if (light_samples == 0)
+        return fail(FR_ERR_INVALID, "light_samples must be positive");
+    if (first_sample == 0)
+        return fail(FR_ERR_INVALID, "sample numbers start at 1");
+    const size_t wh = size_t(t->w) * t->h;
+    if (wh > kStaticSlots)
+        return fail(FR_ERR_INVALID, "image of " + std::to_string(t->w) + "x" +
+                                        std::to_string(t->h) +
+                                        " pixels exceeds the allocation-free render's limit of " +
+                                        std::to_string(kStaticSlots) + " pixels");
+    for (fr_geometry* g : sc->geoms)
+        if (!g->removed && g->bvh_dirty)
+            return fail(FR_ERR_STATE, "the allocation-free render needs a built scene: call "
+                                      "fr_scene_build after changing geometry");
+    if (sc->table_dirty)
+        return fail(FR_ERR_STATE, "the allocation-free render needs a built scene: call "
+                                  "fr_scene_build after changing geometry");
+    if ((s = use_device(t->dev)) != FR_OK)
+        return s;
+    if (!t->dev->static_path) {
+        void* base = nullptr;
+        FR_CUDA(cudaGetSymbolAddress(&base, g_static_path), "looking up the static path state");
+        t->dev->static_path = base;
+    }
+    if (n_render == 0)
+        return FR_OK;
+    PathState S;
+    if (!static_path_state(t->dev->static_path, S))
+        return fail(FR_ERR_STATE, "static path state layout exceeds its array");
+    size_t k = kStaticSlots / wh;
+    if (k > 4096)
+        k = 4096;  // the primary kernel's grid z dimension
+    const uint32_t batch = uint32_t(k);
+    FrameParams P = frame_params(t, sc, p, false, 1);
+    P.light_samples = light_samples;
+    cudaStream_t st = t->dev->stream;
+    FR_CUDA(cudaMemsetAsync(S.ctr, 0, 4 * sizeof(uint32_t), st), "clearing queue lengths");
+    const int CHECK_EVERY = 8;
+    const int MAX_ITER = 1 << 20;
+    for (uint32_t done = 0; done < n_render;) {
+        P.n_samples = first_sample + done;
+        P.batch = batch < n_render - done ? batch : n_render - done;
+        FR_CUDA(cudaMemsetAsync(S.ctr + 3, 0, sizeof(uint32_t), st), "clearing a counter");
+        launch_path_primary(P, S, t->dev->shape, st);
+        t->launches++;
+        int it = 0;
+        while (true) {
+            for (int b = 0; b < CHECK_EVERY; ++b, ++it) {
+                launch_path_shade(P, S, it, t->dev->shape, st);
+                launch_path_extend(P, S, it, t->dev->shape, st);
+                t->launches += 2;
+            }
+            FR_CUDA(cudaGetLastError(), "launching the path tracer");
+            FR_CUDA(cudaMemcpyAsync(t->h_count, S.ctr + ((it - 1) & 1), sizeof(uint32_t),
+                                    cudaMemcpyDeviceToHost, st),
+                    "reading the queue length");
+            FR_CUDA(cudaStreamSynchronize(st), "path tracer");
             if (*t->h_count == 0)
                 break;
             if (it >= MAX_ITER)

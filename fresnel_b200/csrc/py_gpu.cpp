@@ -546,6 +546,15 @@ struct TracerPathH : TracerH {
         check(fr_tracer_render_path(tracer, s->scene, &p, n_samples + 1, k, light_samples));
         n_samples += k;
     }
+    // The same k renders through the allocation-free entry point (the scene must be built).
+    void render_samples_static(std::shared_ptr<SceneH> s, unsigned k)
+    {
+        check_scene(s);
+        s->sync();
+        fr_render_params p = params(*s);
+        check(fr_tracer_render_path_static(tracer, s->scene, &p, n_samples + 1, k, light_samples));
+        n_samples += k;
+    }
 };
 
 template <class A> void export_array(py::module_& m, const char* name)
@@ -681,6 +690,7 @@ PYBIND11_MODULE(_gpu, m)
         .def("reset", &TracerPathH::reset)
         .def("setLightSamples", [](TracerPathH& t, unsigned n) { t.light_samples = n; })
         .def("renderSamples", &TracerPathH::render_samples)
+        .def("renderSamplesStatic", &TracerPathH::render_samples_static)
         .def("primaryHits", [](TracerPathH& t) {
             py::array_t<uint32_t> out({py::ssize_t(t.h), py::ssize_t(t.w), py::ssize_t(2)});
             check(fr_tracer_read_primary_hits(t.tracer, out.mutable_data(), size_t(t.w) * t.h * 8));

@@ -248,6 +248,35 @@ FR_API fr_status fr_tracer_get_stats(const fr_tracer* tr, fr_stats* out);
 FR_API fr_status fr_tracer_read_primary_hits(fr_tracer* tr, uint32_t* host, size_t nbytes);
 FR_API fr_status fr_tracer_reset_stats(fr_tracer* tr);
 
+/* ---------------- allocation-free path render ----------------
+ * No counterpart in the reference.  fr_tracer_render_path keeps its wavefront state (rays,
+ * throughputs, queues) in tracer-owned device memory that it allocates on first use and
+ * reallocates when a call needs a larger batch; cudaFree of the old block waits for the whole
+ * GPU.  fr_tracer_render_path_static renders the same images without allocating any memory: the
+ * wavefront state lives in one fixed array of FR_STATIC_PATH_SLOTS slots of 144 bytes (37.7 MB)
+ * inside the library's device module.  It is for callers that must not allocate inside a render
+ * call: a runtime that reserves the GPU's memory up front for its own pool, or a frame loop
+ * that shares the GPU with other streams and cannot let a cudaFree stall them.
+ *
+ *  - Limit: the image may have at most FR_STATIC_PATH_SLOTS pixels (512 x 512, or any
+ *    w * h <= 262144); larger images return FR_ERR_INVALID.  Each wavefront traces
+ *    FR_STATIC_PATH_SLOTS / (w * h) samples of every pixel (at most 4096).
+ *  - The scene must be built (fr_scene_build after its last change): a build allocates, so a
+ *    scene with stale BVHs or geometry table returns FR_ERR_STATE.
+ *  - The first call on each device looks up the array's address (cudaGetSymbolAddress, which
+ *    may load the library's device module).  Make that first call outside any CUDA stream
+ *    capture.
+ *  - The array is shared by all tracers of the process on one GPU.  Calls that overlap in time
+ *    (several host threads, or several fr_device handles on the same GPU) race on it and give
+ *    wrong images: serialise them.
+ *  - The queue-length counters at the start of the array are cleared by every call; nothing
+ *    else needs to start at zero.  Kernel profiling (fr_device_set_profiling) is ignored here.
+ * Arguments and results are those of fr_tracer_render_path. */
+#define FR_STATIC_PATH_SLOTS 262144u
+FR_API fr_status fr_tracer_render_path_static(fr_tracer* tr, fr_scene* scene,
+                                              const fr_render_params* params, uint32_t first_sample,
+                                              uint32_t n_render, uint32_t light_samples);
+
 /* ---------------- self-tests ---------------- */
 
 /* Diagnostic (no counterpart in the reference): trace n rays (o.xyz, d.xyz, 6 floats each,
