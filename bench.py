@@ -4,16 +4,19 @@ Workload (one step = one full frame): 1,000,000 spheres (r = 0.5, positions unif
 of side 140, per-particle colours), lightbox lighting, perspective camera fit to the scene,
 1920x1080, 256 samples per pixel, 1 light sample -- ``Tracer.Path.sample(scene, 256)``.
 Synthetic, seeded inputs stand in for the scene (the reference publishes no benchmark data).
+``--workload`` selects the other measured configurations (the 1k-sphere 580x580 scene at 64 spp
+x 32 light samples, the mixed-geometry 720p scene, Preview of the 1M-sphere scene).
 
 Prints one JSON line:
   value      trace-only throughput: closest-hit queries per second over the K timed frames,
              scene and BVH resident in HBM, device time from CUDA events on the engine's stream
              (max over ranks); every rank renders its own frame (weak scaling, no collective)
-  e2e        the same metric through the public API with host buffers: each step uploads the
-             sphere arrays from host memory, rebuilds the BVH, renders 256 spp and reads the
+  e2e        the same metric through the public API with host buffers: each step writes the
+             geometry arrays from host memory, rebuilds the BVH, renders the frame and reads the
              sRGB image back
-  roofline   the dominant kernel (BVH traversal of extension rays): algorithmic bytes per ray
-             (measured A/P costs of the oracle BVH) x rays / its device time
+  roofline   the traversal kernel with the most device time: algorithmic bytes per ray (box and
+             primitive test counts of the oracle's BVH on this scene, frozen below) x rays / its
+             device time
   cpu_baseline  the CPU oracle on this host's cores on a bounded sample of the same frame
 ``--impl reference`` times the reference's CPU path (the oracle compiled from the reference's
 own fresnel/common headers) on the same workload and prints the same line with impl=reference.
@@ -31,16 +34,47 @@ import time
 REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
-# Per-ray algorithmic bytes of the traversal kernel: ray in (24) + hit out (16) + 32 B per
-# box test (A per ray) + 16 B per sphere test (P per ray) + 12 B colour at the closest hit.
-# A and P are the oracle BVH's (binned SAH, leaves <= 4) mean costs per extension ray on this
-# scene and camera, measured by oracle/measure_ray_costs.py and frozen here.
-RAY_BOX_TESTS = 37.74
-RAY_PRIM_TESTS = 1.42
-BYTES_PER_RAY = 24 + 16 + 32 * RAY_BOX_TESTS + 16 * RAY_PRIM_TESTS + 12
+METRIC = "Mrays/s on 1M-sphere 1080p path trace"
 
-WIDTH, HEIGHT, SPP, LIGHT_SAMPLES = 1920, 1080, 256, 1
-N_SPHERES, BOX = 1_000_000, 140.0
+
+class Workload:
+    """One measured configuration.
+
+    box_tests / prim_tests: mean AABB and primitive tests per closest-hit query of the oracle's
+    BVH (binned SAH, BVH2, leaves <= 4) on this scene and camera, measured by
+    oracle/measure_ray_costs.py and frozen here; prim_bytes: bytes read per primitive test.
+    Algorithmic bytes per ray = 24 (ray) + 16 (hit) + 32 A + prim_bytes P + 12 (colour).
+    """
+
+    def __init__(self, key, desc, scene, w, h, spp=1, light_samples=1, preview=False, aa_n=1,
+                 box_tests=0.0, prim_tests=0.0, prim_bytes=16):
+        self.key, self.desc, self.scene = key, desc, scene
+        self.w, self.h, self.spp, self.light_samples = w, h, spp, light_samples
+        self.preview, self.aa_n = preview, aa_n
+        self.box_tests, self.prim_tests, self.prim_bytes = box_tests, prim_tests, prim_bytes
+
+    @property
+    def bytes_per_ray(self):
+        return 24 + 16 + 32 * self.box_tests + self.prim_bytes * self.prim_tests + 12
+
+    def build(self, device):
+        from fresnel_b200 import workloads
+        return getattr(workloads, self.scene)(device)
+
+
+WORKLOADS = {
+    "c2": Workload("c2", "config2: 1M spheres r=0.5, box 140, {w}x{h}, {spp} spp, 1 light sample, "
+                   "lightbox", "config2", 1920, 1080, spp=256, box_tests=37.74, prim_tests=1.42),
+    "c2-preview": Workload("c2-preview", "config2 Preview: 1M spheres, {w}x{h}, anti_alias "
+                           "(64 samples per pixel)", "config2", 1920, 1080, preview=True, aa_n=8,
+                           box_tests=29.41, prim_tests=0.95),
+    "c1": Workload("c1", "config1: 1000 spheres r=0.5, box 20, outline 0.1, cloudy, {w}x{h}, "
+                   "{spp} spp x 32 light samples", "config1", 580, 580, spp=64, light_samples=32,
+                   box_tests=37.41, prim_tests=1.81),
+    "c3": Workload("c3", "config3: 200k spheres + 50k bonds + 20k cubes + 10k icosahedra, "
+                   "{w}x{h}, {spp} spp, 1 light sample", "config3", 1280, 720, spp=128,
+                   box_tests=43.51, prim_tests=1.86, prim_bytes=28),
+}
 
 
 def parse():
@@ -49,17 +83,22 @@ def parse():
     p.add_argument("--steps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    p.add_argument("--spp", type=int, default=SPP, help="samples per pixel of one frame")
-    p.add_argument("--width", type=int, default=WIDTH,
+    p.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    p.add_argument("--spp", type=int, default=None, help="samples per pixel of one frame")
+    p.add_argument("--width", type=int, default=None,
                    help="image width (smaller frames only for profiler captures)")
-    p.add_argument("--height", type=int, default=HEIGHT)
+    p.add_argument("--height", type=int, default=None)
     p.add_argument("--cpu-seconds", type=float, default=15.0,
                    help="target duration of the CPU baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--trace-only", action="store_true",
                    help="skip the end-to-end leg and the CPU baseline (profiler captures)")
-    p.add_argument("--profile-kernels", action="store_true", default=True)
-    return p.parse_args()
+    a = p.parse_args()
+    wl = WORKLOADS[a.workload]
+    wl.w = a.width or wl.w
+    wl.h = a.height or wl.h
+    wl.spp = a.spp or wl.spp
+    return a, wl
 
 
 def peaks():
@@ -147,49 +186,70 @@ def pin_gpu(local):
     return local
 
 
-def build_scene(fresnel, device):
-    from fresnel_b200 import workloads
-    return workloads.config2(device, n=N_SPHERES, box=BOX)
+def cpu_baseline(wl, kind, seconds):
+    """Time the CPU oracle on a bounded sample of the frame.
 
-
-def cpu_baseline(kind, seconds, world_rank=0):
-    """Time the CPU oracle on a bounded sample of the frame: random pixels, 1 sample each."""
+    Path: rounds of random pixels of the frame, one pixel sample (x light samples) each.
+    Preview: the frame at 1/8 of the resolution in each direction, same camera and AA level.
+    """
     import numpy
 
     import fresnel_b200 as fresnel  # noqa: F401
     from oracle import cpu_module
     dev = cpu_module.make_device(kind)
-    scene = build_scene(None, dev)
+    scene = wl.build(dev)
     t0 = time.perf_counter()
     scene._scene.handle()  # BVH build, not timed
     build_s = time.perf_counter() - t0
-    tracer = dev.module.TracerPath(dev._device, WIDTH, HEIGHT, LIGHT_SAMPLES)
-    tracer.setSeed(2)
-    rng = numpy.random.default_rng(0)
-    n_pix = 4096
     total_rays = 0
     elapsed = 0.0
     rounds = 0
-    while elapsed < seconds and rounds < 1000:
-        pixels = numpy.sort(rng.choice(WIDTH * HEIGHT, n_pix, replace=False)).astype(numpy.uint32)
-        tracer.stats = cpu_module.OrStats()
-        t0 = time.perf_counter()
-        tracer.render_pixels(scene._scene, pixels, 1 + rounds, 1, want_m2=False)
-        elapsed += time.perf_counter() - t0
-        total_rays += tracer.stats.rays
-        rounds += 1
-        if rounds == 1:
-            # scale the batch so that one round takes about a second
-            per_pix = elapsed / n_pix
-            n_pix = int(min(WIDTH * HEIGHT, max(1024, 1.0 / max(per_pix, 1e-9))))
+    if wl.preview:
+        w, h = max(1, wl.w // 8), max(1, wl.h // 8)
+        tracer = dev.module.TracerDirect(dev._device, w, h)
+        tracer.setAntialiasingN(wl.aa_n)
+        while elapsed < seconds and rounds < 1000:
+            tracer.stats = cpu_module.OrStats()
+            t0 = time.perf_counter()
+            tracer.render(scene._scene)
+            elapsed += time.perf_counter() - t0
+            total_rays += tracer.stats.rays
+            rounds += 1
+        sample = (f"{rounds} Preview renders of the frame at {w}x{h} (AA {wl.aa_n}x{wl.aa_n}), "
+                  f"{total_rays} closest-hit queries in {elapsed:.1f} s "
+                  f"(BVH build {build_s:.1f} s, not timed)")
+    else:
+        tracer = dev.module.TracerPath(dev._device, wl.w, wl.h, wl.light_samples)
+        tracer.setSeed(2)
+        rng = numpy.random.default_rng(0)
+        n_pix = 1024
+        while elapsed < seconds and rounds < 1000:
+            pixels = numpy.sort(rng.choice(wl.w * wl.h, min(n_pix, wl.w * wl.h),
+                                           replace=False)).astype(numpy.uint32)
+            tracer.stats = cpu_module.OrStats()
+            t0 = time.perf_counter()
+            tracer.render_pixels(scene._scene, pixels, 1 + rounds, 1, want_m2=False)
+            elapsed += time.perf_counter() - t0
+            total_rays += tracer.stats.rays
+            rounds += 1
+            if rounds == 1:
+                # scale the batch so that one round takes about a second
+                per_pix = elapsed / len(pixels)
+                n_pix = int(min(wl.w * wl.h, max(256, 1.0 / max(per_pix, 1e-9))))
+        sample = (f"{rounds} rounds of random pixels of the {wl.w}x{wl.h} frame, 1 sample each "
+                  f"x {wl.light_samples} light samples, {total_rays} closest-hit queries in "
+                  f"{elapsed:.1f} s (BVH build {build_s:.1f} s, not timed)")
     return {"value": total_rays / elapsed / 1e6, "unit": "Mrays/s", "cores": os.cpu_count(),
-            "kind": "reference" if kind == "reference" else "port",
-            "sample": f"{rounds} rounds of random pixels of the 1920x1080 frame, 1 sample each, "
-                      f"{total_rays} closest-hit queries in {elapsed:.1f} s "
-                      f"(BVH build {build_s:.1f} s, not timed)"}
+            "kind": "reference" if kind == "reference" else "port", "sample": sample}
 
 
-def run_reference(args):
+def config_of(wl, world):
+    return {"workload": wl.desc.format(w=wl.w, h=wl.h, spp=wl.spp), "width": wl.w,
+            "height": wl.h, "spp": wl.spp if not wl.preview else wl.aa_n * wl.aa_n,
+            "light_samples": wl.light_samples, "parallelism": f"replicas{world}"}
+
+
+def run_reference(args, wl):
     world, rank, _ = dist_init()
     if rank != 0:
         return 0
@@ -197,37 +257,49 @@ def run_reference(args):
     kind = "reference" if os.path.exists(cpu_module.LIB_PATHS["reference"]) else "restated"
     per_step = max(2.0, min(20.0, 60.0 / max(1, args.steps + args.warmup)))
     for _ in range(args.warmup):
-        cpu_baseline(kind, per_step / 4)
-    vals = [cpu_baseline(kind, per_step) for _ in range(args.steps)]
+        cpu_baseline(wl, kind, per_step / 4)
+    vals = [cpu_baseline(wl, kind, per_step) for _ in range(args.steps)]
     v = statistics.median(x["value"] for x in vals)
     base = dict(vals[0])
     base["value"] = v
+    cfg = config_of(wl, world)
+    cfg["inputs"] = "host memory"
     line = {
-        "metric": "Mrays/s on 1M-sphere 1080p path trace", "value": v, "unit": "Mrays/s",
-        "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic (seeded uniform spheres)",
-        "config": {"workload": "config2: 1M spheres r=0.5, box 140, 1920x1080, 256 spp, "
-                               "1 light sample, lightbox", "inputs": "host memory"},
-        "cpu_baseline": base,
+        "metric": METRIC if wl.key == "c2" else f"Mrays/s ({wl.key})",
+        "value": v, "unit": "Mrays/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded)", "config": cfg, "cpu_baseline": base,
         "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
     return 0
 
 
+def host_arrays(scene):
+    """(array, host copy) for every geometry array of the scene (written again each e2e step)."""
+    import numpy
+    out = []
+    for g in scene.geometry:
+        for name in ("position", "points", "radius", "orientation", "color"):
+            try:
+                a = getattr(g, name)
+            except (AttributeError, RuntimeError):
+                continue
+            out.append((a, numpy.array(a[:], copy=True)))
+    return out
+
+
 def main():
-    args = parse()
+    args, wl = parse()
     world, rank, local = dist_init()
     if args.impl == "reference":
-        return run_reference(args)
+        return run_reference(args, wl)
     if world > 1:
         pin_gpu(local)
-    import numpy
     import torch
 
     import fresnel_b200 as fresnel
-    from fresnel_b200 import workloads  # noqa: F401
 
     pg = None
     if world > 1:
@@ -252,16 +324,25 @@ def main():
         return float(t.item())
 
     device = fresnel.Device(mode="gpu", n=1)
-    scene = build_scene(fresnel, device)
-    tracer = fresnel.tracer.Path(device, w=args.width, h=args.height)
-    tracer.seed = 1000 * rank
+    scene = wl.build(device)
     dd = device._device
+    if wl.preview:
+        tracer = fresnel.tracer.Preview(device, w=wl.w, h=wl.h, anti_alias=wl.aa_n > 1)
+
+        def frame():
+            tracer.render(scene)
+    else:
+        tracer = fresnel.tracer.Path(device, w=wl.w, h=wl.h)
+
+        def frame():
+            tracer.sample(scene, samples=wl.spp, light_samples=wl.light_samples)
+    tracer.seed = 1000 * rank
 
     # ---- trace-only: BVH built and resident, K full frames ---------------------------------
     scene._scene.build()
     for _ in range(args.warmup):
-        tracer.sample(scene, samples=args.spp, light_samples=LIGHT_SAMPLES)
-    dd.setProfiling(bool(args.profile_kernels))
+        frame()
+    dd.setProfiling(True)
     tracer._tracer.resetStats()
     if pg is not None:
         pg.barrier()
@@ -270,7 +351,7 @@ def main():
     with ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0)) as clk:
         dd.timerStart()
         for _ in range(args.steps):
-            tracer.sample(scene, samples=args.spp, light_samples=LIGHT_SAMPLES)
+            frame()
         ms = dd.timerStop()
     torch.cuda.synchronize()
     if pg is not None:
@@ -282,22 +363,24 @@ def main():
     rays_all = barrier_sum(rays)
     value = rays_all / (ms_max / 1e3) / 1e6
 
-    # roofline of the dominant traversal kernel (primary rays or extension rays)
+    # roofline of the traversal kernel with the most device time
     hbm, peak_kind = peaks()
-    primary_rays = float(args.width * args.height * args.spp * args.steps)
-    ext_rays = max(0.0, rays - primary_rays)
-    kern = {"k_path_primary": (primary_rays, st["primary_ms"]),
-            "k_path_extend": (ext_rays, st["extend_ms"])}
+    if wl.preview:
+        kern = {"k_preview": (rays, ms, args.steps)}
+    else:
+        primary_rays = float(wl.w * wl.h * wl.spp * args.steps)
+        ext_rays = max(0.0, rays - primary_rays)
+        kern = {"k_path_primary": (primary_rays, st["primary_ms"], st["primary_launches"]),
+                "k_path_extend": (ext_rays, st["extend_ms"], st["extend_launches"])}
     dom = max(kern, key=lambda k: kern[k][1])
-    dom_rays, dom_ms = kern[dom]
-    achieved = (dom_rays * BYTES_PER_RAY) / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else None
-    # DRAM bytes per launch: the per-ray DRAM traffic of this kernel from an ncu capture
+    dom_rays, dom_ms, launches = kern[dom]
+    achieved = (dom_rays * wl.bytes_per_ray) / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else None
+    # DRAM bytes per launch: this kernel's DRAM bytes per ray from an ncu capture
     # (dram__bytes_read.sum + dram__bytes_write.sum over every launch of one frame, divided by
     # that frame's rays) times the mean rays per launch here.
     traffic = None
     prof = os.path.join(REPO, "profiles", "traversal_traffic.json")
-    launches = st["primary_launches"] if dom == "k_path_primary" else st["extend_launches"]
-    if os.path.exists(prof) and launches:
+    if wl.key == "c2" and os.path.exists(prof) and launches:
         try:
             with open(prof) as f:
                 per_ray = json.load(f).get(dom, {}).get("dram_bytes_per_ray")
@@ -310,21 +393,16 @@ def main():
     e2e_ms = []
     out = None
     rays_per_frame = rays / args.steps
-    rng = numpy.random.default_rng(1)
-    h_pos = rng.uniform(-BOX / 2, BOX / 2, (N_SPHERES, 3)).astype(numpy.float32)
-    h_col = rng.uniform(0, 1, (N_SPHERES, 3)).astype(numpy.float32)
-    h_rad = numpy.full(N_SPHERES, 0.5, numpy.float32)
-    geom = scene.geometry[0]
+    arrays = host_arrays(scene)
     builds = 0
     for step in range(0 if args.trace_only else args.warmup + args.steps):
         if step == args.warmup:
             tracer._tracer.resetStats()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        geom.position[:] = h_pos
-        geom.radius[:] = h_rad
-        geom.color[:] = h_col
-        tracer.sample(scene, samples=args.spp, light_samples=LIGHT_SAMPLES)
+        for a, host in arrays:
+            a[:] = host
+        frame()
         out = tracer.output[:]
         dt = (time.perf_counter() - t0) * 1e3
         if step >= args.warmup:
@@ -334,48 +412,52 @@ def main():
         builds = int(tracer._tracer.getStats()["bvh_builds"])
         e2e_step = barrier_max(statistics.mean(e2e_ms))
         e2e_value = barrier_sum(rays_per_frame) / (e2e_step / 1e3) / 1e6
-        assert out is not None and out.shape == (args.height, args.width, 4)
+        assert out is not None and out.shape == (wl.h, wl.w, 4)
         e2e = {"value": e2e_value, "unit": "Mrays/s",
-               "h2d_bytes_per_step": int(h_pos.nbytes + h_col.nbytes + h_rad.nbytes),
+               "h2d_bytes_per_step": int(sum(h.nbytes for _, h in arrays)),
                "d2h_bytes_per_step": int(out.nbytes), "ms_per_step": e2e_step,
                "bvh_builds": builds}
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline and not args.trace_only:
         try:
-            cpu = cpu_baseline("restated", args.cpu_seconds)
+            cpu = cpu_baseline(wl, "restated", args.cpu_seconds)
         except Exception as e:  # the baseline must not hide the GPU result
             cpu = {"value": None, "unit": "Mrays/s", "error": str(e)[:200]}
 
     if rank == 0:
+        cfg = config_of(wl, world)
+        cfg["l2"] = ("inputs larger than L2 (path state of 144 B per slot for every sample in "
+                     "flight, plus the scene arrays and BVH)" if not wl.preview else
+                     "scene arrays and BVH; the image is written once per frame")
         line = {
-            "metric": "Mrays/s on 1M-sphere 1080p path trace", "value": value, "unit": "Mrays/s",
+            "metric": METRIC if wl.key == "c2" else f"Mrays/s ({wl.key})",
+            "value": value, "unit": "Mrays/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded uniform spheres)",
-            "config": {"workload": f"config2: 1M spheres r=0.5, box 140, {args.width}x{args.height}, "
-                                   f"{args.spp} spp, 1 light sample, lightbox",
-                       "spheres": N_SPHERES, "width": args.width, "height": args.height, "spp": args.spp,
-                       "light_samples": LIGHT_SAMPLES,
-                       "l2": "inputs larger than L2 (200 MB path state + 115 MB scene)",
-                       "parallelism": f"replicas{world}"},
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": cfg,
             "rays_per_frame": rays_per_frame,
-            "mpaths_per_s": args.width * args.height * args.spp * args.steps * world / (ms_max / 1e3) / 1e6,
             "gpu_launches": int(st["kernel_launches"]),
-            "kernels": {"primary_ms": st["primary_ms"], "shade_ms": st["shade_ms"],
-                        "extend_ms": st["extend_ms"], "primary_launches": st["primary_launches"],
-                        "shade_launches": st["shade_launches"],
-                        "extend_launches": st["extend_launches"],
-                        "primary_rays": primary_rays, "extension_rays": ext_rays},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
                          "peak_source": peak_kind, "kernel": dom,
                          "rays": dom_rays, "kernel_ms": dom_ms, "launches": launches,
-                         "bytes_per_ray": BYTES_PER_RAY},
+                         "bytes_per_ray": wl.bytes_per_ray},
             "clocks": clk.summary(),
             "e2e": e2e,
             "cpu_baseline": cpu,
         }
+        if not wl.preview:
+            line["mpaths_per_s"] = (wl.w * wl.h * wl.spp * wl.light_samples * args.steps * world
+                                    / (ms_max / 1e3) / 1e6)
+            line["kernels"] = {"primary_ms": st["primary_ms"], "shade_ms": st["shade_ms"],
+                               "extend_ms": st["extend_ms"],
+                               "primary_launches": st["primary_launches"],
+                               "shade_launches": st["shade_launches"],
+                               "extend_launches": st["extend_launches"],
+                               "primary_rays": kern["k_path_primary"][0],
+                               "extension_rays": kern["k_path_extend"][0]}
         print(json.dumps(line))
     if pg is not None:
         pg.barrier()
