@@ -8,12 +8,14 @@
 //                array changed, like OptiX's markDirty, fresnel/gpu/Scene.h:64-83)
 //   fr_tracer    output buffers (linear RGBA f32, sRGB RGBA8) and the path tracer's per-pixel
 //                wavefront state (allocated on first path render)
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <limits>
 #include <string>
 #include <vector>
 
+#include "batch.hpp"
 #include "bvh.hpp"
 #include "fresnel_b200.h"
 #include "render.hpp"
@@ -214,6 +216,42 @@ struct fr_tracer {
             event_pool.push_back(p.b);
         }
         pending.clear();
+    }
+};
+
+// Many path renders traced together (batch.hpp). Items are queued by fr_batch_add_path and
+// traced by fr_batch_render; the tracers and scenes must live until then.
+struct fr_batch {
+    fr_device* dev = nullptr;
+    struct Item {
+        fr_tracer* tr;
+        fr_scene* sc;
+        fr_render_params params;
+        uint32_t first, n, light_samples;
+    };
+    std::vector<Item> items;
+    // device-side plan and path state (their addresses are baked into the graph)
+    DevArray<WaveJob> jobs;
+    DevArray<uint32_t> wave_first, wave_tiles, wave_pixels;
+    DevArray<BatchCtl> ctl;
+    DevArray<float4> prim_o, prim_d, ray_o, ray_d, att, result, sample;
+    DevArray<uint2> prim_hit, ls_depth, hit;
+    DevArray<uint32_t> q0, q1, ctr;
+    size_t slots = 0;  // path-state capacity
+    BatchCtl* h_ctl = nullptr;  // pinned
+    cudaGraphExec_t exec = nullptr;
+    int exec_width = 0;
+    uint32_t exec_mask = 0;
+    cudaStream_t capture = nullptr;
+    fr_batch_stats stats{};
+    ~fr_batch()
+    {
+        if (exec)
+            cudaGraphExecDestroy(exec);
+        if (capture)
+            cudaStreamDestroy(capture);
+        if (h_ctl)
+            cudaFreeHost(h_ctl);
     }
 };
 
@@ -1415,6 +1453,305 @@ fr_status fr_tracer_reset_stats(fr_tracer* t)
         t->kernel_ms[k] = 0.0;
         t->kernel_launches[k] = 0;
     }
+    return FR_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Batched path renders
+// ---------------------------------------------------------------------------------------------
+fr_status fr_batch_create(fr_device* dev, fr_batch** out)
+{
+    FR_CHECK_NULL(dev);
+    FR_CHECK_NULL(out);
+    *out = nullptr;
+    fr_status s = use_device(dev);
+    if (s != FR_OK)
+        return s;
+    fr_batch* b = new fr_batch;
+    b->dev = dev;
+    cudaError_t e = cudaMallocHost((void**)&b->h_ctl, sizeof(BatchCtl));
+    if (e == cudaSuccess)
+        e = cudaStreamCreateWithFlags(&b->capture, cudaStreamNonBlocking);
+    if (e == cudaSuccess)
+        e = b->ctl.reserve(1);
+    if (e != cudaSuccess) {
+        delete b;
+        return cuda_fail(e, "creating a batch");
+    }
+    *out = b;
+    return FR_OK;
+}
+
+fr_status fr_batch_destroy(fr_batch* b)
+{
+    if (!b)
+        return FR_OK;
+    cudaSetDevice(b->dev->ordinal);
+    cudaStreamSynchronize(b->dev->stream);
+    delete b;
+    return FR_OK;
+}
+
+fr_status fr_batch_clear(fr_batch* b)
+{
+    FR_CHECK_NULL(b);
+    b->items.clear();
+    return FR_OK;
+}
+
+fr_status fr_batch_add_path(fr_batch* b, fr_tracer* t, fr_scene* sc, const fr_render_params* p,
+                            uint32_t first_sample, uint32_t n_render, uint32_t light_samples)
+{
+    FR_CHECK_NULL(b);
+    fr_status s = check_params(t, sc, p);
+    if (s != FR_OK)
+        return s;
+    if (t->dev != b->dev)
+        return fail(FR_ERR_INVALID, "the tracer belongs to another device than the batch");
+    if (light_samples == 0)
+        return fail(FR_ERR_INVALID, "light_samples must be positive");
+    if (first_sample == 0)
+        return fail(FR_ERR_INVALID, "sample numbers start at 1");
+    if (n_render == 0)
+        return FR_OK;
+    b->items.push_back({t, sc, *p, first_sample, n_render, light_samples});
+    return FR_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Grow a batch buffer; reports whether its address changed (the graph then has to be redone).
+template <class T> cudaError_t grow(DevArray<T>& a, size_t n, bool& moved)
+{
+    T* old = a.ptr;
+    cudaError_t e = a.reserve(n);
+    if (a.ptr != old)
+        moved = true;
+    return e;
+}
+
+}  // namespace
+
+extern "C" {
+
+fr_status fr_batch_render(fr_batch* b)
+{
+    FR_CHECK_NULL(b);
+    fr_status s = use_device(b->dev);
+    if (s != FR_OK)
+        return s;
+    fr_device* dev = b->dev;
+    if (b->items.empty())
+        return FR_OK;
+
+    // scenes: build what is stale (each scene once)
+    std::vector<fr_scene*> scenes;
+    for (auto& it : b->items)
+        if (std::find(scenes.begin(), scenes.end(), it.sc) == scenes.end())
+            scenes.push_back(it.sc);
+    for (size_t i = 0; i < scenes.size(); ++i) {
+        fr_tracer* owner = nullptr;
+        for (auto& it : b->items)
+            if (it.sc == scenes[i]) {
+                owner = it.tr;
+                break;
+            }
+        if ((s = prepare_scene(scenes[i], owner)) != FR_OK)
+            return s;
+    }
+
+    // path-state capacity: the device's wavefront size, at least one sample of the largest image
+    size_t cap = dev->path_slots;
+    for (auto& it : b->items)
+        cap = std::max(cap, size_t(it.tr->w) * it.tr->h);
+
+    // plan: every item's samples go to waves in sample order, at most one slice of a tracer
+    // per wave, K samples of all pixels per slice; first fit over the waves
+    struct Slice {
+        size_t item;
+        uint32_t first, k;
+    };
+    std::vector<std::vector<Slice>> waves;
+    std::vector<size_t> used;
+    std::vector<std::pair<const fr_tracer*, size_t>> last_wave;  // tracer -> next allowed wave
+    for (size_t i = 0; i < b->items.size(); ++i) {
+        const auto& it = b->items[i];
+        const size_t wh = size_t(it.tr->w) * it.tr->h;
+        size_t min_wave = 0;
+        for (auto& lw : last_wave)
+            if (lw.first == it.tr)
+                min_wave = lw.second;
+        uint32_t done = 0;
+        while (done < it.n) {
+            size_t w = min_wave;
+            while (w < waves.size() && cap - used[w] < wh)
+                ++w;
+            if (w == waves.size()) {
+                waves.emplace_back();
+                used.push_back(0);
+            }
+            size_t k = (cap - used[w]) / wh;
+            k = std::min<size_t>(k, 4096);
+            k = std::min<size_t>(k, it.n - done);
+            waves[w].push_back({i, it.first + done, uint32_t(k)});
+            used[w] += k * wh;
+            done += uint32_t(k);
+            min_wave = w + 1;
+        }
+        bool found = false;
+        for (auto& lw : last_wave)
+            if (lw.first == it.tr) {
+                lw.second = min_wave;
+                found = true;
+            }
+        if (!found)
+            last_wave.push_back({it.tr, min_wave});
+    }
+
+    // render table
+    std::vector<WaveJob> jobs;
+    std::vector<uint32_t> wave_first, wave_tiles, wave_pixels;
+    int width = 4;
+    uint32_t mask = 0;
+    for (auto& wv : waves) {
+        wave_first.push_back(uint32_t(jobs.size()));
+        uint64_t slot = 0, tile = 0, pixel = 0;
+        for (auto& sl : wv) {
+            const auto& it = b->items[sl.item];
+            WaveJob J;
+            std::memset(&J, 0, sizeof(J));
+            J.P = frame_params(it.tr, it.sc, &it.params, false, 1);
+            J.P.light_samples = it.light_samples;
+            J.P.n_samples = sl.first;
+            J.P.batch = sl.k;
+            if (J.P.bvh_width != 4)
+                width = 2;
+            mask |= J.P.type_mask;
+            const uint32_t tx = (it.tr->w + 15) / 16, ty = (it.tr->h + 15) / 16;
+            J.slot_base = uint32_t(slot);
+            J.tile_base = uint32_t(tile);
+            J.pixel_base = uint32_t(pixel);
+            J.tiles_x = tx;
+            J.tiles_per_sample = tx * ty;
+            slot += uint64_t(sl.k) * it.tr->w * it.tr->h;
+            tile += uint64_t(sl.k) * tx * ty;
+            pixel += uint64_t(it.tr->w) * it.tr->h;
+            if (slot > 0xFFFFFFFFull || tile > 0xFFFFFFFFull || pixel > 0xFFFFFFFFull)
+                return fail(FR_ERR_INVALID, "a batch wave exceeds 2^32 slots");
+            jobs.push_back(J);
+        }
+        wave_tiles.push_back(uint32_t(tile));
+        wave_pixels.push_back(uint32_t(pixel));
+    }
+    wave_first.push_back(uint32_t(jobs.size()));
+    if (mask == 0)
+        mask = MASK_SPHERES;  // empty scenes: every ray misses
+
+    bool moved = false;
+    FR_CUDA(grow(b->jobs, jobs.size(), moved), "allocating the batch plan");
+    FR_CUDA(grow(b->wave_first, wave_first.size(), moved), "allocating the batch plan");
+    FR_CUDA(grow(b->wave_tiles, wave_tiles.size(), moved), "allocating the batch plan");
+    FR_CUDA(grow(b->wave_pixels, wave_pixels.size(), moved), "allocating the batch plan");
+    FR_CUDA(grow(b->prim_o, cap, moved), "batch path state");
+    FR_CUDA(grow(b->prim_d, cap, moved), "batch path state");
+    FR_CUDA(grow(b->ray_o, cap, moved), "batch path state");
+    FR_CUDA(grow(b->ray_d, cap, moved), "batch path state");
+    FR_CUDA(grow(b->att, cap, moved), "batch path state");
+    FR_CUDA(grow(b->result, cap, moved), "batch path state");
+    FR_CUDA(grow(b->sample, cap, moved), "batch path state");
+    FR_CUDA(grow(b->prim_hit, cap, moved), "batch path state");
+    FR_CUDA(grow(b->ls_depth, cap, moved), "batch path state");
+    FR_CUDA(grow(b->hit, cap, moved), "batch path state");
+    FR_CUDA(grow(b->q0, cap, moved), "batch path state");
+    FR_CUDA(grow(b->q1, cap, moved), "batch path state");
+    FR_CUDA(grow(b->ctr, 4, moved), "batch path state");
+    b->slots = std::max(b->slots, cap);
+
+    cudaStream_t st = dev->stream;
+    FR_CUDA(cudaMemcpyAsync(b->jobs.ptr, jobs.data(), jobs.size() * sizeof(WaveJob),
+                            cudaMemcpyHostToDevice, st), "uploading the batch plan");
+    FR_CUDA(cudaMemcpyAsync(b->wave_first.ptr, wave_first.data(), wave_first.size() * 4,
+                            cudaMemcpyHostToDevice, st), "uploading the batch plan");
+    FR_CUDA(cudaMemcpyAsync(b->wave_tiles.ptr, wave_tiles.data(), wave_tiles.size() * 4,
+                            cudaMemcpyHostToDevice, st), "uploading the batch plan");
+    FR_CUDA(cudaMemcpyAsync(b->wave_pixels.ptr, wave_pixels.data(), wave_pixels.size() * 4,
+                            cudaMemcpyHostToDevice, st), "uploading the batch plan");
+    std::memset(b->h_ctl, 0, sizeof(BatchCtl));
+    b->h_ctl->n_waves = uint32_t(waves.size());
+    FR_CUDA(cudaMemcpyAsync(b->ctl.ptr, b->h_ctl, sizeof(BatchCtl), cudaMemcpyHostToDevice, st),
+            "uploading the batch plan");
+
+    if (b->exec && (moved || b->exec_width != width || b->exec_mask != mask)) {
+        cudaGraphExecDestroy(b->exec);
+        b->exec = nullptr;
+    }
+    if (!b->exec) {
+        BatchDev B;
+        B.jobs = b->jobs.ptr;
+        B.wave_first = b->wave_first.ptr;
+        B.wave_tiles = b->wave_tiles.ptr;
+        B.wave_pixels = b->wave_pixels.ptr;
+        B.ctl = b->ctl.ptr;
+        B.S.prim_o = b->prim_o.ptr;
+        B.S.prim_d = b->prim_d.ptr;
+        B.S.prim_hit = b->prim_hit.ptr;
+        B.S.ray_o = b->ray_o.ptr;
+        B.S.ray_d = b->ray_d.ptr;
+        B.S.att = b->att.ptr;
+        B.S.result = b->result.ptr;
+        B.S.ls_depth = b->ls_depth.ptr;
+        B.S.hit = b->hit.ptr;
+        B.S.sample = b->sample.ptr;
+        B.S.queue[0] = b->q0.ptr;
+        B.S.queue[1] = b->q1.ptr;
+        B.S.ctr = b->ctr.ptr;
+        FR_CUDA(batch_graph_create(B, width, mask, dev->num_sms, b->capture, &b->exec),
+                "capturing the batch graph");
+        b->exec_width = width;
+        b->exec_mask = mask;
+        b->stats.graph_captures++;
+    }
+    cudaEvent_t e0, e1;
+    FR_CUDA(cudaEventCreate(&e0), "batch timing");
+    FR_CUDA(cudaEventCreate(&e1), "batch timing");
+    cudaEventRecord(e0, st);
+    cudaError_t le = cudaGraphLaunch(b->exec, st);
+    cudaEventRecord(e1, st);
+    if (le == cudaSuccess)
+        le = cudaMemcpyAsync(b->h_ctl, b->ctl.ptr, sizeof(BatchCtl), cudaMemcpyDeviceToHost, st);
+    if (le == cudaSuccess)
+        le = cudaStreamSynchronize(st);
+    float ms = 0.0f;
+    if (le == cudaSuccess)
+        cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (le != cudaSuccess)
+        return cuda_fail(le, "running the batch graph");
+
+    const BatchCtl& c = *b->h_ctl;
+    b->stats.renders += uint32_t(b->items.size());
+    b->stats.waves += uint32_t(waves.size());
+    b->stats.graph_launches += 1;
+    b->stats.shade_extend_pairs += c.pairs;
+    // per wave: begin, primary, fold, end; per pass: 2 shade, 2 extend, 1 condition; 1 start
+    b->stats.kernel_launches += 1 + 4 * uint64_t(waves.size()) + 5 * c.pairs;
+    b->stats.box_tests += c.box_tests;
+    b->stats.prim_tests += c.prim_tests;
+    b->stats.last_ms = ms;
+    b->stats.total_ms += ms;
+    if (c.error)
+        return fail(FR_ERR_DEVICE_LIMIT, "batched path tracer exceeded the bounce iteration cap");
+    return check_status(dev);
+}
+
+fr_status fr_batch_get_stats(const fr_batch* b, fr_batch_stats* out)
+{
+    FR_CHECK_NULL(b);
+    FR_CHECK_NULL(out);
+    *out = b->stats;
     return FR_OK;
 }
 

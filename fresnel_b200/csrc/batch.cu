@@ -1,0 +1,374 @@
+// batch.cu -- kernels and CUDA graph of the batched path tracer (see batch.hpp).
+//
+// The per-slot work is the single-render path tracer's (path_device.cuh: shade_pixel, welford,
+// write_pixel; engine.cuh: trace_closest), so a render gives the same image alone or in a
+// batch. What changes is how a thread finds its render: primary tiles, queued slots and fold
+// pixels carry indices into the current wave, and a binary search over the wave's render table
+// maps them to the render (its scene, camera, lights, outputs and sample numbers).
+#include "batch.hpp"
+#include "path_device.cuh"
+
+namespace fr {
+
+namespace {
+
+// The render of [lo, hi) whose base (member M) is the largest one <= key (bases ascend and
+// jobs[lo].*M <= key).
+template <uint32_t WaveJob::*M>
+__device__ __forceinline__ uint32_t find_job(const WaveJob* jobs, uint32_t lo, uint32_t hi,
+                                             uint32_t key)
+{
+    while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (jobs[mid].*M <= key)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__global__ void k_batch_start(BatchCtl* ctl, cudaGraphConditionalHandle outer)
+{
+    ctl->wave = 0;
+    ctl->inner = 0;
+    ctl->error = 0;
+    ctl->pairs = 0;
+    ctl->box_tests = 0;
+    ctl->prim_tests = 0;
+    cudaGraphSetConditional(outer, ctl->n_waves > 0u ? 1u : 0u);
+}
+
+__global__ void k_wave_begin(BatchDev B, cudaGraphConditionalHandle inner)
+{
+    B.S.ctr[0] = 0;
+    B.S.ctr[1] = 0;
+    B.S.ctr[2] = 0;
+    B.S.ctr[3] = 0;
+    B.ctl->inner = 0;
+    cudaGraphSetConditional(inner, 1u);
+}
+
+// Primary rays of the wave: 16x16 tiles of every render and sample, grid-stride over tiles.
+// Same per-pixel work as k_path_primary.
+template <int WIDTH, uint32_t MASK>
+__global__ void __launch_bounds__(256) k_batch_primary(BatchDev B)
+{
+    const PathState& S = B.S;
+    const uint32_t w = B.ctl->wave;
+    const uint32_t f0 = B.wave_first[w], f1 = B.wave_first[w + 1];
+    const uint32_t n_tiles = B.wave_tiles[w];
+    const uint32_t lane = (threadIdx.x + threadIdx.y * blockDim.x) & 31u;
+    TraceCount tc;
+    for (uint32_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+        const WaveJob& J = B.jobs[find_job<&WaveJob::tile_base>(B.jobs, f0, f1, t)];
+        const FrameParams& P = J.P;
+        const uint32_t lt = t - J.tile_base;
+        const uint32_t k = lt / J.tiles_per_sample;
+        const uint32_t r = lt - k * J.tiles_per_sample;
+        const uint32_t ty = r / J.tiles_x;
+        const uint32_t tx = r - ty * J.tiles_x;
+        const uint32_t i = tx * 16u + threadIdx.x;
+        const uint32_t j = ty * 16u + threadIdx.y;
+        const bool valid = (i < P.w) && (j < P.h);
+        bool push = false;
+        uint32_t slot = 0;
+        if (valid) {
+            const uint32_t p = j * P.w + i;
+            slot = J.slot_base + k * P.w * P.h + p;
+            V3 o, d;
+            camera_ray(P.cam, i, j, P.n_samples + k, o, d);
+            Hit h = trace_closest<WIDTH, MASK>(P.scene, o, d, PATH_TNEAR, tc);
+            S.prim_hit[slot] = make_uint2(h.geom, h.prim);
+            if (h.geom == MISS) {
+                C3 res = P.bg * float(P.light_samples);
+                C3 out = c_div_recip(res, float(P.light_samples));
+                S.sample[slot] = make_float4(out.r, out.g, out.b, P.bg_alpha);
+            } else {
+                S.prim_o[slot] = f4(o);
+                S.prim_d[slot] = f4(d);
+                S.ls_depth[slot] = make_uint2(0u, 0u);
+                S.att[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+                S.result[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                push = true;
+            }
+        }
+        const uint32_t m = __ballot_sync(0xffffffffu, push);
+        if (m) {
+            uint32_t at = 0;
+            if (lane == 0)
+                at = atomicAdd(S.ctr + 1, uint32_t(__popc(m)));
+            at = __shfl_sync(0xffffffffu, at, 0);
+            if (push)
+                S.queue[1][at + __popc(m & ((1u << lane) - 1u))] = slot;
+        }
+        // a warp covers two rows of one tile, so all its lanes belong to render J
+        const uint32_t mv = __ballot_sync(0xffffffffu, valid);
+        if (lane == 0 && mv) {
+            atomicAdd(P.stats + 0, (unsigned long long)__popc(mv));
+            atomicAdd(P.stats + 1, (unsigned long long)__popc(mv) * P.light_samples);
+        }
+    }
+    flush_counts(tc, &B.ctl->box_tests);
+}
+
+__global__ void __launch_bounds__(256) k_batch_shade(BatchDev B, int in_q, int out_q)
+{
+    const PathState& S = B.S;
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        S.ctr[2] = 0;  // work counter of the extend kernel that follows
+    const uint32_t w = B.ctl->wave;
+    const uint32_t f0 = B.wave_first[w], f1 = B.wave_first[w + 1];
+    const uint32_t count = S.ctr[in_q];
+    const uint32_t* inq = S.queue[in_q];
+    uint32_t* outq = S.queue[out_q];
+    uint32_t* outc = S.ctr + out_q;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t base = warp * 32u; base < count; base += n_warps * 32u) {
+        const uint32_t idx = base + lane;
+        bool push = false;
+        uint32_t p = 0;
+        if (idx < count) {
+            p = inq[idx];
+            const WaveJob& J = B.jobs[find_job<&WaveJob::slot_base>(B.jobs, f0, f1, p)];
+            push = shade_pixel(J.P, S, p, p - J.slot_base);
+        }
+        const uint32_t m = __ballot_sync(0xffffffffu, push);
+        if (m) {
+            uint32_t at = 0;
+            if (lane == 0)
+                at = atomicAdd(outc, uint32_t(__popc(m)));
+            at = __shfl_sync(0xffffffffu, at, 0);
+            if (push)
+                outq[at + __popc(m & ((1u << lane) - 1u))] = p;
+        }
+    }
+}
+
+template <int WIDTH, uint32_t MASK>
+__global__ void __launch_bounds__(256) k_batch_extend(BatchDev B, int q)
+{
+    const PathState& S = B.S;
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        S.ctr[q ^ 1] = 0;  // the other queue was consumed by the shade pass that produced q
+    const uint32_t w = B.ctl->wave;
+    const uint32_t f0 = B.wave_first[w], f1 = B.wave_first[w + 1];
+    const uint32_t count = S.ctr[q];
+    const uint32_t* queue = S.queue[q];
+    const uint32_t lane = threadIdx.x & 31u;
+    TraceCount tc;
+    while (true) {
+        uint32_t base = 0;
+        if (lane == 0)
+            base = atomicAdd(S.ctr + 2, 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= count)
+            break;
+        const uint32_t idx = base + lane;
+        const bool act = idx < count;
+        uint32_t jb = 0;
+        if (act) {
+            const uint32_t p = queue[idx];
+            jb = find_job<&WaveJob::slot_base>(B.jobs, f0, f1, p);
+            const V3 o = xyz(S.ray_o[p]);
+            const V3 d = xyz(S.ray_d[p]);
+            Hit h = trace_closest<WIDTH, MASK>(B.jobs[jb].P.scene, o, d, PATH_TNEAR, tc);
+            S.hit[p] = make_uint2(h.geom, h.prim);
+        }
+        // rays per render, one atomic per render present in the warp
+        const uint32_t am = __ballot_sync(0xffffffffu, act);
+        if (act) {
+            const uint32_t same = __match_any_sync(am, jb);
+            if (lane == uint32_t(__ffs(same) - 1))
+                atomicAdd(B.jobs[jb].P.stats + 0, (unsigned long long)__popc(same));
+        }
+    }
+    flush_counts(tc, &B.ctl->box_tests);
+}
+
+__global__ void k_inner_cond(BatchDev B, cudaGraphConditionalHandle inner)
+{
+    BatchCtl* c = B.ctl;
+    c->inner += 1u;
+    c->pairs += 1u;
+    bool more = B.S.ctr[1] != 0u;
+    if (more && c->inner >= BATCH_MAX_PAIRS) {
+        c->error = 1u;
+        more = false;
+    }
+    cudaGraphSetConditional(inner, more ? 1u : 0u);
+}
+
+// Fold each render's samples of the wave into its running mean, in sample order (k_path_fold).
+__global__ void __launch_bounds__(256) k_batch_fold(BatchDev B)
+{
+    const PathState& S = B.S;
+    const uint32_t w = B.ctl->wave;
+    const uint32_t f0 = B.wave_first[w], f1 = B.wave_first[w + 1];
+    const uint32_t n = B.wave_pixels[w];
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const WaveJob& J = B.jobs[find_job<&WaveJob::pixel_base>(B.jobs, f0, f1, q)];
+        const FrameParams& P = J.P;
+        const uint32_t lp = q - J.pixel_base;
+        const uint32_t wh = P.w * P.h;
+        float4 mean = P.linear[lp];
+        for (uint32_t k = 0; k < P.batch; ++k)
+            mean = welford(P, mean, S.sample[size_t(J.slot_base) + size_t(k) * wh + lp],
+                           P.n_samples + k);
+        write_pixel(P, lp, mean.x, mean.y, mean.z, mean.w);
+    }
+}
+
+__global__ void k_wave_end(BatchDev B, cudaGraphConditionalHandle outer)
+{
+    BatchCtl* c = B.ctl;
+    c->wave += 1u;
+    cudaGraphSetConditional(outer, (c->wave < c->n_waves && c->error == 0u) ? 1u : 0u);
+}
+
+template <class K> int grid_for(K kernel, int num_sms, int threads)
+{
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, 0);
+    return num_sms * (n > 0 ? n : 1);
+}
+
+template <int WIDTH, uint32_t MASK> struct Kernels {
+    static void primary(const BatchDev& B, int grid, cudaStream_t s)
+    {
+        k_batch_primary<WIDTH, MASK><<<grid, dim3(16, 16), 0, s>>>(B);
+    }
+    static void extend(const BatchDev& B, int q, int grid, cudaStream_t s)
+    {
+        k_batch_extend<WIDTH, MASK><<<grid, 256, 0, s>>>(B, q);
+    }
+    static int primary_grid(int sms) { return grid_for(k_batch_primary<WIDTH, MASK>, sms, 256); }
+    static int extend_grid(int sms) { return grid_for(k_batch_extend<WIDTH, MASK>, sms, 256); }
+};
+
+// Appends a `while` node after the capture's current leaves and returns its body graph.
+cudaError_t add_while(cudaStream_t s, cudaGraphConditionalHandle h, cudaGraph_t* body)
+{
+    cudaStreamCaptureStatus status;
+    cudaGraph_t graph = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t n_deps = 0;
+    cudaError_t e = cudaStreamGetCaptureInfo(s, &status, nullptr, &graph, &deps, &n_deps);
+    if (e != cudaSuccess)
+        return e;
+    if (status != cudaStreamCaptureStatusActive)
+        return cudaErrorStreamCaptureInvalidated;
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    if ((e = cudaGraphAddNode(&node, graph, deps, n_deps, &cp)) != cudaSuccess)
+        return e;
+    *body = cp.conditional.phGraph_out[0];
+    return cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
+}
+
+cudaGraph_t capturing_graph(cudaStream_t s)
+{
+    cudaStreamCaptureStatus status;
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamGetCaptureInfo(s, &status, nullptr, &graph, nullptr, nullptr) != cudaSuccess)
+        return nullptr;
+    return graph;
+}
+
+template <int WIDTH, uint32_t MASK>
+cudaError_t capture(const BatchDev& B, int num_sms, cudaStream_t s0, cudaGraphExec_t* exec)
+{
+    using KS = Kernels<WIDTH, MASK>;
+    const int g_primary = KS::primary_grid(num_sms);
+    const int g_extend = KS::extend_grid(num_sms);
+    const int g_shade = grid_for(k_batch_shade, num_sms, 256);
+    const int g_fold = num_sms * 8;
+
+    cudaStream_t s1 = nullptr, s2 = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&s1, cudaStreamNonBlocking);
+    if (e == cudaSuccess)
+        e = cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking);
+    cudaGraph_t top = nullptr;
+    bool c0 = false, c1 = false, c2 = false;
+    auto keep = [&](cudaError_t x) {
+        if (e == cudaSuccess)
+            e = x;
+        return e == cudaSuccess;
+    };
+    if (e == cudaSuccess && keep(cudaStreamBeginCapture(s0, cudaStreamCaptureModeRelaxed))) {
+        c0 = true;
+        cudaGraph_t g = capturing_graph(s0);
+        cudaGraphConditionalHandle h_outer;
+        cudaGraph_t outer_body = nullptr;
+        if (keep(g ? cudaGraphConditionalHandleCreate(&h_outer, g, 0, 0) : cudaErrorUnknown)) {
+            k_batch_start<<<1, 1, 0, s0>>>(B.ctl, h_outer);
+            if (keep(cudaGetLastError()) && keep(add_while(s0, h_outer, &outer_body))) {
+                cudaGraphConditionalHandle h_inner;
+                cudaGraph_t inner_body = nullptr;
+                if (keep(cudaGraphConditionalHandleCreate(&h_inner, outer_body, 0, 0)) &&
+                    keep(cudaStreamBeginCaptureToGraph(s1, outer_body, nullptr, nullptr, 0,
+                                                       cudaStreamCaptureModeRelaxed))) {
+                    c1 = true;
+                    k_wave_begin<<<1, 1, 0, s1>>>(B, h_inner);
+                    KS::primary(B, g_primary, s1);
+                    if (keep(cudaGetLastError()) && keep(add_while(s1, h_inner, &inner_body)) &&
+                        keep(cudaStreamBeginCaptureToGraph(s2, inner_body, nullptr, nullptr, 0,
+                                                           cudaStreamCaptureModeRelaxed))) {
+                        c2 = true;
+                        // two iterations per pass: queue 1 -> 0, then 0 -> 1 (the primary
+                        // kernel fills queue 1)
+                        k_batch_shade<<<g_shade, 256, 0, s2>>>(B, 1, 0);
+                        KS::extend(B, 0, g_extend, s2);
+                        k_batch_shade<<<g_shade, 256, 0, s2>>>(B, 0, 1);
+                        KS::extend(B, 1, g_extend, s2);
+                        k_inner_cond<<<1, 1, 0, s2>>>(B, h_inner);
+                        keep(cudaGetLastError());
+                    }
+                    if (c2) {
+                        keep(cudaStreamEndCapture(s2, &inner_body));
+                        c2 = false;
+                    }
+                    k_batch_fold<<<g_fold, 256, 0, s1>>>(B);
+                    k_wave_end<<<1, 1, 0, s1>>>(B, h_outer);
+                    keep(cudaGetLastError());
+                }
+                if (c1) {
+                    keep(cudaStreamEndCapture(s1, &outer_body));
+                    c1 = false;
+                }
+            }
+        }
+    }
+    if (c0)
+        keep(cudaStreamEndCapture(s0, &top));
+    if (e == cudaSuccess)
+        e = cudaGraphInstantiate(exec, top, 0);
+    if (top)
+        cudaGraphDestroy(top);
+    if (s1)
+        cudaStreamDestroy(s1);
+    if (s2)
+        cudaStreamDestroy(s2);
+    return e;
+}
+
+}  // namespace
+
+cudaError_t batch_graph_create(const BatchDev& B, int width, uint32_t type_mask, int num_sms,
+                               cudaStream_t capture_stream, cudaGraphExec_t* exec)
+{
+    const bool spheres_only = (type_mask & ~MASK_SPHERES) == 0u;
+    if (width == 4)
+        return spheres_only ? capture<4, MASK_SPHERES>(B, num_sms, capture_stream, exec)
+                            : capture<4, MASK_ALL>(B, num_sms, capture_stream, exec);
+    return spheres_only ? capture<2, MASK_SPHERES>(B, num_sms, capture_stream, exec)
+                        : capture<2, MASK_ALL>(B, num_sms, capture_stream, exec);
+}
+
+}  // namespace fr

@@ -557,6 +557,75 @@ struct TracerPathH : TracerH {
     }
 };
 
+// Batched path renders (fr_batch_*): add() queues Path renders of any tracers and scenes of the
+// device; render() traces them together and then advances each tracer's sample count.
+struct BatchH {
+    std::shared_ptr<DeviceH> device;
+    fr_batch* batch = nullptr;
+    struct Item {
+        std::shared_ptr<TracerPathH> tracer;
+        std::shared_ptr<SceneH> scene;
+        unsigned k;
+    };
+    std::vector<Item> items;
+    explicit BatchH(std::shared_ptr<DeviceH> d) : device(std::move(d))
+    {
+        check(fr_batch_create(device->dev, &batch));
+    }
+    ~BatchH() { fr_batch_destroy(batch); }
+    // k more samples of `t` on `s`, numbered after the ones already queued for t
+    void add(std::shared_ptr<TracerPathH> t, std::shared_ptr<SceneH> s, unsigned k)
+    {
+        t->check_scene(s);
+        if (t->device != device)
+            throw std::runtime_error("Tracer and Batch devices do not match");
+        if (k == 0)
+            return;
+        unsigned queued = 0;
+        for (auto& it : items)
+            if (it.tracer == t)
+                queued += it.k;
+        s->sync();
+        fr_render_params p = t->params(*s);
+        check(fr_batch_add_path(batch, t->tracer, s->scene, &p, t->n_samples + queued + 1, k,
+                                t->light_samples));
+        items.push_back({t, s, k});
+    }
+    void render()
+    {
+        for (auto& it : items)
+            it.scene->sync();
+        fr_status st = fr_batch_render(batch);
+        if (st == FR_OK)
+            for (auto& it : items)
+                it.tracer->n_samples += it.k;
+        clear();
+        check(st);
+    }
+    void clear()
+    {
+        items.clear();
+        check(fr_batch_clear(batch));
+    }
+    py::dict stats() const
+    {
+        fr_batch_stats st;
+        check(fr_batch_get_stats(batch, &st));
+        py::dict d;
+        d["renders"] = st.renders;
+        d["waves"] = st.waves;
+        d["graph_launches"] = st.graph_launches;
+        d["graph_captures"] = st.graph_captures;
+        d["kernel_launches"] = st.kernel_launches;
+        d["shade_extend_pairs"] = st.shade_extend_pairs;
+        d["box_tests"] = st.box_tests;
+        d["prim_tests"] = st.prim_tests;
+        d["last_ms"] = st.last_ms;
+        d["total_ms"] = st.total_ms;
+        return d;
+    }
+};
+
 template <class A> void export_array(py::module_& m, const char* name)
 {
     py::class_<A, std::shared_ptr<A>>(m, name, py::buffer_protocol())
@@ -696,6 +765,14 @@ PYBIND11_MODULE(_gpu, m)
             check(fr_tracer_read_primary_hits(t.tracer, out.mutable_data(), size_t(t.w) * t.h * 8));
             return out;
         });
+
+    py::class_<BatchH, std::shared_ptr<BatchH>>(m, "Batch")
+        .def(py::init<std::shared_ptr<DeviceH>>())
+        .def("add", &BatchH::add)
+        .def("render", &BatchH::render)
+        .def("clear", &BatchH::clear)
+        .def("getStats", &BatchH::stats)
+        .def("__len__", [](const BatchH& b) { return b.items.size(); });
 
     export_array<ArrayRGBAf>(m, "ArrayRGBAf");
     export_array<ArrayRGBAc>(m, "ArrayRGBAc");

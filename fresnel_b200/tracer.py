@@ -113,3 +113,54 @@ class Path(Tracer):
             # keep later render() calls at one light sample (fresnel/tracer.py:257-259)
             self._tracer.setLightSamples(1)
         return self.output
+
+
+class PathBatch:
+    """Path renders of many tracers and scenes traced together (no counterpart in fresnel).
+
+    ``add(tracer, scene, samples, reset=True, light_samples=1)`` queues what
+    ``tracer.sample(scene, samples, reset, light_samples)`` renders; ``render()`` traces every
+    queued render in one CUDA graph launch. The renders share wavefronts, so many small frames
+    keep the GPU as busy as one large frame. Afterwards each tracer holds the image its own
+    ``sample`` call would have produced. Tracers and scenes can differ in size and content but
+    must belong to the batch's device.
+    """
+
+    def __init__(self, device):
+        self.device = device
+        self._batch = device.module.Batch(device._device)
+        self._queued = []
+
+    def add(self, tracer, scene, samples, reset=True, light_samples=1):
+        if tracer.device is not self.device or scene.device is not self.device:
+            raise RuntimeError("Tracer, Scene and PathBatch devices do not match")
+        if reset:
+            if any(t is tracer for t in self._queued):
+                raise RuntimeError("cannot reset a tracer that already has queued renders")
+            tracer.reset()
+        tracer._tracer.setLightSamples(light_samples)
+        try:
+            self._batch.add(tracer._tracer, scene._scene, samples)
+        finally:
+            tracer._tracer.setLightSamples(1)
+        self._queued.append(tracer)
+
+    def render(self):
+        """Trace everything queued; the queue is empty afterwards."""
+        try:
+            self._batch.render()
+        finally:
+            self._queued = []
+
+    def clear(self):
+        self._batch.clear()
+        self._queued = []
+
+    def __len__(self):
+        return len(self._batch)
+
+    @property
+    def stats(self):
+        """Counters over the batch's lifetime: renders, waves, graph launches and captures,
+        kernels run inside the graphs, device-side loop passes, traversal tests, device ms."""
+        return self._batch.getStats()

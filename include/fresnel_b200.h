@@ -277,6 +277,37 @@ FR_API fr_status fr_tracer_render_path_static(fr_tracer* tr, fr_scene* scene,
                                               const fr_render_params* params, uint32_t first_sample,
                                               uint32_t n_render, uint32_t light_samples);
 
+/* ---------------- batched path renders ----------------
+ * No counterpart in the reference, which renders one Tracer.Path call at a time.  A batch
+ * queues path renders of any tracers, scenes and image sizes on one device and traces them
+ * together: their pixel samples share wavefronts and kernel launches, and the whole batch is
+ * one CUDA graph launch (device-side loops over waves and bounces, no host round trips).  Each
+ * render's output equals what fr_tracer_render_path gives for the same arguments.  Renders of
+ * one tracer are traced in the order they were added.  Tracers and scenes must stay alive until
+ * fr_batch_render returns; fr_batch_render keeps the queue (fr_batch_clear empties it). */
+typedef struct fr_batch fr_batch;
+typedef struct fr_batch_stats {
+    uint32_t renders;             /* renders traced */
+    uint32_t waves;               /* wavefronts (renders that fit the path state together) */
+    uint64_t graph_launches;
+    uint64_t graph_captures;
+    uint64_t kernel_launches;     /* kernels executed inside the graphs */
+    uint64_t shade_extend_pairs;  /* device-side loop passes (two bounces each) */
+    uint64_t box_tests, prim_tests;
+    float last_ms;                /* device time of the last fr_batch_render */
+    double total_ms;
+} fr_batch_stats;
+FR_API fr_status fr_batch_create(fr_device* dev, fr_batch** out);
+FR_API fr_status fr_batch_destroy(fr_batch* batch);
+/* Queue n_render TracerPath::render calls of tr on scene (as fr_tracer_render_path). */
+FR_API fr_status fr_batch_add_path(fr_batch* batch, fr_tracer* tr, fr_scene* scene,
+                                   const fr_render_params* params, uint32_t first_sample,
+                                   uint32_t n_render, uint32_t light_samples);
+FR_API fr_status fr_batch_clear(fr_batch* batch);
+/* Build stale scenes, then trace every queued render. */
+FR_API fr_status fr_batch_render(fr_batch* batch);
+FR_API fr_status fr_batch_get_stats(const fr_batch* batch, fr_batch_stats* out);
+
 /* ---------------- self-tests ---------------- */
 
 /* Diagnostic (no counterpart in the reference): trace n rays (o.xyz, d.xyz, 6 floats each,
