@@ -71,6 +71,7 @@ WORKLOADS = {
     "c1": Workload("c1", "config1: 1000 spheres r=0.5, box 20, outline 0.1, cloudy, {w}x{h}, "
                    "{spp} spp x 32 light samples", "config1", 580, 580, spp=64, light_samples=32,
                    box_tests=37.41, prim_tests=1.81),
+    "c4": Workload("c4", "config4", "config4", 1024, 1024, spp=16),
     "c3": Workload("c3", "config3: 200k spheres + 50k bonds + 20k cubes + 10k icosahedra, "
                    "{w}x{h}, {spp} spp, 1 light sample", "config3", 1280, 720, spp=128,
                    box_tests=43.51, prim_tests=1.86, prim_bytes=28),
@@ -197,7 +198,11 @@ def cpu_baseline(wl, kind, seconds):
     import fresnel_b200 as fresnel  # noqa: F401
     from oracle import cpu_module
     dev = cpu_module.make_device(kind)
-    scene = wl.build(dev)
+    built = wl.build(dev)
+    if isinstance(built, list):  # a frame set: time its first frame
+        scene, fw, fh = built[0]
+    else:
+        scene, fw, fh = built, wl.w, wl.h
     t0 = time.perf_counter()
     scene._scene.handle()  # BVH build, not timed
     build_s = time.perf_counter() - t0
@@ -219,12 +224,12 @@ def cpu_baseline(wl, kind, seconds):
                   f"{total_rays} closest-hit queries in {elapsed:.1f} s "
                   f"(BVH build {build_s:.1f} s, not timed)")
     else:
-        tracer = dev.module.TracerPath(dev._device, wl.w, wl.h, wl.light_samples)
+        tracer = dev.module.TracerPath(dev._device, fw, fh, wl.light_samples)
         tracer.setSeed(2)
         rng = numpy.random.default_rng(0)
         n_pix = 1024
         while elapsed < seconds and rounds < 1000:
-            pixels = numpy.sort(rng.choice(wl.w * wl.h, min(n_pix, wl.w * wl.h),
+            pixels = numpy.sort(rng.choice(fw * fh, min(n_pix, fw * fh),
                                            replace=False)).astype(numpy.uint32)
             tracer.stats = cpu_module.OrStats()
             t0 = time.perf_counter()
@@ -235,8 +240,8 @@ def cpu_baseline(wl, kind, seconds):
             if rounds == 1:
                 # scale the batch so that one round takes about a second
                 per_pix = elapsed / len(pixels)
-                n_pix = int(min(wl.w * wl.h, max(256, 1.0 / max(per_pix, 1e-9))))
-        sample = (f"{rounds} rounds of random pixels of the {wl.w}x{wl.h} frame, 1 sample each "
+                n_pix = int(min(fw * fh, max(256, 1.0 / max(per_pix, 1e-9))))
+        sample = (f"{rounds} rounds of random pixels of the {fw}x{fh} frame, 1 sample each "
                   f"x {wl.light_samples} light samples, {total_rays} closest-hit queries in "
                   f"{elapsed:.1f} s (BVH build {build_s:.1f} s, not timed)")
     return {"value": total_rays / elapsed / 1e6, "unit": "Mrays/s", "cores": os.cpu_count(),
@@ -290,6 +295,127 @@ def host_arrays(scene):
     return out
 
 
+def run_batch_bench(args, world, rank, barrier_max, barrier_sum, clock_index):
+    """Trajectory frame set (64 scenes of 1e4-5e5 spheres, 512^2-1024^2, 16 spp): the frames
+    traced as one PathBatch (one CUDA graph launch) against 64 sequential plain Path.sample
+    calls. Both produce identical images (checked), so the comparison is at equal error."""
+    import numpy
+
+    import fresnel_b200 as fresnel
+    from fresnel_b200 import workloads
+    spp = args.spp or 16
+    device = fresnel.Device(mode="gpu", n=1)
+    dd = device._device
+    frames = workloads.config4(device)
+    for s, _, _ in frames:
+        s._scene.build()
+    plain = [fresnel.tracer.Path(device, w=w, h=h) for _, w, h in frames]
+    batched = [fresnel.tracer.Path(device, w=w, h=h) for _, w, h in frames]
+    for f in range(len(frames)):
+        plain[f].seed = 1000 * rank + f
+        batched[f].seed = 1000 * rank + f
+    batch = fresnel.tracer.PathBatch(device)
+
+    def run_plain():
+        for (s, _, _), t in zip(frames, plain):
+            t.sample(s, samples=spp)
+
+    def run_batch():
+        for (s, _, _), t in zip(frames, batched):
+            batch.add(t, s, samples=spp)
+        batch.render()
+
+    def timed(fn, tracers):
+        for t in tracers:
+            t._tracer.resetStats()
+        dd.synchronize()
+        dd.timerStart()
+        for _ in range(args.steps):
+            fn()
+        ms = dd.timerStop()
+        return ms, float(sum(t._tracer.getStats()["rays"] for t in tracers))
+
+    for _ in range(args.warmup):
+        run_plain()
+        run_batch()
+    ms_plain, rays_plain = timed(run_plain, plain)
+    launches0 = batch.stats["kernel_launches"]
+    with ClockSampler(clock_index) as clk:
+        ms_batch, rays_batch = timed(run_batch, batched)
+    launches = batch.stats["kernel_launches"] - launches0
+    diff = max(float(numpy.abs(numpy.asarray(a.linear_output[:]) -
+                               numpy.asarray(b.linear_output[:])).max())
+               for a, b in zip(plain, batched))
+
+    # end to end: every frame's arrays written from host memory (BVH rebuilt), traced, and its
+    # sRGB image read back
+    arrays = [host_arrays(s) for s, _, _ in frames]
+
+    def e2e(fn, tracers):
+        out_bytes = 0
+        t0 = time.perf_counter()
+        for arr in arrays:
+            for a, host in arr:
+                a[:] = host
+        fn()
+        for t in tracers:
+            out_bytes += t.output[:].nbytes
+        return (time.perf_counter() - t0) * 1e3, out_bytes
+
+    e2e_plain = [e2e(run_plain, plain)[0] for _ in range(args.steps)]
+    e2e_batch = []
+    out_bytes = 0
+    for _ in range(args.steps):
+        ms, out_bytes = e2e(run_batch, batched)
+        e2e_batch.append(ms)
+    in_bytes = sum(h.nbytes for arr in arrays for _, h in arr)
+
+    ms_plain = barrier_max(ms_plain)
+    ms_batch = barrier_max(ms_batch)
+    value = barrier_sum(rays_batch) / (ms_batch / 1e3) / 1e6
+    value_plain = barrier_sum(rays_plain) / (ms_plain / 1e3) / 1e6
+    e2e_b = barrier_max(statistics.mean(e2e_batch))
+    e2e_p = barrier_max(statistics.mean(e2e_plain))
+    rays_frame_set = rays_batch / args.steps
+    hbm, peak_kind = peaks()
+    bpr = WORKLOADS["c2"].bytes_per_ray
+    achieved = rays_batch * bpr / (ms_batch / 1e3) / 1e9
+    if rank == 0:
+        line = {
+            "metric": "Mrays/s (c4: 64-frame set, batched)", "value": value, "unit": "Mrays/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_batch / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": f"config4: 64 frames, 1e4-5e5 spheres at the 1M-sphere "
+                                   f"scene's density, 512^2/768^2/1024^2, {spp} spp, 1 light "
+                                   "sample; one PathBatch vs 64 sequential Path.sample calls",
+                       "frames": len(frames), "spp": spp,
+                       "spheres": int(sum(len(s.geometry[0].position[:]) for s, _, _ in frames)),
+                       "pixels": int(sum(w * h for _, w, h in frames)),
+                       "parallelism": f"replicas{world}",
+                       "l2": "inputs larger than L2 (64 scenes, 2.4 GB path state)"},
+            "plain": {"value": value_plain, "ms_per_step": ms_plain / args.steps,
+                      "e2e_ms_per_step": e2e_p},
+            "batched_over_plain": value / value_plain,
+            "e2e_batched_over_plain": e2e_p / e2e_b,
+            "max_abs_image_difference": diff,
+            "rays_per_frame_set": rays_frame_set,
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": None, "peak_source": peak_kind,
+                         "kernel": "whole batch graph (all kernels)",
+                         "bytes_per_ray": bpr},
+            "clocks": clk.summary(),
+            "e2e": {"value": barrier_sum(rays_frame_set) / (e2e_b / 1e3) / 1e6,
+                    "unit": "Mrays/s", "h2d_bytes_per_step": int(in_bytes),
+                    "d2h_bytes_per_step": int(out_bytes), "ms_per_step": e2e_b},
+            "batch_stats": batch.stats,
+            "cpu_baseline": None,
+        }
+        print(json.dumps(line))
+    return 0
+
+
 def main():
     args, wl = parse()
     world, rank, local = dist_init()
@@ -322,6 +448,14 @@ def main():
         t = torch.tensor([x], dtype=torch.float64, device="cuda")
         pg.all_reduce(t, op=pg.ReduceOp.SUM)
         return float(t.item())
+
+    if wl.key == "c4":
+        rc = run_batch_bench(args, world, rank, barrier_max, barrier_sum,
+                             int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0))
+        if pg is not None:
+            pg.barrier()
+            pg.destroy_process_group()
+        return rc
 
     device = fresnel.Device(mode="gpu", n=1)
     scene = wl.build(device)

@@ -82,6 +82,66 @@ fr_material default_material(float r, float g, float b, float solid)
 
 }  // namespace
 
+// Wavefront state of the path tracer (PathState's arrays), grown on demand.
+struct PathBuffers {
+    DevArray<float4> prim_o, prim_d, ray_o, ray_d, att, result, sample;
+    DevArray<uint2> prim_hit, ls_depth, hit;
+    DevArray<uint32_t> q0, q1, ctr;
+    // slots for n paths; `moved` is set when an array changed address
+    cudaError_t reserve(size_t n, bool* moved = nullptr)
+    {
+        const void* before[13] = {prim_o.ptr, prim_d.ptr, ray_o.ptr, ray_d.ptr, att.ptr,
+                                  result.ptr, sample.ptr, prim_hit.ptr, ls_depth.ptr, hit.ptr,
+                                  q0.ptr, q1.ptr, ctr.ptr};
+        cudaError_t e = cudaSuccess;
+        auto r = [&](auto& a, size_t m) {
+            if (e == cudaSuccess)
+                e = a.reserve(m);
+        };
+        r(prim_o, n);
+        r(prim_d, n);
+        r(ray_o, n);
+        r(ray_d, n);
+        r(att, n);
+        r(result, n);
+        r(sample, n);
+        r(prim_hit, n);
+        r(ls_depth, n);
+        r(hit, n);
+        r(q0, n);
+        r(q1, n);
+        r(ctr, 4);
+        const void* after[13] = {prim_o.ptr, prim_d.ptr, ray_o.ptr, ray_d.ptr, att.ptr,
+                                 result.ptr, sample.ptr, prim_hit.ptr, ls_depth.ptr, hit.ptr,
+                                 q0.ptr, q1.ptr, ctr.ptr};
+        if (moved)
+            for (int k = 0; k < 13; ++k)
+                if (before[k] != after[k])
+                    *moved = true;
+        return e;
+    }
+    PathState state() const
+    {
+        PathState S;
+        S.prim_o = prim_o.ptr;
+        S.prim_d = prim_d.ptr;
+        S.prim_hit = prim_hit.ptr;
+        S.ray_o = ray_o.ptr;
+        S.ray_d = ray_d.ptr;
+        S.att = att.ptr;
+        S.result = result.ptr;
+        S.ls_depth = ls_depth.ptr;
+        S.hit = hit.ptr;
+        S.sample = sample.ptr;
+        S.queue[0] = q0.ptr;
+        S.queue[1] = q1.ptr;
+        S.ctr = ctr.ptr;
+        return S;
+    }
+};
+
+struct fr_tracer;
+
 struct fr_device {
     int ordinal = 0;
     cudaStream_t stream = nullptr;
@@ -97,6 +157,8 @@ struct fr_device {
     int persistent = 0;                    // persistent traversal kernels for 4-wide trees
     std::vector<fr_scene*> scenes;         // to mark BVHs stale when a build option changes
     void* static_path = nullptr;           // this device's copy of g_static_path (looked up once)
+    PathBuffers path;                      // wavefront state shared by the device's tracers
+    const fr_tracer* path_owner = nullptr; // tracer of the last path render in `path`
 };
 
 struct fr_geometry {
@@ -164,10 +226,6 @@ struct fr_tracer {
     uint32_t w = 0, h = 0;
     DevArray<float4> linear;
     DevArray<uint32_t> srgb;
-    // path tracer state
-    DevArray<float4> prim_o, prim_d, ray_o, ray_d, att, result, sample;
-    DevArray<uint2> prim_hit, ls_depth, hit;
-    DevArray<uint32_t> q0, q1, ctr;
     DevArray<uint2> preview_hits;
     DevArray<unsigned long long> stats;
     uint32_t* h_count = nullptr;  // pinned
@@ -234,10 +292,7 @@ struct fr_batch {
     DevArray<WaveJob> jobs;
     DevArray<uint32_t> wave_first, wave_tiles, wave_pixels;
     DevArray<BatchCtl> ctl;
-    DevArray<float4> prim_o, prim_d, ray_o, ray_d, att, result, sample;
-    DevArray<uint2> prim_hit, ls_depth, hit;
-    DevArray<uint32_t> q0, q1, ctr;
-    size_t slots = 0;  // path-state capacity
+    PathBuffers path;
     BatchCtl* h_ctl = nullptr;  // pinned
     cudaGraphExec_t exec = nullptr;
     int exec_width = 0;
@@ -497,39 +552,8 @@ uint32_t batch_size(const fr_tracer* tr, uint32_t remaining)
 fr_status alloc_path_state(fr_tracer* tr, uint32_t batch)
 {
     size_t n = size_t(tr->w) * tr->h * batch;
-    FR_CUDA(tr->prim_o.reserve(n), "path state");
-    FR_CUDA(tr->prim_d.reserve(n), "path state");
-    FR_CUDA(tr->ray_o.reserve(n), "path state");
-    FR_CUDA(tr->ray_d.reserve(n), "path state");
-    FR_CUDA(tr->att.reserve(n), "path state");
-    FR_CUDA(tr->result.reserve(n), "path state");
-    FR_CUDA(tr->sample.reserve(n), "path state");
-    FR_CUDA(tr->prim_hit.reserve(n), "path state");
-    FR_CUDA(tr->ls_depth.reserve(n), "path state");
-    FR_CUDA(tr->hit.reserve(n), "path state");
-    FR_CUDA(tr->q0.reserve(n), "path state");
-    FR_CUDA(tr->q1.reserve(n), "path state");
-    FR_CUDA(tr->ctr.reserve(4), "path state");
+    FR_CUDA(tr->dev->path.reserve(n), "allocating the path state");
     return FR_OK;
-}
-
-PathState path_state(fr_tracer* tr)
-{
-    PathState S;
-    S.prim_o = tr->prim_o.ptr;
-    S.prim_d = tr->prim_d.ptr;
-    S.prim_hit = tr->prim_hit.ptr;
-    S.ray_o = tr->ray_o.ptr;
-    S.ray_d = tr->ray_d.ptr;
-    S.att = tr->att.ptr;
-    S.result = tr->result.ptr;
-    S.ls_depth = tr->ls_depth.ptr;
-    S.hit = tr->hit.ptr;
-    S.sample = tr->sample.ptr;
-    S.queue[0] = tr->q0.ptr;
-    S.queue[1] = tr->q1.ptr;
-    S.ctr = tr->ctr.ptr;
-    return S;
 }
 
 fr_status check_params(const fr_tracer* tr, const fr_scene* sc, const fr_render_params* p)
@@ -1051,6 +1075,8 @@ fr_status fr_tracer_destroy(fr_tracer* t)
     cudaStreamSynchronize(t->dev->stream);
     if (t->h_count)
         cudaFreeHost(t->h_count);
+    if (t->dev->path_owner == t)
+        t->dev->path_owner = nullptr;
     delete t;
     return FR_OK;
 }
@@ -1102,9 +1128,10 @@ fr_status fr_tracer_render_path(fr_tracer* t, fr_scene* sc, const fr_render_para
         return s;
     FrameParams P = frame_params(t, sc, p, false, 1);
     P.light_samples = light_samples;
-    PathState S = path_state(t);
+    PathState S = t->dev->path.state();
+    t->dev->path_owner = t;
     cudaStream_t st = t->dev->stream;
-    FR_CUDA(cudaMemsetAsync(t->ctr.ptr, 0, 4 * sizeof(uint32_t), st), "clearing queue lengths");
+    FR_CUDA(cudaMemsetAsync(S.ctr, 0, 4 * sizeof(uint32_t), st), "clearing queue lengths");
     const int CHECK_EVERY = 8;
     const int MAX_ITER = 1 << 20;
     const bool prof = t->dev->profiling;
@@ -1122,7 +1149,7 @@ fr_status fr_tracer_render_path(fr_tracer* t, fr_scene* sc, const fr_render_para
     for (uint32_t done = 0; done < n_render;) {
         P.n_samples = first_sample + done;
         P.batch = batch < n_render - done ? batch : n_render - done;
-        FR_CUDA(cudaMemsetAsync(t->ctr.ptr + 3, 0, sizeof(uint32_t), st), "clearing a counter");
+        FR_CUDA(cudaMemsetAsync(S.ctr + 3, 0, sizeof(uint32_t), st), "clearing a counter");
         timed(0, [&] { launch_path_primary(P, S, t->dev->shape, st); });
         t->launches++;
         int it = 0;
@@ -1133,7 +1160,7 @@ fr_status fr_tracer_render_path(fr_tracer* t, fr_scene* sc, const fr_render_para
                 t->launches += 2;
             }
             FR_CUDA(cudaGetLastError(), "launching the path tracer");
-            FR_CUDA(cudaMemcpyAsync(t->h_count, t->ctr.ptr + ((it - 1) & 1), sizeof(uint32_t),
+            FR_CUDA(cudaMemcpyAsync(t->h_count, S.ctr + ((it - 1) & 1), sizeof(uint32_t),
                                     cudaMemcpyDeviceToHost, st),
                     "reading the queue length");
             FR_CUDA(cudaStreamSynchronize(st), "path tracer");
@@ -1405,12 +1432,12 @@ fr_status fr_tracer_read_primary_hits(fr_tracer* t, uint32_t* host, size_t nbyte
     size_t n = size_t(t->w) * t->h;
     if (nbytes != n * sizeof(uint2))
         return fail(FR_ERR_INVALID, "primary hit buffer size mismatch");
-    if (t->prim_hit.cap < n)
-        return fail(FR_ERR_STATE, "no path render yet");
+    if (t->dev->path_owner != t || t->dev->path.prim_hit.cap < n)
+        return fail(FR_ERR_STATE, "the device's last path render was not this tracer's");
     fr_status s = use_device(t->dev);
     if (s != FR_OK)
         return s;
-    FR_CUDA(cudaMemcpyAsync(host, t->prim_hit.ptr, nbytes, cudaMemcpyDeviceToHost,
+    FR_CUDA(cudaMemcpyAsync(host, t->dev->path.prim_hit.ptr, nbytes, cudaMemcpyDeviceToHost,
                             t->dev->stream),
             "downloading primary hits");
     FR_CUDA(cudaStreamSynchronize(t->dev->stream), "downloading primary hits");
@@ -1654,20 +1681,7 @@ fr_status fr_batch_render(fr_batch* b)
     FR_CUDA(grow(b->wave_first, wave_first.size(), moved), "allocating the batch plan");
     FR_CUDA(grow(b->wave_tiles, wave_tiles.size(), moved), "allocating the batch plan");
     FR_CUDA(grow(b->wave_pixels, wave_pixels.size(), moved), "allocating the batch plan");
-    FR_CUDA(grow(b->prim_o, cap, moved), "batch path state");
-    FR_CUDA(grow(b->prim_d, cap, moved), "batch path state");
-    FR_CUDA(grow(b->ray_o, cap, moved), "batch path state");
-    FR_CUDA(grow(b->ray_d, cap, moved), "batch path state");
-    FR_CUDA(grow(b->att, cap, moved), "batch path state");
-    FR_CUDA(grow(b->result, cap, moved), "batch path state");
-    FR_CUDA(grow(b->sample, cap, moved), "batch path state");
-    FR_CUDA(grow(b->prim_hit, cap, moved), "batch path state");
-    FR_CUDA(grow(b->ls_depth, cap, moved), "batch path state");
-    FR_CUDA(grow(b->hit, cap, moved), "batch path state");
-    FR_CUDA(grow(b->q0, cap, moved), "batch path state");
-    FR_CUDA(grow(b->q1, cap, moved), "batch path state");
-    FR_CUDA(grow(b->ctr, 4, moved), "batch path state");
-    b->slots = std::max(b->slots, cap);
+    FR_CUDA(b->path.reserve(cap, &moved), "allocating the batch path state");
 
     cudaStream_t st = dev->stream;
     FR_CUDA(cudaMemcpyAsync(b->jobs.ptr, jobs.data(), jobs.size() * sizeof(WaveJob),
@@ -1694,19 +1708,7 @@ fr_status fr_batch_render(fr_batch* b)
         B.wave_tiles = b->wave_tiles.ptr;
         B.wave_pixels = b->wave_pixels.ptr;
         B.ctl = b->ctl.ptr;
-        B.S.prim_o = b->prim_o.ptr;
-        B.S.prim_d = b->prim_d.ptr;
-        B.S.prim_hit = b->prim_hit.ptr;
-        B.S.ray_o = b->ray_o.ptr;
-        B.S.ray_d = b->ray_d.ptr;
-        B.S.att = b->att.ptr;
-        B.S.result = b->result.ptr;
-        B.S.ls_depth = b->ls_depth.ptr;
-        B.S.hit = b->hit.ptr;
-        B.S.sample = b->sample.ptr;
-        B.S.queue[0] = b->q0.ptr;
-        B.S.queue[1] = b->q1.ptr;
-        B.S.ctr = b->ctr.ptr;
+        B.S = b->path.state();
         FR_CUDA(batch_graph_create(B, width, mask, dev->num_sms, b->capture, &b->exec),
                 "capturing the batch graph");
         b->exec_width = width;

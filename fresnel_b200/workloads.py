@@ -159,3 +159,24 @@ def config3(device, scale=1.0, box=100.0):
                   color=numpy.full((len(verts), 3), 0.7, numpy.float32))
     scene.camera = perspective_fit(scene)
     return scene
+
+
+def config4(device, n_frames=64, seed=3):
+    """Trajectory-style frame set: ``n_frames`` independent scenes of the 1M-sphere scene's
+    density (1e6 spheres per 140^3), sphere count log-uniform in [1e4, 5e5], r = 0.5, per-particle
+    colours, the 1M-sphere scene's material and lights; each frame's resolution drawn from
+    512x512, 768x768, 1024x1024 (16 spp, 1 light sample in the benchmark).  Returns a list of
+    (scene, width, height)."""
+    rng = numpy.random.default_rng(seed)
+    rho = 1e6 / 140.0**3
+    frames = []
+    for _ in range(n_frames):
+        n = int(round(math.exp(rng.uniform(math.log(1e4), math.log(5e5)))))
+        box = (n / rho) ** (1.0 / 3.0)
+        res = (512, 768, 1024)[int(rng.integers(3))]
+        scene = random_spheres(device, n, box, 0.5, seed=int(rng.integers(1 << 31)), colors=True,
+                               mat=material.Material(roughness=0.4, metal=0.0, specular=0.5,
+                                                     primitive_color_mix=1.0),
+                               lights=light.lightbox())
+        frames.append((scene, res, res))
+    return frames

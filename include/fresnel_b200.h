@@ -153,10 +153,12 @@ FR_API fr_status fr_device_timer_start(fr_device* dev);
 FR_API fr_status fr_device_timer_stop(fr_device* dev, float* ms);
 /* Engine tuning options of a device (no counterpart in the reference, whose OptiX and Embree
  * backends tune themselves); they apply to BVHs built and renders started afterwards:
- *   "bvh_width"     2 or 4: binary or 4-wide tree traversed by the renderers (default 2)
- *   "leaf_max"      largest leaf the SAH collapse may form (1..16, default 4)
+ *   "bvh_width"     2 or 4: binary or 4-wide tree traversed by the renderers (default 4)
+ *   "leaf_max"      largest leaf the SAH collapse may form (1..16, default 2)
  *   "c_trav"        SAH cost of one node visit relative to one primitive test (default 1)
  *   "path_slots"    path slots traced together by the path tracer (default 33554432)
+ *   "persistent"    1: 4-wide traversal in persistent warps with per-lane refill;
+ *                   0: one ray per thread (default)
  * Setting an option marks every BVH of the device's scenes for rebuild when it changes the
  * tree.  Unknown names or out-of-range values return FR_ERR_INVALID. */
 FR_API fr_status fr_device_set_option(fr_device* dev, const char* name, double value);
@@ -243,16 +245,17 @@ FR_API fr_status fr_tracer_write_linear(fr_tracer* tr, const float* host, size_t
 FR_API fr_status fr_tracer_write_srgb(fr_tracer* tr, const uint8_t* host, size_t nbytes);
 FR_API fr_status fr_tracer_get_stats(const fr_tracer* tr, fr_stats* out);
 /* Parity hook (no counterpart in the reference): the closest hits of the primary rays of the
- * first sample of the last path-render batch, [h][w][2] = (geometry index or 0xFFFFFFFF,
- * primitive index), for comparing traversal variants and the CPU oracle. */
+ * first sample of the last wavefront of the device's last path render, which must have been
+ * this tracer's (else FR_ERR_STATE), [h][w][2] = (geometry index or 0xFFFFFFFF, primitive
+ * index), for comparing traversal variants and the CPU oracle. */
 FR_API fr_status fr_tracer_read_primary_hits(fr_tracer* tr, uint32_t* host, size_t nbytes);
 FR_API fr_status fr_tracer_reset_stats(fr_tracer* tr);
 
 /* ---------------- allocation-free path render ----------------
  * No counterpart in the reference.  fr_tracer_render_path keeps its wavefront state (rays,
- * throughputs, queues) in tracer-owned device memory that it allocates on first use and
- * reallocates when a call needs a larger batch; cudaFree of the old block waits for the whole
- * GPU.  fr_tracer_render_path_static renders the same images without allocating any memory: the
+ * throughputs, queues) in device memory shared by the device's tracers, which it allocates on
+ * first use and reallocates when a call needs a larger wavefront; cudaFree of the old block
+ * waits for the whole GPU.  fr_tracer_render_path_static renders the same images without allocating any memory: the
  * wavefront state lives in one fixed array of FR_STATIC_PATH_SLOTS slots of 144 bytes (37.7 MB)
  * inside the library's device module.  It is for callers that must not allocate inside a render
  * call: a runtime that reserves the GPU's memory up front for its own pool, or a frame loop
