@@ -159,6 +159,7 @@ struct fr_device {
     void* static_path = nullptr;           // this device's copy of g_static_path (looked up once)
     PathBuffers path;                      // wavefront state shared by the device's tracers
     const fr_tracer* path_owner = nullptr; // tracer of the last path render in `path`
+    uint32_t path_k = 0;                   // samples per pixel of that render's last wavefront
 };
 
 struct fr_geometry {
@@ -290,7 +291,7 @@ struct fr_batch {
     std::vector<Item> items;
     // device-side plan and path state (their addresses are baked into the graph)
     DevArray<WaveJob> jobs;
-    DevArray<uint32_t> wave_first, wave_tiles, wave_pixels;
+    DevArray<uint32_t> wave_first, wave_items, wave_pixels;
     DevArray<BatchCtl> ctl;
     PathBuffers path;
     BatchCtl* h_ctl = nullptr;  // pinned
@@ -534,12 +535,15 @@ fr_status alloc_outputs(fr_tracer* tr, uint32_t w, uint32_t h)
     return FR_OK;
 }
 
+// Path slots per sample of a w x h image: the pixels of its 8x8 tiles (edge tiles padded).
+size_t padded_pixels(uint32_t w, uint32_t h) { return size_t((w + 7) / 8) * ((h + 7) / 8) * 64; }
+
 // Samples traced together: a batch of K samples of every pixel fills about
 // dev->path_slots slots (about 144 bytes each).
 uint32_t batch_size(const fr_tracer* tr, uint32_t remaining)
 {
-    size_t wh = size_t(tr->w) * tr->h;
-    size_t k = tr->dev->path_slots / (wh ? wh : 1);
+    size_t wh = padded_pixels(tr->w, tr->h);
+    size_t k = tr->dev->path_slots / wh;
     if (k < 1)
         k = 1;
     if (k > 4096)
@@ -551,7 +555,7 @@ uint32_t batch_size(const fr_tracer* tr, uint32_t remaining)
 
 fr_status alloc_path_state(fr_tracer* tr, uint32_t batch)
 {
-    size_t n = size_t(tr->w) * tr->h * batch;
+    size_t n = padded_pixels(tr->w, tr->h) * batch;
     FR_CUDA(tr->dev->path.reserve(n), "allocating the path state");
     return FR_OK;
 }
@@ -1172,6 +1176,7 @@ fr_status fr_tracer_render_path(fr_tracer* t, fr_scene* sc, const fr_render_para
         }
         launch_path_fold(P, S, st);
         t->launches++;
+        t->dev->path_k = P.batch;
         done += P.batch;
     }
     return check_status(t->dev);
@@ -1245,12 +1250,13 @@ fr_status fr_tracer_render_path_static(fr_tracer* t, fr_scene* sc, const fr_rend
         return fail(FR_ERR_INVALID, "light_samples must be positive");
     if (first_sample == 0)
         return fail(FR_ERR_INVALID, "sample numbers start at 1");
-    const size_t wh = size_t(t->w) * t->h;
+    const size_t wh = padded_pixels(t->w, t->h);
     if (wh > kStaticSlots)
         return fail(FR_ERR_INVALID, "image of " + std::to_string(t->w) + "x" +
                                         std::to_string(t->h) +
                                         " pixels exceeds the allocation-free render's limit of " +
-                                        std::to_string(kStaticSlots) + " pixels");
+                                        std::to_string(kStaticSlots) +
+                                        " pixels (counted in whole 8x8 tiles)");
     for (fr_geometry* g : sc->geoms)
         if (!g->removed && g->bvh_dirty)
             return fail(FR_ERR_STATE, "the allocation-free render needs a built scene: call "
@@ -1432,15 +1438,27 @@ fr_status fr_tracer_read_primary_hits(fr_tracer* t, uint32_t* host, size_t nbyte
     size_t n = size_t(t->w) * t->h;
     if (nbytes != n * sizeof(uint2))
         return fail(FR_ERR_INVALID, "primary hit buffer size mismatch");
-    if (t->dev->path_owner != t || t->dev->path.prim_hit.cap < n)
+    const size_t K = t->dev->path_k;
+    const size_t slots = padded_pixels(t->w, t->h) * K;
+    if (t->dev->path_owner != t || K == 0 || t->dev->path.prim_hit.cap < slots)
         return fail(FR_ERR_STATE, "the device's last path render was not this tracer's");
     fr_status s = use_device(t->dev);
     if (s != FR_OK)
         return s;
-    FR_CUDA(cudaMemcpyAsync(host, t->dev->path.prim_hit.ptr, nbytes, cudaMemcpyDeviceToHost,
-                            t->dev->stream),
+    std::vector<uint2> all(slots);
+    FR_CUDA(cudaMemcpyAsync(all.data(), t->dev->path.prim_hit.ptr, slots * sizeof(uint2),
+                            cudaMemcpyDeviceToHost, t->dev->stream),
             "downloading primary hits");
     FR_CUDA(cudaStreamSynchronize(t->dev->stream), "downloading primary hits");
+    // sample 0 of pixel (i, j) sits at the start of the pixel's K slots in its 8x8 tile
+    const size_t tiles_x = (t->w + 7) / 8;
+    for (uint32_t j = 0; j < t->h; ++j)
+        for (uint32_t i = 0; i < t->w; ++i) {
+            const size_t slot =
+                (((j >> 3) * tiles_x + (i >> 3)) * 64 + ((j & 7u) << 3) + (i & 7u)) * K;
+            host[2 * (size_t(j) * t->w + i)] = all[slot].x;
+            host[2 * (size_t(j) * t->w + i) + 1] = all[slot].y;
+        }
     return FR_OK;
 }
 
@@ -1592,7 +1610,7 @@ fr_status fr_batch_render(fr_batch* b)
     // path-state capacity: the device's wavefront size, at least one sample of the largest image
     size_t cap = dev->path_slots;
     for (auto& it : b->items)
-        cap = std::max(cap, size_t(it.tr->w) * it.tr->h);
+        cap = std::max(cap, padded_pixels(it.tr->w, it.tr->h));
 
     // plan: every item's samples go to waves in sample order, at most one slice of a tracer
     // per wave, K samples of all pixels per slice; first fit over the waves
@@ -1605,7 +1623,7 @@ fr_status fr_batch_render(fr_batch* b)
     std::vector<std::pair<const fr_tracer*, size_t>> last_wave;  // tracer -> next allowed wave
     for (size_t i = 0; i < b->items.size(); ++i) {
         const auto& it = b->items[i];
-        const size_t wh = size_t(it.tr->w) * it.tr->h;
+        const size_t wh = padded_pixels(it.tr->w, it.tr->h);
         size_t min_wave = 0;
         for (auto& lw : last_wave)
             if (lw.first == it.tr)
@@ -1639,12 +1657,12 @@ fr_status fr_batch_render(fr_batch* b)
 
     // render table
     std::vector<WaveJob> jobs;
-    std::vector<uint32_t> wave_first, wave_tiles, wave_pixels;
+    std::vector<uint32_t> wave_first, wave_items, wave_pixels;
     int width = 4;
     uint32_t mask = 0;
     for (auto& wv : waves) {
         wave_first.push_back(uint32_t(jobs.size()));
-        uint64_t slot = 0, tile = 0, pixel = 0;
+        uint64_t slot = 0, item = 0, pixel = 0;
         for (auto& sl : wv) {
             const auto& it = b->items[sl.item];
             WaveJob J;
@@ -1656,20 +1674,17 @@ fr_status fr_batch_render(fr_batch* b)
             if (J.P.bvh_width != 4)
                 width = 2;
             mask |= J.P.type_mask;
-            const uint32_t tx = (it.tr->w + 15) / 16, ty = (it.tr->h + 15) / 16;
             J.slot_base = uint32_t(slot);
-            J.tile_base = uint32_t(tile);
+            J.item_base = uint32_t(item);
             J.pixel_base = uint32_t(pixel);
-            J.tiles_x = tx;
-            J.tiles_per_sample = tx * ty;
-            slot += uint64_t(sl.k) * it.tr->w * it.tr->h;
-            tile += uint64_t(sl.k) * tx * ty;
+            item += uint64_t(padded_pixels(it.tr->w, it.tr->h)) * sl.k;
+            slot = item;
             pixel += uint64_t(it.tr->w) * it.tr->h;
-            if (slot > 0xFFFFFFFFull || tile > 0xFFFFFFFFull || pixel > 0xFFFFFFFFull)
+            if (slot > 0xFFFFFFFFull || item > 0xFFFFFFFFull || pixel > 0xFFFFFFFFull)
                 return fail(FR_ERR_INVALID, "a batch wave exceeds 2^32 slots");
             jobs.push_back(J);
         }
-        wave_tiles.push_back(uint32_t(tile));
+        wave_items.push_back(uint32_t(item));
         wave_pixels.push_back(uint32_t(pixel));
     }
     wave_first.push_back(uint32_t(jobs.size()));
@@ -1679,7 +1694,7 @@ fr_status fr_batch_render(fr_batch* b)
     bool moved = false;
     FR_CUDA(grow(b->jobs, jobs.size(), moved), "allocating the batch plan");
     FR_CUDA(grow(b->wave_first, wave_first.size(), moved), "allocating the batch plan");
-    FR_CUDA(grow(b->wave_tiles, wave_tiles.size(), moved), "allocating the batch plan");
+    FR_CUDA(grow(b->wave_items, wave_items.size(), moved), "allocating the batch plan");
     FR_CUDA(grow(b->wave_pixels, wave_pixels.size(), moved), "allocating the batch plan");
     FR_CUDA(b->path.reserve(cap, &moved), "allocating the batch path state");
 
@@ -1688,7 +1703,7 @@ fr_status fr_batch_render(fr_batch* b)
                             cudaMemcpyHostToDevice, st), "uploading the batch plan");
     FR_CUDA(cudaMemcpyAsync(b->wave_first.ptr, wave_first.data(), wave_first.size() * 4,
                             cudaMemcpyHostToDevice, st), "uploading the batch plan");
-    FR_CUDA(cudaMemcpyAsync(b->wave_tiles.ptr, wave_tiles.data(), wave_tiles.size() * 4,
+    FR_CUDA(cudaMemcpyAsync(b->wave_items.ptr, wave_items.data(), wave_items.size() * 4,
                             cudaMemcpyHostToDevice, st), "uploading the batch plan");
     FR_CUDA(cudaMemcpyAsync(b->wave_pixels.ptr, wave_pixels.data(), wave_pixels.size() * 4,
                             cudaMemcpyHostToDevice, st), "uploading the batch plan");
@@ -1705,7 +1720,7 @@ fr_status fr_batch_render(fr_batch* b)
         BatchDev B;
         B.jobs = b->jobs.ptr;
         B.wave_first = b->wave_first.ptr;
-        B.wave_tiles = b->wave_tiles.ptr;
+        B.wave_items = b->wave_items.ptr;
         B.wave_pixels = b->wave_pixels.ptr;
         B.ctl = b->ctl.ptr;
         B.S = b->path.state();

@@ -2,7 +2,7 @@
 //
 // The per-slot work is the single-render path tracer's (path_device.cuh: shade_pixel, welford,
 // write_pixel; engine.cuh: trace_closest), so a render gives the same image alone or in a
-// batch. What changes is how a thread finds its render: primary tiles, queued slots and fold
+// batch. What changes is how a thread finds its render: primary work items, queued slots and fold
 // pixels carry indices into the current wave, and a binary search over the wave's render table
 // maps them to the render (its scene, camera, lights, outputs and sample numbers).
 #include "batch.hpp"
@@ -49,62 +49,32 @@ __global__ void k_wave_begin(BatchDev B, cudaGraphConditionalHandle inner)
     cudaGraphSetConditional(inner, 1u);
 }
 
-// Primary rays of the wave: 16x16 tiles of every render and sample, grid-stride over tiles.
-// Same per-pixel work as k_path_primary.
+// Primary rays of the wave, grid-stride over its work items (each render's items in
+// primary_item order; a render has a multiple of 64 items, so a warp never spans two renders).
 template <int WIDTH, uint32_t MASK>
 __global__ void __launch_bounds__(256) k_batch_primary(BatchDev B)
 {
     const PathState& S = B.S;
     const uint32_t w = B.ctl->wave;
     const uint32_t f0 = B.wave_first[w], f1 = B.wave_first[w + 1];
-    const uint32_t n_tiles = B.wave_tiles[w];
-    const uint32_t lane = (threadIdx.x + threadIdx.y * blockDim.x) & 31u;
+    const uint32_t n_items = B.wave_items[w];
     TraceCount tc;
-    for (uint32_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
-        const WaveJob& J = B.jobs[find_job<&WaveJob::tile_base>(B.jobs, f0, f1, t)];
+    const uint32_t stride = gridDim.x * blockDim.x;
+    // n_items is a multiple of 64, so whole warps enter and leave the loop together
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g - lane_id() < n_items;
+         g += stride) {
+        const WaveJob& J = B.jobs[find_job<&WaveJob::item_base>(B.jobs, f0, f1, g)];
         const FrameParams& P = J.P;
-        const uint32_t lt = t - J.tile_base;
-        const uint32_t k = lt / J.tiles_per_sample;
-        const uint32_t r = lt - k * J.tiles_per_sample;
-        const uint32_t ty = r / J.tiles_x;
-        const uint32_t tx = r - ty * J.tiles_x;
-        const uint32_t i = tx * 16u + threadIdx.x;
-        const uint32_t j = ty * 16u + threadIdx.y;
-        const bool valid = (i < P.w) && (j < P.h);
+        const PrimaryItem it = primary_item(g - J.item_base, P.w, P.h, P.batch);
         bool push = false;
         uint32_t slot = 0;
-        if (valid) {
-            const uint32_t p = j * P.w + i;
-            slot = J.slot_base + k * P.w * P.h + p;
-            V3 o, d;
-            camera_ray(P.cam, i, j, P.n_samples + k, o, d);
-            Hit h = trace_closest<WIDTH, MASK>(P.scene, o, d, PATH_TNEAR, tc);
-            S.prim_hit[slot] = make_uint2(h.geom, h.prim);
-            if (h.geom == MISS) {
-                C3 res = P.bg * float(P.light_samples);
-                C3 out = c_div_recip(res, float(P.light_samples));
-                S.sample[slot] = make_float4(out.r, out.g, out.b, P.bg_alpha);
-            } else {
-                S.prim_o[slot] = f4(o);
-                S.prim_d[slot] = f4(d);
-                S.ls_depth[slot] = make_uint2(0u, 0u);
-                S.att[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-                S.result[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                push = true;
-            }
+        if (it.valid) {
+            slot = J.slot_base + (g - J.item_base);
+            push = primary_ray<WIDTH, MASK>(P, S, it, slot, tc);
         }
-        const uint32_t m = __ballot_sync(0xffffffffu, push);
-        if (m) {
-            uint32_t at = 0;
-            if (lane == 0)
-                at = atomicAdd(S.ctr + 1, uint32_t(__popc(m)));
-            at = __shfl_sync(0xffffffffu, at, 0);
-            if (push)
-                S.queue[1][at + __popc(m & ((1u << lane) - 1u))] = slot;
-        }
-        // a warp covers two rows of one tile, so all its lanes belong to render J
-        const uint32_t mv = __ballot_sync(0xffffffffu, valid);
-        if (lane == 0 && mv) {
+        push_primary(S, push, slot);
+        const uint32_t mv = __ballot_sync(0xffffffffu, it.valid);
+        if (lane_id() == 0 && mv) {
             atomicAdd(P.stats + 0, (unsigned long long)__popc(mv));
             atomicAdd(P.stats + 1, (unsigned long long)__popc(mv) * P.light_samples);
         }
@@ -212,11 +182,11 @@ __global__ void __launch_bounds__(256) k_batch_fold(BatchDev B)
         const WaveJob& J = B.jobs[find_job<&WaveJob::pixel_base>(B.jobs, f0, f1, q)];
         const FrameParams& P = J.P;
         const uint32_t lp = q - J.pixel_base;
-        const uint32_t wh = P.w * P.h;
+        const uint32_t j = lp / P.w;
+        const uint32_t base = J.slot_base + pixel_slot(lp - j * P.w, j, P.w, P.batch);
         float4 mean = P.linear[lp];
         for (uint32_t k = 0; k < P.batch; ++k)
-            mean = welford(P, mean, S.sample[size_t(J.slot_base) + size_t(k) * wh + lp],
-                           P.n_samples + k);
+            mean = welford(P, mean, S.sample[base + k], P.n_samples + k);
         write_pixel(P, lp, mean.x, mean.y, mean.z, mean.w);
     }
 }
@@ -238,7 +208,7 @@ template <class K> int grid_for(K kernel, int num_sms, int threads)
 template <int WIDTH, uint32_t MASK> struct Kernels {
     static void primary(const BatchDev& B, int grid, cudaStream_t s)
     {
-        k_batch_primary<WIDTH, MASK><<<grid, dim3(16, 16), 0, s>>>(B);
+        k_batch_primary<WIDTH, MASK><<<grid, 256, 0, s>>>(B);
     }
     static void extend(const BatchDev& B, int q, int grid, cudaStream_t s)
     {

@@ -21,11 +21,10 @@ namespace fr {
 // One render of a wave: P.batch samples of every pixel, starting at sample P.n_samples.
 struct WaveJob {
     FrameParams P;
-    uint32_t slot_base;   // first path-state slot of this render in its wave
-    uint32_t tile_base;   // first 16x16 primary tile (over all its samples) in its wave
+    uint32_t slot_base;   // first path-state slot of this render in its wave (slots follow the
+                          // render's primary work items, so item g has slot slot_base + g)
+    uint32_t item_base;   // first primary work item of this render in its wave
     uint32_t pixel_base;  // first fold pixel in its wave
-    uint32_t tiles_x;     // 16x16 tiles per row of the image
-    uint32_t tiles_per_sample;
 };
 
 // Loop state of one batch launch (device memory).
@@ -42,7 +41,7 @@ struct BatchCtl {
 struct BatchDev {
     const WaveJob* jobs;          // renders of all waves; wave w's are [wave_first[w], wave_first[w+1])
     const uint32_t* wave_first;   // [n_waves + 1]
-    const uint32_t* wave_tiles;   // [n_waves] primary tiles of each wave
+    const uint32_t* wave_items;   // [n_waves] primary work items of each wave
     const uint32_t* wave_pixels;  // [n_waves] fold pixels of each wave
     BatchCtl* ctl;
     PathState S;

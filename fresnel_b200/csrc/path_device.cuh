@@ -15,6 +15,48 @@ __device__ __forceinline__ float4 f4(V3 a) { return make_float4(a.x, a.y, a.z, 0
 __device__ __forceinline__ float4 f4(C3 a) { return make_float4(a.r, a.g, a.b, 0.0f); }
 __device__ __forceinline__ C3 rgb3(float4 a) { return c3(a.x, a.y, a.z); }
 
+// Work items of the primary pass: 8x8-pixel tiles in row-major order, a tile's pixels in
+// row-major order, and the K samples of a pixel innermost. A warp then traces two pixels'
+// 16 samples (K = 16) or an 8x4 block of pixels (K = 1): its rays start close together and
+// point the same way, which keeps the warp's traversal steps and node loads shared. The
+// The path state is laid out in the same order: the slot of a render's item g is g itself, so
+// the primary pass writes whole cache lines, and the queues it fills start out in slot order.
+// Slots of pixels outside the image (edge tiles) stay unused.
+struct PrimaryItem {
+    uint32_t i, j, k;
+    bool valid;
+};
+
+__device__ __forceinline__ uint32_t primary_tiles_x(uint32_t w) { return (w + 7u) >> 3; }
+
+__host__ __device__ __forceinline__ uint32_t primary_items(uint32_t w, uint32_t h, uint32_t K)
+{
+    return ((w + 7u) >> 3) * ((h + 7u) >> 3) * 64u * K;
+}
+
+// Slot of sample 0 of pixel (i, j); its K samples follow it.
+__device__ __forceinline__ uint32_t pixel_slot(uint32_t i, uint32_t j, uint32_t w, uint32_t K)
+{
+    return (((j >> 3) * primary_tiles_x(w) + (i >> 3)) * 64u + ((j & 7u) << 3) + (i & 7u)) * K;
+}
+
+__device__ __forceinline__ PrimaryItem primary_item(uint32_t g, uint32_t w, uint32_t h, uint32_t K)
+{
+    const uint32_t per_tile = 64u * K;
+    const uint32_t tile = g / per_tile;
+    const uint32_t r = g - tile * per_tile;
+    const uint32_t px = r / K;
+    const uint32_t tiles_x = primary_tiles_x(w);
+    const uint32_t ty = tile / tiles_x;
+    const uint32_t tx = tile - ty * tiles_x;
+    PrimaryItem it;
+    it.k = r - px * K;
+    it.i = tx * 8u + (px & 7u);
+    it.j = ty * 8u + (px >> 3);
+    it.valid = it.i < w && it.j < h;
+    return it;
+}
+
 __device__ __forceinline__ void write_pixel(const FrameParams& P, uint32_t p, float r, float g,
                                             float b, float a)
 {
@@ -47,9 +89,9 @@ __device__ __forceinline__ float4 welford(const FrameParams& P, float4 old, floa
 __device__ __forceinline__ bool shade_pixel(const FrameParams& P, const PathState& S, uint32_t p,
                                             uint32_t local)
 {
-    const uint32_t wh = P.w * P.h;
-    const uint32_t k = local / wh;
-    const uint32_t pixel = local - k * wh;
+    const PrimaryItem pi = primary_item(local, P.w, P.h, P.batch);
+    const uint32_t k = pi.k;
+    const uint32_t pixel = pi.j * P.w + pi.i;
     const uint32_t n_samples = P.n_samples + k;
     uint2 ld = S.ls_depth[p];
     uint32_t ls = ld.x;
@@ -106,6 +148,46 @@ __device__ __forceinline__ bool shade_pixel(const FrameParams& P, const PathStat
         C3 out = c_div_recip(s.result, float(P.light_samples));
         S.sample[p] = make_float4(out.r, out.g, out.b, ph.x == MISS ? P.bg_alpha : 1.0f);
         return false;
+    }
+}
+
+// Primary ray of one item: closest hit; a miss finishes its pixel sample (every light sample
+// sees the background: radiance bg * L, fresnel/common/TracerPathMethods.h:44-50), a hit
+// initialises the path state. Returns true for a hit (the slot is queued for shading).
+template <int WIDTH, uint32_t MASK>
+__device__ __forceinline__ bool primary_ray(const FrameParams& P, const PathState& S,
+                                            const PrimaryItem& it, uint32_t slot, TraceCount& tc)
+{
+    V3 o, d;
+    camera_ray(P.cam, it.i, it.j, P.n_samples + it.k, o, d);
+    Hit h = trace_closest<WIDTH, MASK>(P.scene, o, d, PATH_TNEAR, tc);
+    S.prim_hit[slot] = make_uint2(h.geom, h.prim);
+    if (h.geom == MISS) {
+        C3 res = P.bg * float(P.light_samples);
+        C3 out = c_div_recip(res, float(P.light_samples));
+        S.sample[slot] = make_float4(out.r, out.g, out.b, P.bg_alpha);
+        return false;
+    }
+    S.prim_o[slot] = f4(o);
+    S.prim_d[slot] = f4(d);
+    S.ls_depth[slot] = make_uint2(0u, 0u);
+    S.att[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+    S.result[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    return true;
+}
+
+// Append the lanes with push set to queue 1 (one atomic per warp).
+__device__ __forceinline__ void push_primary(const PathState& S, bool push, uint32_t slot)
+{
+    const uint32_t lane = lane_id();
+    const uint32_t m = __ballot_sync(0xffffffffu, push);
+    if (m) {
+        uint32_t at = 0;
+        if (lane == 0)
+            at = atomicAdd(S.ctr + 1, uint32_t(__popc(m)));
+        at = __shfl_sync(0xffffffffu, at, 0);
+        if (push)
+            S.queue[1][at + __popc(m & ((1u << lane) - 1u))] = slot;
     }
 }
 

@@ -1,15 +1,19 @@
 // render.cu -- wavefront path tracer and preview tracer kernels.
 //
 // Path tracer (replaces path_ray_gen/path_closest_hit/path_miss, fresnel/gpu/path.cu:70-171,
-// with the CPU loop order of fresnel/cpu/TracerPath.cc:78-255):
-//   primary  one thread per pixel: camera ray for this sample, closest hit (shared by all light
-//            samples of the pixel, as the CPU path caches it)
-//   shade    per queued pixel: hit or miss program of the current light sample; a finished
+// with the CPU loop order of fresnel/cpu/TracerPath.cc:78-255).  A batch traces K samples of
+// every pixel at once, one path slot per (pixel, sample):
+//   primary  one thread per slot, the K samples of a pixel in neighbouring lanes: camera ray,
+//            closest hit (shared by all light samples of the pixel sample, as the CPU path
+//            caches it); a miss finishes its sample, a hit is queued
+//   shade    per queued slot: hit or miss program of the current light sample; a finished
 //            light sample restarts the next one from the cached primary hit in the same thread,
-//            so each pixel's radiance accumulates in the reference's order; a finished pixel
-//            folds its sample into the running mean (Welford) and writes sRGB; a continuing path
-//            is appended to the extension queue (warp-aggregated atomics)
-//   extend   persistent warps pull 32 queued rays at a time and find their closest hits
+//            so each pixel's radiance accumulates in the reference's order; a finished slot
+//            stores its pixel sample; a continuing path is appended to the extension queue
+//            (warp-aggregated atomics)
+//   extend   warps pull 32 queued rays at a time and find their closest hits
+//   fold     per pixel: the batch's K samples, in sample order, into the running mean
+//            (Welford), then the sRGB output
 // The host alternates shade/extend until the queue is empty.
 //
 // Preview (replaces direct_ray_gen/direct_closest_hit, fresnel/gpu/direct.cu, with the CPU
@@ -20,52 +24,27 @@ namespace fr {
 
 namespace {
 
-// Primary rays of every slot.  A primary miss finishes its pixel sample here (every light
-// sample sees the background: radiance bg * L, fresnel/common/TracerPathMethods.h:44-50); a hit
-// is queued in queue 1 for the first shade pass.
+// Primary rays of every slot of the batch, one thread per work item (primary_item order).
 template <int WIDTH, uint32_t MASK>
 __global__ void __launch_bounds__(256) k_path_primary(FrameParams P, PathState S)
 {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t j = blockIdx.y * blockDim.y + threadIdx.y;
-    uint32_t k = blockIdx.z;
-    bool valid = (i < P.w) && (j < P.h);
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t n_items = primary_items(P.w, P.h, P.batch);
+    PrimaryItem it;
+    it.valid = false;
+    if (g < n_items)
+        it = primary_item(g, P.w, P.h, P.batch);
     bool push = false;
     uint32_t slot = 0;
     TraceCount tc;
-    if (valid) {
-        uint32_t p = j * P.w + i;
-        slot = k * P.w * P.h + p;
-        V3 o, d;
-        camera_ray(P.cam, i, j, P.n_samples + k, o, d);
-        Hit h = trace_closest<WIDTH, MASK>(P.scene, o, d, PATH_TNEAR, tc);
-        S.prim_hit[slot] = make_uint2(h.geom, h.prim);
-        if (h.geom == MISS) {
-            C3 res = P.bg * float(P.light_samples);
-            C3 out = c_div_recip(res, float(P.light_samples));
-            S.sample[slot] = make_float4(out.r, out.g, out.b, P.bg_alpha);
-        } else {
-            S.prim_o[slot] = f4(o);
-            S.prim_d[slot] = f4(d);
-            S.ls_depth[slot] = make_uint2(0u, 0u);
-            S.att[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-            S.result[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            push = true;
-        }
+    if (it.valid) {
+        slot = g;
+        push = primary_ray<WIDTH, MASK>(P, S, it, slot, tc);
     }
     flush_counts(tc, P.stats + 3);
-    const uint32_t lane = (threadIdx.x + threadIdx.y * blockDim.x) & 31u;
-    uint32_t m = __ballot_sync(0xffffffffu, push);
-    if (m) {
-        uint32_t at = 0;
-        if (lane == 0)
-            at = atomicAdd(S.ctr + 1, uint32_t(__popc(m)));
-        at = __shfl_sync(0xffffffffu, at, 0);
-        if (push)
-            S.queue[1][at + __popc(m & ((1u << lane) - 1u))] = slot;
-    }
-    uint32_t mv = __ballot_sync(0xffffffffu, valid);
-    if (lane == 0 && mv) {
+    push_primary(S, push, slot);
+    const uint32_t mv = __ballot_sync(0xffffffffu, it.valid);
+    if (lane_id() == 0 && mv) {
         atomicAdd(P.stats + 0, (unsigned long long)__popc(mv));
         atomicAdd(P.stats + 1, (unsigned long long)__popc(mv) * P.light_samples);
     }
@@ -128,20 +107,15 @@ __device__ __forceinline__ void persistent_trace(const FrameParams& P, Src& src,
 struct PrimarySource {
     const FrameParams& P;
     const PathState& S;
-    uint32_t ntx, tiles;  // 16x16 pixel tiles per row, per image
     uint32_t slot;
     __device__ bool begin(uint32_t item, LaneRay& L)
     {
-        uint32_t per = tiles * 256u;
-        uint32_t k = item / per, r = item - k * per;
-        uint32_t tile = r >> 8, within = r & 255u;
-        uint32_t ty = tile / ntx, tx = tile - ty * ntx;
-        uint32_t i = tx * 16u + (within & 15u), j = ty * 16u + (within >> 4);
-        if (i >= P.w || j >= P.h)
+        const PrimaryItem it = primary_item(item, P.w, P.h, P.batch);
+        if (!it.valid)
             return false;
-        slot = k * P.w * P.h + j * P.w + i;
+        slot = item;
         V3 o, d;
-        camera_ray(P.cam, i, j, P.n_samples + k, o, d);
+        camera_ray(P.cam, it.i, it.j, P.n_samples + it.k, o, d);
         lane_begin(L, o, d, PATH_TNEAR);
         return true;
     }
@@ -213,11 +187,10 @@ __device__ __forceinline__ void flush_rays(const FrameParams& P, uint32_t n_rays
 template <uint32_t MASK>
 __global__ void __launch_bounds__(256) k_path_primary_persistent(FrameParams P, PathState S)
 {
-    uint32_t ntx = (P.w + 15u) / 16u, nty = (P.h + 15u) / 16u;
-    PrimarySource src{P, S, ntx, ntx * nty, 0u};
+    PrimarySource src{P, S, 0u};
     TraceCount tc;
     uint32_t n_rays = 0;
-    persistent_trace<MASK>(P, src, P.batch * ntx * nty * 256u, S.ctr + 3, tc, n_rays);
+    persistent_trace<MASK>(P, src, primary_items(P.w, P.h, P.batch), S.ctr + 3, tc, n_rays);
     flush_counts(tc, P.stats + 3);
     flush_rays(P, n_rays, true);
 }
@@ -240,12 +213,13 @@ __global__ void __launch_bounds__(256) k_path_extend_persistent(FrameParams P, P
 __global__ void __launch_bounds__(256) k_path_fold(FrameParams P, PathState S)
 {
     uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t wh = P.w * P.h;
-    if (p >= wh)
+    if (p >= P.w * P.h)
         return;
+    const uint32_t j = p / P.w;
+    const uint32_t base = pixel_slot(p - j * P.w, j, P.w, P.batch);
     float4 mean = P.linear[p];
     for (uint32_t k = 0; k < P.batch; ++k)
-        mean = welford(P, mean, S.sample[size_t(k) * wh + p], P.n_samples + k);
+        mean = welford(P, mean, S.sample[base + k], P.n_samples + k);
     write_pixel(P, p, mean.x, mean.y, mean.z, mean.w);
 }
 
@@ -468,11 +442,10 @@ void launch_path_primary(const FrameParams& P, const PathState& S, const LaunchS
             k_path_primary_persistent<MASK_ALL><<<shape.primary_grid[1], 256, 0, st>>>(P, S);
         return;
     }
-    dim3 block(16, 16);
-    dim3 grid((P.w + 15) / 16, (P.h + 15) / 16, P.batch);
+    const uint32_t n_items = primary_items(P.w, P.h, P.batch);
     auto k = pick(P, k_path_primary<2, MASK_SPHERES>, k_path_primary<2, MASK_ALL>,
                   k_path_primary<4, MASK_SPHERES>, k_path_primary<4, MASK_ALL>);
-    k<<<grid, block, 0, st>>>(P, S);
+    k<<<(n_items + 255) / 256, 256, 0, st>>>(P, S);
 }
 
 void launch_path_fold(const FrameParams& P, const PathState& S, cudaStream_t st)
