@@ -72,6 +72,7 @@ WORKLOADS = {
                    "{spp} spp x 32 light samples", "config1", 580, 580, spp=64, light_samples=32,
                    box_tests=37.41, prim_tests=1.81),
     "c4": Workload("c4", "config4", "config4", 1024, 1024, spp=16),
+    "c5": Workload("c5", "config5", "serving_scene_first", 1280, 720, spp=16),
     "c3": Workload("c3", "config3: 200k spheres + 50k bonds + 20k cubes + 10k icosahedra, "
                    "{w}x{h}, {spp} spp, 1 light sample", "config3", 1280, 720, spp=128,
                    box_tests=43.51, prim_tests=1.86, prim_bytes=28),
@@ -416,6 +417,91 @@ def run_batch_bench(args, world, rank, barrier_max, barrier_sum, clock_index):
     return 0
 
 
+def run_serving_bench(args, world, rank, barrier_max, barrier_sum, clock_index):
+    """Serving trace (config5): Poisson arrivals at 10-500 requests/s over 32 resident scenes of
+    1e3-2e6 primitives (spheres and bonds), 256^2-1080p, 1-64 spp.  The continuous-batching
+    server against the same requests served one at a time by plain Path.sample calls; both are
+    real-time (a request exists only from its arrival on) and read each image back.  Every
+    request's image is compared between the two (identical by construction)."""
+    import numpy
+
+    import fresnel_b200 as fresnel
+    from fresnel_b200 import serving, workloads
+    device = fresnel.Device(mode="gpu", n=1)
+    rates = [10.0, 50.0, 100.0, 250.0, 500.0]
+    window = 4.0  # seconds of arrivals per rate
+    _, sizes = workloads.config5(rates[0], 1)
+    t0 = time.perf_counter()
+    scenes = {k: workloads.serving_scene(device, n, seed=4000 + k) for k, n in sizes.items()}
+    for sc in scenes.values():
+        sc._scene.build()
+    device._device.synchronize()
+    setup_s = time.perf_counter() - t0
+    engine = serving.Engine(device)
+
+    def factory(k):
+        return scenes[k], workloads.serving_scene_bytes(sizes[k])
+
+    # warm-up: kernels, graph capture, tracer pools
+    warm, _ = workloads.config5(1000.0, 24)
+    serving.serve_trace(serving.RenderServer(engine, factory), warm, realtime=False)
+    serving.plain_trace(engine, lambda k: scenes[k], workloads.config5(1000.0, 24)[0],
+                        realtime=False)
+
+    results = []
+    launches = 0
+    top = None
+    with ClockSampler(clock_index) as clk:
+        for rate in rates:
+            n = int(min(400, max(40, round(rate * window))))
+            reqs, _ = workloads.config5(rate, n)
+            srv = serving.RenderServer(engine, factory, hbm_budget=120e9)
+            srv.reserve_tracers({res: 12 for res in workloads.SERVING_RESOLUTIONS})
+            serving.serve_trace(srv, reqs)
+            launches += int(srv.batch.stats["kernel_launches"])
+            alone, _ = workloads.config5(rate, n)
+            serving.plain_trace(engine, lambda k: scenes[k], alone)
+            same = sum(int(numpy.array_equal(a.image, b.image)) for a, b in zip(reqs, alone))
+            row = {"rate_per_s": rate, "requests": n, "served": serving.latency_summary(reqs),
+                   "plain": serving.latency_summary(alone), "identical_images": same,
+                   "steps": srv.steps,
+                   "image_bytes": int(sum(r.image.nbytes for r in reqs))}
+            row["served_over_plain_throughput"] = (row["served"]["mrays_per_s"] /
+                                                   max(row["plain"]["mrays_per_s"], 1e-9))
+            row["plain_over_served_p99"] = row["plain"]["p99_ms"] / row["served"]["p99_ms"]
+            results.append(row)
+            top = row
+    if rank == 0:
+        sv, pl = top["served"], top["plain"]
+        line = {
+            "metric": "serving (c5): Mrays/s and p50/p99 time-to-image, continuous batching vs "
+                      "plain", "value": sv["mrays_per_s"], "unit": "Mrays/s",
+            "n_gpus": world, "steps": len(rates), "warmup": 1,
+            "ms_per_step": sv["span_s"] * 1e3 / sv["requests"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": "config5: Poisson arrivals at 10-500 requests/s, 32 resident "
+                                   "scenes of 1e3-2e6 primitives (80% spheres, 20% bonds), "
+                                   "256^2/640x480/1280x720/1920x1080, 1-64 spp, HBM budget "
+                                   "120 GB", "rates": rates, "window_s": window,
+                       "scene_primitives": int(sum(sizes.values())),
+                       "scene_setup_s": setup_s, "parallelism": f"replicas{world}",
+                       "l2": "inputs larger than L2 (32 resident scenes)"},
+            "p50_ms": sv["p50_ms"], "p99_ms": sv["p99_ms"],
+            "plain": {"mrays_per_s": pl["mrays_per_s"], "p50_ms": pl["p50_ms"],
+                      "p99_ms": pl["p99_ms"]},
+            "rates": results,
+            "gpu_launches": launches,
+            "roofline": None,
+            "clocks": clk.summary(),
+            "e2e": {"value": sv["mrays_per_s"], "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": int(top["image_bytes"] / top["requests"]),
+                    "note": "the served path is end to end: requests in, sRGB images read back"},
+            "cpu_baseline": None,
+        }
+        print(json.dumps(line))
+    return 0
+
+
 def main():
     args, wl = parse()
     world, rank, local = dist_init()
@@ -449,9 +535,10 @@ def main():
         pg.all_reduce(t, op=pg.ReduceOp.SUM)
         return float(t.item())
 
-    if wl.key == "c4":
-        rc = run_batch_bench(args, world, rank, barrier_max, barrier_sum,
-                             int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0))
+    if wl.key in ("c4", "c5"):
+        run = run_batch_bench if wl.key == "c4" else run_serving_bench
+        rc = run(args, world, rank, barrier_max, barrier_sum,
+                 int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0))
         if pg is not None:
             pg.barrier()
             pg.destroy_process_group()

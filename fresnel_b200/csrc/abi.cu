@@ -158,6 +158,7 @@ struct fr_device {
     std::vector<fr_scene*> scenes;         // to mark BVHs stale when a build option changes
     void* static_path = nullptr;           // this device's copy of g_static_path (looked up once)
     PathBuffers path;                      // wavefront state shared by the device's tracers
+    uint32_t* h_count = nullptr;           // pinned word for queue-length readbacks
     const fr_tracer* path_owner = nullptr; // tracer of the last path render in `path`
     uint32_t path_k = 0;                   // samples per pixel of that render's last wavefront
 };
@@ -229,7 +230,6 @@ struct fr_tracer {
     DevArray<uint32_t> srgb;
     DevArray<uint2> preview_hits;
     DevArray<unsigned long long> stats;
-    uint32_t* h_count = nullptr;  // pinned
     uint64_t launches = 0;
     uint64_t builds = 0;
     double build_ms = 0.0;
@@ -649,6 +649,8 @@ fr_status fr_device_create(int n, fr_device** out)
         e = d->status.reserve(1);
     if (e == cudaSuccess)
         e = cudaMemset(d->status.ptr, 0, sizeof(uint32_t));
+    if (e == cudaSuccess)
+        e = cudaMallocHost((void**)&d->h_count, 4 * sizeof(uint32_t));
     if (e != cudaSuccess) {
         delete d;
         return cuda_fail(e, "creating the device");
@@ -671,6 +673,8 @@ fr_status fr_device_destroy(fr_device* d)
     for (int k = 0; k < 2; ++k)
         if (d->timer[k])
             cudaEventDestroy(d->timer[k]);
+    if (d->h_count)
+        cudaFreeHost(d->h_count);
     delete d;
     return FR_OK;
 }
@@ -739,6 +743,11 @@ fr_status fr_device_set_option(fr_device* d, const char* name, double value)
             return fail(FR_ERR_INVALID, "c_trav must be in (0, 100)");
         tree = d->build.c_trav != float(value);
         d->build.c_trav = float(value);
+    } else if (n == "builder") {
+        if (value != 0.0 && value != 1.0)
+            return fail(FR_ERR_INVALID, "builder must be 0 (LBVH) or 1 (PLOC)");
+        tree = d->build.builder != int(value);
+        d->build.builder = int(value);
     } else if (n == "persistent") {
         if (value != 0.0 && value != 1.0)
             return fail(FR_ERR_INVALID, "persistent must be 0 or 1");
@@ -771,6 +780,8 @@ fr_status fr_device_get_option(const fr_device* d, const char* name, double* val
         *value = d->build.c_trav;
     else if (n == "path_slots")
         *value = double(d->path_slots);
+    else if (n == "builder")
+        *value = d->build.builder;
     else if (n == "persistent")
         *value = d->persistent;
     else
@@ -1056,14 +1067,11 @@ fr_status fr_tracer_create(fr_device* dev, uint32_t w, uint32_t h, fr_tracer** o
     cudaError_t e = t->stats.reserve(8);
     if (e == cudaSuccess)
         e = cudaMemsetAsync(t->stats.ptr, 0, 8 * sizeof(unsigned long long), dev->stream);
-    if (e == cudaSuccess)
-        e = cudaMallocHost((void**)&t->h_count, 4 * sizeof(uint32_t));
     if (e != cudaSuccess) {
         delete t;
         return cuda_fail(e, "creating a tracer");
     }
     if ((s = alloc_outputs(t, w, h)) != FR_OK) {
-        cudaFreeHost(t->h_count);
         delete t;
         return s;
     }
@@ -1077,8 +1085,6 @@ fr_status fr_tracer_destroy(fr_tracer* t)
         return FR_OK;
     cudaSetDevice(t->dev->ordinal);
     cudaStreamSynchronize(t->dev->stream);
-    if (t->h_count)
-        cudaFreeHost(t->h_count);
     if (t->dev->path_owner == t)
         t->dev->path_owner = nullptr;
     delete t;
@@ -1164,12 +1170,12 @@ fr_status fr_tracer_render_path(fr_tracer* t, fr_scene* sc, const fr_render_para
                 t->launches += 2;
             }
             FR_CUDA(cudaGetLastError(), "launching the path tracer");
-            FR_CUDA(cudaMemcpyAsync(t->h_count, S.ctr + ((it - 1) & 1), sizeof(uint32_t),
+            FR_CUDA(cudaMemcpyAsync(t->dev->h_count, S.ctr + ((it - 1) & 1), sizeof(uint32_t),
                                     cudaMemcpyDeviceToHost, st),
                     "reading the queue length");
             FR_CUDA(cudaStreamSynchronize(st), "path tracer");
             t->collect();
-            if (*t->h_count == 0)
+            if (*t->dev->h_count == 0)
                 break;
             if (it >= MAX_ITER)
                 return fail(FR_ERR_DEVICE_LIMIT, "path tracer exceeded the bounce iteration cap");
@@ -1300,11 +1306,11 @@ fr_status fr_tracer_render_path_static(fr_tracer* t, fr_scene* sc, const fr_rend
                 t->launches += 2;
             }
             FR_CUDA(cudaGetLastError(), "launching the path tracer");
-            FR_CUDA(cudaMemcpyAsync(t->h_count, S.ctr + ((it - 1) & 1), sizeof(uint32_t),
+            FR_CUDA(cudaMemcpyAsync(t->dev->h_count, S.ctr + ((it - 1) & 1), sizeof(uint32_t),
                                     cudaMemcpyDeviceToHost, st),
                     "reading the queue length");
             FR_CUDA(cudaStreamSynchronize(st), "path tracer");
-            if (*t->h_count == 0)
+            if (*t->dev->h_count == 0)
                 break;
             if (it >= MAX_ITER)
                 return fail(FR_ERR_DEVICE_LIMIT, "path tracer exceeded the bounce iteration cap");

@@ -539,6 +539,214 @@ __global__ void k_collapse4(const float4* nodes2, uint32_t n_nodes2, const uint2
                        __uint_as_float(cnt[3]));
 }
 
+// ---------------------------------------------------------------------------------------------
+// PLOC: parallel locally-ordered clustering (Meister & Bittner, "Parallel Locally-Ordered
+// Clustering for Bounding Volume Hierarchy Construction", IEEE TVCG 2018).  Clusters start as
+// the primitives in Morton order; each round every cluster finds, among the PLOC_R clusters on
+// either side in the current order, the one whose union box has the smallest surface area;
+// mutual nearest neighbours merge into a new node that takes the lower one's place, and the
+// array is compacted.  Ties are broken by (area, index distance, parity of the lower index,
+// lower index), a total order on pairs, so the globally closest pair is always mutual and every
+// round merges; the parity rule pairs (0,1), (2,3), ... when many boxes are equal (coincident
+// primitives), so such runs still halve every round.  Because a new node is
+// only made from two finished clusters, its surface-area cost and the leaf-collapse decision
+// (as in k_refit) are taken when it is created.
+// ---------------------------------------------------------------------------------------------
+constexpr int PLOC_R = 16;
+
+__global__ void k_ploc_init(uint32_t n, const uint32_t* sorted_vals, const float4* box_lo,
+                            const float4* box_hi, float4* nlo, float4* nhi, uint32_t* ncount,
+                            uint8_t* ncol, uint32_t* cid, float c_isect)
+{
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n)
+        return;
+    uint32_t p = sorted_vals[s];
+    float4 lo = box_lo[p], hi = box_hi[p];
+    float a = half_area(make_float3(lo.x, lo.y, lo.z), make_float3(hi.x, hi.y, hi.z));
+    nlo[s] = make_float4(lo.x, lo.y, lo.z, c_isect * a);  // w: surface-area cost
+    nhi[s] = make_float4(hi.x, hi.y, hi.z, 0.0f);
+    ncount[s] = 1u;
+    ncol[s] = 1u;
+    cid[s] = s;
+}
+
+__global__ void __launch_bounds__(256) k_ploc_nn(uint32_t m, const uint32_t* cid,
+                                                 const float4* nlo, const float4* nhi,
+                                                 uint32_t* nn)
+{
+    __shared__ float3 slo[256 + 2 * PLOC_R], shi[256 + 2 * PLOC_R];
+    const int b0 = int(blockIdx.x * 256u);
+    for (int t = int(threadIdx.x); t < 256 + 2 * PLOC_R; t += 256) {
+        int g = b0 - PLOC_R + t;
+        if (g >= 0 && g < int(m)) {
+            uint32_t c = cid[g];
+            float4 lo = nlo[c], hi = nhi[c];
+            slo[t] = make_float3(lo.x, lo.y, lo.z);
+            shi[t] = make_float3(hi.x, hi.y, hi.z);
+        }
+    }
+    __syncthreads();
+    const int i = b0 + int(threadIdx.x);
+    if (i >= int(m))
+        return;
+    const int li = int(threadIdx.x) + PLOC_R;
+    const float3 lo = slo[li], hi = shi[li];
+    float best = __int_as_float(0x7f800000);
+    int bj = -1, bd = 0, bmn = 0;
+    for (int d = 1; d <= PLOC_R; ++d) {
+#pragma unroll
+        for (int sgn = -1; sgn <= 1; sgn += 2) {
+            const int j = i + sgn * d;
+            if (j < 0 || j >= int(m))
+                continue;
+            const int lj = li + sgn * d;
+            float a = half_area(f3min(lo, slo[lj]), f3max(hi, shi[lj]));
+            if (!(a == a))
+                a = __int_as_float(0x7f800000);
+            const int mn = min(i, j);
+            bool better = bj < 0 || a < best;
+            if (!better && a == best) {
+                if (d != bd)
+                    better = d < bd;
+                else if ((mn & 1) != (bmn & 1))
+                    better = (mn & 1) < (bmn & 1);
+                else
+                    better = mn < bmn;
+            }
+            if (better) {
+                best = a;
+                bj = j;
+                bd = d;
+                bmn = mn;
+            }
+        }
+    }
+    nn[i] = bj < 0 ? uint32_t(i) : uint32_t(bj);
+}
+
+// flags: high word 1 if the cluster leads a merge (mutual pair, lower index), low word 1 if a
+// cluster survives at this index (a leader's new node, or an unmerged cluster)
+__global__ void k_ploc_flags(uint32_t m, const uint32_t* nn, unsigned long long* flags)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m)
+        return;
+    uint32_t j = nn[i];
+    bool mutual = j != i && j < m && nn[j] == i;
+    bool lead = mutual && i < j;
+    bool keep = !mutual || i < j;
+    flags[i] = ((unsigned long long)(lead ? 1u : 0u) << 32) | (keep ? 1ull : 0ull);
+}
+
+__global__ void k_ploc_merge(uint32_t m, const uint32_t* cid, const uint32_t* nn,
+                             const unsigned long long* flags, const unsigned long long* prefix,
+                             uint32_t next, uint32_t node_cap, float4* nlo, float4* nhi,
+                             uint2* nchild, uint32_t* ncount, uint8_t* ncol, uint32_t* cid_out,
+                             int leaf_max, float c_trav, float c_isect, uint32_t* status)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m)
+        return;
+    const unsigned long long f = flags[i], pre = prefix[i];
+    const uint32_t out = uint32_t(pre & 0xffffffffull);
+    if (f >> 32) {
+        const uint32_t k = next + uint32_t(pre >> 32);
+        if (k >= node_cap || out >= m) {
+            atomicOr(status, ERR_BUILD);
+            return;
+        }
+        const uint32_t a = cid[i], b = cid[nn[i]];
+        const float4 la = nlo[a], ha = nhi[a], lb = nlo[b], hb = nhi[b];
+        const float3 lo = f3min(make_float3(la.x, la.y, la.z), make_float3(lb.x, lb.y, lb.z));
+        const float3 hi = f3max(make_float3(ha.x, ha.y, ha.z), make_float3(hb.x, hb.y, hb.z));
+        const float area = half_area(lo, hi);
+        const uint32_t count = ncount[a] + ncount[b];
+        const float split_cost = c_trav * area + la.w + lb.w;
+        const float leaf_cost = c_isect * area * float(count);
+        const bool col = count <= uint32_t(leaf_max) && leaf_cost <= split_cost;
+        nlo[k] = make_float4(lo.x, lo.y, lo.z, col ? leaf_cost : split_cost);
+        nhi[k] = make_float4(hi.x, hi.y, hi.z, 0.0f);
+        nchild[k] = make_uint2(a, b);
+        ncount[k] = count;
+        ncol[k] = col ? 1u : 0u;
+        cid_out[out] = k;
+    } else if (f & 1ull) {
+        if (out >= m) {
+            atomicOr(status, ERR_BUILD);
+            return;
+        }
+        cid_out[out] = cid[i];
+    }
+}
+
+// Top-down emission into the compacted binary layout (children of an interior node adjacent,
+// leaves naming a run of leaf slots), one tree level per launch.  Queue items: (node, output
+// slot, first leaf slot).  A leaf of the output tree (a primitive, or a collapsed subtree) lists
+// its primitives left to right into leaf_vals.
+__global__ void k_ploc_emit(uint32_t n, const uint4* in_q, const uint32_t* in_count, uint4* out_q,
+                            uint32_t* out_count, uint32_t* node_counter, uint32_t node_cap,
+                            const float4* nlo, const float4* nhi, const uint2* nchild,
+                            const uint32_t* ncount, const uint8_t* ncol,
+                            const uint32_t* sorted_vals, uint32_t* leaf_vals, float4* nodes,
+                            uint32_t* status)
+{
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= *in_count)
+        return;
+    const uint4 q = in_q[t];
+    const uint32_t k = q.x, slot = q.y, off = q.z;
+    if (k >= 2 * n - 1 || slot >= node_cap) {
+        atomicOr(status, ERR_BUILD);
+        return;
+    }
+    const float4 lo = nlo[k], hi = nhi[k];
+    const uint32_t cnt = ncount[k];
+    if (k < n || ncol[k]) {
+        if (off > n || cnt > n - off) {
+            atomicOr(status, ERR_BUILD);
+            return;
+        }
+        write_node(nodes, slot, lo, hi, off, cnt);
+        uint32_t stack[32];
+        int sp = 0;
+        stack[sp++] = k;
+        uint32_t w = 0;
+        while (sp > 0) {
+            const uint32_t c = stack[--sp];
+            if (c < n) {
+                if (w < cnt)
+                    leaf_vals[off + w] = sorted_vals[c];
+                ++w;
+            } else if (c < 2 * n - 1 && sp + 2 <= 32) {
+                const uint2 ch = nchild[c];
+                stack[sp++] = ch.y;
+                stack[sp++] = ch.x;
+            } else {
+                atomicOr(status, ERR_BUILD);
+                return;
+            }
+        }
+        if (w != cnt)
+            atomicOr(status, ERR_BUILD);
+        return;
+    }
+    const uint32_t p = atomicAdd(node_counter, 2u);
+    if (p + 1u >= node_cap) {
+        atomicOr(status, ERR_BUILD);
+        return;
+    }
+    write_node(nodes, slot, lo, hi, p, 0u);
+    const uint2 ch = nchild[k];
+    const uint32_t o = atomicAdd(out_count, 2u);
+    if (o + 1u >= n) {  // a level of a binary tree over n leaves has fewer than n nodes
+        atomicOr(status, ERR_BUILD);
+        return;
+    }
+    out_q[o] = make_uint4(ch.x, p, off, 0u);
+    out_q[o + 1] = make_uint4(ch.y, p + 1u, off + ncount[ch.x], 0u);
+}
+
 inline uint32_t blocks_for(size_t n, int threads) { return uint32_t((n + threads - 1) / threads); }
 
 }  // namespace
@@ -641,7 +849,31 @@ cudaError_t build_bvh(const BuildInput& in, uint32_t n, const BuildParams& bp, B
     uint32_t* removed = L.take<uint32_t>(n);
     uint32_t* pair_index = L.take<uint32_t>(n);
     uint32_t* cbounds = L.take<uint32_t>(8);
-    uint8_t* cub_tmp = L.take<uint8_t>(sort_bytes > scan_bytes ? sort_bytes : scan_bytes);
+    // PLOC working set (only carved when that builder is selected)
+    const bool ploc = bp.builder == 1 && n >= 2;
+    const size_t nn2 = ploc ? 2 * size_t(n) : 0, nn1 = ploc ? size_t(n) : 0;
+    size_t scan64_bytes = 0;
+    if (ploc)
+        cub::DeviceScan::ExclusiveSum(nullptr, scan64_bytes, (unsigned long long*)nullptr,
+                                      (unsigned long long*)nullptr, int(n), st);
+    float4* p_lo = L.take<float4>(nn2);
+    float4* p_hi = L.take<float4>(nn2);
+    uint2* p_child = L.take<uint2>(nn2);
+    uint32_t* p_count = L.take<uint32_t>(nn2);
+    uint8_t* p_col = L.take<uint8_t>(nn2);
+    uint32_t* p_cid_a = L.take<uint32_t>(nn1);
+    uint32_t* p_cid_b = L.take<uint32_t>(nn1);
+    uint32_t* p_nn = L.take<uint32_t>(nn1);
+    unsigned long long* p_flags = L.take<unsigned long long>(nn1);
+    unsigned long long* p_prefix = L.take<unsigned long long>(nn1);
+    uint4* p_qa = L.take<uint4>(nn1);
+    uint4* p_qb = L.take<uint4>(nn1);
+    uint32_t* p_leaf_vals = L.take<uint32_t>(nn1);
+    uint32_t* p_cnt = L.take<uint32_t>(ploc ? 4 : 0);
+    size_t tmp_need = sort_bytes > scan_bytes ? sort_bytes : scan_bytes;
+    if (scan64_bytes > tmp_need)
+        tmp_need = scan64_bytes;
+    uint8_t* cub_tmp = L.take<uint8_t>(tmp_need);
     if ((e = scratch.reserve(L.bytes)) != cudaSuccess)
         return e;
     L.bind(scratch.ptr);
@@ -663,6 +895,20 @@ cudaError_t build_bvh(const BuildInput& in, uint32_t n, const BuildParams& bp, B
     FR_RELOC(removed);
     FR_RELOC(pair_index);
     FR_RELOC(cbounds);
+    FR_RELOC(p_lo);
+    FR_RELOC(p_hi);
+    FR_RELOC(p_child);
+    FR_RELOC(p_count);
+    FR_RELOC(p_col);
+    FR_RELOC(p_cid_a);
+    FR_RELOC(p_cid_b);
+    FR_RELOC(p_nn);
+    FR_RELOC(p_flags);
+    FR_RELOC(p_prefix);
+    FR_RELOC(p_qa);
+    FR_RELOC(p_qb);
+    FR_RELOC(p_leaf_vals);
+    FR_RELOC(p_cnt);
     FR_RELOC(cub_tmp);
 #undef FR_RELOC
 
@@ -680,10 +926,103 @@ cudaError_t build_bvh(const BuildInput& in, uint32_t n, const BuildParams& bp, B
     if ((e = cub::DeviceRadixSort::SortPairs(cub_tmp, tmp_bytes, keys, keys_sorted, vals,
                                              vals_sorted, int(n), 0, 63, st)) != cudaSuccess)
         return e;
+    const uint32_t* leaf_order = vals_sorted;  // leaf slot -> primitive
     if (n == 1) {
         k_single_leaf<<<1, 1, 0, st>>>(box_lo, box_hi, out.nodes.ptr);
         out.n_nodes = 1;
-    } else {
+    }
+    bool built = n == 1;
+    if (!built && ploc) {
+        const uint32_t node_cap = 2 * n - 1;
+        k_ploc_init<<<blocks_for(n, T), T, 0, st>>>(n, vals_sorted, box_lo, box_hi, p_lo, p_hi,
+                                                   p_count, p_col, p_cid_a, bp.c_isect);
+        uint32_t m = n, next = n;
+        uint32_t* cin = p_cid_a;
+        uint32_t* cout = p_cid_b;
+        bool converged = true;
+        for (int round = 0; m > 1; ++round) {
+            if (round > 1024) {
+                converged = false;
+                break;
+            }
+            k_ploc_nn<<<blocks_for(m, 256), 256, 0, st>>>(m, cin, p_lo, p_hi, p_nn);
+            k_ploc_flags<<<blocks_for(m, T), T, 0, st>>>(m, p_nn, p_flags);
+            size_t tb = tmp_need;
+            if ((e = cub::DeviceScan::ExclusiveSum(cub_tmp, tb, p_flags, p_prefix, int(m), st)) !=
+                cudaSuccess)
+                return e;
+            k_ploc_merge<<<blocks_for(m, T), T, 0, st>>>(m, cin, p_nn, p_flags, p_prefix, next,
+                                                        node_cap, p_lo, p_hi, p_child, p_count,
+                                                        p_col, cout, bp.leaf_max, bp.c_trav,
+                                                        bp.c_isect, status);
+            unsigned long long last[2];
+            if ((e = cudaMemcpyAsync(last, p_flags + (m - 1), 8, cudaMemcpyDeviceToHost, st)) !=
+                cudaSuccess)
+                return e;
+            if ((e = cudaMemcpyAsync(last + 1, p_prefix + (m - 1), 8, cudaMemcpyDeviceToHost,
+                                     st)) != cudaSuccess)
+                return e;
+            if ((e = cudaStreamSynchronize(st)) != cudaSuccess)
+                return e;
+            const uint32_t merges = uint32_t(last[0] >> 32) + uint32_t(last[1] >> 32);
+            const uint32_t kept = uint32_t(last[0] & 0xffffffffull) +
+                                  uint32_t(last[1] & 0xffffffffull);
+            if (merges == 0 || kept >= m || next + merges > node_cap) {
+                converged = false;  // no progress: build the LBVH instead
+                break;
+            }
+            next += merges;
+            m = kept;
+            uint32_t* tmp = cin;
+            cin = cout;
+            cout = tmp;
+        }
+        uint32_t root = 0;
+        if (converged &&
+            (e = cudaMemcpyAsync(&root, cin, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+            return e;
+        // emission: counters [0], [1] queue lengths, [2] output nodes
+        uint32_t init[3] = {1u, 0u, 1u};
+        if ((e = cudaMemcpyAsync(p_cnt, init, sizeof(init), cudaMemcpyHostToDevice, st)) !=
+            cudaSuccess)
+            return e;
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess)
+            return e;
+        uint4 first = make_uint4(root, 0u, 0u, 0u);
+        if ((e = cudaMemcpyAsync(p_qa, &first, sizeof(first), cudaMemcpyHostToDevice, st)) !=
+            cudaSuccess)
+            return e;
+        uint32_t jobs = converged ? 1u : 0u;
+        for (int level = 0; jobs > 0; ++level) {
+            if (level > 4096)
+                return cudaErrorUnknown;
+            uint32_t* cq_in = p_cnt + (level & 1);
+            uint32_t* cq_out = p_cnt + ((level + 1) & 1);
+            uint4* q_in = (level & 1) ? p_qb : p_qa;
+            uint4* q_out = (level & 1) ? p_qa : p_qb;
+            if ((e = cudaMemsetAsync(cq_out, 0, 4, st)) != cudaSuccess)
+                return e;
+            k_ploc_emit<<<blocks_for(jobs, T), T, 0, st>>>(n, q_in, cq_in, q_out, cq_out, p_cnt + 2,
+                                                          node_cap, p_lo, p_hi, p_child, p_count,
+                                                          p_col, vals_sorted, p_leaf_vals,
+                                                          out.nodes.ptr, status);
+            if ((e = cudaMemcpyAsync(&jobs, cq_out, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+                return e;
+            if ((e = cudaStreamSynchronize(st)) != cudaSuccess)
+                return e;
+        }
+        uint32_t n_out = 0;
+        if ((e = cudaMemcpyAsync(&n_out, p_cnt + 2, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+            return e;
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess)
+            return e;
+        if (converged) {
+            out.n_nodes = n_out < node_cap ? n_out : node_cap;
+            leaf_order = p_leaf_vals;
+            built = true;
+        }
+    }
+    if (!built) {
         // unset parents read as 0xffffffff (out of range) and are reported, never followed
         if ((e = cudaMemsetAsync(parent_int, 0xff, n * sizeof(uint32_t), st)) != cudaSuccess)
             return e;
@@ -718,7 +1057,7 @@ cudaError_t build_bvh(const BuildInput& in, uint32_t n, const BuildParams& bp, B
             return e;
         out.n_nodes = 1u + 2u * (tail[0] + tail[1]);
     }
-    k_gather<<<blocks_for(n, T), T, 0, st>>>(in, n, vals_sorted, out.leaf_data.ptr, out.order.ptr);
+    k_gather<<<blocks_for(n, T), T, 0, st>>>(in, n, leaf_order, out.leaf_data.ptr, out.order.ptr);
     if ((e = cudaGetLastError()) != cudaSuccess)
         return e;
     if (bp.width != 4) {

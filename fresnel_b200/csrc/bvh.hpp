@@ -85,6 +85,7 @@ struct BuildInput {
 };
 
 struct BuildParams {
+    int builder = 0;       // 0: LBVH (Karras hierarchy); 1: PLOC (locally-ordered clustering)
     int width = 4;         // 2: binary tree only; 4: also collapse to the 4-wide tree
     int leaf_max = 2;      // largest leaf the SAH collapse may form
     float c_trav = 1.0f;   // cost of one child-pair visit, in units of one primitive test

@@ -180,3 +180,89 @@ def config4(device, n_frames=64, seed=3):
                                lights=light.lightbox())
         frames.append((scene, res, res))
     return frames
+
+
+def near_bonds(rng, pos, n_bonds, cutoff=1.5):
+    """n_bonds pairs (i, j), i uniform, j a uniformly chosen other sphere within ``cutoff`` of i
+    (vectorised over candidates with scipy's cKDTree; spheres without a neighbour are redrawn)."""
+    from scipy.spatial import cKDTree
+    if n_bonds <= 0 or len(pos) < 2:
+        return numpy.zeros((0, 2), numpy.int64)
+    tree = cKDTree(pos)
+    k = min(3, len(pos))
+    out = []
+    have = 0
+    for _ in range(20):
+        cand = rng.integers(len(pos), size=int((n_bonds - have) * 1.5) + 16)
+        d, idx = tree.query(pos[cand], k=k, workers=-1)
+        valid = (d < cutoff) & (idx != cand[:, None]) & (idx < len(pos))
+        pick = numpy.argmax(rng.random(valid.shape) * valid, axis=1)
+        ok = valid[numpy.arange(len(cand)), pick]
+        pairs = numpy.stack([cand[ok], idx[numpy.arange(len(cand)), pick][ok]], axis=1)
+        out.append(pairs[:n_bonds - have])
+        have += len(out[-1])
+        if have >= n_bonds:
+            break
+    return numpy.concatenate(out).astype(numpy.int64)
+
+
+def serving_scene(device, n_prims, seed):
+    """A serving-request scene of ``n_prims`` primitives: 80% spheres at the mixed scene's
+    density (0.2 per unit volume) and radii (log-uniform in [0.3, 0.7]), 20% bonds (r = 0.1)
+    between neighbouring spheres; per-sphere colours, the 1M-sphere scene's material, lightbox
+    lights, perspective camera fit to the scene."""
+    rng = numpy.random.default_rng(seed)
+    ns = max(1, int(round(0.8 * n_prims)))
+    nb = max(0, int(n_prims) - ns)
+    box = (ns / 0.2) ** (1.0 / 3.0)
+    pos = rng.uniform(-box / 2, box / 2, (ns, 3)).astype(numpy.float32)
+    rad = numpy.exp(rng.uniform(math.log(0.3), math.log(0.7), ns)).astype(numpy.float32)
+    scene = Scene(device, lights=light.lightbox())
+    g = geometry.Sphere(scene, position=pos, radius=rad)
+    g.color[:] = rng.uniform(0, 1, (ns, 3)).astype(numpy.float32)
+    g.material = material.Material(roughness=0.4, metal=0.0, specular=0.5, primitive_color_mix=1.0)
+    pairs = near_bonds(rng, pos, nb)
+    if len(pairs):
+        pts = numpy.stack([pos[pairs[:, 0]], pos[pairs[:, 1]]], axis=1)
+        geometry.Cylinder(scene, points=pts, radius=0.1, color=(0.3, 0.3, 0.8))
+    scene.camera = perspective_fit(scene)
+    return scene
+
+
+def serving_scene_bytes(n_prims):
+    """Device bytes of a serving scene (arrays, leaf records, binary and 4-wide BVH nodes)."""
+    return int(160 * 0.8 * n_prims + 200 * 0.2 * n_prims) + (1 << 16)
+
+
+SERVING_RESOLUTIONS = ((256, 256), (640, 480), (1280, 720), (1920, 1080))
+
+
+def config5(rate, n_requests, n_scenes=32, seed=4):
+    """Serving trace: ``n_requests`` Poisson arrivals at ``rate`` per second.  Each request picks
+    a scene key (with probability 0.5, or once all ``n_scenes`` keys are in use, one already
+    used; else the next new key), a resolution uniformly from SERVING_RESOLUTIONS and a sample
+    count round(exp(U(0, ln 64))).  Scene key k has round(exp(U(ln 1e3, ln 2e6))) primitives,
+    the same for every rate.  Returns (requests, {key: n_prims})."""
+    from .serving import Request, log_uniform_int, poisson_arrivals
+    srng = numpy.random.default_rng(seed)
+    sizes = {k: log_uniform_int(srng, 1e3, 2e6) for k in range(n_scenes)}
+    rng = numpy.random.default_rng([seed, int(round(rate * 1000))])
+    arrivals = poisson_arrivals(rate, n_requests, rng)
+    used = []
+    out = []
+    for n, t in enumerate(arrivals):
+        if used and (len(used) == n_scenes or rng.random() < 0.5):
+            key = used[int(rng.integers(len(used)))]
+        else:
+            key = len(used)
+            used.append(key)
+        w, h = SERVING_RESOLUTIONS[int(rng.integers(len(SERVING_RESOLUTIONS)))]
+        spp = max(1, int(round(math.exp(rng.uniform(0.0, math.log(64.0))))))
+        out.append(Request(key, w, h, spp, seed=1000 + n, arrival=float(t), tag=n))
+    return out, sizes
+
+
+def serving_scene_first(device):
+    """The first scene of the serving trace (its per-ray cost stands for the trace's on the CPU)."""
+    _, sizes = config5(10.0, 1)
+    return serving_scene(device, sizes[0], seed=4000)
