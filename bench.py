@@ -310,6 +310,15 @@ def run_batch_bench(args, world, rank, barrier_max, barrier_sum, clock_index):
     frames = workloads.config4(device)
     for s, _, _ in frames:
         s._scene.build()
+    # leaf size, primary tile shape and queue depth from the autotuner, on 2-spp probes of
+    # the frame set itself; both forms below run with the chosen options
+    from fresnel_b200 import autotune
+    t0 = time.perf_counter()
+    tuner = autotune.Tuner(device, probe_spp=2, repeats=2)
+    tuned, probe_ms = tuner.tune([(s, w, h, 1) for s, w, h in frames])
+    tune_s = time.perf_counter() - t0
+    for s, _, _ in frames:
+        s._scene.build()
     plain = [fresnel.tracer.Path(device, w=w, h=h) for _, w, h in frames]
     batched = [fresnel.tracer.Path(device, w=w, h=h) for _, w, h in frames]
     for f in range(len(frames)):
@@ -391,6 +400,8 @@ def run_batch_bench(args, world, rank, barrier_max, barrier_sum, clock_index):
                                    f"scene's density, 512^2/768^2/1024^2, {spp} spp, 1 light "
                                    "sample; one PathBatch vs 64 sequential Path.sample calls",
                        "frames": len(frames), "spp": spp,
+                       "autotune": {"options": tuned, "probe_ms": probe_ms,
+                                    "settings_measured": len(tuner.log), "seconds": tune_s},
                        "spheres": int(sum(len(s.geometry[0].position[:]) for s, _, _ in frames)),
                        "pixels": int(sum(w * h for _, w, h in frames)),
                        "parallelism": f"replicas{world}",

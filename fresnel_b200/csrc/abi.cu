@@ -155,12 +155,14 @@ struct fr_device {
     bool profiling = false;
     size_t path_slots = size_t(32) << 20;  // path slots traced together
     int persistent = 0;                    // persistent traversal kernels for 4-wide trees
+    uint32_t tile_log2 = 3;                // primary work tiles of 2^tile_log2 pixels square
     std::vector<fr_scene*> scenes;         // to mark BVHs stale when a build option changes
     void* static_path = nullptr;           // this device's copy of g_static_path (looked up once)
     PathBuffers path;                      // wavefront state shared by the device's tracers
     uint32_t* h_count = nullptr;           // pinned word for queue-length readbacks
     const fr_tracer* path_owner = nullptr; // tracer of the last path render in `path`
     uint32_t path_k = 0;                   // samples per pixel of that render's last wavefront
+    uint32_t path_tile_log2 = 3;           // and its primary tile size
 };
 
 struct fr_geometry {
@@ -477,6 +479,7 @@ FrameParams frame_params(fr_tracer* tr, fr_scene* sc, const fr_render_params* p,
     if (P.type_mask != 0 && all4)
         P.bvh_width = 4;
     P.persistent = sc->dev->persistent;
+    P.tile_log2 = sc->dev->tile_log2;
     const fr_user_camera& c = p->camera;
     float f_stop = preview ? std::numeric_limits<float>::infinity() : c.f_stop;  // no depth of field in preview
     bool sample_aa = preview ? (aa_n != 1) : true;
@@ -536,13 +539,17 @@ fr_status alloc_outputs(fr_tracer* tr, uint32_t w, uint32_t h)
 }
 
 // Path slots per sample of a w x h image: the pixels of its 8x8 tiles (edge tiles padded).
-size_t padded_pixels(uint32_t w, uint32_t h) { return size_t((w + 7) / 8) * ((h + 7) / 8) * 64; }
+size_t padded_pixels(uint32_t w, uint32_t h, uint32_t tl)
+{
+    const size_t t = size_t(1) << tl;
+    return ((w + t - 1) / t) * ((h + t - 1) / t) * t * t;
+}
 
 // Samples traced together: a batch of K samples of every pixel fills about
 // dev->path_slots slots (about 144 bytes each).
 uint32_t batch_size(const fr_tracer* tr, uint32_t remaining)
 {
-    size_t wh = padded_pixels(tr->w, tr->h);
+    size_t wh = padded_pixels(tr->w, tr->h, tr->dev->tile_log2);
     size_t k = tr->dev->path_slots / wh;
     if (k < 1)
         k = 1;
@@ -555,7 +562,7 @@ uint32_t batch_size(const fr_tracer* tr, uint32_t remaining)
 
 fr_status alloc_path_state(fr_tracer* tr, uint32_t batch)
 {
-    size_t n = padded_pixels(tr->w, tr->h) * batch;
+    size_t n = padded_pixels(tr->w, tr->h, tr->dev->tile_log2) * batch;
     FR_CUDA(tr->dev->path.reserve(n), "allocating the path state");
     return FR_OK;
 }
@@ -743,6 +750,10 @@ fr_status fr_device_set_option(fr_device* d, const char* name, double value)
             return fail(FR_ERR_INVALID, "c_trav must be in (0, 100)");
         tree = d->build.c_trav != float(value);
         d->build.c_trav = float(value);
+    } else if (n == "tile") {
+        if (value != 4.0 && value != 8.0 && value != 16.0)
+            return fail(FR_ERR_INVALID, "tile must be 4, 8 or 16");
+        d->tile_log2 = value == 4.0 ? 2u : value == 8.0 ? 3u : 4u;
     } else if (n == "builder") {
         if (value != 0.0 && value != 1.0)
             return fail(FR_ERR_INVALID, "builder must be 0 (LBVH) or 1 (PLOC)");
@@ -782,6 +793,8 @@ fr_status fr_device_get_option(const fr_device* d, const char* name, double* val
         *value = double(d->path_slots);
     else if (n == "builder")
         *value = d->build.builder;
+    else if (n == "tile")
+        *value = double(1u << d->tile_log2);
     else if (n == "persistent")
         *value = d->persistent;
     else
@@ -1183,6 +1196,7 @@ fr_status fr_tracer_render_path(fr_tracer* t, fr_scene* sc, const fr_render_para
         launch_path_fold(P, S, st);
         t->launches++;
         t->dev->path_k = P.batch;
+        t->dev->path_tile_log2 = P.tile_log2;
         done += P.batch;
     }
     return check_status(t->dev);
@@ -1256,13 +1270,13 @@ fr_status fr_tracer_render_path_static(fr_tracer* t, fr_scene* sc, const fr_rend
         return fail(FR_ERR_INVALID, "light_samples must be positive");
     if (first_sample == 0)
         return fail(FR_ERR_INVALID, "sample numbers start at 1");
-    const size_t wh = padded_pixels(t->w, t->h);
+    const size_t wh = padded_pixels(t->w, t->h, t->dev->tile_log2);
     if (wh > kStaticSlots)
         return fail(FR_ERR_INVALID, "image of " + std::to_string(t->w) + "x" +
                                         std::to_string(t->h) +
                                         " pixels exceeds the allocation-free render's limit of " +
                                         std::to_string(kStaticSlots) +
-                                        " pixels (counted in whole 8x8 tiles)");
+                                        " pixels (counted in whole primary tiles)");
     for (fr_geometry* g : sc->geoms)
         if (!g->removed && g->bvh_dirty)
             return fail(FR_ERR_STATE, "the allocation-free render needs a built scene: call "
@@ -1445,7 +1459,8 @@ fr_status fr_tracer_read_primary_hits(fr_tracer* t, uint32_t* host, size_t nbyte
     if (nbytes != n * sizeof(uint2))
         return fail(FR_ERR_INVALID, "primary hit buffer size mismatch");
     const size_t K = t->dev->path_k;
-    const size_t slots = padded_pixels(t->w, t->h) * K;
+    const uint32_t tl = t->dev->path_tile_log2;
+    const size_t slots = padded_pixels(t->w, t->h, tl) * K;
     if (t->dev->path_owner != t || K == 0 || t->dev->path.prim_hit.cap < slots)
         return fail(FR_ERR_STATE, "the device's last path render was not this tracer's");
     fr_status s = use_device(t->dev);
@@ -1456,12 +1471,13 @@ fr_status fr_tracer_read_primary_hits(fr_tracer* t, uint32_t* host, size_t nbyte
                             cudaMemcpyDeviceToHost, t->dev->stream),
             "downloading primary hits");
     FR_CUDA(cudaStreamSynchronize(t->dev->stream), "downloading primary hits");
-    // sample 0 of pixel (i, j) sits at the start of the pixel's K slots in its 8x8 tile
-    const size_t tiles_x = (t->w + 7) / 8;
+    // sample 0 of pixel (i, j) sits at the start of the pixel's K slots in its tile
+    const size_t T = size_t(1) << tl, mask = T - 1;
+    const size_t tiles_x = (t->w + T - 1) / T;
     for (uint32_t j = 0; j < t->h; ++j)
         for (uint32_t i = 0; i < t->w; ++i) {
             const size_t slot =
-                (((j >> 3) * tiles_x + (i >> 3)) * 64 + ((j & 7u) << 3) + (i & 7u)) * K;
+                ((((j >> tl) * tiles_x + (i >> tl)) << (2 * tl)) + ((j & mask) << tl) + (i & mask)) * K;
             host[2 * (size_t(j) * t->w + i)] = all[slot].x;
             host[2 * (size_t(j) * t->w + i) + 1] = all[slot].y;
         }
@@ -1616,7 +1632,7 @@ fr_status fr_batch_render(fr_batch* b)
     // path-state capacity: the device's wavefront size, at least one sample of the largest image
     size_t cap = dev->path_slots;
     for (auto& it : b->items)
-        cap = std::max(cap, padded_pixels(it.tr->w, it.tr->h));
+        cap = std::max(cap, padded_pixels(it.tr->w, it.tr->h, dev->tile_log2));
 
     // plan: every item's samples go to waves in sample order, at most one slice of a tracer
     // per wave, K samples of all pixels per slice; first fit over the waves
@@ -1629,7 +1645,7 @@ fr_status fr_batch_render(fr_batch* b)
     std::vector<std::pair<const fr_tracer*, size_t>> last_wave;  // tracer -> next allowed wave
     for (size_t i = 0; i < b->items.size(); ++i) {
         const auto& it = b->items[i];
-        const size_t wh = padded_pixels(it.tr->w, it.tr->h);
+        const size_t wh = padded_pixels(it.tr->w, it.tr->h, dev->tile_log2);
         size_t min_wave = 0;
         for (auto& lw : last_wave)
             if (lw.first == it.tr)
@@ -1683,7 +1699,7 @@ fr_status fr_batch_render(fr_batch* b)
             J.slot_base = uint32_t(slot);
             J.item_base = uint32_t(item);
             J.pixel_base = uint32_t(pixel);
-            item += uint64_t(padded_pixels(it.tr->w, it.tr->h)) * sl.k;
+            item += uint64_t(padded_pixels(it.tr->w, it.tr->h, dev->tile_log2)) * sl.k;
             slot = item;
             pixel += uint64_t(it.tr->w) * it.tr->h;
             if (slot > 0xFFFFFFFFull || item > 0xFFFFFFFFull || pixel > 0xFFFFFFFFull)

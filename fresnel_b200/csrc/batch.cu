@@ -65,7 +65,7 @@ __global__ void __launch_bounds__(256) k_batch_primary(BatchDev B)
          g += stride) {
         const WaveJob& J = B.jobs[find_job<&WaveJob::item_base>(B.jobs, f0, f1, g)];
         const FrameParams& P = J.P;
-        const PrimaryItem it = primary_item(g - J.item_base, P.w, P.h, P.batch);
+        const PrimaryItem it = primary_item(g - J.item_base, P.w, P.h, P.batch, P.tile_log2);
         bool push = false;
         uint32_t slot = 0;
         if (it.valid) {
@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(256) k_batch_fold(BatchDev B)
         const FrameParams& P = J.P;
         const uint32_t lp = q - J.pixel_base;
         const uint32_t j = lp / P.w;
-        const uint32_t base = J.slot_base + pixel_slot(lp - j * P.w, j, P.w, P.batch);
+        const uint32_t base = J.slot_base + pixel_slot(lp - j * P.w, j, P.w, P.batch, P.tile_log2);
         float4 mean = P.linear[lp];
         for (uint32_t k = 0; k < P.batch; ++k)
             mean = welford(P, mean, S.sample[base + k], P.n_samples + k);

@@ -15,44 +15,53 @@ __device__ __forceinline__ float4 f4(V3 a) { return make_float4(a.x, a.y, a.z, 0
 __device__ __forceinline__ float4 f4(C3 a) { return make_float4(a.r, a.g, a.b, 0.0f); }
 __device__ __forceinline__ C3 rgb3(float4 a) { return c3(a.x, a.y, a.z); }
 
-// Work items of the primary pass: 8x8-pixel tiles in row-major order, a tile's pixels in
-// row-major order, and the K samples of a pixel innermost. A warp then traces two pixels'
-// 16 samples (K = 16) or an 8x4 block of pixels (K = 1): its rays start close together and
-// point the same way, which keeps the warp's traversal steps and node loads shared. The
-// The path state is laid out in the same order: the slot of a render's item g is g itself, so
-// the primary pass writes whole cache lines, and the queues it fills start out in slot order.
-// Slots of pixels outside the image (edge tiles) stay unused.
+// Work items of the primary pass: T x T-pixel tiles in row-major order (T = 2^tl, 8 by
+// default), a tile's pixels in row-major order, and the K samples of a pixel innermost. A warp
+// then traces two pixels' 16 samples (K = 16) or an 8x4 block of pixels (K = 1, T = 8): its
+// rays start close together and point the same way, which keeps the warp's traversal steps and
+// node loads shared. The path state is laid out in the same order: the slot of a render's item
+// g is g itself, so the primary pass writes whole cache lines, and the queues it fills start
+// out in slot order. Slots of pixels outside the image (edge tiles) stay unused.
 struct PrimaryItem {
     uint32_t i, j, k;
     bool valid;
 };
 
-__device__ __forceinline__ uint32_t primary_tiles_x(uint32_t w) { return (w + 7u) >> 3; }
-
-__host__ __device__ __forceinline__ uint32_t primary_items(uint32_t w, uint32_t h, uint32_t K)
+__host__ __device__ __forceinline__ uint32_t primary_tiles_x(uint32_t w, uint32_t tl)
 {
-    return ((w + 7u) >> 3) * ((h + 7u) >> 3) * 64u * K;
+    return (w + (1u << tl) - 1u) >> tl;
+}
+
+__host__ __device__ __forceinline__ uint32_t primary_items(uint32_t w, uint32_t h, uint32_t K,
+                                                           uint32_t tl)
+{
+    return primary_tiles_x(w, tl) * primary_tiles_x(h, tl) * (1u << (2u * tl)) * K;
 }
 
 // Slot of sample 0 of pixel (i, j); its K samples follow it.
-__device__ __forceinline__ uint32_t pixel_slot(uint32_t i, uint32_t j, uint32_t w, uint32_t K)
+__device__ __forceinline__ uint32_t pixel_slot(uint32_t i, uint32_t j, uint32_t w, uint32_t K,
+                                               uint32_t tl)
 {
-    return (((j >> 3) * primary_tiles_x(w) + (i >> 3)) * 64u + ((j & 7u) << 3) + (i & 7u)) * K;
+    const uint32_t m = (1u << tl) - 1u;
+    return ((((j >> tl) * primary_tiles_x(w, tl) + (i >> tl)) << (2u * tl)) + ((j & m) << tl) +
+            (i & m)) * K;
 }
 
-__device__ __forceinline__ PrimaryItem primary_item(uint32_t g, uint32_t w, uint32_t h, uint32_t K)
+__device__ __forceinline__ PrimaryItem primary_item(uint32_t g, uint32_t w, uint32_t h, uint32_t K,
+                                                    uint32_t tl)
 {
-    const uint32_t per_tile = 64u * K;
+    const uint32_t per_tile = (1u << (2u * tl)) * K;
     const uint32_t tile = g / per_tile;
     const uint32_t r = g - tile * per_tile;
     const uint32_t px = r / K;
-    const uint32_t tiles_x = primary_tiles_x(w);
+    const uint32_t tiles_x = primary_tiles_x(w, tl);
     const uint32_t ty = tile / tiles_x;
     const uint32_t tx = tile - ty * tiles_x;
+    const uint32_t m = (1u << tl) - 1u;
     PrimaryItem it;
     it.k = r - px * K;
-    it.i = tx * 8u + (px & 7u);
-    it.j = ty * 8u + (px >> 3);
+    it.i = (tx << tl) + (px & m);
+    it.j = (ty << tl) + (px >> tl);
     it.valid = it.i < w && it.j < h;
     return it;
 }
@@ -89,7 +98,7 @@ __device__ __forceinline__ float4 welford(const FrameParams& P, float4 old, floa
 __device__ __forceinline__ bool shade_pixel(const FrameParams& P, const PathState& S, uint32_t p,
                                             uint32_t local)
 {
-    const PrimaryItem pi = primary_item(local, P.w, P.h, P.batch);
+    const PrimaryItem pi = primary_item(local, P.w, P.h, P.batch, P.tile_log2);
     const uint32_t k = pi.k;
     const uint32_t pixel = pi.j * P.w + pi.i;
     const uint32_t n_samples = P.n_samples + k;

@@ -29,11 +29,11 @@ template <int WIDTH, uint32_t MASK>
 __global__ void __launch_bounds__(256) k_path_primary(FrameParams P, PathState S)
 {
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t n_items = primary_items(P.w, P.h, P.batch);
+    const uint32_t n_items = primary_items(P.w, P.h, P.batch, P.tile_log2);
     PrimaryItem it;
     it.valid = false;
     if (g < n_items)
-        it = primary_item(g, P.w, P.h, P.batch);
+        it = primary_item(g, P.w, P.h, P.batch, P.tile_log2);
     bool push = false;
     uint32_t slot = 0;
     TraceCount tc;
@@ -110,7 +110,7 @@ struct PrimarySource {
     uint32_t slot;
     __device__ bool begin(uint32_t item, LaneRay& L)
     {
-        const PrimaryItem it = primary_item(item, P.w, P.h, P.batch);
+        const PrimaryItem it = primary_item(item, P.w, P.h, P.batch, P.tile_log2);
         if (!it.valid)
             return false;
         slot = item;
@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(256) k_path_primary_persistent(FrameParams P, 
     PrimarySource src{P, S, 0u};
     TraceCount tc;
     uint32_t n_rays = 0;
-    persistent_trace<MASK>(P, src, primary_items(P.w, P.h, P.batch), S.ctr + 3, tc, n_rays);
+    persistent_trace<MASK>(P, src, primary_items(P.w, P.h, P.batch, P.tile_log2), S.ctr + 3, tc, n_rays);
     flush_counts(tc, P.stats + 3);
     flush_rays(P, n_rays, true);
 }
@@ -216,7 +216,7 @@ __global__ void __launch_bounds__(256) k_path_fold(FrameParams P, PathState S)
     if (p >= P.w * P.h)
         return;
     const uint32_t j = p / P.w;
-    const uint32_t base = pixel_slot(p - j * P.w, j, P.w, P.batch);
+    const uint32_t base = pixel_slot(p - j * P.w, j, P.w, P.batch, P.tile_log2);
     float4 mean = P.linear[p];
     for (uint32_t k = 0; k < P.batch; ++k)
         mean = welford(P, mean, S.sample[base + k], P.n_samples + k);
@@ -442,7 +442,7 @@ void launch_path_primary(const FrameParams& P, const PathState& S, const LaunchS
             k_path_primary_persistent<MASK_ALL><<<shape.primary_grid[1], 256, 0, st>>>(P, S);
         return;
     }
-    const uint32_t n_items = primary_items(P.w, P.h, P.batch);
+    const uint32_t n_items = primary_items(P.w, P.h, P.batch, P.tile_log2);
     auto k = pick(P, k_path_primary<2, MASK_SPHERES>, k_path_primary<2, MASK_ALL>,
                   k_path_primary<4, MASK_SPHERES>, k_path_primary<4, MASK_ALL>);
     k<<<(n_items + 255) / 256, 256, 0, st>>>(P, S);

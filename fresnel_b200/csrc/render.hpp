@@ -24,6 +24,7 @@ struct FrameParams {
     uint32_t n_samples;      // 1-based sample number of the batch's first render
     uint32_t batch;          // samples traced together (slot = k * w * h + pixel)
     uint32_t light_samples;  // light paths per primary ray
+    uint32_t tile_log2;      // primary work in 2^tile_log2-pixel square tiles (path_device.cuh)
     int highlight;
     C3 hl_color;
     float4* linear;     // [h][w] running mean, linear RGBA

@@ -159,6 +159,9 @@ FR_API fr_status fr_device_timer_stop(fr_device* dev, float* ms);
  *   "path_slots"    path slots traced together by the path tracer (default 33554432)
  *   "persistent"    1: 4-wide traversal in persistent warps with per-lane refill;
  *                   0: one ray per thread (default)
+ *   "builder"       0: LBVH (Karras hierarchy, default); 1: PLOC (locally-ordered clustering)
+ *   "tile"          4, 8 (default) or 16: primary rays are traced in square pixel tiles of this
+ *                   size, the samples of a pixel in neighbouring threads
  * Setting an option marks every BVH of the device's scenes for rebuild when it changes the
  * tree.  Unknown names or out-of-range values return FR_ERR_INVALID. */
 FR_API fr_status fr_device_set_option(fr_device* dev, const char* name, double value);
@@ -261,9 +264,10 @@ FR_API fr_status fr_tracer_reset_stats(fr_tracer* tr);
  * call: a runtime that reserves the GPU's memory up front for its own pool, or a frame loop
  * that shares the GPU with other streams and cannot let a cudaFree stall them.
  *
- *  - Limit: the image may have at most FR_STATIC_PATH_SLOTS pixels (512 x 512, or any
- *    w * h <= 262144); larger images return FR_ERR_INVALID.  Each wavefront traces
- *    FR_STATIC_PATH_SLOTS / (w * h) samples of every pixel (at most 4096).
+ *  - Limit: the image may have at most FR_STATIC_PATH_SLOTS pixels, counted with the image
+ *    rounded up to whole primary tiles (8 x 8 by default): 512 x 512 fits; larger images
+ *    return FR_ERR_INVALID.  Each wavefront traces FR_STATIC_PATH_SLOTS / (padded pixels)
+ *    samples of every pixel (at most 4096).
  *  - The scene must be built (fr_scene_build after its last change): a build allocates, so a
  *    scene with stale BVHs or geometry table returns FR_ERR_STATE.
  *  - The first call on each device looks up the array's address (cudaGetSymbolAddress, which
