@@ -156,6 +156,7 @@ struct fr_device {
     size_t path_slots = size_t(32) << 20;  // path slots traced together
     int persistent = 0;                    // persistent traversal kernels for 4-wide trees
     uint32_t tile_log2 = 3;                // primary work tiles of 2^tile_log2 pixels square
+    int refit = 0;                         // refit (not rebuild) trees whose primitives moved
     std::vector<fr_scene*> scenes;         // to mark BVHs stale when a build option changes
     void* static_path = nullptr;           // this device's copy of g_static_path (looked up once)
     PathBuffers path;                      // wavefront state shared by the device's tracers
@@ -182,6 +183,8 @@ struct fr_geometry {
     BvhBuffers bvh;
     bool bvh_dirty = true;
     double last_build_ms = 0.0;
+    uint32_t bvh_n = 0;      // primitives of the tree in `bvh`
+    BuildParams bvh_bp{};    // and the parameters it was built with
 
     uint32_t bvh_prims() const { return type == FR_GEOM_MESH ? n * n_faces : n; }
     DevArray<float>* field(int f, size_t& count)
@@ -234,6 +237,7 @@ struct fr_tracer {
     DevArray<unsigned long long> stats;
     uint64_t launches = 0;
     uint64_t builds = 0;
+    uint64_t refits = 0;
     double build_ms = 0.0;
     // per-kernel timing while profiling: event pairs pending readback, by kernel kind
     std::vector<cudaEvent_t> event_pool;
@@ -389,8 +393,18 @@ fr_status prepare_scene(fr_scene* sc, fr_tracer* tr)
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
         cudaEventRecord(e0, dev->stream);
-        cudaError_t e = build_bvh(in, g->bvh_prims(), dev->build, g->bvh, dev->scratch,
-                                  dev->status.ptr, dev->stream);
+        const BuildParams& bp = dev->build;
+        const bool refit = dev->refit && g->bvh.n_nodes > 0 && g->bvh_n == g->bvh_prims() &&
+                           g->bvh_bp.builder == bp.builder && g->bvh_bp.width == bp.width &&
+                           g->bvh_bp.leaf_max == bp.leaf_max && g->bvh_bp.c_trav == bp.c_trav &&
+                           g->bvh_bp.c_isect == bp.c_isect;
+        cudaError_t e = cudaErrorInvalidValue;
+        if (refit)
+            e = refit_bvh(in, g->bvh_prims(), bp, g->bvh, dev->scratch, dev->status.ptr,
+                          dev->stream);
+        if (!refit || e == cudaErrorInvalidValue)
+            e = build_bvh(in, g->bvh_prims(), bp, g->bvh, dev->scratch, dev->status.ptr,
+                          dev->stream);
         cudaEventRecord(e1, dev->stream);
         cudaEventSynchronize(e1);
         float ms = 0.0f;
@@ -413,8 +427,12 @@ fr_status prepare_scene(fr_scene* sc, fr_tracer* tr)
         }
         if (tr) {
             tr->builds++;
+            if (refit)
+                tr->refits++;
             tr->build_ms = ms;
         }
+        g->bvh_n = g->bvh_prims();
+        g->bvh_bp = bp;
         g->bvh_dirty = false;
         sc->table_dirty = true;
     }
@@ -750,6 +768,10 @@ fr_status fr_device_set_option(fr_device* d, const char* name, double value)
             return fail(FR_ERR_INVALID, "c_trav must be in (0, 100)");
         tree = d->build.c_trav != float(value);
         d->build.c_trav = float(value);
+    } else if (n == "refit") {
+        if (value != 0.0 && value != 1.0)
+            return fail(FR_ERR_INVALID, "refit must be 0 or 1");
+        d->refit = int(value);
     } else if (n == "tile") {
         if (value != 4.0 && value != 8.0 && value != 16.0)
             return fail(FR_ERR_INVALID, "tile must be 4, 8 or 16");
@@ -795,6 +817,8 @@ fr_status fr_device_get_option(const fr_device* d, const char* name, double* val
         *value = d->build.builder;
     else if (n == "tile")
         *value = double(1u << d->tile_log2);
+    else if (n == "refit")
+        *value = d->refit;
     else if (n == "persistent")
         *value = d->persistent;
     else
@@ -1441,6 +1465,7 @@ fr_status fr_tracer_get_stats(const fr_tracer* t, fr_stats* out)
     out->prim_tests = v[4];
     out->kernel_launches = t->launches;
     out->bvh_builds = t->builds;
+    out->bvh_refits = t->refits;
     out->bvh_build_ms = t->build_ms;
     out->primary_ms = t->kernel_ms[0];
     out->shade_ms = t->kernel_ms[1];
@@ -1516,6 +1541,7 @@ fr_status fr_tracer_reset_stats(fr_tracer* t)
     FR_CUDA(cudaStreamSynchronize(t->dev->stream), "clearing tracer counters");
     t->launches = 0;
     t->builds = 0;
+    t->refits = 0;
     for (int k = 0; k < 3; ++k) {
         t->kernel_ms[k] = 0.0;
         t->kernel_launches[k] = 0;

@@ -747,6 +747,87 @@ __global__ void k_ploc_emit(uint32_t n, const uint4* in_q, const uint32_t* in_co
     out_q[o + 1] = make_uint4(ch.y, p + 1u, off + ncount[ch.x], 0u);
 }
 
+// ---------------------------------------------------------------------------------------------
+// Refit: new primitive boxes in an unchanged topology (the primitives moved, their number did
+// not).  Leaves recompute their box from their primitives; each interior node is written by the
+// second of its two children to arrive (one counter per node), as in k_refit.
+// ---------------------------------------------------------------------------------------------
+__global__ void k_parents(const float4* nodes, uint32_t n_nodes, uint32_t* parent,
+                          uint32_t* status)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_nodes)
+        return;
+    if (__float_as_uint(nodes[2 * size_t(i) + 1].w) != 0u)
+        return;  // leaf
+    uint32_t a = __float_as_uint(nodes[2 * size_t(i)].w);
+    if (a == 0u || a + 1u >= n_nodes) {
+        atomicOr(status, ERR_BUILD);
+        return;
+    }
+    parent[a] = i;
+    parent[a + 1] = i;
+}
+
+__global__ void k_refit_tree(float4* nodes, uint32_t n_nodes, const uint32_t* order, uint32_t n,
+                             const float4* box_lo, const float4* box_hi, const uint32_t* parent,
+                             uint32_t* arrive, uint32_t* status)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_nodes)
+        return;
+    const float4 l0 = nodes[2 * size_t(i)], h0 = nodes[2 * size_t(i) + 1];
+    const uint32_t count = __float_as_uint(h0.w);
+    if (count == 0u)
+        return;  // interior: written by its children
+    const uint32_t first = __float_as_uint(l0.w);
+    if (first > n || count > n - first) {
+        atomicOr(status, ERR_BUILD);
+        return;
+    }
+    float3 lo = make_float3(__int_as_float(0x7f800000), __int_as_float(0x7f800000),
+                            __int_as_float(0x7f800000));
+    float3 hi = make_float3(-lo.x, -lo.y, -lo.z);
+    for (uint32_t s = first; s < first + count; ++s) {
+        const uint32_t p = order[s];
+        if (p >= n) {
+            atomicOr(status, ERR_BUILD);
+            return;
+        }
+        const float4 bl = box_lo[p], bh = box_hi[p];
+        lo = f3min(lo, make_float3(bl.x, bl.y, bl.z));
+        hi = f3max(hi, make_float3(bh.x, bh.y, bh.z));
+    }
+    __stcg(&nodes[2 * size_t(i)], make_float4(lo.x, lo.y, lo.z, l0.w));
+    __stcg(&nodes[2 * size_t(i) + 1], make_float4(hi.x, hi.y, hi.z, h0.w));
+    uint32_t node = i == 0u ? 0xFFFFFFFFu : parent[i];
+    for (int guard = 0; node != 0xFFFFFFFFu; ++guard) {
+        if (node >= n_nodes || guard > 4096) {
+            atomicOr(status, ERR_BUILD);
+            return;
+        }
+        __threadfence();
+        if (atomicAdd(arrive + node, 1u) == 0u)
+            return;
+        __threadfence();
+        const float4 nl = __ldcg(&nodes[2 * size_t(node)]);
+        const float4 nh = __ldcg(&nodes[2 * size_t(node) + 1]);
+        const uint32_t a = __float_as_uint(nl.w);
+        if (a + 1u >= n_nodes) {
+            atomicOr(status, ERR_BUILD);
+            return;
+        }
+        const float4 al = __ldcg(&nodes[2 * size_t(a)]), ah = __ldcg(&nodes[2 * size_t(a) + 1]);
+        const float4 bl = __ldcg(&nodes[2 * size_t(a + 1)]),
+                     bh = __ldcg(&nodes[2 * size_t(a + 1) + 1]);
+        const float3 ulo = f3min(make_float3(al.x, al.y, al.z), make_float3(bl.x, bl.y, bl.z));
+        const float3 uhi = f3max(make_float3(ah.x, ah.y, ah.z), make_float3(bh.x, bh.y, bh.z));
+        __stcg(&nodes[2 * size_t(node)], make_float4(ulo.x, ulo.y, ulo.z, nl.w));
+        __stcg(&nodes[2 * size_t(node) + 1], make_float4(uhi.x, uhi.y, uhi.z, nh.w));
+        node = node == 0u ? 0xFFFFFFFFu : parent[node];
+    }
+}
+
 inline uint32_t blocks_for(size_t n, int threads) { return uint32_t((n + threads - 1) / threads); }
 
 }  // namespace
@@ -1058,6 +1139,55 @@ cudaError_t build_bvh(const BuildInput& in, uint32_t n, const BuildParams& bp, B
         out.n_nodes = 1u + 2u * (tail[0] + tail[1]);
     }
     k_gather<<<blocks_for(n, T), T, 0, st>>>(in, n, leaf_order, out.leaf_data.ptr, out.order.ptr);
+    if ((e = cudaGetLastError()) != cudaSuccess)
+        return e;
+    if (bp.width != 4) {
+        out.n_nodes4 = 0;
+        return cudaSuccess;
+    }
+    return collapse4(out, scratch, status, st);
+}
+
+cudaError_t refit_bvh(const BuildInput& in, uint32_t n, const BuildParams& bp, BvhBuffers& out,
+                      Scratch& scratch, uint32_t* status, cudaStream_t st)
+{
+    if (n == 0 || out.n_nodes == 0 || out.order.cap < n || out.leaf_data.cap == 0)
+        return cudaErrorInvalidValue;
+    const int T = 256;
+    const uint32_t nn = out.n_nodes;
+    ScratchLayout L;
+    float4* box_lo = L.take<float4>(n);
+    float4* box_hi = L.take<float4>(n);
+    uint32_t* parent = L.take<uint32_t>(nn);
+    uint32_t* arrive = L.take<uint32_t>(nn);
+    uint32_t* cbounds = L.take<uint32_t>(8);
+    cudaError_t e;
+    if ((e = scratch.reserve(L.bytes)) != cudaSuccess)
+        return e;
+    L.bind(scratch.ptr);
+    box_lo = L.at(box_lo);
+    box_hi = L.at(box_hi);
+    parent = L.at(parent);
+    arrive = L.at(arrive);
+    cbounds = L.at(cbounds);
+    if ((e = cudaMemsetAsync(cbounds, 0xff, 3 * sizeof(uint32_t), st)) != cudaSuccess)
+        return e;
+    if ((e = cudaMemsetAsync(cbounds + 3, 0, 3 * sizeof(uint32_t), st)) != cudaSuccess)
+        return e;
+    uint32_t gb = blocks_for(n, T);
+    if (gb > 4096)
+        gb = 4096;
+    k_bounds<<<gb, T, 0, st>>>(in, n, box_lo, box_hi, cbounds);
+    // same leaf order: re-gather the moved primitives' records in place
+    k_gather<<<blocks_for(n, T), T, 0, st>>>(in, n, out.order.ptr, out.leaf_data.ptr,
+                                             out.order.ptr);
+    if ((e = cudaMemsetAsync(parent, 0xff, nn * sizeof(uint32_t), st)) != cudaSuccess)
+        return e;
+    if ((e = cudaMemsetAsync(arrive, 0, nn * sizeof(uint32_t), st)) != cudaSuccess)
+        return e;
+    k_parents<<<blocks_for(nn, T), T, 0, st>>>(out.nodes.ptr, nn, parent, status);
+    k_refit_tree<<<blocks_for(nn, T), T, 0, st>>>(out.nodes.ptr, nn, out.order.ptr, n, box_lo,
+                                                  box_hi, parent, arrive, status);
     if ((e = cudaGetLastError()) != cudaSuccess)
         return e;
     if (bp.width != 4) {

@@ -106,6 +106,13 @@ size_t leaf_record_float4s(int type);
 // Collapse the binary tree of `out` into its 4-wide tree (called by build_bvh).
 cudaError_t collapse4(BvhBuffers& out, Scratch& scratch, uint32_t* status, cudaStream_t st);
 
+// New boxes for a tree built by build_bvh over the same n primitives (they moved; their number
+// and the build parameters did not): primitive boxes, leaf records and every node's box are
+// recomputed bottom-up in the existing topology, then the 4-wide tree is collapsed again.
+// Returns cudaErrorInvalidValue if `out` holds no tree for n primitives.
+cudaError_t refit_bvh(const BuildInput& in, uint32_t n, const BuildParams& bp, BvhBuffers& out,
+                      Scratch& scratch, uint32_t* status, cudaStream_t st);
+
 // Build the BVH of n primitives (n == 0 leaves an empty tree).  Synchronises the stream once
 // to read back the node count.
 // Construction errors (an inconsistent hierarchy) are reported by or-ing ERR_BUILD into

@@ -477,6 +477,7 @@ struct TracerH {
         d["prim_tests"] = st.prim_tests;
         d["kernel_launches"] = st.kernel_launches;
         d["bvh_builds"] = st.bvh_builds;
+        d["bvh_refits"] = st.bvh_refits;
         d["bvh_build_ms"] = st.bvh_build_ms;
         d["primary_ms"] = st.primary_ms;
         d["shade_ms"] = st.shade_ms;

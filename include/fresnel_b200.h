@@ -122,6 +122,7 @@ typedef struct fr_stats {
     /* per-kernel device time, accumulated only while profiling is on (fr_device_set_profiling) */
     double primary_ms, shade_ms, extend_ms;
     uint64_t primary_launches, shade_launches, extend_launches;
+    uint64_t bvh_refits;    /* of bvh_builds, how many refitted an existing tree */
 } fr_stats;
 
 typedef struct fr_device fr_device;
@@ -162,6 +163,9 @@ FR_API fr_status fr_device_timer_stop(fr_device* dev, float* ms);
  *   "builder"       0: LBVH (Karras hierarchy, default); 1: PLOC (locally-ordered clustering)
  *   "tile"          4, 8 (default) or 16: primary rays are traced in square pixel tiles of this
  *                   size, the samples of a pixel in neighbouring threads
+ *   "refit"         1: when a geometry's arrays change but its primitive count and the build
+ *                   options do not, refit its tree (new boxes, same topology) instead of
+ *                   rebuilding it; 0: always rebuild, as the reference does (default)
  * Setting an option marks every BVH of the device's scenes for rebuild when it changes the
  * tree.  Unknown names or out-of-range values return FR_ERR_INVALID. */
 FR_API fr_status fr_device_set_option(fr_device* dev, const char* name, double value);
