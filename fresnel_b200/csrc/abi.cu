@@ -153,7 +153,7 @@ struct fr_device {
     DevArray<uint32_t> status;  // traversal error bits
     cudaEvent_t timer[2] = {nullptr, nullptr};
     bool profiling = false;
-    size_t path_slots = size_t(32) << 20;  // path slots traced together
+    size_t path_slots = size_t(128) << 20;  // path slots traced together (144 B each)
     int persistent = 0;                    // persistent traversal kernels for 4-wide trees
     uint32_t tile_log2 = 3;                // primary work tiles of 2^tile_log2 pixels square
     int refit = 0;                         // refit (not rebuild) trees whose primitives moved
@@ -1655,10 +1655,15 @@ fr_status fr_batch_render(fr_batch* b)
             return s;
     }
 
-    // path-state capacity: the device's wavefront size, at least one sample of the largest image
-    size_t cap = dev->path_slots;
-    for (auto& it : b->items)
-        cap = std::max(cap, padded_pixels(it.tr->w, it.tr->h, dev->tile_log2));
+    // path-state capacity: the device's wavefront size, but no more than the batch can fill,
+    // and at least one sample of its largest image
+    size_t need = 0, largest = 0;
+    for (auto& it : b->items) {
+        const size_t px = padded_pixels(it.tr->w, it.tr->h, dev->tile_log2);
+        need += px * it.n;
+        largest = std::max(largest, px);
+    }
+    size_t cap = std::max(largest, std::min(dev->path_slots, need));
 
     // plan: every item's samples go to waves in sample order, at most one slice of a tracer
     // per wave, K samples of all pixels per slice; first fit over the waves

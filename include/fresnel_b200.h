@@ -157,7 +157,8 @@ FR_API fr_status fr_device_timer_stop(fr_device* dev, float* ms);
  *   "bvh_width"     2 or 4: binary or 4-wide tree traversed by the renderers (default 4)
  *   "leaf_max"      largest leaf the SAH collapse may form (1..16, default 2)
  *   "c_trav"        SAH cost of one node visit relative to one primitive test (default 1)
- *   "path_slots"    path slots traced together by the path tracer (default 33554432)
+ *   "path_slots"    path slots traced together by the path tracer, 144 bytes each
+ *                   (default 134217728: 18.4 GB; a batch takes at most what it can fill)
  *   "persistent"    1: 4-wide traversal in persistent warps with per-lane refill;
  *                   0: one ray per thread (default)
  *   "builder"       0: LBVH (Karras hierarchy, default); 1: PLOC (locally-ordered clustering)

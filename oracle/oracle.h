@@ -5,7 +5,7 @@
  *
  * Two builds share this interface:
  *   oracle/_build/liboracle.so      restated math (oracle/restated_math.hpp)
- *   oracle/_ref/libfresnel_ref.so   the reference's own fresnel/common/*.h math
+ *   oracle/_ref/libfresnel_ref.so   the reference's own fresnel/common headers
  * Both use the same BVH, the same per-geometry hit glue (restated from
  * fresnel/cpu/Geometry*.cc) and the same tile loops (restated from fresnel/cpu/Tracer*.cc).
  */
