@@ -157,6 +157,7 @@ struct fr_device {
     int persistent = 0;                    // persistent traversal kernels for 4-wide trees
     uint32_t tile_log2 = 3;                // primary work tiles of 2^tile_log2 pixels square
     int refit = 0;                         // refit (not rebuild) trees whose primitives moved
+    int shade_blocks = 3;                  // shade kernel variant (render.hpp FrameParams)
     std::vector<fr_scene*> scenes;         // to mark BVHs stale when a build option changes
     void* static_path = nullptr;           // this device's copy of g_static_path (looked up once)
     PathBuffers path;                      // wavefront state shared by the device's tracers
@@ -498,6 +499,7 @@ FrameParams frame_params(fr_tracer* tr, fr_scene* sc, const fr_render_params* p,
         P.bvh_width = 4;
     P.persistent = sc->dev->persistent;
     P.tile_log2 = sc->dev->tile_log2;
+    P.shade_blocks = sc->dev->shade_blocks;
     const fr_user_camera& c = p->camera;
     float f_stop = preview ? std::numeric_limits<float>::infinity() : c.f_stop;  // no depth of field in preview
     bool sample_aa = preview ? (aa_n != 1) : true;
@@ -768,6 +770,10 @@ fr_status fr_device_set_option(fr_device* d, const char* name, double value)
             return fail(FR_ERR_INVALID, "c_trav must be in (0, 100)");
         tree = d->build.c_trav != float(value);
         d->build.c_trav = float(value);
+    } else if (n == "shade_blocks") {
+        if (value != 0.0 && value != 3.0 && value != 4.0)
+            return fail(FR_ERR_INVALID, "shade_blocks must be 0, 3 or 4");
+        d->shade_blocks = int(value);
     } else if (n == "refit") {
         if (value != 0.0 && value != 1.0)
             return fail(FR_ERR_INVALID, "refit must be 0 or 1");
@@ -819,6 +825,8 @@ fr_status fr_device_get_option(const fr_device* d, const char* name, double* val
         *value = double(1u << d->tile_log2);
     else if (n == "refit")
         *value = d->refit;
+    else if (n == "shade_blocks")
+        *value = d->shade_blocks;
     else if (n == "persistent")
         *value = d->persistent;
     else

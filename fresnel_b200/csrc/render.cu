@@ -223,7 +223,9 @@ __global__ void __launch_bounds__(256) k_path_fold(FrameParams P, PathState S)
     write_pixel(P, p, mean.x, mean.y, mean.z, mean.w);
 }
 
-__global__ void __launch_bounds__(256) k_path_shade(FrameParams P, PathState S, int in_q, int out_q)
+template <int MINB = 1>
+__global__ void __launch_bounds__(256, MINB) k_path_shade(FrameParams P, PathState S, int in_q,
+                                                          int out_q)
 {
     if (blockIdx.x == 0 && threadIdx.x == 0)
         S.ctr[2] = 0;  // work counter of the extend kernel that follows
@@ -419,7 +421,9 @@ template <class K> int blocks_per_sm(K kernel)
 LaunchShape path_launch_shape(int num_sms)
 {
     LaunchShape s;
-    s.shade_grid = num_sms * blocks_per_sm(k_path_shade);
+    s.shade_grid = num_sms * blocks_per_sm(k_path_shade<>);
+    s.shade_grid_occ[0] = num_sms * blocks_per_sm(k_path_shade<3>);
+    s.shade_grid_occ[1] = num_sms * blocks_per_sm(k_path_shade<4>);
     s.extend_grid[0] = num_sms * blocks_per_sm(k_path_extend<2, MASK_SPHERES>);
     s.extend_grid[1] = num_sms * blocks_per_sm(k_path_extend<2, MASK_ALL>);
     s.extend_grid[2] = num_sms * blocks_per_sm(k_path_extend<4, MASK_SPHERES>);
@@ -457,7 +461,13 @@ void launch_path_shade(const FrameParams& P, const PathState& S, int iteration,
                        const LaunchShape& shape, cudaStream_t st)
 {
     // iteration 0 reads the primary hits (queue 1); then the queues alternate
-    k_path_shade<<<shape.shade_grid, 256, 0, st>>>(P, S, (iteration + 1) & 1, iteration & 1);
+    const int in_q = (iteration + 1) & 1, out_q = iteration & 1;
+    if (P.shade_blocks == 3)
+        k_path_shade<3><<<shape.shade_grid_occ[0], 256, 0, st>>>(P, S, in_q, out_q);
+    else if (P.shade_blocks == 4)
+        k_path_shade<4><<<shape.shade_grid_occ[1], 256, 0, st>>>(P, S, in_q, out_q);
+    else
+        k_path_shade<><<<shape.shade_grid, 256, 0, st>>>(P, S, in_q, out_q);
 }
 
 void launch_path_extend(const FrameParams& P, const PathState& S, int iteration,

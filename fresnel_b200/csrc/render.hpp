@@ -25,6 +25,7 @@ struct FrameParams {
     uint32_t batch;          // samples traced together (slot = k * w * h + pixel)
     uint32_t light_samples;  // light paths per primary ray
     uint32_t tile_log2;      // primary work in 2^tile_log2-pixel square tiles (path_device.cuh)
+    int shade_blocks;        // 0: shade kernel as compiled; 3 or 4: register-limited variants
     int highlight;
     C3 hl_color;
     float4* linear;     // [h][w] running mean, linear RGBA
@@ -51,6 +52,7 @@ struct PathState {
 
 struct LaunchShape {
     int shade_grid;
+    int shade_grid_occ[2];   // shade kernel compiled for 3|4 blocks per SM
     int extend_grid[4];      // [width 2|4][spheres only|all types]
     int persistent_grid[2];  // 4-wide persistent extend kernel [spheres only|all types]
     int primary_grid[2];     // 4-wide persistent primary kernel [spheres only|all types]
