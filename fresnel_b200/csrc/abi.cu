@@ -158,6 +158,7 @@ struct fr_device {
     uint32_t tile_log2 = 3;                // primary work tiles of 2^tile_log2 pixels square
     int refit = 0;                         // refit (not rebuild) trees whose primitives moved
     int shade_blocks = 3;                  // shade kernel variant (render.hpp FrameParams)
+    int combined = 1;                      // one tree per scene of several geometries
     std::vector<fr_scene*> scenes;         // to mark BVHs stale when a build option changes
     void* static_path = nullptr;           // this device's copy of g_static_path (looked up once)
     PathBuffers path;                      // wavefront state shared by the device's tracers
@@ -183,6 +184,7 @@ struct fr_geometry {
     DevArray<float> position, radius, color, points, orientation, vertices, planes;
     BvhBuffers bvh;
     bool bvh_dirty = true;
+    uint64_t gen = 0;        // changes whenever the primitives (or the build options) change
     double last_build_ms = 0.0;
     uint32_t bvh_n = 0;      // primitives of the tree in `bvh`
     BuildParams bvh_bp{};    // and the parameters it was built with
@@ -227,6 +229,11 @@ struct fr_scene {
     std::vector<fr_geometry*> geoms;
     DevArray<GeomDev> table;
     bool table_dirty = true;
+    // one tree over the primitives of all enabled geometries (scenes of 2..MAX_PARTS of them)
+    BvhBuffers combined;
+    bool use_combined = false;
+    std::vector<uint64_t> combined_key;  // (geometry, primitives, generation) per part
+    BuildParams combined_bp{};
 };
 
 struct fr_tracer {
@@ -320,6 +327,14 @@ struct fr_batch {
 
 namespace {
 
+uint64_t g_generation = 0;  // source of fr_geometry::gen values (never repeats)
+
+void mark_moved(fr_geometry* g)
+{
+    g->bvh_dirty = true;
+    g->gen = ++g_generation;
+}
+
 fr_status use_device(const fr_device* d)
 {
     FR_CUDA(cudaSetDevice(d->ordinal), "cudaSetDevice");
@@ -370,7 +385,141 @@ fr_status finish_geometry(fr_geometry* g, fr_geometry** out)
     }
     g->scene->geoms.push_back(g);
     g->scene->table_dirty = true;
+    g->gen = ++g_generation;
     *out = g;
+    return FR_OK;
+}
+
+BuildInput build_input(const fr_geometry* g)
+{
+    BuildInput in;
+    in.type = g->type;
+    in.position = g->position.ptr;
+    in.radius = g->radius.ptr;
+    in.points = g->points.ptr;
+    in.orientation = g->orientation.ptr;
+    in.vertices = g->vertices.ptr;
+    in.n_faces = g->n_faces;
+    in.poly_radius = g->poly_radius;
+    return in;
+}
+
+bool same_params(const BuildParams& a, const BuildParams& b)
+{
+    return a.builder == b.builder && a.width == b.width && a.leaf_max == b.leaf_max &&
+           a.c_trav == b.c_trav && a.c_isect == b.c_isect;
+}
+
+// The geometries a combined tree would cover (empty if the scene traces per-geometry trees:
+// combining is off, the trees are binary, or fewer than 2 or more than MAX_PARTS geometries
+// have primitives) and the key that identifies their current contents.
+std::vector<fr_geometry*> combined_parts(const fr_scene* sc, std::vector<uint64_t>& key)
+{
+    std::vector<fr_geometry*> parts;
+    key.clear();
+    const fr_device* dev = sc->dev;
+    if (!dev->combined || dev->build.width != 4)
+        return parts;
+    for (fr_geometry* g : sc->geoms)
+        if (!g->removed && g->enabled && g->bvh_prims() > 0)
+            parts.push_back(g);
+    if (parts.size() < 2 || parts.size() > size_t(MAX_PARTS)) {
+        parts.clear();
+        return parts;
+    }
+    for (fr_geometry* g : parts) {
+        key.push_back(reinterpret_cast<uintptr_t>(g));
+        key.push_back(g->bvh_prims());
+        key.push_back(g->gen);
+    }
+    return parts;
+}
+
+// Whether prepare_scene would build anything.
+bool scene_needs_build(const fr_scene* sc)
+{
+    std::vector<uint64_t> key;
+    if (!combined_parts(sc, key).empty())
+        return !sc->use_combined || key != sc->combined_key;
+    for (fr_geometry* g : sc->geoms)
+        if (!g->removed && g->bvh_dirty)
+            return true;
+    return false;
+}
+
+fr_status check_build_status(fr_device* dev)
+{
+    uint32_t stw = 0;
+    FR_CUDA(cudaMemcpy(&stw, dev->status.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost),
+            "reading the build status");
+    if (stw & ERR_BUILD) {
+        cudaMemset(dev->status.ptr, 0, sizeof(uint32_t));
+        return fail(FR_ERR_DEVICE_LIMIT, "BVH construction produced an inconsistent tree");
+    }
+    return FR_OK;
+}
+
+// Build (or refit) the scene's combined tree over `parts`.
+fr_status build_combined(fr_scene* sc, fr_tracer* tr, const std::vector<fr_geometry*>& parts,
+                         const std::vector<uint64_t>& key)
+{
+    fr_device* dev = sc->dev;
+    PartsInput in;
+    std::memset(&in, 0, sizeof(in));
+    uint32_t n = 0;
+    in.n_parts = uint32_t(parts.size());
+    for (uint32_t p = 0; p < in.n_parts; ++p) {
+        fr_geometry* g = parts[p];
+        in.part[p] = build_input(g);
+        in.first[p] = n;
+        uint32_t gi = 0;
+        while (sc->geoms[gi] != g)
+            ++gi;
+        in.geom[p] = gi;
+        n += g->bvh_prims();
+    }
+    in.first[in.n_parts] = n;
+    const BuildParams& bp = dev->build;
+    // same geometries and counts, other contents: the topology can be kept
+    bool same_layout = sc->combined.n_nodes > 0 && sc->combined_key.size() == key.size() &&
+                       same_params(sc->combined_bp, bp);
+    for (size_t i = 0; same_layout && i < key.size(); i += 3)
+        same_layout = sc->combined_key[i] == key[i] && sc->combined_key[i + 1] == key[i + 1];
+    const bool refit = dev->refit && same_layout;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, dev->stream);
+    cudaError_t e = cudaErrorInvalidValue;
+    if (refit)
+        e = refit_bvh(in, n, bp, sc->combined, dev->scratch, dev->status.ptr, dev->stream);
+    if (!refit || e == cudaErrorInvalidValue)
+        e = build_bvh(in, n, bp, sc->combined, dev->scratch, dev->status.ptr, dev->stream);
+    cudaEventRecord(e1, dev->stream);
+    cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess)
+        return cuda_fail(e, "building a BVH");
+    fr_status s = check_build_status(dev);
+    if (s != FR_OK) {
+        sc->combined.n_nodes = 0;
+        sc->combined.n_nodes4 = 0;
+        sc->use_combined = false;
+        sc->combined_key.clear();
+        return s;
+    }
+    if (tr) {
+        tr->builds++;
+        if (refit)
+            tr->refits++;
+        tr->build_ms = ms;
+    }
+    sc->combined_key = key;
+    sc->combined_bp = bp;
+    sc->use_combined = true;
     return FR_OK;
 }
 
@@ -378,27 +527,28 @@ fr_status finish_geometry(fr_geometry* g, fr_geometry** out)
 fr_status prepare_scene(fr_scene* sc, fr_tracer* tr)
 {
     fr_device* dev = sc->dev;
+    std::vector<uint64_t> key;
+    const std::vector<fr_geometry*> parts = combined_parts(sc, key);
+    if (!parts.empty()) {
+        if (!sc->use_combined || key != sc->combined_key) {
+            fr_status s = build_combined(sc, tr, parts, key);
+            if (s != FR_OK)
+                return s;
+        }
+    } else {
+        sc->use_combined = false;
+    }
     for (fr_geometry* g : sc->geoms) {
-        if (g->removed || !g->bvh_dirty)
+        if (sc->use_combined || g->removed || !g->bvh_dirty)
             continue;
-        BuildInput in;
-        in.type = g->type;
-        in.position = g->position.ptr;
-        in.radius = g->radius.ptr;
-        in.points = g->points.ptr;
-        in.orientation = g->orientation.ptr;
-        in.vertices = g->vertices.ptr;
-        in.n_faces = g->n_faces;
-        in.poly_radius = g->poly_radius;
+        BuildInput in = build_input(g);
         cudaEvent_t e0, e1;
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
         cudaEventRecord(e0, dev->stream);
         const BuildParams& bp = dev->build;
         const bool refit = dev->refit && g->bvh.n_nodes > 0 && g->bvh_n == g->bvh_prims() &&
-                           g->bvh_bp.builder == bp.builder && g->bvh_bp.width == bp.width &&
-                           g->bvh_bp.leaf_max == bp.leaf_max && g->bvh_bp.c_trav == bp.c_trav &&
-                           g->bvh_bp.c_isect == bp.c_isect;
+                           same_params(g->bvh_bp, bp);
         cudaError_t e = cudaErrorInvalidValue;
         if (refit)
             e = refit_bvh(in, g->bvh_prims(), bp, g->bvh, dev->scratch, dev->status.ptr,
@@ -488,16 +638,33 @@ FrameParams frame_params(fr_tracer* tr, fr_scene* sc, const fr_render_params* p,
     P.scene.status = sc->dev->status.ptr;
     P.type_mask = 0;
     P.bvh_width = 2;
-    bool all4 = true;
-    for (fr_geometry* g : sc->geoms) {
-        if (!g->enabled || g->removed || g->bvh.n_nodes == 0)
-            continue;
-        P.type_mask |= 1u << g->type;
-        all4 = all4 && g->bvh.n_nodes4 > 0;
-    }
-    if (P.type_mask != 0 && all4)
-        P.bvh_width = 4;
     P.persistent = sc->dev->persistent;
+    if (sc->use_combined && sc->combined.n_nodes4 > 0) {
+        for (fr_geometry* g : sc->geoms)
+            if (g->enabled && !g->removed && g->bvh_prims() > 0)
+                P.type_mask |= 1u << g->type;
+        P.bvh_width = 4;
+        P.persistent = 0;  // the persistent kernels step through per-geometry trees
+        P.scene.n_nodes4 = sc->combined.n_nodes4;
+        uint32_t n = 0;
+        for (size_t i = 1; i < sc->combined_key.size(); i += 3)
+            n += uint32_t(sc->combined_key[i]);
+        P.scene.n_prims = n;
+        P.scene.nodes4 = sc->combined.nodes4.ptr;
+        P.scene.leaf_data = sc->combined.leaf_data.ptr;
+        P.scene.leaf_geom = sc->combined.leaf_geom.ptr;
+        P.scene.order = sc->combined.order.ptr;
+    } else {
+        bool all4 = true;
+        for (fr_geometry* g : sc->geoms) {
+            if (!g->enabled || g->removed || g->bvh.n_nodes == 0)
+                continue;
+            P.type_mask |= 1u << g->type;
+            all4 = all4 && g->bvh.n_nodes4 > 0;
+        }
+        if (P.type_mask != 0 && all4)
+            P.bvh_width = 4;
+    }
     P.tile_log2 = sc->dev->tile_log2;
     P.shade_blocks = sc->dev->shade_blocks;
     const fr_user_camera& c = p->camera;
@@ -770,6 +937,11 @@ fr_status fr_device_set_option(fr_device* d, const char* name, double value)
             return fail(FR_ERR_INVALID, "c_trav must be in (0, 100)");
         tree = d->build.c_trav != float(value);
         d->build.c_trav = float(value);
+    } else if (n == "combined") {
+        if (value != 0.0 && value != 1.0)
+            return fail(FR_ERR_INVALID, "combined must be 0 or 1");
+        tree = d->combined != int(value);
+        d->combined = int(value);
     } else if (n == "shade_blocks") {
         if (value != 0.0 && value != 3.0 && value != 4.0)
             return fail(FR_ERR_INVALID, "shade_blocks must be 0, 3 or 4");
@@ -801,7 +973,7 @@ fr_status fr_device_set_option(fr_device* d, const char* name, double value)
     if (tree)
         for (fr_scene* sc : d->scenes)
             for (fr_geometry* g : sc->geoms)
-                g->bvh_dirty = true;
+                mark_moved(g);
     return FR_OK;
 }
 
@@ -827,6 +999,8 @@ fr_status fr_device_get_option(const fr_device* d, const char* name, double* val
         *value = d->refit;
     else if (n == "shade_blocks")
         *value = d->shade_blocks;
+    else if (n == "combined")
+        *value = d->combined;
     else if (n == "persistent")
         *value = d->persistent;
     else
@@ -1015,7 +1189,7 @@ fr_status fr_geometry_write(fr_geometry* g, int field, const void* host, size_t 
             "uploading a geometry array");
     FR_CUDA(cudaStreamSynchronize(g->scene->dev->stream), "uploading a geometry array");
     if (field != FR_FIELD_COLOR)
-        g->bvh_dirty = true;  // colours do not move primitives
+        mark_moved(g);  // colours do not move primitives
     return FR_OK;
 }
 
@@ -1090,7 +1264,7 @@ fr_status fr_geometry_set_color_by_face(fr_geometry* g, float f)
 fr_status fr_geometry_update(fr_geometry* g)
 {
     FR_CHECK_NULL(g);
-    g->bvh_dirty = true;
+    mark_moved(g);
     return FR_OK;
 }
 
@@ -1309,10 +1483,9 @@ fr_status fr_tracer_render_path_static(fr_tracer* t, fr_scene* sc, const fr_rend
                                         " pixels exceeds the allocation-free render's limit of " +
                                         std::to_string(kStaticSlots) +
                                         " pixels (counted in whole primary tiles)");
-    for (fr_geometry* g : sc->geoms)
-        if (!g->removed && g->bvh_dirty)
-            return fail(FR_ERR_STATE, "the allocation-free render needs a built scene: call "
-                                      "fr_scene_build after changing geometry");
+    if (scene_needs_build(sc))
+        return fail(FR_ERR_STATE, "the allocation-free render needs a built scene: call "
+                                  "fr_scene_build after changing geometry");
     if (sc->table_dirty)
         return fail(FR_ERR_STATE, "the allocation-free render needs a built scene: call "
                                   "fr_scene_build after changing geometry");

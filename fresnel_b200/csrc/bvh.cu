@@ -106,6 +106,21 @@ __device__ Box prim_bounds(const BuildInput& in, uint32_t i)
     return inflate(b);
 }
 
+// Part of combined primitive i (the last part whose first index is <= i).
+__device__ __forceinline__ uint32_t part_of(const PartsInput& in, uint32_t i)
+{
+    uint32_t p = 0;
+    while (p + 1u < in.n_parts && i >= in.first[p + 1])
+        ++p;
+    return p;
+}
+
+__device__ Box prim_bounds(const PartsInput& in, uint32_t i)
+{
+    const uint32_t p = part_of(in, i);
+    return prim_bounds(in.part[p], i - in.first[p]);
+}
+
 // float <-> order-preserving uint32 for atomic min/max of the centroid bounds
 __device__ __forceinline__ uint32_t f2o(float f)
 {
@@ -117,8 +132,8 @@ __device__ __forceinline__ float o2f(uint32_t u)
     return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
 }
 
-__global__ void k_bounds(BuildInput in, uint32_t n, float4* box_lo, float4* box_hi,
-                         uint32_t* cbounds)
+template <class In>
+__global__ void k_bounds(In in, uint32_t n, float4* box_lo, float4* box_hi, uint32_t* cbounds)
 {
     uint32_t lmin[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, lmax[3] = {0u, 0u, 0u};
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -388,43 +403,85 @@ __global__ void k_single_leaf(const float4* box_lo, const float4* box_hi, float4
     write_node(nodes, 0, box_lo[0], box_hi[0], 0u, 1u);
 }
 
-// Leaf-ordered copies of the primitive data the intersection loop reads.
-__global__ void k_gather(BuildInput in, uint32_t n, const uint32_t* sorted_vals, float4* leaf_data,
-                         uint32_t* order)
+// The record the intersection loop reads for primitive p, written at r (1 float4 for a sphere,
+// 2 for the other types).
+__device__ __forceinline__ void write_record(const BuildInput& in, uint32_t p, float4* r)
 {
-    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n)
-        return;
-    uint32_t p = sorted_vals[s];
-    order[s] = p;
     switch (in.type) {
     case FR_GEOM_SPHERE: {
         V3 c = load3(in.position, p);
-        leaf_data[s] = make_float4(c.x, c.y, c.z, in.radius[p]);
+        r[0] = make_float4(c.x, c.y, c.z, in.radius[p]);
         break;
     }
     case FR_GEOM_CYLINDER: {
         V3 A = load3(in.points, 2 * p), B = load3(in.points, 2 * p + 1);
-        leaf_data[2 * s] = make_float4(A.x, A.y, A.z, in.radius[p]);
-        leaf_data[2 * s + 1] = make_float4(B.x, B.y, B.z, 0.0f);
+        r[0] = make_float4(A.x, A.y, A.z, in.radius[p]);
+        r[1] = make_float4(B.x, B.y, B.z, 0.0f);
         break;
     }
     case FR_GEOM_POLYHEDRON: {
         V3 c = load3(in.position, p);
         Qt q = loadq(in.orientation, p);
-        leaf_data[2 * s] = make_float4(c.x, c.y, c.z, 0.0f);
-        leaf_data[2 * s + 1] = make_float4(q.s, q.v.x, q.v.y, q.v.z);
+        r[0] = make_float4(c.x, c.y, c.z, 0.0f);
+        r[1] = make_float4(q.s, q.v.x, q.v.y, q.v.z);
         break;
     }
     default: {
         uint32_t inst = p / in.n_faces, face = p - inst * in.n_faces;
         V3 c = load3(in.position, inst);
         Qt q = loadq(in.orientation, inst);
-        leaf_data[2 * s] = make_float4(c.x, c.y, c.z, __uint_as_float(face));
-        leaf_data[2 * s + 1] = make_float4(q.s, q.v.x, q.v.y, q.v.z);
+        r[0] = make_float4(c.x, c.y, c.z, __uint_as_float(face));
+        r[1] = make_float4(q.s, q.v.x, q.v.y, q.v.z);
         break;
     }
     }
+}
+
+// Leaf-ordered copies of the primitive data the intersection loop reads.
+__global__ void k_gather(BuildInput in, uint32_t n, const uint32_t* sorted_vals, float4* leaf_data,
+                         uint32_t* order, uint32_t* /*leaf_geom*/)
+{
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n)
+        return;
+    uint32_t p = sorted_vals[s];
+    order[s] = p;
+    write_record(in, p, leaf_data + (in.type == FR_GEOM_SPHERE ? s : 2 * size_t(s)));
+}
+
+// Combined trees: sorted_vals holds combined indices; order gets the index within the geometry.
+__global__ void k_gather(PartsInput in, uint32_t n, const uint32_t* sorted_vals,
+                         float4* leaf_data, uint32_t* order, uint32_t* leaf_geom)
+{
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n)
+        return;
+    const uint32_t g = sorted_vals[s];
+    const uint32_t p = part_of(in, g);
+    const uint32_t local = g - in.first[p];
+    order[s] = local;
+    leaf_geom[s] = in.geom[p];
+    write_record(in.part[p], local, leaf_data + 2 * size_t(s));
+}
+
+// Combined trees being refitted: the combined index of each leaf slot, from its geometry and
+// its index within it.
+__global__ void k_combined_order(PartsInput in, uint32_t n, const uint32_t* order,
+                                 const uint32_t* leaf_geom, uint32_t* combined, uint32_t* status)
+{
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n)
+        return;
+    const uint32_t gi = leaf_geom[s];
+    uint32_t p = 0;
+    while (p < in.n_parts && in.geom[p] != gi)
+        ++p;
+    if (p == in.n_parts || order[s] >= in.first[p + 1] - in.first[p]) {
+        atomicOr(status, ERR_BUILD);
+        combined[s] = 0;
+        return;
+    }
+    combined[s] = in.first[p] + order[s];
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -834,6 +891,13 @@ inline uint32_t blocks_for(size_t n, int threads) { return uint32_t((n + threads
 
 size_t leaf_record_float4s(int type) { return type == FR_GEOM_SPHERE ? 1 : 2; }
 
+namespace {
+size_t record_size(const BuildInput& in) { return leaf_record_float4s(in.type); }
+size_t record_size(const PartsInput&) { return 2; }
+constexpr bool is_parts(const BuildInput&) { return false; }
+constexpr bool is_parts(const PartsInput&) { return true; }
+}  // namespace
+
 // Collapse the binary tree in out.nodes into out.nodes4 (top-down, one launch per level).
 cudaError_t collapse4(BvhBuffers& out, Scratch& scratch, uint32_t* status, cudaStream_t st)
 {
@@ -888,14 +952,15 @@ cudaError_t collapse4(BvhBuffers& out, Scratch& scratch, uint32_t* status, cudaS
     return cudaGetLastError();
 }
 
-cudaError_t build_bvh(const BuildInput& in, uint32_t n, const BuildParams& bp, BvhBuffers& out,
-                      Scratch& scratch, uint32_t* status, cudaStream_t st)
+template <class In>
+static cudaError_t build_impl(const In& in, uint32_t n, const BuildParams& bp, BvhBuffers& out,
+                              Scratch& scratch, uint32_t* status, cudaStream_t st)
 {
     out.n_nodes = 0;
     if (n == 0)
         return cudaSuccess;
     const int T = 256;
-    const size_t rec = leaf_record_float4s(in.type);
+    const size_t rec = record_size(in);
     // persistent outputs
     cudaError_t e;
     if ((e = out.nodes.reserve(size_t(2) * (2 * size_t(n) - 1))) != cudaSuccess)
@@ -903,6 +968,8 @@ cudaError_t build_bvh(const BuildInput& in, uint32_t n, const BuildParams& bp, B
     if ((e = out.leaf_data.reserve(rec * n)) != cudaSuccess)
         return e;
     if ((e = out.order.reserve(n)) != cudaSuccess)
+        return e;
+    if (is_parts(in) && (e = out.leaf_geom.reserve(n)) != cudaSuccess)
         return e;
 
     // scratch carve-up
@@ -1138,7 +1205,8 @@ cudaError_t build_bvh(const BuildInput& in, uint32_t n, const BuildParams& bp, B
             return e;
         out.n_nodes = 1u + 2u * (tail[0] + tail[1]);
     }
-    k_gather<<<blocks_for(n, T), T, 0, st>>>(in, n, leaf_order, out.leaf_data.ptr, out.order.ptr);
+    k_gather<<<blocks_for(n, T), T, 0, st>>>(in, n, leaf_order, out.leaf_data.ptr, out.order.ptr,
+                                             out.leaf_geom.ptr);
     if ((e = cudaGetLastError()) != cudaSuccess)
         return e;
     if (bp.width != 4) {
@@ -1148,10 +1216,24 @@ cudaError_t build_bvh(const BuildInput& in, uint32_t n, const BuildParams& bp, B
     return collapse4(out, scratch, status, st);
 }
 
-cudaError_t refit_bvh(const BuildInput& in, uint32_t n, const BuildParams& bp, BvhBuffers& out,
-                      Scratch& scratch, uint32_t* status, cudaStream_t st)
+static void k_combined_order_for(const BuildInput&, uint32_t, BvhBuffers&, uint32_t*, uint32_t*,
+                                 cudaStream_t)
 {
-    if (n == 0 || out.n_nodes == 0 || out.order.cap < n || out.leaf_data.cap == 0)
+}
+
+static void k_combined_order_for(const PartsInput& in, uint32_t n, BvhBuffers& out,
+                                 uint32_t* combined, uint32_t* status, cudaStream_t st)
+{
+    k_combined_order<<<blocks_for(n, 256), 256, 0, st>>>(in, n, out.order.ptr, out.leaf_geom.ptr,
+                                                         combined, status);
+}
+
+template <class In>
+static cudaError_t refit_impl(const In& in, uint32_t n, const BuildParams& bp, BvhBuffers& out,
+                              Scratch& scratch, uint32_t* status, cudaStream_t st)
+{
+    if (n == 0 || out.n_nodes == 0 || out.order.cap < n || out.leaf_data.cap < record_size(in) * n ||
+        (is_parts(in) && out.leaf_geom.cap < n))
         return cudaErrorInvalidValue;
     const int T = 256;
     const uint32_t nn = out.n_nodes;
@@ -1161,6 +1243,7 @@ cudaError_t refit_bvh(const BuildInput& in, uint32_t n, const BuildParams& bp, B
     uint32_t* parent = L.take<uint32_t>(nn);
     uint32_t* arrive = L.take<uint32_t>(nn);
     uint32_t* cbounds = L.take<uint32_t>(8);
+    uint32_t* combined = L.take<uint32_t>(is_parts(in) ? n : 0);
     cudaError_t e;
     if ((e = scratch.reserve(L.bytes)) != cudaSuccess)
         return e;
@@ -1170,6 +1253,13 @@ cudaError_t refit_bvh(const BuildInput& in, uint32_t n, const BuildParams& bp, B
     parent = L.at(parent);
     arrive = L.at(arrive);
     cbounds = L.at(cbounds);
+    combined = L.at(combined);
+    // leaf slot -> index in the build's numbering (the geometry's own, or the combined one)
+    const uint32_t* slot_prim = out.order.ptr;
+    if (is_parts(in)) {
+        k_combined_order_for(in, n, out, combined, status, st);
+        slot_prim = combined;
+    }
     if ((e = cudaMemsetAsync(cbounds, 0xff, 3 * sizeof(uint32_t), st)) != cudaSuccess)
         return e;
     if ((e = cudaMemsetAsync(cbounds + 3, 0, 3 * sizeof(uint32_t), st)) != cudaSuccess)
@@ -1179,14 +1269,14 @@ cudaError_t refit_bvh(const BuildInput& in, uint32_t n, const BuildParams& bp, B
         gb = 4096;
     k_bounds<<<gb, T, 0, st>>>(in, n, box_lo, box_hi, cbounds);
     // same leaf order: re-gather the moved primitives' records in place
-    k_gather<<<blocks_for(n, T), T, 0, st>>>(in, n, out.order.ptr, out.leaf_data.ptr,
-                                             out.order.ptr);
+    k_gather<<<blocks_for(n, T), T, 0, st>>>(in, n, slot_prim, out.leaf_data.ptr, out.order.ptr,
+                                             out.leaf_geom.ptr);
     if ((e = cudaMemsetAsync(parent, 0xff, nn * sizeof(uint32_t), st)) != cudaSuccess)
         return e;
     if ((e = cudaMemsetAsync(arrive, 0, nn * sizeof(uint32_t), st)) != cudaSuccess)
         return e;
     k_parents<<<blocks_for(nn, T), T, 0, st>>>(out.nodes.ptr, nn, parent, status);
-    k_refit_tree<<<blocks_for(nn, T), T, 0, st>>>(out.nodes.ptr, nn, out.order.ptr, n, box_lo,
+    k_refit_tree<<<blocks_for(nn, T), T, 0, st>>>(out.nodes.ptr, nn, slot_prim, n, box_lo,
                                                   box_hi, parent, arrive, status);
     if ((e = cudaGetLastError()) != cudaSuccess)
         return e;
@@ -1195,6 +1285,30 @@ cudaError_t refit_bvh(const BuildInput& in, uint32_t n, const BuildParams& bp, B
         return cudaSuccess;
     }
     return collapse4(out, scratch, status, st);
+}
+
+cudaError_t build_bvh(const BuildInput& in, uint32_t n, const BuildParams& bp, BvhBuffers& out,
+                      Scratch& scratch, uint32_t* status, cudaStream_t st)
+{
+    return build_impl(in, n, bp, out, scratch, status, st);
+}
+
+cudaError_t build_bvh(const PartsInput& in, uint32_t n, const BuildParams& bp, BvhBuffers& out,
+                      Scratch& scratch, uint32_t* status, cudaStream_t st)
+{
+    return build_impl(in, n, bp, out, scratch, status, st);
+}
+
+cudaError_t refit_bvh(const BuildInput& in, uint32_t n, const BuildParams& bp, BvhBuffers& out,
+                      Scratch& scratch, uint32_t* status, cudaStream_t st)
+{
+    return refit_impl(in, n, bp, out, scratch, status, st);
+}
+
+cudaError_t refit_bvh(const PartsInput& in, uint32_t n, const BuildParams& bp, BvhBuffers& out,
+                      Scratch& scratch, uint32_t* status, cudaStream_t st)
+{
+    return refit_impl(in, n, bp, out, scratch, status, st);
 }
 
 }  // namespace fr

@@ -84,6 +84,16 @@ struct BuildInput {
     float poly_radius;
 };
 
+// Several geometries' primitives in one tree (a scene's combined BVH): primitive i of the
+// combined numbering is primitive i - first[p] of part p, where first[p] <= i < first[p + 1].
+constexpr int MAX_PARTS = 8;
+struct PartsInput {
+    BuildInput part[MAX_PARTS];
+    uint32_t first[MAX_PARTS + 1];
+    uint32_t geom[MAX_PARTS];  // scene geometry index of each part
+    uint32_t n_parts;
+};
+
 struct BuildParams {
     int builder = 0;       // 0: LBVH (Karras hierarchy); 1: PLOC (locally-ordered clustering)
     int width = 4;         // 2: binary tree only; 4: also collapse to the 4-wide tree
@@ -97,7 +107,8 @@ struct BvhBuffers {
     DevArray<float4> nodes4;     // 4-wide tree traversed by the renderers, 8 float4 per node
     uint32_t n_nodes4 = 0;
     DevArray<float4> leaf_data;  // leaf_record_float4s(type) per primitive
-    DevArray<uint32_t> order;    // leaf slot -> primitive index
+    DevArray<uint32_t> order;    // leaf slot -> primitive index (within its geometry)
+    DevArray<uint32_t> leaf_geom;  // combined trees: leaf slot -> scene geometry index
     uint32_t n_nodes = 0;
 };
 
@@ -111,6 +122,13 @@ cudaError_t collapse4(BvhBuffers& out, Scratch& scratch, uint32_t* status, cudaS
 // recomputed bottom-up in the existing topology, then the 4-wide tree is collapsed again.
 // Returns cudaErrorInvalidValue if `out` holds no tree for n primitives.
 cudaError_t refit_bvh(const BuildInput& in, uint32_t n, const BuildParams& bp, BvhBuffers& out,
+                      Scratch& scratch, uint32_t* status, cudaStream_t st);
+
+// The same for a combined tree over the parts of `in` (n = in.first[in.n_parts] primitives):
+// every leaf slot holds 2 float4 (a sphere uses the first) and its geometry in leaf_geom.
+cudaError_t refit_bvh(const PartsInput& in, uint32_t n, const BuildParams& bp, BvhBuffers& out,
+                      Scratch& scratch, uint32_t* status, cudaStream_t st);
+cudaError_t build_bvh(const PartsInput& in, uint32_t n, const BuildParams& bp, BvhBuffers& out,
                       Scratch& scratch, uint32_t* status, cudaStream_t st);
 
 // Build the BVH of n primitives (n == 0 leaves an empty tree).  Synchronises the stream once

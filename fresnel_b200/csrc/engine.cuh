@@ -66,6 +66,15 @@ struct SceneDev {
     const GeomDev* geoms;
     uint32_t n_geoms;
     uint32_t* status;  // error bits (device)
+    // Combined 4-wide tree over the primitives of several geometries (n_nodes4 == 0: none, each
+    // enabled geometry's own tree is traversed in turn): leaf slot s holds 2 float4 of its
+    // primitive's record, its geometry (leaf_geom) and its index within the geometry (order).
+    uint32_t n_nodes4;
+    uint32_t n_prims;
+    const float4* nodes4;
+    const float4* leaf_data;
+    const uint32_t* leaf_geom;
+    const uint32_t* order;
 };
 
 // --------------------------------------------------------------------------------------------
@@ -388,24 +397,25 @@ __device__ __forceinline__ void cswap(uint32_t& a, uint32_t& b)
 // five-comparator sorting network on keys (distance bits | child slot), the nearest is visited
 // next and the others are pushed far to near on a 64-entry per-thread stack.  Everything stays
 // in registers (no dynamically indexed arrays besides the stack).
-template <int TYPE>
-__device__ __forceinline__ void traverse4(const GeomDev& g, uint32_t gi, const RayK& ray,
-                                          float tnear, float& tmax, uint32_t& hit_geom,
-                                          uint32_t& hit_slot, uint32_t* status, TraceCount& tc)
+// `leaf(first, count)` tests the primitives of one leaf and lowers tmax on a closer hit.
+template <class Leaf>
+__device__ __forceinline__ void traverse4_core(const float4* nodes4, uint32_t n_nodes4,
+                                               uint32_t n_prims, const RayK& ray, float& tmax,
+                                               uint32_t* status, TraceCount& tc, Leaf&& leaf)
 {
-    if (g.n_nodes4 == 0)
+    if (n_nodes4 == 0)
         return;
     uint32_t stack_node[TRAVERSAL_STACK];
     float stack_t[TRAVERSAL_STACK];
     int sp = 0;
     uint32_t cur = 0;
-    uint32_t guard = g.n_nodes4 + 8u;
+    uint32_t guard = n_nodes4 + 8u;
     while (true) {
         if (--guard == 0u) {
             atomicOr(status, ERR_ITERATION_CAP);
             return;
         }
-        const float4* np = g.nodes4 + 8 * size_t(cur);
+        const float4* np = nodes4 + 8 * size_t(cur);
         const float4 lx = ldg4(np), hx = ldg4(np + 1), ly = ldg4(np + 2), hy = ldg4(np + 3),
                      lz = ldg4(np + 4), hz = ldg4(np + 5);
         const uint4 ci = __ldg(reinterpret_cast<const uint4*>(np + 6));
@@ -435,11 +445,11 @@ __device__ __forceinline__ void traverse4(const GeomDev& g, uint32_t gi, const R
             leaves &= leaves - 1u;
             uint32_t first = pick4(ci.x, ci.y, ci.z, ci.w, k);
             uint32_t count = pick4(cc.x, cc.y, cc.z, cc.w, k);
-            if (first > g.n_prims || count > g.n_prims - first) {
+            if (first > n_prims || count > n_prims - first) {
                 atomicOr(status, ERR_BAD_NODE);
                 return;
             }
-            leaf_test<TYPE>(g, gi, ray, first, count, tnear, tmax, hit_geom, hit_slot, tc);
+            leaf(first, count);
         }
         // interior children: key = entry distance bits (non-negative float) | child slot
         auto key = [&](bool h, uint32_t cck, float te, uint32_t k) {
@@ -469,7 +479,7 @@ __device__ __forceinline__ void traverse4(const GeomDev& g, uint32_t gi, const R
                 }
             }
             cur = pick4(ci.x, ci.y, ci.z, ci.w, k0 & 3u);
-            if (cur >= g.n_nodes4) {
+            if (cur >= n_nodes4) {
                 atomicOr(status, ERR_BAD_NODE);
                 return;
             }
@@ -480,12 +490,72 @@ __device__ __forceinline__ void traverse4(const GeomDev& g, uint32_t gi, const R
             --sp;
             if (stack_t[sp] <= tmax) {
                 cur = stack_node[sp];
-                found = cur < g.n_nodes4;
+                found = cur < n_nodes4;
                 break;
             }
         }
         if (!found)
             return;
+    }
+}
+
+template <int TYPE>
+__device__ __forceinline__ void traverse4(const GeomDev& g, uint32_t gi, const RayK& ray,
+                                          float tnear, float& tmax, uint32_t& hit_geom,
+                                          uint32_t& hit_slot, uint32_t* status, TraceCount& tc)
+{
+    traverse4_core(g.nodes4, g.n_nodes4, g.n_prims, ray, tmax, status, tc,
+                   [&](uint32_t first, uint32_t count) {
+                       leaf_test<TYPE>(g, gi, ray, first, count, tnear, tmax, hit_geom, hit_slot,
+                                       tc);
+                   });
+}
+
+// Leaf of a combined tree: each slot names its geometry; the primitive test is that geometry
+// type's (only the types in MASK are compiled in).
+template <uint32_t MASK>
+__device__ __forceinline__ void leaf_test_mixed(const SceneDev& sc, const RayK& ray,
+                                                uint32_t first, uint32_t count, float tnear,
+                                                float& tmax, uint32_t& hit_geom,
+                                                uint32_t& hit_slot, TraceCount& tc)
+{
+    tc.prim += count;
+    for (uint32_t s = first; s < first + count; ++s) {
+        const uint32_t gi = __ldg(sc.leaf_geom + s);
+        if (gi >= sc.n_geoms)
+            continue;
+        const GeomDev& g = sc.geoms[gi];
+        const int type = g.type;
+        const float4 a = ldg4(sc.leaf_data + 2 * size_t(s));
+        float t = 0.0f;
+        bool ok = false;
+        if ((MASK & (1u << FR_GEOM_SPHERE)) && type == FR_GEOM_SPHERE) {
+            ok = sphere_t(ray.o, ray.d, v3(a.x, a.y, a.z), a.w, t);
+        } else if ((MASK & (1u << FR_GEOM_CYLINDER)) && type == FR_GEOM_CYLINDER) {
+            const float4 b = ldg4(sc.leaf_data + 2 * size_t(s) + 1);
+            float de;
+            V3 N;
+            uint32_t ci;
+            ok = isect_spherocylinder(t, de, N, ci, ray.o, ray.d, v3(a.x, a.y, a.z),
+                                      v3(b.x, b.y, b.z), a.w);
+        } else if ((MASK & (1u << FR_GEOM_POLYHEDRON)) && type == FR_GEOM_POLYHEDRON) {
+            const float4 b = ldg4(sc.leaf_data + 2 * size_t(s) + 1);
+            PolyHit ph = poly_planes(g, ray.o, ray.d, v3(a.x, a.y, a.z), Qt{b.x, v3(b.y, b.z, b.w)},
+                                     tnear, tmax);
+            ok = ph.hit;
+            t = ph.t;
+        } else if ((MASK & (1u << FR_GEOM_MESH)) && type == FR_GEOM_MESH) {
+            const float4 b = ldg4(sc.leaf_data + 2 * size_t(s) + 1);
+            TriHit th = mesh_triangle(g, __float_as_uint(a.w), ray.o, ray.d, v3(a.x, a.y, a.z),
+                                      Qt{b.x, v3(b.y, b.z, b.w)});
+            ok = th.hit;
+            t = th.t;
+        }
+        if (ok && (tnear < t) && (t < tmax)) {
+            tmax = t;
+            hit_geom = gi;
+            hit_slot = s;
+        }
     }
 }
 
@@ -508,6 +578,16 @@ __device__ __forceinline__ Hit trace_closest(const SceneDev& sc, V3 o, V3 d, flo
     RayK ray = make_rayk(o, d);
     float tmax = __int_as_float(0x7f800000);  // +inf
     uint32_t hg = MISS, hs = 0;
+    if (WIDTH == 4 && sc.n_nodes4 != 0) {
+        traverse4_core(sc.nodes4, sc.n_nodes4, sc.n_prims, ray, tmax, sc.status, tc,
+                       [&](uint32_t first, uint32_t count) {
+                           leaf_test_mixed<MASK>(sc, ray, first, count, tnear, tmax, hg, hs, tc);
+                       });
+        Hit h;
+        h.geom = hg;
+        h.prim = (hg == MISS) ? 0u : __ldg(sc.order + hs);
+        return h;
+    }
     for (uint32_t gi = 0; gi < sc.n_geoms; ++gi) {
         const GeomDev& g = sc.geoms[gi];
         if (!g.enabled)
