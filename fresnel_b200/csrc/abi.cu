@@ -1998,6 +1998,21 @@ fr_status fr_batch_render(fr_batch* b)
     return check_status(dev);
 }
 
+fr_status fr_batch_reserve(fr_batch* b, size_t slots)
+{
+    FR_CHECK_NULL(b);
+    fr_status s = use_device(b->dev);
+    if (s != FR_OK)
+        return s;
+    bool moved = false;
+    FR_CUDA(b->path.reserve(slots, &moved), "allocating the batch path state");
+    if (moved && b->exec) {
+        cudaGraphExecDestroy(b->exec);
+        b->exec = nullptr;
+    }
+    return FR_OK;
+}
+
 fr_status fr_batch_get_stats(const fr_batch* b, fr_batch_stats* out)
 {
     FR_CHECK_NULL(b);

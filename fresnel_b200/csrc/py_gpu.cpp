@@ -773,6 +773,7 @@ PYBIND11_MODULE(_gpu, m)
         .def("render", &BatchH::render)
         .def("clear", &BatchH::clear)
         .def("getStats", &BatchH::stats)
+        .def("reserve", [](BatchH& b, size_t slots) { check(fr_batch_reserve(b.batch, slots)); })
         .def("__len__", [](const BatchH& b) { return b.items.size(); });
 
     export_array<ArrayRGBAf>(m, "ArrayRGBAf");

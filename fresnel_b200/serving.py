@@ -70,6 +70,12 @@ class Engine:
     def new_batch(self):
         return self._tracer_mod.PathBatch(self.device)
 
+    def reserve(self, batch, paths):
+        """Size the batch's path state for a full step up front (at most the device's wavefront
+        size), so that no step pays for growing it."""
+        slots = int(self.device._device.getOption("path_slots"))
+        batch.reserve(min(int(paths), slots))
+
     @staticmethod
     def start(tracer, seed):
         """Clear the tracer's image and set the seed of the request it now serves."""
@@ -95,7 +101,9 @@ class RenderServer:
         scene_factory: ``key -> (scene, nbytes)``; called once per key while it is resident.
         hbm_budget: bytes for resident scenes plus the accumulation buffers of active requests.
         step_paths: path budget (pixels x samples) of one step, filled shortest remaining
-            work first (``plan_step``).
+            work first (``plan_step``).  While all outstanding work fits in
+            ``max_step_paths`` (8 x step_paths by default), a step takes all of it: at light
+            load nothing is sliced, and a large request finishes in one launch.
         max_active: at most this many admitted requests (their buffers count against the
             budget; a request takes a tracer from the pool when it is first traced).
         keep_linear: also read back each finished request's linear (float) image.
@@ -103,9 +111,11 @@ class RenderServer:
     """
 
     def __init__(self, engine, scene_factory, hbm_budget=120e9, step_paths=32 << 20,
-                 max_active=256, keep_linear=False, clock=time.perf_counter, aging_s=1.0):
+                 max_active=256, keep_linear=False, clock=time.perf_counter, aging_s=1.0,
+                 max_step_paths=None):
         self.engine = engine
         self.aging_s = float(aging_s)
+        self.max_step_paths = int(8 * step_paths if max_step_paths is None else max_step_paths)
         self.scene_factory = scene_factory
         self.hbm_budget = float(hbm_budget)
         self.step_paths = int(step_paths)
@@ -120,6 +130,9 @@ class RenderServer:
         self.bytes_in_use = 0.0
         self.steps = 0
         self.batch = engine.new_batch()
+        reserve = getattr(engine, "reserve", None)
+        if reserve is not None:
+            reserve(self.batch, self.max_step_paths)
         # host seconds spent per phase of step() (admit, queue slices, trace, retire)
         self.phase_s = {"admit": 0.0, "queue": 0.0, "trace": 0.0, "retire": 0.0}
 
@@ -196,7 +209,10 @@ class RenderServer:
             rem = r.w * r.h * (r.samples - r.done_samples)
             return (rem / (1.0 + max(0.0, now - r.t_arrive) / self.aging_s), r.t_arrive)
 
+        remaining = sum(r.w * r.h * (r.samples - r.done_samples) for r in self.active)
         budget = self.step_paths
+        if remaining <= self.max_step_paths:
+            budget = max(budget, remaining)
         plan = []
         for r in sorted(self.active, key=key):
             px = r.w * r.h

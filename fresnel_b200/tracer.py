@@ -156,6 +156,11 @@ class PathBatch:
         self._batch.clear()
         self._queued = []
 
+    def reserve(self, paths):
+        """Allocate the path state for ``paths`` pixel samples in flight now, so that renders
+        that fit allocate nothing (it grows on demand otherwise)."""
+        self._batch.reserve(int(paths))
+
     def __len__(self):
         return len(self._batch)
 

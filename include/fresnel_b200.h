@@ -322,6 +322,9 @@ FR_API fr_status fr_batch_add_path(fr_batch* batch, fr_tracer* tr, fr_scene* sce
 FR_API fr_status fr_batch_clear(fr_batch* batch);
 /* Build stale scenes, then trace every queued render. */
 FR_API fr_status fr_batch_render(fr_batch* batch);
+/* Allocate the batch's path state for `slots` path slots now (144 bytes each), so that later
+ * fr_batch_render calls whose waves fit need no allocation (a render grows it on demand). */
+FR_API fr_status fr_batch_reserve(fr_batch* batch, size_t slots);
 FR_API fr_status fr_batch_get_stats(const fr_batch* batch, fr_batch_stats* out);
 
 /* ---------------- self-tests ---------------- */

@@ -225,7 +225,7 @@ def test_serving_trace_generator():
 def test_plan_prefers_short_work_and_ages():
     t = [0.0]
     srv = serving.RenderServer(FakeEngine(), factory({0: 10}), step_paths=1000,
-                               clock=lambda: t[0], aging_s=1.0)
+                               clock=lambda: t[0], aging_s=1.0, max_step_paths=1000)
     big = serving.Request(0, 10, 10, 50, tag="big")      # 5000 paths left
     small = serving.Request(0, 10, 10, 2, tag="small")   # 200 paths left
     srv.submit(big, now=0.0)
@@ -242,3 +242,16 @@ def test_plan_prefers_short_work_and_ages():
     assert srv.plan_step(now=0.0)[0][0].tag == "small"
     late.t_arrive = 10.0
     assert [r.tag for r, _ in srv.plan_step(now=10.0)][:2] == ["small", "big"]
+
+
+def test_light_load_runs_everything_in_one_step():
+    srv = serving.RenderServer(FakeEngine(), factory({0: 10}), step_paths=1000)
+    big = serving.Request(0, 40, 40, 3, tag="big")    # 4800 paths: above one step's budget,
+    small = serving.Request(0, 10, 10, 2, tag="small")  # but all work fits 8 steps' worth
+    srv.submit(big, now=0.0)
+    srv.submit(small, now=0.0)
+    srv._admit()
+    plan = dict((r.tag, k) for r, k in srv.plan_step(now=0.0))
+    assert plan == {"small": 2, "big": 3}
+    srv.step()
+    assert srv.idle() and srv.steps == 1
