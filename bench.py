@@ -169,6 +169,40 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
+class Replicas:
+    """Cross-rank bookkeeping of a replicas run (one process per GPU, each rendering its own
+    frames; no data moves between ranks): a barrier, and the max (time) or sum (rays) of one
+    number over the ranks.  With no process group every call is the identity."""
+
+    def __init__(self, dist=None, device="cuda"):
+        self.dist = dist
+        self.device = device
+
+    def _reduce(self, x, op):
+        if self.dist is None:
+            return x
+        import torch
+        t = torch.tensor([float(x)], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    def max(self, x):
+        return x if self.dist is None else self._reduce(x, self.dist.ReduceOp.MAX)
+
+    def sum(self, x):
+        return x if self.dist is None else self._reduce(x, self.dist.ReduceOp.SUM)
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def close(self):
+        if self.dist is not None:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
 def dist_init():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -531,28 +565,14 @@ def main():
         torch.cuda.set_device(0)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
         pg = dist
-
-    def barrier_max(x):
-        if pg is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
-
-    def barrier_sum(x):
-        if pg is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.SUM)
-        return float(t.item())
+    reps = Replicas(pg, "cuda")
+    barrier_max, barrier_sum = reps.max, reps.sum
 
     if wl.key in ("c4", "c5"):
         run = run_batch_bench if wl.key == "c4" else run_serving_bench
         rc = run(args, world, rank, barrier_max, barrier_sum,
                  int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0))
-        if pg is not None:
-            pg.barrier()
-            pg.destroy_process_group()
+        reps.close()
         return rc
 
     device = fresnel.Device(mode="gpu", n=1)
@@ -576,8 +596,7 @@ def main():
         frame()
     dd.setProfiling(True)
     tracer._tracer.resetStats()
-    if pg is not None:
-        pg.barrier()
+    reps.barrier()
     torch.cuda.synchronize()
     dd.synchronize()
     with ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0)) as clk:
@@ -586,8 +605,7 @@ def main():
             frame()
         ms = dd.timerStop()
     torch.cuda.synchronize()
-    if pg is not None:
-        pg.barrier()
+    reps.barrier()
     st = tracer._tracer.getStats()
     dd.setProfiling(False)
     rays = float(st["rays"])
@@ -691,9 +709,7 @@ def main():
                                "primary_rays": kern["k_path_primary"][0],
                                "extension_rays": kern["k_path_extend"][0]}
         print(json.dumps(line))
-    if pg is not None:
-        pg.barrier()
-        pg.destroy_process_group()
+    reps.close()
     return 0
 
 
