@@ -159,6 +159,7 @@ struct fr_device {
     int refit = 0;                         // refit (not rebuild) trees whose primitives moved
     int shade_blocks = 3;                  // shade kernel variant (render.hpp FrameParams)
     int combined = 1;                      // one tree per scene of several geometries
+    int packet = 0;                        // warp-cooperative primary traversal
     std::vector<fr_scene*> scenes;         // to mark BVHs stale when a build option changes
     void* static_path = nullptr;           // this device's copy of g_static_path (looked up once)
     PathBuffers path;                      // wavefront state shared by the device's tracers
@@ -667,6 +668,7 @@ FrameParams frame_params(fr_tracer* tr, fr_scene* sc, const fr_render_params* p,
     }
     P.tile_log2 = sc->dev->tile_log2;
     P.shade_blocks = sc->dev->shade_blocks;
+    P.packet = sc->dev->packet;
     const fr_user_camera& c = p->camera;
     float f_stop = preview ? std::numeric_limits<float>::infinity() : c.f_stop;  // no depth of field in preview
     bool sample_aa = preview ? (aa_n != 1) : true;
@@ -937,6 +939,10 @@ fr_status fr_device_set_option(fr_device* d, const char* name, double value)
             return fail(FR_ERR_INVALID, "c_trav must be in (0, 100)");
         tree = d->build.c_trav != float(value);
         d->build.c_trav = float(value);
+    } else if (n == "packet") {
+        if (value != 0.0 && value != 1.0)
+            return fail(FR_ERR_INVALID, "packet must be 0 or 1");
+        d->packet = int(value);
     } else if (n == "combined") {
         if (value != 0.0 && value != 1.0)
             return fail(FR_ERR_INVALID, "combined must be 0 or 1");
@@ -1001,6 +1007,8 @@ fr_status fr_device_get_option(const fr_device* d, const char* name, double* val
         *value = d->shade_blocks;
     else if (n == "combined")
         *value = d->combined;
+    else if (n == "packet")
+        *value = d->packet;
     else if (n == "persistent")
         *value = d->persistent;
     else

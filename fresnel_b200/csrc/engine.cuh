@@ -499,6 +499,130 @@ __device__ __forceinline__ void traverse4_core(const float4* nodes4, uint32_t n_
     }
 }
 
+// Warp-cooperative form of traverse4_core for coherent rays (neighbouring samples of the same
+// pixels): the warp walks one node sequence; each lane tests its own ray against a node's four
+// children and its own leaves; the warp descends into every interior child that some lane hits,
+// nearest first by the smallest entry distance over the lanes, and drops a stacked subtree once
+// its entry distance is beyond every lane's closest hit.  Each lane therefore tests exactly the
+// leaves its own ray reaches with its own closest distance, as in traverse4_core, and gets the
+// same closest hit (the visiting order only matters between primitives at exactly equal t).
+// The stack is the warp's own (shared memory, TRAVERSAL_STACK entries).  All 32 lanes must call
+// together; lanes without a ray pass active = false.
+template <class Leaf>
+__device__ __forceinline__ void traverse4_packet_core(const float4* nodes4, uint32_t n_nodes4,
+                                                      uint32_t n_prims, const RayK& ray,
+                                                      bool active, float& tmax, uint32_t* status,
+                                                      TraceCount& tc, uint32_t* stk_node,
+                                                      float* stk_t, Leaf&& leaf)
+{
+    constexpr uint32_t FULL = 0xffffffffu, NONE = 0xFFFFFFFFu;
+    if (n_nodes4 == 0)
+        return;
+    const bool lead = (threadIdx.x & 31u) == 0u;
+    int sp = 0;
+    uint32_t cur = 0;
+    uint32_t guard = n_nodes4 + 8u;
+    while (true) {
+        if (--guard == 0u) {
+            if (lead)
+                atomicOr(status, ERR_ITERATION_CAP);
+            return;
+        }
+        const float4* np = nodes4 + 8 * size_t(cur);
+        const float4 lx = ldg4(np), hx = ldg4(np + 1), ly = ldg4(np + 2), hy = ldg4(np + 3),
+                     lz = ldg4(np + 4), hz = ldg4(np + 5);
+        const uint4 ci = __ldg(reinterpret_cast<const uint4*>(np + 6));
+        const uint4 cc = __ldg(reinterpret_cast<const uint4*>(np + 7));
+        if (active)
+            tc.box += 4;
+        float te0, te1, te2, te3;
+        auto test = [&](float lxk, float hxk, float lyk, float hyk, float lzk, float hzk,
+                        uint32_t cck, float& te) {
+            float tx0 = fmaf(lxk, ray.inv.x, ray.oinv.x), tx1 = fmaf(hxk, ray.inv.x, ray.oinv.x);
+            float ty0 = fmaf(lyk, ray.inv.y, ray.oinv.y), ty1 = fmaf(hyk, ray.inv.y, ray.oinv.y);
+            float tz0 = fmaf(lzk, ray.inv.z, ray.oinv.z), tz1 = fmaf(hzk, ray.inv.z, ray.oinv.z);
+            float t0 = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), 0.0f));
+            float t1 = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tmax));
+            te = t0;
+            return active && t0 <= t1 && cck != EMPTY_CHILD;
+        };
+        const bool h0 = test(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, cc.x, te0);
+        const bool h1 = test(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, cc.y, te1);
+        const bool h2 = test(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, cc.z, te2);
+        const bool h3 = test(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, cc.w, te3);
+        // leaves: the warp goes through every leaf some lane hits; each lane tests its own
+        const uint32_t leaves = (h0 && cc.x != 0u ? 1u : 0u) | (h1 && cc.y != 0u ? 2u : 0u) |
+                                (h2 && cc.z != 0u ? 4u : 0u) | (h3 && cc.w != 0u ? 8u : 0u);
+        uint32_t any_leaves = __reduce_or_sync(FULL, leaves);
+        while (any_leaves) {
+            const uint32_t k = uint32_t(__ffs(any_leaves) - 1);
+            any_leaves &= any_leaves - 1u;
+            const uint32_t first = pick4(ci.x, ci.y, ci.z, ci.w, k);
+            const uint32_t count = pick4(cc.x, cc.y, cc.z, cc.w, k);
+            if (first > n_prims || count > n_prims - first) {
+                if (lead)
+                    atomicOr(status, ERR_BAD_NODE);
+                return;
+            }
+            if (leaves & (1u << k))
+                leaf(first, count);
+        }
+        // interior children, keyed by the nearest entry over the lanes that reach them
+        auto key = [&](bool h, uint32_t cck, float te, uint32_t k) {
+            const uint32_t own = (h && cck == 0u && te <= tmax) ? __float_as_uint(te) : NONE;
+            const uint32_t m = __reduce_min_sync(FULL, own);
+            return m == NONE ? NONE : ((m & ~3u) | k);
+        };
+        uint32_t k0 = key(h0, cc.x, te0, 0), k1 = key(h1, cc.y, te1, 1);
+        uint32_t k2 = key(h2, cc.z, te2, 2), k3 = key(h3, cc.w, te3, 3);
+        cswap(k0, k1);
+        cswap(k2, k3);
+        cswap(k0, k2);
+        cswap(k1, k3);
+        cswap(k1, k2);
+        if (k0 != NONE) {
+            const uint32_t ks[3] = {k3, k2, k1};
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                if (ks[a] != NONE) {
+                    if (sp < TRAVERSAL_STACK) {
+                        if (lead) {
+                            stk_node[sp] = pick4(ci.x, ci.y, ci.z, ci.w, ks[a] & 3u);
+                            stk_t[sp] = __uint_as_float(ks[a] & ~3u);
+                        }
+                        ++sp;
+                    } else if (lead) {
+                        atomicOr(status, ERR_STACK_OVERFLOW);
+                    }
+                }
+            }
+            __syncwarp();
+            cur = pick4(ci.x, ci.y, ci.z, ci.w, k0 & 3u);
+            if (cur >= n_nodes4) {
+                if (lead)
+                    atomicOr(status, ERR_BAD_NODE);
+                return;
+            }
+            continue;
+        }
+        // the farthest any lane still needs to look (closest hits are non-negative)
+        const float reach =
+            __uint_as_float(__reduce_max_sync(FULL, active ? __float_as_uint(tmax) : 0u));
+        bool found = false;
+        while (sp > 0) {
+            --sp;
+            if (stk_t[sp] <= reach) {
+                cur = stk_node[sp];
+                found = cur < n_nodes4;
+                break;
+            }
+        }
+        __syncwarp();
+        if (!found)
+            return;
+    }
+}
+
 template <int TYPE>
 __device__ __forceinline__ void traverse4(const GeomDev& g, uint32_t gi, const RayK& ray,
                                           float tnear, float& tmax, uint32_t& hit_geom,
@@ -599,6 +723,52 @@ __device__ __forceinline__ Hit trace_closest(const SceneDev& sc, V3 o, V3 d, flo
         else                                                                      \
             traverse<T>(g, gi, ray, tnear, tmax, hg, hs, sc.status, tc);         \
         continue;                                                                 \
+    }
+        FR_TRAVERSE(FR_GEOM_SPHERE)
+        FR_TRAVERSE(FR_GEOM_CYLINDER)
+        FR_TRAVERSE(FR_GEOM_POLYHEDRON)
+        FR_TRAVERSE(FR_GEOM_MESH)
+#undef FR_TRAVERSE
+    }
+    Hit h;
+    h.geom = hg;
+    h.prim = (hg == MISS) ? 0u : __ldg(sc.geoms[hg].order + hs);
+    return h;
+}
+
+// Closest hit for coherent rays with the warp-cooperative traversal (4-wide trees only).  All
+// 32 lanes of the warp call together; `active` marks the lanes that have a ray.
+template <uint32_t MASK>
+__device__ __forceinline__ Hit trace_closest_packet(const SceneDev& sc, V3 o, V3 d, bool active,
+                                                    float tnear, TraceCount& tc,
+                                                    uint32_t* stk_node, float* stk_t)
+{
+    RayK ray = make_rayk(o, d);
+    float tmax = __int_as_float(0x7f800000);  // +inf
+    uint32_t hg = MISS, hs = 0;
+    if (sc.n_nodes4 != 0) {
+        traverse4_packet_core(sc.nodes4, sc.n_nodes4, sc.n_prims, ray, active, tmax, sc.status,
+                              tc, stk_node, stk_t, [&](uint32_t first, uint32_t count) {
+                                  leaf_test_mixed<MASK>(sc, ray, first, count, tnear, tmax, hg,
+                                                        hs, tc);
+                              });
+        Hit h;
+        h.geom = hg;
+        h.prim = (hg == MISS) ? 0u : __ldg(sc.order + hs);
+        return h;
+    }
+    for (uint32_t gi = 0; gi < sc.n_geoms; ++gi) {
+        const GeomDev& g = sc.geoms[gi];
+        if (!g.enabled)
+            continue;
+#define FR_TRAVERSE(T)                                                                     \
+    if ((MASK & (1u << T)) && g.type == T) {                                               \
+        traverse4_packet_core(g.nodes4, g.n_nodes4, g.n_prims, ray, active, tmax, sc.status, \
+                              tc, stk_node, stk_t, [&](uint32_t first, uint32_t count) {   \
+                                  leaf_test<T>(g, gi, ray, first, count, tnear, tmax, hg, hs, \
+                                               tc);                                        \
+                              });                                                          \
+        continue;                                                                          \
     }
         FR_TRAVERSE(FR_GEOM_SPHERE)
         FR_TRAVERSE(FR_GEOM_CYLINDER)

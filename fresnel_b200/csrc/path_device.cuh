@@ -163,13 +163,9 @@ __device__ __forceinline__ bool shade_pixel(const FrameParams& P, const PathStat
 // Primary ray of one item: closest hit; a miss finishes its pixel sample (every light sample
 // sees the background: radiance bg * L, fresnel/common/TracerPathMethods.h:44-50), a hit
 // initialises the path state. Returns true for a hit (the slot is queued for shading).
-template <int WIDTH, uint32_t MASK>
-__device__ __forceinline__ bool primary_ray(const FrameParams& P, const PathState& S,
-                                            const PrimaryItem& it, uint32_t slot, TraceCount& tc)
+__device__ __forceinline__ bool primary_finish(const FrameParams& P, const PathState& S,
+                                               uint32_t slot, V3 o, V3 d, Hit h)
 {
-    V3 o, d;
-    camera_ray(P.cam, it.i, it.j, P.n_samples + it.k, o, d);
-    Hit h = trace_closest<WIDTH, MASK>(P.scene, o, d, PATH_TNEAR, tc);
     S.prim_hit[slot] = make_uint2(h.geom, h.prim);
     if (h.geom == MISS) {
         C3 res = P.bg * float(P.light_samples);
@@ -183,6 +179,16 @@ __device__ __forceinline__ bool primary_ray(const FrameParams& P, const PathStat
     S.att[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
     S.result[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     return true;
+}
+
+template <int WIDTH, uint32_t MASK>
+__device__ __forceinline__ bool primary_ray(const FrameParams& P, const PathState& S,
+                                            const PrimaryItem& it, uint32_t slot, TraceCount& tc)
+{
+    V3 o, d;
+    camera_ray(P.cam, it.i, it.j, P.n_samples + it.k, o, d);
+    Hit h = trace_closest<WIDTH, MASK>(P.scene, o, d, PATH_TNEAR, tc);
+    return primary_finish(P, S, slot, o, d, h);
 }
 
 // Append the lanes with push set to queue 1 (one atomic per warp).

@@ -25,7 +25,7 @@ namespace fr {
 namespace {
 
 // Primary rays of every slot of the batch, one thread per work item (primary_item order).
-template <int WIDTH, uint32_t MASK>
+template <int WIDTH, uint32_t MASK, bool PACKET = false>
 __global__ void __launch_bounds__(256) k_path_primary(FrameParams P, PathState S)
 {
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -37,7 +37,21 @@ __global__ void __launch_bounds__(256) k_path_primary(FrameParams P, PathState S
     bool push = false;
     uint32_t slot = 0;
     TraceCount tc;
-    if (it.valid) {
+    if (PACKET) {
+        // a warp's rays are neighbouring samples of the same pixels: trace them as a packet
+        __shared__ uint32_t stk_node[8][TRAVERSAL_STACK];
+        __shared__ float stk_t[8][TRAVERSAL_STACK];
+        const uint32_t w = threadIdx.x >> 5;
+        V3 o = v3(0.0f, 0.0f, 0.0f), d = v3(0.0f, 0.0f, 1.0f);
+        if (it.valid)
+            camera_ray(P.cam, it.i, it.j, P.n_samples + it.k, o, d);
+        Hit h = trace_closest_packet<MASK>(P.scene, o, d, it.valid, PATH_TNEAR, tc, stk_node[w],
+                                           stk_t[w]);
+        if (it.valid) {
+            slot = g;
+            push = primary_finish(P, S, slot, o, d, h);
+        }
+    } else if (it.valid) {
         slot = g;
         push = primary_ray<WIDTH, MASK>(P, S, it, slot, tc);
     }
@@ -449,6 +463,8 @@ void launch_path_primary(const FrameParams& P, const PathState& S, const LaunchS
     const uint32_t n_items = primary_items(P.w, P.h, P.batch, P.tile_log2);
     auto k = pick(P, k_path_primary<2, MASK_SPHERES>, k_path_primary<2, MASK_ALL>,
                   k_path_primary<4, MASK_SPHERES>, k_path_primary<4, MASK_ALL>);
+    if (P.bvh_width == 4 && P.packet)
+        k = spheres_only ? k_path_primary<4, MASK_SPHERES, true> : k_path_primary<4, MASK_ALL, true>;
     k<<<(n_items + 255) / 256, 256, 0, st>>>(P, S);
 }
 

@@ -26,6 +26,7 @@ struct FrameParams {
     uint32_t light_samples;  // light paths per primary ray
     uint32_t tile_log2;      // primary work in 2^tile_log2-pixel square tiles (path_device.cuh)
     int shade_blocks;        // 0: shade kernel as compiled; 3 or 4: register-limited variants
+    int packet;              // 1: primary rays traced warp-cooperatively (4-wide trees)
     int highlight;
     C3 hl_color;
     float4* linear;     // [h][w] running mean, linear RGBA

@@ -164,6 +164,8 @@ FR_API fr_status fr_device_timer_stop(fr_device* dev, float* ms);
  *   "builder"       0: LBVH (Karras hierarchy, default); 1: PLOC (locally-ordered clustering)
  *   "tile"          4, 8 (default) or 16: primary rays are traced in square pixel tiles of this
  *                   size, the samples of a pixel in neighbouring threads
+ *   "packet"        1: primary rays traced warp-cooperatively (one node sequence per warp, a
+ *                   shared stack); 0: one ray per thread (default)
  *   "combined"      1 (default): a scene of 2 to 8 enabled geometries gets one BVH over all
  *                   their primitives; 0: each geometry's own BVH, traversed in turn
  *   "shade_blocks"  3 (default) or 4: the shade kernel compiled to fit that many 256-thread
