@@ -397,6 +397,33 @@ __device__ __forceinline__ void cswap(uint32_t& a, uint32_t& b)
 // five-comparator sorting network on keys (distance bits | child slot), the nearest is visited
 // next and the others are pushed far to near on a 64-entry per-thread stack.  Everything stays
 // in registers (no dynamically indexed arrays besides the stack).
+// Node float4 holding each axis's near planes for this ray (the far planes are the other one of
+// the pair): a 4-wide node stores lo.x, hi.x, lo.y, hi.y, lo.z, hi.z, and a ray whose direction
+// component is negative enters through the hi plane.
+struct NearFar {
+    int x, y, z;
+};
+
+__device__ __forceinline__ NearFar near_far(const RayK& r)
+{
+    return NearFar{r.inv.x < 0.0f ? 1 : 0, r.inv.y < 0.0f ? 3 : 2, r.inv.z < 0.0f ? 5 : 4};
+}
+
+// Slab test of one child against its near (n) and far (f) planes: the same entry and exit
+// distances as min/max over the lo/hi planes for every non-empty box (a fused multiply-add is
+// monotonic in the plane), with half the min/max operations.  Empty boxes (lo > hi) are missed.
+__device__ __forceinline__ bool slab4_child(const RayK& ray, float nx, float fx, float ny, float fy,
+                                            float nz, float fz, float tmax, float& te)
+{
+    const float tnx = fmaf(nx, ray.inv.x, ray.oinv.x), tfx = fmaf(fx, ray.inv.x, ray.oinv.x);
+    const float tny = fmaf(ny, ray.inv.y, ray.oinv.y), tfy = fmaf(fy, ray.inv.y, ray.oinv.y);
+    const float tnz = fmaf(nz, ray.inv.z, ray.oinv.z), tfz = fmaf(fz, ray.inv.z, ray.oinv.z);
+    const float t0 = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
+    const float t1 = fminf(fminf(tfx, tfy), fminf(tfz, tmax));
+    te = t0;
+    return t0 <= t1;
+}
+
 // `leaf(first, count)` tests the primitives of one leaf and lowers tmax on a closer hit.
 template <class Leaf>
 __device__ __forceinline__ void traverse4_core(const float4* nodes4, uint32_t n_nodes4,
@@ -410,33 +437,28 @@ __device__ __forceinline__ void traverse4_core(const float4* nodes4, uint32_t n_
     int sp = 0;
     uint32_t cur = 0;
     uint32_t guard = n_nodes4 + 8u;
+    const NearFar nf = near_far(ray);
     while (true) {
         if (--guard == 0u) {
             atomicOr(status, ERR_ITERATION_CAP);
             return;
         }
         const float4* np = nodes4 + 8 * size_t(cur);
-        const float4 lx = ldg4(np), hx = ldg4(np + 1), ly = ldg4(np + 2), hy = ldg4(np + 3),
-                     lz = ldg4(np + 4), hz = ldg4(np + 5);
+        const float4 nx = ldg4(np + nf.x), fx = ldg4(np + (nf.x ^ 1)), ny = ldg4(np + nf.y),
+                     fy = ldg4(np + (nf.y ^ 1)), nz = ldg4(np + nf.z), fz = ldg4(np + (nf.z ^ 1));
         const uint4 ci = __ldg(reinterpret_cast<const uint4*>(np + 6));
         const uint4 cc = __ldg(reinterpret_cast<const uint4*>(np + 7));
         tc.box += 4;
         float te0, te1, te2, te3;
         bool h0, h1, h2, h3;
-        auto test = [&](float lxk, float hxk, float lyk, float hyk, float lzk, float hzk,
+        auto test = [&](float nxk, float fxk, float nyk, float fyk, float nzk, float fzk,
                         uint32_t cck, float& te) {
-            float tx0 = fmaf(lxk, ray.inv.x, ray.oinv.x), tx1 = fmaf(hxk, ray.inv.x, ray.oinv.x);
-            float ty0 = fmaf(lyk, ray.inv.y, ray.oinv.y), ty1 = fmaf(hyk, ray.inv.y, ray.oinv.y);
-            float tz0 = fmaf(lzk, ray.inv.z, ray.oinv.z), tz1 = fmaf(hzk, ray.inv.z, ray.oinv.z);
-            float t0 = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), 0.0f));
-            float t1 = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tmax));
-            te = t0;
-            return t0 <= t1 && cck != EMPTY_CHILD;
+            return slab4_child(ray, nxk, fxk, nyk, fyk, nzk, fzk, tmax, te) && cck != EMPTY_CHILD;
         };
-        h0 = test(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, cc.x, te0);
-        h1 = test(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, cc.y, te1);
-        h2 = test(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, cc.z, te2);
-        h3 = test(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, cc.w, te3);
+        h0 = test(nx.x, fx.x, ny.x, fy.x, nz.x, fz.x, cc.x, te0);
+        h1 = test(nx.y, fx.y, ny.y, fy.y, nz.y, fz.y, cc.y, te1);
+        h2 = test(nx.z, fx.z, ny.z, fy.z, nz.z, fz.z, cc.z, te2);
+        h3 = test(nx.w, fx.w, ny.w, fy.w, nz.w, fz.w, cc.w, te3);
         // leaves: one shared copy of the primitive loop, iterated over a bit mask
         uint32_t leaves = (h0 && cc.x != 0u ? 1u : 0u) | (h1 && cc.y != 0u ? 2u : 0u) |
                           (h2 && cc.z != 0u ? 4u : 0u) | (h3 && cc.w != 0u ? 8u : 0u);
@@ -522,6 +544,7 @@ __device__ __forceinline__ void traverse4_packet_core(const float4* nodes4, uint
     int sp = 0;
     uint32_t cur = 0;
     uint32_t guard = n_nodes4 + 8u;
+    const NearFar nf = near_far(ray);
     while (true) {
         if (--guard == 0u) {
             if (lead)
@@ -529,27 +552,22 @@ __device__ __forceinline__ void traverse4_packet_core(const float4* nodes4, uint
             return;
         }
         const float4* np = nodes4 + 8 * size_t(cur);
-        const float4 lx = ldg4(np), hx = ldg4(np + 1), ly = ldg4(np + 2), hy = ldg4(np + 3),
-                     lz = ldg4(np + 4), hz = ldg4(np + 5);
+        const float4 nx = ldg4(np + nf.x), fx = ldg4(np + (nf.x ^ 1)), ny = ldg4(np + nf.y),
+                     fy = ldg4(np + (nf.y ^ 1)), nz = ldg4(np + nf.z), fz = ldg4(np + (nf.z ^ 1));
         const uint4 ci = __ldg(reinterpret_cast<const uint4*>(np + 6));
         const uint4 cc = __ldg(reinterpret_cast<const uint4*>(np + 7));
         if (active)
             tc.box += 4;
         float te0, te1, te2, te3;
-        auto test = [&](float lxk, float hxk, float lyk, float hyk, float lzk, float hzk,
+        auto test = [&](float nxk, float fxk, float nyk, float fyk, float nzk, float fzk,
                         uint32_t cck, float& te) {
-            float tx0 = fmaf(lxk, ray.inv.x, ray.oinv.x), tx1 = fmaf(hxk, ray.inv.x, ray.oinv.x);
-            float ty0 = fmaf(lyk, ray.inv.y, ray.oinv.y), ty1 = fmaf(hyk, ray.inv.y, ray.oinv.y);
-            float tz0 = fmaf(lzk, ray.inv.z, ray.oinv.z), tz1 = fmaf(hzk, ray.inv.z, ray.oinv.z);
-            float t0 = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), 0.0f));
-            float t1 = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tmax));
-            te = t0;
-            return active && t0 <= t1 && cck != EMPTY_CHILD;
+            return active && slab4_child(ray, nxk, fxk, nyk, fyk, nzk, fzk, tmax, te) &&
+                   cck != EMPTY_CHILD;
         };
-        const bool h0 = test(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, cc.x, te0);
-        const bool h1 = test(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, cc.y, te1);
-        const bool h2 = test(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, cc.z, te2);
-        const bool h3 = test(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, cc.w, te3);
+        const bool h0 = test(nx.x, fx.x, ny.x, fy.x, nz.x, fz.x, cc.x, te0);
+        const bool h1 = test(nx.y, fx.y, ny.y, fy.y, nz.y, fz.y, cc.y, te1);
+        const bool h2 = test(nx.z, fx.z, ny.z, fy.z, nz.z, fz.z, cc.z, te2);
+        const bool h3 = test(nx.w, fx.w, ny.w, fy.w, nz.w, fz.w, cc.w, te3);
         // leaves: the warp goes through every leaf some lane hits; each lane tests its own
         const uint32_t leaves = (h0 && cc.x != 0u ? 1u : 0u) | (h1 && cc.y != 0u ? 2u : 0u) |
                                 (h2 && cc.z != 0u ? 4u : 0u) | (h3 && cc.w != 0u ? 8u : 0u);
