@@ -160,6 +160,7 @@ struct fr_device {
     int shade_blocks = 3;                  // shade kernel variant (render.hpp FrameParams)
     int combined = 1;                      // one tree per scene of several geometries
     int packet = 0;                        // warp-cooperative primary traversal
+    int refill = 0;                        // extension rays with per-lane refill
     std::vector<fr_scene*> scenes;         // to mark BVHs stale when a build option changes
     void* static_path = nullptr;           // this device's copy of g_static_path (looked up once)
     PathBuffers path;                      // wavefront state shared by the device's tracers
@@ -655,6 +656,7 @@ FrameParams frame_params(fr_tracer* tr, fr_scene* sc, const fr_render_params* p,
         P.scene.leaf_data = sc->combined.leaf_data.ptr;
         P.scene.leaf_geom = sc->combined.leaf_geom.ptr;
         P.scene.order = sc->combined.order.ptr;
+        P.refill_geom = -2;
     } else {
         bool all4 = true;
         for (fr_geometry* g : sc->geoms) {
@@ -665,10 +667,22 @@ FrameParams frame_params(fr_tracer* tr, fr_scene* sc, const fr_render_params* p,
         }
         if (P.type_mask != 0 && all4)
             P.bvh_width = 4;
+        int only = -1, n_enabled = 0;
+        for (size_t i = 0; i < sc->geoms.size(); ++i) {
+            const fr_geometry* g = sc->geoms[i];
+            if (g->enabled && !g->removed && g->bvh.n_nodes > 0) {
+                only = int(i);
+                ++n_enabled;
+            }
+        }
+        if (n_enabled == 1)
+            P.refill_geom = only;
     }
     P.tile_log2 = sc->dev->tile_log2;
     P.shade_blocks = sc->dev->shade_blocks;
     P.packet = sc->dev->packet;
+    P.refill = sc->dev->refill;
+    P.refill_geom = -1;
     const fr_user_camera& c = p->camera;
     float f_stop = preview ? std::numeric_limits<float>::infinity() : c.f_stop;  // no depth of field in preview
     bool sample_aa = preview ? (aa_n != 1) : true;
@@ -939,6 +953,10 @@ fr_status fr_device_set_option(fr_device* d, const char* name, double value)
             return fail(FR_ERR_INVALID, "c_trav must be in (0, 100)");
         tree = d->build.c_trav != float(value);
         d->build.c_trav = float(value);
+    } else if (n == "refill") {
+        if (value != 0.0 && value != 1.0)
+            return fail(FR_ERR_INVALID, "refill must be 0 or 1");
+        d->refill = int(value);
     } else if (n == "packet") {
         if (value != 0.0 && value != 1.0)
             return fail(FR_ERR_INVALID, "packet must be 0 or 1");
@@ -1009,6 +1027,8 @@ fr_status fr_device_get_option(const fr_device* d, const char* name, double* val
         *value = d->combined;
     else if (n == "packet")
         *value = d->packet;
+    else if (n == "refill")
+        *value = d->refill;
     else if (n == "persistent")
         *value = d->persistent;
     else

@@ -424,7 +424,90 @@ __device__ __forceinline__ bool slab4_child(const RayK& ray, float nx, float fx,
     return t0 <= t1;
 }
 
-// `leaf(first, count)` tests the primitives of one leaf and lowers tmax on a closer hit.
+// One visit of a 4-wide node: test its four children, test the leaves the ray hits (through
+// `leaf(first, count)`, which lowers tmax on a closer hit), descend into the nearest interior
+// child hit and push the others far to near, or pop the next stacked node still in reach.
+// Returns false once nothing is left to visit (or a bad index was met and reported).
+template <class Leaf>
+__device__ __forceinline__ bool visit4(const float4* nodes4, uint32_t n_nodes4, uint32_t n_prims,
+                                       const RayK& ray, const NearFar& nf, float& tmax,
+                                       uint32_t& cur, int& sp, uint32_t* stack_node,
+                                       float* stack_t, uint32_t* status, TraceCount& tc,
+                                       Leaf&& leaf)
+{
+    const float4* np = nodes4 + 8 * size_t(cur);
+    const float4 nx = ldg4(np + nf.x), fx = ldg4(np + (nf.x ^ 1)), ny = ldg4(np + nf.y),
+                 fy = ldg4(np + (nf.y ^ 1)), nz = ldg4(np + nf.z), fz = ldg4(np + (nf.z ^ 1));
+    const uint4 ci = __ldg(reinterpret_cast<const uint4*>(np + 6));
+    const uint4 cc = __ldg(reinterpret_cast<const uint4*>(np + 7));
+    tc.box += 4;
+    float te0, te1, te2, te3;
+    auto test = [&](float nxk, float fxk, float nyk, float fyk, float nzk, float fzk,
+                    uint32_t cck, float& te) {
+        return slab4_child(ray, nxk, fxk, nyk, fyk, nzk, fzk, tmax, te) && cck != EMPTY_CHILD;
+    };
+    const bool h0 = test(nx.x, fx.x, ny.x, fy.x, nz.x, fz.x, cc.x, te0);
+    const bool h1 = test(nx.y, fx.y, ny.y, fy.y, nz.y, fz.y, cc.y, te1);
+    const bool h2 = test(nx.z, fx.z, ny.z, fy.z, nz.z, fz.z, cc.z, te2);
+    const bool h3 = test(nx.w, fx.w, ny.w, fy.w, nz.w, fz.w, cc.w, te3);
+    // leaves: one shared copy of the primitive loop, iterated over a bit mask
+    uint32_t leaves = (h0 && cc.x != 0u ? 1u : 0u) | (h1 && cc.y != 0u ? 2u : 0u) |
+                      (h2 && cc.z != 0u ? 4u : 0u) | (h3 && cc.w != 0u ? 8u : 0u);
+    while (leaves) {
+        const uint32_t k = uint32_t(__ffs(leaves) - 1);
+        leaves &= leaves - 1u;
+        const uint32_t first = pick4(ci.x, ci.y, ci.z, ci.w, k);
+        const uint32_t count = pick4(cc.x, cc.y, cc.z, cc.w, k);
+        if (first > n_prims || count > n_prims - first) {
+            atomicOr(status, ERR_BAD_NODE);
+            return false;
+        }
+        leaf(first, count);
+    }
+    // interior children: key = entry distance bits (non-negative float) | child slot
+    auto key = [&](bool h, uint32_t cck, float te, uint32_t k) {
+        return (h && cck == 0u && te <= tmax) ? ((__float_as_uint(te) & ~3u) | k) : 0xFFFFFFFFu;
+    };
+    uint32_t k0 = key(h0, cc.x, te0, 0), k1 = key(h1, cc.y, te1, 1);
+    uint32_t k2 = key(h2, cc.z, te2, 2), k3 = key(h3, cc.w, te3, 3);
+    cswap(k0, k1);
+    cswap(k2, k3);
+    cswap(k0, k2);
+    cswap(k1, k3);
+    cswap(k1, k2);
+    if (k0 != 0xFFFFFFFFu) {
+        // push the farther ones (far to near), descend into the nearest
+        const uint32_t ks[3] = {k3, k2, k1};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            if (ks[a] != 0xFFFFFFFFu) {
+                const uint32_t node = pick4(ci.x, ci.y, ci.z, ci.w, ks[a] & 3u);
+                if (sp < TRAVERSAL_STACK) {
+                    stack_node[sp] = node;
+                    stack_t[sp] = __uint_as_float(ks[a] & ~3u);
+                    ++sp;
+                } else {
+                    atomicOr(status, ERR_STACK_OVERFLOW);
+                }
+            }
+        }
+        cur = pick4(ci.x, ci.y, ci.z, ci.w, k0 & 3u);
+        if (cur >= n_nodes4) {
+            atomicOr(status, ERR_BAD_NODE);
+            return false;
+        }
+        return true;
+    }
+    while (sp > 0) {
+        --sp;
+        if (stack_t[sp] <= tmax) {
+            cur = stack_node[sp];
+            return cur < n_nodes4;
+        }
+    }
+    return false;
+}
+
 template <class Leaf>
 __device__ __forceinline__ void traverse4_core(const float4* nodes4, uint32_t n_nodes4,
                                                uint32_t n_prims, const RayK& ray, float& tmax,
@@ -443,80 +526,8 @@ __device__ __forceinline__ void traverse4_core(const float4* nodes4, uint32_t n_
             atomicOr(status, ERR_ITERATION_CAP);
             return;
         }
-        const float4* np = nodes4 + 8 * size_t(cur);
-        const float4 nx = ldg4(np + nf.x), fx = ldg4(np + (nf.x ^ 1)), ny = ldg4(np + nf.y),
-                     fy = ldg4(np + (nf.y ^ 1)), nz = ldg4(np + nf.z), fz = ldg4(np + (nf.z ^ 1));
-        const uint4 ci = __ldg(reinterpret_cast<const uint4*>(np + 6));
-        const uint4 cc = __ldg(reinterpret_cast<const uint4*>(np + 7));
-        tc.box += 4;
-        float te0, te1, te2, te3;
-        bool h0, h1, h2, h3;
-        auto test = [&](float nxk, float fxk, float nyk, float fyk, float nzk, float fzk,
-                        uint32_t cck, float& te) {
-            return slab4_child(ray, nxk, fxk, nyk, fyk, nzk, fzk, tmax, te) && cck != EMPTY_CHILD;
-        };
-        h0 = test(nx.x, fx.x, ny.x, fy.x, nz.x, fz.x, cc.x, te0);
-        h1 = test(nx.y, fx.y, ny.y, fy.y, nz.y, fz.y, cc.y, te1);
-        h2 = test(nx.z, fx.z, ny.z, fy.z, nz.z, fz.z, cc.z, te2);
-        h3 = test(nx.w, fx.w, ny.w, fy.w, nz.w, fz.w, cc.w, te3);
-        // leaves: one shared copy of the primitive loop, iterated over a bit mask
-        uint32_t leaves = (h0 && cc.x != 0u ? 1u : 0u) | (h1 && cc.y != 0u ? 2u : 0u) |
-                          (h2 && cc.z != 0u ? 4u : 0u) | (h3 && cc.w != 0u ? 8u : 0u);
-        while (leaves) {
-            uint32_t k = uint32_t(__ffs(leaves) - 1);
-            leaves &= leaves - 1u;
-            uint32_t first = pick4(ci.x, ci.y, ci.z, ci.w, k);
-            uint32_t count = pick4(cc.x, cc.y, cc.z, cc.w, k);
-            if (first > n_prims || count > n_prims - first) {
-                atomicOr(status, ERR_BAD_NODE);
-                return;
-            }
-            leaf(first, count);
-        }
-        // interior children: key = entry distance bits (non-negative float) | child slot
-        auto key = [&](bool h, uint32_t cck, float te, uint32_t k) {
-            return (h && cck == 0u && te <= tmax) ? ((__float_as_uint(te) & ~3u) | k) : 0xFFFFFFFFu;
-        };
-        uint32_t k0 = key(h0, cc.x, te0, 0), k1 = key(h1, cc.y, te1, 1);
-        uint32_t k2 = key(h2, cc.z, te2, 2), k3 = key(h3, cc.w, te3, 3);
-        cswap(k0, k1);
-        cswap(k2, k3);
-        cswap(k0, k2);
-        cswap(k1, k3);
-        cswap(k1, k2);
-        if (k0 != 0xFFFFFFFFu) {
-            // push the farther ones (far to near), descend into the nearest
-            uint32_t ks[3] = {k3, k2, k1};
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                if (ks[a] != 0xFFFFFFFFu) {
-                    uint32_t node = pick4(ci.x, ci.y, ci.z, ci.w, ks[a] & 3u);
-                    if (sp < TRAVERSAL_STACK) {
-                        stack_node[sp] = node;
-                        stack_t[sp] = __uint_as_float(ks[a] & ~3u);
-                        ++sp;
-                    } else {
-                        atomicOr(status, ERR_STACK_OVERFLOW);
-                    }
-                }
-            }
-            cur = pick4(ci.x, ci.y, ci.z, ci.w, k0 & 3u);
-            if (cur >= n_nodes4) {
-                atomicOr(status, ERR_BAD_NODE);
-                return;
-            }
-            continue;
-        }
-        bool found = false;
-        while (sp > 0) {
-            --sp;
-            if (stack_t[sp] <= tmax) {
-                cur = stack_node[sp];
-                found = cur < n_nodes4;
-                break;
-            }
-        }
-        if (!found)
+        if (!visit4(nodes4, n_nodes4, n_prims, ray, nf, tmax, cur, sp, stack_node, stack_t,
+                    status, tc, leaf))
             return;
     }
 }

@@ -303,6 +303,115 @@ __global__ void __launch_bounds__(256) k_path_extend(FrameParams P, PathState S,
     flush_counts(tc, P.stats + 3);
 }
 
+// ---------------------------------------------------------------------------------------------
+// Extension rays with per-lane refill: a lane whose ray is finished takes the next queued ray as
+// soon as at least REFILL_MIN lanes of its warp are idle (one atomic per refill), so the lanes of
+// a warp do not wait for the warp's slowest ray.  Each lane runs the same node visits (visit4)
+// as the one-ray-per-thread kernel.  Scenes with a combined tree or a single enabled geometry
+// (P.refill_geom: -2 combined, else the geometry's index).
+// ---------------------------------------------------------------------------------------------
+constexpr uint32_t REFILL_MIN = 8;
+
+template <uint32_t MASK>
+__global__ void __launch_bounds__(256) k_path_extend_refill(FrameParams P, PathState S, int q)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        S.ctr[q ^ 1] = 0;  // the other queue was consumed by the shade pass that produced q
+    const uint32_t count = S.ctr[q];
+    const uint32_t* queue = S.queue[q];
+    const uint32_t lane = lane_id();
+    const uint32_t below = (1u << lane) - 1u;
+    const SceneDev& sc = P.scene;
+    const bool combined = P.refill_geom < 0;
+    const uint32_t gi = combined ? 0u : uint32_t(P.refill_geom);
+    const GeomDev& g = sc.geoms[gi];
+    const float4* nodes4 = combined ? sc.nodes4 : g.nodes4;
+    const uint32_t n_nodes4 = combined ? sc.n_nodes4 : g.n_nodes4;
+    const uint32_t n_prims = combined ? sc.n_prims : g.n_prims;
+    const int type = combined ? -1 : g.type;
+    uint32_t stack_node[TRAVERSAL_STACK];
+    float stack_t[TRAVERSAL_STACK];
+    TraceCount tc;
+    bool active = false, exhausted = false;
+    uint32_t p = 0, cur = 0, guard = 0, hg = MISS, hs = 0;
+    int sp = 0;
+    float tmax = 0.0f;
+    RayK ray;
+    NearFar nf{0, 2, 4};
+    unsigned long long rays = 0;
+    auto leaf = [&](uint32_t first, uint32_t n) {
+        if (combined) {
+            leaf_test_mixed<MASK>(sc, ray, first, n, PATH_TNEAR, tmax, hg, hs, tc);
+            return;
+        }
+#define FR_LEAF(T)                                                                       \
+    if ((MASK & (1u << T)) && type == T) {                                               \
+        leaf_test<T>(g, gi, ray, first, n, PATH_TNEAR, tmax, hg, hs, tc);                 \
+        return;                                                                          \
+    }
+        FR_LEAF(FR_GEOM_SPHERE)
+        FR_LEAF(FR_GEOM_CYLINDER)
+        FR_LEAF(FR_GEOM_POLYHEDRON)
+        FR_LEAF(FR_GEOM_MESH)
+#undef FR_LEAF
+    };
+    while (true) {
+        const uint32_t idle = __ballot_sync(0xffffffffu, !active);
+        if (!exhausted && (__popc(idle) >= int(REFILL_MIN) || idle == 0xffffffffu)) {
+            const uint32_t n = uint32_t(__popc(idle));
+            uint32_t base = 0;
+            if (lane == 0)
+                base = atomicAdd(S.ctr + 2, n);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (base + n >= count)
+                exhausted = true;
+            if (!active) {
+                const uint32_t item = base + uint32_t(__popc(idle & below));
+                if (item < count) {
+                    p = queue[item];
+                    ray = make_rayk(xyz(S.ray_o[p]), xyz(S.ray_d[p]));
+                    nf = near_far(ray);
+                    tmax = __int_as_float(0x7f800000);
+                    hg = MISS;
+                    hs = 0;
+                    cur = 0;
+                    sp = 0;
+                    guard = n_nodes4 + 8u;
+                    active = n_nodes4 != 0;
+                    if (!active)
+                        S.hit[p] = make_uint2(MISS, 0u);
+                    ++rays;
+                }
+            }
+        }
+        if (__ballot_sync(0xffffffffu, active) == 0u) {
+            if (exhausted)
+                break;
+            continue;
+        }
+        if (active) {
+            bool more = false;
+            if (--guard == 0u)
+                atomicOr(sc.status, ERR_ITERATION_CAP);
+            else
+                more = visit4(nodes4, n_nodes4, n_prims, ray, nf, tmax, cur, sp, stack_node,
+                              stack_t, sc.status, tc, leaf);
+            if (!more) {
+                uint32_t prim = 0;
+                if (hg != MISS)
+                    prim = __ldg((combined ? sc.order : sc.geoms[hg].order) + hs);
+                S.hit[p] = make_uint2(hg, prim);
+                active = false;
+            }
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1)
+        rays += __shfl_xor_sync(0xffffffffu, rays, off);
+    if (lane == 0 && rays)
+        atomicAdd(P.stats + 0, rays);
+    flush_counts(tc, P.stats + 3);
+}
+
 // Representative-point area-light shading of one preview sample
 // (fresnel/cpu/TracerDirect.cc:120-200).
 __device__ __forceinline__ C3 preview_shade(const FrameParams& P, const GeomDev& g,
@@ -437,6 +546,8 @@ LaunchShape path_launch_shape(int num_sms)
     LaunchShape s;
     s.shade_grid = num_sms * blocks_per_sm(k_path_shade<>);
     s.shade_grid_occ[0] = num_sms * blocks_per_sm(k_path_shade<3>);
+    s.refill_grid[0] = num_sms * blocks_per_sm(k_path_extend_refill<MASK_SPHERES>);
+    s.refill_grid[1] = num_sms * blocks_per_sm(k_path_extend_refill<MASK_ALL>);
     s.shade_grid_occ[1] = num_sms * blocks_per_sm(k_path_shade<4>);
     s.extend_grid[0] = num_sms * blocks_per_sm(k_path_extend<2, MASK_SPHERES>);
     s.extend_grid[1] = num_sms * blocks_per_sm(k_path_extend<2, MASK_ALL>);
@@ -496,6 +607,13 @@ void launch_path_extend(const FrameParams& P, const PathState& S, int iteration,
             k_path_extend_persistent<MASK_SPHERES><<<shape.persistent_grid[0], 256, 0, st>>>(P, S, q);
         else
             k_path_extend_persistent<MASK_ALL><<<shape.persistent_grid[1], 256, 0, st>>>(P, S, q);
+        return;
+    }
+    if (P.bvh_width == 4 && P.refill && P.refill_geom != -1) {
+        if (spheres_only)
+            k_path_extend_refill<MASK_SPHERES><<<shape.refill_grid[0], 256, 0, st>>>(P, S, q);
+        else
+            k_path_extend_refill<MASK_ALL><<<shape.refill_grid[1], 256, 0, st>>>(P, S, q);
         return;
     }
     int grid = shape.extend_grid[(P.bvh_width == 4 ? 2 : 0) + (spheres_only ? 0 : 1)];

@@ -27,6 +27,9 @@ struct FrameParams {
     uint32_t tile_log2;      // primary work in 2^tile_log2-pixel square tiles (path_device.cuh)
     int shade_blocks;        // 0: shade kernel as compiled; 3 or 4: register-limited variants
     int packet;              // 1: primary rays traced warp-cooperatively (4-wide trees)
+    int refill;              // 1: extension rays with per-lane refill where refill_geom != -1
+    int refill_geom;         // -2: the scene's combined tree; >= 0: its one enabled geometry;
+                             // -1: several per-geometry trees (refill not available)
     int highlight;
     C3 hl_color;
     float4* linear;     // [h][w] running mean, linear RGBA
@@ -54,6 +57,7 @@ struct PathState {
 struct LaunchShape {
     int shade_grid;
     int shade_grid_occ[2];   // shade kernel compiled for 3|4 blocks per SM
+    int refill_grid[2];      // extension kernel with per-lane refill [spheres only|all types]
     int extend_grid[4];      // [width 2|4][spheres only|all types]
     int persistent_grid[2];  // 4-wide persistent extend kernel [spheres only|all types]
     int primary_grid[2];     // 4-wide persistent primary kernel [spheres only|all types]

@@ -1,4 +1,5 @@
-"""Warp-cooperative primary traversal (device option "packet") against per-ray traversal.
+"""Traversal variants against one ray per thread: warp-cooperative primary rays (device option
+"packet") and extension rays with per-lane refill (device option "refill").
 
 Each lane of a packet tests exactly the leaves its own ray reaches, so the primary hits must be
 the same as with one ray per thread (only primitives at exactly equal distance could be ordered
@@ -22,22 +23,23 @@ SCENES = {
 }
 
 
+@pytest.mark.parametrize("option", ["packet", "refill"])
 @pytest.mark.parametrize("name", list(SCENES))
-def test_packet_matches_per_ray(name, gpu_device):
+def test_variant_matches_per_ray(name, option, gpu_device):
     build, w, h = SCENES[name]
     dd = gpu_device._device
-    old = dd.getOption("packet")
+    old = dd.getOption(option)
     out = []
     try:
-        for packet in (0, 1):
-            dd.setOption("packet", packet)
+        for value in (0, 1):
+            dd.setOption(option, value)
             scene = build(gpu_device)
             t = fresnel.tracer.Path(gpu_device, w=w, h=h)
             t.seed = 17
             t.sample(scene, samples=8, reset=False)
             out.append((numpy.array(t.linear_output[:], copy=True), t._tracer.primaryHits()))
     finally:
-        dd.setOption("packet", old)
+        dd.setOption(option, old)
     (la, ha), (lb, hb) = out
     assert numpy.count_nonzero(ha[..., 0] != 0xFFFFFFFF) > 0
     same_hits = numpy.all(ha == hb, axis=-1).mean()
