@@ -46,3 +46,25 @@ def test_variant_matches_per_ray(name, option, gpu_device):
     assert same_hits >= 0.9999, f"{same_hits:.5%} of primary hits agree"
     close = numpy.all(numpy.abs(la - lb) <= 1e-5, axis=-1).mean()
     assert close >= 0.999, f"{close:.4%} of pixels agree"
+
+
+def test_combined_tree_matches_per_geometry_trees(gpu_device):
+    """A mixed scene traced through its combined tree finds the same closest hits as through
+    one tree per geometry (Preview hit ids; exact-distance ties aside)."""
+    from parity import preview_hits
+    dd = gpu_device._device
+    old = dd.getOption("combined")
+    out = []
+    try:
+        for combined in (0, 1):
+            dd.setOption("combined", combined)
+            scene = workloads.config3(gpu_device, scale=0.01)
+            out.append(preview_hits(gpu_device, scene, 160, 90, 2))
+    finally:
+        dd.setOption("combined", old)
+    (ha, la, _), (hb, lb, _) = out
+    assert numpy.count_nonzero(ha[..., 0]) > 0
+    same = numpy.all(ha == hb, axis=-1).mean()
+    assert same >= 0.9999, f"{same:.5%} of hit ids agree"
+    agree = numpy.all(numpy.all(ha == hb, axis=-1), axis=-1)
+    assert numpy.abs(la - lb)[agree].max() <= 1e-6
