@@ -245,6 +245,7 @@ struct fr_tracer {
     DevArray<uint32_t> srgb;
     DevArray<uint2> preview_hits;
     DevArray<unsigned long long> stats;
+    DevArray<uint32_t> hist;  // Tracer.histogram counts
     uint64_t launches = 0;
     uint64_t builds = 0;
     uint64_t refits = 0;
@@ -1625,6 +1626,44 @@ fr_status fr_tracer_read_srgb(fr_tracer* t, uint8_t* host, size_t nbytes)
     FR_CUDA(cudaMemcpyAsync(host, t->srgb.ptr, nbytes, cudaMemcpyDeviceToHost, t->dev->stream),
             "downloading the sRGB output");
     FR_CUDA(cudaStreamSynchronize(t->dev->stream), "downloading the sRGB output");
+    return FR_OK;
+}
+
+fr_status fr_tracer_histogram(fr_tracer* t, uint32_t* counts, size_t nbytes)
+{
+    FR_CHECK_NULL(t);
+    FR_CHECK_NULL(counts);
+    if (nbytes != size_t(HIST_BINS) * 4 * sizeof(uint32_t))
+        return fail(FR_ERR_INVALID, "histogram size mismatch: " + std::to_string(HIST_BINS) +
+                                        " x 4 counts of 4 bytes");
+    fr_status s = use_device(t->dev);
+    if (s != FR_OK)
+        return s;
+    FR_CUDA(t->hist.reserve(size_t(HIST_BINS) * 4), "allocating the histogram");
+    cudaStream_t st = t->dev->stream;
+    FR_CUDA(cudaMemsetAsync(t->hist.ptr, 0, nbytes, st), "clearing the histogram");
+    launch_histogram(t->linear.ptr, t->w * t->h, t->hist.ptr, t->dev->num_sms, st);
+    FR_CUDA(cudaGetLastError(), "launching the histogram");
+    FR_CUDA(cudaMemcpyAsync(counts, t->hist.ptr, nbytes, cudaMemcpyDeviceToHost, st),
+            "downloading the histogram");
+    FR_CUDA(cudaStreamSynchronize(st), "histogram");
+    return FR_OK;
+}
+
+fr_status fr_host_alloc(size_t nbytes, void** out)
+{
+    FR_CHECK_NULL(out);
+    *out = nullptr;
+    if (nbytes == 0)
+        return fail(FR_ERR_INVALID, "host allocation of 0 bytes");
+    FR_CUDA(cudaHostAlloc(out, nbytes, cudaHostAllocPortable), "allocating page-locked host memory");
+    return FR_OK;
+}
+
+fr_status fr_host_free(void* host)
+{
+    if (host)
+        FR_CUDA(cudaFreeHost(host), "freeing page-locked host memory");
     return FR_OK;
 }
 

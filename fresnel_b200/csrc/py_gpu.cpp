@@ -57,8 +57,54 @@ struct GeometryCore {
 // ---------------------------------------------------------------------------------------------
 // arrays
 // ---------------------------------------------------------------------------------------------
+// Host copy of an array in page-locked memory (fr_host_alloc), so that uploads and downloads
+// run at full link speed without a staging copy; plain heap memory if none can be had.
+class HostStore {
+public:
+    HostStore() = default;
+    HostStore(const HostStore&) = delete;
+    HostStore& operator=(const HostStore&) = delete;
+    ~HostStore() { release(); }
+    void assign(size_t n)
+    {
+        release();
+        if (n == 0)
+            return;
+        void* p = nullptr;
+        if (fr_host_alloc(n, &p) == FR_OK) {
+            ptr_ = static_cast<unsigned char*>(p);
+            pinned_ = true;
+        } else {
+            heap_.assign(n, 0);
+            ptr_ = heap_.data();
+        }
+        n_ = n;
+        std::memset(ptr_, 0, n);
+    }
+    unsigned char* data() { return ptr_; }
+    size_t size() const { return n_; }
+    bool empty() const { return n_ == 0; }
+    bool pinned() const { return pinned_; }
+
+private:
+    void release()
+    {
+        if (pinned_)
+            fr_host_free(ptr_);
+        heap_.clear();
+        heap_.shrink_to_fit();
+        ptr_ = nullptr;
+        n_ = 0;
+        pinned_ = false;
+    }
+    unsigned char* ptr_ = nullptr;
+    size_t n_ = 0;
+    bool pinned_ = false;
+    std::vector<unsigned char> heap_;
+};
+
 struct ArrayBase {
-    std::vector<unsigned char> data;
+    HostStore data;
     std::vector<py::ssize_t> shape;
     size_t item = 4;        // bytes per scalar
     std::string format;     // python struct format of one scalar
@@ -136,7 +182,7 @@ std::shared_ptr<A> make_array(std::vector<py::ssize_t> shape, bool byte_scalar =
     a->item = byte_scalar ? 1 : 4;
     a->format = byte_scalar ? py::format_descriptor<unsigned char>::format()
                             : py::format_descriptor<float>::format();
-    a->data.assign(a->count() * a->item, 0);
+    a->data.assign(a->count() * a->item);
     return a;
 }
 
@@ -746,7 +792,22 @@ PYBIND11_MODULE(_gpu, m)
         .def("getSeed", [](TracerH& t) { return t.seed; })
         .def("setSeed", [](TracerH& t, unsigned s) { t.seed = s; })
         .def("getStats", &TracerH::stats)
-        .def("resetStats", [](TracerH& t) { check(fr_tracer_reset_stats(t.tracer)); });
+        .def("resetStats", [](TracerH& t) { check(fr_tracer_reset_stats(t.tracer)); })
+        .def("setLinearOutput",
+             [](TracerH& t, py::array_t<float, py::array::c_style | py::array::forcecast> a) {
+                 // parity hook (no counterpart in the reference): upload an (h, w, 4) linear
+                 // RGBA image into the output buffer
+                 if (a.ndim() != 3 || a.shape(0) != py::ssize_t(t.h) ||
+                     a.shape(1) != py::ssize_t(t.w) || a.shape(2) != 4)
+                     throw std::runtime_error("expected a float32 image of shape (h, w, 4)");
+                 check(fr_tracer_write_linear(t.tracer, a.data(), size_t(a.size()) * sizeof(float)));
+             })
+        .def("histogram", [](TracerH& t) {
+            // device-side Tracer.histogram counts, [512][4] uint32 (lightness, R, G, B)
+            py::array_t<uint32_t> out({py::ssize_t(512), py::ssize_t(4)});
+            check(fr_tracer_histogram(t.tracer, out.mutable_data(), 512 * 4 * sizeof(uint32_t)));
+            return out;
+        });
 
     py::class_<TracerDirectH, TracerH, std::shared_ptr<TracerDirectH>>(m, "TracerDirect")
         .def(py::init<std::shared_ptr<DeviceH>, unsigned, unsigned>())

@@ -237,6 +237,44 @@ __global__ void __launch_bounds__(256) k_path_fold(FrameParams P, PathState S)
     write_pixel(P, p, mean.x, mean.y, mean.z, mean.w);
 }
 
+// Tracer.histogram (fresnel/tracer.py:79-108) over the linear output, with numpy's float32
+// arithmetic: for every pixel with alpha > 0, the lightness l = (0.21 r + 0.72 g) + 0.07 b
+// (each product and sum rounded to float32) and r, g, b are raised to float32(1/2.2) and
+// counted in HIST_BINS equal bins over [0, 1]; 1 falls in the last bin, values outside
+// [0, 1] and NaN in none.  The power is evaluated in double and rounded once to float32.
+// counts[bin * 4 + channel], channels (l, r, g, b); counts must be zero on entry.
+__global__ void __launch_bounds__(256) k_histogram(const float4* linear, uint32_t n,
+                                                   uint32_t* counts)
+{
+    __shared__ uint32_t h[HIST_BINS * 4];
+    for (uint32_t i = threadIdx.x; i < HIST_BINS * 4; i += blockDim.x)
+        h[i] = 0;
+    __syncthreads();
+    const double e = double(float(1.0 / 2.2));
+    auto count = [&](float x, uint32_t c) {
+        const float v = __double2float_rn(pow(double(x), e));
+        if (v >= 0.0f && v <= 1.0f) {
+            const uint32_t b = min(uint32_t(v * float(HIST_BINS)), HIST_BINS - 1u);
+            atomicAdd(&h[b * 4u + c], 1u);
+        }
+    };
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const float4 a = ldg4(linear + p);
+        if (!(a.w > 0.0f))
+            continue;
+        const float l = __fadd_rn(__fadd_rn(__fmul_rn(float(0.21), a.x), __fmul_rn(float(0.72), a.y)),
+                                  __fmul_rn(float(0.07), a.z));
+        count(l, 0);
+        count(a.x, 1);
+        count(a.y, 2);
+        count(a.z, 3);
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < HIST_BINS * 4; i += blockDim.x)
+        if (h[i])
+            atomicAdd(counts + i, h[i]);
+}
+
 template <int MINB = 1>
 __global__ void __launch_bounds__(256, MINB) k_path_shade(FrameParams P, PathState S, int in_q,
                                                           int out_q)
@@ -620,6 +658,14 @@ void launch_path_extend(const FrameParams& P, const PathState& S, int iteration,
     auto k = pick(P, k_path_extend<2, MASK_SPHERES>, k_path_extend<2, MASK_ALL>,
                   k_path_extend<4, MASK_SPHERES>, k_path_extend<4, MASK_ALL>);
     k<<<grid, 256, 0, st>>>(P, S, q);
+}
+
+void launch_histogram(const float4* linear, uint32_t n, uint32_t* counts, int num_sms,
+                      cudaStream_t st)
+{
+    const uint32_t blocks = (n + 255u) / 256u;
+    const uint32_t cap = uint32_t(num_sms > 0 ? num_sms : 1) * 4u;
+    k_histogram<<<blocks < cap ? (blocks ? blocks : 1u) : cap, 256, 0, st>>>(linear, n, counts);
 }
 
 void launch_preview(const FrameParams& P, uint32_t aa_n, uint2* hits, cudaStream_t st)

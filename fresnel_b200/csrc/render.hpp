@@ -80,6 +80,11 @@ void launch_path_fold(const FrameParams& P, const PathState& S, cudaStream_t st)
 // Diagnostic comparison of the two 4-wide traversal forms (sphere scenes).
 void launch_traversal_compare(const SceneDev& sc, const float* rays, uint32_t n, uint32_t* out,
                               cudaStream_t st);
+// Tracer.histogram: counts[HIST_BINS][4] (lightness, R, G, B) of the visible pixels of a
+// linear RGBA image of n pixels; counts must be zeroed first.
+constexpr uint32_t HIST_BINS = 512;
+void launch_histogram(const float4* linear, uint32_t n, uint32_t* counts, int num_sms,
+                      cudaStream_t st);
 // TracerDirect::render
 void launch_preview(const FrameParams& P, uint32_t aa_n, uint2* hits, cudaStream_t st);
 

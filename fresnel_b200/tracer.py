@@ -9,6 +9,9 @@ import numpy
 from . import _common
 from . import util
 
+# numpy.histogram's bin edges for 512 bins over [0, 1] of float32 data (Tracer.histogram)
+_HIST_EDGES = numpy.histogram(numpy.zeros(0, numpy.float32), bins=512, range=[0, 1])[1]
+
 
 class Tracer:
     """Base class (fresnel/tracer.py:20-154)."""
@@ -34,18 +37,11 @@ class Tracer:
 
     def histogram(self):
         """Lightness and R, G, B histograms (512 bins, gamma 2.2) of the visible pixels
-        (fresnel/tracer.py:79-108).  Returns ``(hist[512, 4], bin_upper_edges)``."""
-        a = numpy.array(self.linear_output[:])
-        img = a[a[:, :, 3] > 0]
-        r, g, b = img[:, 0], img[:, 1], img[:, 2]
-        lum = 0.21 * r + 0.72 * g + 0.07 * b
-        n = 512
-        cols = []
-        bins = None
-        for ch in (lum, r, g, b):
-            h, bins = numpy.histogram(ch**(1 / 2.2), bins=n, range=[0, 1])
-            cols.append(h)
-        return numpy.stack(cols, axis=1), bins[1:]
+        (fresnel/tracer.py:79-108), computed on the device from the linear output (only the
+        8 KB of counts cross to the host).  Returns ``(hist[512, 4] int64, bin_upper_edges)``;
+        the edges are numpy.histogram's for 512 bins over [0, 1]."""
+        counts = self._tracer.histogram()
+        return counts.astype(numpy.int64), _HIST_EDGES[1:].copy()
 
     @property
     def output(self):

@@ -259,6 +259,17 @@ FR_API fr_status fr_tracer_read_linear(fr_tracer* tr, float* host, size_t nbytes
 FR_API fr_status fr_tracer_read_srgb(fr_tracer* tr, uint8_t* host, size_t nbytes);
 FR_API fr_status fr_tracer_write_linear(fr_tracer* tr, const float* host, size_t nbytes);
 FR_API fr_status fr_tracer_write_srgb(fr_tracer* tr, const uint8_t* host, size_t nbytes);
+/* Tracer.histogram (fresnel/tracer.py:79-108) computed on the device from the linear output:
+ * counts[512][4] (nbytes = 8192) of the pixels with alpha > 0, columns lightness
+ * l = 0.21 r + 0.72 g + 0.07 b, R, G, B, each value raised to 1/2.2 and binned over [0, 1] in
+ * 512 equal bins as numpy.histogram does (float32 arithmetic as numpy's; the power rounded
+ * once from double precision, where numpy's float32 power may differ by an ulp). */
+FR_API fr_status fr_tracer_histogram(fr_tracer* tr, uint32_t* counts, size_t nbytes);
+/* Page-locked host memory (no counterpart in the reference, whose arrays live in pageable
+ * memory, fresnel/gpu/Array.h:98-223): fr_tracer_read_* and fr_geometry_write copy to and
+ * from it at full link speed without a staging copy.  fr_host_free(NULL) does nothing. */
+FR_API fr_status fr_host_alloc(size_t nbytes, void** out);
+FR_API fr_status fr_host_free(void* host);
 FR_API fr_status fr_tracer_get_stats(const fr_tracer* tr, fr_stats* out);
 /* Parity hook (no counterpart in the reference): the closest hits of the primary rays of the
  * first sample of the last wavefront of the device's last path render, which must have been
