@@ -184,6 +184,8 @@ struct fr_geometry {
     fr_material material{}, outline{};
     float outline_width = 0.0f;
     DevArray<float> position, radius, color, points, orientation, vertices, planes;
+    DevArray<float> angle;         // polygon: [n] radians; orientation holds their quaternions
+    float rounding_radius = 0.0f;  // polygon
     BvhBuffers bvh;
     bool bvh_dirty = true;
     uint64_t gen = 0;        // changes whenever the primitives (or the build options) change
@@ -199,7 +201,7 @@ struct fr_geometry {
         case FR_FIELD_POSITION:
             if (type == FR_GEOM_CYLINDER)
                 return nullptr;
-            count = size_t(n) * 3;
+            count = size_t(n) * (type == FR_GEOM_POLYGON ? 2 : 3);
             return &position;
         case FR_FIELD_RADIUS:
             if (type != FR_GEOM_SPHERE && type != FR_GEOM_CYLINDER)
@@ -221,6 +223,11 @@ struct fr_geometry {
                 return nullptr;
             count = size_t(n) * 4;
             return &orientation;
+        case FR_FIELD_ANGLE:
+            if (type != FR_GEOM_POLYGON)
+                return nullptr;
+            count = n;
+            return &angle;
         }
         return nullptr;
     }
@@ -380,7 +387,7 @@ fr_status finish_geometry(fr_geometry* g, fr_geometry** out)
         delete g;
         return s;
     }
-    for (int f = 0; f <= FR_FIELD_ORIENTATION; ++f) {
+    for (int f = 0; f <= FR_FIELD_ANGLE; ++f) {
         if ((s = alloc_field(g, f)) != FR_OK) {
             delete g;
             return s;
@@ -614,6 +621,8 @@ fr_status prepare_scene(fr_scene* sc, fr_tracer* tr)
             d.planes = g->planes.ptr;
             d.n_faces = g->n_faces;
             d.n_planes = g->n_planes;
+            d.n_vertices = g->type == FR_GEOM_POLYGON ? g->n_vertices : 0u;
+            d.rounding_radius = g->rounding_radius;
             d.color_by_face = g->color_by_face;
             d.outline_width = g->outline_width;
             d.material = to_mat(g->material);
@@ -1166,6 +1175,55 @@ fr_status fr_geometry_create_mesh(fr_scene* scene, const float* vertices, uint32
     return finish_geometry(g, out);
 }
 
+fr_status fr_geometry_create_polygon(fr_scene* scene, const float* vertices, uint32_t n_vertices,
+                                     float rounding_radius, uint32_t n, fr_geometry** out)
+{
+    if (n_vertices)
+        FR_CHECK_NULL(vertices);
+    fr_geometry* g = nullptr;
+    fr_status s = new_geometry(scene, FR_GEOM_POLYGON, n, out, &g);
+    if (s != FR_OK)
+        return s;
+    g->n_vertices = n_vertices;
+    g->rounding_radius = rounding_radius;
+    // bounding radius: the farthest vertex plus the rounding (fresnel/cpu/GeometryPolygon.cc:58-67)
+    float r = 0.0f;
+    for (uint32_t i = 0; i < n_vertices; ++i) {
+        const float x = vertices[2 * i], y = vertices[2 * i + 1];
+        r = std::max(r, sqrtf(x * x + y * y));
+    }
+    g->poly_radius = r + rounding_radius;
+    // every angle starts at 0: its quaternion is the identity
+    std::vector<float> q(size_t(n) * 4, 0.0f);
+    for (uint32_t i = 0; i < n; ++i)
+        q[4 * size_t(i)] = 1.0f;
+    cudaError_t e = use_device(scene->dev) == FR_OK ? g->vertices.reserve(size_t(n_vertices) * 2)
+                                                    : cudaErrorUnknown;
+    if (e == cudaSuccess && n_vertices)
+        e = cudaMemcpy(g->vertices.ptr, vertices, size_t(n_vertices) * 2 * sizeof(float),
+                       cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = g->orientation.reserve(q.size());
+    if (e == cudaSuccess && n)
+        e = cudaMemcpy(g->orientation.ptr, q.data(), q.size() * sizeof(float),
+                       cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        delete g;
+        return cuda_fail(e, "uploading polygon vertices");
+    }
+    return finish_geometry(g, out);
+}
+
+fr_status fr_geometry_get_radius(const fr_geometry* g, float* radius)
+{
+    FR_CHECK_NULL(g);
+    FR_CHECK_NULL(radius);
+    if (g->type != FR_GEOM_POLYGON)
+        return fail(FR_ERR_INVALID, "only polygon geometries have a radius");
+    *radius = g->poly_radius;
+    return FR_OK;
+}
+
 fr_status fr_geometry_destroy(fr_geometry* g)
 {
     if (!g)
@@ -1213,9 +1271,30 @@ fr_status fr_geometry_write(fr_geometry* g, int field, const void* host, size_t 
     fr_status s = use_device(g->scene->dev);
     if (s != FR_OK)
         return s;
+    if (field == FR_FIELD_ANGLE && (offset % sizeof(float) != 0 || nbytes % sizeof(float) != 0))
+        return fail(FR_ERR_INVALID, "angle writes must cover whole floats");
     FR_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(a->ptr) + offset, host, nbytes,
                             cudaMemcpyHostToDevice, g->scene->dev->stream),
             "uploading a geometry array");
+    if (field == FR_FIELD_ANGLE) {
+        // the rotation quaternion of each angle, computed here on the host as the reference's
+        // CPU path does, quat::fromAxisAngle((0, 0, 1), angle) (fresnel/cpu/GeometryPolygon.cc:
+        // 153, fresnel/common/VectorMath.h:924-928 with cosf/sinf)
+        const float* a_host = static_cast<const float*>(host);
+        const size_t first = offset / sizeof(float), count = nbytes / sizeof(float);
+        std::vector<float> q(count * 4);
+        for (size_t k = 0; k < count; ++k) {
+            const float half = a_host[k] / 2.0f;
+            const float sh = sinf(half);
+            q[4 * k] = cosf(half);
+            q[4 * k + 1] = sh * 0.0f;
+            q[4 * k + 2] = sh * 0.0f;
+            q[4 * k + 3] = sh * 1.0f;
+        }
+        FR_CUDA(cudaMemcpyAsync(g->orientation.ptr + 4 * first, q.data(), q.size() * sizeof(float),
+                                cudaMemcpyHostToDevice, g->scene->dev->stream),
+                "uploading polygon rotations");
+    }
     FR_CUDA(cudaStreamSynchronize(g->scene->dev->stream), "uploading a geometry array");
     if (field != FR_FIELD_COLOR)
         mark_moved(g);  // colours do not move primitives

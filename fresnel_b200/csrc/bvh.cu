@@ -92,12 +92,19 @@ __device__ Box prim_bounds(const BuildInput& in, uint32_t i)
         grow(b, v3(p.x + r, p.y + r, p.z + r));
         break;
     }
-    default: {
+    case FR_GEOM_MESH: {
         uint32_t inst = i / in.n_faces, face = i - inst * in.n_faces;
         V3 p = load3(in.position, inst);
         Qt q = loadq(in.orientation, inst);
         for (int k = 0; k < 3; ++k)
             grow(b, rotate(q, load3(in.vertices, 3 * face + k)) + p);
+        break;
+    }
+    default: {  // polygon in the z = 0 plane (fresnel/cpu/GeometryPolygon.cc:89-104)
+        const float x = in.position[2 * size_t(i)], y = in.position[2 * size_t(i) + 1];
+        const float r = in.poly_radius;
+        grow(b, v3(x - r, y - r, 0.0f - 1e-5f));
+        grow(b, v3(x + r, y + r, 0.0f + 1e-5f));
         break;
     }
     }
@@ -426,11 +433,17 @@ __device__ __forceinline__ void write_record(const BuildInput& in, uint32_t p, f
         r[1] = make_float4(q.s, q.v.x, q.v.y, q.v.z);
         break;
     }
-    default: {
+    case FR_GEOM_MESH: {
         uint32_t inst = p / in.n_faces, face = p - inst * in.n_faces;
         V3 c = load3(in.position, inst);
         Qt q = loadq(in.orientation, inst);
         r[0] = make_float4(c.x, c.y, c.z, __uint_as_float(face));
+        r[1] = make_float4(q.s, q.v.x, q.v.y, q.v.z);
+        break;
+    }
+    default: {  // polygon: 2-D position and the rotation quaternion about z
+        Qt q = loadq(in.orientation, p);
+        r[0] = make_float4(in.position[2 * size_t(p)], in.position[2 * size_t(p) + 1], 0.0f, 0.0f);
         r[1] = make_float4(q.s, q.v.x, q.v.y, q.v.z);
         break;
     }

@@ -81,7 +81,7 @@ struct BuildInput {
     const float* orientation;
     const float* vertices;
     uint32_t n_faces;
-    float poly_radius;
+    float poly_radius;  // polyhedron / polygon: bounding radius about the position
 };
 
 // Several geometries' primitives in one tree (a scene's combined BVH): primitive i of the

@@ -56,6 +56,8 @@ struct GeomDev {
     const float* planes;  // [n_planes][9]: origin, unit normal, colour
     uint32_t n_faces;
     uint32_t n_planes;
+    uint32_t n_vertices;    // polygon: vertices [n_vertices][2]
+    float rounding_radius;  // polygon
     float color_by_face;
     float outline_width;
     Mat material;
@@ -230,6 +232,67 @@ __device__ __forceinline__ TriHit mesh_triangle(const GeomDev& g, uint32_t face,
     return r;
 }
 
+// Rounded polygon in the z = 0 plane (fresnel/cpu/GeometryPolygon.cc:146-230): the ray, taken
+// into the polygon's frame, meets the plane at t; the hit point counts if its signed distance to
+// the outline (negative inside, by the crossing-number test of :113-140 and the point-segment
+// distance of fresnel/common/GeometryMath.h:28-39) is at most the rounding radius.  d is the
+// outline distance (rounding radius minus the signed distance), n the plane normal facing the
+// ray (double sided), both in the polygon's frame.
+struct PgHit {
+    bool hit;
+    float t, d;
+    V3 n;
+};
+
+__device__ __forceinline__ float pg_min(float a, float b) { return (b < a) ? b : a; }  // std::min
+__device__ __forceinline__ float pg_max(float a, float b) { return (a < b) ? b : a; }  // std::max
+
+__device__ __forceinline__ PgHit polygon_hit(const GeomDev& g, V3 o, V3 d, float px, float py,
+                                             Qt q)
+{
+    PgHit r;
+    r.hit = false;
+    r.t = r.d = 0.0f;
+    r.n = v3(0, 0, 1);
+    const V3 dl = rotate(conj(q), d);
+    const V3 ol = rotate(conj(q), o - v3(px, py, 0.0f));
+    const V3 n = v3(0, 0, 1);
+    const V3 p = v3(0, 0, 0);
+    const float dd = -dot(n, p);
+    const float denom = dot(n, dl);
+    const float t = -(dd + dot(n, ol)) / denom;
+    if (double(fabsf(denom)) < 1e-5)
+        return r;
+    const V3 rh = ol + t * dl;
+    // crossing number and the distance to the nearest edge
+    const float2* vt = reinterpret_cast<const float2*>(g.vertices);
+    const uint32_t nv = g.n_vertices;
+    float min_d = 3.402823466e+38f;
+    bool odd = false;
+    float2 vj = nv ? __ldg(vt + (nv - 1u)) : make_float2(0.0f, 0.0f);
+    for (uint32_t i = 0; i < nv; ++i) {
+        const float2 vi = __ldg(vt + i);
+        const float abx = vj.x - vi.x, aby = vj.y - vi.y;
+        const float L = abx * abx + aby * aby;
+        const float s = pg_max(0.0f, pg_min(1.0f, ((rh.x - vi.x) * abx + (rh.y - vi.y) * aby) / L));
+        const float wx = rh.x - (vi.x + s * abx), wy = rh.y - (vi.y + s * aby);
+        min_d = pg_min(min_d, sqrtf(wx * wx + wy * wy));
+        if ((vi.y < rh.y && vj.y >= rh.y) || (vj.y < rh.y && vi.y >= rh.y)) {
+            if (vi.x + (rh.y - vi.y) / (vj.y - vi.y) * (vj.x - vi.x) < rh.x)
+                odd = !odd;
+        }
+        vj = vi;
+    }
+    const float d_edge = odd ? -min_d : min_d;
+    if (d_edge > g.rounding_radius)
+        return r;
+    r.d = g.rounding_radius - d_edge;
+    r.t = t;
+    r.n = (dot(n, dl) < 0.0f) ? n : -n;
+    r.hit = true;
+    return r;
+}
+
 // box and primitive tests of one thread (summed into the tracer's counters per warp)
 struct TraceCount {
     uint32_t box = 0;
@@ -262,12 +325,17 @@ __device__ __forceinline__ void leaf_test(const GeomDev& g, uint32_t gi, const R
                                      tnear, tmax);
             ok = ph.hit;
             t = ph.t;
-        } else {
+        } else if (TYPE == FR_GEOM_MESH) {
             float4 a = ldg4(g.leaf_data + 2 * s), b = ldg4(g.leaf_data + 2 * s + 1);
             TriHit th = mesh_triangle(g, __float_as_uint(a.w), ray.o, ray.d, v3(a.x, a.y, a.z),
                                       Qt{b.x, v3(b.y, b.z, b.w)});
             ok = th.hit;
             t = th.t;
+        } else {
+            float4 a = ldg4(g.leaf_data + 2 * s), b = ldg4(g.leaf_data + 2 * s + 1);
+            PgHit ph = polygon_hit(g, ray.o, ray.d, a.x, a.y, Qt{b.x, v3(b.y, b.z, b.w)});
+            ok = ph.hit;
+            t = ph.t;
         }
         if (ok && (tnear < t) && (t < tmax)) {
             tmax = t;
@@ -703,6 +771,11 @@ __device__ __forceinline__ void leaf_test_mixed(const SceneDev& sc, const RayK& 
                                       Qt{b.x, v3(b.y, b.z, b.w)});
             ok = th.hit;
             t = th.t;
+        } else if ((MASK & (1u << FR_GEOM_POLYGON)) && type == FR_GEOM_POLYGON) {
+            const float4 b = ldg4(sc.leaf_data + 2 * size_t(s) + 1);
+            PgHit ph = polygon_hit(g, ray.o, ray.d, a.x, a.y, Qt{b.x, v3(b.y, b.z, b.w)});
+            ok = ph.hit;
+            t = ph.t;
         }
         if (ok && (tnear < t) && (t < tmax)) {
             tmax = t;
@@ -719,7 +792,7 @@ struct Hit {
 
 // Geometry-type masks a kernel is specialised for (bit FR_GEOM_* set = type handled).
 constexpr uint32_t MASK_SPHERES = 1u << FR_GEOM_SPHERE;
-constexpr uint32_t MASK_ALL = 0xFu;
+constexpr uint32_t MASK_ALL = 0x1Fu;  // every FR_GEOM_* type
 
 // Closest hit over all enabled geometries of the scene.  WIDTH selects the binary (2) or
 // 4-wide (4) tree; MASK the geometry types compiled in (the host only launches a MASK that
@@ -757,6 +830,7 @@ __device__ __forceinline__ Hit trace_closest(const SceneDev& sc, V3 o, V3 d, flo
         FR_TRAVERSE(FR_GEOM_CYLINDER)
         FR_TRAVERSE(FR_GEOM_POLYHEDRON)
         FR_TRAVERSE(FR_GEOM_MESH)
+        FR_TRAVERSE(FR_GEOM_POLYGON)
 #undef FR_TRAVERSE
     }
     Hit h;
@@ -803,6 +877,7 @@ __device__ __forceinline__ Hit trace_closest_packet(const SceneDev& sc, V3 o, V3
         FR_TRAVERSE(FR_GEOM_CYLINDER)
         FR_TRAVERSE(FR_GEOM_POLYHEDRON)
         FR_TRAVERSE(FR_GEOM_MESH)
+        FR_TRAVERSE(FR_GEOM_POLYGON)
 #undef FR_TRAVERSE
     }
     Hit h;
@@ -858,6 +933,9 @@ __device__ __forceinline__ void leaf_dispatch(const GeomDev& g, LaneRay& L, uint
     else if ((MASK & (1u << FR_GEOM_MESH)) && g.type == FR_GEOM_MESH)
         leaf_test<FR_GEOM_MESH>(g, L.gi, L.ray, first, count, L.tnear, L.tmax, L.hit_geom,
                                 L.hit_slot, tc);
+    else if ((MASK & (1u << FR_GEOM_POLYGON)) && g.type == FR_GEOM_POLYGON)
+        leaf_test<FR_GEOM_POLYGON>(g, L.gi, L.ray, first, count, L.tnear, L.tmax, L.hit_geom,
+                                   L.hit_slot, tc);
 }
 
 // One step of the lane's traversal; returns false once the ray is finished (every enabled
@@ -1073,6 +1151,16 @@ __device__ __forceinline__ Surface hit_surface(const GeomDev& g, uint32_t prim, 
             }
         }
         s.d_edge = min_d;
+        break;
+    }
+    case FR_GEOM_POLYGON: {  // fresnel/cpu/GeometryPolygon.cc:146-230
+        Qt q = loadq(g.orientation, prim);
+        PgHit ph = polygon_hit(g, o, d, __ldg(g.position + 2 * size_t(prim)),
+                               __ldg(g.position + 2 * size_t(prim) + 1), q);
+        s.t = ph.t;
+        s.d_edge = ph.d;
+        s.Ng = rotate(q, ph.n);
+        s.color = loadc3(g.color, prim);
         break;
     }
     default: {  // mesh, fresnel/cpu/GeometryMesh.cc:115-193

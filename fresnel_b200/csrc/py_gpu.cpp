@@ -2,7 +2,7 @@
 //
 // Class and method names follow fresnel's `_gpu` module (fresnel/gpu/module-gpu.cc:27-43):
 // Device, Scene, Geometry, GeometrySphere, GeometryCylinder, GeometryConvexPolyhedron,
-// GeometryMesh, Tracer, TracerDirect, TracerPath and the Array* buffer classes.  Everything
+// GeometryMesh, GeometryPolygon, Tracer, TracerDirect, TracerPath and the Array* buffer classes.  Everything
 // below is host bookkeeping; all rendering work happens in libfrb200 (include/fresnel_b200.h).
 //
 // Arrays: geometry arrays keep an authoritative host copy; unmap() marks the array stale and
@@ -173,6 +173,8 @@ using ArrayRGBf = ArrayK<2>;
 using ArrayVec3f = ArrayK<3>;
 using ArrayQuat3f = ArrayK<4>;
 using Array_f = ArrayK<5>;
+using ArrayVec2f = ArrayK<6>;
+using ArrayRGBc = ArrayK<7>;
 
 template <class A>
 std::shared_ptr<A> make_array(std::vector<py::ssize_t> shape, bool byte_scalar = false)
@@ -442,6 +444,35 @@ struct GeometryMeshH : GeometryH {
         orientation = add_array<ArrayQuat3f>(FR_FIELD_ORIENTATION, {py::ssize_t(n), 4});
         color = add_array<ArrayRGBf>(FR_FIELD_COLOR, {py::ssize_t(nv), 3});
         attach();
+    }
+};
+
+struct GeometryPolygonH : GeometryH {
+    std::shared_ptr<ArrayVec2f> position;
+    std::shared_ptr<Array_f> angle;
+    std::shared_ptr<ArrayRGBf> color;
+    // argument checks of fresnel/cpu/GeometryPolygon.cc:46-52
+    GeometryPolygonH(std::shared_ptr<SceneH> s, farray vertices, float rounding_radius, unsigned n)
+        : GeometryH(std::move(s))
+    {
+        if (vertices.ndim() != 2)
+            throw std::runtime_error("vertices must be a 2-dimensional array");
+        if (vertices.shape(1) != 2)
+            throw std::runtime_error("vertices must be a Nvert by 2 array");
+        fr_geometry* g = nullptr;
+        check(fr_geometry_create_polygon(scene->scene, vertices.data(),
+                                         unsigned(vertices.shape(0)), rounding_radius, n, &g));
+        own(g);
+        position = add_array<ArrayVec2f>(FR_FIELD_POSITION, {py::ssize_t(n), 2});
+        angle = add_array<Array_f>(FR_FIELD_ANGLE, {py::ssize_t(n)});
+        color = add_array<ArrayRGBf>(FR_FIELD_COLOR, {py::ssize_t(n), 3});
+        attach();
+    }
+    float getRadius() const
+    {
+        float r = 0.0f;
+        check(fr_geometry_get_radius(geom, &r));
+        return r;
     }
 };
 
@@ -779,6 +810,13 @@ PYBIND11_MODULE(_gpu, m)
         .def("getOrientationBuffer", [](GeometryMeshH& g) { return g.orientation; })
         .def("getColorBuffer", [](GeometryMeshH& g) { return g.color; });
 
+    py::class_<GeometryPolygonH, GeometryH, std::shared_ptr<GeometryPolygonH>>(m, "GeometryPolygon")
+        .def(py::init<std::shared_ptr<SceneH>, farray, float, unsigned>())
+        .def("getPositionBuffer", [](GeometryPolygonH& g) { return g.position; })
+        .def("getAngleBuffer", [](GeometryPolygonH& g) { return g.angle; })
+        .def("getColorBuffer", [](GeometryPolygonH& g) { return g.color; })
+        .def("getRadius", &GeometryPolygonH::getRadius);
+
     py::class_<TracerH, std::shared_ptr<TracerH>>(m, "Tracer")
         .def("render", &TracerH::render)
         .def("resize", &TracerH::resize)
@@ -843,4 +881,6 @@ PYBIND11_MODULE(_gpu, m)
     export_array<ArrayVec3f>(m, "ArrayVec3f");
     export_array<ArrayQuat3f>(m, "ArrayQuat3f");
     export_array<Array_f>(m, "Array_f");
+    export_array<ArrayVec2f>(m, "ArrayVec2f");
+    export_array<ArrayRGBc>(m, "ArrayRGBc");
 }

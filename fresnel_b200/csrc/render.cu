@@ -391,6 +391,7 @@ __global__ void __launch_bounds__(256) k_path_extend_refill(FrameParams P, PathS
         FR_LEAF(FR_GEOM_CYLINDER)
         FR_LEAF(FR_GEOM_POLYHEDRON)
         FR_LEAF(FR_GEOM_MESH)
+        FR_LEAF(FR_GEOM_POLYGON)
 #undef FR_LEAF
     };
     while (true) {

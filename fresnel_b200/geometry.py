@@ -192,15 +192,50 @@ class Box(Cylinder):
 
 
 class Polygon(Geometry):
-    """Rounded polygons in the xy plane (fresnel/geometry.py:391-501).
+    """Simple polygons in the xy plane with per-primitive 2-D position, rotation angle and
+    colour, rounded by ``rounding_radius`` (fresnel/geometry.py:391-501).
 
-    Not provided by the B200 backend: constructing one raises ``RuntimeError``.
+    ``vertices`` (N_vert, 2) lists one polygon's outline counter-clockwise (concave shapes are
+    allowed); every primitive is that polygon placed at its position and rotated about z by its
+    angle.  Polygons are double sided.
     """
 
     def __init__(self, scene, vertices, position=(0, 0), angle=0, color=(0, 0, 0),
                  rounding_radius=0, N=None, material=None, outline_material=None,
                  outline_width=0.0):
-        raise RuntimeError("Polygon geometry is not implemented by the B200 backend")
+        if N is None:
+            N = len(position)
+        self._geometry = scene.device.module.GeometryPolygon(scene._scene, vertices,
+                                                             rounding_radius, N)
+        self._setup(scene, material, outline_material, outline_width)
+        self.position[:] = position
+        self.angle[:] = angle
+        self.color[:] = color
+        self._attach(scene)
+
+    @property
+    def position(self):
+        """(N, 2) `util.Array`: the position of each polygon."""
+        return self._array(self._geometry.getPositionBuffer())
+
+    @property
+    def angle(self):
+        """(N, ) `util.Array`: the rotation angle of each polygon (radians)."""
+        return self._array(self._geometry.getAngleBuffer())
+
+    @property
+    def color(self):
+        """(N, 3) `util.Array`: the colour of each polygon."""
+        return self._array(self._geometry.getColorBuffer())
+
+    def get_extents(self):
+        """Lower and upper corners, shape (2, 3): the polygons' bounding squares, 1e-5 thick in z
+        (fresnel/geometry.py:487-501)."""
+        pos = self.position[:]
+        r = self._geometry.getRadius()
+        res2d = numpy.array([numpy.min(pos - r, axis=0), numpy.max(pos + r, axis=0)])
+        return numpy.array([[res2d[0][0], res2d[0][1], -1e-5],
+                            [res2d[1][0], res2d[1][1], 1e-5]])
 
 
 class Sphere(Geometry):

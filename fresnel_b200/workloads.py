@@ -134,6 +134,44 @@ def bonds(rng, pos, n_bonds, cutoff=1.5):
     return numpy.array(out, dtype=numpy.int64).reshape(-1, 2)
 
 
+# the concave pentagon of fresnel's polygon tests, counter-clockwise
+POLYGON_OUTLINE = [[-1, -1], [1, -1], [1, 1], [0, 0], [-1, 1]]
+
+
+def polygons(device, nx=20, ny=15, spacing=2.5, rounding_radius=0.15, seed=5, spheres=0,
+             perspective=True):
+    """nx*ny rounded concave pentagons (half size of fresnel's test shape) on a jittered grid in
+    the z = 0 plane, random angles and colours, outlined; optionally ``spheres`` spheres floating
+    above the plane (a scene of two geometry types, traced through one combined tree)."""
+    rng = numpy.random.default_rng(seed)
+    gx, gy = numpy.meshgrid(numpy.arange(nx) - (nx - 1) / 2, numpy.arange(ny) - (ny - 1) / 2)
+    pos = numpy.stack([gx.ravel(), gy.ravel()], axis=1) * spacing
+    pos += rng.uniform(-0.2, 0.2, pos.shape)
+    n = len(pos)
+    scene = Scene(device, lights=light.rembrandt())
+    g = geometry.Polygon(scene, vertices=numpy.array(POLYGON_OUTLINE, numpy.float32) * 0.5,
+                         position=pos.astype(numpy.float32),
+                         angle=rng.uniform(-math.pi, math.pi, n).astype(numpy.float32),
+                         color=rng.uniform(0, 1, (n, 3)).astype(numpy.float32),
+                         rounding_radius=rounding_radius, outline_width=0.05)
+    g.material = material.Material(roughness=0.5, specular=0.3, primitive_color_mix=1.0)
+    if spheres:
+        sp = numpy.column_stack([rng.uniform(-nx, nx, spheres), rng.uniform(-ny, ny, spheres),
+                                 rng.uniform(0.8, 4.0, spheres)]) * numpy.array([spacing / 2,
+                                                                                  spacing / 2, 1])
+        geometry.Sphere(scene, position=sp.astype(numpy.float32), radius=0.6,
+                        material=material.Material(color=color.linear((0.9, 0.6, 0.2)),
+                                                   roughness=0.3))
+    if perspective:
+        scene.camera = camera.Perspective(position=(0, -1.1 * ny * spacing, 0.9 * ny * spacing),
+                                          look_at=(0, 0, 0), up=(0, 0, 1), focal_length=0.5,
+                                          height=0.35)
+    else:
+        scene.camera = camera.Orthographic(position=(0, 0, 10), look_at=(0, 0, 0), up=(0, 1, 0),
+                                           height=ny * spacing)
+    return scene
+
+
 def config3(device, scale=1.0, box=100.0):
     """Mixed scene: 200k spheres (r log-uniform in [0.3, 0.7]), 50k bonds (r = 0.1), 20k unit
     cubes and 10k icosahedra in a cube of side 100 (1280x720, 128 spp in the benchmark).

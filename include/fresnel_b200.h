@@ -97,16 +97,18 @@ enum {
     FR_GEOM_SPHERE = 0,
     FR_GEOM_CYLINDER = 1,
     FR_GEOM_POLYHEDRON = 2,
-    FR_GEOM_MESH = 3
+    FR_GEOM_MESH = 3,
+    FR_GEOM_POLYGON = 4
 };
 
 /* Per-geometry arrays exposed through the Python Array proxy. */
 enum {
-    FR_FIELD_POSITION = 0,    /* sphere/polyhedron/mesh: [N][3] f32 */
+    FR_FIELD_POSITION = 0,    /* sphere/polyhedron/mesh: [N][3] f32; polygon: [N][2] f32 */
     FR_FIELD_RADIUS = 1,      /* sphere/cylinder: [N] f32 */
-    FR_FIELD_COLOR = 2,       /* sphere/polyhedron: [N][3]; cylinder: [N][2][3]; mesh: [n_verts][3] */
+    FR_FIELD_COLOR = 2,       /* sphere/polyhedron/polygon: [N][3]; cylinder: [N][2][3]; mesh: [n_verts][3] */
     FR_FIELD_POINTS = 3,      /* cylinder: [N][2][3] f32 */
-    FR_FIELD_ORIENTATION = 4  /* polyhedron/mesh: [N][4] f32 quaternion (s, x, y, z) */
+    FR_FIELD_ORIENTATION = 4, /* polyhedron/mesh: [N][4] f32 quaternion (s, x, y, z) */
+    FR_FIELD_ANGLE = 5        /* polygon: [N] f32, rotation about z in radians */
 };
 
 /* Counters accumulated by a tracer since creation (or the last fr_tracer_reset_stats). */
@@ -204,6 +206,16 @@ FR_API fr_status fr_geometry_create_polyhedron(fr_scene* scene, const float* pla
 /* GeometryMesh(Scene, vertices[nv][3], N) (fresnel/cpu/GeometryMesh.cc:20-72; nv % 3 == 0). */
 FR_API fr_status fr_geometry_create_mesh(fr_scene* scene, const float* vertices, uint32_t n_vertices,
                                   uint32_t n, fr_geometry** out);
+/* GeometryPolygon(Scene, vertices[nv][2], rounding_radius, N) (fresnel/cpu/GeometryPolygon.cc:
+ * 20-82): simple polygons (vertices counter-clockwise, concave allowed) in the xy plane, each
+ * placed at its 2-D position and rotated about z by its angle, rounded by rounding_radius
+ * (spheropolygons), double sided.  n_vertices >= 1. */
+FR_API fr_status fr_geometry_create_polygon(fr_scene* scene, const float* vertices,
+                                            uint32_t n_vertices, float rounding_radius, uint32_t n,
+                                            fr_geometry** out);
+/* GeometryPolygon::getRadius: the largest vertex distance from the origin plus the rounding
+ * radius (the half extent of each polygon's bounding square). */
+FR_API fr_status fr_geometry_get_radius(const fr_geometry* geom, float* radius);
 /* ~Geometry / Geometry::remove (fresnel/gpu/Geometry.cc:18-58). */
 FR_API fr_status fr_geometry_destroy(fr_geometry* geom);
 /* Geometry::remove (fresnel/gpu/Geometry.cc:47-58): detach for good; enable/disable then fail. */

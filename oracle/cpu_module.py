@@ -21,7 +21,7 @@ LIB_PATHS = {
     "reference": os.path.join(HERE, "_ref", "libfresnel_ref.so"),
 }
 
-FR_GEOM_SPHERE, FR_GEOM_CYLINDER, FR_GEOM_POLYHEDRON, FR_GEOM_MESH = 0, 1, 2, 3
+FR_GEOM_SPHERE, FR_GEOM_CYLINDER, FR_GEOM_POLYHEDRON, FR_GEOM_MESH, FR_GEOM_POLYGON = 0, 1, 2, 3, 4
 
 _fp = ctypes.POINTER(ctypes.c_float)
 _up = ctypes.POINTER(ctypes.c_uint32)
@@ -61,7 +61,8 @@ class OrGeometryDesc(ctypes.Structure):
                 ("plane_origin", _fp), ("plane_normal", _fp), ("plane_color", _fp),
                 ("n_planes", ctypes.c_uint32), ("poly_radius", ctypes.c_float),
                 ("color_by_face", ctypes.c_float), ("material", FrMaterial),
-                ("outline_material", FrMaterial), ("outline_width", ctypes.c_float)]
+                ("outline_material", FrMaterial), ("outline_width", ctypes.c_float),
+                ("angle", _fp), ("rounding_radius", ctypes.c_float)]
 
 
 class OrStats(ctypes.Structure):
@@ -521,6 +522,48 @@ class GeometryMesh(Geometry):
         d.vertices, d.n_vertices = ptr(self._vertices), self._vertices.shape[0]
 
 
+class GeometryPolygon(Geometry):
+    """fresnel/cpu/GeometryPolygon.cc:20-82: vertices (N_vert, 2); position (N, 2), angle (N,),
+    colour (N, 3) per polygon; the radius is the farthest vertex plus the rounding radius."""
+
+    def __init__(self, scene, vertices, rounding_radius, N):
+        v = numpy.ascontiguousarray(vertices, dtype=numpy.float32)
+        if v.ndim != 2:
+            raise RuntimeError("vertices must be a 2-dimensional array")
+        if v.shape[1] != 2:
+            raise RuntimeError("vertices must be a Nvert by 2 array")
+        super().__init__(scene)
+        self._vertices = v
+        self._rounding_radius = float(numpy.float32(rounding_radius))
+        r = numpy.float32(0)
+        for x, y in v:
+            r = max(r, numpy.sqrt(numpy.float32(x * x) + numpy.float32(y * y), dtype=numpy.float32))
+        self._radius = float(numpy.float32(r + numpy.float32(self._rounding_radius)))
+        self._position = _buffer((N, 2))
+        self._angle = _buffer((N,))
+        self._color = _buffer((N, 3))
+
+    def getPositionBuffer(self):
+        return self._position
+
+    def getAngleBuffer(self):
+        return self._angle
+
+    def getColorBuffer(self):
+        return self._color
+
+    def getRadius(self):
+        return self._radius
+
+    def _fill(self, d, keep):
+        p, a, c = _c(self._position), _c(self._angle), _c(self._color)
+        keep += [p, a, c]
+        self._fill_common(d, FR_GEOM_POLYGON, p.shape[0])
+        d.position, d.angle, d.color = ptr(p), ptr(a), ptr(c)
+        d.vertices, d.n_vertices = ptr(self._vertices), self._vertices.shape[0]
+        d.rounding_radius = self._rounding_radius
+
+
 class Tracer:
     """fresnel/cpu/Tracer.cc: output buffers, highlight warning, seed."""
 
@@ -708,5 +751,5 @@ class _ModuleView:
 
 
 __all__ = ["Device", "Scene", "Geometry", "GeometrySphere", "GeometryCylinder",
-           "GeometryConvexPolyhedron", "GeometryMesh", "Tracer", "TracerDirect", "TracerPath",
-           "load", "make_device"]
+           "GeometryConvexPolyhedron", "GeometryMesh", "GeometryPolygon", "Tracer", "TracerDirect",
+           "TracerPath", "load", "make_device"]

@@ -41,6 +41,9 @@ typedef struct or_geometry_desc {
     fr_material material;
     fr_material outline_material;
     float outline_width;
+    /* polygon: position is [n][2], vertices [n_vertices][2], colour [n][3] */
+    const float* angle; /* polygon [n] radians */
+    float rounding_radius;
 } or_geometry_desc;
 
 typedef struct or_stats {

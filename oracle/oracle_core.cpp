@@ -1,7 +1,7 @@
 // oracle_core.cpp -- TEST INFRASTRUCTURE (CPU oracle), not part of the product.
 //
 // A CPU restatement of fresnel's Embree backend: per-geometry closest-hit glue restated from
-// fresnel/cpu/Geometry{Sphere,Cylinder,ConvexPolyhedron,Mesh}.cc, the tile loops of
+// fresnel/cpu/Geometry{Sphere,Cylinder,ConvexPolyhedron,Mesh,Polygon}.cc, the tile loops of
 // fresnel/cpu/TracerPath.cc and fresnel/cpu/TracerDirect.cc, and a binned-SAH BVH2 standing in
 // for Embree's scene BVH (closest-hit results do not depend on the BVH except for exact ties
 // in t).  The shading/intersection arithmetic comes from namespace M, which is either the
@@ -57,6 +57,10 @@ struct Geom {
     std::vector<F3> plane_origin, plane_normal;
     std::vector<RGB3> plane_color;
     float poly_radius = 0, color_by_face = 0;
+    // polygon: 2-D positions, rotation quaternions (from the angles), 2-D outline vertices
+    std::vector<float> pos2, verts2;
+    std::vector<Quat> pq;
+    float rounding_radius = 0, pg_radius = 0;
     Mat material{}, outline{};
     float outline_width = 0;
     uint32_t prim_count() const { return type == FR_GEOM_MESH ? n * n_faces : n; }
@@ -170,6 +174,12 @@ Box prim_box(const Geom& g, uint32_t prim)
             F3 v = M::rotate(q, g.vertices[3 * face + k]) + p;
             box_grow(b, v.x, v.y, v.z);
         }
+        break;
+    }
+    case FR_GEOM_POLYGON: {  // fresnel/cpu/GeometryPolygon.cc:89-104
+        const float x = g.pos2[2 * prim], y = g.pos2[2 * prim + 1], r = g.pg_radius;
+        box_grow(b, x - r, y - r, float(0.0 - 1e-5));
+        box_grow(b, x + r, y + r, float(0.0 + 1e-5));
         break;
     }
     }
@@ -492,6 +502,59 @@ inline void glue_mesh(const Geom& g, uint32_t gi, uint32_t item, F3 o, F3 dir, f
     }
 }
 
+// fresnel/cpu/GeometryPolygon.cc:146-230: the ray in the polygon's frame meets the z = 0 plane;
+// the hit point's distance to the outline (is_inside, :113-140, with the point-segment distance
+// of fresnel/common/GeometryMath.h:28-39), signed negative inside, must not exceed the rounding
+// radius.  Double sided: the normal faces the ray.
+inline void glue_polygon(const Geom& g, uint32_t gi, uint32_t prim, F3 o, F3 dir, float tnear,
+                         Hit& h)
+{
+    using frm::dot;
+    const F3 pos_world{g.pos2[2 * prim], g.pos2[2 * prim + 1], 0.0f};
+    const Quat q = g.pq[prim];
+    const F3 dl = M::rotate(M::conj(q), dir);
+    const F3 ol = M::rotate(M::conj(q), o - pos_world);
+    const F3 n{0, 0, 1};
+    const F3 p{0, 0, 0};
+    const float d = -dot(n, p);
+    const float denom = dot(n, dl);
+    const float t_hit = -(d + dot(n, ol)) / denom;
+    if (double(std::fabs(denom)) < 1e-5)
+        return;
+    const F3 r_hit = ol + t_hit * dl;
+    // is_inside: crossing number (odd = inside) and the distance to the nearest edge
+    const uint32_t nvert = uint32_t(g.verts2.size() / 2);
+    float min_d = FLT_MAX;
+    bool odd = false;
+    uint32_t j = nvert - 1;
+    for (uint32_t i = 0; i < nvert; ++i) {
+        const float xi = g.verts2[2 * i], yi = g.verts2[2 * i + 1];
+        const float xj = g.verts2[2 * j], yj = g.verts2[2 * j + 1];
+        const float dist = M::point_segment_distance(r_hit.x, r_hit.y, xi, yi, xj, yj);
+        min_d = (dist < min_d) ? dist : min_d;  // std::min(min_d, dist)
+        if ((yi < r_hit.y && yj >= r_hit.y) || (yj < r_hit.y && yi >= r_hit.y)) {
+            if (xi + (r_hit.y - yi) / (yj - yi) * (xj - xi) < r_hit.x)
+                odd = !odd;
+        }
+        j = i;
+    }
+    float d_edge = min_d;
+    if (odd)
+        d_edge = -d_edge;
+    if (d_edge > g.rounding_radius)
+        return;
+    const float shade_d = g.rounding_radius - d_edge;
+    if ((tnear < t_hit) & (t_hit < h.t)) {
+        h.t = t_hit;
+        h.geom = gi;
+        h.prim = prim;
+        const F3 n_flip = (dot(n, dl) < 0.0f) ? n : -n;
+        h.Ng = M::rotate(q, n_flip);
+        h.color = g.color[prim];
+        h.d = shade_d;
+    }
+}
+
 struct Counters {
     uint64_t rays = 0, box = 0, prim = 0, paths = 0, nonfinite = 0;
 };
@@ -556,6 +619,9 @@ Hit trace(const or_scene& s, F3 o, F3 d, float tnear, Counters& c)
                     break;
                 case FR_GEOM_MESH:
                     glue_mesh(g, r.geom, r.prim, o, d, tnear, h);
+                    break;
+                case FR_GEOM_POLYGON:
+                    glue_polygon(g, r.geom, r.prim, o, d, tnear, h);
                     break;
                 }
             }
@@ -743,6 +809,22 @@ or_scene* or_scene_create(const or_geometry_desc* gd, uint32_t n_geoms, int leaf
             g.vertices = f3(d.vertices, d.n_vertices);
             g.color = c3(d.color, d.n_vertices);
             break;
+        case FR_GEOM_POLYGON: {  // fresnel/cpu/GeometryPolygon.cc:20-82
+            g.pos2.assign(d.position, d.position + 2 * size_t(d.n));
+            g.color = c3(d.color, d.n);
+            g.verts2.assign(d.vertices, d.vertices + 2 * size_t(d.n_vertices));
+            g.rounding_radius = d.rounding_radius;
+            float r = 0;
+            for (uint32_t i = 0; i < d.n_vertices; ++i) {
+                const float x = d.vertices[2 * i], y = d.vertices[2 * i + 1];
+                r = std::max(r, sqrtf(x * x + y * y));
+            }
+            g.pg_radius = r + d.rounding_radius;
+            g.pq.resize(d.n);
+            for (uint32_t i = 0; i < d.n; ++i)
+                g.pq[i] = M::from_axis_angle(F3{0, 0, 1}, d.angle[i]);
+            break;
+        }
         default:
             delete s;
             return nullptr;
@@ -1038,6 +1120,9 @@ int or_prim_hit(const or_scene* s, uint32_t geom, uint32_t prim, const float o[3
         break;
     case FR_GEOM_POLYHEDRON:
         glue_polyhedron(g, geom, prim, oo, dd, tnear, h);
+        break;
+    case FR_GEOM_POLYGON:
+        glue_polygon(g, geom, prim, oo, dd, tnear, h);
         break;
     default:
         glue_mesh(g, geom, prim, oo, dd, tnear, h);

@@ -13,6 +13,7 @@
 
 #include "common/Camera.h"
 #include "common/ColorMath.h"
+#include "common/GeometryMath.h"
 #include "common/IntersectCylinder.h"
 #include "common/IntersectSphere.h"
 #include "common/IntersectTriangle.h"
@@ -210,6 +211,13 @@ inline F3 rotate(Quat a, F3 b) { return V(fresnel::rotate(Q(a), V(b))); }
 inline Quat from_axis_angle(F3 axis, float theta)
 {
     return Q(fresnel::quat<float>::fromAxisAngle(V(axis), theta));
+}
+
+inline float point_segment_distance(float px, float py, float ax, float ay, float bx, float by)
+{
+    return fresnel::point_line_segment_distance(fresnel::vec2<float>(px, py),
+                                                fresnel::vec2<float>(ax, ay),
+                                                fresnel::vec2<float>(bx, by));
 }
 
 inline bool isect_sphere(float& t, float& d_edge, F3& N, F3 o, F3 d, F3 p, float r)

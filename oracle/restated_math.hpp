@@ -81,6 +81,19 @@ inline Quat from_axis_angle(F3 axis, float theta)
     return Quat{cosf(theta / 2.0f), sinf(theta / 2.0f) * axis};
 }
 
+// Distance from p to the segment ab in 2-D (fresnel/common/GeometryMath.h:28-39): clamp the
+// projection parameter with std::min/std::max semantics, then the length of p - projection.
+inline float point_segment_distance(float px, float py, float ax, float ay, float bx, float by)
+{
+    const float abx = bx - ax, aby = by - ay;
+    const float L = abx * abx + aby * aby;
+    const float q = ((px - ax) * abx + (py - ay) * aby) / L;
+    const float lo = (q < 1.0f) ? q : 1.0f;  // std::min(1.0f, q)
+    const float t = (0.0f < lo) ? lo : 0.0f;  // std::max(0.0f, lo)
+    const float vx = px - (ax + t * abx), vy = py - (ay + t * aby);
+    return sqrtf(vx * vx + vy * vy);
+}
+
 // ---------------------------------------------------------------------------------------------
 // Philox4x32-10 and u01 (Random123 semantics used at fresnel/common/RayGen.h:49-61,
 // fresnel/common/Camera.h:190-201,230-242)

@@ -30,6 +30,10 @@ CASES = {
                         {"samples": 8, "light_samples": 2, "seed": 5}),
     "dense_path": (lambda d: workloads.config2(d, n=5000, box=140.0 * (0.005)**(1 / 3)), "path",
                    64, 36, {"samples": 8, "light_samples": 1, "seed": 1}),
+    "polygons_preview": (lambda d: workloads.polygons(d, spheres=30), "preview", 96, 72,
+                         {"aa_n": 2}),
+    "polygons_path": (lambda d: workloads.polygons(d, nx=10, ny=8, spheres=20), "path", 64, 48,
+                      {"samples": 6, "light_samples": 1, "seed": 3}),
 }
 
 

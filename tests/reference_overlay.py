@@ -18,8 +18,8 @@ REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 REFERENCE = os.environ.get("FRESNEL_REFERENCE", "/root/reference")
 PKG = os.path.join(REFERENCE, "fresnel")
 
-# Geometry that the product does not implement (out of scope of the hot path).
-EXCLUDED_TESTS = ["test_geometry_polygon.py"]
+# Reference test files left out of the overlay run (none: every geometry is implemented).
+EXCLUDED_TESTS = []
 
 _COMMON_SHIM = """from fresnel_b200._common import *  # noqa: F401,F403
 from fresnel_b200._common import find_polyhedron_faces  # noqa: F401

@@ -143,8 +143,9 @@ def test_geometry_argument_errors(gpu_device):
                                                   'face_normal': numpy.zeros((2, 3)),
                                                   'face_color': numpy.zeros((3, 3)),
                                                   'radius': 1.0}, N=1)
-    with pytest.raises(RuntimeError):
-        fresnel.geometry.Polygon(scene, vertices=[[0, 0], [1, 0], [0, 1]])
+    with pytest.raises(RuntimeError, match="Nvert by 2"):
+        fresnel.geometry.Polygon(scene, vertices=[[0, 0, 0], [1, 0, 0], [0, 1, 0]],
+                                 position=[[0, 0]])
 
 
 def test_light_proxy_and_camera(gpu_device):

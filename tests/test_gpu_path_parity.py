@@ -24,6 +24,7 @@ SAME_SEED = {
     "dense_spheres": (lambda d: workloads.config2(d, n=20000,
                                                   box=140.0 * (0.02)**(1 / 3)), 96, 54, 6, 1),
     "mixed": (lambda d: workloads.config3(d, scale=0.002), 96, 54, 4, 1),
+    "polygons_spheres": (lambda d: workloads.polygons(d, spheres=60), 96, 72, 6, 2),
 }
 
 

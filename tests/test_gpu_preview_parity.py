@@ -34,6 +34,10 @@ SCENES = {
     "dense_spheres": (_dense, 192, 108),
     "mixed": (lambda d: workloads.config3(d, scale=0.002), 160, 90),
     "mixed_large": (lambda d: workloads.config3(d, scale=0.02), 128, 72),
+    "polygons": (workloads.polygons, 160, 120),
+    "polygons_spheres": (lambda d: workloads.polygons(d, spheres=60), 160, 120),
+    "polygons_ortho": (lambda d: workloads.polygons(d, perspective=False, rounding_radius=0.0),
+                       150, 112),
 }
 
 

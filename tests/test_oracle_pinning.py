@@ -2,7 +2,8 @@
 
 1. The oracle core compiled against the reference's own fresnel/common/*.h headers
    (oracle/_ref) and against the restatement (oracle/_build) gives bit-identical images on
-   every geometry type, both tracers, orthographic and perspective (depth of field) cameras.
+   every geometry type (polygons included), both tracers, orthographic and perspective (depth
+   of field) cameras.
 2. The reference's own pytest suite, run unmodified on the oracle, passes its golden-image
    comparisons (fresnel/test/reference/*.png).
 3. The oracle reproduces the committed golden fixtures bit for bit.
@@ -49,6 +50,7 @@ SCENES = {
     "mixed": lambda d: workloads.config3(d, scale=0.002),
     "dof": _dof,
     "materials": _materials,
+    "polygons": lambda d: workloads.polygons(d, nx=8, ny=6, spheres=10),
 }
 
 
@@ -125,7 +127,8 @@ def test_reference_suite_on_oracle():
 
 
 @pytest.mark.parametrize("name", ["hex_preview", "hex_preview_aa", "mixed_preview",
-                                  "spheres_1k_path", "dense_path"])
+                                  "spheres_1k_path", "dense_path", "polygons_preview",
+                                  "polygons_path"])
 def test_oracle_reproduces_golden_fixtures(name):
     import golden.make_golden as mg
     dev = cpu_module.make_device("restated")
