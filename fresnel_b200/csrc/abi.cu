@@ -651,6 +651,7 @@ FrameParams frame_params(fr_tracer* tr, fr_scene* sc, const fr_render_params* p,
     P.type_mask = 0;
     P.bvh_width = 2;
     P.persistent = sc->dev->persistent;
+    P.refill_geom = -1;  // no tree the refill kernel can walk (set below when there is one)
     if (sc->use_combined && sc->combined.n_nodes4 > 0) {
         for (fr_geometry* g : sc->geoms)
             if (g->enabled && !g->removed && g->bvh_prims() > 0)
@@ -692,7 +693,6 @@ FrameParams frame_params(fr_tracer* tr, fr_scene* sc, const fr_render_params* p,
     P.shade_blocks = sc->dev->shade_blocks;
     P.packet = sc->dev->packet;
     P.refill = sc->dev->refill;
-    P.refill_geom = -1;
     const fr_user_camera& c = p->camera;
     float f_stop = preview ? std::numeric_limits<float>::infinity() : c.f_stop;  // no depth of field in preview
     bool sample_aa = preview ? (aa_n != 1) : true;
