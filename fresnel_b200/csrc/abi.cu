@@ -18,6 +18,7 @@
 #include "batch.hpp"
 #include "bvh.hpp"
 #include "fresnel_b200.h"
+#include "grid.hpp"
 #include "render.hpp"
 
 using namespace fr;
@@ -161,6 +162,8 @@ struct fr_device {
     int combined = 1;                      // one tree per scene of several geometries
     int packet = 0;                        // warp-cooperative primary traversal
     int refill = 0;                        // extension rays with per-lane refill
+    int accel = 2;                         // sphere grid: 0 never, 1 whenever possible, 2 auto
+    float grid_cells_per_prim = 1.5f;      // grid cells per sphere
     std::vector<fr_scene*> scenes;         // to mark BVHs stale when a build option changes
     void* static_path = nullptr;           // this device's copy of g_static_path (looked up once)
     PathBuffers path;                      // wavefront state shared by the device's tracers
@@ -243,6 +246,12 @@ struct fr_scene {
     bool use_combined = false;
     std::vector<uint64_t> combined_key;  // (geometry, primitives, generation) per part
     BuildParams combined_bp{};
+    // uniform grid over the scene's one sphere geometry (instead of its BVH)
+    GridBuffers grid;
+    bool use_grid = false;
+    std::vector<uint64_t> grid_key;  // (geometry, primitives, generation, mode, density) last tried
+    uint32_t grid_geom = 0;          // scene index of that geometry
+    GridReport grid_report;
 };
 
 struct fr_tracer {
@@ -256,6 +265,8 @@ struct fr_tracer {
     uint64_t launches = 0;
     uint64_t builds = 0;
     uint64_t refits = 0;
+    uint64_t grid_builds = 0;
+    uint32_t last_grid = 0;  // whether the last render traced through a sphere grid
     double build_ms = 0.0;
     // per-kernel timing while profiling: event pairs pending readback, by kernel kind
     std::vector<cudaEvent_t> event_pool;
@@ -445,10 +456,45 @@ std::vector<fr_geometry*> combined_parts(const fr_scene* sc, std::vector<uint64_
     return parts;
 }
 
+// The sphere geometry a grid may replace the BVH of: the scene's only enabled geometry, when
+// it holds spheres and the device allows grids (nullptr otherwise).  key identifies what a grid
+// build depends on; gi receives the geometry's scene index.
+fr_geometry* grid_candidate(const fr_scene* sc, std::vector<uint64_t>& key, uint32_t& gi)
+{
+    key.clear();
+    const fr_device* dev = sc->dev;
+    if (dev->accel == 0)
+        return nullptr;
+    fr_geometry* found = nullptr;
+    for (uint32_t i = 0; i < sc->geoms.size(); ++i) {
+        fr_geometry* g = sc->geoms[i];
+        if (g->removed || !g->enabled || g->bvh_prims() == 0)
+            continue;
+        if (found || g->type != FR_GEOM_SPHERE)
+            return nullptr;
+        found = g;
+        gi = i;
+    }
+    if (!found)
+        return nullptr;
+    uint32_t density_bits;
+    std::memcpy(&density_bits, &dev->grid_cells_per_prim, sizeof(density_bits));
+    key = {reinterpret_cast<uintptr_t>(found), found->n, found->gen, uint64_t(dev->accel),
+           density_bits};
+    return found;
+}
+
 // Whether prepare_scene would build anything.
 bool scene_needs_build(const fr_scene* sc)
 {
     std::vector<uint64_t> key;
+    uint32_t gi = 0;
+    if (grid_candidate(sc, key, gi)) {
+        if (key != sc->grid_key)
+            return true;
+        if (sc->use_grid)
+            return false;
+    }
     if (!combined_parts(sc, key).empty())
         return !sc->use_combined || key != sc->combined_key;
     for (fr_geometry* g : sc->geoms)
@@ -533,12 +579,62 @@ fr_status build_combined(fr_scene* sc, fr_tracer* tr, const std::vector<fr_geome
     return FR_OK;
 }
 
-// Build stale BVHs and refresh the device geometry table.
+// Build (or decline) the grid of the scene's sphere geometry g when its inputs changed.
+fr_status prepare_grid(fr_scene* sc, fr_tracer* tr, fr_geometry* g, uint32_t gi,
+                       const std::vector<uint64_t>& key)
+{
+    fr_device* dev = sc->dev;
+    GridParams gp;
+    gp.mode = dev->accel;
+    gp.cells_per_prim = dev->grid_cells_per_prim;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, dev->stream);
+    cudaError_t e = build_grid(g->position.ptr, g->radius.ptr, g->n, gp, sc->grid, dev->scratch,
+                               dev->stream, sc->grid_report);
+    cudaEventRecord(e1, dev->stream);
+    cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) {
+        sc->use_grid = false;
+        sc->grid_key.clear();
+        return cuda_fail(e, "building a sphere grid");
+    }
+    sc->grid_key = key;
+    sc->grid_geom = gi;
+    sc->use_grid = sc->grid_report.built;
+    if (!sc->use_grid) {  // the BVH serves this scene: free the grid's arrays
+        sc->grid.cell_start.release();
+        sc->grid.ref_sphere.release();
+        sc->grid.ref_prim.release();
+    } else if (tr) {
+        tr->grid_builds++;
+        tr->build_ms = ms;
+    }
+    return FR_OK;
+}
+
+// Build the stale acceleration structures (grid or BVHs) and refresh the device geometry table.
 fr_status prepare_scene(fr_scene* sc, fr_tracer* tr)
 {
     fr_device* dev = sc->dev;
     std::vector<uint64_t> key;
-    const std::vector<fr_geometry*> parts = combined_parts(sc, key);
+    uint32_t gi = 0;
+    fr_geometry* gg = grid_candidate(sc, key, gi);
+    if (!gg) {
+        sc->use_grid = false;
+        sc->grid_key.clear();
+    } else if (key != sc->grid_key) {
+        fr_status s = prepare_grid(sc, tr, gg, gi, key);
+        if (s != FR_OK)
+            return s;
+    }
+    const std::vector<fr_geometry*> parts =
+        sc->use_grid ? std::vector<fr_geometry*>() : combined_parts(sc, key);
     if (!parts.empty()) {
         if (!sc->use_combined || key != sc->combined_key) {
             fr_status s = build_combined(sc, tr, parts, key);
@@ -549,7 +645,7 @@ fr_status prepare_scene(fr_scene* sc, fr_tracer* tr)
         sc->use_combined = false;
     }
     for (fr_geometry* g : sc->geoms) {
-        if (sc->use_combined || g->removed || !g->bvh_dirty)
+        if (sc->use_grid || sc->use_combined || g->removed || !g->bvh_dirty)
             continue;
         BuildInput in = build_input(g);
         cudaEvent_t e0, e1;
@@ -652,7 +748,33 @@ FrameParams frame_params(fr_tracer* tr, fr_scene* sc, const fr_render_params* p,
     P.bvh_width = 2;
     P.persistent = sc->dev->persistent;
     P.refill_geom = -1;  // no tree the refill kernel can walk (set below when there is one)
-    if (sc->use_combined && sc->combined.n_nodes4 > 0) {
+    if (sc->use_grid) {
+        const GridBuffers& G = sc->grid;
+        GridDev& d = P.scene.grid;
+        d.n_cells = G.n_cells;
+        d.nx = G.dims[0];
+        d.ny = G.dims[1];
+        d.nz = G.dims[2];
+        d.lox = G.lo[0];
+        d.loy = G.lo[1];
+        d.loz = G.lo[2];
+        d.hix = G.hi[0];
+        d.hiy = G.hi[1];
+        d.hiz = G.hi[2];
+        d.hx = G.cell[0];
+        d.hy = G.cell[1];
+        d.hz = G.cell[2];
+        d.ihx = 1.0f / G.cell[0];
+        d.ihy = 1.0f / G.cell[1];
+        d.ihz = 1.0f / G.cell[2];
+        d.geom = sc->grid_geom;
+        d.cell_start = G.cell_start.ptr;
+        d.ref_sphere = G.ref_sphere.ptr;
+        d.ref_prim = G.ref_prim.ptr;
+        P.type_mask = 1u << FR_GEOM_SPHERE;
+        P.bvh_width = 4;
+        P.persistent = 0;  // the persistent and packet kernels walk trees
+    } else if (sc->use_combined && sc->combined.n_nodes4 > 0) {
         for (fr_geometry* g : sc->geoms)
             if (g->enabled && !g->removed && g->bvh_prims() > 0)
                 P.type_mask |= 1u << g->type;
@@ -691,8 +813,9 @@ FrameParams frame_params(fr_tracer* tr, fr_scene* sc, const fr_render_params* p,
     }
     P.tile_log2 = sc->dev->tile_log2;
     P.shade_blocks = sc->dev->shade_blocks;
-    P.packet = sc->dev->packet;
-    P.refill = sc->dev->refill;
+    P.packet = sc->use_grid ? 0 : sc->dev->packet;
+    P.refill = sc->use_grid ? 0 : sc->dev->refill;
+    tr->last_grid = sc->use_grid ? 1u : 0u;
     const fr_user_camera& c = p->camera;
     float f_stop = preview ? std::numeric_limits<float>::infinity() : c.f_stop;  // no depth of field in preview
     bool sample_aa = preview ? (aa_n != 1) : true;
@@ -997,6 +1120,14 @@ fr_status fr_device_set_option(fr_device* d, const char* name, double value)
         if (value != 0.0 && value != 1.0)
             return fail(FR_ERR_INVALID, "persistent must be 0 or 1");
         d->persistent = int(value);
+    } else if (n == "accel") {
+        if (!(value == 0.0 || value == 1.0 || value == 2.0))
+            return fail(FR_ERR_INVALID, "accel must be 0 (BVH), 1 (sphere grid) or 2 (automatic)");
+        d->accel = int(value);
+    } else if (n == "grid_density") {
+        if (!(value > 0.0 && value <= 64.0))
+            return fail(FR_ERR_INVALID, "grid_density must be in (0, 64]");
+        d->grid_cells_per_prim = float(value);
     } else if (n == "path_slots") {
         if (!(value >= 1.0 && value <= 1e9))
             return fail(FR_ERR_INVALID, "path_slots must be in [1, 1e9]");
@@ -1025,6 +1156,10 @@ fr_status fr_device_get_option(const fr_device* d, const char* name, double* val
         *value = d->build.c_trav;
     else if (n == "path_slots")
         *value = double(d->path_slots);
+    else if (n == "accel")
+        *value = d->accel;
+    else if (n == "grid_density")
+        *value = d->grid_cells_per_prim;
     else if (n == "builder")
         *value = d->build.builder;
     else if (n == "tile")
@@ -1173,6 +1308,18 @@ fr_status fr_geometry_create_mesh(fr_scene* scene, const float* vertices, uint32
         return cuda_fail(e, "uploading mesh vertices");
     }
     return finish_geometry(g, out);
+}
+
+fr_status fr_scene_get_accel(const fr_scene* sc, int* grid, char* reason, size_t cap)
+{
+    FR_CHECK_NULL(sc);
+    FR_CHECK_NULL(grid);
+    *grid = sc->use_grid ? 1 : 0;
+    if (reason && cap) {
+        const char* r = (!sc->use_grid && !sc->grid_key.empty()) ? sc->grid_report.reason : "";
+        std::snprintf(reason, cap, "%s", r);
+    }
+    return FR_OK;
 }
 
 fr_status fr_geometry_create_polygon(fr_scene* scene, const float* vertices, uint32_t n_vertices,
@@ -1800,6 +1947,8 @@ fr_status fr_tracer_get_stats(const fr_tracer* t, fr_stats* out)
     out->primary_launches = t->kernel_launches[0];
     out->shade_launches = t->kernel_launches[1];
     out->extend_launches = t->kernel_launches[2];
+    out->grid_builds = t->grid_builds;
+    out->last_render_grid = t->last_grid;
     return FR_OK;
 }
 

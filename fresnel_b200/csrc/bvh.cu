@@ -62,9 +62,14 @@ __device__ __forceinline__ Box empty_box()
     return Box{make_float3(inf, inf, inf), make_float3(-inf, -inf, -inf)};
 }
 
-// Bounds of one primitive (fresnel/cpu/GeometrySphere.cc:60-73, GeometryCylinder.cc:55-70,
-// GeometryConvexPolyhedron.cc:119-132, GeometryMesh.cc:81-113).  Non-finite bounds (e.g. an
-// infinite radius) give an empty box, which no ray enters.
+__device__ __forceinline__ float std_min(float a, float b) { return (b < a) ? b : a; }
+__device__ __forceinline__ float std_max(float a, float b) { return (a < b) ? b : a; }
+
+// Bounds of one primitive, with the reference's formulas (fresnel/cpu/GeometrySphere.cc:60-73,
+// GeometryCylinder.cc:55-70, GeometryConvexPolyhedron.cc:119-132, GeometryMesh.cc:81-113,
+// GeometryPolygon.cc:89-104).  A box that is not finite or has lower > upper (e.g. a negative or
+// infinite radius) is empty, so no ray enters it: Embree leaves such primitives out of its
+// tree.
 __device__ Box prim_bounds(const BuildInput& in, uint32_t i)
 {
     Box b = empty_box();
@@ -72,24 +77,24 @@ __device__ Box prim_bounds(const BuildInput& in, uint32_t i)
     case FR_GEOM_SPHERE: {
         V3 p = load3(in.position, i);
         float r = in.radius[i];
-        grow(b, v3(p.x - r, p.y - r, p.z - r));
-        grow(b, v3(p.x + r, p.y + r, p.z + r));
+        b.lo = make_float3(p.x - r, p.y - r, p.z - r);
+        b.hi = make_float3(p.x + r, p.y + r, p.z + r);
         break;
     }
     case FR_GEOM_CYLINDER: {
         V3 A = load3(in.points, 2 * i), B = load3(in.points, 2 * i + 1);
         float r = in.radius[i];
-        grow(b, v3(A.x - r, A.y - r, A.z - r));
-        grow(b, v3(A.x + r, A.y + r, A.z + r));
-        grow(b, v3(B.x - r, B.y - r, B.z - r));
-        grow(b, v3(B.x + r, B.y + r, B.z + r));
+        b.lo = make_float3(std_min(A.x - r, B.x - r), std_min(A.y - r, B.y - r),
+                           std_min(A.z - r, B.z - r));
+        b.hi = make_float3(std_max(A.x + r, B.x + r), std_max(A.y + r, B.y + r),
+                           std_max(A.z + r, B.z + r));
         break;
     }
     case FR_GEOM_POLYHEDRON: {
         V3 p = load3(in.position, i);
         float r = in.poly_radius;
-        grow(b, v3(p.x - r, p.y - r, p.z - r));
-        grow(b, v3(p.x + r, p.y + r, p.z + r));
+        b.lo = make_float3(p.x - r, p.y - r, p.z - r);
+        b.hi = make_float3(p.x + r, p.y + r, p.z + r);
         break;
     }
     case FR_GEOM_MESH: {
@@ -100,11 +105,11 @@ __device__ Box prim_bounds(const BuildInput& in, uint32_t i)
             grow(b, rotate(q, load3(in.vertices, 3 * face + k)) + p);
         break;
     }
-    default: {  // polygon in the z = 0 plane (fresnel/cpu/GeometryPolygon.cc:89-104)
+    default: {  // polygon in the z = 0 plane
         const float x = in.position[2 * size_t(i)], y = in.position[2 * size_t(i) + 1];
         const float r = in.poly_radius;
-        grow(b, v3(x - r, y - r, 0.0f - 1e-5f));
-        grow(b, v3(x + r, y + r, 0.0f + 1e-5f));
+        b.lo = make_float3(x - r, y - r, 0.0f - 1e-5f);
+        b.hi = make_float3(x + r, y + r, 0.0f + 1e-5f);
         break;
     }
     }

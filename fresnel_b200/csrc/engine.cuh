@@ -64,10 +64,28 @@ struct GeomDev {
     Mat outline;
 };
 
+// Uniform grid over the spheres of one geometry (n_cells == 0: the scene has none).  Cell
+// (ix, iy, iz) spans lo + (i, i + 1) * h per axis and is numbered (iz * ny + iy) * nx + ix; its
+// sphere references are [cell_start[c], cell_start[c + 1]), each a copy of the sphere (x, y, z, r)
+// and its index.  A sphere is referenced by every cell its padded bounding box touches.
+struct GridDev {
+    uint32_t n_cells;
+    uint32_t nx, ny, nz;
+    float lox, loy, loz;
+    float hix, hiy, hiz;  // far corner (lo + n * h)
+    float hx, hy, hz;     // cell size
+    float ihx, ihy, ihz;  // 1 / cell size
+    uint32_t geom;        // scene index of the sphere geometry
+    const uint32_t* cell_start;
+    const float4* ref_sphere;
+    const uint32_t* ref_prim;
+};
+
 struct SceneDev {
     const GeomDev* geoms;
     uint32_t n_geoms;
     uint32_t* status;  // error bits (device)
+    GridDev grid;      // sphere scenes traced through a uniform grid instead of a BVH
     // Combined 4-wide tree over the primitives of several geometries (n_nodes4 == 0: none, each
     // enabled geometry's own tree is traversed in turn): leaf slot s holds 2 float4 of its
     // primitive's record, its geometry (leaf_geom) and its index within the geometry (order).
@@ -790,6 +808,78 @@ struct Hit {
     uint32_t prim;  // index into the geometry's user arrays
 };
 
+// Closest sphere hit through a uniform grid: a 3-D DDA walk over the cells the ray crosses
+// (Amanatides & Woo, "A fast voxel traversal algorithm for ray tracing", Eurographics 1987),
+// testing every sphere a cell references with the same sphere test and acceptance rule as the
+// BVH leaves.  The walk stops once the closest hit so far lies before the exit from the current
+// cell: a sphere the ray meets earlier touches a cell already walked (boxes are padded well
+// beyond the rounding of the cell boundaries), so it has been tested.  Cell exits are
+// recomputed from the plane positions at every step, so rounding does not accumulate.
+// slot receives the reference index of the hit (unchanged on a miss).
+__device__ __forceinline__ void trace_grid(const GridDev& G, const RayK& ray, float tnear,
+                                           float& tmax, uint32_t& slot, TraceCount& tc)
+{
+    float tx0 = fmaf(G.lox, ray.inv.x, ray.oinv.x), tx1 = fmaf(G.hix, ray.inv.x, ray.oinv.x);
+    float ty0 = fmaf(G.loy, ray.inv.y, ray.oinv.y), ty1 = fmaf(G.hiy, ray.inv.y, ray.oinv.y);
+    float tz0 = fmaf(G.loz, ray.inv.z, ray.oinv.z), tz1 = fmaf(G.hiz, ray.inv.z, ray.oinv.z);
+    const float t_in = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), 0.0f));
+    const float t_out = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fmaxf(tz0, tz1));
+    if (!(t_in <= t_out))
+        return;  // misses the grid (or NaN)
+    // the cell holding the entry point (clamped: the entry lies on the grid's surface)
+    auto cell_of = [](float p, float lo, float ih, uint32_t n) {
+        const float u = (p - lo) * ih;
+        return u >= 0.0f ? int(fminf(u, float(n - 1u))) : 0;  // NaN compares false: cell 0
+    };
+    int ix = cell_of(ray.o.x + t_in * ray.d.x, G.lox, G.ihx, G.nx);
+    int iy = cell_of(ray.o.y + t_in * ray.d.y, G.loy, G.ihy, G.ny);
+    int iz = cell_of(ray.o.z + t_in * ray.d.z, G.loz, G.ihz, G.nz);
+    const int sx = ray.inv.x >= 0.0f ? 1 : -1;
+    const int sy = ray.inv.y >= 0.0f ? 1 : -1;
+    const int sz = ray.inv.z >= 0.0f ? 1 : -1;
+    // distance to the plane the ray leaves cell i through, along one axis
+    auto exit_t = [](int i, int s, float lo, float h, float inv, float oinv) {
+        return fmaf(fmaf(float(i + (s > 0 ? 1 : 0)), h, lo), inv, oinv);
+    };
+    float tnx = exit_t(ix, sx, G.lox, G.hx, ray.inv.x, ray.oinv.x);
+    float tny = exit_t(iy, sy, G.loy, G.hy, ray.inv.y, ray.oinv.y);
+    float tnz = exit_t(iz, sz, G.loz, G.hz, ray.inv.z, ray.oinv.z);
+    uint32_t guard = G.nx + G.ny + G.nz + 3u;
+    while (true) {
+        const uint32_t c = (uint32_t(iz) * G.ny + uint32_t(iy)) * G.nx + uint32_t(ix);
+        const uint32_t first = __ldg(G.cell_start + c), last = __ldg(G.cell_start + c + 1);
+        tc.box += 1;
+        tc.prim += last - first;
+        for (uint32_t k = first; k < last; ++k) {
+            const float4 q = ldg4(G.ref_sphere + k);
+            float t;
+            if (sphere_t(ray.o, ray.d, v3(q.x, q.y, q.z), q.w, t) && (tnear < t) && (t < tmax)) {
+                tmax = t;
+                slot = k;
+            }
+        }
+        const float t_cell = fminf(tnx, fminf(tny, tnz));
+        if (tmax <= t_cell || t_cell >= t_out || --guard == 0u)
+            return;
+        if (tnx <= tny && tnx <= tnz) {
+            ix += sx;
+            if (ix < 0 || ix >= int(G.nx))
+                return;
+            tnx = exit_t(ix, sx, G.lox, G.hx, ray.inv.x, ray.oinv.x);
+        } else if (tny <= tnz) {
+            iy += sy;
+            if (iy < 0 || iy >= int(G.ny))
+                return;
+            tny = exit_t(iy, sy, G.loy, G.hy, ray.inv.y, ray.oinv.y);
+        } else {
+            iz += sz;
+            if (iz < 0 || iz >= int(G.nz))
+                return;
+            tnz = exit_t(iz, sz, G.loz, G.hz, ray.inv.z, ray.oinv.z);
+        }
+    }
+}
+
 // Geometry-type masks a kernel is specialised for (bit FR_GEOM_* set = type handled).
 constexpr uint32_t MASK_SPHERES = 1u << FR_GEOM_SPHERE;
 constexpr uint32_t MASK_ALL = 0x1Fu;  // every FR_GEOM_* type
@@ -804,6 +894,14 @@ __device__ __forceinline__ Hit trace_closest(const SceneDev& sc, V3 o, V3 d, flo
     RayK ray = make_rayk(o, d);
     float tmax = __int_as_float(0x7f800000);  // +inf
     uint32_t hg = MISS, hs = 0;
+    if (MASK == MASK_SPHERES && sc.grid.n_cells != 0) {
+        uint32_t slot = MISS;
+        trace_grid(sc.grid, ray, tnear, tmax, slot, tc);
+        Hit h;
+        h.geom = slot == MISS ? MISS : sc.grid.geom;
+        h.prim = slot == MISS ? 0u : __ldg(sc.grid.ref_prim + slot);
+        return h;
+    }
     if (WIDTH == 4 && sc.n_nodes4 != 0) {
         traverse4_core(sc.nodes4, sc.n_nodes4, sc.n_prims, ray, tmax, sc.status, tc,
                        [&](uint32_t first, uint32_t count) {

@@ -1,0 +1,53 @@
+// grid.hpp -- uniform grid over the spheres of one geometry, the acceleration structure the
+// renderers use instead of a BVH for large, evenly spread sphere sets (device option "accel").
+#ifndef FR_GRID_HPP
+#define FR_GRID_HPP
+
+#include "bvh.hpp"
+
+namespace fr {
+
+struct GridBuffers {
+    DevArray<uint32_t> cell_start;   // n_cells + 1 offsets into the references
+    DevArray<float4> ref_sphere;     // per reference: the sphere (x, y, z, r)
+    DevArray<uint32_t> ref_prim;     // per reference: the sphere's index in its geometry
+    DevArray<uint32_t> prim_count;   // build temporaries kept between builds: cells per sphere
+    DevArray<uint32_t> prim_offset;  // and their exclusive prefix sum
+    uint32_t n_cells = 0;            // 0: no grid
+    uint32_t n_refs = 0;
+    uint32_t dims[3] = {0, 0, 0};
+    float lo[3] = {0, 0, 0};
+    float hi[3] = {0, 0, 0};
+    float cell[3] = {0, 0, 0};
+};
+
+struct GridParams {
+    float cells_per_prim = 1.5f;         // cells per sphere (sets the cell size)
+    int mode = 2;                        // 1: build whenever the spheres allow; 2: only when the
+                                         //    grid is expected to beat the BVH
+    uint32_t min_prims = 8192;           // mode 2: fewer spheres keep the BVH
+    float max_cells_per_ray = 6.0f;      // mode 2: estimated cells a ray crosses before a hit
+    uint32_t max_refs_per_cell = 64;     // mode 2: a fuller cell means clustered spheres
+    uint32_t max_cells_per_prim = 4096;  // any mode: a sphere spanning more cells stops the build
+};
+
+// Outcome of one build attempt.
+struct GridReport {
+    bool built = false;
+    const char* reason = "";   // why the grid was not built
+    uint32_t n_valid = 0;      // spheres with a finite, non-empty box
+    double cells_per_ray = 0;  // estimated cells crossed per ray before a hit
+    uint32_t max_refs = 0;     // fullest cell
+};
+
+// Builds the grid of the n spheres (positions [n][3], radii [n]) on `st` and waits for it.
+// Returns a CUDA error only for device failures; a grid that should not be used (mode 2 rules,
+// a sphere spanning too many cells, no valid sphere) leaves out.n_cells == 0 with
+// report.built == false and report.reason set.
+cudaError_t build_grid(const float* position, const float* radius, uint32_t n,
+                       const GridParams& gp, GridBuffers& out, Scratch& scratch, cudaStream_t st,
+                       GridReport& report);
+
+}  // namespace fr
+
+#endif

@@ -555,6 +555,8 @@ struct TracerH {
         d["kernel_launches"] = st.kernel_launches;
         d["bvh_builds"] = st.bvh_builds;
         d["bvh_refits"] = st.bvh_refits;
+        d["grid_builds"] = st.grid_builds;
+        d["grid"] = st.last_render_grid;
         d["bvh_build_ms"] = st.bvh_build_ms;
         d["primary_ms"] = st.primary_ms;
         d["shade_ms"] = st.shade_ms;
@@ -748,6 +750,14 @@ PYBIND11_MODULE(_gpu, m)
 
     py::class_<SceneH, std::shared_ptr<SceneH>>(m, "Scene")
         .def(py::init<std::shared_ptr<DeviceH>>())
+        .def("getAccel",
+             [](SceneH& s) {
+                 // (uses a sphere grid, why not when one was considered) after the last build
+                 int grid = 0;
+                 char reason[128];
+                 check(fr_scene_get_accel(s.scene, &grid, reason, sizeof(reason)));
+                 return py::make_tuple(grid != 0, std::string(reason));
+             })
         .def("setCamera", [](SceneH& s, const UserCamera& c) { s.camera = c; })
         .def("getCamera", [](SceneH& s) -> UserCamera& { return s.camera; },
              py::return_value_policy::reference_internal)

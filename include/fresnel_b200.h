@@ -125,6 +125,8 @@ typedef struct fr_stats {
     double primary_ms, shade_ms, extend_ms;
     uint64_t primary_launches, shade_launches, extend_launches;
     uint64_t bvh_refits;    /* of bvh_builds, how many refitted an existing tree */
+    uint64_t grid_builds;   /* sphere grids built (device option "accel") */
+    uint32_t last_render_grid; /* 1 if the last render traced through a sphere grid */
 } fr_stats;
 
 typedef struct fr_device fr_device;
@@ -177,6 +179,13 @@ FR_API fr_status fr_device_timer_stop(fr_device* dev, float* ms);
  *   "refit"         1: when a geometry's arrays change but its primitive count and the build
  *                   options do not, refit its tree (new boxes, same topology) instead of
  *                   rebuilding it; 0: always rebuild, as the reference does (default)
+ *   "accel"         acceleration structure of a scene whose only enabled geometry is a sphere
+ *                   geometry: 0: its BVH; 1: a uniform grid of the spheres (walked cell by cell
+ *                   along each ray); 2 (default): the grid when it is expected to be faster
+ *                   (at least 8192 spheres, a ray crossing at most 6 cells on average before a
+ *                   hit, no cell with more than 64 spheres), else the BVH.  Other scenes always
+ *                   use BVHs.  The closest hits do not depend on the choice (ties aside).
+ *   "grid_density"  grid cells per sphere (default 1.5; (0, 64])
  * Setting an option marks every BVH of the device's scenes for rebuild when it changes the
  * tree.  Unknown names or out-of-range values return FR_ERR_INVALID. */
 FR_API fr_status fr_device_set_option(fr_device* dev, const char* name, double value);
@@ -189,6 +198,10 @@ FR_API fr_status fr_device_set_profiling(fr_device* dev, int enable);
 
 /* Scene::Scene (fresnel/gpu/Scene.cc:15-28). */
 FR_API fr_status fr_scene_create(fr_device* dev, fr_scene** out);
+/* Which acceleration structure the scene's last build chose (no counterpart in the reference):
+ * *grid = 1 for a sphere grid, 0 for BVHs; reason (nullable, cap bytes) receives why a grid was
+ * not chosen when one was considered ("" otherwise). */
+FR_API fr_status fr_scene_get_accel(const fr_scene* scene, int* grid, char* reason, size_t cap);
 FR_API fr_status fr_scene_destroy(fr_scene* scene);
 
 /* ---------------- geometry: fresnel/gpu/Geometry*.cc ---------------- */

@@ -136,9 +136,17 @@ inline float box_area(const Box& b)
     return 2.0f * (dx * dy + dy * dz + dz * dx);
 }
 
-// Primitive bounds (fresnel/cpu/GeometrySphere.cc:60-73, GeometryCylinder.cc:55-70,
-// GeometryConvexPolyhedron.cc:119-132, GeometryMesh.cc:81-113), inflated by a small relative
-// margin so that rounding in the box test can never cull a primitive the intersector accepts.
+inline Box box_of(float lx, float ly, float lz, float ux, float uy, float uz)
+{
+    return Box{{lx, ly, lz}, {ux, uy, uz}};
+}
+
+// Primitive bounds with the reference's formulas (fresnel/cpu/GeometrySphere.cc:60-73,
+// GeometryCylinder.cc:55-70, GeometryConvexPolyhedron.cc:119-132, GeometryMesh.cc:81-113,
+// GeometryPolygon.cc:89-104): a box with lower > upper (a negative radius) or a non-finite
+// bound is left out of the tree, as Embree leaves out invalid user-geometry boxes.  Valid boxes
+// are inflated by a small relative margin so that rounding in the box test can never cull a
+// primitive the intersector accepts.
 Box prim_box(const Geom& g, uint32_t prim)
 {
     Box b = box_empty();
@@ -146,24 +154,21 @@ Box prim_box(const Geom& g, uint32_t prim)
     case FR_GEOM_SPHERE: {
         F3 p = g.position[prim];
         float r = g.radius[prim];
-        box_grow(b, p.x - r, p.y - r, p.z - r);
-        box_grow(b, p.x + r, p.y + r, p.z + r);
+        b = box_of(p.x - r, p.y - r, p.z - r, p.x + r, p.y + r, p.z + r);
         break;
     }
     case FR_GEOM_CYLINDER: {
         F3 A = g.points[2 * prim], B = g.points[2 * prim + 1];
         float r = g.radius[prim];
-        box_grow(b, A.x - r, A.y - r, A.z - r);
-        box_grow(b, A.x + r, A.y + r, A.z + r);
-        box_grow(b, B.x - r, B.y - r, B.z - r);
-        box_grow(b, B.x + r, B.y + r, B.z + r);
+        b = box_of(std::min(A.x - r, B.x - r), std::min(A.y - r, B.y - r),
+                   std::min(A.z - r, B.z - r), std::max(A.x + r, B.x + r),
+                   std::max(A.y + r, B.y + r), std::max(A.z + r, B.z + r));
         break;
     }
     case FR_GEOM_POLYHEDRON: {
         F3 p = g.position[prim];
         float r = g.poly_radius;
-        box_grow(b, p.x - r, p.y - r, p.z - r);
-        box_grow(b, p.x + r, p.y + r, p.z + r);
+        b = box_of(p.x - r, p.y - r, p.z - r, p.x + r, p.y + r, p.z + r);
         break;
     }
     case FR_GEOM_MESH: {
@@ -176,13 +181,15 @@ Box prim_box(const Geom& g, uint32_t prim)
         }
         break;
     }
-    case FR_GEOM_POLYGON: {  // fresnel/cpu/GeometryPolygon.cc:89-104
+    case FR_GEOM_POLYGON: {
         const float x = g.pos2[2 * prim], y = g.pos2[2 * prim + 1], r = g.pg_radius;
-        box_grow(b, x - r, y - r, float(0.0 - 1e-5));
-        box_grow(b, x + r, y + r, float(0.0 + 1e-5));
+        b = box_of(x - r, y - r, float(0.0 - 1e-5), x + r, y + r, float(0.0 + 1e-5));
         break;
     }
     }
+    for (int k = 0; k < 3; ++k)
+        if (!(std::isfinite(b.lo[k]) && std::isfinite(b.hi[k]) && b.lo[k] <= b.hi[k]))
+            return box_empty();
     float scale = 0;
     for (int k = 0; k < 3; ++k)
         scale = std::max(scale, std::max(std::fabs(b.lo[k]), std::fabs(b.hi[k])));

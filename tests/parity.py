@@ -31,3 +31,33 @@ def path_render(device, scene, w, h, samples, light_samples=1, seed=None):
         t.seed = seed
     t.sample(scene, samples=samples, light_samples=light_samples)
     return numpy.array(t.linear_output[:]), numpy.array(t.output[:]), t
+
+
+def odd_radii_scene(device, n=3000, seed=5):
+    """Spheres among which some radii are negative, infinite, NaN or zero, and cylinders with
+    some infinite or NaN radii: the reference's bounds of those are inverted or not finite, so
+    they are never hit.  (A negative cylinder radius is left out: the reference's bounds of such
+    a cylinder can be valid yet smaller than the capsule its intersector hits, so which rays
+    reach it depends on each tree's boxes.)"""
+    import fresnel_b200 as fresnel
+    rng = numpy.random.default_rng(seed)
+    pos = rng.uniform(-12, 12, (n, 3)).astype(numpy.float32)
+    r = rng.uniform(0.2, 0.9, n).astype(numpy.float32)
+    r[::97] = -0.5
+    r[1::101] = numpy.inf
+    r[2::103] = numpy.nan
+    r[3::107] = 0.0
+    scene = fresnel.Scene(device)
+    fresnel.geometry.Sphere(scene, position=pos, radius=r,
+                            material=fresnel.material.Material(color=(0.3, 0.6, 0.9)))
+    m = 400
+    a = rng.uniform(-12, 12, (m, 3)).astype(numpy.float32)
+    pts = numpy.stack([a, a + rng.normal(0, 1.5, (m, 3)).astype(numpy.float32)], axis=1)
+    rc = numpy.full(m, 0.15, numpy.float32)
+    rc[::7] = numpy.inf
+    rc[1::11] = numpy.nan
+    fresnel.geometry.Cylinder(scene, points=pts, radius=rc,
+                              material=fresnel.material.Material(color=(0.9, 0.5, 0.2)))
+    scene.camera = fresnel.camera.Orthographic(position=(0, 0, 40), look_at=(0, 0, 0),
+                                               up=(0, 1, 0), height=26)
+    return scene

@@ -15,7 +15,7 @@ import pytest
 import fresnel_b200 as fresnel
 from fresnel_b200 import workloads
 from grazing import classify
-from parity import preview_hits
+from parity import odd_radii_scene, preview_hits
 
 pytestmark = pytest.mark.gpu
 
@@ -34,6 +34,7 @@ SCENES = {
     "dense_spheres": (_dense, 192, 108),
     "mixed": (lambda d: workloads.config3(d, scale=0.002), 160, 90),
     "mixed_large": (lambda d: workloads.config3(d, scale=0.02), 128, 72),
+    "odd_radii": (odd_radii_scene, 120, 120),
     "polygons": (workloads.polygons, 160, 120),
     "polygons_spheres": (lambda d: workloads.polygons(d, spheres=60), 160, 120),
     "polygons_ortho": (lambda d: workloads.polygons(d, perspective=False, rounding_radius=0.0),
