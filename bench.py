@@ -625,6 +625,16 @@ def main():
     dom = max(kern, key=lambda k: kern[k][1])
     dom_rays, dom_ms, launches = kern[dom]
     achieved = (dom_rays * wl.bytes_per_ray) / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else None
+    # The algorithmic bytes above are those of the reference's BVH (fixed box and primitive
+    # tests per ray).  The bytes of the structure this run traversed, from the engine's own
+    # counters over the frame: per ray 24 B in, 16 B out, 12 B of colour, then per node box
+    # test 32 B (BVH) or per grid cell 8 B of offsets, and 16 B per sphere tested.
+    grid = bool(st.get("grid", 0))
+    per_box = 8.0 if grid else 32.0
+    run_bytes = (52.0 + per_box * st["box_tests"] / rays + 16.0 * st["prim_tests"] / rays
+                 if rays > 0 else None)
+    achieved_run = ((dom_rays * run_bytes) / (dom_ms / 1e3) / 1e9
+                    if dom_ms > 0 and run_bytes else None)
     # DRAM bytes per launch: this kernel's DRAM bytes per ray from an ncu capture
     # (dram__bytes_read.sum + dram__bytes_write.sum over every launch of one frame, divided by
     # that frame's rays) times the mean rays per launch here.
@@ -659,14 +669,15 @@ def main():
             e2e_ms.append(dt)
     e2e = None
     if e2e_ms:
-        builds = int(tracer._tracer.getStats()["bvh_builds"])
+        est = tracer._tracer.getStats()
+        builds = int(est["bvh_builds"]) + int(est.get("grid_builds", 0))
         e2e_step = barrier_max(statistics.mean(e2e_ms))
         e2e_value = barrier_sum(rays_per_frame) / (e2e_step / 1e3) / 1e6
         assert out is not None and out.shape == (wl.h, wl.w, 4)
         e2e = {"value": e2e_value, "unit": "Mrays/s",
                "h2d_bytes_per_step": int(sum(h.nbytes for _, h in arrays)),
                "d2h_bytes_per_step": int(out.nbytes), "ms_per_step": e2e_step,
-               "bvh_builds": builds}
+               "builds": builds}
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline and not args.trace_only:
@@ -677,6 +688,7 @@ def main():
 
     if rank == 0:
         cfg = config_of(wl, world)
+        cfg["accel"] = "sphere grid" if grid else "bvh"
         cfg["l2"] = ("inputs larger than L2 (path state of 144 B per slot for every sample in "
                      "flight, plus the scene arrays and BVH)" if not wl.preview else
                      "scene arrays and BVH; the image is written once per frame")
@@ -693,7 +705,14 @@ def main():
                          "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
                          "peak_source": peak_kind, "kernel": dom,
                          "rays": dom_rays, "kernel_ms": dom_ms, "launches": launches,
-                         "bytes_per_ray": wl.bytes_per_ray},
+                         "bytes_per_ray": wl.bytes_per_ray,
+                         "accel": "grid" if grid else "bvh",
+                         "bytes_per_ray_run": run_bytes, "achieved_run": achieved_run,
+                         "frac_run": (achieved_run / hbm) if achieved_run else None,
+                         "note": ("bytes_per_ray is the reference BVH's per-ray work; the "
+                                  "sphere grid reads bytes_per_ray_run, so frac above 1 "
+                                  "means less work per ray, not more bandwidth")
+                         if grid else None},
             "clocks": clk.summary(),
             "e2e": e2e,
             "cpu_baseline": cpu,

@@ -2189,6 +2189,7 @@ fr_status fr_batch_render(fr_batch* b)
     std::vector<uint32_t> wave_first, wave_items, wave_pixels;
     int width = 4;
     uint32_t mask = 0;
+    bool all_grid = true;  // every render traces a sphere grid: the grid-only kernels serve
     for (auto& wv : waves) {
         wave_first.push_back(uint32_t(jobs.size()));
         uint64_t slot = 0, item = 0, pixel = 0;
@@ -2203,6 +2204,7 @@ fr_status fr_batch_render(fr_batch* b)
             if (J.P.bvh_width != 4)
                 width = 2;
             mask |= J.P.type_mask;
+            all_grid = all_grid && J.P.scene.grid.n_cells != 0;
             J.slot_base = uint32_t(slot);
             J.item_base = uint32_t(item);
             J.pixel_base = uint32_t(pixel);
@@ -2216,6 +2218,8 @@ fr_status fr_batch_render(fr_batch* b)
         wave_items.push_back(uint32_t(item));
         wave_pixels.push_back(uint32_t(pixel));
     }
+    if (all_grid && !jobs.empty())
+        mask = MASK_GRID;
     wave_first.push_back(uint32_t(jobs.size()));
     if (mask == 0)
         mask = MASK_SPHERES;  // empty scenes: every ray misses

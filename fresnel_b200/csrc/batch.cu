@@ -333,6 +333,8 @@ cudaError_t capture(const BatchDev& B, int num_sms, cudaStream_t s0, cudaGraphEx
 cudaError_t batch_graph_create(const BatchDev& B, int width, uint32_t type_mask, int num_sms,
                                cudaStream_t capture_stream, cudaGraphExec_t* exec)
 {
+    if (type_mask == MASK_GRID)  // every render of the batch traces a sphere grid
+        return capture<4, MASK_GRID>(B, num_sms, capture_stream, exec);
     const bool spheres_only = (type_mask & ~MASK_SPHERES) == 0u;
     if (width == 4)
         return spheres_only ? capture<4, MASK_SPHERES>(B, num_sms, capture_stream, exec)

@@ -52,7 +52,8 @@ struct BatchDev {
 constexpr uint32_t BATCH_MAX_PAIRS = 1u << 16;
 
 // Capture the whole-batch graph for trees of `width` (2 or 4) and the geometry types in
-// `type_mask`, grids sized for num_sms. The buffers behind B must outlive the graph.
+// `type_mask` (MASK_GRID: every render traces a sphere grid), grids sized for num_sms. The
+// buffers behind B must outlive the graph.
 cudaError_t batch_graph_create(const BatchDev& B, int width, uint32_t type_mask, int num_sms,
                                cudaStream_t capture_stream, cudaGraphExec_t* exec);
 

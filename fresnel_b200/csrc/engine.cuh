@@ -880,28 +880,31 @@ __device__ __forceinline__ void trace_grid(const GridDev& G, const RayK& ray, fl
     }
 }
 
+__device__ __forceinline__ Hit trace_grid_hit(const GridDev& G, const RayK& ray, float tnear,
+                                              float tmax, TraceCount& tc)
+{
+    uint32_t slot = MISS;
+    trace_grid(G, ray, tnear, tmax, slot, tc);
+    Hit h;
+    h.geom = slot == MISS ? MISS : G.geom;
+    h.prim = slot == MISS ? 0u : __ldg(G.ref_prim + slot);
+    return h;
+}
+
 // Geometry-type masks a kernel is specialised for (bit FR_GEOM_* set = type handled).
 constexpr uint32_t MASK_SPHERES = 1u << FR_GEOM_SPHERE;
 constexpr uint32_t MASK_ALL = 0x1Fu;  // every FR_GEOM_* type
+// Kernels specialised for a scene of spheres traced through its uniform grid (SceneDev::grid),
+// with no BVH code compiled in.
+constexpr uint32_t MASK_GRID = 1u << 31;
 
-// Closest hit over all enabled geometries of the scene.  WIDTH selects the binary (2) or
-// 4-wide (4) tree; MASK the geometry types compiled in (the host only launches a MASK that
-// covers every enabled geometry of the scene).
+// Closest hit through the scene's BVHs: its combined tree, or each enabled geometry's tree.
 template <int WIDTH, uint32_t MASK>
-__device__ __forceinline__ Hit trace_closest(const SceneDev& sc, V3 o, V3 d, float tnear,
-                                             TraceCount& tc)
+__device__ __forceinline__ Hit trace_closest_bvh(const SceneDev& sc, const RayK& ray, float tnear,
+                                                 TraceCount& tc)
 {
-    RayK ray = make_rayk(o, d);
     float tmax = __int_as_float(0x7f800000);  // +inf
     uint32_t hg = MISS, hs = 0;
-    if (MASK == MASK_SPHERES && sc.grid.n_cells != 0) {
-        uint32_t slot = MISS;
-        trace_grid(sc.grid, ray, tnear, tmax, slot, tc);
-        Hit h;
-        h.geom = slot == MISS ? MISS : sc.grid.geom;
-        h.prim = slot == MISS ? 0u : __ldg(sc.grid.ref_prim + slot);
-        return h;
-    }
     if (WIDTH == 4 && sc.n_nodes4 != 0) {
         traverse4_core(sc.nodes4, sc.n_nodes4, sc.n_prims, ray, tmax, sc.status, tc,
                        [&](uint32_t first, uint32_t count) {
@@ -935,6 +938,25 @@ __device__ __forceinline__ Hit trace_closest(const SceneDev& sc, V3 o, V3 d, flo
     h.geom = hg;
     h.prim = (hg == MISS) ? 0u : __ldg(sc.geoms[hg].order + hs);
     return h;
+}
+
+// Closest hit over all enabled geometries of the scene.  WIDTH selects the binary (2) or
+// 4-wide (4) tree; MASK the geometry types compiled in (the host only launches a MASK that
+// covers every enabled geometry of the scene), or MASK_GRID for the sphere grid alone.
+template <int WIDTH, uint32_t MASK>
+__device__ __forceinline__ Hit trace_closest(const SceneDev& sc, V3 o, V3 d, float tnear,
+                                             TraceCount& tc)
+{
+    const RayK ray = make_rayk(o, d);
+    const float tmax = __int_as_float(0x7f800000);  // +inf
+    if constexpr (MASK == MASK_GRID) {
+        return trace_grid_hit(sc.grid, ray, tnear, tmax, tc);
+    } else {
+        // kernels for BVH scenes also serve grid scenes (a batch may mix both)
+        if ((MASK & MASK_SPHERES) && sc.grid.n_cells != 0)
+            return trace_grid_hit(sc.grid, ray, tnear, tmax, tc);
+        return trace_closest_bvh<WIDTH, MASK>(sc, ray, tnear, tc);
+    }
 }
 
 // Closest hit for coherent rays with the warp-cooperative traversal (4-wide trees only).  All

@@ -37,7 +37,7 @@ __global__ void __launch_bounds__(256) k_path_primary(FrameParams P, PathState S
     bool push = false;
     uint32_t slot = 0;
     TraceCount tc;
-    if (PACKET) {
+    if constexpr (PACKET) {
         // a warp's rays are neighbouring samples of the same pixels: trace them as a packet
         __shared__ uint32_t stk_node[8][TRAVERSAL_STACK];
         __shared__ float stk_t[8][TRAVERSAL_STACK];
@@ -592,6 +592,7 @@ LaunchShape path_launch_shape(int num_sms)
     s.extend_grid[1] = num_sms * blocks_per_sm(k_path_extend<2, MASK_ALL>);
     s.extend_grid[2] = num_sms * blocks_per_sm(k_path_extend<4, MASK_SPHERES>);
     s.extend_grid[3] = num_sms * blocks_per_sm(k_path_extend<4, MASK_ALL>);
+    s.extend_grid_sphere_grid = num_sms * blocks_per_sm(k_path_extend<4, MASK_GRID>);
     s.persistent_grid[0] = num_sms * blocks_per_sm(k_path_extend_persistent<MASK_SPHERES>);
     s.persistent_grid[1] = num_sms * blocks_per_sm(k_path_extend_persistent<MASK_ALL>);
     s.primary_grid[0] = num_sms * blocks_per_sm(k_path_primary_persistent<MASK_SPHERES>);
@@ -603,6 +604,11 @@ void launch_path_primary(const FrameParams& P, const PathState& S, const LaunchS
                          cudaStream_t st)
 {
     bool spheres_only = (P.type_mask & ~MASK_SPHERES) == 0u;
+    if (P.scene.grid.n_cells != 0) {
+        const uint32_t n = primary_items(P.w, P.h, P.batch, P.tile_log2);
+        k_path_primary<4, MASK_GRID><<<(n + 255) / 256, 256, 0, st>>>(P, S);
+        return;
+    }
     if (P.bvh_width == 4 && P.persistent) {
         if (spheres_only)
             k_path_primary_persistent<MASK_SPHERES><<<shape.primary_grid[0], 256, 0, st>>>(P, S);
@@ -641,6 +647,10 @@ void launch_path_extend(const FrameParams& P, const PathState& S, int iteration,
 {
     bool spheres_only = (P.type_mask & ~MASK_SPHERES) == 0u;
     int q = iteration & 1;
+    if (P.scene.grid.n_cells != 0) {
+        k_path_extend<4, MASK_GRID><<<shape.extend_grid_sphere_grid, 256, 0, st>>>(P, S, q);
+        return;
+    }
     if (P.bvh_width == 4 && P.persistent) {
         if (spheres_only)
             k_path_extend_persistent<MASK_SPHERES><<<shape.persistent_grid[0], 256, 0, st>>>(P, S, q);
@@ -675,6 +685,8 @@ void launch_preview(const FrameParams& P, uint32_t aa_n, uint2* hits, cudaStream
     dim3 grid((P.w + 15) / 16, (P.h + 15) / 16);
     auto k = pick(P, k_preview<2, MASK_SPHERES>, k_preview<2, MASK_ALL>,
                   k_preview<4, MASK_SPHERES>, k_preview<4, MASK_ALL>);
+    if (P.scene.grid.n_cells != 0)
+        k = k_preview<4, MASK_GRID>;
     k<<<grid, block, 0, st>>>(P, aa_n, hits);
 }
 

@@ -59,6 +59,7 @@ struct LaunchShape {
     int shade_grid_occ[2];   // shade kernel compiled for 3|4 blocks per SM
     int refill_grid[2];      // extension kernel with per-lane refill [spheres only|all types]
     int extend_grid[4];      // [width 2|4][spheres only|all types]
+    int extend_grid_sphere_grid;  // scenes traced through a uniform sphere grid
     int persistent_grid[2];  // 4-wide persistent extend kernel [spheres only|all types]
     int primary_grid[2];     // 4-wide persistent primary kernel [spheres only|all types]
 };
