@@ -102,12 +102,17 @@ __device__ __forceinline__ bool shade_pixel(const FrameParams& P, const PathStat
     const uint32_t k = pi.k;
     const uint32_t pixel = pi.j * P.w + pi.i;
     const uint32_t n_samples = P.n_samples + k;
-    uint2 ld = S.ls_depth[p];
+    const uint2 ld = S.ls_depth[p];
     uint32_t ls = ld.x;
     PathS s;
-    s.result = rgb3(S.result[p]);
-    s.att = rgb3(S.att[p]);
     s.depth = ld.y;
+    if (ls == 0u && s.depth == 0u) {  // a fresh primary hit (primary_finish)
+        s.result = c3(0.0f, 0.0f, 0.0f);
+        s.att = c3(1.0f, 1.0f, 1.0f);
+    } else {
+        s.result = rgb3(S.result[p]);
+        s.att = rgb3(S.att[p]);
+    }
     s.origin = v3(0, 0, 0);
     s.dir = v3(0, 0, 0);
     const uint2 ph = S.prim_hit[p];
@@ -162,7 +167,9 @@ __device__ __forceinline__ bool shade_pixel(const FrameParams& P, const PathStat
 
 // Primary ray of one item: closest hit; a miss finishes its pixel sample (every light sample
 // sees the background: radiance bg * L, fresnel/common/TracerPathMethods.h:44-50), a hit
-// initialises the path state. Returns true for a hit (the slot is queued for shading).
+// stores the ray and starts the path: (light sample, depth) = (0, 0), which tells the shade
+// pass that the throughput is 1 and the radiance 0 (not stored).  Returns true for a hit (the
+// slot is queued for shading).
 __device__ __forceinline__ bool primary_finish(const FrameParams& P, const PathState& S,
                                                uint32_t slot, V3 o, V3 d, Hit h)
 {
@@ -176,8 +183,6 @@ __device__ __forceinline__ bool primary_finish(const FrameParams& P, const PathS
     S.prim_o[slot] = f4(o);
     S.prim_d[slot] = f4(d);
     S.ls_depth[slot] = make_uint2(0u, 0u);
-    S.att[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-    S.result[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     return true;
 }
 

@@ -147,9 +147,7 @@ struct PrimarySource {
             } else {
                 S.prim_o[slot] = f4(L.ray.o);
                 S.prim_d[slot] = f4(L.ray.d);
-                S.ls_depth[slot] = make_uint2(0u, 0u);
-                S.att[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-                S.result[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                S.ls_depth[slot] = make_uint2(0u, 0u);  // see primary_finish
                 push = true;
             }
         }
