@@ -179,11 +179,18 @@ FR_HD void camera_ray(const CamK& k, uint32_t i, uint32_t j, uint32_t sample, V3
     }
     V3 F = k.p - k.w * k.focal_d;
     V3 C = F + plane * k.focal_h;
-    U4 r = philox(0u, 0u, sample, TAG_APERTURE, pixel, k.seed);
-    float theta = u01(r.x) * 2.0f * PI_F;
-    float rad = u01(r.y) * k.aperture * 0.5f;
-    V3 offset = rad * cosf(theta) * k.u + rad * sinf(theta) * k.v;
-    origin = k.p + offset;
+    if (k.aperture == 0.0f && k.p.x != 0.0f && k.p.y != 0.0f && k.p.z != 0.0f) {
+        // pinhole (f_stop infinite): the lens sample is scaled by a zero aperture, so the offset
+        // is a signed zero in each component and p + offset is exactly p (no component of p is
+        // zero); the lens sample need not be drawn
+        origin = k.p;
+    } else {
+        U4 r = philox(0u, 0u, sample, TAG_APERTURE, pixel, k.seed);
+        float theta = u01(r.x) * 2.0f * PI_F;
+        float rad = u01(r.y) * k.aperture * 0.5f;
+        V3 offset = rad * cosf(theta) * k.u + rad * sinf(theta) * k.v;
+        origin = k.p + offset;
+    }
     dir = C - origin;
     dir = dir * (1.0f / sqrtf(dot(dir, dir)));
 }
