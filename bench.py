@@ -594,7 +594,6 @@ def main():
     scene._scene.build()
     for _ in range(args.warmup):
         frame()
-    dd.setProfiling(True)
     tracer._tracer.resetStats()
     reps.barrier()
     torch.cuda.synchronize()
@@ -607,7 +606,18 @@ def main():
     torch.cuda.synchronize()
     reps.barrier()
     st = tracer._tracer.getStats()
+    # Per-kernel device times from the same K frames rendered again with CUDA events around
+    # every launch (the events cost about 2% of a frame, so the timed frames above run without).
+    dd.setProfiling(True)
+    tracer._tracer.resetStats()
+    for _ in range(args.steps):
+        frame()
+    dd.synchronize()
+    pst = tracer._tracer.getStats()
     dd.setProfiling(False)
+    for key in ("primary_ms", "shade_ms", "extend_ms", "primary_launches", "shade_launches",
+                "extend_launches"):
+        st[key] = pst[key]
     rays = float(st["rays"])
     ms_max = barrier_max(ms)
     rays_all = barrier_sum(rays)

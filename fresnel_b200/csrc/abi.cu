@@ -163,6 +163,7 @@ struct fr_device {
     int packet = 0;                        // warp-cooperative primary traversal
     int refill = 0;                        // extension rays with per-lane refill
     int accel = 2;                         // sphere grid: 0 never, 1 whenever possible, 2 auto
+    int fuse_shade = 1;                    // primary rays shaded in the primary pass
     float grid_cells_per_prim = 1.5f;      // grid cells per sphere
     std::vector<fr_scene*> scenes;         // to mark BVHs stale when a build option changes
     void* static_path = nullptr;           // this device's copy of g_static_path (looked up once)
@@ -1120,6 +1121,10 @@ fr_status fr_device_set_option(fr_device* d, const char* name, double value)
         if (value != 0.0 && value != 1.0)
             return fail(FR_ERR_INVALID, "persistent must be 0 or 1");
         d->persistent = int(value);
+    } else if (n == "fuse_shade") {
+        if (!(value == 0.0 || value == 1.0))
+            return fail(FR_ERR_INVALID, "fuse_shade must be 0 or 1");
+        d->fuse_shade = int(value);
     } else if (n == "accel") {
         if (!(value == 0.0 || value == 1.0 || value == 2.0))
             return fail(FR_ERR_INVALID, "accel must be 0 (BVH), 1 (sphere grid) or 2 (automatic)");
@@ -1158,6 +1163,8 @@ fr_status fr_device_get_option(const fr_device* d, const char* name, double* val
         *value = double(d->path_slots);
     else if (n == "accel")
         *value = d->accel;
+    else if (n == "fuse_shade")
+        *value = d->fuse_shade;
     else if (n == "grid_density")
         *value = d->grid_cells_per_prim;
     else if (n == "builder")
@@ -1633,13 +1640,21 @@ fr_status fr_tracer_render_path(fr_tracer* t, fr_scene* sc, const fr_render_para
     for (uint32_t done = 0; done < n_render;) {
         P.n_samples = first_sample + done;
         P.batch = batch < n_render - done ? batch : n_render - done;
-        FR_CUDA(cudaMemsetAsync(S.ctr + 3, 0, sizeof(uint32_t), st), "clearing a counter");
-        timed(0, [&] { launch_path_primary(P, S, t->dev->shape, st); });
+        // primary rays shaded at once: the first shade pass is folded into the primary pass
+        const bool fused = t->dev->fuse_shade && !P.persistent && !P.packet;
+        if (fused) {
+            FR_CUDA(cudaMemsetAsync(S.ctr, 0, 4 * sizeof(uint32_t), st), "clearing the queues");
+            timed(0, [&] { launch_path_primary_shade(P, S, st); });
+        } else {
+            FR_CUDA(cudaMemsetAsync(S.ctr + 3, 0, sizeof(uint32_t), st), "clearing a counter");
+            timed(0, [&] { launch_path_primary(P, S, t->dev->shape, st); });
+        }
         t->launches++;
         int it = 0;
         while (true) {
             for (int b = 0; b < CHECK_EVERY; ++b, ++it) {
-                timed(1, [&] { launch_path_shade(P, S, it, t->dev->shape, st); });
+                if (!(fused && it == 0))
+                    timed(1, [&] { launch_path_shade(P, S, it, t->dev->shape, st); });
                 timed(2, [&] { launch_path_extend(P, S, it, t->dev->shape, st); });
                 t->launches += 2;
             }

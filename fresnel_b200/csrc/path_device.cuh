@@ -92,35 +92,28 @@ __device__ __forceinline__ float4 welford(const FrameParams& P, float4 old, floa
     return make_float4(nr, ng, nb, na);
 }
 
-// Shade the current path vertex of one slot; returns true if the path needs another closest hit.
-// p indexes the path state; local = k * w * h + pixel numbers the slot within its render (equal
-// to p for a single render, p minus the render's first slot in a batch of renders).
-__device__ __forceinline__ bool shade_pixel(const FrameParams& P, const PathState& S, uint32_t p,
-                                            uint32_t local)
+// The shading loop of one slot from its current state (TracerPath's hit/miss programs,
+// fresnel/common/TracerPathMethods.h:36-168, light samples in order): shade the vertex, then
+// either store the continuing path (returns true: it needs another closest hit) or restart the
+// next light sample from the cached primary hit, or store the finished pixel sample (returns
+// false).  FIRST_IN_REGS: the first vertex's ray (ro0, rd0) and hit (the primary hit ph) come
+// from the caller's registers instead of the path state.
+template <bool FIRST_IN_REGS>
+__device__ __forceinline__ bool shade_core(const FrameParams& P, const PathState& S, uint32_t p,
+                                           uint32_t pixel, uint32_t n_samples, uint32_t ls,
+                                           PathS s, uint2 ph, V3 ro0, V3 rd0)
 {
-    const PrimaryItem pi = primary_item(local, P.w, P.h, P.batch, P.tile_log2);
-    const uint32_t k = pi.k;
-    const uint32_t pixel = pi.j * P.w + pi.i;
-    const uint32_t n_samples = P.n_samples + k;
-    const uint2 ld = S.ls_depth[p];
-    uint32_t ls = ld.x;
-    PathS s;
-    s.depth = ld.y;
-    if (ls == 0u && s.depth == 0u) {  // a fresh primary hit (primary_finish)
-        s.result = c3(0.0f, 0.0f, 0.0f);
-        s.att = c3(1.0f, 1.0f, 1.0f);
-    } else {
-        s.result = rgb3(S.result[p]);
-        s.att = rgb3(S.att[p]);
-    }
-    s.origin = v3(0, 0, 0);
-    s.dir = v3(0, 0, 0);
-    const uint2 ph = S.prim_hit[p];
     const uint32_t key1 = P.cam.seed;
+    bool first = FIRST_IN_REGS;
     while (true) {
         V3 ro, rd;
         uint2 h;
-        if (s.depth == 0) {
+        if (FIRST_IN_REGS && first) {
+            ro = ro0;
+            rd = rd0;
+            h = ph;
+            first = false;
+        } else if (s.depth == 0) {
             ro = xyz(S.prim_o[p]);
             rd = xyz(S.prim_d[p]);
             h = ph;
@@ -165,6 +158,31 @@ __device__ __forceinline__ bool shade_pixel(const FrameParams& P, const PathStat
     }
 }
 
+// Shade the current path vertex of one slot; returns true if the path needs another closest hit.
+// p indexes the path state; local = k * w * h + pixel numbers the slot within its render (equal
+// to p for a single render, p minus the render's first slot in a batch of renders).
+__device__ __forceinline__ bool shade_pixel(const FrameParams& P, const PathState& S, uint32_t p,
+                                            uint32_t local)
+{
+    const PrimaryItem pi = primary_item(local, P.w, P.h, P.batch, P.tile_log2);
+    const uint32_t pixel = pi.j * P.w + pi.i;
+    const uint32_t n_samples = P.n_samples + pi.k;
+    const uint2 ld = S.ls_depth[p];
+    PathS s;
+    s.depth = ld.y;
+    if (ld.x == 0u && s.depth == 0u) {  // a fresh primary hit (primary_finish)
+        s.result = c3(0.0f, 0.0f, 0.0f);
+        s.att = c3(1.0f, 1.0f, 1.0f);
+    } else {
+        s.result = rgb3(S.result[p]);
+        s.att = rgb3(S.att[p]);
+    }
+    s.origin = v3(0, 0, 0);
+    s.dir = v3(0, 0, 0);
+    return shade_core<false>(P, S, p, pixel, n_samples, ld.x, s, S.prim_hit[p], v3(0, 0, 0),
+                             v3(0, 0, 0));
+}
+
 // Primary ray of one item: closest hit; a miss finishes its pixel sample (every light sample
 // sees the background: radiance bg * L, fresnel/common/TracerPathMethods.h:44-50), a hit
 // stores the ray and starts the path: (light sample, depth) = (0, 0), which tells the shade
@@ -194,6 +212,53 @@ __device__ __forceinline__ bool primary_ray(const FrameParams& P, const PathStat
     camera_ray(P.cam, it.i, it.j, P.n_samples + it.k, o, d);
     Hit h = trace_closest<WIDTH, MASK>(P.scene, o, d, PATH_TNEAR, tc);
     return primary_finish(P, S, slot, o, d, h);
+}
+
+// Primary ray of one item shaded at once (the first shade pass folded into the primary pass): a
+// miss finishes its pixel sample as in primary_finish; a hit is shaded from registers, without
+// storing the primary ray (unless a later light sample restarts from it) or reading anything
+// back.  Returns true when the path continues (its extension ray is stored; queue it).
+template <int WIDTH, uint32_t MASK>
+__device__ __forceinline__ bool primary_shade(const FrameParams& P, const PathState& S,
+                                              const PrimaryItem& it, uint32_t slot, TraceCount& tc)
+{
+    V3 o, d;
+    camera_ray(P.cam, it.i, it.j, P.n_samples + it.k, o, d);
+    Hit h = trace_closest<WIDTH, MASK>(P.scene, o, d, PATH_TNEAR, tc);
+    const uint2 ph = make_uint2(h.geom, h.prim);
+    S.prim_hit[slot] = ph;
+    if (h.geom == MISS) {
+        C3 res = P.bg * float(P.light_samples);
+        C3 out = c_div_recip(res, float(P.light_samples));
+        S.sample[slot] = make_float4(out.r, out.g, out.b, P.bg_alpha);
+        return false;
+    }
+    if (P.light_samples > 1u) {  // later light samples restart from the primary ray
+        S.prim_o[slot] = f4(o);
+        S.prim_d[slot] = f4(d);
+    }
+    PathS s;
+    s.result = c3(0.0f, 0.0f, 0.0f);
+    s.att = c3(1.0f, 1.0f, 1.0f);
+    s.depth = 0;
+    s.origin = v3(0, 0, 0);
+    s.dir = v3(0, 0, 0);
+    return shade_core<true>(P, S, slot, it.j * P.w + it.i, P.n_samples + it.k, 0u, s, ph, o, d);
+}
+
+// Append the lanes with push set to queue q (one atomic per warp).
+__device__ __forceinline__ void push_queue(const PathState& S, int q, bool push, uint32_t slot)
+{
+    const uint32_t lane = lane_id();
+    const uint32_t m = __ballot_sync(0xffffffffu, push);
+    if (m) {
+        uint32_t at = 0;
+        if (lane == 0)
+            at = atomicAdd(S.ctr + q, uint32_t(__popc(m)));
+        at = __shfl_sync(0xffffffffu, at, 0);
+        if (push)
+            S.queue[q][at + __popc(m & ((1u << lane) - 1u))] = slot;
+    }
 }
 
 // Append the lanes with push set to queue 1 (one atomic per warp).

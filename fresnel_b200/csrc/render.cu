@@ -64,6 +64,32 @@ __global__ void __launch_bounds__(256) k_path_primary(FrameParams P, PathState S
     }
 }
 
+// Primary rays with their first shading (device option "fuse_shade"): one thread per work item
+// as k_path_primary; continuing paths go straight to the extension queue (queue 0), so the
+// frame's first shade pass is not launched.  Limited to 3 blocks of 256 threads per SM, as the
+// shade kernel.
+template <int WIDTH, uint32_t MASK>
+__global__ void __launch_bounds__(256, 3) k_path_primary_shade(FrameParams P, PathState S)
+{
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t n_items = primary_items(P.w, P.h, P.batch, P.tile_log2);
+    PrimaryItem it;
+    it.valid = false;
+    if (g < n_items)
+        it = primary_item(g, P.w, P.h, P.batch, P.tile_log2);
+    bool push = false;
+    TraceCount tc;
+    if (it.valid)
+        push = primary_shade<WIDTH, MASK>(P, S, it, g, tc);
+    flush_counts(tc, P.stats + 3);
+    push_queue(S, 0, push, g);
+    const uint32_t mv = __ballot_sync(0xffffffffu, it.valid);
+    if (lane_id() == 0 && mv) {
+        atomicAdd(P.stats + 0, (unsigned long long)__popc(mv));
+        atomicAdd(P.stats + 1, (unsigned long long)__popc(mv) * P.light_samples);
+    }
+}
+
 // ---------------------------------------------------------------------------------------------
 // Persistent traversal with per-lane refill (4-wide trees): a warp steps one node visit at a
 // time; whenever at least REFILL lanes are idle, they claim new work items with one atomic, so
@@ -619,6 +645,16 @@ void launch_path_primary(const FrameParams& P, const PathState& S, const LaunchS
                   k_path_primary<4, MASK_SPHERES>, k_path_primary<4, MASK_ALL>);
     if (P.bvh_width == 4 && P.packet)
         k = spheres_only ? k_path_primary<4, MASK_SPHERES, true> : k_path_primary<4, MASK_ALL, true>;
+    k<<<(n_items + 255) / 256, 256, 0, st>>>(P, S);
+}
+
+void launch_path_primary_shade(const FrameParams& P, const PathState& S, cudaStream_t st)
+{
+    const uint32_t n_items = primary_items(P.w, P.h, P.batch, P.tile_log2);
+    auto k = pick(P, k_path_primary_shade<2, MASK_SPHERES>, k_path_primary_shade<2, MASK_ALL>,
+                  k_path_primary_shade<4, MASK_SPHERES>, k_path_primary_shade<4, MASK_ALL>);
+    if (P.scene.grid.n_cells != 0)
+        k = k_path_primary_shade<4, MASK_GRID>;
     k<<<(n_items + 255) / 256, 256, 0, st>>>(P, S);
 }
 

@@ -76,6 +76,10 @@ void launch_path_shade(const FrameParams& P, const PathState& S, int iteration,
                        const LaunchShape& shape, cudaStream_t st);
 void launch_path_extend(const FrameParams& P, const PathState& S, int iteration,
                         const LaunchShape& shape, cudaStream_t st);
+// Or, instead of the primary pass and the first shade pass: primary rays shaded at once, the
+// continuing paths in queue 0 (all four counters must be zero); the loop then starts with the
+// extend of iteration 0.
+void launch_path_primary_shade(const FrameParams& P, const PathState& S, cudaStream_t st);
 // ... then fold the batch's samples into each pixel's running mean, in sample order.
 void launch_path_fold(const FrameParams& P, const PathState& S, cudaStream_t st);
 // Diagnostic comparison of the two 4-wide traversal forms (sphere scenes).
