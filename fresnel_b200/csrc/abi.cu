@@ -1122,8 +1122,8 @@ fr_status fr_device_set_option(fr_device* d, const char* name, double value)
             return fail(FR_ERR_INVALID, "persistent must be 0 or 1");
         d->persistent = int(value);
     } else if (n == "fuse_shade") {
-        if (!(value == 0.0 || value == 1.0))
-            return fail(FR_ERR_INVALID, "fuse_shade must be 0 or 1");
+        if (!(value == 0.0 || value == 1.0 || value == 2.0))
+            return fail(FR_ERR_INVALID, "fuse_shade must be 0, 1 or 2");
         d->fuse_shade = int(value);
     } else if (n == "accel") {
         if (!(value == 0.0 || value == 1.0 || value == 2.0))
@@ -1651,15 +1651,32 @@ fr_status fr_tracer_render_path(fr_tracer* t, fr_scene* sc, const fr_render_para
         }
         t->launches++;
         int it = 0;
+        // bounces fused too: by default for sphere-grid scenes only (a BVH walk in a kernel
+        // compiled for 3 blocks per SM is slower than the separate passes)
+        const bool bounces =
+            fused && (t->dev->fuse_shade == 2 || P.scene.grid.n_cells != 0);
         while (true) {
             for (int b = 0; b < CHECK_EVERY; ++b, ++it) {
+                if (bounces) {
+                    // trace and shade queue it&1 into queue (it&1)^1, cleared first with the
+                    // work counter
+                    FR_CUDA(cudaMemsetAsync(S.ctr + ((it & 1) ^ 1), 0, sizeof(uint32_t), st),
+                            "clearing a queue");
+                    FR_CUDA(cudaMemsetAsync(S.ctr + 2, 0, sizeof(uint32_t), st),
+                            "clearing a counter");
+                    timed(2, [&] { launch_path_bounce(P, S, it, t->dev->shape, st); });
+                    t->launches += 1;
+                    continue;
+                }
                 if (!(fused && it == 0))
                     timed(1, [&] { launch_path_shade(P, S, it, t->dev->shape, st); });
                 timed(2, [&] { launch_path_extend(P, S, it, t->dev->shape, st); });
                 t->launches += 2;
             }
             FR_CUDA(cudaGetLastError(), "launching the path tracer");
-            FR_CUDA(cudaMemcpyAsync(t->dev->h_count, S.ctr + ((it - 1) & 1), sizeof(uint32_t),
+            // the output queue of the last shade pass (or of the last bounce)
+            const int last_q = bounces ? (((it - 1) & 1) ^ 1) : ((it - 1) & 1);
+            FR_CUDA(cudaMemcpyAsync(t->dev->h_count, S.ctr + last_q, sizeof(uint32_t),
                                     cudaMemcpyDeviceToHost, st),
                     "reading the queue length");
             FR_CUDA(cudaStreamSynchronize(st), "path tracer");

@@ -96,12 +96,12 @@ __device__ __forceinline__ float4 welford(const FrameParams& P, float4 old, floa
 // fresnel/common/TracerPathMethods.h:36-168, light samples in order): shade the vertex, then
 // either store the continuing path (returns true: it needs another closest hit) or restart the
 // next light sample from the cached primary hit, or store the finished pixel sample (returns
-// false).  FIRST_IN_REGS: the first vertex's ray (ro0, rd0) and hit (the primary hit ph) come
-// from the caller's registers instead of the path state.
+// false).  FIRST_IN_REGS: the first vertex's ray (ro0, rd0) and hit (h0) come from the
+// caller's registers instead of the path state.
 template <bool FIRST_IN_REGS>
 __device__ __forceinline__ bool shade_core(const FrameParams& P, const PathState& S, uint32_t p,
                                            uint32_t pixel, uint32_t n_samples, uint32_t ls,
-                                           PathS s, uint2 ph, V3 ro0, V3 rd0)
+                                           PathS s, uint2 ph, V3 ro0, V3 rd0, uint2 h0)
 {
     const uint32_t key1 = P.cam.seed;
     bool first = FIRST_IN_REGS;
@@ -111,7 +111,7 @@ __device__ __forceinline__ bool shade_core(const FrameParams& P, const PathState
         if (FIRST_IN_REGS && first) {
             ro = ro0;
             rd = rd0;
-            h = ph;
+            h = h0;
             first = false;
         } else if (s.depth == 0) {
             ro = xyz(S.prim_o[p]);
@@ -180,7 +180,7 @@ __device__ __forceinline__ bool shade_pixel(const FrameParams& P, const PathStat
     s.origin = v3(0, 0, 0);
     s.dir = v3(0, 0, 0);
     return shade_core<false>(P, S, p, pixel, n_samples, ld.x, s, S.prim_hit[p], v3(0, 0, 0),
-                             v3(0, 0, 0));
+                             v3(0, 0, 0), make_uint2(0u, 0u));
 }
 
 // Primary ray of one item: closest hit; a miss finishes its pixel sample (every light sample
@@ -243,7 +243,30 @@ __device__ __forceinline__ bool primary_shade(const FrameParams& P, const PathSt
     s.depth = 0;
     s.origin = v3(0, 0, 0);
     s.dir = v3(0, 0, 0);
-    return shade_core<true>(P, S, slot, it.j * P.w + it.i, P.n_samples + it.k, 0u, s, ph, o, d);
+    return shade_core<true>(P, S, slot, it.j * P.w + it.i, P.n_samples + it.k, 0u, s, ph, o, d,
+                            ph);
+}
+
+// Extension ray of slot p traced and its hit shaded at once (a bounce): the path state is read as
+// the shade pass reads it, with the ray and the hit from registers.  Returns true when the path
+// continues (its next extension ray is stored; queue it).
+template <int WIDTH, uint32_t MASK>
+__device__ __forceinline__ bool bounce(const FrameParams& P, const PathState& S, uint32_t p,
+                                       TraceCount& tc)
+{
+    const V3 o = xyz(S.ray_o[p]);
+    const V3 d = xyz(S.ray_d[p]);
+    const Hit hit = trace_closest<WIDTH, MASK>(P.scene, o, d, PATH_TNEAR, tc);
+    const PrimaryItem pi = primary_item(p, P.w, P.h, P.batch, P.tile_log2);
+    const uint2 ld = S.ls_depth[p];
+    PathS s;
+    s.depth = ld.y;
+    s.result = rgb3(S.result[p]);
+    s.att = rgb3(S.att[p]);
+    s.origin = v3(0, 0, 0);
+    s.dir = v3(0, 0, 0);
+    return shade_core<true>(P, S, p, pi.j * P.w + pi.i, P.n_samples + pi.k, ld.x, s,
+                            S.prim_hit[p], o, d, make_uint2(hit.geom, hit.prim));
 }
 
 // Append the lanes with push set to queue q (one atomic per warp).

@@ -365,6 +365,38 @@ __global__ void __launch_bounds__(256) k_path_extend(FrameParams P, PathState S,
     flush_counts(tc, P.stats + 3);
 }
 
+// Extension rays traced and shaded at once (device option "fuse_shade"): the rays of queue q are
+// taken 32 per warp as in k_path_extend; the continuing paths go to queue q ^ 1, whose length
+// and the work counter (ctr[2]) must be zero at launch.  Limited to 3 blocks per SM, as the
+// shade kernel.
+template <int WIDTH, uint32_t MASK>
+__global__ void __launch_bounds__(256, 3) k_path_bounce(FrameParams P, PathState S, int q)
+{
+    const uint32_t count = S.ctr[q];
+    const uint32_t* queue = S.queue[q];
+    const uint32_t lane = threadIdx.x & 31u;
+    TraceCount tc;
+    while (true) {
+        uint32_t base = 0;
+        if (lane == 0)
+            base = atomicAdd(S.ctr + 2, 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= count)
+            break;
+        const uint32_t idx = base + lane;
+        bool push = false;
+        uint32_t p = 0;
+        if (idx < count) {
+            p = queue[idx];
+            push = bounce<WIDTH, MASK>(P, S, p, tc);
+        }
+        push_queue(S, q ^ 1, push, p);
+        if (lane == 0)
+            atomicAdd(P.stats + 0, (unsigned long long)min(32u, count - base));
+    }
+    flush_counts(tc, P.stats + 3);
+}
+
 // ---------------------------------------------------------------------------------------------
 // Extension rays with per-lane refill: a lane whose ray is finished takes the next queued ray as
 // soon as at least REFILL_MIN lanes of its warp are idle (one atomic per refill), so the lanes of
@@ -617,6 +649,7 @@ LaunchShape path_launch_shape(int num_sms)
     s.extend_grid[2] = num_sms * blocks_per_sm(k_path_extend<4, MASK_SPHERES>);
     s.extend_grid[3] = num_sms * blocks_per_sm(k_path_extend<4, MASK_ALL>);
     s.extend_grid_sphere_grid = num_sms * blocks_per_sm(k_path_extend<4, MASK_GRID>);
+    s.bounce_grid = num_sms * 3;  // k_path_bounce is compiled for 3 blocks per SM
     s.persistent_grid[0] = num_sms * blocks_per_sm(k_path_extend_persistent<MASK_SPHERES>);
     s.persistent_grid[1] = num_sms * blocks_per_sm(k_path_extend_persistent<MASK_ALL>);
     s.primary_grid[0] = num_sms * blocks_per_sm(k_path_primary_persistent<MASK_SPHERES>);
@@ -703,6 +736,17 @@ void launch_path_extend(const FrameParams& P, const PathState& S, int iteration,
     auto k = pick(P, k_path_extend<2, MASK_SPHERES>, k_path_extend<2, MASK_ALL>,
                   k_path_extend<4, MASK_SPHERES>, k_path_extend<4, MASK_ALL>);
     k<<<grid, 256, 0, st>>>(P, S, q);
+}
+
+void launch_path_bounce(const FrameParams& P, const PathState& S, int iteration,
+                        const LaunchShape& shape, cudaStream_t st)
+{
+    const int q = iteration & 1;
+    auto k = pick(P, k_path_bounce<2, MASK_SPHERES>, k_path_bounce<2, MASK_ALL>,
+                  k_path_bounce<4, MASK_SPHERES>, k_path_bounce<4, MASK_ALL>);
+    if (P.scene.grid.n_cells != 0)
+        k = k_path_bounce<4, MASK_GRID>;
+    k<<<shape.bounce_grid, 256, 0, st>>>(P, S, q);
 }
 
 void launch_histogram(const float4* linear, uint32_t n, uint32_t* counts, int num_sms,

@@ -60,6 +60,7 @@ struct LaunchShape {
     int refill_grid[2];      // extension kernel with per-lane refill [spheres only|all types]
     int extend_grid[4];      // [width 2|4][spheres only|all types]
     int extend_grid_sphere_grid;  // scenes traced through a uniform sphere grid
+    int bounce_grid;              // fused extension and shading (k_path_bounce)
     int persistent_grid[2];  // 4-wide persistent extend kernel [spheres only|all types]
     int primary_grid[2];     // 4-wide persistent primary kernel [spheres only|all types]
 };
@@ -80,6 +81,11 @@ void launch_path_extend(const FrameParams& P, const PathState& S, int iteration,
 // continuing paths in queue 0 (all four counters must be zero); the loop then starts with the
 // extend of iteration 0.
 void launch_path_primary_shade(const FrameParams& P, const PathState& S, cudaStream_t st);
+// With the primary pass shaded at once, iteration i may instead be one fused bounce: the rays of
+// q[i&1] traced and shaded, continuing paths into q[(i&1)^1] (whose length and ctr[2] must be
+// zero).
+void launch_path_bounce(const FrameParams& P, const PathState& S, int iteration,
+                        const LaunchShape& shape, cudaStream_t st);
 // ... then fold the batch's samples into each pixel's running mean, in sample order.
 void launch_path_fold(const FrameParams& P, const PathState& S, cudaStream_t st);
 // Diagnostic comparison of the two 4-wide traversal forms (sphere scenes).

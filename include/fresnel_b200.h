@@ -188,7 +188,9 @@ FR_API fr_status fr_device_timer_stop(fr_device* dev, float* ms);
  *   "grid_density"  grid cells per sphere (default 1.5; (0, 64])
  *   "fuse_shade"    1 (default): the primary pass also shades each primary hit and queues the
  *                   continuing paths itself (the first shade pass of a wavefront is not
- *                   launched); 0: separate passes.  The same images either way.
+ *                   launched), and for scenes traced through a sphere grid each bounce traces
+ *                   and shades in one kernel; 2: bounces fused for every scene; 0: separate
+ *                   passes.  The same images in every case.
  * Setting an option marks every BVH of the device's scenes for rebuild when it changes the
  * tree.  Unknown names or out-of-range values return FR_ERR_INVALID. */
 FR_API fr_status fr_device_set_option(fr_device* dev, const char* name, double value);

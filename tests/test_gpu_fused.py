@@ -1,0 +1,43 @@
+"""Shading fused into the tracing passes (device option "fuse_shade") gives the same images as
+separate passes: every slot does the same arithmetic on the same values, only in another
+kernel, so the linear outputs must be identical.  Covers several light samples per pixel sample
+(later light samples restart from the stored primary ray), the sphere grid, the BVH of one
+geometry and the combined BVH of a mixed scene."""
+
+import numpy
+import pytest
+
+import fresnel_b200 as fresnel
+from fresnel_b200 import workloads
+
+pytestmark = pytest.mark.gpu
+
+SCENES = {
+    "spheres_1k_32ls": (workloads.config1, 96, 96, 3, 8),
+    "dense_grid": (lambda d: workloads.config2(d, n=20000, box=140.0 * 0.02**(1 / 3)), 120, 68,
+                   6, 1),
+    "mixed": (lambda d: workloads.config3(d, scale=0.002), 96, 54, 4, 2),
+}
+
+
+@pytest.mark.parametrize("name", list(SCENES))
+def test_fused_passes_give_identical_images(name, gpu_device):
+    build, w, h, spp, ls = SCENES[name]
+    dd = gpu_device._device
+    old = dd.getOption("fuse_shade")
+    out = []
+    try:
+        for fuse in (0, 1, 2):
+            dd.setOption("fuse_shade", fuse)
+            scene = build(gpu_device)
+            t = fresnel.tracer.Path(gpu_device, w=w, h=h)
+            t.seed = 3
+            t.sample(scene, samples=spp, light_samples=ls)
+            out.append((numpy.array(t.linear_output[:], copy=True),
+                        t._tracer.getStats()["rays"]))
+    finally:
+        dd.setOption("fuse_shade", old)
+    (a, ra), (b, rb), (c, rc) = out
+    assert numpy.isfinite(a).all() and numpy.count_nonzero(a[..., 3]) > 0
+    assert numpy.array_equal(a, b) and numpy.array_equal(a, c)
+    assert ra == rb == rc
