@@ -630,8 +630,12 @@ def main():
     else:
         primary_rays = float(wl.w * wl.h * wl.spp * args.steps)
         ext_rays = max(0.0, rays - primary_rays)
-        kern = {"k_path_primary": (primary_rays, st["primary_ms"], st["primary_launches"]),
-                "k_path_extend": (ext_rays, st["extend_ms"], st["extend_launches"])}
+        # with fused shading (device option fuse_shade) the primary kernel also shades, and
+        # without shade launches each bounce traces and shades in one kernel
+        primary_name = "k_path_primary_shade" if dd.getOption("fuse_shade") else "k_path_primary"
+        ext_name = "k_path_bounce" if st["shade_launches"] == 0 else "k_path_extend"
+        kern = {primary_name: (primary_rays, st["primary_ms"], st["primary_launches"]),
+                ext_name: (ext_rays, st["extend_ms"], st["extend_launches"])}
     dom = max(kern, key=lambda k: kern[k][1])
     dom_rays, dom_ms, launches = kern[dom]
     achieved = (dom_rays * wl.bytes_per_ray) / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else None
@@ -735,8 +739,8 @@ def main():
                                "primary_launches": st["primary_launches"],
                                "shade_launches": st["shade_launches"],
                                "extend_launches": st["extend_launches"],
-                               "primary_rays": kern["k_path_primary"][0],
-                               "extension_rays": kern["k_path_extend"][0]}
+                               "primary_rays": primary_rays, "extension_rays": ext_rays,
+                               "primary_kernel": primary_name, "extension_kernel": ext_name}
         print(json.dumps(line))
     reps.close()
     return 0
