@@ -2251,7 +2251,7 @@ fr_status fr_batch_render(fr_batch* b)
         wave_pixels.push_back(uint32_t(pixel));
     }
     if (all_grid && !jobs.empty())
-        mask = MASK_GRID;
+        mask = dev->fuse_shade ? MASK_GRID_FUSED : MASK_GRID;
     wave_first.push_back(uint32_t(jobs.size()));
     if (mask == 0)
         mask = MASK_SPHERES;  // empty scenes: every ray misses

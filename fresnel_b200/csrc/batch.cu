@@ -158,12 +158,90 @@ __global__ void __launch_bounds__(256) k_batch_extend(BatchDev B, int q)
     flush_counts(tc, &B.ctl->box_tests);
 }
 
-__global__ void k_inner_cond(BatchDev B, cudaGraphConditionalHandle inner)
+// Primary rays of the wave shaded at once (k_path_primary_shade), continuing paths into queue 0.
+template <int WIDTH, uint32_t MASK>
+__global__ void __launch_bounds__(256, 3) k_batch_primary_shade(BatchDev B)
+{
+    const PathState& S = B.S;
+    const uint32_t w = B.ctl->wave;
+    const uint32_t f0 = B.wave_first[w], f1 = B.wave_first[w + 1];
+    const uint32_t n_items = B.wave_items[w];
+    TraceCount tc;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g - lane_id() < n_items;
+         g += stride) {
+        const WaveJob& J = B.jobs[find_job<&WaveJob::item_base>(B.jobs, f0, f1, g)];
+        const FrameParams& P = J.P;
+        const PrimaryItem it = primary_item(g - J.item_base, P.w, P.h, P.batch, P.tile_log2);
+        bool push = false;
+        uint32_t slot = 0;
+        if (it.valid) {
+            slot = J.slot_base + (g - J.item_base);
+            push = primary_shade<WIDTH, MASK>(P, S, it, slot, tc);
+        }
+        push_queue(S, 0, push, slot);
+        const uint32_t mv = __ballot_sync(0xffffffffu, it.valid);
+        if (lane_id() == 0 && mv) {
+            atomicAdd(P.stats + 0, (unsigned long long)__popc(mv));
+            atomicAdd(P.stats + 1, (unsigned long long)__popc(mv) * P.light_samples);
+        }
+    }
+    flush_counts(tc, &B.ctl->box_tests);
+}
+
+// One bounce of the wave (k_path_bounce): the rays of queue q traced and shaded, continuing paths
+// into queue q ^ 1, whose length and the work counter are cleared before the launch.
+template <int WIDTH, uint32_t MASK>
+__global__ void __launch_bounds__(256, 3) k_batch_bounce(BatchDev B, int q)
+{
+    const PathState& S = B.S;
+    const uint32_t w = B.ctl->wave;
+    const uint32_t f0 = B.wave_first[w], f1 = B.wave_first[w + 1];
+    const uint32_t count = S.ctr[q];
+    const uint32_t* queue = S.queue[q];
+    const uint32_t lane = threadIdx.x & 31u;
+    TraceCount tc;
+    while (true) {
+        uint32_t base = 0;
+        if (lane == 0)
+            base = atomicAdd(S.ctr + 2, 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= count)
+            break;
+        const uint32_t idx = base + lane;
+        const bool act = idx < count;
+        uint32_t jb = 0, p = 0;
+        bool push = false;
+        if (act) {
+            p = queue[idx];
+            jb = find_job<&WaveJob::slot_base>(B.jobs, f0, f1, p);
+            push = bounce<WIDTH, MASK>(B.jobs[jb].P, S, p, p - B.jobs[jb].slot_base, tc);
+        }
+        push_queue(S, q ^ 1, push, p);
+        // rays per render, one atomic per render present in the warp
+        const uint32_t am = __ballot_sync(0xffffffffu, act);
+        if (act) {
+            const uint32_t same = __match_any_sync(am, jb);
+            if (lane == uint32_t(__ffs(same) - 1))
+                atomicAdd(B.jobs[jb].P.stats + 0, (unsigned long long)__popc(same));
+        }
+    }
+    flush_counts(tc, &B.ctl->box_tests);
+}
+
+// Before a fused bounce: the output queue q and the work counter start at zero.
+__global__ void k_clear_queue(BatchDev B, int q)
+{
+    B.S.ctr[q] = 0;
+    B.S.ctr[2] = 0;
+}
+
+__global__ void k_inner_cond(BatchDev B, cudaGraphConditionalHandle inner, int q_next)
 {
     BatchCtl* c = B.ctl;
     c->inner += 1u;
     c->pairs += 1u;
-    bool more = B.S.ctr[1] != 0u;
+    bool more = B.S.ctr[q_next] != 0u;
     if (more && c->inner >= BATCH_MAX_PAIRS) {
         c->error = 1u;
         more = false;
@@ -251,12 +329,16 @@ cudaGraph_t capturing_graph(cudaStream_t s)
     return graph;
 }
 
-template <int WIDTH, uint32_t MASK>
+// FUSED: shading folded into the tracing kernels (k_batch_primary_shade, k_batch_bounce), as the
+// single-render path does for sphere-grid scenes.
+template <int WIDTH, uint32_t MASK, bool FUSED = false>
 cudaError_t capture(const BatchDev& B, int num_sms, cudaStream_t s0, cudaGraphExec_t* exec)
 {
     using KS = Kernels<WIDTH, MASK>;
-    const int g_primary = KS::primary_grid(num_sms);
-    const int g_extend = KS::extend_grid(num_sms);
+    const int g_primary = FUSED ? grid_for(k_batch_primary_shade<WIDTH, MASK>, num_sms, 256)
+                                : KS::primary_grid(num_sms);
+    const int g_extend = FUSED ? grid_for(k_batch_bounce<WIDTH, MASK>, num_sms, 256)
+                               : KS::extend_grid(num_sms);
     const int g_shade = grid_for(k_batch_shade, num_sms, 256);
     const int g_fold = num_sms * 8;
 
@@ -286,18 +368,31 @@ cudaError_t capture(const BatchDev& B, int num_sms, cudaStream_t s0, cudaGraphEx
                                                        cudaStreamCaptureModeRelaxed))) {
                     c1 = true;
                     k_wave_begin<<<1, 1, 0, s1>>>(B, h_inner);
-                    KS::primary(B, g_primary, s1);
+                    if (FUSED)
+                        k_batch_primary_shade<WIDTH, MASK><<<g_primary, 256, 0, s1>>>(B);
+                    else
+                        KS::primary(B, g_primary, s1);
                     if (keep(cudaGetLastError()) && keep(add_while(s1, h_inner, &inner_body)) &&
                         keep(cudaStreamBeginCaptureToGraph(s2, inner_body, nullptr, nullptr, 0,
                                                            cudaStreamCaptureModeRelaxed))) {
                         c2 = true;
-                        // two iterations per pass: queue 1 -> 0, then 0 -> 1 (the primary
-                        // kernel fills queue 1)
-                        k_batch_shade<<<g_shade, 256, 0, s2>>>(B, 1, 0);
-                        KS::extend(B, 0, g_extend, s2);
-                        k_batch_shade<<<g_shade, 256, 0, s2>>>(B, 0, 1);
-                        KS::extend(B, 1, g_extend, s2);
-                        k_inner_cond<<<1, 1, 0, s2>>>(B, h_inner);
+                        if (FUSED) {
+                            // two bounces per pass: queue 0 -> 1, then 1 -> 0 (the fused
+                            // primary kernel fills queue 0)
+                            k_clear_queue<<<1, 1, 0, s2>>>(B, 1);
+                            k_batch_bounce<WIDTH, MASK><<<g_extend, 256, 0, s2>>>(B, 0);
+                            k_clear_queue<<<1, 1, 0, s2>>>(B, 0);
+                            k_batch_bounce<WIDTH, MASK><<<g_extend, 256, 0, s2>>>(B, 1);
+                            k_inner_cond<<<1, 1, 0, s2>>>(B, h_inner, 0);
+                        } else {
+                            // two iterations per pass: queue 1 -> 0, then 0 -> 1 (the primary
+                            // kernel fills queue 1)
+                            k_batch_shade<<<g_shade, 256, 0, s2>>>(B, 1, 0);
+                            KS::extend(B, 0, g_extend, s2);
+                            k_batch_shade<<<g_shade, 256, 0, s2>>>(B, 0, 1);
+                            KS::extend(B, 1, g_extend, s2);
+                            k_inner_cond<<<1, 1, 0, s2>>>(B, h_inner, 1);
+                        }
                         keep(cudaGetLastError());
                     }
                     if (c2) {
@@ -333,6 +428,8 @@ cudaError_t capture(const BatchDev& B, int num_sms, cudaStream_t s0, cudaGraphEx
 cudaError_t batch_graph_create(const BatchDev& B, int width, uint32_t type_mask, int num_sms,
                                cudaStream_t capture_stream, cudaGraphExec_t* exec)
 {
+    if (type_mask == MASK_GRID_FUSED)  // every render traces a sphere grid, shading fused
+        return capture<4, MASK_GRID, true>(B, num_sms, capture_stream, exec);
     if (type_mask == MASK_GRID)  // every render of the batch traces a sphere grid
         return capture<4, MASK_GRID>(B, num_sms, capture_stream, exec);
     const bool spheres_only = (type_mask & ~MASK_SPHERES) == 0u;

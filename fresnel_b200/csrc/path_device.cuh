@@ -248,16 +248,17 @@ __device__ __forceinline__ bool primary_shade(const FrameParams& P, const PathSt
 }
 
 // Extension ray of slot p traced and its hit shaded at once (a bounce): the path state is read as
-// the shade pass reads it, with the ray and the hit from registers.  Returns true when the path
-// continues (its next extension ray is stored; queue it).
+// the shade pass reads it, with the ray and the hit from registers.  local numbers the slot
+// within its render (as for shade_pixel).  Returns true when the path continues (its next
+// extension ray is stored; queue it).
 template <int WIDTH, uint32_t MASK>
 __device__ __forceinline__ bool bounce(const FrameParams& P, const PathState& S, uint32_t p,
-                                       TraceCount& tc)
+                                       uint32_t local, TraceCount& tc)
 {
     const V3 o = xyz(S.ray_o[p]);
     const V3 d = xyz(S.ray_d[p]);
     const Hit hit = trace_closest<WIDTH, MASK>(P.scene, o, d, PATH_TNEAR, tc);
-    const PrimaryItem pi = primary_item(p, P.w, P.h, P.batch, P.tile_log2);
+    const PrimaryItem pi = primary_item(local, P.w, P.h, P.batch, P.tile_log2);
     const uint2 ld = S.ls_depth[p];
     PathS s;
     s.depth = ld.y;

@@ -388,7 +388,7 @@ __global__ void __launch_bounds__(256, 3) k_path_bounce(FrameParams P, PathState
         uint32_t p = 0;
         if (idx < count) {
             p = queue[idx];
-            push = bounce<WIDTH, MASK>(P, S, p, tc);
+            push = bounce<WIDTH, MASK>(P, S, p, p, tc);
         }
         push_queue(S, q ^ 1, push, p);
         if (lane == 0)
