@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(256) k_batch_extend(BatchDev B, int q)
 
 // Primary rays of the wave shaded at once (k_path_primary_shade), continuing paths into queue 0.
 template <int WIDTH, uint32_t MASK>
-__global__ void __launch_bounds__(256, 3) k_batch_primary_shade(BatchDev B)
+__global__ void __launch_bounds__(256, fused_blocks(MASK)) k_batch_primary_shade(BatchDev B)
 {
     const PathState& S = B.S;
     const uint32_t w = B.ctl->wave;
@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(256, 3) k_batch_primary_shade(BatchDev B)
 // One bounce of the wave (k_path_bounce): the rays of queue q traced and shaded, continuing paths
 // into queue q ^ 1, whose length and the work counter are cleared before the launch.
 template <int WIDTH, uint32_t MASK>
-__global__ void __launch_bounds__(256, 3) k_batch_bounce(BatchDev B, int q)
+__global__ void __launch_bounds__(256, fused_blocks(MASK)) k_batch_bounce(BatchDev B, int q)
 {
     const PathState& S = B.S;
     const uint32_t w = B.ctl->wave;

@@ -66,10 +66,10 @@ __global__ void __launch_bounds__(256) k_path_primary(FrameParams P, PathState S
 
 // Primary rays with their first shading (device option "fuse_shade"): one thread per work item
 // as k_path_primary; continuing paths go straight to the extension queue (queue 0), so the
-// frame's first shade pass is not launched.  Limited to 3 blocks of 256 threads per SM, as the
-// shade kernel.
+// frame's first shade pass is not launched.  Limited to fused_blocks<MASK> blocks of 256 threads
+// per SM.
 template <int WIDTH, uint32_t MASK>
-__global__ void __launch_bounds__(256, 3) k_path_primary_shade(FrameParams P, PathState S)
+__global__ void __launch_bounds__(256, fused_blocks(MASK)) k_path_primary_shade(FrameParams P, PathState S)
 {
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t n_items = primary_items(P.w, P.h, P.batch, P.tile_log2);
@@ -367,10 +367,10 @@ __global__ void __launch_bounds__(256) k_path_extend(FrameParams P, PathState S,
 
 // Extension rays traced and shaded at once (device option "fuse_shade"): the rays of queue q are
 // taken 32 per warp as in k_path_extend; the continuing paths go to queue q ^ 1, whose length
-// and the work counter (ctr[2]) must be zero at launch.  Limited to 3 blocks per SM, as the
-// shade kernel.
+// and the work counter (ctr[2]) must be zero at launch.  Limited to fused_blocks<MASK> blocks per
+// SM.
 template <int WIDTH, uint32_t MASK>
-__global__ void __launch_bounds__(256, 3) k_path_bounce(FrameParams P, PathState S, int q)
+__global__ void __launch_bounds__(256, fused_blocks(MASK)) k_path_bounce(FrameParams P, PathState S, int q)
 {
     const uint32_t count = S.ctr[q];
     const uint32_t* queue = S.queue[q];
@@ -649,7 +649,8 @@ LaunchShape path_launch_shape(int num_sms)
     s.extend_grid[2] = num_sms * blocks_per_sm(k_path_extend<4, MASK_SPHERES>);
     s.extend_grid[3] = num_sms * blocks_per_sm(k_path_extend<4, MASK_ALL>);
     s.extend_grid_sphere_grid = num_sms * blocks_per_sm(k_path_extend<4, MASK_GRID>);
-    s.bounce_grid = num_sms * 3;  // k_path_bounce is compiled for 3 blocks per SM
+    s.bounce_grid[0] = num_sms * fused_blocks(MASK_ALL);
+    s.bounce_grid[1] = num_sms * fused_blocks(MASK_GRID);
     s.persistent_grid[0] = num_sms * blocks_per_sm(k_path_extend_persistent<MASK_SPHERES>);
     s.persistent_grid[1] = num_sms * blocks_per_sm(k_path_extend_persistent<MASK_ALL>);
     s.primary_grid[0] = num_sms * blocks_per_sm(k_path_primary_persistent<MASK_SPHERES>);
@@ -744,9 +745,10 @@ void launch_path_bounce(const FrameParams& P, const PathState& S, int iteration,
     const int q = iteration & 1;
     auto k = pick(P, k_path_bounce<2, MASK_SPHERES>, k_path_bounce<2, MASK_ALL>,
                   k_path_bounce<4, MASK_SPHERES>, k_path_bounce<4, MASK_ALL>);
-    if (P.scene.grid.n_cells != 0)
+    const bool grid = P.scene.grid.n_cells != 0;
+    if (grid)
         k = k_path_bounce<4, MASK_GRID>;
-    k<<<shape.bounce_grid, 256, 0, st>>>(P, S, q);
+    k<<<shape.bounce_grid[grid ? 1 : 0], 256, 0, st>>>(P, S, q);
 }
 
 void launch_histogram(const float4* linear, uint32_t n, uint32_t* counts, int num_sms,
