@@ -132,6 +132,11 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # nvidia-smi takes a moment to start: the timed region begins after its first sample
+            t_end = time.monotonic() + 5.0
+            while not self.samples and self.proc.poll() is None and time.monotonic() < t_end:
+                time.sleep(0.02)
+            self.samples.clear()
         except Exception:
             self.proc = None
         return self
@@ -144,6 +149,10 @@ class ClockSampler:
 
     def __exit__(self, *a):
         if self.proc is not None:
+            # a timed region shorter than the sampling period still gets the sample after it
+            t_end = time.monotonic() + 1.0
+            while not self.samples and self.proc.poll() is None and time.monotonic() < t_end:
+                time.sleep(0.02)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)

@@ -97,35 +97,38 @@ __device__ __forceinline__ float4 welford(const FrameParams& P, float4 old, floa
 // either store the continuing path (returns true: it needs another closest hit) or restart the
 // next light sample from the cached primary hit, or store the finished pixel sample (returns
 // false).  FIRST_IN_REGS: the first vertex's ray (ro0, rd0) and hit (h0) come from the
-// caller's registers instead of the path state.
+// caller's registers instead of the path state.  A light sample that ends at the primary vertex
+// (an outline or solid hit, a killed or terminated path) hands the next one the same ray, hit
+// and surface: those are kept in registers, not reloaded and recomputed.
 template <bool FIRST_IN_REGS>
 __device__ __forceinline__ bool shade_core(const FrameParams& P, const PathState& S, uint32_t p,
                                            uint32_t pixel, uint32_t n_samples, uint32_t ls,
                                            PathS s, uint2 ph, V3 ro0, V3 rd0, uint2 h0)
 {
     const uint32_t key1 = P.cam.seed;
-    bool first = FIRST_IN_REGS;
+    V3 ro, rd;
+    uint2 h;
+    if (FIRST_IN_REGS) {
+        ro = ro0;
+        rd = rd0;
+        h = h0;
+    } else if (s.depth == 0) {
+        ro = xyz(S.prim_o[p]);
+        rd = xyz(S.prim_d[p]);
+        h = ph;
+    } else {
+        ro = xyz(S.ray_o[p]);
+        rd = xyz(S.ray_d[p]);
+        h = S.hit[p];
+    }
+    Surface sf;
+    bool have_sf = false;  // sf holds the surface of (ro, rd, h)
     while (true) {
-        V3 ro, rd;
-        uint2 h;
-        if (FIRST_IN_REGS && first) {
-            ro = ro0;
-            rd = rd0;
-            h = h0;
-            first = false;
-        } else if (s.depth == 0) {
-            ro = xyz(S.prim_o[p]);
-            rd = xyz(S.prim_d[p]);
-            h = ph;
-        } else {
-            ro = xyz(S.ray_o[p]);
-            rd = xyz(S.ray_d[p]);
-            h = S.hit[p];
-        }
         s.done = false;
         if (h.x != MISS) {
             const GeomDev& g = P.scene.geoms[h.x];
-            Surface sf = hit_surface(g, h.y, ro, rd, PATH_TNEAR);
+            if (!have_sf)
+                sf = hit_surface(g, h.y, ro, rd, PATH_TNEAR);
             uint32_t sample = (n_samples - 1u) * P.light_samples + ls;
             path_hit(s, g.material, g.outline, sf.d_edge, g.outline_width, sf.color, sf.Ng, ro, rd,
                      sf.t, pixel, key1, sample);
@@ -147,6 +150,14 @@ __device__ __forceinline__ bool shade_core(const FrameParams& P, const PathState
         }
         if (ls + 1u < P.light_samples) {
             ++ls;
+            if (s.depth == 0) {  // the next light sample starts from this same vertex
+                have_sf = true;
+            } else {
+                ro = xyz(S.prim_o[p]);
+                rd = xyz(S.prim_d[p]);
+                h = ph;
+                have_sf = false;
+            }
             s.depth = 0;
             s.att = c3(1.0f, 1.0f, 1.0f);
             continue;
