@@ -92,106 +92,138 @@ __device__ __forceinline__ float4 welford(const FrameParams& P, float4 old, floa
     return make_float4(nr, ng, nb, na);
 }
 
-// The shading loop of one slot from its current state (TracerPath's hit/miss programs,
-// fresnel/common/TracerPathMethods.h:36-168, light samples in order): shade the vertex, then
-// either store the continuing path (returns true: it needs another closest hit) or restart the
-// next light sample from the cached primary hit, or store the finished pixel sample (returns
-// false).  FIRST_IN_REGS: the first vertex's ray (ro0, rd0) and hit (h0) come from the
-// caller's registers instead of the path state.  A light sample that ends at the primary vertex
-// (an outline or solid hit, a killed or terminated path) hands the next one the same ray, hit
-// and surface: those are kept in registers, not reloaded and recomputed.
-template <bool FIRST_IN_REGS>
-__device__ __forceinline__ bool shade_core(const FrameParams& P, const PathState& S, uint32_t p,
-                                           uint32_t pixel, uint32_t n_samples, uint32_t ls,
-                                           PathS s, uint2 ph, V3 ro0, V3 rd0, uint2 h0)
-{
-    const uint32_t key1 = P.cam.seed;
-    V3 ro, rd;
-    uint2 h;
-    if (FIRST_IN_REGS) {
-        ro = ro0;
-        rd = rd0;
-        h = h0;
-    } else if (s.depth == 0) {
-        ro = xyz(S.prim_o[p]);
-        rd = xyz(S.prim_d[p]);
-        h = ph;
-    } else {
-        ro = xyz(S.ray_o[p]);
-        rd = xyz(S.ray_d[p]);
-        h = S.hit[p];
-    }
+// One slot being shaded: its path state in registers, with the vertex to shade next (the ray
+// ro, rd and its hit h).  sf caches the surface of that vertex once computed (have_sf): a light
+// sample that ends at the primary vertex (an outline or solid hit, a killed or terminated path)
+// hands the next one the same ray, hit and surface, which are then neither reloaded nor
+// recomputed.
+struct ShadeLane {
+    uint32_t p;          // path-state slot
+    uint32_t pixel;      // j * w + i
+    uint32_t n_samples;  // 1-based sample number of the slot's pixel sample
+    uint32_t ls;         // light sample
+    PathS s;
+    uint2 ph;            // primary hit
+    uint2 h;             // hit of the vertex to shade
+    V3 ro, rd;           // its ray
     Surface sf;
-    bool have_sf = false;  // sf holds the surface of (ro, rd, h)
-    while (true) {
-        s.done = false;
-        if (h.x != MISS) {
-            const GeomDev& g = P.scene.geoms[h.x];
-            if (!have_sf)
-                sf = hit_surface(g, h.y, ro, rd, PATH_TNEAR);
-            uint32_t sample = (n_samples - 1u) * P.light_samples + ls;
-            path_hit(s, g.material, g.outline, sf.d_edge, g.outline_width, sf.color, sf.Ng, ro, rd,
-                     sf.t, pixel, key1, sample);
-        } else if (s.depth == 0) {
-            // a primary miss shows the background (fresnel/common/TracerPathMethods.h:44-50)
-            s.result = P.bg * float(P.light_samples);
-            s.done = true;
+    bool have_sf;
+};
+
+// Outcome of one shade_step.
+enum ShadeStep : int {
+    STEP_CONTINUE = 0,  // the path continues: its extension ray is stored, queue the slot
+    STEP_FINISHED = 1,  // the pixel sample is stored in S.sample
+    STEP_RESTART = 2    // the light sample ended; the lane now holds the next one's first vertex
+};
+
+// The lane state of slot p from the path state (the shade pass's view of a queued slot); local
+// numbers the slot within its render (equal to p for a single render, p minus the render's
+// first slot in a batch of renders).  A fresh primary hit, (light sample, depth) = (0, 0), has
+// throughput 1 and radiance 0, which are not stored.
+__device__ __forceinline__ void shade_load(const FrameParams& P, const PathState& S, uint32_t p,
+                                           uint32_t local, ShadeLane& L)
+{
+    const PrimaryItem pi = primary_item(local, P.w, P.h, P.batch, P.tile_log2);
+    L.p = p;
+    L.pixel = pi.j * P.w + pi.i;
+    L.n_samples = P.n_samples + pi.k;
+    const uint2 ld = S.ls_depth[p];
+    L.ls = ld.x;
+    L.s.depth = ld.y;
+    if (ld.x == 0u && ld.y == 0u) {
+        L.s.result = c3(0.0f, 0.0f, 0.0f);
+        L.s.att = c3(1.0f, 1.0f, 1.0f);
+    } else {
+        L.s.result = rgb3(S.result[p]);
+        L.s.att = rgb3(S.att[p]);
+    }
+    L.s.origin = v3(0, 0, 0);
+    L.s.dir = v3(0, 0, 0);
+    L.ph = S.prim_hit[p];
+    if (ld.y == 0u) {
+        L.ro = xyz(S.prim_o[p]);
+        L.rd = xyz(S.prim_d[p]);
+        L.h = L.ph;
+    } else {
+        L.ro = xyz(S.ray_o[p]);
+        L.rd = xyz(S.ray_d[p]);
+        L.h = S.hit[p];
+    }
+    L.have_sf = false;
+}
+
+// Shade the lane's current vertex (TracerPath's hit/miss programs,
+// fresnel/common/TracerPathMethods.h:36-168, light samples in order), then store the continuing
+// path, or move to the next light sample from the cached primary hit, or store the finished
+// pixel sample (fresnel/cpu/TracerPath.cc:228: radiance / L, alpha).
+__device__ __forceinline__ ShadeStep shade_step(const FrameParams& P, const PathState& S,
+                                                ShadeLane& L)
+{
+    PathS& s = L.s;
+    s.done = false;
+    if (L.h.x != MISS) {
+        const GeomDev& g = P.scene.geoms[L.h.x];
+        if (!L.have_sf)
+            L.sf = hit_surface(g, L.h.y, L.ro, L.rd, PATH_TNEAR);
+        const uint32_t sample = (L.n_samples - 1u) * P.light_samples + L.ls;
+        path_hit(s, g.material, g.outline, L.sf.d_edge, g.outline_width, L.sf.color, L.sf.Ng,
+                 L.ro, L.rd, L.sf.t, L.pixel, P.cam.seed, sample);
+    } else if (s.depth == 0) {
+        // a primary miss shows the background (fresnel/common/TracerPathMethods.h:44-50)
+        s.result = P.bg * float(P.light_samples);
+        s.done = true;
+    } else {
+        path_miss_lights(s, P.lights, L.rd);
+    }
+    const uint32_t p = L.p;
+    if (!s.done) {
+        s.depth += 1u;
+        S.ray_o[p] = f4(s.origin);
+        S.ray_d[p] = f4(s.dir);
+        S.att[p] = f4(s.att);
+        S.result[p] = f4(s.result);
+        S.ls_depth[p] = make_uint2(L.ls, s.depth);
+        return STEP_CONTINUE;
+    }
+    if (L.ls + 1u < P.light_samples) {
+        ++L.ls;
+        if (s.depth == 0) {  // the next light sample starts from this same vertex
+            L.have_sf = true;
         } else {
-            path_miss_lights(s, P.lights, rd);
+            L.ro = xyz(S.prim_o[p]);
+            L.rd = xyz(S.prim_d[p]);
+            L.h = L.ph;
+            L.have_sf = false;
         }
-        if (!s.done) {
-            s.depth += 1u;
-            S.ray_o[p] = f4(s.origin);
-            S.ray_d[p] = f4(s.dir);
-            S.att[p] = f4(s.att);
-            S.result[p] = f4(s.result);
-            S.ls_depth[p] = make_uint2(ls, s.depth);
-            return true;
-        }
-        if (ls + 1u < P.light_samples) {
-            ++ls;
-            if (s.depth == 0) {  // the next light sample starts from this same vertex
-                have_sf = true;
-            } else {
-                ro = xyz(S.prim_o[p]);
-                rd = xyz(S.prim_d[p]);
-                h = ph;
-                have_sf = false;
-            }
-            s.depth = 0;
-            s.att = c3(1.0f, 1.0f, 1.0f);
-            continue;
-        }
-        // the pixel sample (fresnel/cpu/TracerPath.cc:228): radiance / L, alpha
-        C3 out = c_div_recip(s.result, float(P.light_samples));
-        S.sample[p] = make_float4(out.r, out.g, out.b, ph.x == MISS ? P.bg_alpha : 1.0f);
-        return false;
+        s.depth = 0;
+        s.att = c3(1.0f, 1.0f, 1.0f);
+        return STEP_RESTART;
+    }
+    C3 out = c_div_recip(s.result, float(P.light_samples));
+    S.sample[p] = make_float4(out.r, out.g, out.b, L.ph.x == MISS ? P.bg_alpha : 1.0f);
+    return STEP_FINISHED;
+}
+
+// Shade a lane until its path needs another closest hit (returns true) or its pixel sample is
+// finished (returns false).
+__device__ __forceinline__ bool shade_run(const FrameParams& P, const PathState& S, ShadeLane& L)
+{
+    while (true) {
+        const ShadeStep r = shade_step(P, S, L);
+        if (r != STEP_RESTART)
+            return r == STEP_CONTINUE;
     }
 }
 
 // Shade the current path vertex of one slot; returns true if the path needs another closest hit.
-// p indexes the path state; local = k * w * h + pixel numbers the slot within its render (equal
-// to p for a single render, p minus the render's first slot in a batch of renders).
+// p indexes the path state; local = k * w * h + pixel numbers the slot within its render.
 __device__ __forceinline__ bool shade_pixel(const FrameParams& P, const PathState& S, uint32_t p,
                                             uint32_t local)
 {
-    const PrimaryItem pi = primary_item(local, P.w, P.h, P.batch, P.tile_log2);
-    const uint32_t pixel = pi.j * P.w + pi.i;
-    const uint32_t n_samples = P.n_samples + pi.k;
-    const uint2 ld = S.ls_depth[p];
-    PathS s;
-    s.depth = ld.y;
-    if (ld.x == 0u && s.depth == 0u) {  // a fresh primary hit (primary_finish)
-        s.result = c3(0.0f, 0.0f, 0.0f);
-        s.att = c3(1.0f, 1.0f, 1.0f);
-    } else {
-        s.result = rgb3(S.result[p]);
-        s.att = rgb3(S.att[p]);
-    }
-    s.origin = v3(0, 0, 0);
-    s.dir = v3(0, 0, 0);
-    return shade_core<false>(P, S, p, pixel, n_samples, ld.x, s, S.prim_hit[p], v3(0, 0, 0),
-                             v3(0, 0, 0), make_uint2(0u, 0u));
+    ShadeLane L;
+    shade_load(P, S, p, local, L);
+    return shade_run(P, S, L);
 }
 
 // Primary ray of one item: closest hit; a miss finishes its pixel sample (every light sample
@@ -248,14 +280,22 @@ __device__ __forceinline__ bool primary_shade(const FrameParams& P, const PathSt
         S.prim_o[slot] = f4(o);
         S.prim_d[slot] = f4(d);
     }
-    PathS s;
-    s.result = c3(0.0f, 0.0f, 0.0f);
-    s.att = c3(1.0f, 1.0f, 1.0f);
-    s.depth = 0;
-    s.origin = v3(0, 0, 0);
-    s.dir = v3(0, 0, 0);
-    return shade_core<true>(P, S, slot, it.j * P.w + it.i, P.n_samples + it.k, 0u, s, ph, o, d,
-                            ph);
+    ShadeLane L;
+    L.p = slot;
+    L.pixel = it.j * P.w + it.i;
+    L.n_samples = P.n_samples + it.k;
+    L.ls = 0;
+    L.s.result = c3(0.0f, 0.0f, 0.0f);
+    L.s.att = c3(1.0f, 1.0f, 1.0f);
+    L.s.depth = 0;
+    L.s.origin = v3(0, 0, 0);
+    L.s.dir = v3(0, 0, 0);
+    L.ph = ph;
+    L.h = ph;
+    L.ro = o;
+    L.rd = d;
+    L.have_sf = false;
+    return shade_run(P, S, L);
 }
 
 // Extension ray of slot p traced and its hit shaded at once (a bounce): the path state is read as
@@ -271,14 +311,22 @@ __device__ __forceinline__ bool bounce(const FrameParams& P, const PathState& S,
     const Hit hit = trace_closest<WIDTH, MASK>(P.scene, o, d, PATH_TNEAR, tc);
     const PrimaryItem pi = primary_item(local, P.w, P.h, P.batch, P.tile_log2);
     const uint2 ld = S.ls_depth[p];
-    PathS s;
-    s.depth = ld.y;
-    s.result = rgb3(S.result[p]);
-    s.att = rgb3(S.att[p]);
-    s.origin = v3(0, 0, 0);
-    s.dir = v3(0, 0, 0);
-    return shade_core<true>(P, S, p, pi.j * P.w + pi.i, P.n_samples + pi.k, ld.x, s,
-                            S.prim_hit[p], o, d, make_uint2(hit.geom, hit.prim));
+    ShadeLane L;
+    L.p = p;
+    L.pixel = pi.j * P.w + pi.i;
+    L.n_samples = P.n_samples + pi.k;
+    L.ls = ld.x;
+    L.s.depth = ld.y;
+    L.s.result = rgb3(S.result[p]);
+    L.s.att = rgb3(S.att[p]);
+    L.s.origin = v3(0, 0, 0);
+    L.s.dir = v3(0, 0, 0);
+    L.ph = S.prim_hit[p];
+    L.h = make_uint2(hit.geom, hit.prim);
+    L.ro = o;
+    L.rd = d;
+    L.have_sf = false;
+    return shade_run(P, S, L);
 }
 
 // Append the lanes with push set to queue q (one atomic per warp).

@@ -299,6 +299,15 @@ __global__ void __launch_bounds__(256) k_histogram(const float4* linear, uint32_
             atomicAdd(counts + i, h[i]);
 }
 
+// Shade pass: the slots of queue in_q, continuing paths appended to queue out_q.  A slot's
+// light samples that end at the primary vertex are shaded one after another by the same lane, so
+// lanes finish their slots after different numbers of steps (up to the light-sample count); a
+// lane whose slot is done takes the next slot of its warp's share of the queue (groups of 32
+// slots, warp w owning groups w, w + n_warps, ...) while the others carry on, so the warp's lanes
+// stay busy until the share runs out.  The continuing slots are staged per warp in shared memory
+// and appended to out_q 32 at a time: the extension pass takes its rays 32 per warp in queue
+// order, and a run of one warp's slots (a few neighbouring pixel samples, whose rays start from
+// about the same point) traces more coherently than slots interleaved from many warps.
 template <int MINB = 1>
 __global__ void __launch_bounds__(256, MINB) k_path_shade(FrameParams P, PathState S, int in_q,
                                                           int out_q)
@@ -307,28 +316,70 @@ __global__ void __launch_bounds__(256, MINB) k_path_shade(FrameParams P, PathSta
         S.ctr[2] = 0;  // work counter of the extend kernel that follows
     const uint32_t count = S.ctr[in_q];
     const uint32_t* inq = S.queue[in_q];
-    uint32_t* outq = S.queue[out_q];
-    uint32_t* outc = S.ctr + out_q;
     const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t below = (1u << lane) - 1u;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t base = warp * 32u; base < count; base += n_warps * 32u) {
-        uint32_t idx = base + lane;
-        bool push = false;
-        uint32_t p = 0;
-        if (idx < count) {
-            p = inq[idx];
-            push = shade_pixel(P, S, p, p);
+    __shared__ uint32_t stage[8][64];  // blocks of 256 threads: 8 warps
+    uint32_t* staged = stage[threadIdx.x >> 5];
+    uint32_t n_staged = 0;  // warp-uniform, below 32 between iterations
+    uint32_t* outq = S.queue[out_q];
+    uint32_t* outc = S.ctr + out_q;
+    uint32_t taken = 0;  // positions of the warp's share handed out so far (warp-uniform)
+    bool busy = false;
+    ShadeLane L;
+    L.p = 0;
+    while (true) {
+        const uint32_t idle = __ballot_sync(0xffffffffu, !busy);
+        if (idle) {
+            if (!busy) {
+                const uint32_t k = taken + __popc(idle & below);
+                const uint32_t idx = (warp + (k >> 5) * n_warps) * 32u + (k & 31u);
+                if (idx < count) {
+                    const uint32_t p = inq[idx];
+                    shade_load(P, S, p, p, L);
+                    busy = true;
+                }
+            }
+            taken += __popc(idle);
         }
-        uint32_t m = __ballot_sync(0xffffffffu, push);
-        if (m) {
+        if (!__any_sync(0xffffffffu, busy))
+            break;
+        bool push = false;
+        if (busy) {
+            const ShadeStep r = shade_step(P, S, L);
+            if (r != STEP_RESTART) {
+                busy = false;
+                push = r == STEP_CONTINUE;
+            }
+        }
+        const uint32_t m = __ballot_sync(0xffffffffu, push);
+        if (push)
+            staged[n_staged + __popc(m & below)] = L.p;
+        n_staged += __popc(m);
+        if (n_staged >= 32u) {
+            __syncwarp();
             uint32_t at = 0;
             if (lane == 0)
-                at = atomicAdd(outc, uint32_t(__popc(m)));
+                at = atomicAdd(outc, 32u);
             at = __shfl_sync(0xffffffffu, at, 0);
-            if (push)
-                outq[at + __popc(m & ((1u << lane) - 1u))] = p;
+            outq[at + lane] = staged[lane];
+            const uint32_t rest = staged[32u + lane];
+            __syncwarp();
+            n_staged -= 32u;
+            if (lane < n_staged)
+                staged[lane] = rest;
+            __syncwarp();
         }
+    }
+    if (n_staged) {
+        __syncwarp();
+        uint32_t at = 0;
+        if (lane == 0)
+            at = atomicAdd(outc, n_staged);
+        at = __shfl_sync(0xffffffffu, at, 0);
+        if (lane < n_staged)
+            outq[at + lane] = staged[lane];
     }
 }
 
