@@ -87,28 +87,19 @@ struct U4 {
     uint32_t x, y, z, w;
 };
 
-FR_HD uint32_t mulhi32(uint32_t a, uint32_t b)
-{
-#ifdef __CUDA_ARCH__
-    return __umulhi(a, b);
-#else
-    return uint32_t((uint64_t(a) * uint64_t(b)) >> 32);
-#endif
-}
-
 FR_HD U4 philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1)
 {
     const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
     const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
 #pragma unroll
     for (int round = 0; round < 10; ++round) {
-        uint32_t hi0 = mulhi32(M0, c0), lo0 = M0 * c0;
-        uint32_t hi1 = mulhi32(M1, c2), lo1 = M1 * c2;
-        uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        // one 32x32 -> 64-bit product per multiplier gives both halves
+        const uint64_t p0 = uint64_t(M0) * c0, p1 = uint64_t(M1) * c2;
+        uint32_t n0 = uint32_t(p1 >> 32) ^ c1 ^ k0, n2 = uint32_t(p0 >> 32) ^ c3 ^ k1;
         c0 = n0;
-        c1 = lo1;
+        c1 = uint32_t(p1);
         c2 = n2;
-        c3 = lo0;
+        c3 = uint32_t(p0);
         k0 += W0;
         k1 += W1;
     }
