@@ -815,7 +815,7 @@ FrameParams frame_params(fr_tracer* tr, fr_scene* sc, const fr_render_params* p,
     P.tile_log2 = sc->dev->tile_log2;
     P.shade_blocks = sc->dev->shade_blocks;
     P.packet = sc->use_grid ? 0 : sc->dev->packet;
-    P.refill = sc->use_grid ? 0 : sc->dev->refill;
+    P.refill = sc->dev->refill;
     tr->last_grid = sc->use_grid ? 1u : 0u;
     const fr_user_camera& c = p->camera;
     float f_stop = preview ? std::numeric_limits<float>::infinity() : c.f_stop;  // no depth of field in preview
@@ -1654,7 +1654,7 @@ fr_status fr_tracer_render_path(fr_tracer* t, fr_scene* sc, const fr_render_para
         // bounces fused too: by default for sphere-grid scenes only (a BVH walk in a kernel
         // compiled for 3 blocks per SM is slower than the separate passes)
         const bool bounces =
-            fused && (t->dev->fuse_shade == 2 || P.scene.grid.n_cells != 0);
+            fused && (t->dev->fuse_shade == 2 || (P.scene.grid.n_cells != 0 && !P.refill));
         while (true) {
             for (int b = 0; b < CHECK_EVERY; ++b, ++it) {
                 if (bounces) {

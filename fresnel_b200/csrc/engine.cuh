@@ -817,94 +817,129 @@ struct Hit {
 // recomputed from the plane positions at every step, so rounding does not accumulate.  The next
 // cell's reference range is loaded before this cell's spheres are tested, and spheres are
 // loaded two at a time, to shorten the chain of dependent loads (extension pass 5% faster).
-// slot receives the reference index of the hit (unchanged on a miss).
-__device__ __forceinline__ void trace_grid(const GridDev& G, const RayK& ray, float tnear,
-                                           float& tmax, uint32_t& slot, TraceCount& tc)
+//
+// The walk is split into grid_walk_begin (entry cell) and grid_walk_step (one cell), so that a
+// kernel can interleave the cells of different rays in one lane (per-lane refill).
+struct GridWalk {
+    int ix, iy, iz;         // current cell
+    float tnx, tny, tnz;    // distances to the planes the ray leaves it through, per axis
+    float t_out;            // distance at which the ray leaves the grid
+    uint32_t first, last;   // the current cell's reference range
+    uint32_t guard;         // cells left before the walk is cut (a bound, never reached)
+};
+
+__device__ __forceinline__ float grid_exit_t(int i, float inv, float lo, float h, float oinv)
+{
+    return fmaf(fmaf(float(i + (inv >= 0.0f ? 1 : 0)), h, lo), inv, oinv);
+}
+
+__device__ __forceinline__ uint32_t grid_cell_id(const GridDev& G, int x, int y, int z)
+{
+    return (uint32_t(z) * G.ny + uint32_t(y)) * G.nx + uint32_t(x);
+}
+
+// Sets up the walk of `ray`; false when the ray misses the grid (nothing to walk).
+__device__ __forceinline__ bool grid_walk_begin(const GridDev& G, const RayK& ray, GridWalk& W)
 {
     float tx0 = fmaf(G.lox, ray.inv.x, ray.oinv.x), tx1 = fmaf(G.hix, ray.inv.x, ray.oinv.x);
     float ty0 = fmaf(G.loy, ray.inv.y, ray.oinv.y), ty1 = fmaf(G.hiy, ray.inv.y, ray.oinv.y);
     float tz0 = fmaf(G.loz, ray.inv.z, ray.oinv.z), tz1 = fmaf(G.hiz, ray.inv.z, ray.oinv.z);
     const float t_in = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), 0.0f));
-    const float t_out = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fmaxf(tz0, tz1));
-    if (!(t_in <= t_out))
-        return;  // misses the grid (or NaN)
+    W.t_out = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fmaxf(tz0, tz1));
+    if (!(t_in <= W.t_out))
+        return false;  // misses the grid (or NaN)
     // the cell holding the entry point (clamped: the entry lies on the grid's surface)
     auto cell_of = [](float p, float lo, float ih, uint32_t n) {
         const float u = (p - lo) * ih;
         return u >= 0.0f ? int(fminf(u, float(n - 1u))) : 0;  // NaN compares false: cell 0
     };
-    int ix = cell_of(ray.o.x + t_in * ray.d.x, G.lox, G.ihx, G.nx);
-    int iy = cell_of(ray.o.y + t_in * ray.d.y, G.loy, G.ihy, G.ny);
-    int iz = cell_of(ray.o.z + t_in * ray.d.z, G.loz, G.ihz, G.nz);
+    W.ix = cell_of(ray.o.x + t_in * ray.d.x, G.lox, G.ihx, G.nx);
+    W.iy = cell_of(ray.o.y + t_in * ray.d.y, G.loy, G.ihy, G.ny);
+    W.iz = cell_of(ray.o.z + t_in * ray.d.z, G.loz, G.ihz, G.nz);
+    W.tnx = grid_exit_t(W.ix, ray.inv.x, G.lox, G.hx, ray.oinv.x);
+    W.tny = grid_exit_t(W.iy, ray.inv.y, G.loy, G.hy, ray.oinv.y);
+    W.tnz = grid_exit_t(W.iz, ray.inv.z, G.loz, G.hz, ray.oinv.z);
+    W.guard = G.nx + G.ny + G.nz + 3u;
+    const uint32_t c = grid_cell_id(G, W.ix, W.iy, W.iz);
+    W.first = __ldg(G.cell_start + c);
+    W.last = __ldg(G.cell_start + c + 1);
+    return true;
+}
+
+// Tests the spheres of the walk's current cell and moves to the next cell; false when the walk
+// is over (the closest hit lies before the cell's exit, or the ray leaves the grid).  slot
+// receives the reference index of a closer hit.
+__device__ __forceinline__ bool grid_walk_step(const GridDev& G, const RayK& ray, float tnear,
+                                               float& tmax, uint32_t& slot, GridWalk& W,
+                                               TraceCount& tc)
+{
+    // the next cell along the ray, and its reference range loaded now so that the load
+    // overlaps the sphere tests of this cell
     const int sx = ray.inv.x >= 0.0f ? 1 : -1;
     const int sy = ray.inv.y >= 0.0f ? 1 : -1;
     const int sz = ray.inv.z >= 0.0f ? 1 : -1;
-    // distance to the plane the ray leaves cell i through, along one axis
-    auto exit_t = [](int i, int s, float lo, float h, float inv, float oinv) {
-        return fmaf(fmaf(float(i + (s > 0 ? 1 : 0)), h, lo), inv, oinv);
-    };
-    float tnx = exit_t(ix, sx, G.lox, G.hx, ray.inv.x, ray.oinv.x);
-    float tny = exit_t(iy, sy, G.loy, G.hy, ray.inv.y, ray.oinv.y);
-    float tnz = exit_t(iz, sz, G.loz, G.hz, ray.inv.z, ray.oinv.z);
-    uint32_t guard = G.nx + G.ny + G.nz + 3u;
-    auto cell_id = [&](int x, int y, int z) {
-        return (uint32_t(z) * G.ny + uint32_t(y)) * G.nx + uint32_t(x);
-    };
-    uint32_t first = __ldg(G.cell_start + cell_id(ix, iy, iz));
-    uint32_t last = __ldg(G.cell_start + cell_id(ix, iy, iz) + 1);
-    while (true) {
-        // the next cell along the ray, and its reference range loaded now so that the load
-        // overlaps the sphere tests of this cell
-        const float t_cell = fminf(tnx, fminf(tny, tnz));
-        const int axis = (tnx <= tny && tnx <= tnz) ? 0 : (tny <= tnz ? 1 : 2);
-        const int nx = ix + (axis == 0 ? sx : 0), ny = iy + (axis == 1 ? sy : 0),
-                  nz = iz + (axis == 2 ? sz : 0);
-        const bool more = t_cell < t_out && nx >= 0 && nx < int(G.nx) && ny >= 0 &&
-                          ny < int(G.ny) && nz >= 0 && nz < int(G.nz);
-        uint32_t next_first = 0, next_last = 0;
-        if (more) {
-            const uint32_t nc = cell_id(nx, ny, nz);
-            next_first = __ldg(G.cell_start + nc);
-            next_last = __ldg(G.cell_start + nc + 1);
+    const float t_cell = fminf(W.tnx, fminf(W.tny, W.tnz));
+    const int axis = (W.tnx <= W.tny && W.tnx <= W.tnz) ? 0 : (W.tny <= W.tnz ? 1 : 2);
+    const int nx = W.ix + (axis == 0 ? sx : 0), ny = W.iy + (axis == 1 ? sy : 0),
+              nz = W.iz + (axis == 2 ? sz : 0);
+    const bool more = t_cell < W.t_out && nx >= 0 && nx < int(G.nx) && ny >= 0 &&
+                      ny < int(G.ny) && nz >= 0 && nz < int(G.nz);
+    uint32_t next_first = 0, next_last = 0;
+    if (more) {
+        const uint32_t nc = grid_cell_id(G, nx, ny, nz);
+        next_first = __ldg(G.cell_start + nc);
+        next_last = __ldg(G.cell_start + nc + 1);
+    }
+    const uint32_t last = W.last;
+    tc.box += 1;
+    tc.prim += last - W.first;
+    uint32_t k = W.first;
+    for (; k + 1 < last; k += 2) {  // two spheres in flight
+        const float4 q0 = ldg4(G.ref_sphere + k), q1 = ldg4(G.ref_sphere + k + 1);
+        float t0, t1;
+        if (sphere_t(ray.o, ray.d, v3(q0.x, q0.y, q0.z), q0.w, t0) && (tnear < t0) &&
+            (t0 < tmax)) {
+            tmax = t0;
+            slot = k;
         }
-        tc.box += 1;
-        tc.prim += last - first;
-        uint32_t k = first;
-        for (; k + 1 < last; k += 2) {  // two spheres in flight
-            const float4 q0 = ldg4(G.ref_sphere + k), q1 = ldg4(G.ref_sphere + k + 1);
-            float t0, t1;
-            if (sphere_t(ray.o, ray.d, v3(q0.x, q0.y, q0.z), q0.w, t0) && (tnear < t0) &&
-                (t0 < tmax)) {
-                tmax = t0;
-                slot = k;
-            }
-            if (sphere_t(ray.o, ray.d, v3(q1.x, q1.y, q1.z), q1.w, t1) && (tnear < t1) &&
-                (t1 < tmax)) {
-                tmax = t1;
-                slot = k + 1;
-            }
+        if (sphere_t(ray.o, ray.d, v3(q1.x, q1.y, q1.z), q1.w, t1) && (tnear < t1) &&
+            (t1 < tmax)) {
+            tmax = t1;
+            slot = k + 1;
         }
-        if (k < last) {
-            const float4 q = ldg4(G.ref_sphere + k);
-            float t;
-            if (sphere_t(ray.o, ray.d, v3(q.x, q.y, q.z), q.w, t) && (tnear < t) && (t < tmax)) {
-                tmax = t;
-                slot = k;
-            }
+    }
+    if (k < last) {
+        const float4 q = ldg4(G.ref_sphere + k);
+        float t;
+        if (sphere_t(ray.o, ray.d, v3(q.x, q.y, q.z), q.w, t) && (tnear < t) && (t < tmax)) {
+            tmax = t;
+            slot = k;
         }
-        if (tmax <= t_cell || !more || --guard == 0u)
-            return;
-        ix = nx;
-        iy = ny;
-        iz = nz;
-        if (axis == 0)
-            tnx = exit_t(ix, sx, G.lox, G.hx, ray.inv.x, ray.oinv.x);
-        else if (axis == 1)
-            tny = exit_t(iy, sy, G.loy, G.hy, ray.inv.y, ray.oinv.y);
-        else
-            tnz = exit_t(iz, sz, G.loz, G.hz, ray.inv.z, ray.oinv.z);
-        first = next_first;
-        last = next_last;
+    }
+    if (tmax <= t_cell || !more || --W.guard == 0u)
+        return false;
+    W.ix = nx;
+    W.iy = ny;
+    W.iz = nz;
+    if (axis == 0)
+        W.tnx = grid_exit_t(W.ix, ray.inv.x, G.lox, G.hx, ray.oinv.x);
+    else if (axis == 1)
+        W.tny = grid_exit_t(W.iy, ray.inv.y, G.loy, G.hy, ray.oinv.y);
+    else
+        W.tnz = grid_exit_t(W.iz, ray.inv.z, G.loz, G.hz, ray.oinv.z);
+    W.first = next_first;
+    W.last = next_last;
+    return true;
+}
+
+// The whole walk of one ray.
+__device__ __forceinline__ void trace_grid(const GridDev& G, const RayK& ray, float tnear,
+                                           float& tmax, uint32_t& slot, TraceCount& tc)
+{
+    GridWalk W;
+    if (!grid_walk_begin(G, ray, W))
+        return;
+    while (grid_walk_step(G, ray, tnear, tmax, slot, W, tc)) {
     }
 }
 

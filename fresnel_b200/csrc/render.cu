@@ -558,6 +558,68 @@ __global__ void __launch_bounds__(256) k_path_extend_refill(FrameParams P, PathS
     flush_counts(tc, P.stats + 3);
 }
 
+// Extension rays through the sphere grid with per-lane refill (device option "refill"): a lane
+// walks one cell of its ray per iteration, and a lane whose walk is over stores the hit and
+// takes the next queued ray as soon as REFILL_MIN lanes of its warp are idle, so the warp is not
+// held by its longest walk.  The hits are shaded by the separate shade pass.
+__global__ void __launch_bounds__(256) k_path_extend_grid_refill(FrameParams P, PathState S, int q)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        S.ctr[q ^ 1] = 0;  // the other queue was consumed by the shade pass that produced q
+    const uint32_t count = S.ctr[q];
+    const uint32_t* queue = S.queue[q];
+    const uint32_t lane = lane_id();
+    const uint32_t below = (1u << lane) - 1u;
+    const GridDev& G = P.scene.grid;
+    TraceCount tc;
+    bool active = false, exhausted = false;
+    uint32_t p = 0, slot = MISS;
+    float tmax = 0.0f;
+    RayK ray;
+    GridWalk W;
+    unsigned long long rays = 0;
+    while (true) {
+        const uint32_t idle = __ballot_sync(0xffffffffu, !active);
+        if (!exhausted && (__popc(idle) >= int(REFILL_MIN) || idle == 0xffffffffu)) {
+            const uint32_t n = uint32_t(__popc(idle));
+            uint32_t base = 0;
+            if (lane == 0)
+                base = atomicAdd(S.ctr + 2, n);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (base + n >= count)
+                exhausted = true;
+            if (!active) {
+                const uint32_t item = base + uint32_t(__popc(idle & below));
+                if (item < count) {
+                    p = queue[item];
+                    ray = make_rayk(xyz(S.ray_o[p]), xyz(S.ray_d[p]));
+                    tmax = __int_as_float(0x7f800000);
+                    slot = MISS;
+                    active = grid_walk_begin(G, ray, W);
+                    if (!active)
+                        S.hit[p] = make_uint2(MISS, 0u);
+                    ++rays;
+                }
+            }
+        }
+        if (__ballot_sync(0xffffffffu, active) == 0u) {
+            if (exhausted)
+                break;
+            continue;
+        }
+        if (active && !grid_walk_step(G, ray, PATH_TNEAR, tmax, slot, W, tc)) {
+            S.hit[p] = slot == MISS ? make_uint2(MISS, 0u)
+                                    : make_uint2(G.geom, __ldg(G.ref_prim + slot));
+            active = false;
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1)
+        rays += __shfl_xor_sync(0xffffffffu, rays, off);
+    if (lane == 0 && rays)
+        atomicAdd(P.stats + 0, rays);
+    flush_counts(tc, P.stats + 3);
+}
+
 // Representative-point area-light shading of one preview sample
 // (fresnel/cpu/TracerDirect.cc:120-200).
 __device__ __forceinline__ C3 preview_shade(const FrameParams& P, const GeomDev& g,
@@ -700,6 +762,7 @@ LaunchShape path_launch_shape(int num_sms)
     s.extend_grid[2] = num_sms * blocks_per_sm(k_path_extend<4, MASK_SPHERES>);
     s.extend_grid[3] = num_sms * blocks_per_sm(k_path_extend<4, MASK_ALL>);
     s.extend_grid_sphere_grid = num_sms * blocks_per_sm(k_path_extend<4, MASK_GRID>);
+    s.refill_grid_sphere_grid = num_sms * blocks_per_sm(k_path_extend_grid_refill);
     s.bounce_grid[0] = num_sms * fused_blocks(MASK_ALL);
     s.bounce_grid[1] = num_sms * fused_blocks(MASK_GRID);
     s.persistent_grid[0] = num_sms * blocks_per_sm(k_path_extend_persistent<MASK_SPHERES>);
@@ -767,7 +830,10 @@ void launch_path_extend(const FrameParams& P, const PathState& S, int iteration,
     bool spheres_only = (P.type_mask & ~MASK_SPHERES) == 0u;
     int q = iteration & 1;
     if (P.scene.grid.n_cells != 0) {
-        k_path_extend<4, MASK_GRID><<<shape.extend_grid_sphere_grid, 256, 0, st>>>(P, S, q);
+        if (P.refill)
+            k_path_extend_grid_refill<<<shape.refill_grid_sphere_grid, 256, 0, st>>>(P, S, q);
+        else
+            k_path_extend<4, MASK_GRID><<<shape.extend_grid_sphere_grid, 256, 0, st>>>(P, S, q);
         return;
     }
     if (P.bvh_width == 4 && P.persistent) {

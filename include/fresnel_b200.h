@@ -171,7 +171,8 @@ FR_API fr_status fr_device_timer_stop(fr_device* dev, float* ms);
  *   "packet"        1: primary rays traced warp-cooperatively (one node sequence per warp, a
  *                   shared stack); 0: one ray per thread (default)
  *   "refill"        1: extension rays with per-lane refill (a warp's idle lanes take new rays
- *                   without waiting for its slowest ray; scenes with one tree); 0: default
+ *                   without waiting for its slowest ray; scenes with one tree, and sphere-grid
+ *                   scenes, whose bounces then trace and shade in separate passes); 0: default
  *   "combined"      1 (default): a scene of 2 to 8 enabled geometries gets one BVH over all
  *                   their primitives; 0: each geometry's own BVH, traversed in turn
  *   "shade_blocks"  3 (default) or 4: the shade kernel compiled to fit that many 256-thread

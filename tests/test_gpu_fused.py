@@ -41,3 +41,26 @@ def test_fused_passes_give_identical_images(name, gpu_device):
     assert numpy.isfinite(a).all() and numpy.count_nonzero(a[..., 3]) > 0
     assert numpy.array_equal(a, b) and numpy.array_equal(a, c)
     assert ra == rb == rc
+
+
+def test_grid_refill_extension_gives_identical_images(gpu_device):
+    """Device option "refill" on a sphere-grid scene: extension rays walk the grid with per-lane
+    refill and are shaded by the separate shade pass; the same arithmetic as the fused bounces."""
+    dd = gpu_device._device
+    old = dd.getOption("refill")
+    out = []
+    try:
+        for refill in (0, 1):
+            dd.setOption("refill", refill)
+            scene = workloads.config2(gpu_device, n=20000, box=140.0 * 0.02**(1 / 3))
+            t = fresnel.tracer.Path(gpu_device, w=120, h=68)
+            t.seed = 5
+            t.sample(scene, samples=6, light_samples=2)
+            out.append((numpy.array(t.linear_output[:], copy=True),
+                        t._tracer.getStats()["rays"]))
+    finally:
+        dd.setOption("refill", old)
+    (a, ra), (b, rb) = out
+    assert numpy.isfinite(a).all() and numpy.count_nonzero(a[..., 3]) > 0
+    assert numpy.array_equal(a, b)
+    assert ra == rb
