@@ -82,7 +82,9 @@ WORKLOADS = {
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=3)
+    # 10 frames of the default workload take about 0.8 s: enough for a few clock samples at
+    # nvidia-smi's 200 ms period inside the timed region
+    p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="engine", choices=["engine", "reference"])
     p.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
