@@ -14,8 +14,8 @@ except ImportError:  # pragma: no cover - PIL is optional
 
 # Whole-array copies of at least this many bytes between numpy and a mapped buffer are split
 # into row blocks copied on several threads (numpy releases the GIL while it copies): one core
-# copies about 10 GB/s, so a 1M-sphere scene's arrays (28 MB) or a 1080p image would otherwise
-# spend milliseconds in a single memcpy.
+# copies some 5-10 GB/s, so a 1M-sphere scene's arrays (28 MB) would otherwise spend several
+# milliseconds in a single memcpy.
 PARALLEL_COPY_BYTES = 1 << 22
 
 _pool = None
