@@ -1783,6 +1783,10 @@ fr_status fr_tracer_render_path_static(fr_tracer* t, fr_scene* sc, const fr_rend
         FR_CUDA(cudaGetSymbolAddress(&base, g_static_path), "looking up the static path state");
         t->dev->static_path = base;
     }
+    // The device's allocating path state may still hold this tracer's earlier render; its
+    // primary hits do not describe the image this call writes.
+    if (t->dev->path_owner == t)
+        t->dev->path_owner = nullptr;
     if (n_render == 0)
         return FR_OK;
     PathState S;

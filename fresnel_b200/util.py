@@ -20,14 +20,15 @@ PARALLEL_COPY_BYTES = 1 << 22
 
 _pool = None
 _pool_pid = None
+_pool_workers = 1
 
 
 def _copy_pool():
     """The copy threads of this process (made again in a forked child, which has none)."""
-    global _pool, _pool_pid
+    global _pool, _pool_pid, _pool_workers
     if _pool is None or _pool_pid != os.getpid():
-        _pool = ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1),
-                                   thread_name_prefix="fresnel-copy")
+        _pool_workers = min(8, os.cpu_count() or 1)
+        _pool = ThreadPoolExecutor(max_workers=_pool_workers, thread_name_prefix="fresnel-copy")
         _pool_pid = os.getpid()
     return _pool
 
@@ -51,7 +52,7 @@ def _copy_rows(dst, src):
     ordinary numpy assignment, so the result equals the single assignment element for element."""
     pool = _copy_pool()
     n = dst.shape[0]
-    step = -(-n // pool._max_workers)
+    step = -(-n // _pool_workers)
     futures = [pool.submit(dst.__setitem__, slice(i, i + step), src[i:i + step])
                for i in range(0, n, step)]
     for fut in futures:

@@ -17,7 +17,8 @@ import json
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-PKG = "/root/reference/fresnel"
+# the reference tree: FRESNEL_REFERENCE, else where this container mounts it
+PKG = os.path.join(os.environ.get("FRESNEL_REFERENCE", "/root/reference"), "fresnel")
 HANDLES = ("_geometry", "_tracer", "_scene", "_device")
 
 

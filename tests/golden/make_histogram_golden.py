@@ -20,7 +20,9 @@ sys.path.insert(0, REPO)
 
 from oracle import output_path  # noqa: E402
 
-REFERENCE = "/root/reference/fresnel/tracer.py"
+# the reference tree: FRESNEL_REFERENCE, else where this container mounts it
+REFERENCE = os.path.join(os.environ.get("FRESNEL_REFERENCE", "/root/reference"), "fresnel",
+                         "tracer.py")
 
 
 def reference_histogram():

@@ -5,7 +5,10 @@ tracer-owned allocations. It traces fewer samples per wavefront (262144 slots / 
 path's arithmetic depends only on its (pixel, sample, light sample), and the running mean folds
 samples in sample order. Its images must therefore equal the allocating entry point's. The test
 compares them within 1e-6 after each of two calls in a row (the second call continues the first
-one's running mean). It also checks the size limit and the built-scene rule.
+one's running mean), on a sphere scene traced through its BVH, a dense sphere scene traced
+through the sphere grid (also with the persistent and per-lane-refill kernel options) and a
+scene of every geometry type traced through one combined tree. It also checks the size limit,
+the built-scene rule, and that a static render leaves no stale primary hits behind.
 
 The file name sorts last so that pytest collects it after every other test. It passes alone too.
 """
@@ -25,8 +28,15 @@ def _scene(device):
     return workloads.config1(device)
 
 
-def _pair(device, w, h, light_samples):
-    scene = _scene(device)
+SCENES = {
+    "spheres_bvh": (workloads.config1, False),
+    "dense_grid": (lambda d: workloads.config2(d, n=20000, box=140.0 * 0.02**(1 / 3)), True),
+    "mixed": (lambda d: workloads.config3(d, scale=0.002), False),
+}
+
+
+def _pair(device, w, h, light_samples, build=_scene):
+    scene = build(device)
     a = fresnel.tracer.Path(device, w=w, h=h)
     b = fresnel.tracer.Path(device, w=w, h=h)
     for t in (a, b):
@@ -36,10 +46,7 @@ def _pair(device, w, h, light_samples):
     return scene, a, b
 
 
-@pytest.mark.parametrize("w,h,spp,ls", [(200, 150, 24, 1), (96, 64, 10, 3)])
-def test_static_render_matches_allocating_render(gpu_device, w, h, spp, ls):
-    scene, a, b = _pair(gpu_device, w, h, ls)
-    scene._scene.build()
+def _compare(scene, a, b, w, h, spp):
     for call in range(2):
         a._tracer.renderSamples(scene._scene, spp)
         b._tracer.renderSamplesStatic(scene._scene, spp)
@@ -53,6 +60,47 @@ def test_static_render_matches_allocating_render(gpu_device, w, h, spp, ls):
         sb = numpy.array(b.output[:], copy=True)
         assert (numpy.abs(sa.astype(int) - sb.astype(int)) <= 1).all()
     assert a._tracer.getNumSamples() == b._tracer.getNumSamples() == 2 * spp
+
+
+@pytest.mark.parametrize("w,h,spp,ls", [(200, 150, 24, 1), (96, 64, 10, 3)])
+def test_static_render_matches_allocating_render(gpu_device, w, h, spp, ls):
+    scene, a, b = _pair(gpu_device, w, h, ls)
+    scene._scene.build()
+    _compare(scene, a, b, w, h, spp)
+
+
+@pytest.mark.parametrize("name", list(SCENES))
+def test_static_render_matches_on_each_structure(gpu_device, name):
+    build, grid = SCENES[name]
+    scene, a, b = _pair(gpu_device, 160, 96, 2, build)
+    scene._scene.build()
+    assert scene._scene.getAccel()[0] == grid
+    _compare(scene, a, b, 160, 96, 6)
+
+
+@pytest.mark.parametrize("option", ["persistent", "refill"])
+def test_static_render_matches_with_kernel_options(gpu_device, option):
+    dd = gpu_device._device
+    old = dd.getOption(option)
+    try:
+        dd.setOption(option, 1)
+        build, _ = SCENES["dense_grid"]
+        scene, a, b = _pair(gpu_device, 128, 80, 1, build)
+        scene._scene.build()
+        _compare(scene, a, b, 128, 80, 5)
+    finally:
+        dd.setOption(option, old)
+
+
+def test_static_render_leaves_no_stale_primary_hits(gpu_device):
+    scene = _scene(gpu_device)
+    t = fresnel.tracer.Path(gpu_device, w=64, h=48)
+    scene._scene.build()
+    t._tracer.renderSamples(scene._scene, 2)
+    assert t._tracer.primaryHits().shape[:2] == (48, 64)
+    t._tracer.renderSamplesStatic(scene._scene, 2)
+    with pytest.raises(RuntimeError, match="last path render was not this tracer's"):
+        t._tracer.primaryHits()
 
 
 def test_static_render_limits(gpu_device):
