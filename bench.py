@@ -233,18 +233,53 @@ def pin_gpu(local):
     return local
 
 
-def cpu_baseline(wl, kind, seconds):
-    """Time the CPU oracle on a bounded sample of the frame.
+def load_workloads():
+    """The scene generators (fresnel_b200/workloads.py).  When fresnel_b200 is not imported
+    (the reference arm), the file is loaded on its own by path, so that no module of the engine
+    package, and none of its compiled libraries, is loaded."""
+    if "fresnel_b200" in sys.modules:
+        from fresnel_b200 import workloads
+        return workloads
+    import importlib.util
+    name = "fresnel_b200_workloads_standalone"
+    if name not in sys.modules:
+        spec = importlib.util.spec_from_file_location(
+            name, os.path.join(REPO, "fresnel_b200", "workloads.py"))
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        sys.modules[name] = mod
+    return sys.modules[name]
+
+
+_REFERENCE_API = {}
+
+
+def reference_device(kind):
+    """A CPU device of fresnel's own Python package (the reference's fresnel/*.py, staged
+    beside the reference-built oracle) whose compiled backend is the CPU oracle of ``kind``
+    and whose value types are the oracle's plain-Python ones: no library of the engine is
+    loaded."""
+    if kind not in _REFERENCE_API:
+        import tempfile
+
+        from oracle import reference_package
+        root = tempfile.mkdtemp(prefix="fresnel_reference_")
+        _REFERENCE_API[kind] = reference_package.import_fresnel(root, "oracle-values", kind)
+    fresnel = _REFERENCE_API[kind]
+    return fresnel.Device(mode="cpu")
+
+
+def cpu_baseline(wl, dev, seconds, kind):
+    """Time the CPU oracle on a bounded sample of the frame; ``dev`` is a fresnel-API device
+    whose backend is the oracle.
 
     Path: rounds of random pixels of the frame, one pixel sample (x light samples) each.
     Preview: the frame at 1/8 of the resolution in each direction, same camera and AA level.
     """
     import numpy
 
-    import fresnel_b200 as fresnel  # noqa: F401
     from oracle import cpu_module
-    dev = cpu_module.make_device(kind)
-    built = wl.build(dev)
+    built = getattr(load_workloads(), wl.scene)(dev)
     if isinstance(built, list):  # a frame set: time its first frame
         scene, fw, fh = built[0]
     else:
@@ -291,36 +326,55 @@ def cpu_baseline(wl, kind, seconds):
                   f"x {wl.light_samples} light samples, {total_rays} closest-hit queries in "
                   f"{elapsed:.1f} s (BVH build {build_s:.1f} s, not timed)")
     return {"value": total_rays / elapsed / 1e6, "unit": "Mrays/s", "cores": os.cpu_count(),
-            "kind": "reference" if kind == "reference" else "port", "sample": sample}
+            "kind": "reference" if kind == "reference" else "port", "sample": sample,
+            "implementation": CPU_PATH_NOTE}
+
+
+# What the CPU figures are: the reference's CPU renderer uses Embree 4 for its BVH and
+# traversal (fresnel/cpu/Scene.cc:15-28), which is not installed; both CPU legs run the oracle's
+# scalar binned-SAH BVH2 with the same shading arithmetic instead.
+CPU_PATH_NOTE = ("CPU restatement of fresnel's Embree path: fresnel's TracerPath/TracerDirect "
+                 "loops and shading over a scalar binned-SAH BVH2 (Embree 4 is not installed), "
+                 "all host threads")
 
 
 def config_of(wl, world):
+    """The workload description both arms print."""
+    if wl.preview:
+        l2 = "scene arrays and BVH larger than L2 at this size; the image is written once per frame"
+    else:
+        l2 = ("inputs larger than L2 (path state of every sample in flight, plus the scene "
+              "arrays and acceleration structure)")
     return {"workload": wl.desc.format(w=wl.w, h=wl.h, spp=wl.spp), "width": wl.w,
             "height": wl.h, "spp": wl.spp if not wl.preview else wl.aa_n * wl.aa_n,
-            "light_samples": wl.light_samples, "parallelism": f"replicas{world}"}
+            "light_samples": wl.light_samples, "parallelism": f"replicas{world}", "l2": l2}
 
 
 def run_reference(args, wl):
+    """The reference arm: fresnel's own Python package over the oracle compiled from fresnel's
+    own fresnel/common headers (oracle/_ref), timed on this host's cores on bounded samples of
+    the same frame.  Under torchrun only rank 0 works."""
     world, rank, _ = dist_init()
     if rank != 0:
         return 0
     from oracle import cpu_module
     kind = "reference" if os.path.exists(cpu_module.LIB_PATHS["reference"]) else "restated"
+    dev = reference_device(kind)
     per_step = max(2.0, min(20.0, 60.0 / max(1, args.steps + args.warmup)))
     for _ in range(args.warmup):
-        cpu_baseline(wl, kind, per_step / 4)
-    vals = [cpu_baseline(wl, kind, per_step) for _ in range(args.steps)]
+        cpu_baseline(wl, dev, per_step / 4, kind)
+    vals = [cpu_baseline(wl, dev, per_step, kind) for _ in range(args.steps)]
     v = statistics.median(x["value"] for x in vals)
     base = dict(vals[0])
     base["value"] = v
-    cfg = config_of(wl, world)
-    cfg["inputs"] = "host memory"
     line = {
         "metric": METRIC if wl.key == "c2" else f"Mrays/s ({wl.key})",
         "value": v, "unit": "Mrays/s", "impl": "reference",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded)", "config": cfg, "cpu_baseline": base,
+        "data": "synthetic (seeded)", "config": config_of(wl, world), "cpu_baseline": base,
+        "api": f"fresnel's own Python package ({dev.__class__.__module__}) on the "
+               f"{'reference-header' if kind == 'reference' else 'restated'} CPU oracle",
         "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -649,15 +703,19 @@ def main():
                 ext_name: (ext_rays, st["extend_ms"], st["extend_launches"])}
     dom = max(kern, key=lambda k: kern[k][1])
     dom_rays, dom_ms, launches = kern[dom]
-    achieved = (dom_rays * wl.bytes_per_ray) / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else None
-    # The algorithmic bytes above are those of the reference's BVH (fixed box and primitive
-    # tests per ray).  The bytes of the structure this run traversed, from the engine's own
-    # counters over the frame: per ray 24 B in, 16 B out, 12 B of colour, then per node box
-    # test 32 B (BVH) or per grid cell 8 B of offsets, and 16 B per sphere tested.
+    # Algorithmic bytes per ray of the structure this run traversed, from the engine's own
+    # counters over the frame: 24 B of ray in, 16 B of hit out, 12 B of colour at the hit, then
+    # per BVH box test 32 B or per grid cell 8 B of reference range, and 16 B per sphere tested.
     grid = bool(st.get("grid", 0))
     per_box = 8.0 if grid else 32.0
     run_bytes = (52.0 + per_box * st["box_tests"] / rays + 16.0 * st["prim_tests"] / rays
                  if rays > 0 else None)
+    # The roofline's bytes: for a grid, those of the grid walked; for a BVH, the reference BVH's
+    # fixed box and primitive tests per ray (wl.bytes_per_ray).  The reference-BVH figure of a
+    # grid run is kept beside it: it counts the work a BVH would do, not what the kernel read.
+    bpr = run_bytes if grid else wl.bytes_per_ray
+    achieved = (dom_rays * bpr) / (dom_ms / 1e3) / 1e9 if dom_ms > 0 and bpr else None
+    achieved_ref = (dom_rays * wl.bytes_per_ray) / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else None
     achieved_run = ((dom_rays * run_bytes) / (dom_ms / 1e3) / 1e9
                     if dom_ms > 0 and run_bytes else None)
     # DRAM bytes per launch: this kernel's DRAM bytes per ray from an ncu capture
@@ -673,6 +731,13 @@ def main():
                 traffic = per_ray * dom_rays / launches
         except Exception:
             traffic = None
+
+    # Step-level cross-check: every ray of the timed frames at the bytes of the structure walked,
+    # plus 36 B per pixel sample (accumulate read + write, sRGB write), over the frames' time.
+    pix_samples = float(wl.w * wl.h * (wl.aa_n * wl.aa_n if wl.preview else wl.spp * wl.light_samples)
+                        * args.steps)
+    step_bps = ((rays * run_bytes + 36.0 * pix_samples) / (ms / 1e3)
+                if run_bytes and ms > 0 else None)
 
     # ---- end to end through the public API with host buffers ----------------------------------
     e2e_ms = []
@@ -707,16 +772,14 @@ def main():
     cpu = None
     if rank == 0 and not args.no_cpu_baseline and not args.trace_only:
         try:
-            cpu = cpu_baseline(wl, "restated", args.cpu_seconds)
+            from oracle import cpu_module
+            cpu = cpu_baseline(wl, cpu_module.make_device("restated"), args.cpu_seconds,
+                               "restated")
         except Exception as e:  # the baseline must not hide the GPU result
             cpu = {"value": None, "unit": "Mrays/s", "error": str(e)[:200]}
 
     if rank == 0:
         cfg = config_of(wl, world)
-        cfg["accel"] = "sphere grid" if grid else "bvh"
-        cfg["l2"] = ("inputs larger than L2 (path state of 144 B per slot for every sample in "
-                     "flight, plus the scene arrays and BVH)" if not wl.preview else
-                     "scene arrays and BVH; the image is written once per frame")
         line = {
             "metric": METRIC if wl.key == "c2" else f"Mrays/s ({wl.key})",
             "value": value, "unit": "Mrays/s",
@@ -724,20 +787,24 @@ def main():
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
             "config": cfg,
+            "accel": "sphere grid" if grid else "bvh",
             "rays_per_frame": rays_per_frame,
             "gpu_launches": int(st["kernel_launches"]),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
                          "peak_source": peak_kind, "kernel": dom,
                          "rays": dom_rays, "kernel_ms": dom_ms, "launches": launches,
-                         "bytes_per_ray": wl.bytes_per_ray,
+                         "bytes_per_ray": bpr,
+                         "bytes_per_ray_basis": ("sphere grid walked: 52 + 8 per cell + 16 per "
+                                                 "sphere tested, engine counters" if grid else
+                                                 "reference BVH: 52 + 32 A + S P, oracle counts"),
                          "accel": "grid" if grid else "bvh",
                          "bytes_per_ray_run": run_bytes, "achieved_run": achieved_run,
                          "frac_run": (achieved_run / hbm) if achieved_run else None,
-                         "note": ("bytes_per_ray is the reference BVH's per-ray work; the "
-                                  "sphere grid reads bytes_per_ray_run, so frac above 1 "
-                                  "means less work per ray, not more bandwidth")
-                         if grid else None},
+                         "bytes_per_ray_ref_bvh": wl.bytes_per_ray,
+                         "frac_ref_bvh_bytes": (achieved_ref / hbm) if achieved_ref else None,
+                         "step_bytes_per_s": step_bps,
+                         "step_frac": step_bps / 1e9 / hbm if step_bps else None},
             "clocks": clk.summary(),
             "e2e": e2e,
             "cpu_baseline": cpu,

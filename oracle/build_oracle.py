@@ -3,8 +3,10 @@
 Outputs
   oracle/_build/liboracle.so      restated math (oracle/restated_math.hpp)
   oracle/_ref/libfresnel_ref.so   the reference's own fresnel/common/*.h math, compiled from the
-                                  reference tree when it is present (this is the only file in
-                                  the repository that reads the reference sources).
+                                  reference tree when it is present
+  oracle/_ref/fresnel_src/        the reference's Python package and test suite, copied
+                                  unmodified from the reference tree when it is present
+                                  (oracle/reference_package.py)
 
 Both are compiled with g++ -O3 -ffp-contract=off so that no fused multiply-add changes a rounding
 the reference does not make.  Run ``python oracle/build_oracle.py``.
@@ -63,6 +65,11 @@ def build(verbose=False, force=False):
                   "-I", os.path.join(REFERENCE, "fresnel", "common"),
                   *SOURCES, "-o", ref], verbose)
         out.append(ref)
+        sys.path.insert(0, REPO)
+        from oracle import reference_package
+        staged = reference_package.stage(verbose)
+        if staged:
+            out.append(staged)
     return out
 
 

@@ -162,8 +162,16 @@ def lights_struct(lights):
 
 
 def _common_module():
-    from fresnel_b200 import _common
-    return _common
+    """The value types handed back to the caller: those of fresnel_b200._common when the
+    caller's package is already loaded (tests compare the two backends through one API),
+    otherwise the oracle's own plain-Python ones (oracle/values.py), so that the oracle runs
+    with no compiled module of the product loaded."""
+    import sys
+    if "fresnel_b200" in sys.modules:
+        from fresnel_b200 import _common
+        return _common
+    from oracle import values
+    return values
 
 
 def _copy_material(m):
