@@ -165,9 +165,30 @@ struct PolyHit {
     V3 ol, dl;
 };
 
-// slab test over the face planes (fresnel/cpu/GeometryConvexPolyhedron.cc:146-224)
+// Exact ties.  A primitive hit at exactly the distance of the closest hit so far (coincident
+// surfaces: duplicated primitives, shared end caps, rounding-level crossings) wins when its
+// (geometry, primitive) index is the lower one, so that the closest hit does not depend on the
+// order in which a structure (either BVH builder, the sphere grid, the oracle's tree) offers
+// the candidates; fresnel's CPU path keeps whichever its Embree traversal offered first.  A ray
+// without a hit yet never ties.  `cand_prim` is read only when the geometries are equal.
+template <class CandPrim, class BestPrim>
+__device__ __forceinline__ bool tie_wins(uint32_t cand_geom, uint32_t best_geom,
+                                         const CandPrim& cand_prim, const BestPrim& best_prim)
+{
+    return best_geom != MISS &&
+           (cand_geom < best_geom || (cand_geom == best_geom && cand_prim() < best_prim()));
+}
+
+struct NoTie {
+    __device__ __forceinline__ bool operator()() const { return false; }
+};
+
+// slab test over the face planes (fresnel/cpu/GeometryConvexPolyhedron.cc:146-224); the entry
+// (else the exit) distance is accepted when it lies in (tnear, tfar), or equals tfar and
+// `tie()` says the primitive wins the tie.
+template <class Tie = NoTie>
 __device__ __forceinline__ PolyHit poly_planes(const GeomDev& g, V3 o, V3 d, V3 pos, Qt q,
-                                               float tnear, float tfar)
+                                               float tnear, float tfar, const Tie& tie = Tie())
 {
     PolyHit r;
     r.hit = false;
@@ -210,14 +231,15 @@ __device__ __forceinline__ PolyHit poly_planes(const GeomDev& g, V3 o, V3 d, V3 
     }
     if (t0 > t1)
         return r;
-    if ((tnear < t0) & (t0 < tfar)) {
+    if ((tnear < t0) & ((t0 < tfar) || (t0 == tfar && tie()))) {
         r.hit = true;
         r.t = tfar = t0;
         r.n = t0n;
         r.p = t0p;
         r.plane = t0_plane;
+        return r;  // the exit (t1 >= t0) cannot be closer
     }
-    if ((tnear < t1) & (t1 < tfar)) {
+    if ((tnear < t1) & ((t1 < tfar) || (t1 == tfar && tie()))) {
         r.hit = true;
         r.t = tfar = t1;
         r.n = t1n;
@@ -325,6 +347,12 @@ __device__ __forceinline__ void leaf_test(const GeomDev& g, uint32_t gi, const R
 {
     tc.prim += count;
     for (uint32_t s = first; s < first + count; ++s) {
+        // exact tie with the closest hit so far: the lower (geometry, primitive) index wins
+        const auto tie = [&]() {
+            return tie_wins(
+                gi, hit_geom, [&]() { return __ldg(g.order + s); },
+                [&]() { return __ldg(g.order + hit_slot); });
+        };
         float t = 0.0f;
         bool ok;
         if (TYPE == FR_GEOM_SPHERE) {
@@ -340,7 +368,7 @@ __device__ __forceinline__ void leaf_test(const GeomDev& g, uint32_t gi, const R
         } else if (TYPE == FR_GEOM_POLYHEDRON) {
             float4 a = ldg4(g.leaf_data + 2 * s), b = ldg4(g.leaf_data + 2 * s + 1);
             PolyHit ph = poly_planes(g, ray.o, ray.d, v3(a.x, a.y, a.z), Qt{b.x, v3(b.y, b.z, b.w)},
-                                     tnear, tmax);
+                                     tnear, tmax, tie);
             ok = ph.hit;
             t = ph.t;
         } else if (TYPE == FR_GEOM_MESH) {
@@ -355,7 +383,7 @@ __device__ __forceinline__ void leaf_test(const GeomDev& g, uint32_t gi, const R
             ok = ph.hit;
             t = ph.t;
         }
-        if (ok && (tnear < t) && (t < tmax)) {
+        if (ok && (tnear < t) && ((t < tmax) || (t == tmax && tie()))) {
             tmax = t;
             hit_geom = gi;
             hit_slot = s;
@@ -766,6 +794,12 @@ __device__ __forceinline__ void leaf_test_mixed(const SceneDev& sc, const RayK& 
         const GeomDev& g = sc.geoms[gi];
         const int type = g.type;
         const float4 a = ldg4(sc.leaf_data + 2 * size_t(s));
+        // exact tie with the closest hit so far: the lower (geometry, primitive) index wins
+        const auto tie = [&]() {
+            return tie_wins(
+                gi, hit_geom, [&]() { return __ldg(sc.order + s); },
+                [&]() { return __ldg(sc.order + hit_slot); });
+        };
         float t = 0.0f;
         bool ok = false;
         if ((MASK & (1u << FR_GEOM_SPHERE)) && type == FR_GEOM_SPHERE) {
@@ -780,7 +814,7 @@ __device__ __forceinline__ void leaf_test_mixed(const SceneDev& sc, const RayK& 
         } else if ((MASK & (1u << FR_GEOM_POLYHEDRON)) && type == FR_GEOM_POLYHEDRON) {
             const float4 b = ldg4(sc.leaf_data + 2 * size_t(s) + 1);
             PolyHit ph = poly_planes(g, ray.o, ray.d, v3(a.x, a.y, a.z), Qt{b.x, v3(b.y, b.z, b.w)},
-                                     tnear, tmax);
+                                     tnear, tmax, tie);
             ok = ph.hit;
             t = ph.t;
         } else if ((MASK & (1u << FR_GEOM_MESH)) && type == FR_GEOM_MESH) {
@@ -795,7 +829,7 @@ __device__ __forceinline__ void leaf_test_mixed(const SceneDev& sc, const RayK& 
             ok = ph.hit;
             t = ph.t;
         }
-        if (ok && (tnear < t) && (t < tmax)) {
+        if (ok && (tnear < t) && ((t < tmax) || (t == tmax && tie()))) {
             tmax = t;
             hit_geom = gi;
             hit_slot = s;
@@ -893,17 +927,21 @@ __device__ __forceinline__ bool grid_walk_step(const GridDev& G, const RayK& ray
     const uint32_t last = W.last;
     tc.box += 1;
     tc.prim += last - W.first;
+    // exact tie with the closest hit so far: the lower sphere index wins (one geometry)
+    const auto tie = [&](uint32_t r) {
+        return slot != MISS && __ldg(G.ref_prim + r) < __ldg(G.ref_prim + slot);
+    };
     uint32_t k = W.first;
     for (; k + 1 < last; k += 2) {  // two spheres in flight
         const float4 q0 = ldg4(G.ref_sphere + k), q1 = ldg4(G.ref_sphere + k + 1);
         float t0, t1;
         if (sphere_t(ray.o, ray.d, v3(q0.x, q0.y, q0.z), q0.w, t0) && (tnear < t0) &&
-            (t0 < tmax)) {
+            ((t0 < tmax) || (t0 == tmax && tie(k)))) {
             tmax = t0;
             slot = k;
         }
         if (sphere_t(ray.o, ray.d, v3(q1.x, q1.y, q1.z), q1.w, t1) && (tnear < t1) &&
-            (t1 < tmax)) {
+            ((t1 < tmax) || (t1 == tmax && tie(k + 1)))) {
             tmax = t1;
             slot = k + 1;
         }
@@ -911,7 +949,8 @@ __device__ __forceinline__ bool grid_walk_step(const GridDev& G, const RayK& ray
     if (k < last) {
         const float4 q = ldg4(G.ref_sphere + k);
         float t;
-        if (sphere_t(ray.o, ray.d, v3(q.x, q.y, q.z), q.w, t) && (tnear < t) && (t < tmax)) {
+        if (sphere_t(ray.o, ray.d, v3(q.x, q.y, q.z), q.w, t) && (tnear < t) &&
+            ((t < tmax) || (t == tmax && tie(k)))) {
             tmax = t;
             slot = k;
         }

@@ -635,12 +635,12 @@ __device__ __forceinline__ C3 preview_shade(const FrameParams& P, const GeomDev&
         V3 l = P.lights.dir[li];
         V3 r = -v + (2.0f * n * dot(n, v));
         float half = P.lights.theta[li];
-        float cos_half = cosf(half);
+        float cos_half = hcos(half);
         float ldotr = dot(l, r);
         if (ldotr < cos_half) {
             V3 ax = cross(l, r);
             ax = div_recip(ax, sqrtf(dot(ax, ax)));
-            Qt q = from_axis_angle(ax, -acosf(ldotr) + half);
+            Qt q = from_axis_angle(ax, -hacos(ldotr) + half);
             r = rotate(q, r);
         }
         C3 f_d = c3(0, 0, 0), f_s = c3(0, 0, 0);

@@ -3,8 +3,10 @@
 // A CPU restatement of fresnel's Embree backend: per-geometry closest-hit glue restated from
 // fresnel/cpu/Geometry{Sphere,Cylinder,ConvexPolyhedron,Mesh,Polygon}.cc, the tile loops of
 // fresnel/cpu/TracerPath.cc and fresnel/cpu/TracerDirect.cc, and a binned-SAH BVH2 standing in
-// for Embree's scene BVH (closest-hit results do not depend on the BVH except for exact ties
-// in t).  The shading/intersection arithmetic comes from namespace M, which is either the
+// for Embree's scene BVH.  Closest-hit results do not depend on the BVH: Embree keeps whichever
+// of two primitives hit at exactly the same t its traversal offers first, and the oracle, like
+// the engine, instead gives such exact ties to the lower (geometry, primitive) index
+// (accept_hit below).  The shading/intersection arithmetic comes from namespace M, which is either the
 // restatement (restated_math.hpp) or the reference's own headers (ref_math_adapter.hpp,
 // selected with -DFR_ORACLE_REFERENCE_MATH).
 //
@@ -331,6 +333,18 @@ struct Hit {
     float d;
 };
 
+// Acceptance of a candidate hit at t (fresnel/cpu/GeometrySphere.cc:101: tnear < t < tfar), with
+// exact ties at tfar broken toward the lower (geometry, primitive) index; a ray with no hit yet
+// never ties.
+inline bool accept_hit(float t, float tnear, const Hit& h, uint32_t gi, uint32_t prim)
+{
+    if (!(tnear < t))
+        return false;
+    if (t < h.t)
+        return true;
+    return t == h.t && h.geom != UINT32_MAX && (gi < h.geom || (gi == h.geom && prim < h.prim));
+}
+
 // fresnel/cpu/GeometrySphere.cc:81-118
 inline void glue_sphere(const Geom& g, uint32_t gi, uint32_t prim, F3 o, F3 dir, float tnear,
                         Hit& h)
@@ -340,7 +354,7 @@ inline void glue_sphere(const Geom& g, uint32_t gi, uint32_t prim, F3 o, F3 dir,
     float t = 0, d = 0;
     F3 N;
     bool hit = M::isect_sphere(t, d, N, o, dir, p, r);
-    if (hit && (tnear < t) && (t < h.t)) {
+    if (hit && accept_hit(t, tnear, h, gi, prim)) {
         h.t = t;
         h.geom = gi;
         h.prim = prim;
@@ -360,7 +374,7 @@ inline void glue_cylinder(const Geom& g, uint32_t gi, uint32_t prim, F3 o, F3 di
     F3 N{0, 0, 0};
     unsigned ci = 0;
     bool hit = M::isect_spherocylinder(t, d, N, ci, o, dir, A, B, r);
-    if (hit && (tnear < t) && (t < h.t)) {
+    if (hit && accept_hit(t, tnear, h, gi, prim)) {
         h.t = t;
         h.geom = gi;
         h.prim = prim;
@@ -415,18 +429,16 @@ inline void glue_polyhedron(const Geom& g, uint32_t gi, uint32_t prim, F3 o, F3 
     float t_hit = 0;
     bool hit = false;
     F3 n_hit{0, 0, 0}, p_hit{0, 0, 0};
-    float tfar = h.t;
     Hit cand = h;
-    if ((tnear < t0) & (t0 < tfar)) {
-        t_hit = tfar = t0;
+    if (accept_hit(t0, tnear, h, gi, prim)) {
+        t_hit = t0;
         cand.Ng = M::rotate(q, t0n);
         n_hit = t0n;
         p_hit = t0p;
         cand.color = frm::lerp(g.color_by_face, g.color[prim], g.plane_color[t0_plane]);
         hit = true;
-    }
-    if ((tnear < t1) & (t1 < tfar)) {
-        t_hit = tfar = t1;
+    } else if (accept_hit(t1, tnear, h, gi, prim)) {  // the exit (t1 >= t0)
+        t_hit = t1;
         cand.Ng = M::rotate(q, t1n);
         n_hit = t1n;
         p_hit = t1p;
@@ -499,7 +511,7 @@ inline void glue_mesh(const Geom& g, uint32_t gi, uint32_t item, F3 o, F3 dir, f
     if (!M::isect_triangle(u, v, w, t, d, n, ol, ol + dl, v0, v1, v2)
         && !M::isect_triangle(v, u, w, t, d, n, ol, ol + dl, v1, v0, v2))
         return;
-    if ((tnear < t) & (t < h.t)) {
+    if (accept_hit(t, tnear, h, gi, item)) {
         h.t = t;
         h.geom = gi;
         h.prim = item;
@@ -551,7 +563,7 @@ inline void glue_polygon(const Geom& g, uint32_t gi, uint32_t prim, F3 o, F3 dir
     if (d_edge > g.rounding_radius)
         return;
     const float shade_d = g.rounding_radius - d_edge;
-    if ((tnear < t_hit) & (t_hit < h.t)) {
+    if (accept_hit(t_hit, tnear, h, gi, prim)) {
         h.t = t_hit;
         h.geom = gi;
         h.prim = prim;

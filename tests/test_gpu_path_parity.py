@@ -15,6 +15,7 @@ import pytest
 
 from fresnel_b200 import workloads
 from parity import path_render
+from parity_record import record
 
 pytestmark = pytest.mark.gpu
 
@@ -37,6 +38,8 @@ def test_path_same_seed(name, gpu_device, oracle_device):
     assert gt._tracer.getNumSamples() == spp
     close = numpy.all(numpy.abs(gl - ol) <= 1e-3, axis=-1)
     frac = close.mean()
+    record("test_path_same_seed", check="same_seed", scene=name, width=w, height=h, spp=spp,
+           light_samples=ls, within_1e3=float(frac), max_abs=float(numpy.abs(gl - ol).max()))
     assert frac >= 0.99, f"only {frac:.4%} of pixels within 1e-3"
     assert numpy.all(g8[..., 3] == o8[..., 3])
 
@@ -56,6 +59,9 @@ def test_path_monte_carlo_error(gpu_device, oracle_device):
     se2 = var / gpu_spp + var / ref_spp
     mask = se2 > 1e-12
     z = (g - lin[:, :3])[mask] / numpy.sqrt(se2[mask])
+    record("test_path_monte_carlo_error", check="monte_carlo", scene="spheres_1k", spp=gpu_spp,
+           oracle_spp=ref_spp, values=int(z.size), mean_z2=float(numpy.mean(z**2)),
+           frac_abs_z_gt_2=float(numpy.mean(numpy.abs(z) > 2)))
     assert z.size > 100
     assert numpy.mean(z**2) <= 1.2, f"mean z^2 = {numpy.mean(z**2):.3f}"
     assert numpy.mean(numpy.abs(z) > 2) <= 0.06

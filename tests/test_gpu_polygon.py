@@ -9,7 +9,7 @@ import numpy
 import pytest
 
 import fresnel_b200 as fresnel
-from grazing import classify
+from grazing import check_hits
 from parity import preview_hits
 
 pytestmark = pytest.mark.gpu
@@ -53,10 +53,8 @@ def test_reference_scenes_match_oracle(rounding_radius, outline, aa_n, gpu_devic
     oscene = reference_scene(oracle_device, rounding_radius, outline)
     oh, ol, o8 = preview_hits(oracle_device, oscene, w, h, aa_n)
     assert numpy.count_nonzero(oh[..., 0]) > 0
-    mism = numpy.any(gh != oh, axis=-1)
-    n_grazing, real = classify(oracle_device, oscene, w, h, aa_n, gh, oh)
-    assert not real, f"non-grazing hit disagreements: {real[:5]}"
-    assert mism.mean() <= 1e-3
+    mism = check_hits("test_reference_scenes_match_oracle", oracle_device, oscene, w, h, aa_n,
+                      gh, oh, scene=f"polygons r={rounding_radius} outline={outline}")
     agree = ~numpy.any(mism, axis=-1)
     assert numpy.abs(gl - ol)[agree].max() <= 1e-3
     assert numpy.all(g8 == o8, axis=-1)[agree].mean() >= 0.999
@@ -107,6 +105,5 @@ def test_rotating_polygons_rebuilds_their_tree(gpu_device, oracle_device):
         s.geometry[0].angle[:] = ang
     gh, gl, _ = preview_hits(gpu_device, scenes[0], 90, 60, 1)
     oh, ol, _ = preview_hits(oracle_device, scenes[1], 90, 60, 1)
-    n_grazing, real = classify(oracle_device, scenes[1], 90, 60, 1, gh, oh)
-    assert not real
-    assert numpy.any(gh != oh, axis=-1).mean() <= 1e-3
+    check_hits("test_rotating_polygons_rebuilds_their_tree", oracle_device, scenes[1], 90, 60,
+               1, gh, oh, scene="polygons rotated")

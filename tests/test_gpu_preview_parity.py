@@ -3,8 +3,9 @@
 Bars (from the reference CPU path as normative): hit ids bit-exact except at grazing samples --
 every disagreement is classified with the oracle (tests/grazing.py: an exact or rounding-level
 tie in t between the two primitives, or a ray within rounding of a silhouette) and none may be
-non-grazing; grazing disagreements are reported and must stay below 1e-3 of the samples (the
-stated rate is printed); linear RGB within 1e-3 wherever the hits agree; sRGB bytes equal on at
+non-grazing; all disagreements together stay at or below 1e-4 of the samples (each measured
+rate is written through parity_record); linear RGB within 1e-3 wherever the hits agree; sRGB
+bytes equal on at
 least 99.9% of pixels (transcendental functions differ in the last place between CUDA and the
 host libm).
 """
@@ -14,12 +15,11 @@ import pytest
 
 import fresnel_b200 as fresnel
 from fresnel_b200 import workloads
-from grazing import classify
+from grazing import check_hits
 from parity import odd_radii_scene, preview_hits
 
 pytestmark = pytest.mark.gpu
 
-GRAZING_MAX = 1e-3
 RGB_TOL = 1e-3
 
 
@@ -60,14 +60,9 @@ def test_preview_matches_oracle(name, aa_n, builder, gpu_device, oracle_device):
     oscene = build(oracle_device)
     oh, ol, o8 = preview_hits(oracle_device, oscene, w, h, aa_n)
     assert gh.shape == oh.shape
-    mism = numpy.any(gh != oh, axis=-1)
     assert numpy.count_nonzero(oh[..., 0]) > 0, "scene shows no geometry"
-    n_grazing, real = classify(oracle_device, oscene, w, h, aa_n, gh, oh)
-    rate = mism.mean()
-    print(f"{name} aa={aa_n}: {numpy.count_nonzero(mism)} of {mism.size} hit ids differ "
-          f"({rate:.2e}), all grazing: {not real}")
-    assert not real, f"non-grazing hit disagreements: {real[:5]}"
-    assert rate <= GRAZING_MAX
+    mism = check_hits("test_preview_matches_oracle", oracle_device, oscene, w, h, aa_n, gh, oh,
+                      scene=name, builder=("lbvh", "ploc")[builder])
     agree = ~numpy.any(mism, axis=-1)
     err = numpy.abs(gl - ol)[agree].max()
     assert err <= RGB_TOL, f"linear RGB differs by {err}"

@@ -1,0 +1,199 @@
+"""Parity at the benchmark sizes: the measured configurations themselves against the CPU oracle.
+
+* 1M-sphere scene (1,000,000 spheres r = 0.5 in a cube of side 140, per-particle colours,
+  lightbox), 1920x1080:
+  - Path, 256 samples per pixel, 1 light sample, the engine's defaults for the frame (the
+    sphere grid, fused trace-and-shade bounces, wavefronts of 64 samples per pixel) and again
+    through the BVH (device option accel = 0).  Same seed: on 4096 seeded pixels the oracle's
+    own render of those pixels (same seed, samples 1..256) must agree within 1e-3 on >= 99% of
+    them, alpha equal.  Monte Carlo: the same GPU image against a 4096-sample oracle render of
+    2048 other seeded pixels under an independent seed, z per pixel and channel: at most 6% of
+    |z| > 2, mean z^2 <= 1.2 with the largest 0.5% set aside (_monte_carlo).
+  - Preview with anti-aliasing (8x8 = 64 samples per pixel, 132.7M closest-hit queries), grid
+    and BVH: every closest-hit id of every sample against the oracle's; disagreements are
+    classified (tests/grazing.py) and none may be non-grazing; all disagreements together at
+    most 1e-4 of the samples; linear RGB within 1e-3 where every sample of a pixel agrees.
+* Mixed scene at full size (200k spheres, 50k bonds, 20k cubes, 10k icosahedra = 470k
+  primitives, one combined tree), 1280x720: Preview hit ids at 4x4 samples per pixel, and Path
+  at 128 samples per pixel: the Monte Carlo test on 2048 seeded pixels and the same-seed test
+  on 4096 (>= 99% within 1e-3).
+
+Every measured rate is written through parity_record.record.
+"""
+
+import numpy
+import pytest
+
+import fresnel_b200 as fresnel
+from fresnel_b200 import workloads
+from grazing import classify
+from parity import preview_hits
+from parity_record import record
+
+pytestmark = [pytest.mark.gpu, pytest.mark.slow]
+
+MISMATCH_MAX = 1e-4  # closest-hit id disagreements (grazing ones included) per sample
+RGB_TOL = 1e-3
+SAME_SEED_TOL = 1e-3
+SAME_SEED_FRAC = 0.99
+
+
+@pytest.fixture
+def accel(request, gpu_device):
+    """The engine's acceleration-structure option for the scenes built inside the test."""
+    dd = gpu_device._device
+    old = dd.getOption("accel")
+    dd.setOption("accel", request.param)
+    yield request.param
+    dd.setOption("accel", old)
+
+
+_ORACLE = {}
+
+
+def _oracle_scene(oracle_device, key, build):
+    """The oracle's scene, built once per module and kept (its BVH takes seconds at 1M)."""
+    if key not in _ORACLE:
+        s = build(oracle_device)
+        s._scene.handle()
+        _ORACLE[key] = s
+    return _ORACLE[key]
+
+
+def _pixels(n, w, h, seed):
+    rng = numpy.random.default_rng(seed)
+    return numpy.sort(rng.choice(w * h, size=n, replace=False)).astype(numpy.uint32)
+
+
+def _gpu_path(gpu_device, build, w, h, spp, seed):
+    scene = build(gpu_device)
+    t = fresnel.tracer.Path(gpu_device, w=w, h=h)
+    t.seed = seed
+    t.sample(scene, samples=spp, light_samples=1)
+    grid = bool(scene._scene.getAccel()[0])
+    lin = numpy.array(t.linear_output[:], copy=True)
+    assert t.seed == seed + 1 and t._tracer.getNumSamples() == spp
+    return lin, grid, t._tracer.getStats()
+
+
+def _same_seed(test, oscene, oracle_device, gl, w, h, spp, seed_used, extra):
+    pix = _pixels(4096, w, h, 11)
+    t = oracle_device.module.TracerPath(oracle_device._device, w, h, 1)
+    t.setSeed(seed_used)
+    lin, _, _ = t.render_pixels(oscene._scene, pix, 1, spp, want_m2=False)
+    g = gl.reshape(-1, 4)[pix]
+    diff = numpy.abs(g - lin)
+    close = numpy.all(diff <= SAME_SEED_TOL, axis=-1)
+    frac = float(close.mean())
+    record(test, check="same_seed", pixels=len(pix), spp=spp, within_1e3=frac,
+           max_abs=float(diff.max()), median_abs=float(numpy.median(diff)), **extra)
+    assert frac >= SAME_SEED_FRAC, f"only {frac:.4%} of pixels within {SAME_SEED_TOL}"
+    assert numpy.array_equal(g[:, 3], lin[:, 3])
+
+
+def _monte_carlo(test, oscene, oracle_device, gl, w, h, spp, seed_used, extra):
+    """z = (gpu - oracle_4096) / sqrt(s2/spp + s2/4096) per pixel and channel, s2 the oracle's
+    per-pixel sample variance.  Bars: at most 6% of |z| > 2 ("within 2x the Monte Carlo
+    standard error") and mean z^2 <= 1.2 after the largest 0.5% of z^2 are set aside: a light
+    of small solid angle makes rare very bright samples, so a few pixels' 4096-sample variance
+    understates their spread; the oracle's own render at the GPU's seed and sample count is
+    scored the same way and recorded beside it."""
+    ref_spp = 4096
+    pix = _pixels(2048, w, h, 12)
+    t = oracle_device.module.TracerPath(oracle_device._device, w, h, 1)
+    t.setSeed(99)
+    lin, _, m2 = t.render_pixels(oscene._scene, pix, 1, ref_spp)
+    t.setSeed(seed_used)
+    own, _, _ = t.render_pixels(oscene._scene, pix, 1, spp, want_m2=False)
+    var = m2 / (ref_spp - 1)
+    se2 = var / spp + var / ref_spp
+    mask = se2 > 1e-12
+
+    def score(img):
+        z = (img[:, :3] - lin[:, :3])[mask] / numpy.sqrt(se2[mask])
+        z2 = numpy.sort(z**2)
+        trimmed = float(z2[:int(len(z2) * 0.995)].mean())
+        return z, float(z2.mean()), trimmed, float(numpy.mean(numpy.abs(z) > 2))
+
+    z, mz2, tz2, out2 = score(gl.reshape(-1, 4)[pix])
+    _, omz2, otz2, oout2 = score(own)
+    record(test, check="monte_carlo", pixels=len(pix), spp=spp, oracle_spp=ref_spp,
+           values=int(z.size), mean_z2=mz2, mean_z2_trimmed=tz2, frac_abs_z_gt_2=out2,
+           oracle_same_spp={"mean_z2": omz2, "mean_z2_trimmed": otz2, "frac_abs_z_gt_2": oout2},
+           **extra)
+    assert z.size > 1000
+    assert tz2 <= 1.2, f"trimmed mean z^2 = {tz2:.3f}"
+    assert out2 <= 0.06
+
+
+def _preview(test, gpu_device, oracle_device, gscene, oscene, w, h, aa_n, extra):
+    gh, gl, g8 = preview_hits(gpu_device, gscene, w, h, aa_n)
+    oh, ol, o8 = preview_hits(oracle_device, oscene, w, h, aa_n)
+    assert gh.shape == oh.shape == (h, w, aa_n * aa_n, 2)
+    assert numpy.count_nonzero(oh[..., 0]) > 0
+    mism = numpy.any(gh != oh, axis=-1)
+    n_mism = int(numpy.count_nonzero(mism))
+    kinds = {}
+    n_grazing, real = classify(oracle_device, oscene, w, h, aa_n, gh, oh, kinds=kinds)
+    rate = n_mism / mism.size
+    agree = ~numpy.any(mism, axis=-1)
+    err = float(numpy.abs(gl - ol)[agree].max())
+    srgb_same = float(numpy.all(g8 == o8, axis=-1)[agree].mean())
+    record(test, check="preview_hits", samples=int(mism.size), mismatches=n_mism,
+           grazing=n_grazing, grazing_kinds=kinds, non_grazing=len(real), rate=rate,
+           rgb_max_abs=err,
+           srgb_identical=srgb_same, **extra)
+    del gh, oh
+    assert not real, f"non-grazing hit disagreements: {real[:5]}"
+    assert rate <= MISMATCH_MAX, f"{n_mism} of {mism.size} closest hits differ ({rate:.2e})"
+    assert err <= RGB_TOL, f"linear RGB differs by {err}"
+    assert srgb_same >= 0.999
+
+
+# ---- 1M spheres, 1920x1080 ---------------------------------------------------------------------
+C2_W, C2_H, C2_SPP = 1920, 1080, 256
+
+
+@pytest.mark.parametrize("accel", [2, 0], ids=["default_grid", "bvh"], indirect=True)
+def test_config2_path(accel, gpu_device, oracle_device):
+    gl, grid, st = _gpu_path(gpu_device, workloads.config2, C2_W, C2_H, C2_SPP, seed=7)
+    assert grid == (accel == 2), "the 1M-sphere frame should be traced as configured"
+    assert numpy.isfinite(gl).all()
+    oscene = _oracle_scene(oracle_device, "config2", workloads.config2)
+    extra = {"scene": "config2 1M spheres", "width": C2_W, "height": C2_H,
+             "structure": "sphere grid" if grid else "bvh", "gpu_rays": int(st["rays"])}
+    _same_seed("test_config2_path", oscene, oracle_device, gl, C2_W, C2_H, C2_SPP, 8, extra)
+    _monte_carlo("test_config2_path", oscene, oracle_device, gl, C2_W, C2_H, C2_SPP, 8, extra)
+
+
+@pytest.mark.parametrize("accel", [2, 0], ids=["default_grid", "bvh"], indirect=True)
+def test_config2_preview_anti_aliased(accel, gpu_device, oracle_device):
+    gscene = workloads.config2(gpu_device)
+    oscene = _oracle_scene(oracle_device, "config2", workloads.config2)
+    gscene._scene.build()
+    grid = bool(gscene._scene.getAccel()[0])
+    assert grid == (accel == 2)
+    _preview("test_config2_preview_anti_aliased", gpu_device, oracle_device, gscene, oscene,
+             C2_W, C2_H, 8, {"scene": "config2 1M spheres", "width": C2_W, "height": C2_H,
+                             "aa": 8, "structure": "sphere grid" if grid else "bvh"})
+
+
+# ---- mixed scene, 470k primitives, 1280x720 ----------------------------------------------------
+C3_W, C3_H, C3_SPP = 1280, 720, 128
+
+
+def test_config3_preview(gpu_device, oracle_device):
+    gscene = workloads.config3(gpu_device)
+    oscene = _oracle_scene(oracle_device, "config3", workloads.config3)
+    _preview("test_config3_preview", gpu_device, oracle_device, gscene, oscene, C3_W, C3_H, 4,
+             {"scene": "config3 mixed 470k primitives", "width": C3_W, "height": C3_H, "aa": 4})
+
+
+def test_config3_path(gpu_device, oracle_device):
+    gl, grid, st = _gpu_path(gpu_device, workloads.config3, C3_W, C3_H, C3_SPP, seed=7)
+    assert not grid
+    oscene = _oracle_scene(oracle_device, "config3", workloads.config3)
+    extra = {"scene": "config3 mixed 470k primitives", "width": C3_W, "height": C3_H,
+             "structure": "combined bvh", "gpu_rays": int(st["rays"])}
+    _monte_carlo("test_config3_path", oscene, oracle_device, gl, C3_W, C3_H, C3_SPP, 8, extra)
+    _same_seed("test_config3_path", oscene, oracle_device, gl, C3_W, C3_H, C3_SPP, 8, extra)
