@@ -96,7 +96,10 @@ def parse():
                    help="target duration of the CPU baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--trace-only", action="store_true",
-                   help="skip the end-to-end leg and the CPU baseline (profiler captures)")
+                   help="skip the end-to-end leg, the CPU baseline and the further "
+                        "configurations (profiler captures)")
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the further configurations the default run reports under 'also'")
     a = p.parse_args()
     wl = WORKLOADS[a.workload]
     wl.w = a.width or wl.w
@@ -395,10 +398,12 @@ def host_arrays(scene):
     return out
 
 
-def run_batch_bench(args, world, rank, barrier_max, barrier_sum, clock_index):
+def run_batch_bench(args, world, rank, barrier_max, barrier_sum, clock_index, emit=True):
     """Trajectory frame set (64 scenes of 1e4-5e5 spheres, 512^2-1024^2, 16 spp): the frames
     traced as one PathBatch (one CUDA graph launch) against 64 sequential plain Path.sample
-    calls. Both produce identical images (checked), so the comparison is at equal error."""
+    calls, and against fresnel's own form of Path.sample, one render call per sample
+    (fresnel/tracer.py:250-260).  All three produce identical images (checked), so the
+    comparison is at equal error.  Returns the JSON line (printed by rank 0 when ``emit``)."""
     import numpy
 
     import fresnel_b200 as fresnel
@@ -410,7 +415,7 @@ def run_batch_bench(args, world, rank, barrier_max, barrier_sum, clock_index):
     for s, _, _ in frames:
         s._scene.build()
     # leaf size, primary tile shape and queue depth from the autotuner, on 2-spp probes of
-    # the frame set itself; both forms below run with the chosen options
+    # the frame set itself; every form below runs with the chosen options
     from fresnel_b200 import autotune
     t0 = time.perf_counter()
     tuner = autotune.Tuner(device, probe_spp=2, repeats=2)
@@ -420,41 +425,59 @@ def run_batch_bench(args, world, rank, barrier_max, barrier_sum, clock_index):
         s._scene.build()
     plain = [fresnel.tracer.Path(device, w=w, h=h) for _, w, h in frames]
     batched = [fresnel.tracer.Path(device, w=w, h=h) for _, w, h in frames]
-    for f in range(len(frames)):
-        plain[f].seed = 1000 * rank + f
-        batched[f].seed = 1000 * rank + f
+    per_sample = [fresnel.tracer.Path(device, w=w, h=h) for _, w, h in frames]
     batch = fresnel.tracer.PathBatch(device)
+    # every step renders each frame from the same seed in all three forms, so their images
+    # must be identical
+    seeds = [1000 * rank + f for f in range(len(frames))]
 
     def run_plain():
-        for (s, _, _), t in zip(frames, plain):
+        for (s, _, _), t, seed in zip(frames, plain, seeds):
+            t.seed = seed
             t.sample(s, samples=spp)
 
+    def run_per_sample():
+        # fresnel's Path.sample: reset, then one render (returning the output) per sample
+        for (s, _, _), t, seed in zip(frames, per_sample, seeds):
+            t.seed = seed
+            t.reset()
+            for _ in range(spp):
+                t.render(s)
+
     def run_batch():
-        for (s, _, _), t in zip(frames, batched):
+        for (s, _, _), t, seed in zip(frames, batched, seeds):
+            t.seed = seed
             batch.add(t, s, samples=spp)
         batch.render()
 
-    def timed(fn, tracers):
+    def timed(fn, tracers, steps):
         for t in tracers:
             t._tracer.resetStats()
         dd.synchronize()
         dd.timerStart()
-        for _ in range(args.steps):
+        for _ in range(steps):
             fn()
         ms = dd.timerStop()
-        return ms, float(sum(t._tracer.getStats()["rays"] for t in tracers))
+        sts = [t._tracer.getStats() for t in tracers]
+        return ms, float(sum(x["rays"] for x in sts)), sts
 
     for _ in range(args.warmup):
         run_plain()
         run_batch()
-    ms_plain, rays_plain = timed(run_plain, plain)
+    run_per_sample()
+    ms_plain, rays_plain, _ = timed(run_plain, plain, args.steps)
+    ms_per_sample, rays_per_sample, _ = timed(run_per_sample, per_sample, max(1, args.steps // 2))
     launches0 = batch.stats["kernel_launches"]
     with ClockSampler(clock_index) as clk:
-        ms_batch, rays_batch = timed(run_batch, batched)
+        ms_batch, rays_batch, bst = timed(run_batch, batched, args.steps)
     launches = batch.stats["kernel_launches"] - launches0
-    diff = max(float(numpy.abs(numpy.asarray(a.linear_output[:]) -
-                               numpy.asarray(b.linear_output[:])).max())
-               for a, b in zip(plain, batched))
+
+    def maxdiff(xs, ys):
+        return max(float(numpy.abs(numpy.asarray(a.linear_output[:]) -
+                                   numpy.asarray(b.linear_output[:])).max())
+                   for a, b in zip(xs, ys))
+    diff = maxdiff(plain, batched)
+    diff_per_sample = maxdiff(per_sample, batched)
 
     # end to end: every frame's arrays written from host memory (BVH rebuilt), traced, and its
     # sRGB image read back
@@ -481,65 +504,82 @@ def run_batch_bench(args, world, rank, barrier_max, barrier_sum, clock_index):
 
     ms_plain = barrier_max(ms_plain)
     ms_batch = barrier_max(ms_batch)
+    ms_per_sample = barrier_max(ms_per_sample)
     value = barrier_sum(rays_batch) / (ms_batch / 1e3) / 1e6
     value_plain = barrier_sum(rays_plain) / (ms_plain / 1e3) / 1e6
+    value_per_sample = barrier_sum(rays_per_sample) / (ms_per_sample / 1e3) / 1e6
     e2e_b = barrier_max(statistics.mean(e2e_batch))
     e2e_p = barrier_max(statistics.mean(e2e_plain))
     rays_frame_set = rays_batch / args.steps
     hbm, peak_kind = peaks()
-    bpr = WORKLOADS["c2"].bytes_per_ray
-    achieved = rays_batch * bpr / (ms_batch / 1e3) / 1e9
-    if rank == 0:
-        line = {
-            "metric": "Mrays/s (c4: 64-frame set, batched)", "value": value, "unit": "Mrays/s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms_batch / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": {"workload": f"config4: 64 frames, 1e4-5e5 spheres at the 1M-sphere "
-                                   f"scene's density, 512^2/768^2/1024^2, {spp} spp, 1 light "
-                                   "sample; one PathBatch vs 64 sequential Path.sample calls",
-                       "frames": len(frames), "spp": spp,
-                       "autotune": {"options": tuned, "probe_ms": probe_ms,
-                                    "settings_measured": len(tuner.log), "seconds": tune_s},
-                       "spheres": int(sum(len(s.geometry[0].position[:]) for s, _, _ in frames)),
-                       "pixels": int(sum(w * h for _, w, h in frames)),
-                       "parallelism": f"replicas{world}",
-                       "l2": "inputs larger than L2 (64 scenes, 2.4 GB path state)"},
-            "plain": {"value": value_plain, "ms_per_step": ms_plain / args.steps,
-                      "e2e_ms_per_step": e2e_p},
-            "batched_over_plain": value / value_plain,
-            "e2e_batched_over_plain": e2e_p / e2e_b,
-            "max_abs_image_difference": diff,
-            "rays_per_frame_set": rays_frame_set,
-            "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": None, "peak_source": peak_kind,
-                         "kernel": "whole batch graph (all kernels)",
-                         "bytes_per_ray": bpr},
-            "clocks": clk.summary(),
-            "e2e": {"value": barrier_sum(rays_frame_set) / (e2e_b / 1e3) / 1e6,
-                    "unit": "Mrays/s", "h2d_bytes_per_step": int(in_bytes),
-                    "d2h_bytes_per_step": int(out_bytes), "ms_per_step": e2e_b},
-            "batch_stats": batch.stats,
-            "cpu_baseline": None,
-        }
+    # bytes of the structures walked (sphere grids: 52 + 8 per cell + 16 per sphere tested)
+    box = sum(float(x["box_tests"]) for x in bst)
+    prim = sum(float(x["prim_tests"]) for x in bst)
+    grid = all(int(x.get("grid", 0)) for x in bst)
+    bpr = (52.0 + (8.0 if grid else 32.0) * box / rays_batch + 16.0 * prim / rays_batch
+           if rays_batch else None)
+    achieved = rays_batch * bpr / (ms_batch / 1e3) / 1e9 if bpr else None
+    line = {
+        "metric": "Mrays/s (c4: 64-frame set, batched)", "value": value, "unit": "Mrays/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_batch / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": f"config4: 64 frames, 1e4-5e5 spheres at the 1M-sphere "
+                               f"scene's density, 512^2/768^2/1024^2, {spp} spp, 1 light "
+                               "sample; one PathBatch vs 64 sequential Path.sample calls",
+                   "frames": len(frames), "spp": spp,
+                   "autotune": {"options": tuned, "probe_ms": probe_ms,
+                                "settings_measured": len(tuner.log), "seconds": tune_s},
+                   "spheres": int(sum(len(s.geometry[0].position[:]) for s, _, _ in frames)),
+                   "pixels": int(sum(w * h for _, w, h in frames)),
+                   "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2 (64 scenes, 2.4 GB path state)"},
+        "plain": {"value": value_plain, "ms_per_step": ms_plain / args.steps,
+                  "e2e_ms_per_step": e2e_p},
+        "plain_per_sample": {"value": value_per_sample,
+                             "ms_per_step": ms_per_sample / max(1, args.steps // 2),
+                             "form": "fresnel's Path.sample: one render call per sample"},
+        "batched_over_plain": value / value_plain,
+        "batched_over_plain_per_sample": value / value_per_sample,
+        "e2e_batched_over_plain": e2e_p / e2e_b,
+        "max_abs_image_difference": diff,
+        "max_abs_image_difference_per_sample": diff_per_sample,
+        "rays_per_frame_set": rays_frame_set,
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm if achieved else None, "traffic": None,
+                     "peak_source": peak_kind, "kernel": "whole batch graph (all kernels)",
+                     "bytes_per_ray": bpr,
+                     "bytes_per_ray_basis": "sphere grids walked, engine counters"
+                     if grid else "structures walked, engine counters"},
+        "clocks": clk.summary(),
+        "e2e": {"value": barrier_sum(rays_frame_set) / (e2e_b / 1e3) / 1e6,
+                "unit": "Mrays/s", "h2d_bytes_per_step": int(in_bytes),
+                "d2h_bytes_per_step": int(out_bytes), "ms_per_step": e2e_b},
+        "batch_stats": batch.stats,
+        "cpu_baseline": None,
+    }
+    if rank == 0 and emit:
         print(json.dumps(line))
-    return 0
+    return line
 
 
-def run_serving_bench(args, world, rank, barrier_max, barrier_sum, clock_index):
+def run_serving_bench(args, world, rank, barrier_max, barrier_sum, clock_index, emit=True,
+                      rates=(10.0, 50.0, 100.0, 250.0, 500.0), window=4.0, per_sample=True):
     """Serving trace (config5): Poisson arrivals at 10-500 requests/s over 32 resident scenes of
     1e3-2e6 primitives (spheres and bonds), 256^2-1080p, 1-64 spp.  The continuous-batching
-    server against the same requests served one at a time by plain Path.sample calls; both are
-    real-time (a request exists only from its arrival on) and read each image back.  Every
-    request's image is compared between the two (identical by construction)."""
+    server against the same requests served one at a time by plain Path.sample calls, and (with
+    ``per_sample``) by fresnel's own form of Path.sample, one render call per sample
+    (fresnel/tracer.py:250-260); all are real-time (a request exists only from its arrival on)
+    and read each image back.  Every request's image is compared between the server and the
+    plain run (identical by construction).  Returns the JSON line (printed by rank 0 when
+    ``emit``); the headline figures are those of the highest rate."""
     import numpy
 
     import fresnel_b200 as fresnel
     from fresnel_b200 import serving, workloads
     device = fresnel.Device(mode="gpu", n=1)
-    rates = [10.0, 50.0, 100.0, 250.0, 500.0]
-    window = 4.0  # seconds of arrivals per rate
+    rates = list(rates)
     _, sizes = workloads.config5(rates[0], 1)
     t0 = time.perf_counter()
     scenes = {k: workloads.serving_scene(device, n, seed=4000 + k) for k, n in sizes.items()}
@@ -579,37 +619,52 @@ def run_serving_bench(args, world, rank, barrier_max, barrier_sum, clock_index):
             row["served_over_plain_throughput"] = (row["served"]["mrays_per_s"] /
                                                    max(row["plain"]["mrays_per_s"], 1e-9))
             row["plain_over_served_p99"] = row["plain"]["p99_ms"] / row["served"]["p99_ms"]
+            if per_sample:
+                each, _ = workloads.config5(rate, n)
+                serving.plain_trace(engine, lambda k: scenes[k], each, per_sample=True)
+                row["plain_per_sample"] = serving.latency_summary(each)
+                row["plain_per_sample"]["identical_images"] = sum(
+                    int(numpy.array_equal(a.image, b.image)) for a, b in zip(reqs, each))
+                row["served_over_plain_per_sample_throughput"] = (
+                    row["served"]["mrays_per_s"] /
+                    max(row["plain_per_sample"]["mrays_per_s"], 1e-9))
+                row["plain_per_sample_over_served_p99"] = (
+                    row["plain_per_sample"]["p99_ms"] / row["served"]["p99_ms"])
             results.append(row)
             top = row
-    if rank == 0:
-        sv, pl = top["served"], top["plain"]
-        line = {
-            "metric": "serving (c5): Mrays/s and p50/p99 time-to-image, continuous batching vs "
-                      "plain", "value": sv["mrays_per_s"], "unit": "Mrays/s",
-            "n_gpus": world, "steps": len(rates), "warmup": 1,
-            "ms_per_step": sv["span_s"] * 1e3 / sv["requests"], "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": {"workload": "config5: Poisson arrivals at 10-500 requests/s, 32 resident "
-                                   "scenes of 1e3-2e6 primitives (80% spheres, 20% bonds), "
-                                   "256^2/640x480/1280x720/1920x1080, 1-64 spp, HBM budget "
-                                   "120 GB", "rates": rates, "window_s": window,
-                       "scene_primitives": int(sum(sizes.values())),
-                       "scene_setup_s": setup_s, "parallelism": f"replicas{world}",
-                       "l2": "inputs larger than L2 (32 resident scenes)"},
-            "p50_ms": sv["p50_ms"], "p99_ms": sv["p99_ms"],
-            "plain": {"mrays_per_s": pl["mrays_per_s"], "p50_ms": pl["p50_ms"],
-                      "p99_ms": pl["p99_ms"]},
-            "rates": results,
-            "gpu_launches": launches,
-            "roofline": None,
-            "clocks": clk.summary(),
-            "e2e": {"value": sv["mrays_per_s"], "unit": "Mrays/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": int(top["image_bytes"] / top["requests"]),
-                    "note": "the served path is end to end: requests in, sRGB images read back"},
-            "cpu_baseline": None,
-        }
+    sv, pl = top["served"], top["plain"]
+    line = {
+        "metric": "serving (c5): Mrays/s and p50/p99 time-to-image, continuous batching vs "
+                  "plain", "value": sv["mrays_per_s"], "unit": "Mrays/s",
+        "n_gpus": world, "steps": len(rates), "warmup": 1,
+        "ms_per_step": sv["span_s"] * 1e3 / sv["requests"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": "config5: Poisson arrivals, 32 resident scenes of 1e3-2e6 "
+                               "primitives (80% spheres, 20% bonds), "
+                               "256^2/640x480/1280x720/1920x1080, 1-64 spp, HBM budget "
+                               "120 GB", "rates": rates, "window_s": window,
+                   "scene_primitives": int(sum(sizes.values())),
+                   "scene_setup_s": setup_s, "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2 (32 resident scenes)"},
+        "p50_ms": sv["p50_ms"], "p99_ms": sv["p99_ms"],
+        "plain": {"mrays_per_s": pl["mrays_per_s"], "p50_ms": pl["p50_ms"],
+                  "p99_ms": pl["p99_ms"]},
+        "rates": results,
+        "gpu_launches": launches,
+        "roofline": None,
+        "clocks": clk.summary(),
+        "e2e": {"value": sv["mrays_per_s"], "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": int(top["image_bytes"] / top["requests"]),
+                "note": "the served path is end to end: requests in, sRGB images read back"},
+        "cpu_baseline": None,
+    }
+    if "plain_per_sample" in top:
+        pp = top["plain_per_sample"]
+        line["plain_per_sample"] = {"mrays_per_s": pp["mrays_per_s"], "p50_ms": pp["p50_ms"],
+                                    "p99_ms": pp["p99_ms"]}
+    if rank == 0 and emit:
         print(json.dumps(line))
-    return 0
+    return line
 
 
 def main():
@@ -633,12 +688,12 @@ def main():
     reps = Replicas(pg, "cuda")
     barrier_max, barrier_sum = reps.max, reps.sum
 
+    clock_index = int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0)
     if wl.key in ("c4", "c5"):
         run = run_batch_bench if wl.key == "c4" else run_serving_bench
-        rc = run(args, world, rank, barrier_max, barrier_sum,
-                 int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0))
+        run(args, world, rank, barrier_max, barrier_sum, clock_index)
         reps.close()
-        return rc
+        return 0
 
     device = fresnel.Device(mode="gpu", n=1)
     scene = wl.build(device)
@@ -819,9 +874,105 @@ def main():
                                "extend_launches": st["extend_launches"],
                                "primary_rays": primary_rays, "extension_rays": ext_rays,
                                "primary_kernel": primary_name, "extension_kernel": ext_name}
+    extras = None
+    if wl.key == "c2" and not args.trace_only and not args.no_extras:
+        extras = run_extras(args, wl, fresnel, device, world, rank, barrier_max, barrier_sum,
+                            clock_index)
+    if rank == 0:
+        if extras:
+            line["also"] = extras
         print(json.dumps(line))
     reps.close()
     return 0
+
+
+def bvh_frames(args, wl, fresnel, device, rank, barrier_max, barrier_sum, steps=4, warmup=2):
+    """The headline frame traced through the LBVH (device option accel = 0) instead of the
+    sphere grid: Mrays/s over ``steps`` frames, the per-kernel device times of the same frames
+    rendered again, and the dominant kernel's fraction on the reference BVH's algorithmic bytes
+    per ray (the structure this run walks is a BVH too)."""
+    dd = device._device
+    old = dd.getOption("accel")
+    dd.setOption("accel", 0)
+    try:
+        scene = wl.build(device)
+        tracer = fresnel.tracer.Path(device, w=wl.w, h=wl.h)
+        tracer.seed = 1000 * rank + 500
+        scene._scene.build()
+
+        def frame():
+            tracer.sample(scene, samples=wl.spp, light_samples=wl.light_samples)
+        for _ in range(warmup):
+            frame()
+        tracer._tracer.resetStats()
+        dd.synchronize()
+        dd.timerStart()
+        for _ in range(steps):
+            frame()
+        ms = dd.timerStop()
+        st = tracer._tracer.getStats()
+        dd.setProfiling(True)
+        tracer._tracer.resetStats()
+        for _ in range(steps):
+            frame()
+        dd.synchronize()
+        pst = tracer._tracer.getStats()
+        dd.setProfiling(False)
+        assert not st.get("grid", 0), "the LBVH frame was traced through a grid"
+    finally:
+        dd.setOption("accel", old)
+    rays = float(st["rays"])
+    ms_max = barrier_max(ms)
+    value = barrier_sum(rays) / (ms_max / 1e3) / 1e6
+    primary_rays = float(wl.w * wl.h * wl.spp * steps)
+    kern = {"primary": (primary_rays, pst["primary_ms"], pst["primary_launches"]),
+            "extension": (max(0.0, rays - primary_rays), pst["extend_ms"],
+                          pst["extend_launches"]),
+            "shade": (0.0, pst["shade_ms"], pst["shade_launches"])}
+    dom = max(("primary", "extension"), key=lambda k: kern[k][1])
+    dom_rays, dom_ms, _ = kern[dom]
+    hbm, peak_kind = peaks()
+    achieved = dom_rays * wl.bytes_per_ray / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else None
+    names = {"primary": "k_path_primary_shade" if dd.getOption("fuse_shade") else
+             "k_path_primary", "extension": "k_path_extend" if pst["shade_launches"] else
+             "k_path_bounce", "shade": "k_path_shade"}
+    return {"workload": wl.desc.format(w=wl.w, h=wl.h, spp=wl.spp) + ", traced through the "
+                        "LBVH (accel = 0)",
+            "value": value, "unit": "Mrays/s", "ms_per_step": ms_max / steps, "steps": steps,
+            "warmup": warmup, "rays_per_frame": rays / steps,
+            "kernels_ms_per_frame": {names[k]: v[1] / steps for k, v in kern.items()},
+            "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved,
+                         "peak": hbm, "peak_source": peak_kind, "unit": "GB/s",
+                         "frac": achieved / hbm if achieved else None,
+                         "bytes_per_ray": wl.bytes_per_ray,
+                         "bytes_per_ray_basis": "reference BVH: 52 + 32 A + S P, oracle counts",
+                         "box_tests_per_ray_run": float(st["box_tests"]) / rays,
+                         "prim_tests_per_ray_run": float(st["prim_tests"]) / rays}}
+
+
+def run_extras(args, wl, fresnel, device, world, rank, barrier_max, barrier_sum, clock_index):
+    """Further measured configurations reported under "also" by the default run, so that one
+    timed run covers them: the headline frame through the LBVH, the 64-frame batched set
+    (config4) against plain and per-sample calls, and serving (config5) at 100 requests/s with
+    p50/p99 against plain and per-sample serving.  A failure is reported, not raised."""
+    out = {}
+    small = argparse.Namespace(**vars(args))
+    small.steps, small.warmup, small.spp = 2, 1, None
+    for key, fn in (
+            ("c2_bvh", lambda: bvh_frames(args, wl, fresnel, device, rank, barrier_max,
+                                          barrier_sum)),
+            ("c4_batched", lambda: run_batch_bench(small, world, rank, barrier_max, barrier_sum,
+                                                   clock_index, emit=False)),
+            ("c5_serving", lambda: run_serving_bench(small, world, rank, barrier_max,
+                                                     barrier_sum, clock_index, emit=False,
+                                                     rates=(100.0,), window=3.0))):
+        t0 = time.perf_counter()
+        try:
+            out[key] = fn()
+        except Exception as e:  # an extra must not hide the headline result
+            out[key] = {"error": f"{type(e).__name__}: {str(e)[:300]}"}
+        out[key]["wall_s"] = time.perf_counter() - t0
+    return out
 
 
 if __name__ == "__main__":

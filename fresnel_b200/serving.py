@@ -296,9 +296,11 @@ def serve_trace(server, requests, realtime=True):
 
 
 def plain_trace(engine, scene_of, requests, realtime=True, clock=time.perf_counter,
-                keep_linear=False):
+                keep_linear=False, per_sample=False):
     """Baseline: the same requests served one at a time in arrival order, each by one plain
-    ``Path.sample`` call on its own (pooled) tracer, image read back after the call."""
+    ``Path.sample`` call on its own (pooled) tracer, image read back after the call.  With
+    ``per_sample`` each request is rendered the way fresnel's own ``Path.sample`` does it
+    (fresnel/tracer.py:250-260): one ``render`` call per sample, each returning the output."""
     t0 = clock()
     pool = collections.defaultdict(list)
     for r in sorted(requests, key=lambda q: q.arrival):
@@ -310,8 +312,15 @@ def plain_trace(engine, scene_of, requests, realtime=True, clock=time.perf_count
         r.t_admit = clock()
         engine.start(t, r.seed)
         before = engine.rays(t)
-        t.sample(scene_of(r.scene_key), samples=r.samples, reset=False,
-                 light_samples=r.light_samples)
+        if per_sample:
+            scene = scene_of(r.scene_key)
+            t._tracer.setLightSamples(r.light_samples)
+            for _ in range(r.samples):
+                t.render(scene)
+            t._tracer.setLightSamples(1)
+        else:
+            t.sample(scene_of(r.scene_key), samples=r.samples, reset=False,
+                     light_samples=r.light_samples)
         r.image, r.linear = engine.read(t, keep_linear)
         r.rays = engine.rays(t) - before
         r.done_samples = r.samples
