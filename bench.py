@@ -76,6 +76,7 @@ WORKLOADS = {
     "c3": Workload("c3", "config3: 200k spheres + 50k bonds + 20k cubes + 10k icosahedra, "
                    "{w}x{h}, {spp} spp, 1 light sample", "config3", 1280, 720, spp=128,
                    box_tests=43.51, prim_tests=1.86, prim_bytes=28),
+    "tour": Workload("tour", "kernel tour", "config2", 1920, 1080),
 }
 
 
@@ -694,6 +695,12 @@ def main():
         run(args, world, rank, barrier_max, barrier_sum, clock_index)
         reps.close()
         return 0
+    if wl.key == "tour":
+        line = run_tour(fresnel)
+        if rank == 0:
+            print(json.dumps(line))
+        reps.close()
+        return 0
 
     device = fresnel.Device(mode="gpu", n=1)
     scene = wl.build(device)
@@ -884,6 +891,57 @@ def main():
         print(json.dumps(line))
     reps.close()
     return 0
+
+
+def run_tour(fresnel):
+    """One pass over every kernel family on cases of a few GB at most (the input of a
+    per-kernel profiler capture): the LBVH build of the 1M-sphere scene, its sphere-grid build,
+    Preview of it at 1920x1080 with 8x8 anti-aliasing through the grid, a 480x270 16-spp path
+    render (the fold), the histogram of a 1080p image, a batch of 4 sphere-grid frames and a
+    batch of a mixed scene.  Prints the device time of each stage."""
+    from fresnel_b200 import workloads
+    dev = fresnel.Device(mode="gpu", n=1)
+    dd = dev._device
+    dd.setOption("path_slots", 4 << 20)
+    out = {}
+
+    def stage(name, fn):
+        dd.synchronize()
+        dd.timerStart()
+        fn()
+        out[name + "_ms"] = dd.timerStop()
+    dd.setOption("accel", 0)
+    s_bvh = workloads.config2(dev)
+    stage("lbvh_build_1m", s_bvh._scene.build)
+    dd.setOption("accel", 1)
+    s_grid = workloads.config2(dev)
+    stage("grid_build_1m", s_grid._scene.build)
+    p = fresnel.tracer.Preview(dev, w=1920, h=1080, anti_alias=True)
+    stage("preview_1080p_aa8", lambda: p.render(s_grid))
+    t = fresnel.tracer.Path(dev, w=480, h=270)
+    stage("path_480x270_16spp", lambda: t.sample(s_grid, samples=16))
+    t2 = fresnel.tracer.Path(dev, w=1920, h=1080)
+    t2.sample(s_grid, samples=1)
+    stage("histogram_1080p", t2.histogram)
+    dd.setOption("accel", 2)
+    frames = workloads.config4(dev, n_frames=4, seed=3)
+    b = fresnel.tracer.PathBatch(dev)
+    tracers = [fresnel.tracer.Path(dev, w=w // 2, h=h // 2) for _, w, h in frames]
+
+    def batch_frames():
+        for (s, _, _), tr in zip(frames, tracers):
+            b.add(tr, s, samples=4)
+        b.render()
+    stage("batch_4_frames", batch_frames)
+    mix = workloads.config3(dev, scale=0.05)
+    b2 = fresnel.tracer.PathBatch(dev)
+    tr = fresnel.tracer.Path(dev, w=320, h=180)
+
+    def batch_mixed():
+        b2.add(tr, mix, samples=4)
+        b2.render()
+    stage("batch_mixed", batch_mixed)
+    return {"metric": "kernel tour: device ms per stage", "stages": out}
 
 
 def bvh_frames(args, wl, fresnel, device, rank, barrier_max, barrier_sum, steps=4, warmup=2):

@@ -164,6 +164,7 @@ struct fr_device {
     int refill = 0;                        // extension rays with per-lane refill
     int accel = 2;                         // sphere grid: 0 never, 1 whenever possible, 2 auto
     int fuse_shade = 1;                    // primary rays shaded in the primary pass
+    int tail_after = 2;                    // fused bounce launches before the tail kernel (0: none)
     float grid_cells_per_prim = 1.5f;      // grid cells per sphere
     std::vector<fr_scene*> scenes;         // to mark BVHs stale when a build option changes
     void* static_path = nullptr;           // this device's copy of g_static_path (looked up once)
@@ -1125,6 +1126,10 @@ fr_status fr_device_set_option(fr_device* d, const char* name, double value)
         if (!(value == 0.0 || value == 1.0 || value == 2.0))
             return fail(FR_ERR_INVALID, "fuse_shade must be 0, 1 or 2");
         d->fuse_shade = int(value);
+    } else if (n == "tail") {
+        if (!(value >= 0.0 && value <= 64.0 && value == double(int(value))))
+            return fail(FR_ERR_INVALID, "tail must be an integer in [0, 64]");
+        d->tail_after = int(value);
     } else if (n == "accel") {
         if (!(value == 0.0 || value == 1.0 || value == 2.0))
             return fail(FR_ERR_INVALID, "accel must be 0 (BVH), 1 (sphere grid) or 2 (automatic)");
@@ -1163,6 +1168,8 @@ fr_status fr_device_get_option(const fr_device* d, const char* name, double* val
         *value = double(d->path_slots);
     else if (n == "accel")
         *value = d->accel;
+    else if (n == "tail")
+        *value = d->tail_after;
     else if (n == "fuse_shade")
         *value = d->fuse_shade;
     else if (n == "grid_density")
@@ -1655,6 +1662,27 @@ fr_status fr_tracer_render_path(fr_tracer* t, fr_scene* sc, const fr_render_para
         // compiled for 3 blocks per SM is slower than the separate passes)
         const bool bounces =
             fused && (t->dev->fuse_shade == 2 || (P.scene.grid.n_cells != 0 && !P.refill));
+        if (bounces && t->dev->tail_after > 0) {
+            // a few bounce launches while the queues are long, then every path's remaining
+            // bounces in one launch: the wavefront needs no queue-length read-back
+            for (int b = 0; b < t->dev->tail_after; ++b, ++it) {
+                FR_CUDA(cudaMemsetAsync(S.ctr + ((it & 1) ^ 1), 0, sizeof(uint32_t), st),
+                        "clearing a queue");
+                FR_CUDA(cudaMemsetAsync(S.ctr + 2, 0, sizeof(uint32_t), st), "clearing a counter");
+                timed(2, [&] { launch_path_bounce(P, S, it, t->dev->shape, st); });
+                t->launches += 1;
+            }
+            FR_CUDA(cudaMemsetAsync(S.ctr + 2, 0, sizeof(uint32_t), st), "clearing a counter");
+            timed(2, [&] { launch_path_tail(P, S, it, t->dev->shape, st); });
+            t->launches += 1;
+            FR_CUDA(cudaGetLastError(), "launching the path tracer");
+            launch_path_fold(P, S, st);
+            t->launches++;
+            t->dev->path_k = P.batch;
+            t->dev->path_tile_log2 = P.tile_log2;
+            done += P.batch;
+            continue;
+        }
         while (true) {
             for (int b = 0; b < CHECK_EVERY; ++b, ++it) {
                 if (bounces) {
@@ -1692,7 +1720,9 @@ fr_status fr_tracer_render_path(fr_tracer* t, fr_scene* sc, const fr_render_para
         t->dev->path_tile_log2 = P.tile_log2;
         done += P.batch;
     }
-    return check_status(t->dev);
+    s = check_status(t->dev);
+    t->collect();  // the stream is synchronised: profiling events of the tail launches are done
+    return s;
 }
 
 // ---------------------------------------------------------------------------------------------

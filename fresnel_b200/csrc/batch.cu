@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(256) k_batch_shade(BatchDev B, int in_q, int o
         bool push = false;
         uint32_t p = 0;
         if (idx < count) {
-            p = inq[idx];
+            p = ld_cs(inq + (idx));
             const WaveJob& J = B.jobs[find_job<&WaveJob::slot_base>(B.jobs, f0, f1, p)];
             push = shade_pixel(J.P, S, p, p - J.slot_base);
         }
@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(256) k_batch_shade(BatchDev B, int in_q, int o
                 at = atomicAdd(outc, uint32_t(__popc(m)));
             at = __shfl_sync(0xffffffffu, at, 0);
             if (push)
-                outq[at + __popc(m & ((1u << lane) - 1u))] = p;
+                st_cs(outq + (at + __popc(m & ((1u << lane) - 1u))), p);
         }
     }
 }
@@ -140,12 +140,12 @@ __global__ void __launch_bounds__(256) k_batch_extend(BatchDev B, int q)
         const bool act = idx < count;
         uint32_t jb = 0;
         if (act) {
-            const uint32_t p = queue[idx];
+            const uint32_t p = ld_cs(queue + (idx));
             jb = find_job<&WaveJob::slot_base>(B.jobs, f0, f1, p);
-            const V3 o = xyz(S.ray_o[p]);
-            const V3 d = xyz(S.ray_d[p]);
+            const V3 o = xyz(ld_cs(S.ray_o + (p)));
+            const V3 d = xyz(ld_cs(S.ray_d + (p)));
             Hit h = trace_closest<WIDTH, MASK>(B.jobs[jb].P.scene, o, d, PATH_TNEAR, tc);
-            S.hit[p] = make_uint2(h.geom, h.prim);
+            st_cs(S.hit + (p), make_uint2(h.geom, h.prim));
         }
         // rays per render, one atomic per render present in the warp
         const uint32_t am = __ballot_sync(0xffffffffu, act);
@@ -213,7 +213,7 @@ __global__ void __launch_bounds__(256, fused_blocks(MASK)) k_batch_bounce(BatchD
         uint32_t jb = 0, p = 0;
         bool push = false;
         if (act) {
-            p = queue[idx];
+            p = ld_cs(queue + (idx));
             jb = find_job<&WaveJob::slot_base>(B.jobs, f0, f1, p);
             push = bounce<WIDTH, MASK>(B.jobs[jb].P, S, p, p - B.jobs[jb].slot_base, tc);
         }

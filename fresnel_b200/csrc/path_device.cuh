@@ -15,6 +15,20 @@ __device__ __forceinline__ float4 f4(V3 a) { return make_float4(a.x, a.y, a.z, 0
 __device__ __forceinline__ float4 f4(C3 a) { return make_float4(a.r, a.g, a.b, 0.0f); }
 __device__ __forceinline__ C3 rgb3(float4 a) { return c3(a.x, a.y, a.z); }
 
+// Path-state and queue accesses are streamed: each slot's values are read and written once per
+// pass, and the wavefront (gigabytes) is far larger than L2, so they are loaded and stored with
+// the evict-first (.cs) policy, which leaves L2 to the scene and its acceleration structure.
+template <class T>
+__device__ __forceinline__ T ld_cs(const T* a)
+{
+    return __ldcs(a);
+}
+template <class T>
+__device__ __forceinline__ void st_cs(T* a, T v)
+{
+    __stcs(a, v);
+}
+
 // Work items of the primary pass: T x T-pixel tiles in row-major order (T = 2^tl, 8 by
 // default), a tile's pixels in row-major order, and the K samples of a pixel innermost. A warp
 // then traces two pixels' 16 samples (K = 16) or an 8x4 block of pixels (K = 1, T = 8): its
@@ -128,27 +142,27 @@ __device__ __forceinline__ void shade_load(const FrameParams& P, const PathState
     L.p = p;
     L.pixel = pi.j * P.w + pi.i;
     L.n_samples = P.n_samples + pi.k;
-    const uint2 ld = S.ls_depth[p];
+    const uint2 ld = ld_cs(S.ls_depth + (p));
     L.ls = ld.x;
     L.s.depth = ld.y;
     if (ld.x == 0u && ld.y == 0u) {
         L.s.result = c3(0.0f, 0.0f, 0.0f);
         L.s.att = c3(1.0f, 1.0f, 1.0f);
     } else {
-        L.s.result = rgb3(S.result[p]);
-        L.s.att = rgb3(S.att[p]);
+        L.s.result = rgb3(ld_cs(S.result + (p)));
+        L.s.att = rgb3(ld_cs(S.att + (p)));
     }
     L.s.origin = v3(0, 0, 0);
     L.s.dir = v3(0, 0, 0);
-    L.ph = S.prim_hit[p];
+    L.ph = ld_cs(S.prim_hit + (p));
     if (ld.y == 0u) {
-        L.ro = xyz(S.prim_o[p]);
-        L.rd = xyz(S.prim_d[p]);
+        L.ro = xyz(ld_cs(S.prim_o + (p)));
+        L.rd = xyz(ld_cs(S.prim_d + (p)));
         L.h = L.ph;
     } else {
-        L.ro = xyz(S.ray_o[p]);
-        L.rd = xyz(S.ray_d[p]);
-        L.h = S.hit[p];
+        L.ro = xyz(ld_cs(S.ray_o + (p)));
+        L.rd = xyz(ld_cs(S.ray_d + (p)));
+        L.h = ld_cs(S.hit + (p));
     }
     L.have_sf = false;
 }
@@ -179,11 +193,11 @@ __device__ __forceinline__ ShadeStep shade_step(const FrameParams& P, const Path
     const uint32_t p = L.p;
     if (!s.done) {
         s.depth += 1u;
-        S.ray_o[p] = f4(s.origin);
-        S.ray_d[p] = f4(s.dir);
-        S.att[p] = f4(s.att);
-        S.result[p] = f4(s.result);
-        S.ls_depth[p] = make_uint2(L.ls, s.depth);
+        st_cs(S.ray_o + (p), f4(s.origin));
+        st_cs(S.ray_d + (p), f4(s.dir));
+        st_cs(S.att + (p), f4(s.att));
+        st_cs(S.result + (p), f4(s.result));
+        st_cs(S.ls_depth + (p), make_uint2(L.ls, s.depth));
         return STEP_CONTINUE;
     }
     if (L.ls + 1u < P.light_samples) {
@@ -191,8 +205,8 @@ __device__ __forceinline__ ShadeStep shade_step(const FrameParams& P, const Path
         if (s.depth == 0) {  // the next light sample starts from this same vertex
             L.have_sf = true;
         } else {
-            L.ro = xyz(S.prim_o[p]);
-            L.rd = xyz(S.prim_d[p]);
+            L.ro = xyz(ld_cs(S.prim_o + (p)));
+            L.rd = xyz(ld_cs(S.prim_d + (p)));
             L.h = L.ph;
             L.have_sf = false;
         }
@@ -201,7 +215,7 @@ __device__ __forceinline__ ShadeStep shade_step(const FrameParams& P, const Path
         return STEP_RESTART;
     }
     C3 out = c_div_recip(s.result, float(P.light_samples));
-    S.sample[p] = make_float4(out.r, out.g, out.b, L.ph.x == MISS ? P.bg_alpha : 1.0f);
+    st_cs(S.sample + (p), make_float4(out.r, out.g, out.b, L.ph.x == MISS ? P.bg_alpha : 1.0f));
     return STEP_FINISHED;
 }
 
@@ -234,16 +248,16 @@ __device__ __forceinline__ bool shade_pixel(const FrameParams& P, const PathStat
 __device__ __forceinline__ bool primary_finish(const FrameParams& P, const PathState& S,
                                                uint32_t slot, V3 o, V3 d, Hit h)
 {
-    S.prim_hit[slot] = make_uint2(h.geom, h.prim);
+    st_cs(S.prim_hit + (slot), make_uint2(h.geom, h.prim));
     if (h.geom == MISS) {
         C3 res = P.bg * float(P.light_samples);
         C3 out = c_div_recip(res, float(P.light_samples));
-        S.sample[slot] = make_float4(out.r, out.g, out.b, P.bg_alpha);
+        st_cs(S.sample + (slot), make_float4(out.r, out.g, out.b, P.bg_alpha));
         return false;
     }
-    S.prim_o[slot] = f4(o);
-    S.prim_d[slot] = f4(d);
-    S.ls_depth[slot] = make_uint2(0u, 0u);
+    st_cs(S.prim_o + (slot), f4(o));
+    st_cs(S.prim_d + (slot), f4(d));
+    st_cs(S.ls_depth + (slot), make_uint2(0u, 0u));
     return true;
 }
 
@@ -269,16 +283,16 @@ __device__ __forceinline__ bool primary_shade(const FrameParams& P, const PathSt
     camera_ray(P.cam, it.i, it.j, P.n_samples + it.k, o, d);
     Hit h = trace_closest<WIDTH, MASK>(P.scene, o, d, PATH_TNEAR, tc);
     const uint2 ph = make_uint2(h.geom, h.prim);
-    S.prim_hit[slot] = ph;
+    st_cs(S.prim_hit + (slot), ph);
     if (h.geom == MISS) {
         C3 res = P.bg * float(P.light_samples);
         C3 out = c_div_recip(res, float(P.light_samples));
-        S.sample[slot] = make_float4(out.r, out.g, out.b, P.bg_alpha);
+        st_cs(S.sample + (slot), make_float4(out.r, out.g, out.b, P.bg_alpha));
         return false;
     }
     if (P.light_samples > 1u) {  // later light samples restart from the primary ray
-        S.prim_o[slot] = f4(o);
-        S.prim_d[slot] = f4(d);
+        st_cs(S.prim_o + (slot), f4(o));
+        st_cs(S.prim_d + (slot), f4(d));
     }
     ShadeLane L;
     L.p = slot;
@@ -306,22 +320,22 @@ template <int WIDTH, uint32_t MASK>
 __device__ __forceinline__ bool bounce(const FrameParams& P, const PathState& S, uint32_t p,
                                        uint32_t local, TraceCount& tc)
 {
-    const V3 o = xyz(S.ray_o[p]);
-    const V3 d = xyz(S.ray_d[p]);
+    const V3 o = xyz(ld_cs(S.ray_o + (p)));
+    const V3 d = xyz(ld_cs(S.ray_d + (p)));
     const Hit hit = trace_closest<WIDTH, MASK>(P.scene, o, d, PATH_TNEAR, tc);
     const PrimaryItem pi = primary_item(local, P.w, P.h, P.batch, P.tile_log2);
-    const uint2 ld = S.ls_depth[p];
+    const uint2 ld = ld_cs(S.ls_depth + (p));
     ShadeLane L;
     L.p = p;
     L.pixel = pi.j * P.w + pi.i;
     L.n_samples = P.n_samples + pi.k;
     L.ls = ld.x;
     L.s.depth = ld.y;
-    L.s.result = rgb3(S.result[p]);
-    L.s.att = rgb3(S.att[p]);
+    L.s.result = rgb3(ld_cs(S.result + (p)));
+    L.s.att = rgb3(ld_cs(S.att + (p)));
     L.s.origin = v3(0, 0, 0);
     L.s.dir = v3(0, 0, 0);
-    L.ph = S.prim_hit[p];
+    L.ph = ld_cs(S.prim_hit + (p));
     L.h = make_uint2(hit.geom, hit.prim);
     L.ro = o;
     L.rd = d;
@@ -340,7 +354,7 @@ __device__ __forceinline__ void push_queue(const PathState& S, int q, bool push,
             at = atomicAdd(S.ctr + q, uint32_t(__popc(m)));
         at = __shfl_sync(0xffffffffu, at, 0);
         if (push)
-            S.queue[q][at + __popc(m & ((1u << lane) - 1u))] = slot;
+            st_cs(S.queue[q] + (at + __popc(m & ((1u << lane) - 1u))), slot);
     }
 }
 
@@ -355,7 +369,7 @@ __device__ __forceinline__ void push_primary(const PathState& S, bool push, uint
             at = atomicAdd(S.ctr + 1, uint32_t(__popc(m)));
         at = __shfl_sync(0xffffffffu, at, 0);
         if (push)
-            S.queue[1][at + __popc(m & ((1u << lane) - 1u))] = slot;
+            st_cs(S.queue[1] + (at + __popc(m & ((1u << lane) - 1u))), slot);
     }
 }
 

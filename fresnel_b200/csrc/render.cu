@@ -165,15 +165,15 @@ struct PrimarySource {
         bool push = false;
         if (done) {
             uint32_t prim = L.hit_geom == MISS ? 0u : __ldg(P.scene.geoms[L.hit_geom].order + L.hit_slot);
-            S.prim_hit[slot] = make_uint2(L.hit_geom, prim);
+            st_cs(S.prim_hit + (slot), make_uint2(L.hit_geom, prim));
             if (L.hit_geom == MISS) {
                 C3 res = P.bg * float(P.light_samples);
                 C3 out = c_div_recip(res, float(P.light_samples));
-                S.sample[slot] = make_float4(out.r, out.g, out.b, P.bg_alpha);
+                st_cs(S.sample + (slot), make_float4(out.r, out.g, out.b, P.bg_alpha));
             } else {
-                S.prim_o[slot] = f4(L.ray.o);
-                S.prim_d[slot] = f4(L.ray.d);
-                S.ls_depth[slot] = make_uint2(0u, 0u);  // see primary_finish
+                st_cs(S.prim_o + (slot), f4(L.ray.o));
+                st_cs(S.prim_d + (slot), f4(L.ray.d));
+                st_cs(S.ls_depth + (slot), make_uint2(0u, 0u));  // see primary_finish
                 push = true;
             }
         }
@@ -185,7 +185,7 @@ struct PrimarySource {
                 at = atomicAdd(S.ctr + 1, uint32_t(__popc(m)));
             at = __shfl_sync(0xffffffffu, at, 0);
             if (push)
-                S.queue[1][at + __popc(m & ((1u << lane) - 1u))] = slot;
+                st_cs(S.queue[1] + (at + __popc(m & ((1u << lane) - 1u))), slot);
         }
     }
 };
@@ -197,15 +197,15 @@ struct ExtendSource {
     uint32_t slot;
     __device__ bool begin(uint32_t item, LaneRay& L)
     {
-        slot = queue[item];
-        lane_begin(L, xyz(S.ray_o[slot]), xyz(S.ray_d[slot]), PATH_TNEAR);
+        slot = ld_cs(queue + (item));
+        lane_begin(L, xyz(ld_cs(S.ray_o + (slot))), xyz(ld_cs(S.ray_d + (slot))), PATH_TNEAR);
         return true;
     }
     __device__ void finish(bool done, uint32_t, const LaneRay& L)
     {
         if (done) {
             uint32_t prim = L.hit_geom == MISS ? 0u : __ldg(P.scene.geoms[L.hit_geom].order + L.hit_slot);
-            S.hit[slot] = make_uint2(L.hit_geom, prim);
+            st_cs(S.hit + (slot), make_uint2(L.hit_geom, prim));
         }
     }
 };
@@ -336,7 +336,7 @@ __global__ void __launch_bounds__(256, MINB) k_path_shade(FrameParams P, PathSta
                 const uint32_t k = taken + __popc(idle & below);
                 const uint32_t idx = (warp + (k >> 5) * n_warps) * 32u + (k & 31u);
                 if (idx < count) {
-                    const uint32_t p = inq[idx];
+                    const uint32_t p = ld_cs(inq + (idx));
                     shade_load(P, S, p, p, L);
                     busy = true;
                 }
@@ -403,11 +403,11 @@ __global__ void __launch_bounds__(256) k_path_extend(FrameParams P, PathState S,
         for (uint32_t sub = 0; sub < CHUNK; sub += 32) {
             uint32_t idx = base + sub + lane;
             if (idx < count) {
-                uint32_t p = queue[idx];
-                V3 o = xyz(S.ray_o[p]);
-                V3 d = xyz(S.ray_d[p]);
+                uint32_t p = ld_cs(queue + (idx));
+                V3 o = xyz(ld_cs(S.ray_o + (p)));
+                V3 d = xyz(ld_cs(S.ray_d + (p)));
                 Hit h = trace_closest<WIDTH, MASK>(P.scene, o, d, PATH_TNEAR, tc);
-                S.hit[p] = make_uint2(h.geom, h.prim);
+                st_cs(S.hit + (p), make_uint2(h.geom, h.prim));
             }
         }
         if (lane == 0)
@@ -438,13 +438,73 @@ __global__ void __launch_bounds__(256, fused_blocks(MASK)) k_path_bounce(FramePa
         bool push = false;
         uint32_t p = 0;
         if (idx < count) {
-            p = queue[idx];
+            p = ld_cs(queue + (idx));
             push = bounce<WIDTH, MASK>(P, S, p, p, tc);
         }
         push_queue(S, q ^ 1, push, p);
         if (lane == 0)
             atomicAdd(P.stats + 0, (unsigned long long)min(32u, count - base));
     }
+    flush_counts(tc, P.stats + 3);
+}
+
+// The tail of a wavefront's bounces in one launch (sphere-grid scenes): once the early bounces
+// have retired most paths, the launches of later bounces carry few rays each and every launch
+// lasts as long as its longest grid walk.  Here each lane follows its path bounce after bounce
+// (trace, shade, store, read back) until the path finishes, then takes the next path of queue q
+// (lanes that are idle together share one atomic), so the walks of different bounces overlap
+// instead of being serialised launch by launch.  Every path runs the same per-bounce arithmetic
+// as in k_path_bounce.  The work counter (ctr[2]) must be zero at launch; no queue is written.
+// A path longer than TAIL_MAX_DEPTH further bounces is cut and reported (never reached: Russian
+// roulette ends paths long before).
+constexpr uint32_t TAIL_MAX_DEPTH = 1u << 16;
+
+template <int WIDTH, uint32_t MASK>
+__global__ void __launch_bounds__(256, fused_blocks(MASK)) k_path_tail(FrameParams P, PathState S, int q)
+{
+    const uint32_t count = S.ctr[q];
+    const uint32_t* queue = S.queue[q];
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t below = (1u << lane) - 1u;
+    TraceCount tc;
+    bool active = false, exhausted = false;
+    uint32_t p = 0, guard = 0;
+    unsigned long long rays = 0;
+    while (true) {
+        const uint32_t idle = __ballot_sync(0xffffffffu, !active);
+        if (idle && !exhausted) {
+            const uint32_t n = uint32_t(__popc(idle));
+            uint32_t base = 0;
+            if (lane == 0)
+                base = atomicAdd(S.ctr + 2, n);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (base + n >= count)
+                exhausted = true;
+            if (!active) {
+                const uint32_t item = base + uint32_t(__popc(idle & below));
+                if (item < count) {
+                    p = ld_cs(queue + item);
+                    active = true;
+                    guard = TAIL_MAX_DEPTH;
+                }
+            }
+        }
+        if (__ballot_sync(0xffffffffu, active) == 0u)
+            break;
+        if (active) {
+            ++rays;
+            if (!bounce<WIDTH, MASK>(P, S, p, p, tc)) {
+                active = false;
+            } else if (--guard == 0u) {
+                atomicOr(P.scene.status, ERR_ITERATION_CAP);
+                active = false;
+            }
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1)
+        rays += __shfl_xor_sync(0xffffffffu, rays, off);
+    if (lane == 0 && rays)
+        atomicAdd(P.stats + 0, rays);
     flush_counts(tc, P.stats + 3);
 }
 
@@ -514,8 +574,8 @@ __global__ void __launch_bounds__(256) k_path_extend_refill(FrameParams P, PathS
             if (!active) {
                 const uint32_t item = base + uint32_t(__popc(idle & below));
                 if (item < count) {
-                    p = queue[item];
-                    ray = make_rayk(xyz(S.ray_o[p]), xyz(S.ray_d[p]));
+                    p = ld_cs(queue + (item));
+                    ray = make_rayk(xyz(ld_cs(S.ray_o + (p))), xyz(ld_cs(S.ray_d + (p))));
                     nf = near_far(ray);
                     tmax = __int_as_float(0x7f800000);
                     hg = MISS;
@@ -525,7 +585,7 @@ __global__ void __launch_bounds__(256) k_path_extend_refill(FrameParams P, PathS
                     guard = n_nodes4 + 8u;
                     active = n_nodes4 != 0;
                     if (!active)
-                        S.hit[p] = make_uint2(MISS, 0u);
+                        st_cs(S.hit + (p), make_uint2(MISS, 0u));
                     ++rays;
                 }
             }
@@ -546,7 +606,7 @@ __global__ void __launch_bounds__(256) k_path_extend_refill(FrameParams P, PathS
                 uint32_t prim = 0;
                 if (hg != MISS)
                     prim = __ldg((combined ? sc.order : sc.geoms[hg].order) + hs);
-                S.hit[p] = make_uint2(hg, prim);
+                st_cs(S.hit + (p), make_uint2(hg, prim));
                 active = false;
             }
         }
@@ -591,13 +651,13 @@ __global__ void __launch_bounds__(256) k_path_extend_grid_refill(FrameParams P, 
             if (!active) {
                 const uint32_t item = base + uint32_t(__popc(idle & below));
                 if (item < count) {
-                    p = queue[item];
-                    ray = make_rayk(xyz(S.ray_o[p]), xyz(S.ray_d[p]));
+                    p = ld_cs(queue + (item));
+                    ray = make_rayk(xyz(ld_cs(S.ray_o + (p))), xyz(ld_cs(S.ray_d + (p))));
                     tmax = __int_as_float(0x7f800000);
                     slot = MISS;
                     active = grid_walk_begin(G, ray, W);
                     if (!active)
-                        S.hit[p] = make_uint2(MISS, 0u);
+                        st_cs(S.hit + (p), make_uint2(MISS, 0u));
                     ++rays;
                 }
             }
@@ -608,8 +668,8 @@ __global__ void __launch_bounds__(256) k_path_extend_grid_refill(FrameParams P, 
             continue;
         }
         if (active && !grid_walk_step(G, ray, PATH_TNEAR, tmax, slot, W, tc)) {
-            S.hit[p] = slot == MISS ? make_uint2(MISS, 0u)
-                                    : make_uint2(G.geom, __ldg(G.ref_prim + slot));
+            st_cs(S.hit + (p), slot == MISS ? make_uint2(MISS, 0u)
+                                            : make_uint2(G.geom, __ldg(G.ref_prim + slot)));
             active = false;
         }
     }
@@ -865,6 +925,18 @@ void launch_path_bounce(const FrameParams& P, const PathState& S, int iteration,
     const bool grid = P.scene.grid.n_cells != 0;
     if (grid)
         k = k_path_bounce<4, MASK_GRID>;
+    k<<<shape.bounce_grid[grid ? 1 : 0], 256, 0, st>>>(P, S, q);
+}
+
+void launch_path_tail(const FrameParams& P, const PathState& S, int iteration,
+                      const LaunchShape& shape, cudaStream_t st)
+{
+    const int q = iteration & 1;
+    auto k = pick(P, k_path_tail<2, MASK_SPHERES>, k_path_tail<2, MASK_ALL>,
+                  k_path_tail<4, MASK_SPHERES>, k_path_tail<4, MASK_ALL>);
+    const bool grid = P.scene.grid.n_cells != 0;
+    if (grid)
+        k = k_path_tail<4, MASK_GRID>;
     k<<<shape.bounce_grid[grid ? 1 : 0], 256, 0, st>>>(P, S, q);
 }
 

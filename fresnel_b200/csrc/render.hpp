@@ -87,6 +87,9 @@ void launch_path_primary_shade(const FrameParams& P, const PathState& S, cudaStr
 // zero).
 void launch_path_bounce(const FrameParams& P, const PathState& S, int iteration,
                         const LaunchShape& shape, cudaStream_t st);
+// The remaining bounces of every path in queue (iteration & 1) in one launch (k_path_tail).
+void launch_path_tail(const FrameParams& P, const PathState& S, int iteration,
+                      const LaunchShape& shape, cudaStream_t st);
 // ... then fold the batch's samples into each pixel's running mean, in sample order.
 void launch_path_fold(const FrameParams& P, const PathState& S, cudaStream_t st);
 // Diagnostic comparison of the two 4-wide traversal forms (sphere scenes).

@@ -61,3 +61,17 @@ def odd_radii_scene(device, n=3000, seed=5):
     scene.camera = fresnel.camera.Orthographic(position=(0, 0, 40), look_at=(0, 0, 0),
                                                up=(0, 1, 0), height=26)
     return scene
+
+
+def oracle_path_image(oracle_device, scene, w, h, seed, samples, light_samples=1):
+    """The oracle's Path image of ``samples`` samples (numbers 1..samples) rendered with
+    exactly ``seed`` (the seed a GPU tracer renders with after its own reset/seed schedule)."""
+    t = oracle_device.module.TracerPath(oracle_device._device, w, h, light_samples)
+    t.setSeed(seed)
+    t.renderSamples(scene._scene, samples)
+    return numpy.array(t.getLinearOutputBuffer(), copy=True)
+
+
+def same_seed_fraction(gpu_linear, oracle_linear, tol=1e-3):
+    """Fraction of pixels whose linear RGBA agree within ``tol`` in every channel."""
+    return float(numpy.all(numpy.abs(gpu_linear - oracle_linear) <= tol, axis=-1).mean())

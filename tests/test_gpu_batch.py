@@ -130,3 +130,35 @@ def test_batch_errors(gpu_device):
     assert len(batch) == 0
     batch.render()  # empty batch: nothing to do
     assert t._tracer.getNumSamples() == 0
+
+
+def test_batch_matches_oracle(gpu_device, oracle_device, small_slots):
+    """Renders batched together (several waves, mixed scenes, sizes, sample and light-sample
+    counts, mixed geometry) against the CPU oracle rendering each alone with the seed the tracer
+    renders with: >= 99% of pixels within 1e-3 (the same-seed bar of the plain Path tests)."""
+    from parity import oracle_path_image, same_seed_fraction
+    from parity_record import record
+
+    def builds():
+        return [lambda d: workloads.random_spheres(d, 300, 12.0, seed=3, outline_width=0.05),
+                lambda d: workloads.random_spheres(d, 2000, 30.0, seed=4, colors=True,
+                                                   lights=fresnel.light.lightbox()),
+                lambda d: workloads.config3(d, scale=0.005)]
+    gscenes = [b(gpu_device) for b in builds()]
+    oscenes = [b(oracle_device) for b in builds()]
+    cases = [(0, 64, 48, 6, 1), (1, 100, 80, 5, 1), (2, 72, 40, 4, 2), (1, 40, 56, 3, 3)]
+    batch = fresnel.tracer.PathBatch(gpu_device)
+    tracers = []
+    for n, (k, w, h, spp, ls) in enumerate(cases):
+        t = fresnel.tracer.Path(gpu_device, w=w, h=h)
+        t.seed = 40 + n
+        batch.add(t, gscenes[k], samples=spp, light_samples=ls)
+        tracers.append(t)
+    batch.render()
+    assert batch.stats["waves"] > 1
+    for n, ((k, w, h, spp, ls), t) in enumerate(zip(cases, tracers)):
+        ora = oracle_path_image(oracle_device, oscenes[k], w, h, 41 + n, spp, ls)
+        frac = same_seed_fraction(numpy.array(t.linear_output[:], copy=True), ora)
+        record("test_batch_matches_oracle", check="same_seed", render=n, width=w, height=h,
+               spp=spp, light_samples=ls, within_1e3=frac)
+        assert frac >= 0.99, f"render {n}: {frac:.4%} of pixels within 1e-3"

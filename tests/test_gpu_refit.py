@@ -1,5 +1,6 @@
 """BVH refit (device option "refit"): after the primitives move, the refitted tree must find the
-same closest hits as a tree built from scratch for the moved primitives.
+same closest hits as a tree built from scratch for the moved primitives, and the same ones as
+the CPU oracle rendering the moved arrays.
 
 Each case renders a scene once (building its trees), moves every primitive (positions jittered,
 radii and orientations changed, counts kept), renders again with refit on, and compares the
@@ -12,7 +13,9 @@ import pytest
 
 import fresnel_b200 as fresnel
 from fresnel_b200 import workloads
-from parity import preview_hits
+from grazing import check_hits
+from parity import oracle_path_image, preview_hits, same_seed_fraction
+from parity_record import record
 
 pytestmark = pytest.mark.gpu
 
@@ -90,3 +93,32 @@ def test_refit_matches_rebuild(name, gpu_device, refit_on):
     assert numpy.abs(refit_lin - fresh_lin).max() <= 1e-6
     close = numpy.all(numpy.abs(refit_path - numpy.array(t2.linear_output[:])) <= 1e-5, axis=-1)
     assert close.mean() >= 0.999
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_refit_matches_oracle(name, gpu_device, oracle_device, refit_on):
+    """The refitted scene against the oracle's own scene of the moved arrays (fresnel/util.py:
+    54-62 and fresnel/gpu/Scene.h:64-83: an array write marks the geometry for update):
+    Preview hit ids within the hit-id bar, same-seed Path on >= 99% of pixels within 1e-3."""
+    build = CASES[name]
+    scene = build(gpu_device)
+    w, h = 120, 90
+    preview_hits(gpu_device, scene, w, h, 1)  # builds the trees
+    _move(scene, numpy.random.default_rng(6))
+    t = fresnel.tracer.Path(gpu_device, w=w, h=h)
+    t.seed = 4
+    t._tracer.resetStats()
+    t.sample(scene, samples=4)
+    st = t._tracer.getStats()
+    assert st["bvh_refits"] == st["bvh_builds"] >= 1
+    gpath = numpy.array(t.linear_output[:], copy=True)
+    gh, _, _ = preview_hits(gpu_device, scene, w, h, 2)
+
+    oscene = build(oracle_device)
+    _copy_arrays(scene, oscene)
+    oscene.camera = scene.camera
+    oh, _, _ = preview_hits(oracle_device, oscene, w, h, 2)
+    check_hits("test_refit_matches_oracle", oracle_device, oscene, w, h, 2, gh, oh, scene=name)
+    frac = same_seed_fraction(gpath, oracle_path_image(oracle_device, oscene, w, h, 5, 4))
+    record("test_refit_matches_oracle", check="same_seed", scene=name, within_1e3=frac)
+    assert frac >= 0.99

@@ -11,6 +11,8 @@ import numpy
 import pytest
 
 from fresnel_b200 import serving, workloads
+from parity import oracle_path_image, same_seed_fraction
+from parity_record import record
 
 pytestmark = pytest.mark.gpu
 
@@ -44,3 +46,26 @@ def test_served_equals_alone(gpu_device):
         assert rays == r.rays > 0
     s = serving.latency_summary(reqs)
     assert s["requests"] == len(reqs)
+
+
+def test_served_matches_oracle(gpu_device, oracle_device):
+    """Requests served in a mix (sliced over several steps) against the CPU oracle rendering
+    each request alone with the request's seed: >= 99% of pixels within 1e-3."""
+    sizes = {0: 1200, 1: 3000}
+    scenes = {k: workloads.serving_scene(gpu_device, n, seed=70 + k) for k, n in sizes.items()}
+    oscenes = {k: workloads.serving_scene(oracle_device, n, seed=70 + k)
+               for k, n in sizes.items()}
+    reqs = [serving.Request(i % 2, w, h, spp, seed=900 + i, arrival=0.0, tag=i)
+            for i, (w, h, spp) in enumerate([(64, 48, 5), (96, 64, 3), (40, 40, 8),
+                                             (80, 60, 4), (72, 40, 6)])]
+    engine = serving.Engine(gpu_device)
+    srv = serving.RenderServer(engine, lambda k: (scenes[k], workloads.serving_scene_bytes(sizes[k])),
+                               step_paths=12000, max_active=3, keep_linear=True)
+    serving.serve_trace(srv, reqs, realtime=False)
+    assert srv.steps > 2
+    for r in reqs:
+        ora = oracle_path_image(oracle_device, oscenes[r.scene_key], r.w, r.h, r.seed, r.samples)
+        frac = same_seed_fraction(r.linear, ora)
+        record("test_served_matches_oracle", check="same_seed", request=r.tag,
+               width=r.w, height=r.h, spp=r.samples, within_1e3=frac)
+        assert frac >= 0.99, f"request {r.tag}: {frac:.4%} of pixels within 1e-3"
