@@ -229,6 +229,73 @@ __global__ void __launch_bounds__(256, fused_blocks(MASK)) k_batch_bounce(BatchD
     flush_counts(tc, &B.ctl->box_tests);
 }
 
+// The remaining bounces of every path of queue q in one launch (k_path_tail): each lane follows
+// its path to the end, then takes the next one (idle lanes share one atomic); a path's rays are
+// added to its render's count when it ends.  The work counter must be zero at launch; no queue is
+// written.
+template <int WIDTH, uint32_t MASK>
+__global__ void __launch_bounds__(256, fused_blocks(MASK)) k_batch_tail(BatchDev B, int q)
+{
+    const PathState& S = B.S;
+    const uint32_t w = B.ctl->wave;
+    const uint32_t f0 = B.wave_first[w], f1 = B.wave_first[w + 1];
+    const uint32_t count = S.ctr[q];
+    const uint32_t* queue = S.queue[q];
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t below = (1u << lane) - 1u;
+    TraceCount tc;
+    bool active = false, exhausted = false;
+    uint32_t p = 0, jb = 0, guard = 0;
+    unsigned long long rays = 0;
+    while (true) {
+        const uint32_t idle = __ballot_sync(0xffffffffu, !active);
+        if (idle && !exhausted) {
+            const uint32_t n = uint32_t(__popc(idle));
+            uint32_t base = 0;
+            if (lane == 0)
+                base = atomicAdd(S.ctr + 2, n);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (base + n >= count)
+                exhausted = true;
+            if (!active) {
+                const uint32_t item = base + uint32_t(__popc(idle & below));
+                if (item < count) {
+                    p = ld_cs(queue + item);
+                    jb = find_job<&WaveJob::slot_base>(B.jobs, f0, f1, p);
+                    active = true;
+                    guard = TAIL_MAX_DEPTH;
+                    rays = 0;
+                }
+            }
+        }
+        if (__ballot_sync(0xffffffffu, active) == 0u)
+            break;
+        if (active) {
+            ++rays;
+            const FrameParams& P = B.jobs[jb].P;
+            bool more = bounce<WIDTH, MASK>(P, S, p, p - B.jobs[jb].slot_base, tc);
+            if (more && --guard == 0u) {
+                atomicOr(P.scene.status, ERR_ITERATION_CAP);
+                more = false;
+            }
+            if (!more) {
+                atomicAdd(P.stats + 0, rays);
+                active = false;
+            }
+        }
+    }
+    flush_counts(tc, &B.ctl->box_tests);
+}
+
+__global__ void k_wave_begin_flat(BatchDev B)
+{
+    B.S.ctr[0] = 0;
+    B.S.ctr[1] = 0;
+    B.S.ctr[2] = 0;
+    B.S.ctr[3] = 0;
+    B.ctl->inner = 0;
+}
+
 // Before a fused bounce: the output queue q and the work counter start at zero.
 __global__ void k_clear_queue(BatchDev B, int q)
 {
@@ -363,36 +430,42 @@ cudaError_t capture(const BatchDev& B, int num_sms, cudaStream_t s0, cudaGraphEx
             if (keep(cudaGetLastError()) && keep(add_while(s0, h_outer, &outer_body))) {
                 cudaGraphConditionalHandle h_inner;
                 cudaGraph_t inner_body = nullptr;
-                if (keep(cudaGraphConditionalHandleCreate(&h_inner, outer_body, 0, 0)) &&
+                if (FUSED &&
                     keep(cudaStreamBeginCaptureToGraph(s1, outer_body, nullptr, nullptr, 0,
                                                        cudaStreamCaptureModeRelaxed))) {
+                    // a wave without a bounce loop: two bounce launches while the queues are
+                    // long (queue 0 -> 1 -> 0; the fused primary kernel fills queue 0), then
+                    // every path's remaining bounces in one launch (k_batch_tail)
+                    c1 = true;
+                    k_wave_begin_flat<<<1, 1, 0, s1>>>(B);
+                    k_batch_primary_shade<WIDTH, MASK><<<g_primary, 256, 0, s1>>>(B);
+                    k_clear_queue<<<1, 1, 0, s1>>>(B, 1);
+                    k_batch_bounce<WIDTH, MASK><<<g_extend, 256, 0, s1>>>(B, 0);
+                    k_clear_queue<<<1, 1, 0, s1>>>(B, 0);
+                    k_batch_bounce<WIDTH, MASK><<<g_extend, 256, 0, s1>>>(B, 1);
+                    k_clear_queue<<<1, 1, 0, s1>>>(B, 1);
+                    k_batch_tail<WIDTH, MASK><<<g_extend, 256, 0, s1>>>(B, 0);
+                    k_batch_fold<<<g_fold, 256, 0, s1>>>(B);
+                    k_wave_end<<<1, 1, 0, s1>>>(B, h_outer);
+                    keep(cudaGetLastError());
+                } else if (!FUSED &&
+                           keep(cudaGraphConditionalHandleCreate(&h_inner, outer_body, 0, 0)) &&
+                           keep(cudaStreamBeginCaptureToGraph(s1, outer_body, nullptr, nullptr, 0,
+                                                              cudaStreamCaptureModeRelaxed))) {
                     c1 = true;
                     k_wave_begin<<<1, 1, 0, s1>>>(B, h_inner);
-                    if (FUSED)
-                        k_batch_primary_shade<WIDTH, MASK><<<g_primary, 256, 0, s1>>>(B);
-                    else
-                        KS::primary(B, g_primary, s1);
+                    KS::primary(B, g_primary, s1);
                     if (keep(cudaGetLastError()) && keep(add_while(s1, h_inner, &inner_body)) &&
                         keep(cudaStreamBeginCaptureToGraph(s2, inner_body, nullptr, nullptr, 0,
                                                            cudaStreamCaptureModeRelaxed))) {
                         c2 = true;
-                        if (FUSED) {
-                            // two bounces per pass: queue 0 -> 1, then 1 -> 0 (the fused
-                            // primary kernel fills queue 0)
-                            k_clear_queue<<<1, 1, 0, s2>>>(B, 1);
-                            k_batch_bounce<WIDTH, MASK><<<g_extend, 256, 0, s2>>>(B, 0);
-                            k_clear_queue<<<1, 1, 0, s2>>>(B, 0);
-                            k_batch_bounce<WIDTH, MASK><<<g_extend, 256, 0, s2>>>(B, 1);
-                            k_inner_cond<<<1, 1, 0, s2>>>(B, h_inner, 0);
-                        } else {
-                            // two iterations per pass: queue 1 -> 0, then 0 -> 1 (the primary
-                            // kernel fills queue 1)
-                            k_batch_shade<<<g_shade, 256, 0, s2>>>(B, 1, 0);
-                            KS::extend(B, 0, g_extend, s2);
-                            k_batch_shade<<<g_shade, 256, 0, s2>>>(B, 0, 1);
-                            KS::extend(B, 1, g_extend, s2);
-                            k_inner_cond<<<1, 1, 0, s2>>>(B, h_inner, 1);
-                        }
+                        // two iterations per pass: queue 1 -> 0, then 0 -> 1 (the primary
+                        // kernel fills queue 1)
+                        k_batch_shade<<<g_shade, 256, 0, s2>>>(B, 1, 0);
+                        KS::extend(B, 0, g_extend, s2);
+                        k_batch_shade<<<g_shade, 256, 0, s2>>>(B, 0, 1);
+                        KS::extend(B, 1, g_extend, s2);
+                        k_inner_cond<<<1, 1, 0, s2>>>(B, h_inner, 1);
                         keep(cudaGetLastError());
                     }
                     if (c2) {

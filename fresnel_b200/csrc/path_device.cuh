@@ -10,6 +10,10 @@ namespace {
 
 constexpr float PATH_TNEAR = 1e-3f;  // fresnel/cpu/TracerPath.cc:121,167
 
+// Bound on the bounces a tail kernel follows one path for (never reached: Russian roulette ends
+// paths long before); a path cut there sets ERR_ITERATION_CAP.
+constexpr uint32_t TAIL_MAX_DEPTH = 1u << 16;
+
 __device__ __forceinline__ V3 xyz(float4 a) { return v3(a.x, a.y, a.z); }
 __device__ __forceinline__ float4 f4(V3 a) { return make_float4(a.x, a.y, a.z, 0.0f); }
 __device__ __forceinline__ float4 f4(C3 a) { return make_float4(a.r, a.g, a.b, 0.0f); }

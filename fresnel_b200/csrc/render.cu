@@ -455,9 +455,7 @@ __global__ void __launch_bounds__(256, fused_blocks(MASK)) k_path_bounce(FramePa
 // (lanes that are idle together share one atomic), so the walks of different bounces overlap
 // instead of being serialised launch by launch.  Every path runs the same per-bounce arithmetic
 // as in k_path_bounce.  The work counter (ctr[2]) must be zero at launch; no queue is written.
-// A path longer than TAIL_MAX_DEPTH further bounces is cut and reported (never reached: Russian
-// roulette ends paths long before).
-constexpr uint32_t TAIL_MAX_DEPTH = 1u << 16;
+// A path longer than TAIL_MAX_DEPTH further bounces is cut and reported.
 
 template <int WIDTH, uint32_t MASK>
 __global__ void __launch_bounds__(256, fused_blocks(MASK)) k_path_tail(FrameParams P, PathState S, int q)

@@ -60,9 +60,9 @@ def test_served_matches_oracle(gpu_device, oracle_device):
                                              (80, 60, 4), (72, 40, 6)])]
     engine = serving.Engine(gpu_device)
     srv = serving.RenderServer(engine, lambda k: (scenes[k], workloads.serving_scene_bytes(sizes[k])),
-                               step_paths=12000, max_active=3, keep_linear=True)
+                               step_paths=8000, max_active=3, keep_linear=True)
     serving.serve_trace(srv, reqs, realtime=False)
-    assert srv.steps > 2
+    assert srv.steps >= 2
     for r in reqs:
         ora = oracle_path_image(oracle_device, oscenes[r.scene_key], r.w, r.h, r.seed, r.samples)
         frac = same_seed_fraction(r.linear, ora)
