@@ -164,7 +164,7 @@ struct fr_device {
     int refill = 0;                        // extension rays with per-lane refill
     int accel = 2;                         // sphere grid: 0 never, 1 whenever possible, 2 auto
     int fuse_shade = 1;                    // primary rays shaded in the primary pass
-    int tail_after = 2;                    // fused bounce launches before the tail kernel (0: none)
+    int tail_after = 1;                    // fused bounce launches before the tail kernel (-1: none)
     float grid_cells_per_prim = 1.5f;      // grid cells per sphere
     std::vector<fr_scene*> scenes;         // to mark BVHs stale when a build option changes
     void* static_path = nullptr;           // this device's copy of g_static_path (looked up once)
@@ -1127,8 +1127,8 @@ fr_status fr_device_set_option(fr_device* d, const char* name, double value)
             return fail(FR_ERR_INVALID, "fuse_shade must be 0, 1 or 2");
         d->fuse_shade = int(value);
     } else if (n == "tail") {
-        if (!(value >= 0.0 && value <= 64.0 && value == double(int(value))))
-            return fail(FR_ERR_INVALID, "tail must be an integer in [0, 64]");
+        if (!(value >= -1.0 && value <= 64.0 && value == double(int(value))))
+            return fail(FR_ERR_INVALID, "tail must be an integer in [-1, 64]");
         d->tail_after = int(value);
     } else if (n == "accel") {
         if (!(value == 0.0 || value == 1.0 || value == 2.0))
@@ -1662,7 +1662,7 @@ fr_status fr_tracer_render_path(fr_tracer* t, fr_scene* sc, const fr_render_para
         // compiled for 3 blocks per SM is slower than the separate passes)
         const bool bounces =
             fused && (t->dev->fuse_shade == 2 || (P.scene.grid.n_cells != 0 && !P.refill));
-        if (bounces && t->dev->tail_after > 0) {
+        if (bounces && t->dev->tail_after >= 0) {
             // a few bounce launches while the queues are long, then every path's remaining
             // bounces in one launch: the wavefront needs no queue-length read-back
             for (int b = 0; b < t->dev->tail_after; ++b, ++it) {

@@ -428,6 +428,8 @@ struct LightsK {
     V3 dir[4];
     C3 color[4];
     float theta[4];
+    float cos_theta[4];  // cos(theta), the cone test's threshold (taken before the clamp)
+    float sin_half[4];   // sin(min(theta, pi/2)), the normalisation of the light's radiance
     uint32_t n;
 };
 
@@ -486,13 +488,10 @@ FR_HD void path_miss_lights(PathS& s, const LightsK& L, V3 ray_dir)
 {
     for (uint32_t i = 0; i < L.n; ++i) {
         V3 l = L.dir[i];
-        float half = L.theta[i];
-        float cos_half = hcos(half);
-        if (half > PI_F / 2.0f)
-            half = PI_F / 2.0f;
+        const float cos_half = L.cos_theta[i];
         float ldotd = dot(l, ray_dir);
         if (ldotd >= cos_half)
-            s.result = s.result + c_div_recip(s.att * L.color[i], hsin(half));
+            s.result = s.result + c_div_recip(s.att * L.color[i], L.sin_half[i]);
     }
     s.done = true;
 }
@@ -563,6 +562,8 @@ FR_HD LightsK lights_to_world(const V3* dir_cam, const C3* color, const float* t
         L.dir[i] = v3(0, 0, 0);
         L.color[i] = c3(0, 0, 0);
         L.theta[i] = 0.0f;
+        L.cos_theta[i] = 1.0f;
+        L.sin_half[i] = 0.0f;
     }
     for (uint32_t i = 0; i < n; ++i) {
         L.color[i] = color[i];
@@ -570,6 +571,11 @@ FR_HD LightsK lights_to_world(const V3* dir_cam, const C3* color, const float* t
         v = v * (1.0f / sqrtf(dot(v, v)));
         L.dir[i] = v.x * k.u + v.y * k.v + v.z * k.w;
         L.theta[i] = theta[i];
+        // the miss program's per-light constants (TracerPathMethods.h:57-61), once per frame
+        // instead of per escaping ray; on the host, with the C library's cosf/sinf
+        L.cos_theta[i] = hcos(theta[i]);
+        const float half = theta[i] > PI_F / 2.0f ? PI_F / 2.0f : theta[i];
+        L.sin_half[i] = hsin(half);
     }
     return L;
 }

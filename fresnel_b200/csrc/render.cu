@@ -693,7 +693,7 @@ __device__ __forceinline__ C3 preview_shade(const FrameParams& P, const GeomDev&
         V3 l = P.lights.dir[li];
         V3 r = -v + (2.0f * n * dot(n, v));
         float half = P.lights.theta[li];
-        float cos_half = hcos(half);
+        const float cos_half = P.lights.cos_theta[li];
         float ldotr = dot(l, r);
         if (ldotr < cos_half) {
             V3 ax = cross(l, r);

@@ -64,3 +64,29 @@ def test_grid_refill_extension_gives_identical_images(gpu_device):
     assert numpy.isfinite(a).all() and numpy.count_nonzero(a[..., 3]) > 0
     assert numpy.array_equal(a, b)
     assert ra == rb
+
+
+def test_tail_kernel_gives_identical_images(gpu_device):
+    """Device option "tail": the fused bounces of a sphere-grid scene run as that many bounce
+    launches and then one persistent launch that follows every remaining path to its end (-1:
+    bounce launches only).  Each path's arithmetic is the same, so the images and ray counts must
+    be identical."""
+    dd = gpu_device._device
+    old = dd.getOption("tail")
+    out = []
+    try:
+        for tail in (-1, 0, 1, 3):
+            dd.setOption("tail", tail)
+            scene = workloads.config2(gpu_device, n=20000, box=140.0 * 0.02**(1 / 3))
+            t = fresnel.tracer.Path(gpu_device, w=120, h=68)
+            t.seed = 6
+            t.sample(scene, samples=7, light_samples=2)
+            out.append((numpy.array(t.linear_output[:], copy=True),
+                        t._tracer.getStats()["rays"]))
+    finally:
+        dd.setOption("tail", old)
+    base, rays = out[0]
+    assert numpy.isfinite(base).all() and numpy.count_nonzero(base[..., 3]) > 0
+    for img, r in out[1:]:
+        assert numpy.array_equal(base, img)
+        assert r == rays
