@@ -761,6 +761,10 @@ def main():
         # without shade launches each bounce traces and shades in one kernel
         primary_name = "k_path_primary_shade" if dd.getOption("fuse_shade") else "k_path_primary"
         ext_name = "k_path_bounce" if st["shade_launches"] == 0 else "k_path_extend"
+        if ext_name == "k_path_bounce" and dd.getOption("tail") >= 0:
+            # the fused bounces of a wavefront: bounce launches, then one tail launch that
+            # follows every remaining path (timed together as the extension kernels)
+            ext_name = "k_path_bounce+k_path_tail"
         kern = {primary_name: (primary_rays, st["primary_ms"], st["primary_launches"]),
                 ext_name: (ext_rays, st["extend_ms"], st["extend_launches"])}
     dom = max(kern, key=lambda k: kern[k][1])
