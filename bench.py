@@ -44,18 +44,30 @@ class Workload:
     BVH (binned SAH, BVH2, leaves <= 4) on this scene and camera, measured by
     oracle/measure_ray_costs.py and frozen here; prim_bytes: bytes read per primitive test.
     Algorithmic bytes per ray = 24 (ray) + 16 (hit) + 32 A + prim_bytes P + 12 (colour).
+    grid_cells / grid_spheres: mean cells visited and spheres tested per closest-hit query of the
+    uniform sphere grid (1.5 cells per sphere), measured by the oracle's restatement of the grid
+    walk on the rays of an oracle render of the frame (oracle/measure_ray_costs.py --grid) and
+    frozen here.  Algorithmic bytes per ray through the grid = 52 + 8 C + 16 S.
     """
 
     def __init__(self, key, desc, scene, w, h, spp=1, light_samples=1, preview=False, aa_n=1,
-                 box_tests=0.0, prim_tests=0.0, prim_bytes=16):
+                 box_tests=0.0, prim_tests=0.0, prim_bytes=16, grid_cells=None,
+                 grid_spheres=None):
         self.key, self.desc, self.scene = key, desc, scene
         self.w, self.h, self.spp, self.light_samples = w, h, spp, light_samples
         self.preview, self.aa_n = preview, aa_n
         self.box_tests, self.prim_tests, self.prim_bytes = box_tests, prim_tests, prim_bytes
+        self.grid_cells, self.grid_spheres = grid_cells, grid_spheres
 
     @property
     def bytes_per_ray(self):
         return 24 + 16 + 32 * self.box_tests + self.prim_bytes * self.prim_tests + 12
+
+    @property
+    def grid_bytes_per_ray(self):
+        if self.grid_cells is None:
+            return None
+        return 52 + 8 * self.grid_cells + 16 * self.grid_spheres
 
     def build(self, device):
         from fresnel_b200 import workloads
@@ -64,7 +76,8 @@ class Workload:
 
 WORKLOADS = {
     "c2": Workload("c2", "config2: 1M spheres r=0.5, box 140, {w}x{h}, {spp} spp, 1 light sample, "
-                   "lightbox", "config2", 1920, 1080, spp=256, box_tests=37.74, prim_tests=1.42),
+                   "lightbox", "config2", 1920, 1080, spp=256, box_tests=37.74, prim_tests=1.42,
+                   grid_cells=2.997, grid_spheres=8.005),
     "c2-preview": Workload("c2-preview", "config2 Preview: 1M spheres, {w}x{h}, anti_alias "
                            "(64 samples per pixel)", "config2", 1920, 1080, preview=True, aa_n=8,
                            box_tests=29.41, prim_tests=0.95),
@@ -776,10 +789,16 @@ def main():
     per_box = 8.0 if grid else 32.0
     run_bytes = (52.0 + per_box * st["box_tests"] / rays + 16.0 * st["prim_tests"] / rays
                  if rays > 0 else None)
-    # The roofline's bytes: for a grid, those of the grid walked; for a BVH, the reference BVH's
-    # fixed box and primitive tests per ray (wl.bytes_per_ray).  The reference-BVH figure of a
-    # grid run is kept beside it: it counts the work a BVH would do, not what the kernel read.
-    bpr = run_bytes if grid else wl.bytes_per_ray
+    # The roofline's bytes: for a grid, those of the grid walked (the oracle's frozen cells and
+    # spheres per ray when the workload has them, else this run's counters); for a BVH, the
+    # reference BVH's fixed box and primitive tests per ray (wl.bytes_per_ray).  The
+    # reference-BVH figure of a grid run is kept beside it: it counts the work a BVH would do,
+    # not what the kernel read.
+    if grid:
+        bpr = wl.grid_bytes_per_ray if wl.grid_bytes_per_ray and wl.w * wl.h == 1920 * 1080 \
+            else run_bytes
+    else:
+        bpr = wl.bytes_per_ray
     achieved = (dom_rays * bpr) / (dom_ms / 1e3) / 1e9 if dom_ms > 0 and bpr else None
     achieved_ref = (dom_rays * wl.bytes_per_ray) / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else None
     achieved_run = ((dom_rays * run_bytes) / (dom_ms / 1e3) / 1e9
@@ -861,8 +880,12 @@ def main():
                          "peak_source": peak_kind, "kernel": dom,
                          "rays": dom_rays, "kernel_ms": dom_ms, "launches": launches,
                          "bytes_per_ray": bpr,
-                         "bytes_per_ray_basis": ("sphere grid walked: 52 + 8 per cell + 16 per "
-                                                 "sphere tested, engine counters" if grid else
+                         "bytes_per_ray_basis": (("sphere grid walked: 52 + 8 per cell + 16 "
+                                                  "per sphere tested, oracle counts" if
+                                                  bpr != run_bytes else
+                                                  "sphere grid walked: 52 + 8 per cell + 16 "
+                                                  "per sphere tested, engine counters")
+                                                 if grid else
                                                  "reference BVH: 52 + 32 A + S P, oracle counts"),
                          "accel": "grid" if grid else "bvh",
                          "bytes_per_ray_run": run_bytes, "achieved_run": achieved_run,

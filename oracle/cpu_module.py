@@ -111,6 +111,11 @@ def load(kind="restated"):
                                   ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _fp]
     lib.or_brdf.argtypes = [ctypes.POINTER(FrMaterial), _fp, _fp, _fp, _fp, _fp]
     lib.or_math_kind.restype = ctypes.c_char_p
+    lib.or_set_ray_log.argtypes = [_fp, ctypes.c_uint64]
+    lib.or_ray_log_count.restype = ctypes.c_uint64
+    lib.or_grid_walk_stats.argtypes = [ctypes.c_void_p, ctypes.c_uint32, _fp, _fp, ctypes.c_uint32,
+                                       ctypes.c_float, _fp, ctypes.c_uint64, ctypes.c_int,
+                                       ctypes.POINTER(ctypes.c_double)]
     _LIBS[kind] = lib
     return lib
 

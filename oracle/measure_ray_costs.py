@@ -8,8 +8,14 @@ algorithmic bytes per ray = 24 + 16 + 32 A + prim_bytes P + 12.
 Path workloads: n_pixels random pixels of the frame, spp samples each.  Preview: the frame at
 1/8 of the resolution in each direction with the workload's AA level (same camera).
 
-Run: python oracle/measure_ray_costs.py [workload] [n_pixels] [spp]   (workload: c1, c2, c3,
-c2-preview; default c2)
+Sphere-grid costs (``--grid``): the same render with the oracle's ray log on, then every logged
+ray walked through the oracle's restatement of the engine's uniform sphere grid (1.5 cells per
+sphere, oracle_core.cpp: build_sphere_grid / walk_sphere_grid): cells visited (C) and spheres
+tested (S) per ray, and the number of rays whose grid hit differs from the oracle's BVH hit.
+bench.py freezes C and S for the sphere-grid roofline: bytes per ray = 52 + 8 C + 16 S.
+
+Run: python oracle/measure_ray_costs.py [workload] [n_pixels] [spp] [--grid]  (workload: c1,
+c2, c3, c2-preview; default c2)
 """
 
 import os
@@ -20,6 +26,50 @@ import numpy
 
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, REPO)
+
+
+def grid_costs(key="c2", n_pixels=4096, spp=4, cells_per_sphere=1.5, max_rays=2_000_000):
+    """Cells and spheres per ray of the sphere grid, on the rays of an oracle render."""
+    import ctypes
+
+    import bench
+    from oracle import cpu_module
+    wl = bench.WORKLOADS[key]
+    dev = cpu_module.make_device("restated")
+    scene = wl.build(dev)
+    scene._scene.handle()
+    g = scene.geometry[0]
+    pos = numpy.ascontiguousarray(g.position[:], dtype=numpy.float32)
+    rad = numpy.ascontiguousarray(g.radius[:], dtype=numpy.float32)
+    lib = dev._device.lib
+    log = numpy.zeros((max_rays, 7), numpy.float32)
+    tr = dev.module.TracerPath(dev._device, wl.w, wl.h, wl.light_samples)
+    tr.setSeed(2)
+    rng = numpy.random.default_rng(0)
+    pixels = numpy.sort(rng.choice(wl.w * wl.h, min(n_pixels, wl.w * wl.h),
+                                   replace=False)).astype(numpy.uint32)
+    lib.or_set_ray_log(cpu_module.ptr(log), max_rays)
+    try:
+        tr.render_pixels(scene._scene, pixels, 1, int(spp), want_m2=False)
+    finally:
+        n = int(lib.or_ray_log_count())
+        lib.or_set_ray_log(None, 0)
+    n = min(n, max_rays)
+    out = (ctypes.c_double * 6)()
+    rc = lib.or_grid_walk_stats(scene._scene.handle(), 0, cpu_module.ptr(pos), cpu_module.ptr(rad),
+                                len(rad), float(cells_per_sphere), cpu_module.ptr(log), n, 0, out)
+    if rc != 0:
+        raise RuntimeError("grid construction failed")
+    res = {"rays": int(out[0]), "cells_per_ray": out[1], "spheres_per_ray": out[2],
+           "rays_hitting_differently": int(out[3]), "cells": int(out[4]), "refs": int(out[5]),
+           "bytes_per_ray": 52 + 8 * out[1] + 16 * out[2]}
+    print(f"workload {key}: {n_pixels} pixels x {spp} spp, {res['rays']} rays through a grid of "
+          f"{res['cells']} cells and {res['refs']} sphere references")
+    print(f"C (cells per ray)   = {res['cells_per_ray']:.3f}")
+    print(f"S (spheres per ray) = {res['spheres_per_ray']:.3f}")
+    print(f"bytes per ray = 52 + 8 C + 16 S = {res['bytes_per_ray']:.1f}")
+    print(f"rays whose grid hit differs from the BVH hit: {res['rays_hitting_differently']}")
+    return res
 
 
 def main(key="c2", n_pixels=20000, spp=2):
@@ -54,5 +104,8 @@ def main(key="c2", n_pixels=20000, spp=2):
 
 
 if __name__ == "__main__":
-    a = sys.argv[1:]
-    main(a[0] if a else "c2", *(int(x) for x in a[1:3]))
+    a = [x for x in sys.argv[1:] if x != "--grid"]
+    if "--grid" in sys.argv:
+        grid_costs(a[0] if a else "c2", *(int(x) for x in a[1:3]))
+    else:
+        main(a[0] if a else "c2", *(int(x) for x in a[1:3]))

@@ -104,6 +104,18 @@ void or_brdf(const fr_material* m, const float l[3], const float v[3], const flo
              const float shading_color[3], float out[3]);
 const char* or_math_kind(void);
 
+/* Record the rays trace() answers (7 floats each: origin, direction, tnear) into buffer, up to
+   capacity; NULL stops recording.  or_ray_log_count: rays seen since the buffer was set. */
+void or_set_ray_log(float* buffer, uint64_t capacity);
+uint64_t or_ray_log_count(void);
+
+/* The engine's uniform sphere grid over (pos, rad), restated, walked by n_rays logged rays: out =
+   {rays, cells per ray, spheres tested per ray, rays whose grid hit differs from the oracle's BVH
+   hit on geometry sphere_geom, cells, references}.  Returns 0 on success. */
+int or_grid_walk_stats(const or_scene* s, uint32_t sphere_geom, const float* pos, const float* rad,
+                       uint32_t n, float cells_per_sphere, const float* rays, uint64_t n_rays,
+                       int nthreads, double out[6]);
+
 #ifdef __cplusplus
 }
 #endif

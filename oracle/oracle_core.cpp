@@ -593,6 +593,27 @@ inline bool slab(const Node& nd, const float o[3], const float inv[3], float tma
     return t0 <= t1;
 }
 
+// Optional log of the rays trace() answers (or_set_ray_log): 7 floats per ray (origin,
+// direction, tnear), appended by every thread; rays past the capacity are counted, not stored.
+float* g_ray_log = nullptr;
+uint64_t g_ray_log_cap = 0;
+std::atomic<uint64_t> g_ray_log_n{0};
+
+inline void log_ray(F3 o, F3 d, float tnear)
+{
+    const uint64_t i = g_ray_log_n.fetch_add(1, std::memory_order_relaxed);
+    if (i < g_ray_log_cap) {
+        float* r = g_ray_log + 7 * i;
+        r[0] = o.x;
+        r[1] = o.y;
+        r[2] = o.z;
+        r[3] = d.x;
+        r[4] = d.y;
+        r[5] = d.z;
+        r[6] = tnear;
+    }
+}
+
 // Closest hit in (tnear, inf): Embree's rtcIntersect1 with fresnel's user geometries.
 Hit trace(const or_scene& s, F3 o, F3 d, float tnear, Counters& c)
 {
@@ -601,6 +622,8 @@ Hit trace(const or_scene& s, F3 o, F3 d, float tnear, Counters& c)
     h.geom = UINT32_MAX;
     h.prim = 0;
     c.rays++;
+    if (g_ray_log)
+        log_ray(o, d, tnear);
     if (s.nodes.empty())
         return h;
     float of[3] = {o.x, o.y, o.z};
@@ -682,6 +705,190 @@ Hit trace(const or_scene& s, F3 o, F3 d, float tnear, Counters& c)
             break;
     }
     return h;
+}
+
+// ---------------------------------------------------------------------------------------------
+// The engine's uniform sphere grid, restated on the CPU to measure what walking it costs per ray
+// (cells visited, spheres tested) on rays the oracle's own renders trace.  Definition: every
+// sphere's box (centre -+ r; left out when not finite or inverted), padded by 1e-5 * max|coord| +
+// 1e-6 * (sum of extents); the grid spans the union of the padded boxes; cell size
+// h = cbrt(volume / (cells_per_sphere * valid spheres)), dims = ceil(extent / h) clamped to
+// [1, 1024] per axis (h grown by 1.25 until at most 2^26 cells); each cell lists the spheres whose
+// padded box overlaps it, in sphere order.  Walk: a 3-D DDA (Amanatides & Woo 1987) from the cell
+// of the ray's entry point; each visited cell's spheres are tested (tnear < t < tmax); the walk
+// stops once the closest hit so far lies before the cell's exit.
+// ---------------------------------------------------------------------------------------------
+struct SphereGrid {
+    float lo[3], hi[3], cell[3], ih[3];
+    int n[3];
+    std::vector<uint32_t> start;  // per cell: first reference; start[cells] = total
+    std::vector<uint32_t> refs;   // sphere indices
+    const float* pos = nullptr;
+    const float* rad = nullptr;
+};
+
+inline bool sphere_box_padded(const float* pos, const float* rad, uint32_t i, float blo[3],
+                              float bhi[3])
+{
+    const float r = rad[i];
+    bool ok = true;
+    for (int k = 0; k < 3; ++k) {
+        const float c = pos[3 * size_t(i) + k];
+        blo[k] = c - r;
+        bhi[k] = c + r;
+        ok = ok && std::isfinite(blo[k]) && std::isfinite(bhi[k]) && blo[k] <= bhi[k];
+    }
+    if (!ok)
+        return false;
+    float scale = 0.0f, ext = 0.0f;
+    for (int k = 0; k < 3; ++k) {
+        scale = std::max(scale, std::max(std::fabs(blo[k]), std::fabs(bhi[k])));
+        ext += bhi[k] - blo[k];
+    }
+    const float pad = 1e-5f * scale + 1e-6f * ext + 1e-30f;
+    for (int k = 0; k < 3; ++k) {
+        blo[k] -= pad;
+        bhi[k] += pad;
+    }
+    return true;
+}
+
+inline int grid_cell_index(float x, float lo, float ih, int n)
+{
+    const float u = std::floor((x - lo) * ih);
+    return int(std::min(std::max(u, 0.0f), float(n - 1)));
+}
+
+bool build_sphere_grid(const float* pos, const float* rad, uint32_t n, float cells_per_sphere,
+                       SphereGrid& G)
+{
+    G.pos = pos;
+    G.rad = rad;
+    float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    uint32_t valid = 0;
+    float blo[3], bhi[3];
+    for (uint32_t i = 0; i < n; ++i) {
+        if (!sphere_box_padded(pos, rad, i, blo, bhi))
+            continue;
+        for (int k = 0; k < 3; ++k) {
+            mn[k] = std::min(mn[k], blo[k]);
+            mx[k] = std::max(mx[k], bhi[k]);
+        }
+        ++valid;
+    }
+    if (valid == 0)
+        return false;
+    double lo[3], ext[3], scale = 1.0;
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = mn[k];
+        ext[k] = double(mx[k]) - lo[k];
+        scale = std::max(scale, std::max(std::fabs(lo[k]), std::fabs(lo[k] + ext[k])));
+    }
+    for (int k = 0; k < 3; ++k)
+        ext[k] = std::max(ext[k], 1e-6 * scale);
+    const double volume = ext[0] * ext[1] * ext[2];
+    double h = std::cbrt(volume / (double(cells_per_sphere) * valid));
+    for (int pass = 0; pass < 64; ++pass) {
+        double cells = 1.0;
+        for (int k = 0; k < 3; ++k) {
+            G.n[k] = int(std::min(1024.0, std::max(1.0, std::ceil(ext[k] / h))));
+            cells *= G.n[k];
+        }
+        if (cells <= double(1u << 26))
+            break;
+        h *= 1.25;
+    }
+    for (int k = 0; k < 3; ++k) {
+        G.lo[k] = float(lo[k]);
+        G.cell[k] = float(ext[k] / G.n[k]) * (1.0f + 4e-7f);
+        G.ih[k] = 1.0f / G.cell[k];
+        G.hi[k] = G.lo[k] + float(G.n[k]) * G.cell[k];
+    }
+    const size_t cells = size_t(G.n[0]) * G.n[1] * G.n[2];
+    std::vector<uint32_t> count(cells + 1, 0);
+    auto for_cells = [&](uint32_t i, auto&& f) {
+        if (!sphere_box_padded(pos, rad, i, blo, bhi))
+            return;
+        int a[3], b[3];
+        for (int k = 0; k < 3; ++k) {
+            a[k] = grid_cell_index(blo[k], G.lo[k], G.ih[k], G.n[k]);
+            b[k] = grid_cell_index(bhi[k], G.lo[k], G.ih[k], G.n[k]);
+        }
+        for (int z = a[2]; z <= b[2]; ++z)
+            for (int y = a[1]; y <= b[1]; ++y)
+                for (int x = a[0]; x <= b[0]; ++x)
+                    f((size_t(z) * G.n[1] + y) * G.n[0] + x);
+    };
+    for (uint32_t i = 0; i < n; ++i)
+        for_cells(i, [&](size_t c) { count[c + 1]++; });
+    for (size_t c = 0; c < cells; ++c)
+        count[c + 1] += count[c];
+    G.start = count;
+    G.refs.assign(count[cells], 0);
+    std::vector<uint32_t> fill(count.begin(), count.end() - 1);
+    for (uint32_t i = 0; i < n; ++i)
+        for_cells(i, [&](size_t c) { G.refs[fill[c]++] = i; });
+    return true;
+}
+
+// Walks one ray; returns the closest sphere (UINT32_MAX: none) and counts cells and spheres.
+uint32_t walk_sphere_grid(const SphereGrid& G, F3 o, F3 d, float tnear, uint64_t& cells,
+                          uint64_t& tests)
+{
+    float inv[3], oinv[3];
+    const float of[3] = {o.x, o.y, o.z}, df[3] = {d.x, d.y, d.z};
+    for (int k = 0; k < 3; ++k) {
+        const float a = std::fabs(df[k]);
+        inv[k] = 1.0f / (a < 1e-30f ? std::copysign(1e-30f, df[k]) : df[k]);
+        oinv[k] = -of[k] * inv[k];
+    }
+    float t0[3], t1[3];
+    for (int k = 0; k < 3; ++k) {
+        t0[k] = std::fma(G.lo[k], inv[k], oinv[k]);
+        t1[k] = std::fma(G.hi[k], inv[k], oinv[k]);
+    }
+    const float t_in = std::max(std::max(std::min(t0[0], t1[0]), std::min(t0[1], t1[1])),
+                                std::max(std::min(t0[2], t1[2]), 0.0f));
+    const float t_out = std::min(std::min(std::max(t0[0], t1[0]), std::max(t0[1], t1[1])),
+                                 std::max(t0[2], t1[2]));
+    if (!(t_in <= t_out))
+        return UINT32_MAX;
+    int c[3], s[3];
+    float tn[3];
+    for (int k = 0; k < 3; ++k) {
+        const float u = (of[k] + t_in * df[k] - G.lo[k]) * G.ih[k];
+        c[k] = u >= 0.0f ? int(std::min(u, float(G.n[k] - 1))) : 0;
+        s[k] = inv[k] >= 0.0f ? 1 : -1;
+        tn[k] = std::fma(std::fma(float(c[k] + (inv[k] >= 0.0f ? 1 : 0)), G.cell[k], G.lo[k]), inv[k],
+                         oinv[k]);
+    }
+    float tmax = INFINITY;
+    uint32_t best = UINT32_MAX;
+    for (int guard = G.n[0] + G.n[1] + G.n[2] + 3; guard > 0; --guard) {
+        const size_t cell = (size_t(c[2]) * G.n[1] + c[1]) * G.n[0] + c[0];
+        ++cells;
+        for (uint32_t r = G.start[cell]; r < G.start[cell + 1]; ++r) {
+            const uint32_t i = G.refs[r];
+            ++tests;
+            float t = 0, de = 0;
+            F3 N;
+            const F3 p{G.pos[3 * size_t(i)], G.pos[3 * size_t(i) + 1], G.pos[3 * size_t(i) + 2]};
+            if (M::isect_sphere(t, de, N, o, d, p, G.rad[i]) && tnear < t &&
+                (t < tmax || (t == tmax && i < best))) {
+                tmax = t;
+                best = i;
+            }
+        }
+        const float t_cell = std::min(tn[0], std::min(tn[1], tn[2]));
+        const int axis = (tn[0] <= tn[1] && tn[0] <= tn[2]) ? 0 : (tn[1] <= tn[2] ? 1 : 2);
+        c[axis] += s[axis];
+        if (tmax <= t_cell || !(t_cell < t_out) || c[axis] < 0 || c[axis] >= G.n[axis])
+            break;
+        tn[axis] = std::fma(std::fma(float(c[axis] + (inv[axis] >= 0.0f ? 1 : 0)), G.cell[axis],
+                                     G.lo[axis]),
+                            inv[axis], oinv[axis]);
+    }
+    return best;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1203,6 +1410,52 @@ void or_brdf(const fr_material* m, const float l[3], const float v[3], const flo
     out[0] = r.r;
     out[1] = r.g;
     out[2] = r.b;
+}
+
+void or_set_ray_log(float* buffer, uint64_t capacity)
+{
+    g_ray_log = buffer;
+    g_ray_log_cap = buffer ? capacity : 0;
+    g_ray_log_n.store(0);
+}
+
+uint64_t or_ray_log_count(void) { return g_ray_log_n.load(); }
+
+int or_grid_walk_stats(const or_scene* s, uint32_t sphere_geom, const float* pos, const float* rad,
+                       uint32_t n, float cells_per_sphere, const float* rays, uint64_t n_rays,
+                       int nthreads, double out[6])
+{
+    SphereGrid G;
+    if (!build_sphere_grid(pos, rad, n, cells_per_sphere, G))
+        return 1;
+    const uint32_t chunks = uint32_t(std::min<uint64_t>(n_rays, 4096));
+    std::vector<uint64_t> cells(chunks, 0), tests(chunks, 0), differ(chunks, 0);
+    parallel_tiles(chunks, nthreads, [&](uint32_t ch, int) {
+        const uint64_t a = n_rays * ch / chunks, b = n_rays * (ch + 1) / chunks;
+        for (uint64_t i = a; i < b; ++i) {
+            const float* r = rays + 7 * i;
+            const F3 o{r[0], r[1], r[2]}, d{r[3], r[4], r[5]};
+            const uint32_t g = walk_sphere_grid(G, o, d, r[6], cells[ch], tests[ch]);
+            Counters c;
+            const Hit h = trace(*s, o, d, r[6], c);
+            const uint32_t b_prim = (h.geom == sphere_geom) ? h.prim : UINT32_MAX;
+            if (g != b_prim)
+                differ[ch]++;
+        }
+    });
+    double tc = 0, tt = 0, td = 0;
+    for (uint32_t ch = 0; ch < chunks; ++ch) {
+        tc += double(cells[ch]);
+        tt += double(tests[ch]);
+        td += double(differ[ch]);
+    }
+    out[0] = double(n_rays);
+    out[1] = n_rays ? tc / double(n_rays) : 0.0;
+    out[2] = n_rays ? tt / double(n_rays) : 0.0;
+    out[3] = td;
+    out[4] = double(G.start.size() - 1);
+    out[5] = double(G.refs.size());
+    return 0;
 }
 
 }  // extern "C"
