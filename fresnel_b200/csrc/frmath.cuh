@@ -375,21 +375,6 @@ FR_HD void tangent_frame(V3 n, V3& tx, V3& ty)
     ty = cross(n, tx);
 }
 
-FR_HD V3 sample_ggx(const Mat& m, float xi0, float xi1, V3 v, V3 n)  // Material.h:230-256
-{
-    float alpha = m.roughness * m.roughness;
-    float phi = 2.0f * PI_F * xi0;
-    float cos_t = sqrtf((1.0f - xi1) / (1.0f + (alpha * alpha - 1.0f) * xi1));
-    float sin_t = sqrtf(1.0f - cos_t * cos_t);
-    float sp, cp;
-    hsincos(phi, sp, cp);
-    V3 ht = v3(sin_t * cp, sin_t * sp, cos_t);
-    V3 tx, ty;
-    tangent_frame(n, tx, ty);
-    V3 h = tx * ht.x + ty * ht.y + n * ht.z;
-    return 2.0f * dot(v, h) * h - v;
-}
-
 FR_HD float pdf_ggx(const Mat& m, V3 l, V3 v, V3 n)  // Material.h:258-280
 {
     V3 hh = l + v;
@@ -401,18 +386,6 @@ FR_HD float pdf_ggx(const Mat& m, V3 l, V3 v, V3 n)  // Material.h:258-280
     float D = ggx_d(alpha_sq, ndoth);
     float pdf = D * ndoth / (4.0f * ldoth);
     return (pdf > 0.0f) ? pdf : 0.0f;
-}
-
-FR_HD V3 sample_diffuse(float xi0, float xi1, V3 n)  // Material.h:282-304
-{
-    const float r = sqrtf(xi0);
-    const float theta = 2 * PI_F * xi1;
-    float st, ct;
-    hsincos(theta, st, ct);
-    V3 vt = v3(r * ct, r * st, sqrtf(1.0f - xi0));
-    V3 tx, ty;
-    tangent_frame(n, tx, ty);
-    return tx * vt.x + ty * vt.y + n * vt.z;
 }
 
 FR_HD float pdf_diffuse(V3 l, V3 n)  // Material.h:306-313
@@ -443,21 +416,35 @@ FR_HD V3 mis_direction(float& factor, bool& transmit, V3 v, V3 n, uint32_t depth
     U4 r = philox(0u, depth, sample, TAG_MIS, key0, key1);
     float xi0 = u01(r.x), xi1 = u01(r.y);
     float choice_mis = u01(r.z), choice_trans = u01(r.w);
-    V3 l;
     transmit = (choice_trans <= m.spec_trans);
-    if (transmit) {
-        l = -v;
-    } else if (choice_mis <= 0.5f) {
-        l = sample_diffuse(xi0, xi1, n);
-        float pd = pdf_diffuse(l, n);
-        float pg = pdf_ggx(m, l, v, n);
-        factor = (pd / (pd + pg)) / (0.5f * pd);
-    } else {
-        l = sample_ggx(m, xi0, xi1, v, n);
-        float pd = pdf_diffuse(l, n);
-        float pg = pdf_ggx(m, l, v, n);
-        factor = (pg / (pd + pg)) / (0.5f * pg);
+    if (transmit)
+        return -v;
+    // Both samplers (sample_diffuse, sample_ggx) build a vector (rho cos a, rho sin a, z) in the
+    // tangent frame of n; only rho, a and z differ.  Those are chosen per branch and the rest is
+    // shared, so that lanes of a warp that chose different samplers run the sin/cos, the frame
+    // and both pdfs together (the same operations in the same order as the two samplers).
+    const bool diffuse = choice_mis <= 0.5f;
+    float rho, a, z;
+    if (diffuse) {  // sample_diffuse (Material.h:282-304)
+        rho = sqrtf(xi0);
+        a = 2 * PI_F * xi1;
+        z = sqrtf(1.0f - xi0);
+    } else {  // sample_ggx (Material.h:230-256)
+        float alpha = m.roughness * m.roughness;
+        a = 2.0f * PI_F * xi0;
+        z = sqrtf((1.0f - xi1) / (1.0f + (alpha * alpha - 1.0f) * xi1));
+        rho = sqrtf(1.0f - z * z);
     }
+    float sa, ca;
+    hsincos(a, sa, ca);
+    const V3 vt = v3(rho * ca, rho * sa, z);
+    V3 tx, ty;
+    tangent_frame(n, tx, ty);
+    const V3 w = tx * vt.x + ty * vt.y + n * vt.z;
+    const V3 l = diffuse ? w : 2.0f * dot(v, w) * w - v;
+    float pd = pdf_diffuse(l, n);
+    float pg = pdf_ggx(m, l, v, n);
+    factor = diffuse ? (pd / (pd + pg)) / (0.5f * pd) : (pg / (pd + pg)) / (0.5f * pg);
     return l;
 }
 
