@@ -185,13 +185,20 @@ FR_API fr_status fr_device_timer_stop(fr_device* dev, float* ms);
  *                   along each ray); 2 (default): the grid when it is expected to be faster
  *                   (at least 8192 spheres, a ray crossing at most 6 cells on average before a
  *                   hit, no cell with more than 64 spheres), else the BVH.  Other scenes always
- *                   use BVHs.  The closest hits do not depend on the choice (ties aside).
+ *                   use BVHs.  The closest hits do not depend on the choice: primitives hit
+ *                   at exactly the same distance go to the lower (geometry, primitive) index
+ *                   in every structure.
  *   "grid_density"  grid cells per sphere (default 1.5; (0, 64])
  *   "fuse_shade"    1 (default): the primary pass also shades each primary hit and queues the
  *                   continuing paths itself (the first shade pass of a wavefront is not
  *                   launched), and for scenes traced through a sphere grid each bounce traces
  *                   and shades in one kernel; 2: bounces fused for every scene; 0: separate
  *                   passes.  The same images in every case.
+ *   "tail"          fused sphere-grid bounces: after this many bounce launches per wavefront
+ *                   (0..64, default 1), one persistent launch follows every remaining path to
+ *                   its end (a lane takes the next path once its own ends), with no queue
+ *                   read-back; -1: a bounce launch per bounce until the queue is empty.  The
+ *                   same images in every case.
  * Setting an option marks every BVH of the device's scenes for rebuild when it changes the
  * tree.  Unknown names or out-of-range values return FR_ERR_INVALID. */
 FR_API fr_status fr_device_set_option(fr_device* dev, const char* name, double value);
