@@ -55,6 +55,7 @@ class Workload:
                  grid_spheres=None):
         self.key, self.desc, self.scene = key, desc, scene
         self.w, self.h, self.spp, self.light_samples = w, h, spp, light_samples
+        self.full_size = (w, h)  # the frozen per-ray costs were measured on this frame
         self.preview, self.aa_n = preview, aa_n
         self.box_tests, self.prim_tests, self.prim_bytes = box_tests, prim_tests, prim_bytes
         self.grid_cells, self.grid_spheres = grid_cells, grid_spheres
@@ -83,7 +84,7 @@ WORKLOADS = {
                            box_tests=29.41, prim_tests=0.95),
     "c1": Workload("c1", "config1: 1000 spheres r=0.5, box 20, outline 0.1, cloudy, {w}x{h}, "
                    "{spp} spp x 32 light samples", "config1", 580, 580, spp=64, light_samples=32,
-                   box_tests=37.41, prim_tests=1.81),
+                   box_tests=37.41, prim_tests=1.81, grid_cells=5.038, grid_spheres=10.793),
     "c4": Workload("c4", "config4", "config4", 1024, 1024, spp=16),
     "c5": Workload("c5", "config5", "serving_scene_first", 1280, 720, spp=16),
     "c3": Workload("c3", "config3: 200k spheres + 50k bonds + 20k cubes + 10k icosahedra, "
@@ -482,9 +483,13 @@ def run_batch_bench(args, world, rank, barrier_max, barrier_sum, clock_index, em
     ms_plain, rays_plain, _ = timed(run_plain, plain, args.steps)
     ms_per_sample, rays_per_sample, _ = timed(run_per_sample, per_sample, max(1, args.steps // 2))
     launches0 = batch.stats["kernel_launches"]
+    box0, prim0 = batch.stats["box_tests"], batch.stats["prim_tests"]
     with ClockSampler(clock_index) as clk:
         ms_batch, rays_batch, bst = timed(run_batch, batched, args.steps)
     launches = batch.stats["kernel_launches"] - launches0
+    # a batch counts its traversal work itself (the tracers count only their rays)
+    box = float(batch.stats["box_tests"] - box0)
+    prim = float(batch.stats["prim_tests"] - prim0)
 
     def maxdiff(xs, ys):
         return max(float(numpy.abs(numpy.asarray(a.linear_output[:]) -
@@ -527,8 +532,6 @@ def run_batch_bench(args, world, rank, barrier_max, barrier_sum, clock_index, em
     rays_frame_set = rays_batch / args.steps
     hbm, peak_kind = peaks()
     # bytes of the structures walked (sphere grids: 52 + 8 per cell + 16 per sphere tested)
-    box = sum(float(x["box_tests"]) for x in bst)
-    prim = sum(float(x["prim_tests"]) for x in bst)
     grid = all(int(x.get("grid", 0)) for x in bst)
     bpr = (52.0 + (8.0 if grid else 32.0) * box / rays_batch + 16.0 * prim / rays_batch
            if rays_batch else None)
@@ -795,8 +798,8 @@ def main():
     # reference-BVH figure of a grid run is kept beside it: it counts the work a BVH would do,
     # not what the kernel read.
     if grid:
-        bpr = wl.grid_bytes_per_ray if wl.grid_bytes_per_ray and wl.w * wl.h == 1920 * 1080 \
-            else run_bytes
+        bpr = (wl.grid_bytes_per_ray if wl.grid_bytes_per_ray and (wl.w, wl.h) == wl.full_size
+               else run_bytes)
     else:
         bpr = wl.bytes_per_ray
     achieved = (dom_rays * bpr) / (dom_ms / 1e3) / 1e9 if dom_ms > 0 and bpr else None

@@ -2352,11 +2352,11 @@ fr_status fr_batch_render(fr_batch* b)
     b->stats.waves += uint32_t(waves.size());
     b->stats.graph_launches += 1;
     b->stats.shade_extend_pairs += c.pairs;
-    // fused sphere-grid waves: begin, primary, 2 queue clears, bounce, tail, fold, end;
+    // fused sphere-grid waves: begin, primary, 3 queue clears, 2 bounces, tail, fold, end;
     // otherwise per wave: begin, primary, fold, end, and per pass: 2 shade, 2 extend, 1
     // condition; 1 start
     if (b->exec_mask == MASK_GRID_FUSED)
-        b->stats.kernel_launches += 1 + 8 * uint64_t(waves.size());
+        b->stats.kernel_launches += 1 + 10 * uint64_t(waves.size());
     else
         b->stats.kernel_launches += 1 + 4 * uint64_t(waves.size()) + 5 * c.pairs;
     b->stats.box_tests += c.box_tests;

@@ -5,8 +5,9 @@
 //      the BVH builder pads its boxes), their union, the number of valid spheres and the sum of
 //      r^2 (one pass with warp reductions and atomics);
 //   2. on the host: the cell size (cells_per_prim cells per sphere over the union's volume) and,
-//      in automatic mode, the estimated number of cells a ray crosses before it meets a sphere,
-//      mean free path / cell size with mean free path = volume / (n pi <r^2>);
+//      in automatic mode, the estimated number of cells a ray crosses before it meets a sphere
+//      or leaves the grid, min(mean free path / cell size, nx + ny + nz) with mean free path =
+//      volume / (n pi <r^2>);
 //   3. cells per sphere, their prefix sum, then one (cell, sphere) pair per covered cell written
 //      in sphere order and radix-sorted by cell (stable, so each cell lists its spheres in index
 //      order and the build is deterministic);
@@ -289,6 +290,8 @@ cudaError_t build_grid(const float* position, const float* radius, uint32_t n,
     const double pi = 3.14159265358979323846;
     rep.cells_per_ray =
         mean_r2 > 0.0 ? volume / (rep.n_valid * pi * mean_r2) / h_mean + 1.0 : 1e30;
+    // a ray leaves the grid after at most nx + ny + nz cells
+    rep.cells_per_ray = std::min(rep.cells_per_ray, double(dims[0]) + dims[1] + dims[2]);
     if (gp.mode == 2) {
         if (rep.n_valid < gp.min_prims) {
             rep.reason = "too few spheres";

@@ -25,8 +25,12 @@ struct GridParams {
     float cells_per_prim = 1.5f;         // cells per sphere (sets the cell size)
     int mode = 2;                        // 1: build whenever the spheres allow; 2: only when the
                                          //    grid is expected to beat the BVH
-    uint32_t min_prims = 8192;           // mode 2: fewer spheres keep the BVH
-    float max_cells_per_ray = 6.0f;      // mode 2: estimated cells a ray crosses before a hit
+    // Mode 2 thresholds.  Measured on sphere scenes of 100 to 1M spheres at densities from the
+    // 1M-sphere scene's down to one sphere per 4e5 volume units, the grid traced every one of
+    // them faster than the BVH (1.4x to 2x); what keeps the BVH is clustering.
+    uint32_t min_prims = 1;              // mode 2: fewer spheres keep the BVH
+    float max_cells_per_ray = 1024.0f;   // mode 2: estimated cells a ray crosses before a hit
+                                         //    or before it leaves the grid
     uint32_t max_refs_per_cell = 64;     // mode 2: a fuller cell means clustered spheres
     uint32_t max_cells_per_prim = 4096;  // any mode: a sphere spanning more cells stops the build
 };
@@ -36,7 +40,7 @@ struct GridReport {
     bool built = false;
     const char* reason = "";   // why the grid was not built
     uint32_t n_valid = 0;      // spheres with a finite, non-empty box
-    double cells_per_ray = 0;  // estimated cells crossed per ray before a hit
+    double cells_per_ray = 0;  // estimated cells crossed per ray before a hit or the grid's exit
     uint32_t max_refs = 0;     // fullest cell
 };
 

@@ -182,9 +182,9 @@ FR_API fr_status fr_device_timer_stop(fr_device* dev, float* ms);
  *                   rebuilding it; 0: always rebuild, as the reference does (default)
  *   "accel"         acceleration structure of a scene whose only enabled geometry is a sphere
  *                   geometry: 0: its BVH; 1: a uniform grid of the spheres (walked cell by cell
- *                   along each ray); 2 (default): the grid when it is expected to be faster
- *                   (at least 8192 spheres, a ray crossing at most 6 cells on average before a
- *                   hit, no cell with more than 64 spheres), else the BVH.  Other scenes always
+ *                   along each ray); 2 (default): the grid unless the spheres are clustered
+ *                   (a cell with more than 64 spheres) or a ray would cross more than 1024
+ *                   cells on average, else the BVH.  Other scenes always
  *                   use BVHs.  The closest hits do not depend on the choice: primitives hit
  *                   at exactly the same distance go to the lower (geometry, primitive) index
  *                   in every structure.

@@ -128,9 +128,9 @@ def test_automatic_choice(accel, gpu_device):
     accel(2)
     cases = {
         "dense": (_dense, True, ""),
-        "spheres_1k": (workloads.config1, False, "too few spheres"),
-        "sparse": (lambda d: workloads.random_spheres(d, 20000, 2000.0, 0.5, seed=3), False,
-                   "spheres too sparse"),
+        "spheres_1k": (workloads.config1, True, ""),
+        "hex": (workloads.hex_spheres, True, ""),
+        "sparse": (lambda d: workloads.random_spheres(d, 20000, 2000.0, 0.5, seed=3), True, ""),
         "clustered": (_dense_with_clump, False, "spheres too clustered"),
     }
     for name, (build, grid, reason) in cases.items():

@@ -22,11 +22,15 @@ pytestmark = pytest.mark.gpu
 
 @pytest.fixture
 def refit_on(gpu_device):
+    """Refit on, and sphere scenes traced through their BVH (refit is a BVH operation; the
+    automatic choice would give them a sphere grid, which is rebuilt instead)."""
     dd = gpu_device._device
-    old = dd.getOption("refit")
+    old = dd.getOption("refit"), dd.getOption("accel")
     dd.setOption("refit", 1)
+    dd.setOption("accel", 0)
     yield
-    dd.setOption("refit", old)
+    dd.setOption("refit", old[0])
+    dd.setOption("accel", old[1])
 
 
 def _move(scene, rng):

@@ -28,10 +28,10 @@ def _scene(device):
     return workloads.config1(device)
 
 
-SCENES = {
-    "spheres_bvh": (workloads.config1, False),
-    "dense_grid": (lambda d: workloads.config2(d, n=20000, box=140.0 * 0.02**(1 / 3)), True),
-    "mixed": (lambda d: workloads.config3(d, scale=0.002), False),
+SCENES = {  # scene, device option "accel", traced through a sphere grid
+    "spheres_bvh": (workloads.config1, 0, False),
+    "dense_grid": (lambda d: workloads.config2(d, n=20000, box=140.0 * 0.02**(1 / 3)), 2, True),
+    "mixed": (lambda d: workloads.config3(d, scale=0.002), 2, False),
 }
 
 
@@ -71,11 +71,17 @@ def test_static_render_matches_allocating_render(gpu_device, w, h, spp, ls):
 
 @pytest.mark.parametrize("name", list(SCENES))
 def test_static_render_matches_on_each_structure(gpu_device, name):
-    build, grid = SCENES[name]
-    scene, a, b = _pair(gpu_device, 160, 96, 2, build)
-    scene._scene.build()
-    assert scene._scene.getAccel()[0] == grid
-    _compare(scene, a, b, 160, 96, 6)
+    build, accel, grid = SCENES[name]
+    dd = gpu_device._device
+    old = dd.getOption("accel")
+    try:
+        dd.setOption("accel", accel)
+        scene, a, b = _pair(gpu_device, 160, 96, 2, build)
+        scene._scene.build()
+        assert scene._scene.getAccel()[0] == grid
+        _compare(scene, a, b, 160, 96, 6)
+    finally:
+        dd.setOption("accel", old)
 
 
 @pytest.mark.parametrize("option", ["persistent", "refill"])
@@ -84,7 +90,7 @@ def test_static_render_matches_with_kernel_options(gpu_device, option):
     old = dd.getOption(option)
     try:
         dd.setOption(option, 1)
-        build, _ = SCENES["dense_grid"]
+        build, _, _ = SCENES["dense_grid"]
         scene, a, b = _pair(gpu_device, 128, 80, 1, build)
         scene._scene.build()
         _compare(scene, a, b, 128, 80, 5)
