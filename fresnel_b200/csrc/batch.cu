@@ -507,6 +507,8 @@ cudaError_t batch_graph_create(const BatchDev& B, int width, uint32_t type_mask,
         return capture<4, MASK_GRID, true>(B, num_sms, capture_stream, exec);
     if (type_mask == MASK_GRID)  // every render of the batch traces a sphere grid
         return capture<4, MASK_GRID>(B, num_sms, capture_stream, exec);
+    if (type_mask == MASK_GRID_PARTS_FUSED)  // every render traces a grid over its parts
+        return capture<4, MASK_GRID_PARTS, true>(B, num_sms, capture_stream, exec);
     const bool spheres_only = (type_mask & ~MASK_SPHERES) == 0u;
     if (width == 4)
         return spheres_only ? capture<4, MASK_SPHERES>(B, num_sms, capture_stream, exec)

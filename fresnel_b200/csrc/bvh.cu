@@ -1305,6 +1305,35 @@ static cudaError_t refit_impl(const In& in, uint32_t n, const BuildParams& bp, B
     return collapse4(out, scratch, status, st);
 }
 
+namespace {
+__global__ void k_part_boxes(PartsInput in, uint32_t n, float4* lo, float4* hi)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const Box b = prim_bounds(in, i);
+    lo[i] = make_float4(b.lo.x, b.lo.y, b.lo.z, 0.0f);
+    hi[i] = make_float4(b.hi.x, b.hi.y, b.hi.z, 0.0f);
+}
+}  // namespace
+
+cudaError_t parts_boxes(const PartsInput& in, uint32_t n, float4* lo, float4* hi, cudaStream_t st)
+{
+    if (n == 0)
+        return cudaSuccess;
+    k_part_boxes<<<(n + 255) / 256, 256, 0, st>>>(in, n, lo, hi);
+    return cudaGetLastError();
+}
+
+cudaError_t gather_parts(const PartsInput& in, const uint32_t* prims, uint32_t total,
+                         float4* data, uint32_t* order, uint32_t* geom, cudaStream_t st)
+{
+    if (total == 0)
+        return cudaSuccess;
+    k_gather<<<(total + 255) / 256, 256, 0, st>>>(in, total, prims, data, order, geom);
+    return cudaGetLastError();
+}
+
 cudaError_t build_bvh(const BuildInput& in, uint32_t n, const BuildParams& bp, BvhBuffers& out,
                       Scratch& scratch, uint32_t* status, cudaStream_t st)
 {

@@ -131,6 +131,15 @@ cudaError_t refit_bvh(const PartsInput& in, uint32_t n, const BuildParams& bp, B
 cudaError_t build_bvh(const PartsInput& in, uint32_t n, const BuildParams& bp, BvhBuffers& out,
                       Scratch& scratch, uint32_t* status, cudaStream_t st);
 
+// The padded box of each of the n primitives of the parts of `in` (one thread per primitive, as
+// the tree builds compute them; an empty box, lower > upper, for a primitive left out).
+cudaError_t parts_boxes(const PartsInput& in, uint32_t n, float4* lo, float4* hi, cudaStream_t st);
+
+// For each of `total` references to primitives of `in` (combined numbering, prims[r]): its
+// leaf-slot record (2 float4 at data + 2 r), its index within its geometry and its geometry.
+cudaError_t gather_parts(const PartsInput& in, const uint32_t* prims, uint32_t total,
+                         float4* data, uint32_t* order, uint32_t* geom, cudaStream_t st);
+
 // Build the BVH of n primitives (n == 0 leaves an empty tree).  Synchronises the stream once
 // to read back the node count.
 // Construction errors (an inconsistent hierarchy) are reported by or-ing ERR_BUILD into

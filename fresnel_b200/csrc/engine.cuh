@@ -79,13 +79,17 @@ struct GridDev {
     const uint32_t* cell_start;
     const float4* ref_sphere;
     const uint32_t* ref_prim;
+    // 1: a grid over the primitives of several geometries (or one non-sphere geometry); its
+    // references are records laid out as a combined tree's leaf slots (SceneDev::leaf_data,
+    // leaf_geom, order), and ref_sphere / ref_prim / geom are unused
+    uint32_t parts;
 };
 
 struct SceneDev {
     const GeomDev* geoms;
     uint32_t n_geoms;
     uint32_t* status;  // error bits (device)
-    GridDev grid;      // sphere scenes traced through a uniform grid instead of a BVH
+    GridDev grid;      // scenes traced through a uniform grid instead of a BVH
     // Combined 4-wide tree over the primitives of several geometries (n_nodes4 == 0: none, each
     // enabled geometry's own tree is traversed in turn): leaf slot s holds 2 float4 of its
     // primitive's record, its geometry (leaf_geom) and its index within the geometry (order).
@@ -900,15 +904,16 @@ __device__ __forceinline__ bool grid_walk_begin(const GridDev& G, const RayK& ra
     return true;
 }
 
-// Tests the spheres of the walk's current cell and moves to the next cell; false when the walk
-// is over (the closest hit lies before the cell's exit, or the ray leaves the grid).  slot
-// receives the reference index of a closer hit.
-__device__ __forceinline__ bool grid_walk_step(const GridDev& G, const RayK& ray, float tnear,
-                                               float& tmax, uint32_t& slot, GridWalk& W,
-                                               TraceCount& tc)
+// Tests the primitives of the walk's current cell (test(first, last) over its reference range)
+// and moves to the next cell; false when the walk is over (the closest hit so far, tmax, lies
+// before the cell's exit, or the ray leaves the grid).
+template <class CellTest>
+__device__ __forceinline__ bool grid_walk_visit(const GridDev& G, const RayK& ray,
+                                                const float& tmax, GridWalk& W, TraceCount& tc,
+                                                const CellTest& test)
 {
     // the next cell along the ray, and its reference range loaded now so that the load
-    // overlaps the sphere tests of this cell
+    // overlaps the primitive tests of this cell
     const int sx = ray.inv.x >= 0.0f ? 1 : -1;
     const int sy = ray.inv.y >= 0.0f ? 1 : -1;
     const int sz = ray.inv.z >= 0.0f ? 1 : -1;
@@ -924,37 +929,8 @@ __device__ __forceinline__ bool grid_walk_step(const GridDev& G, const RayK& ray
         next_first = __ldg(G.cell_start + nc);
         next_last = __ldg(G.cell_start + nc + 1);
     }
-    const uint32_t last = W.last;
     tc.box += 1;
-    tc.prim += last - W.first;
-    // exact tie with the closest hit so far: the lower sphere index wins (one geometry)
-    const auto tie = [&](uint32_t r) {
-        return slot != MISS && __ldg(G.ref_prim + r) < __ldg(G.ref_prim + slot);
-    };
-    uint32_t k = W.first;
-    for (; k + 1 < last; k += 2) {  // two spheres in flight
-        const float4 q0 = ldg4(G.ref_sphere + k), q1 = ldg4(G.ref_sphere + k + 1);
-        float t0, t1;
-        if (sphere_t(ray.o, ray.d, v3(q0.x, q0.y, q0.z), q0.w, t0) && (tnear < t0) &&
-            ((t0 < tmax) || (t0 == tmax && tie(k)))) {
-            tmax = t0;
-            slot = k;
-        }
-        if (sphere_t(ray.o, ray.d, v3(q1.x, q1.y, q1.z), q1.w, t1) && (tnear < t1) &&
-            ((t1 < tmax) || (t1 == tmax && tie(k + 1)))) {
-            tmax = t1;
-            slot = k + 1;
-        }
-    }
-    if (k < last) {
-        const float4 q = ldg4(G.ref_sphere + k);
-        float t;
-        if (sphere_t(ray.o, ray.d, v3(q.x, q.y, q.z), q.w, t) && (tnear < t) &&
-            ((t < tmax) || (t == tmax && tie(k)))) {
-            tmax = t;
-            slot = k;
-        }
-    }
+    test(W.first, W.last);
     if (tmax <= t_cell || !more || --W.guard == 0u)
         return false;
     W.ix = nx;
@@ -969,6 +945,45 @@ __device__ __forceinline__ bool grid_walk_step(const GridDev& G, const RayK& ray
     W.first = next_first;
     W.last = next_last;
     return true;
+}
+
+// One cell of a sphere grid's walk (grid_walk_visit with the sphere tests); slot receives the
+// reference index of a closer hit.
+__device__ __forceinline__ bool grid_walk_step(const GridDev& G, const RayK& ray, float tnear,
+                                               float& tmax, uint32_t& slot, GridWalk& W,
+                                               TraceCount& tc)
+{
+    return grid_walk_visit(G, ray, tmax, W, tc, [&](uint32_t first, uint32_t last) {
+        tc.prim += last - first;
+        // exact tie with the closest hit so far: the lower sphere index wins (one geometry)
+        const auto tie = [&](uint32_t r) {
+            return slot != MISS && __ldg(G.ref_prim + r) < __ldg(G.ref_prim + slot);
+        };
+        uint32_t k = first;
+        for (; k + 1 < last; k += 2) {  // two spheres in flight
+            const float4 q0 = ldg4(G.ref_sphere + k), q1 = ldg4(G.ref_sphere + k + 1);
+            float t0, t1;
+            if (sphere_t(ray.o, ray.d, v3(q0.x, q0.y, q0.z), q0.w, t0) && (tnear < t0) &&
+                ((t0 < tmax) || (t0 == tmax && tie(k)))) {
+                tmax = t0;
+                slot = k;
+            }
+            if (sphere_t(ray.o, ray.d, v3(q1.x, q1.y, q1.z), q1.w, t1) && (tnear < t1) &&
+                ((t1 < tmax) || (t1 == tmax && tie(k + 1)))) {
+                tmax = t1;
+                slot = k + 1;
+            }
+        }
+        if (k < last) {
+            const float4 q = ldg4(G.ref_sphere + k);
+            float t;
+            if (sphere_t(ray.o, ray.d, v3(q.x, q.y, q.z), q.w, t) && (tnear < t) &&
+                ((t < tmax) || (t == tmax && tie(k)))) {
+                tmax = t;
+                slot = k;
+            }
+        }
+    });
 }
 
 // The whole walk of one ray.
@@ -993,12 +1008,37 @@ __device__ __forceinline__ Hit trace_grid_hit(const GridDev& G, const RayK& ray,
     return h;
 }
 
+// Closest hit through a grid over the primitives of several geometries (GridDev::parts): the
+// same walk, with each cell's references tested as the leaf slots of a combined tree (the test
+// and acceptance rule of every geometry type, ties to the lower (geometry, primitive) index).
+template <uint32_t TYPES>
+__device__ __forceinline__ Hit trace_grid_parts(const SceneDev& sc, const RayK& ray, float tnear,
+                                                float tmax, TraceCount& tc)
+{
+    const GridDev& G = sc.grid;
+    uint32_t hg = MISS, hs = 0;
+    GridWalk W;
+    if (grid_walk_begin(G, ray, W)) {
+        while (grid_walk_visit(G, ray, tmax, W, tc, [&](uint32_t first, uint32_t last) {
+            leaf_test_mixed<TYPES>(sc, ray, first, last - first, tnear, tmax, hg, hs, tc);
+        })) {
+        }
+    }
+    Hit h;
+    h.geom = hg;
+    h.prim = hg == MISS ? 0u : __ldg(sc.order + hs);
+    return h;
+}
+
 // Geometry-type masks a kernel is specialised for (bit FR_GEOM_* set = type handled).
 constexpr uint32_t MASK_SPHERES = 1u << FR_GEOM_SPHERE;
 constexpr uint32_t MASK_ALL = 0x1Fu;  // every FR_GEOM_* type
 // Kernels specialised for a scene of spheres traced through its uniform grid (SceneDev::grid),
 // with no BVH code compiled in.
 constexpr uint32_t MASK_GRID = 1u << 31;
+// Kernels specialised for a scene traced through a grid over its parts (GridDev::parts = 1),
+// every geometry type compiled in, no BVH code.
+constexpr uint32_t MASK_GRID_PARTS = MASK_GRID | MASK_ALL;
 
 // Blocks of 256 threads per SM the fused trace-and-shade kernels are compiled for.  The grid walk
 // fits 64 registers with few spills, and the fourth block hides its memory latency better (1080p
@@ -1052,7 +1092,8 @@ __device__ __forceinline__ Hit trace_closest_bvh(const SceneDev& sc, const RayK&
 
 // Closest hit over all enabled geometries of the scene.  WIDTH selects the binary (2) or
 // 4-wide (4) tree; MASK the geometry types compiled in (the host only launches a MASK that
-// covers every enabled geometry of the scene), or MASK_GRID for the sphere grid alone.
+// covers every enabled geometry of the scene), MASK_GRID for the sphere grid alone, or
+// MASK_GRID_PARTS for a grid over the scene's parts.
 template <int WIDTH, uint32_t MASK>
 __device__ __forceinline__ Hit trace_closest(const SceneDev& sc, V3 o, V3 d, float tnear,
                                              TraceCount& tc)
@@ -1061,10 +1102,16 @@ __device__ __forceinline__ Hit trace_closest(const SceneDev& sc, V3 o, V3 d, flo
     const float tmax = __int_as_float(0x7f800000);  // +inf
     if constexpr (MASK == MASK_GRID) {
         return trace_grid_hit(sc.grid, ray, tnear, tmax, tc);
+    } else if constexpr ((MASK & MASK_GRID) != 0u) {
+        return trace_grid_parts<MASK & MASK_ALL>(sc, ray, tnear, tmax, tc);
     } else {
         // kernels for BVH scenes also serve grid scenes (a batch may mix both)
-        if ((MASK & MASK_SPHERES) && sc.grid.n_cells != 0)
-            return trace_grid_hit(sc.grid, ray, tnear, tmax, tc);
+        if (sc.grid.n_cells != 0) {
+            if (sc.grid.parts)
+                return trace_grid_parts<MASK>(sc, ray, tnear, tmax, tc);
+            if (MASK & MASK_SPHERES)
+                return trace_grid_hit(sc.grid, ray, tnear, tmax, tc);
+        }
         return trace_closest_bvh<WIDTH, MASK>(sc, ray, tnear, tc);
     }
 }

@@ -1,18 +1,22 @@
-// grid.cu -- construction of the uniform sphere grid traced by trace_grid (engine.cuh).
+// grid.cu -- construction of the uniform grids traced by trace_grid and trace_grid_parts
+// (engine.cuh): over the spheres of one geometry, or over the primitives of the scene's parts.
 //
 // Steps, all on the stream of the build:
-//   1. bounding box of every sphere (centre +- radius, as the reference computes it, padded as
-//      the BVH builder pads its boxes), their union, the number of valid spheres and the sum of
-//      r^2 (one pass with warp reductions and atomics);
-//   2. on the host: the cell size (cells_per_prim cells per sphere over the union's volume) and,
-//      in automatic mode, the estimated number of cells a ray crosses before it meets a sphere
-//      or leaves the grid, min(mean free path / cell size, nx + ny + nz) with mean free path =
-//      volume / (n pi <r^2>);
-//   3. cells per sphere, their prefix sum, then one (cell, sphere) pair per covered cell written
-//      in sphere order and radix-sorted by cell (stable, so each cell lists its spheres in index
-//      order and the build is deterministic);
+//   1. bounding box of every primitive (a sphere's centre +- radius, as the reference computes
+//      it, padded as the BVH builder pads its boxes; a part's primitive box as the tree builds
+//      compute it), their union, the number of valid primitives and the sum of their mean
+//      cross-sections / pi (r^2 for a sphere, surface / (4 pi) for a box) (one pass with warp
+//      reductions and atomics);
+//   2. on the host: the cell size (cells_per_prim cells per primitive over the union's volume)
+//      and, in automatic mode, the estimated number of cells a ray crosses before it meets a
+//      primitive or leaves the grid, min(mean free path / cell size, nx + ny + nz) with mean
+//      free path = volume / (n pi <r^2>);
+//   3. cells per primitive, their prefix sum, then one (cell, primitive) pair per covered cell
+//      written in primitive order and radix-sorted by cell (stable, so each cell lists its
+//      primitives in index order and the build is deterministic);
 //   4. references per cell, their prefix sum (cell_start), the fullest cell, and the reference
-//      records: a copy of the sphere (x, y, z, r) and its index.
+//      records: for spheres a copy of the sphere (x, y, z, r) and its index; for parts the
+//      record, geometry and index of a combined tree's leaf slot.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -74,6 +78,44 @@ __device__ __forceinline__ SBox sphere_box(const float* pos, const float* rad, u
     return b;
 }
 
+// The primitives a grid is built over: a box per primitive (ok = false: left out) and its mean
+// cross-section / pi.
+struct SphereSource {
+    const float* pos;
+    const float* rad;
+    __device__ __forceinline__ SBox box(uint32_t i) const { return sphere_box(pos, rad, i); }
+    __device__ __forceinline__ double xsec(uint32_t i) const
+    {
+        const double r = double(rad[i]);
+        return r * r;
+    }
+};
+
+struct BoxSource {
+    const float4* lo;
+    const float4* hi;
+    __device__ __forceinline__ SBox box(uint32_t i) const
+    {
+        const float4 a = lo[i], b = hi[i];
+        SBox r;
+        r.lo[0] = a.x;
+        r.lo[1] = a.y;
+        r.lo[2] = a.z;
+        r.hi[0] = b.x;
+        r.hi[1] = b.y;
+        r.hi[2] = b.z;
+        r.ok = a.x <= b.x && a.y <= b.y && a.z <= b.z;  // the tree builds' empty box fails this
+        return r;
+    }
+    // a convex body's mean projected area is a quarter of its surface (Cauchy)
+    __device__ __forceinline__ double xsec(uint32_t i) const
+    {
+        const float4 a = lo[i], b = hi[i];
+        const double ex = double(b.x) - a.x, ey = double(b.y) - a.y, ez = double(b.z) - a.z;
+        return 2.0 * (ex * ey + ey * ez + ez * ex) / (4.0 * 3.14159265358979323846);
+    }
+};
+
 struct Shape {
     float lo[3], ih[3];
     uint32_t n[3];
@@ -85,22 +127,21 @@ __device__ __forceinline__ int cell_index(float x, const Shape& g, int k)
     return int(fminf(fmaxf(u, 0.0f), float(g.n[k] - 1u)));
 }
 
-// words: [0..2] min lo (order-preserving), [3..5] max hi, [6] valid spheres
-__global__ void k_grid_bounds(const float* pos, const float* rad, uint32_t n, uint32_t* words,
-                              double* r2sum)
+// words: [0..2] min lo (order-preserving), [3..5] max hi, [6] valid primitives
+template <class Src>
+__global__ void k_grid_bounds(Src src, uint32_t n, uint32_t* words, double* r2sum)
 {
     uint32_t mn[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, mx[3] = {0u, 0u, 0u}, cnt = 0;
     double r2 = 0.0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const SBox b = sphere_box(pos, rad, i);
+        const SBox b = src.box(i);
         if (!b.ok)
             continue;
         for (int k = 0; k < 3; ++k) {
             mn[k] = min(mn[k], f2o(b.lo[k]));
             mx[k] = max(mx[k], f2o(b.hi[k]));
         }
-        const double r = double(rad[i]);
-        r2 += r * r;
+        r2 += src.xsec(i);
         ++cnt;
     }
     for (int off = 16; off > 0; off >>= 1) {
@@ -121,14 +162,15 @@ __global__ void k_grid_bounds(const float* pos, const float* rad, uint32_t n, ui
     }
 }
 
-// cells covered by each sphere (0 for invalid ones); flag bit 0: a sphere covers too many
-__global__ void k_grid_count(const float* pos, const float* rad, uint32_t n, Shape g,
-                             uint32_t max_per_prim, uint32_t* counts, uint32_t* flag)
+// cells covered by each primitive (0 for invalid ones); flag bit 0: one covers too many
+template <class Src>
+__global__ void k_grid_count(Src src, uint32_t n, Shape g, uint32_t max_per_prim,
+                             uint32_t* counts, uint32_t* flag)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
-    const SBox b = sphere_box(pos, rad, i);
+    const SBox b = src.box(i);
     uint32_t c = 0;
     if (b.ok) {
         unsigned long long m = 1;
@@ -142,14 +184,14 @@ __global__ void k_grid_count(const float* pos, const float* rad, uint32_t n, Sha
     counts[i] = c;
 }
 
-__global__ void k_grid_emit(const float* pos, const float* rad, uint32_t n, Shape g,
-                            const uint32_t* counts, const uint32_t* offsets, uint32_t* keys,
-                            uint32_t* vals)
+template <class Src>
+__global__ void k_grid_emit(Src src, uint32_t n, Shape g, const uint32_t* counts,
+                            const uint32_t* offsets, uint32_t* keys, uint32_t* vals)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || counts[i] == 0)
         return;
-    const SBox b = sphere_box(pos, rad, i);
+    const SBox b = src.box(i);
     int i0[3], i1[3];
     for (int k = 0; k < 3; ++k) {
         i0[k] = cell_index(b.lo[k], g, k);
@@ -209,15 +251,42 @@ uint32_t blocks_for(size_t n, uint32_t cap = 0x7fffffffu)
 
 }  // namespace
 
-cudaError_t build_grid(const float* position, const float* radius, uint32_t n,
-                       const GridParams& gp, GridBuffers& out, Scratch& scratch, cudaStream_t st,
-                       GridReport& rep)
+namespace {
+
+// Why a grid was not built, in the words of its primitives.
+struct Reasons {
+    const char *none, *no_valid, *few, *sparse, *spans, *refs, *clustered;
+};
+const Reasons SPHERE_REASONS = {"no spheres",
+                                "no valid sphere",
+                                "too few spheres",
+                                "spheres too sparse",
+                                "a sphere spans too many cells",
+                                "too many sphere references",
+                                "spheres too clustered"};
+const Reasons PART_REASONS = {"no primitives",
+                              "no valid primitive",
+                              "too few primitives",
+                              "primitives too sparse",
+                              "a primitive spans too many cells",
+                              "too many primitive references",
+                              "primitives too clustered"};
+
+// Steps 1-4 but the reference records: cell_start, the shape, and the primitive of every
+// reference in *vals_sorted (scratch memory, valid until the scratch is next reserved).  A grid
+// that should not be used leaves out.n_cells == 0 with rep.built false and rep.reason set.
+template <class Src>
+cudaError_t build_cells(const Src& src, uint32_t n, const Reasons& why, const GridParams& gp,
+                        GridBuffers& out, Scratch& scratch, cudaStream_t st, GridReport& rep,
+                        const uint32_t*& vals_out, uint32_t& total_out)
 {
     rep = GridReport();
     out.n_cells = 0;
     out.n_refs = 0;
+    vals_out = nullptr;
+    total_out = 0;
     if (n == 0) {
-        rep.reason = "no spheres";
+        rep.reason = why.none;
         return cudaSuccess;
     }
     cudaError_t e;
@@ -241,7 +310,7 @@ cudaError_t build_grid(const float* position, const float* radius, uint32_t n,
         return e;
     if ((e = cudaMemsetAsync(r2sum, 0, sizeof(double), st)) != cudaSuccess)
         return e;
-    k_grid_bounds<<<blocks_for(n, 148u * 8u), 256, 0, st>>>(position, radius, n, words, r2sum);
+    k_grid_bounds<<<blocks_for(n, 148u * 8u), 256, 0, st>>>(src, n, words, r2sum);
     uint32_t hw[16];
     double hr2 = 0.0;
     if ((e = cudaMemcpyAsync(hw, words, sizeof(hw), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
@@ -251,7 +320,7 @@ cudaError_t build_grid(const float* position, const float* radius, uint32_t n,
         return e;
     rep.n_valid = hw[6];
     if (rep.n_valid == 0) {
-        rep.reason = "no valid sphere";
+        rep.reason = why.no_valid;
         return cudaSuccess;
     }
     // ---- 2. cell size and the automatic choice
@@ -294,11 +363,11 @@ cudaError_t build_grid(const float* position, const float* radius, uint32_t n,
     rep.cells_per_ray = std::min(rep.cells_per_ray, double(dims[0]) + dims[1] + dims[2]);
     if (gp.mode == 2) {
         if (rep.n_valid < gp.min_prims) {
-            rep.reason = "too few spheres";
+            rep.reason = why.few;
             return cudaSuccess;
         }
         if (rep.cells_per_ray > gp.max_cells_per_ray) {
-            rep.reason = "spheres too sparse";
+            rep.reason = why.sparse;
             return cudaSuccess;
         }
     }
@@ -312,7 +381,7 @@ cudaError_t build_grid(const float* position, const float* radius, uint32_t n,
     if ((e = out.prim_count.reserve(n)) != cudaSuccess ||
         (e = out.prim_offset.reserve(n)) != cudaSuccess)
         return e;
-    k_grid_count<<<blocks_for(n), 256, 0, st>>>(position, radius, n, g, gp.max_cells_per_prim,
+    k_grid_count<<<blocks_for(n), 256, 0, st>>>(src, n, g, gp.max_cells_per_prim,
                                                  out.prim_count.ptr, words + 8);
     if ((e = cub::DeviceScan::ExclusiveSum(scan_tmp, scan_n_bytes, out.prim_count.ptr,
                                            out.prim_offset.ptr, int(n), st)) != cudaSuccess)
@@ -326,13 +395,13 @@ cudaError_t build_grid(const float* position, const float* radius, uint32_t n,
         (e = cudaStreamSynchronize(st)) != cudaSuccess)
         return e;
     if (flag) {
-        rep.reason = "a sphere spans too many cells";
+        rep.reason = why.spans;
         return cudaSuccess;
     }
     const uint64_t total64 = uint64_t(last[0]) + last[1];
     if (total64 == 0 || total64 > uint64_t(1u << 30) ||
         total64 > 32 * uint64_t(rep.n_valid) + (uint64_t(1) << 20)) {
-        rep.reason = "too many sphere references";
+        rep.reason = why.refs;
         return cudaSuccess;
     }
     const uint32_t total = uint32_t(total64);
@@ -364,12 +433,10 @@ cudaError_t build_grid(const float* position, const float* radius, uint32_t n,
     cell_counts = L2.at(cell_counts);
     max_word = L2.at(max_word);
     tmp = L2.at(tmp);
-    if ((e = out.cell_start.reserve(size_t(nc) + 1)) != cudaSuccess ||
-        (e = out.ref_sphere.reserve(total)) != cudaSuccess ||
-        (e = out.ref_prim.reserve(total)) != cudaSuccess)
+    if ((e = out.cell_start.reserve(size_t(nc) + 1)) != cudaSuccess)
         return e;
-    k_grid_emit<<<blocks_for(n), 256, 0, st>>>(position, radius, n, g, out.prim_count.ptr,
-                                                out.prim_offset.ptr, keys, vals);
+    k_grid_emit<<<blocks_for(n), 256, 0, st>>>(src, n, g, out.prim_count.ptr, out.prim_offset.ptr,
+                                                keys, vals);
     if ((e = cub::DeviceRadixSort::SortPairs(tmp, sort_bytes, keys, keys_sorted, vals,
                                              vals_sorted, int(total), 0, end_bit, st)) !=
         cudaSuccess)
@@ -384,8 +451,6 @@ cudaError_t build_grid(const float* position, const float* radius, uint32_t n,
     if ((e = cub::DeviceScan::ExclusiveSum(tmp, scan_c_bytes, cell_counts, out.cell_start.ptr,
                                            int(nc + 1), st)) != cudaSuccess)
         return e;
-    k_grid_gather<<<blocks_for(total), 256, 0, st>>>(vals_sorted, total, position, radius,
-                                                      out.ref_sphere.ptr, out.ref_prim.ptr);
     uint32_t max_refs = 0;
     if ((e = cudaGetLastError()) != cudaSuccess ||
         (e = cudaMemcpyAsync(&max_refs, max_word, 4, cudaMemcpyDeviceToHost, st)) !=
@@ -394,17 +459,71 @@ cudaError_t build_grid(const float* position, const float* radius, uint32_t n,
         return e;
     rep.max_refs = max_refs;
     if (gp.mode == 2 && max_refs > gp.max_refs_per_cell) {
-        rep.reason = "spheres too clustered";
+        rep.reason = why.clustered;
         return cudaSuccess;
     }
-    out.n_cells = nc;
-    out.n_refs = total;
     for (int k = 0; k < 3; ++k) {
         out.dims[k] = dims[k];
         out.lo[k] = flo[k];
         out.hi[k] = fhi[k];
         out.cell[k] = cell[k];
     }
+    vals_out = vals_sorted;
+    total_out = total;
+    return cudaSuccess;
+}
+
+}  // namespace
+
+cudaError_t build_grid(const float* position, const float* radius, uint32_t n,
+                       const GridParams& gp, GridBuffers& out, Scratch& scratch, cudaStream_t st,
+                       GridReport& rep)
+{
+    const uint32_t* vals = nullptr;
+    uint32_t total = 0;
+    cudaError_t e = build_cells(SphereSource{position, radius}, n, SPHERE_REASONS, gp, out,
+                                scratch, st, rep, vals, total);
+    if (e != cudaSuccess || vals == nullptr)
+        return e;
+    if ((e = out.ref_sphere.reserve(total)) != cudaSuccess ||
+        (e = out.ref_prim.reserve(total)) != cudaSuccess)
+        return e;
+    k_grid_gather<<<blocks_for(total), 256, 0, st>>>(vals, total, position, radius,
+                                                      out.ref_sphere.ptr, out.ref_prim.ptr);
+    if ((e = cudaGetLastError()) != cudaSuccess || (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return e;
+    out.parts = false;
+    out.n_cells = uint32_t(uint64_t(out.dims[0]) * out.dims[1] * out.dims[2]);
+    out.n_refs = total;
+    rep.built = true;
+    rep.reason = "";
+    return cudaSuccess;
+}
+
+cudaError_t build_grid(const PartsInput& in, uint32_t n, const GridParams& gp, GridBuffers& out,
+                       Scratch& scratch, cudaStream_t st, GridReport& rep)
+{
+    cudaError_t e;
+    if (n != 0 && ((e = out.box_lo.reserve(n)) != cudaSuccess ||
+                   (e = out.box_hi.reserve(n)) != cudaSuccess ||
+                   (e = parts_boxes(in, n, out.box_lo.ptr, out.box_hi.ptr, st)) != cudaSuccess))
+        return e;
+    const uint32_t* vals = nullptr;
+    uint32_t total = 0;
+    e = build_cells(BoxSource{out.box_lo.ptr, out.box_hi.ptr}, n, PART_REASONS, gp, out, scratch,
+                    st, rep, vals, total);
+    if (e != cudaSuccess || vals == nullptr)
+        return e;
+    if ((e = out.ref_data.reserve(2 * size_t(total))) != cudaSuccess ||
+        (e = out.ref_prim.reserve(total)) != cudaSuccess ||
+        (e = out.ref_geom.reserve(total)) != cudaSuccess ||
+        (e = gather_parts(in, vals, total, out.ref_data.ptr, out.ref_prim.ptr, out.ref_geom.ptr,
+                          st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return e;
+    out.parts = true;
+    out.n_cells = uint32_t(uint64_t(out.dims[0]) * out.dims[1] * out.dims[2]);
+    out.n_refs = total;
     rep.built = true;
     rep.reason = "";
     return cudaSuccess;

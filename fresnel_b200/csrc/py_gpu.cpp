@@ -752,11 +752,12 @@ PYBIND11_MODULE(_gpu, m)
         .def(py::init<std::shared_ptr<DeviceH>>())
         .def("getAccel",
              [](SceneH& s) {
-                 // (uses a sphere grid, why not when one was considered) after the last build
+                 // (grid kind: 0 BVHs, 1 sphere grid, 2 grid over the scene's parts; why no
+                 // grid when one was considered) after the last build
                  int grid = 0;
                  char reason[128];
                  check(fr_scene_get_accel(s.scene, &grid, reason, sizeof(reason)));
-                 return py::make_tuple(grid != 0, std::string(reason));
+                 return py::make_tuple(grid, std::string(reason));
              })
         .def("setCamera", [](SceneH& s, const UserCamera& c) { s.camera = c; })
         .def("getCamera", [](SceneH& s) -> UserCamera& { return s.camera; },

@@ -821,8 +821,10 @@ LaunchShape path_launch_shape(int num_sms)
     s.extend_grid[3] = num_sms * blocks_per_sm(k_path_extend<4, MASK_ALL>);
     s.extend_grid_sphere_grid = num_sms * blocks_per_sm(k_path_extend<4, MASK_GRID>);
     s.refill_grid_sphere_grid = num_sms * blocks_per_sm(k_path_extend_grid_refill);
+    s.extend_grid_parts_grid = num_sms * blocks_per_sm(k_path_extend<4, MASK_GRID_PARTS>);
     s.bounce_grid[0] = num_sms * fused_blocks(MASK_ALL);
     s.bounce_grid[1] = num_sms * fused_blocks(MASK_GRID);
+    s.bounce_grid[2] = num_sms * fused_blocks(MASK_GRID_PARTS);
     s.persistent_grid[0] = num_sms * blocks_per_sm(k_path_extend_persistent<MASK_SPHERES>);
     s.persistent_grid[1] = num_sms * blocks_per_sm(k_path_extend_persistent<MASK_ALL>);
     s.primary_grid[0] = num_sms * blocks_per_sm(k_path_primary_persistent<MASK_SPHERES>);
@@ -830,13 +832,20 @@ LaunchShape path_launch_shape(int num_sms)
     return s;
 }
 
+// The kernels a frame runs: 0 for BVH scenes, 1 for a sphere grid, 2 for a grid over parts.
+static int grid_kind(const FrameParams& P)
+{
+    return P.scene.grid.n_cells == 0 ? 0 : (P.scene.grid.parts ? 2 : 1);
+}
+
 void launch_path_primary(const FrameParams& P, const PathState& S, const LaunchShape& shape,
                          cudaStream_t st)
 {
     bool spheres_only = (P.type_mask & ~MASK_SPHERES) == 0u;
-    if (P.scene.grid.n_cells != 0) {
+    if (const int gk = grid_kind(P)) {
         const uint32_t n = primary_items(P.w, P.h, P.batch, P.tile_log2);
-        k_path_primary<4, MASK_GRID><<<(n + 255) / 256, 256, 0, st>>>(P, S);
+        auto k = gk == 1 ? k_path_primary<4, MASK_GRID> : k_path_primary<4, MASK_GRID_PARTS>;
+        k<<<(n + 255) / 256, 256, 0, st>>>(P, S);
         return;
     }
     if (P.bvh_width == 4 && P.persistent) {
@@ -859,8 +868,8 @@ void launch_path_primary_shade(const FrameParams& P, const PathState& S, cudaStr
     const uint32_t n_items = primary_items(P.w, P.h, P.batch, P.tile_log2);
     auto k = pick(P, k_path_primary_shade<2, MASK_SPHERES>, k_path_primary_shade<2, MASK_ALL>,
                   k_path_primary_shade<4, MASK_SPHERES>, k_path_primary_shade<4, MASK_ALL>);
-    if (P.scene.grid.n_cells != 0)
-        k = k_path_primary_shade<4, MASK_GRID>;
+    if (const int gk = grid_kind(P))
+        k = gk == 1 ? k_path_primary_shade<4, MASK_GRID> : k_path_primary_shade<4, MASK_GRID_PARTS>;
     k<<<(n_items + 255) / 256, 256, 0, st>>>(P, S);
 }
 
@@ -887,8 +896,10 @@ void launch_path_extend(const FrameParams& P, const PathState& S, int iteration,
 {
     bool spheres_only = (P.type_mask & ~MASK_SPHERES) == 0u;
     int q = iteration & 1;
-    if (P.scene.grid.n_cells != 0) {
-        if (P.refill)
+    if (const int gk = grid_kind(P)) {
+        if (gk == 2)
+            k_path_extend<4, MASK_GRID_PARTS><<<shape.extend_grid_parts_grid, 256, 0, st>>>(P, S, q);
+        else if (P.refill)
             k_path_extend_grid_refill<<<shape.refill_grid_sphere_grid, 256, 0, st>>>(P, S, q);
         else
             k_path_extend<4, MASK_GRID><<<shape.extend_grid_sphere_grid, 256, 0, st>>>(P, S, q);
@@ -920,10 +931,10 @@ void launch_path_bounce(const FrameParams& P, const PathState& S, int iteration,
     const int q = iteration & 1;
     auto k = pick(P, k_path_bounce<2, MASK_SPHERES>, k_path_bounce<2, MASK_ALL>,
                   k_path_bounce<4, MASK_SPHERES>, k_path_bounce<4, MASK_ALL>);
-    const bool grid = P.scene.grid.n_cells != 0;
-    if (grid)
-        k = k_path_bounce<4, MASK_GRID>;
-    k<<<shape.bounce_grid[grid ? 1 : 0], 256, 0, st>>>(P, S, q);
+    const int gk = grid_kind(P);
+    if (gk)
+        k = gk == 1 ? k_path_bounce<4, MASK_GRID> : k_path_bounce<4, MASK_GRID_PARTS>;
+    k<<<shape.bounce_grid[gk], 256, 0, st>>>(P, S, q);
 }
 
 void launch_path_tail(const FrameParams& P, const PathState& S, int iteration,
@@ -932,10 +943,10 @@ void launch_path_tail(const FrameParams& P, const PathState& S, int iteration,
     const int q = iteration & 1;
     auto k = pick(P, k_path_tail<2, MASK_SPHERES>, k_path_tail<2, MASK_ALL>,
                   k_path_tail<4, MASK_SPHERES>, k_path_tail<4, MASK_ALL>);
-    const bool grid = P.scene.grid.n_cells != 0;
-    if (grid)
-        k = k_path_tail<4, MASK_GRID>;
-    k<<<shape.bounce_grid[grid ? 1 : 0], 256, 0, st>>>(P, S, q);
+    const int gk = grid_kind(P);
+    if (gk)
+        k = gk == 1 ? k_path_tail<4, MASK_GRID> : k_path_tail<4, MASK_GRID_PARTS>;
+    k<<<shape.bounce_grid[gk], 256, 0, st>>>(P, S, q);
 }
 
 void launch_histogram(const float4* linear, uint32_t n, uint32_t* counts, int num_sms,
@@ -952,8 +963,8 @@ void launch_preview(const FrameParams& P, uint32_t aa_n, uint2* hits, cudaStream
     dim3 grid((P.w + 15) / 16, (P.h + 15) / 16);
     auto k = pick(P, k_preview<2, MASK_SPHERES>, k_preview<2, MASK_ALL>,
                   k_preview<4, MASK_SPHERES>, k_preview<4, MASK_ALL>);
-    if (P.scene.grid.n_cells != 0)
-        k = k_preview<4, MASK_GRID>;
+    if (const int gk = grid_kind(P))
+        k = gk == 1 ? k_preview<4, MASK_GRID> : k_preview<4, MASK_GRID_PARTS>;
     k<<<grid, block, 0, st>>>(P, aa_n, hits);
 }
 

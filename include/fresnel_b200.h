@@ -125,7 +125,7 @@ typedef struct fr_stats {
     double primary_ms, shade_ms, extend_ms;
     uint64_t primary_launches, shade_launches, extend_launches;
     uint64_t bvh_refits;    /* of bvh_builds, how many refitted an existing tree */
-    uint64_t grid_builds;   /* sphere grids built (device option "accel") */
+    uint64_t grid_builds;   /* grids built (device option "accel") */
     uint32_t last_render_grid; /* 1 if the last render traced through a sphere grid */
 } fr_stats;
 
@@ -180,15 +180,18 @@ FR_API fr_status fr_device_timer_stop(fr_device* dev, float* ms);
  *   "refit"         1: when a geometry's arrays change but its primitive count and the build
  *                   options do not, refit its tree (new boxes, same topology) instead of
  *                   rebuilding it; 0: always rebuild, as the reference does (default)
- *   "accel"         acceleration structure of a scene whose only enabled geometry is a sphere
- *                   geometry: 0: its BVH; 1: a uniform grid of the spheres (walked cell by cell
- *                   along each ray); 2 (default): the grid unless the spheres are clustered
- *                   (a cell with more than 64 spheres) or a ray would cross more than 1024
- *                   cells on average, else the BVH.  Other scenes always
- *                   use BVHs.  The closest hits do not depend on the choice: primitives hit
- *                   at exactly the same distance go to the lower (geometry, primitive) index
- *                   in every structure.
- *   "grid_density"  grid cells per sphere (default 1.5; (0, 64])
+ *   "accel"         acceleration structure: 0: BVHs; 1: a uniform grid (walked cell by cell
+ *                   along each ray) over the spheres of a scene whose only enabled geometry
+ *                   holds spheres, else over the primitives of all its enabled geometries (at
+ *                   most 8); 2 (default): the same grids, over parts only when every enabled
+ *                   geometry holds spheres or cylinders, and only unless the primitives are
+ *                   clustered (a cell with more than 64 of them) or a ray would cross more
+ *                   than 1024 cells on average; else BVHs.  A primitive spanning more than
+ *                   4096 cells leaves any scene to its BVHs.
+ *                   The closest hits do not depend on the choice: primitives hit at exactly
+ *                   the same distance go to the lower (geometry, primitive) index in every
+ *                   structure.
+ *   "grid_density"  grid cells per primitive (default 1.5; (0, 64])
  *   "fuse_shade"    1 (default): the primary pass also shades each primary hit and queues the
  *                   continuing paths itself (the first shade pass of a wavefront is not
  *                   launched), and for scenes traced through a sphere grid each bounce traces
@@ -212,8 +215,9 @@ FR_API fr_status fr_device_set_profiling(fr_device* dev, int enable);
 /* Scene::Scene (fresnel/gpu/Scene.cc:15-28). */
 FR_API fr_status fr_scene_create(fr_device* dev, fr_scene** out);
 /* Which acceleration structure the scene's last build chose (no counterpart in the reference):
- * *grid = 1 for a sphere grid, 0 for BVHs; reason (nullable, cap bytes) receives why a grid was
- * not chosen when one was considered ("" otherwise). */
+ * *grid = 1 for a sphere grid, 2 for a grid over the primitives of several geometries (or of one
+ * non-sphere geometry), 0 for BVHs; reason (nullable, cap bytes) receives why a grid was not
+ * chosen when one was considered ("" otherwise). */
 FR_API fr_status fr_scene_get_accel(const fr_scene* scene, int* grid, char* reason, size_t cap);
 FR_API fr_status fr_scene_destroy(fr_scene* scene);
 

@@ -6,8 +6,9 @@ path's arithmetic depends only on its (pixel, sample, light sample), and the run
 samples in sample order. Its images must therefore equal the allocating entry point's. The test
 compares them within 1e-6 after each of two calls in a row (the second call continues the first
 one's running mean), on a sphere scene traced through its BVH, a dense sphere scene traced
-through the sphere grid (also with the persistent and per-lane-refill kernel options) and a
-scene of every geometry type traced through one combined tree. It also checks the size limit,
+through the sphere grid (also with the persistent and per-lane-refill kernel options), a scene
+of every geometry type traced through one combined tree and a scene of spheres and bonds traced
+through the grid over its parts. It also checks the size limit,
 the built-scene rule, and that a static render leaves no stale primary hits behind.
 
 The file name sorts last so that pytest collects it after every other test. It passes alone too.
@@ -28,10 +29,11 @@ def _scene(device):
     return workloads.config1(device)
 
 
-SCENES = {  # scene, device option "accel", traced through a sphere grid
-    "spheres_bvh": (workloads.config1, 0, False),
-    "dense_grid": (lambda d: workloads.config2(d, n=20000, box=140.0 * 0.02**(1 / 3)), 2, True),
-    "mixed": (lambda d: workloads.config3(d, scale=0.002), 2, False),
+SCENES = {  # scene, device option "accel", grid kind (0 trees, 1 sphere grid, 2 parts grid)
+    "spheres_bvh": (workloads.config1, 0, 0),
+    "dense_grid": (lambda d: workloads.config2(d, n=20000, box=140.0 * 0.02**(1 / 3)), 2, 1),
+    "mixed": (lambda d: workloads.config3(d, scale=0.002), 2, 0),
+    "parts_grid": (lambda d: workloads.serving_scene(d, 4000, 5), 2, 2),
 }
 
 
