@@ -9,6 +9,7 @@
 //   fr_tracer    output buffers (linear RGBA f32, sRGB RGBA8) and the path tracer's per-pixel
 //                wavefront state (allocated on first path render)
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <limits>
@@ -183,6 +184,7 @@ struct fr_geometry {
     uint32_t n_vertices = 0;
     uint32_t n_planes = 0;
     float poly_radius = 0.0f;
+    float mesh_radius = 0.0f;  // mesh: the largest vertex distance from the instance origin
     float color_by_face = 0.0f;
     bool enabled = true;
     bool removed = false;
@@ -463,12 +465,12 @@ std::vector<fr_geometry*> combined_parts(const fr_scene* sc, std::vector<uint64_
 // only enabled geometry when it holds spheres (kind 1, a sphere grid; gi receives its scene
 // index), else the trees of all its enabled geometries, at most MAX_PARTS (kind 2, a grid over
 // their primitives; parts receives them in scene order).  In automatic mode (accel 2) a grid
-// over parts is considered only when they hold spheres and cylinders: there it traced scenes of
-// 1e4 to 2e6 primitives 1.5x to 1.8x faster than the trees, while polyhedra and meshes, whose
-// boxes span many cells and whose tests cost several sphere tests, made it slower than the
-// combined tree (the 470k-primitive mixed scene: 89.7-110.6 against 80.1 ms per frame at 0.75
-// to 6 cells per primitive).  key identifies what a grid build depends on.  Returns the kind,
-// or 0 when no grid applies.
+// over parts is considered only when none of them is a mesh: spheres and bonds of 1e4 to 2e6
+// primitives traced 1.5x to 1.8x faster than through the trees, the mixed scene without its
+// icosahedra (200k spheres, 50k bonds, 20k cubes) 1.38x and 1080 polygons with 400 spheres
+// 1.38x, but 10k icosahedra alone (200k triangles) 1.8x slower: each triangle is a reference
+// tested after its instance's bounding sphere, where a tree culls triangle by triangle.  key
+// identifies what a grid build depends on.  Returns the kind, or 0 when no grid applies.
 int grid_candidate(const fr_scene* sc, std::vector<uint64_t>& key, uint32_t& gi,
                    std::vector<fr_geometry*>* parts = nullptr)
 {
@@ -493,7 +495,7 @@ int grid_candidate(const fr_scene* sc, std::vector<uint64_t>& key, uint32_t& gi,
     const int kind = (on.size() == 1 && on[0]->type == FR_GEOM_SPHERE) ? 1 : 2;
     if (kind == 2 && dev->accel == 2)
         for (const fr_geometry* g : on)
-            if (g->type != FR_GEOM_SPHERE && g->type != FR_GEOM_CYLINDER)
+            if (g->type == FR_GEOM_MESH)
                 return 0;
     uint32_t density_bits;
     std::memcpy(&density_bits, &dev->grid_cells_per_prim, sizeof(density_bits));
@@ -774,6 +776,7 @@ fr_status prepare_scene(fr_scene* sc, fr_tracer* tr)
             d.n_planes = g->n_planes;
             d.n_vertices = g->type == FR_GEOM_POLYGON ? g->n_vertices : 0u;
             d.rounding_radius = g->rounding_radius;
+            d.bound_radius = g->type == FR_GEOM_MESH ? g->mesh_radius : g->poly_radius;
             d.color_by_face = g->color_by_face;
             d.outline_width = g->outline_width;
             d.material = to_mat(g->material);
@@ -1376,6 +1379,15 @@ fr_status fr_geometry_create_mesh(fr_scene* scene, const float* vertices, uint32
         return s;
     g->n_vertices = n_vertices;
     g->n_faces = n_vertices / 3;
+    double r2 = 0.0;  // a NaN vertex is passed over: its triangles have no valid box anyway
+    for (uint32_t i = 0; i < n_vertices; ++i) {
+        const double x = vertices[3 * size_t(i)], y = vertices[3 * size_t(i) + 1],
+                     z = vertices[3 * size_t(i) + 2];
+        const double q = x * x + y * y + z * z;
+        if (q > r2)
+            r2 = q;
+    }
+    g->mesh_radius = float(std::sqrt(r2) * (1.0 + 1e-6));
     cudaError_t e = use_device(scene->dev) == FR_OK ? g->vertices.reserve(size_t(n_vertices) * 3)
                                                     : cudaErrorUnknown;
     if (e == cudaSuccess && n_vertices)

@@ -58,6 +58,8 @@ struct GeomDev {
     uint32_t n_planes;
     uint32_t n_vertices;    // polygon: vertices [n_vertices][2]
     float rounding_radius;  // polygon
+    float bound_radius;     // polyhedron, polygon: bounding radius about the position; mesh: the
+                            // largest vertex distance from the instance origin
     float color_by_face;
     float outline_width;
     Mat material;
@@ -782,6 +784,48 @@ __device__ __forceinline__ void traverse4(const GeomDev& g, uint32_t gi, const R
                    });
 }
 
+// Test of leaf slot s of a combined tree (or reference s of a grid over parts) of geometry g,
+// its record's first float4 in a: whether the ray meets the primitive, and where (t).  tmax and
+// tie serve the polyhedron slab test's acceptance of an exit at exactly tmax.
+template <uint32_t MASK, class Tie>
+__device__ __forceinline__ bool mixed_prim_t(const SceneDev& sc, const GeomDev& g, int type,
+                                             float4 a, uint32_t s, const RayK& ray, float tnear,
+                                             float tmax, const Tie& tie, float& t)
+{
+    t = 0.0f;
+    if ((MASK & (1u << FR_GEOM_SPHERE)) && type == FR_GEOM_SPHERE)
+        return sphere_t(ray.o, ray.d, v3(a.x, a.y, a.z), a.w, t);
+    if ((MASK & (1u << FR_GEOM_CYLINDER)) && type == FR_GEOM_CYLINDER) {
+        const float4 b = ldg4(sc.leaf_data + 2 * size_t(s) + 1);
+        float de;
+        V3 N;
+        uint32_t ci;
+        return isect_spherocylinder(t, de, N, ci, ray.o, ray.d, v3(a.x, a.y, a.z),
+                                    v3(b.x, b.y, b.z), a.w);
+    }
+    if ((MASK & (1u << FR_GEOM_POLYHEDRON)) && type == FR_GEOM_POLYHEDRON) {
+        const float4 b = ldg4(sc.leaf_data + 2 * size_t(s) + 1);
+        PolyHit ph = poly_planes(g, ray.o, ray.d, v3(a.x, a.y, a.z), Qt{b.x, v3(b.y, b.z, b.w)},
+                                 tnear, tmax, tie);
+        t = ph.t;
+        return ph.hit;
+    }
+    if ((MASK & (1u << FR_GEOM_MESH)) && type == FR_GEOM_MESH) {
+        const float4 b = ldg4(sc.leaf_data + 2 * size_t(s) + 1);
+        TriHit th = mesh_triangle(g, __float_as_uint(a.w), ray.o, ray.d, v3(a.x, a.y, a.z),
+                                  Qt{b.x, v3(b.y, b.z, b.w)});
+        t = th.t;
+        return th.hit;
+    }
+    if ((MASK & (1u << FR_GEOM_POLYGON)) && type == FR_GEOM_POLYGON) {
+        const float4 b = ldg4(sc.leaf_data + 2 * size_t(s) + 1);
+        PgHit ph = polygon_hit(g, ray.o, ray.d, a.x, a.y, Qt{b.x, v3(b.y, b.z, b.w)});
+        t = ph.t;
+        return ph.hit;
+    }
+    return false;
+}
+
 // Leaf of a combined tree: each slot names its geometry; the primitive test is that geometry
 // type's (only the types in MASK are compiled in).
 template <uint32_t MASK>
@@ -796,7 +840,6 @@ __device__ __forceinline__ void leaf_test_mixed(const SceneDev& sc, const RayK& 
         if (gi >= sc.n_geoms)
             continue;
         const GeomDev& g = sc.geoms[gi];
-        const int type = g.type;
         const float4 a = ldg4(sc.leaf_data + 2 * size_t(s));
         // exact tie with the closest hit so far: the lower (geometry, primitive) index wins
         const auto tie = [&]() {
@@ -804,35 +847,98 @@ __device__ __forceinline__ void leaf_test_mixed(const SceneDev& sc, const RayK& 
                 gi, hit_geom, [&]() { return __ldg(sc.order + s); },
                 [&]() { return __ldg(sc.order + hit_slot); });
         };
-        float t = 0.0f;
-        bool ok = false;
-        if ((MASK & (1u << FR_GEOM_SPHERE)) && type == FR_GEOM_SPHERE) {
-            ok = sphere_t(ray.o, ray.d, v3(a.x, a.y, a.z), a.w, t);
-        } else if ((MASK & (1u << FR_GEOM_CYLINDER)) && type == FR_GEOM_CYLINDER) {
-            const float4 b = ldg4(sc.leaf_data + 2 * size_t(s) + 1);
-            float de;
-            V3 N;
-            uint32_t ci;
-            ok = isect_spherocylinder(t, de, N, ci, ray.o, ray.d, v3(a.x, a.y, a.z),
-                                      v3(b.x, b.y, b.z), a.w);
-        } else if ((MASK & (1u << FR_GEOM_POLYHEDRON)) && type == FR_GEOM_POLYHEDRON) {
-            const float4 b = ldg4(sc.leaf_data + 2 * size_t(s) + 1);
-            PolyHit ph = poly_planes(g, ray.o, ray.d, v3(a.x, a.y, a.z), Qt{b.x, v3(b.y, b.z, b.w)},
-                                     tnear, tmax, tie);
-            ok = ph.hit;
-            t = ph.t;
-        } else if ((MASK & (1u << FR_GEOM_MESH)) && type == FR_GEOM_MESH) {
-            const float4 b = ldg4(sc.leaf_data + 2 * size_t(s) + 1);
-            TriHit th = mesh_triangle(g, __float_as_uint(a.w), ray.o, ray.d, v3(a.x, a.y, a.z),
-                                      Qt{b.x, v3(b.y, b.z, b.w)});
-            ok = th.hit;
-            t = th.t;
-        } else if ((MASK & (1u << FR_GEOM_POLYGON)) && type == FR_GEOM_POLYGON) {
-            const float4 b = ldg4(sc.leaf_data + 2 * size_t(s) + 1);
-            PgHit ph = polygon_hit(g, ray.o, ray.d, a.x, a.y, Qt{b.x, v3(b.y, b.z, b.w)});
-            ok = ph.hit;
-            t = ph.t;
+        float t;
+        const bool ok = mixed_prim_t<MASK>(sc, g, g.type, a, s, ray, tnear, tmax, tie, t);
+        if (ok && (tnear < t) && ((t < tmax) || (t == tmax && tie()))) {
+            tmax = t;
+            hit_geom = gi;
+            hit_slot = s;
         }
+    }
+}
+
+// The references of one cell of a grid over parts: as leaf_test_mixed, but a primitive other
+// than a sphere is tested only when the ray segment (0, tmax) enters its bounding box (the
+// cylinder's, or the box about the position of the polyhedron's or polygon's bounding radius,
+// padded beyond the tree builds' padding) as a tree's box test would allow, a mesh triangle only
+// when the ray meets the bounding sphere of its instance (the mesh's largest vertex distance
+// times the squared norm of the instance's quaternion, as rotate() scales, with a margin) before
+// the closest hit, and none again right after the same primitive (last_geom, last_prim: a
+// primitive spanning several cells along the ray; its test and the acceptance are exact, so a
+// repeat could not change the hit).
+template <uint32_t MASK>
+__device__ __forceinline__ void parts_cell_test(const SceneDev& sc, const RayK& ray,
+                                                uint32_t first, uint32_t last, float tnear,
+                                                float& tmax, uint32_t& hit_geom,
+                                                uint32_t& hit_slot, uint32_t& last_geom,
+                                                uint32_t& last_prim, TraceCount& tc)
+{
+    tc.prim += last - first;
+    for (uint32_t s = first; s < last; ++s) {
+        const uint32_t gi = __ldg(sc.leaf_geom + s);
+        if (gi >= sc.n_geoms)
+            continue;
+        const GeomDev& g = sc.geoms[gi];
+        const int type = g.type;
+        const float4 a = ldg4(sc.leaf_data + 2 * size_t(s));
+        if (type == FR_GEOM_MESH) {
+            // the instance's bounding sphere: its largest vertex distance, scaled as rotate()
+            // scales by the quaternion's squared norm, with a relative margin for rounding
+            // (the distance of its centre from the ray's line from a cross product, which keeps
+            // its precision when the centre is far from the ray's origin)
+            const float4 b = ldg4(sc.leaf_data + 2 * size_t(s) + 1);
+            const float r = g.bound_radius * (b.x * b.x + b.y * b.y + b.z * b.z + b.w * b.w);
+            const V3 oc = v3(a.x, a.y, a.z) - ray.o;
+            const float scale = fmaxf(fmaxf(fabsf(oc.x), fabsf(oc.y)), fabsf(oc.z)) + r;
+            const float rp = r + 1e-4f * scale + 1e-5f;
+            const float dd = dot(ray.d, ray.d), bb = dot(oc, ray.d);
+            const V3 cr = cross(oc, ray.d);
+            if (!(dot(cr, cr) <= rp * rp * dd))
+                continue;  // the line misses the sphere
+            const float reach = rp * sqrtf(dd);
+            if (bb + reach < 0.0f || bb - reach > tmax * dd)
+                continue;  // the sphere lies behind the origin or beyond the closest hit
+            const uint32_t prim = __ldg(sc.order + s);
+            if (gi == last_geom && prim == last_prim)
+                continue;
+            last_geom = gi;
+            last_prim = prim;
+        } else if (type != FR_GEOM_SPHERE) {
+            float4 lo, hi;
+            if (type == FR_GEOM_CYLINDER) {
+                const float4 b = ldg4(sc.leaf_data + 2 * size_t(s) + 1);
+                lo = make_float4(fminf(a.x, b.x) - a.w, fminf(a.y, b.y) - a.w,
+                                 fminf(a.z, b.z) - a.w, 0.0f);
+                hi = make_float4(fmaxf(a.x, b.x) + a.w, fmaxf(a.y, b.y) + a.w,
+                                 fmaxf(a.z, b.z) + a.w, 0.0f);
+            } else {
+                const float r = g.bound_radius;
+                const float rz = type == FR_GEOM_POLYGON ? 0.0f : r;
+                lo = make_float4(a.x - r, a.y - r, a.z - rz, 0.0f);
+                hi = make_float4(a.x + r, a.y + r, a.z + rz, 0.0f);
+            }
+            const float scale = fmaxf(fmaxf(fmaxf(fabsf(lo.x), fabsf(hi.x)),
+                                            fmaxf(fabsf(lo.y), fabsf(hi.y))),
+                                      fmaxf(fabsf(lo.z), fabsf(hi.z)));
+            const float pad = 1e-4f * scale + 1e-5f;
+            lo = make_float4(lo.x - pad, lo.y - pad, lo.z - pad, 0.0f);
+            hi = make_float4(hi.x + pad, hi.y + pad, hi.z + pad, 0.0f);
+            float tentry;
+            if (!slab(ray, lo, hi, tmax, tentry))
+                continue;
+            const uint32_t prim = __ldg(sc.order + s);
+            if (gi == last_geom && prim == last_prim)
+                continue;
+            last_geom = gi;
+            last_prim = prim;
+        }
+        const auto tie = [&]() {
+            return tie_wins(
+                gi, hit_geom, [&]() { return __ldg(sc.order + s); },
+                [&]() { return __ldg(sc.order + hit_slot); });
+        };
+        float t;
+        const bool ok = mixed_prim_t<MASK>(sc, g, type, a, s, ray, tnear, tmax, tie, t);
         if (ok && (tnear < t) && ((t < tmax) || (t == tmax && tie()))) {
             tmax = t;
             hit_geom = gi;
@@ -1010,17 +1116,18 @@ __device__ __forceinline__ Hit trace_grid_hit(const GridDev& G, const RayK& ray,
 
 // Closest hit through a grid over the primitives of several geometries (GridDev::parts): the
 // same walk, with each cell's references tested as the leaf slots of a combined tree (the test
-// and acceptance rule of every geometry type, ties to the lower (geometry, primitive) index).
+// and acceptance rule of every geometry type, ties to the lower (geometry, primitive) index) by
+// parts_cell_test.
 template <uint32_t TYPES>
 __device__ __forceinline__ Hit trace_grid_parts(const SceneDev& sc, const RayK& ray, float tnear,
                                                 float tmax, TraceCount& tc)
 {
     const GridDev& G = sc.grid;
-    uint32_t hg = MISS, hs = 0;
+    uint32_t hg = MISS, hs = 0, last_g = MISS, last_p = 0;
     GridWalk W;
     if (grid_walk_begin(G, ray, W)) {
         while (grid_walk_visit(G, ray, tmax, W, tc, [&](uint32_t first, uint32_t last) {
-            leaf_test_mixed<TYPES>(sc, ray, first, last - first, tnear, tmax, hg, hs, tc);
+            parts_cell_test<TYPES>(sc, ray, first, last, tnear, tmax, hg, hs, last_g, last_p, tc);
         })) {
         }
     }

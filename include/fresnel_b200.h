@@ -183,8 +183,8 @@ FR_API fr_status fr_device_timer_stop(fr_device* dev, float* ms);
  *   "accel"         acceleration structure: 0: BVHs; 1: a uniform grid (walked cell by cell
  *                   along each ray) over the spheres of a scene whose only enabled geometry
  *                   holds spheres, else over the primitives of all its enabled geometries (at
- *                   most 8); 2 (default): the same grids, over parts only when every enabled
- *                   geometry holds spheres or cylinders, and only unless the primitives are
+ *                   most 8); 2 (default): the same grids, over parts only when no enabled
+ *                   geometry is a mesh, and only unless the primitives are
  *                   clustered (a cell with more than 64 of them) or a ray would cross more
  *                   than 1024 cells on average; else BVHs.  A primitive spanning more than
  *                   4096 cells leaves any scene to its BVHs.

@@ -1,5 +1,5 @@
 """Scenes of several geometries (or of one geometry that is not spheres) traced through the grid
-over their parts (device option "accel": 1 forces it, 2 chooses it for spheres and cylinders)
+over their parts (device option "accel": 1 forces it, 2 chooses it when no geometry is a mesh)
 against the CPU oracle: the same closest hits (exact-t ties and rays grazing a silhouette aside,
 classified by tests/grazing.py), same-seed path images within the oracle's bar, the same images
 as the trees give, and the automatic choice.
@@ -51,12 +51,21 @@ def _icosahedra(d):
     return s
 
 
+def _mixed_without_mesh(d):
+    s = _mixed(d)
+    for g in s.geometry:
+        if type(g).__name__ == "Mesh":
+            g.disable()
+    return s
+
+
 # name: (builder, width, height, accel mode that must give the parts grid)
 SCENES = {
     "spheres_bonds": (_spheres_bonds, 160, 90, 2),
     "mixed": (_mixed, 160, 90, 1),
-    "polygons_and_spheres": (_polygons_and_spheres, 128, 96, 1),
+    "polygons_and_spheres": (_polygons_and_spheres, 128, 96, 2),
     "icosahedra": (_icosahedra, 128, 96, 1),
+    "mixed_without_mesh": (_mixed_without_mesh, 160, 90, 2),
     "odd_radii": (odd_radii_scene, 120, 120, 2),
 }
 
@@ -108,8 +117,9 @@ def test_automatic_choice_over_parts(accel, gpu_device):
     accel(2)
     cases = {
         "spheres_bonds": (_spheres_bonds, PARTS_GRID),
-        "mixed": (_mixed, 0),  # polyhedra and meshes keep the trees
-        "polygons_and_spheres": (_polygons_and_spheres, 0),
+        "mixed": (_mixed, 0),  # a mesh keeps the trees
+        "mixed_without_mesh": (_mixed_without_mesh, PARTS_GRID),
+        "polygons_and_spheres": (_polygons_and_spheres, PARTS_GRID),
         "icosahedra": (_icosahedra, 0),
     }
     for name, (build, kind) in cases.items():
