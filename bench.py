@@ -787,10 +787,13 @@ def main():
     dom_rays, dom_ms, launches = kern[dom]
     # Algorithmic bytes per ray of the structure this run traversed, from the engine's own
     # counters over the frame: 24 B of ray in, 16 B of hit out, 12 B of colour at the hit, then
-    # per BVH box test 32 B or per grid cell 8 B of reference range, and 16 B per sphere tested.
-    grid = bool(st.get("grid", 0))
+    # per BVH box test 32 B or per grid cell 8 B of reference range, and 16 B per sphere tested
+    # (a grid over parts: 36 B per reference, its 32 B record and 4 B geometry index).
+    grid_kind = int(st.get("grid", 0))
+    grid = grid_kind != 0
     per_box = 8.0 if grid else 32.0
-    run_bytes = (52.0 + per_box * st["box_tests"] / rays + 16.0 * st["prim_tests"] / rays
+    per_prim = 36.0 if grid_kind == 2 else 16.0
+    run_bytes = (52.0 + per_box * st["box_tests"] / rays + per_prim * st["prim_tests"] / rays
                  if rays > 0 else None)
     # The roofline's bytes: for a grid, those of the grid walked (the oracle's frozen cells and
     # spheres per ray when the workload has them, else this run's counters); for a BVH, the
@@ -799,7 +802,7 @@ def main():
     # not what the kernel read.
     if grid:
         bpr = (wl.grid_bytes_per_ray if wl.grid_bytes_per_ray and (wl.w, wl.h) == wl.full_size
-               else run_bytes)
+               and grid_kind == 1 else run_bytes)
     else:
         bpr = wl.bytes_per_ray
     achieved = (dom_rays * bpr) / (dom_ms / 1e3) / 1e9 if dom_ms > 0 and bpr else None
@@ -875,7 +878,7 @@ def main():
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
             "config": cfg,
-            "accel": "sphere grid" if grid else "bvh",
+            "accel": {0: "bvh", 1: "sphere grid", 2: "grid over parts"}[grid_kind],
             "rays_per_frame": rays_per_frame,
             "gpu_launches": int(st["kernel_launches"]),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
@@ -888,6 +891,9 @@ def main():
                                                   bpr != run_bytes else
                                                   "sphere grid walked: 52 + 8 per cell + 16 "
                                                   "per sphere tested, engine counters")
+                                                 if grid_kind == 1 else
+                                                 "grid over parts walked: 52 + 8 per cell + 36 "
+                                                 "per reference tested, engine counters"
                                                  if grid else
                                                  "reference BVH: 52 + 32 A + S P, oracle counts"),
                          "accel": "grid" if grid else "bvh",

@@ -192,6 +192,7 @@ struct fr_geometry {
     float outline_width = 0.0f;
     DevArray<float> position, radius, color, points, orientation, vertices, planes;
     DevArray<float> angle;         // polygon: [n] radians; orientation holds their quaternions
+    DevArray<float4> face_box;     // mesh: per face its local box (lo, hi), padded
     float rounding_radius = 0.0f;  // polygon
     BvhBuffers bvh;
     bool bvh_dirty = true;
@@ -271,7 +272,7 @@ struct fr_tracer {
     uint64_t builds = 0;
     uint64_t refits = 0;
     uint64_t grid_builds = 0;
-    uint32_t last_grid = 0;  // whether the last render traced through a sphere grid
+    uint32_t last_grid = 0;  // the last render's grid: 0 none, 1 sphere grid, 2 grid over parts
     double build_ms = 0.0;
     // per-kernel timing while profiling: event pairs pending readback, by kernel kind
     std::vector<cudaEvent_t> event_pool;
@@ -427,6 +428,7 @@ BuildInput build_input(const fr_geometry* g)
     in.vertices = g->vertices.ptr;
     in.n_faces = g->n_faces;
     in.poly_radius = g->poly_radius;
+    in.instances = 0;
     return in;
 }
 
@@ -464,13 +466,12 @@ std::vector<fr_geometry*> combined_parts(const fr_scene* sc, std::vector<uint64_
 // What a grid may replace (nothing when the device option accel is 0): the tree of the scene's
 // only enabled geometry when it holds spheres (kind 1, a sphere grid; gi receives its scene
 // index), else the trees of all its enabled geometries, at most MAX_PARTS (kind 2, a grid over
-// their primitives; parts receives them in scene order).  In automatic mode (accel 2) a grid
-// over parts is considered only when none of them is a mesh: spheres and bonds of 1e4 to 2e6
-// primitives traced 1.5x to 1.8x faster than through the trees, the mixed scene without its
-// icosahedra (200k spheres, 50k bonds, 20k cubes) 1.38x and 1080 polygons with 400 spheres
-// 1.38x, but 10k icosahedra alone (200k triangles) 1.8x slower: each triangle is a reference
-// tested after its instance's bounding sphere, where a tree culls triangle by triangle.  key
-// identifies what a grid build depends on.  Returns the kind, or 0 when no grid applies.
+// their primitives, a mesh by instance; parts receives them in scene order).  The automatic
+// mode (accel 2) applies the grid's own rules (clustering, sparseness) to both kinds: measured
+// against the trees, spheres and bonds of 1e4 to 2e6 primitives traced 1.5x to 1.9x faster
+// through a grid over parts, the mixed scene (spheres, bonds, cubes, icosahedra) 1.15x, 10k
+// icosahedra alone 1.66x, 1080 polygons with 400 spheres 1.38x.  key identifies what a grid
+// build depends on.  Returns the kind, or 0 when no grid applies.
 int grid_candidate(const fr_scene* sc, std::vector<uint64_t>& key, uint32_t& gi,
                    std::vector<fr_geometry*>* parts = nullptr)
 {
@@ -493,10 +494,6 @@ int grid_candidate(const fr_scene* sc, std::vector<uint64_t>& key, uint32_t& gi,
     if (on.empty() || on.size() > size_t(MAX_PARTS))
         return 0;
     const int kind = (on.size() == 1 && on[0]->type == FR_GEOM_SPHERE) ? 1 : 2;
-    if (kind == 2 && dev->accel == 2)
-        for (const fr_geometry* g : on)
-            if (g->type == FR_GEOM_MESH)
-                return 0;
     uint32_t density_bits;
     std::memcpy(&density_bits, &dev->grid_cells_per_prim, sizeof(density_bits));
     key.push_back(uint64_t(kind));
@@ -545,8 +542,10 @@ fr_status check_build_status(fr_device* dev)
 }
 
 // The build input over the primitives of `parts` (at most MAX_PARTS geometries of sc); n
-// receives their number.
-PartsInput parts_input(const fr_scene* sc, const std::vector<fr_geometry*>& parts, uint32_t& n)
+// receives their number.  mesh_instances: a mesh contributes one primitive per instance (grids
+// over parts) rather than one per triangle (trees).
+PartsInput parts_input(const fr_scene* sc, const std::vector<fr_geometry*>& parts, uint32_t& n,
+                       bool mesh_instances = false)
 {
     PartsInput in;
     std::memset(&in, 0, sizeof(in));
@@ -555,12 +554,14 @@ PartsInput parts_input(const fr_scene* sc, const std::vector<fr_geometry*>& part
     for (uint32_t p = 0; p < in.n_parts; ++p) {
         fr_geometry* g = parts[p];
         in.part[p] = build_input(g);
+        const bool inst = mesh_instances && g->type == FR_GEOM_MESH;
+        in.part[p].instances = inst ? 1 : 0;
         in.first[p] = n;
         uint32_t gi = 0;
         while (sc->geoms[gi] != g)
             ++gi;
         in.geom[p] = gi;
-        n += g->bvh_prims();
+        n += inst ? g->n : g->bvh_prims();
     }
     in.first[in.n_parts] = n;
     return in;
@@ -637,7 +638,7 @@ fr_status prepare_grid(fr_scene* sc, fr_tracer* tr, int kind, uint32_t gi,
                        dev->stream, sc->grid_report);
     } else {
         uint32_t n = 0;
-        const PartsInput in = parts_input(sc, parts, n);
+        const PartsInput in = parts_input(sc, parts, n, true);
         e = build_grid(in, n, gp, sc->grid, dev->scratch, dev->stream, sc->grid_report);
     }
     cudaEventRecord(e1, dev->stream);
@@ -662,9 +663,9 @@ fr_status prepare_grid(fr_scene* sc, fr_tracer* tr, int kind, uint32_t gi,
         G.ref_data.release();
         G.ref_geom.release();
     }
-    G.box_lo.release();  // build temporaries of a parts grid
-    G.box_hi.release();
     if (!sc->use_grid) {  // BVHs serve this scene
+        G.box_lo.release();  // (kept otherwise, as the other build temporaries, for rebuilds)
+        G.box_hi.release();
         G.cell_start.release();
         G.ref_prim.release();
     } else if (tr) {
@@ -777,6 +778,7 @@ fr_status prepare_scene(fr_scene* sc, fr_tracer* tr)
             d.n_vertices = g->type == FR_GEOM_POLYGON ? g->n_vertices : 0u;
             d.rounding_radius = g->rounding_radius;
             d.bound_radius = g->type == FR_GEOM_MESH ? g->mesh_radius : g->poly_radius;
+            d.face_box = g->face_box.ptr;
             d.color_by_face = g->color_by_face;
             d.outline_width = g->outline_width;
             d.material = to_mat(g->material);
@@ -884,7 +886,7 @@ FrameParams frame_params(fr_tracer* tr, fr_scene* sc, const fr_render_params* p,
     P.shade_blocks = sc->dev->shade_blocks;
     P.packet = sc->use_grid ? 0 : sc->dev->packet;
     P.refill = sc->dev->refill;
-    tr->last_grid = sc->use_grid ? 1u : 0u;
+    tr->last_grid = sc->use_grid ? (sc->grid.parts ? 2u : 1u) : 0u;
     const fr_user_camera& c = p->camera;
     float f_stop = preview ? std::numeric_limits<float>::infinity() : c.f_stop;  // no depth of field in preview
     bool sample_aa = preview ? (aa_n != 1) : true;
@@ -926,6 +928,7 @@ fr_status check_status(fr_device* dev)
         return fail(FR_ERR_DEVICE_LIMIT,
                     (st & ERR_STACK_OVERFLOW) ? "BVH traversal stack overflow (tree too deep)"
                     : (st & ERR_BAD_NODE)     ? "BVH traversal met an out-of-range node"
+                    : (st & ERR_KERNEL)       ? "a kernel met an acceleration structure it lacks"
                                               : "BVH traversal iteration cap reached");
     }
     return FR_OK;
@@ -1388,10 +1391,45 @@ fr_status fr_geometry_create_mesh(fr_scene* scene, const float* vertices, uint32
             r2 = q;
     }
     g->mesh_radius = float(std::sqrt(r2) * (1.0 + 1e-6));
+    // each face's box in the instance frame, padded like the tree builds' boxes (a filter in
+    // front of the face's test in grids over parts; a face with a NaN vertex gets an empty box)
+    std::vector<float4> boxes(2 * size_t(g->n_faces));
+    for (uint32_t f = 0; f < g->n_faces; ++f) {
+        float lo[3], hi[3];
+        bool ok = true;
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = INFINITY;
+            hi[k] = -INFINITY;
+            for (int v = 0; v < 3; ++v) {
+                const float x = vertices[3 * (3 * size_t(f) + v) + k];
+                ok = ok && std::isfinite(x);
+                lo[k] = std::min(lo[k], x);
+                hi[k] = std::max(hi[k], x);
+            }
+        }
+        float scale = 0.0f, ext = 0.0f;
+        for (int k = 0; k < 3; ++k) {
+            scale = std::max(scale, std::max(std::fabs(lo[k]), std::fabs(hi[k])));
+            ext += hi[k] - lo[k];
+        }
+        const float pad = 1e-5f * scale + 1e-6f * ext + 1e-30f;
+        if (!ok) {
+            boxes[2 * size_t(f)] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+            boxes[2 * size_t(f) + 1] = make_float4(-1.0f, -1.0f, -1.0f, 0.0f);
+        } else {
+            boxes[2 * size_t(f)] = make_float4(lo[0] - pad, lo[1] - pad, lo[2] - pad, 0.0f);
+            boxes[2 * size_t(f) + 1] = make_float4(hi[0] + pad, hi[1] + pad, hi[2] + pad, 0.0f);
+        }
+    }
     cudaError_t e = use_device(scene->dev) == FR_OK ? g->vertices.reserve(size_t(n_vertices) * 3)
                                                     : cudaErrorUnknown;
     if (e == cudaSuccess && n_vertices)
         e = cudaMemcpy(g->vertices.ptr, vertices, size_t(n_vertices) * 3 * sizeof(float),
+                       cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && g->n_faces)
+        e = g->face_box.reserve(boxes.size());
+    if (e == cudaSuccess && g->n_faces)
+        e = cudaMemcpy(g->face_box.ptr, boxes.data(), boxes.size() * sizeof(float4),
                        cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
         delete g;
@@ -2365,7 +2403,7 @@ fr_status fr_batch_render(fr_batch* b)
     if (all_grid && !jobs.empty())
         mask = dev->fuse_shade ? MASK_GRID_FUSED : MASK_GRID;
     else if (all_parts && !jobs.empty() && dev->fuse_shade)
-        mask = MASK_GRID_PARTS_FUSED;
+        mask = (mask & (1u << FR_GEOM_MESH)) ? MASK_GRID_PARTS_FUSED : MASK_GRID_PARTS_NO_MESH_FUSED;
     wave_first.push_back(uint32_t(jobs.size()));
     if (mask == 0)
         mask = MASK_SPHERES;  // empty scenes: every ray misses
@@ -2435,7 +2473,8 @@ fr_status fr_batch_render(fr_batch* b)
     // fused grid waves: begin, primary, 3 queue clears, 2 bounces, tail, fold, end;
     // otherwise per wave: begin, primary, fold, end, and per pass: 2 shade, 2 extend, 1
     // condition; 1 start
-    if (b->exec_mask == MASK_GRID_FUSED || b->exec_mask == MASK_GRID_PARTS_FUSED)
+    if (b->exec_mask == MASK_GRID_FUSED || b->exec_mask == MASK_GRID_PARTS_FUSED ||
+        b->exec_mask == MASK_GRID_PARTS_NO_MESH_FUSED)
         b->stats.kernel_launches += 1 + 10 * uint64_t(waves.size());
     else
         b->stats.kernel_launches += 1 + 4 * uint64_t(waves.size()) + 5 * c.pairs;

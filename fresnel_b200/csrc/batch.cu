@@ -509,12 +509,16 @@ cudaError_t batch_graph_create(const BatchDev& B, int width, uint32_t type_mask,
         return capture<4, MASK_GRID>(B, num_sms, capture_stream, exec);
     if (type_mask == MASK_GRID_PARTS_FUSED)  // every render traces a grid over its parts
         return capture<4, MASK_GRID_PARTS, true>(B, num_sms, capture_stream, exec);
+    if (type_mask == MASK_GRID_PARTS_NO_MESH_FUSED)  // the same, no mesh among the parts
+        return capture<4, MASK_GRID_PARTS_NO_MESH, true>(B, num_sms, capture_stream, exec);
+    // renders tracing trees, sphere grids or grids over parts (MASK_MAY_PARTS)
     const bool spheres_only = (type_mask & ~MASK_SPHERES) == 0u;
+    constexpr uint32_t SPH = MASK_SPHERES | MASK_MAY_PARTS, ALL = MASK_ALL | MASK_MAY_PARTS;
     if (width == 4)
-        return spheres_only ? capture<4, MASK_SPHERES>(B, num_sms, capture_stream, exec)
-                            : capture<4, MASK_ALL>(B, num_sms, capture_stream, exec);
-    return spheres_only ? capture<2, MASK_SPHERES>(B, num_sms, capture_stream, exec)
-                        : capture<2, MASK_ALL>(B, num_sms, capture_stream, exec);
+        return spheres_only ? capture<4, SPH>(B, num_sms, capture_stream, exec)
+                            : capture<4, ALL>(B, num_sms, capture_stream, exec);
+    return spheres_only ? capture<2, SPH>(B, num_sms, capture_stream, exec)
+                        : capture<2, ALL>(B, num_sms, capture_stream, exec);
 }
 
 }  // namespace fr

@@ -54,10 +54,12 @@ constexpr uint32_t BATCH_MAX_PAIRS = 1u << 16;
 // Capture the whole-batch graph for trees of `width` (2 or 4) and the geometry types in
 // `type_mask` (MASK_GRID: every render traces a sphere grid; MASK_GRID_FUSED: the same with the
 // shading folded into the tracing kernels; MASK_GRID_PARTS_FUSED: every render traces a grid over
-// its parts, shading folded in), grids sized for num_sms. The buffers behind B must outlive the
+// its parts, shading folded in; MASK_GRID_PARTS_NO_MESH_FUSED: the same without a mesh), grids
+// sized for num_sms. The buffers behind B must outlive the
 // graph.
 constexpr uint32_t MASK_GRID_FUSED = (1u << 31) | (1u << 30);
 constexpr uint32_t MASK_GRID_PARTS_FUSED = MASK_GRID_PARTS | (1u << 30);
+constexpr uint32_t MASK_GRID_PARTS_NO_MESH_FUSED = MASK_GRID_PARTS_NO_MESH | (1u << 30);
 cudaError_t batch_graph_create(const BatchDev& B, int width, uint32_t type_mask, int num_sms,
                                cudaStream_t capture_stream, cudaGraphExec_t* exec);
 

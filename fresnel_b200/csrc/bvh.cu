@@ -98,6 +98,13 @@ __device__ Box prim_bounds(const BuildInput& in, uint32_t i)
         break;
     }
     case FR_GEOM_MESH: {
+        if (in.instances) {  // the whole instance: every face's vertices
+            V3 p = load3(in.position, i);
+            Qt q = loadq(in.orientation, i);
+            for (uint32_t k = 0; k < 3 * in.n_faces; ++k)
+                grow(b, rotate(q, load3(in.vertices, k)) + p);
+            break;
+        }
         uint32_t inst = i / in.n_faces, face = i - inst * in.n_faces;
         V3 p = load3(in.position, inst);
         Qt q = loadq(in.orientation, inst);
@@ -438,8 +445,9 @@ __device__ __forceinline__ void write_record(const BuildInput& in, uint32_t p, f
         r[1] = make_float4(q.s, q.v.x, q.v.y, q.v.z);
         break;
     }
-    case FR_GEOM_MESH: {
-        uint32_t inst = p / in.n_faces, face = p - inst * in.n_faces;
+    case FR_GEOM_MESH: {  // (an instance record when in.instances: face 0)
+        uint32_t inst = in.instances ? p : p / in.n_faces;
+        uint32_t face = in.instances ? 0u : p - inst * in.n_faces;
         V3 c = load3(in.position, inst);
         Qt q = loadq(in.orientation, inst);
         r[0] = make_float4(c.x, c.y, c.z, __uint_as_float(face));

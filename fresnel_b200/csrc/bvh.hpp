@@ -82,6 +82,8 @@ struct BuildInput {
     const float* vertices;
     uint32_t n_faces;
     float poly_radius;  // polyhedron / polygon: bounding radius about the position
+    int instances;      // mesh: one primitive per instance (grids over parts) instead of one
+                        // per triangle (trees)
 };
 
 // Several geometries' primitives in one tree (a scene's combined BVH): primitive i of the

@@ -36,6 +36,7 @@ constexpr uint32_t ERR_STACK_OVERFLOW = 1u;
 constexpr uint32_t ERR_ITERATION_CAP = 2u;
 constexpr uint32_t ERR_BAD_NODE = 4u;    // a BVH index out of range (never followed)
 constexpr uint32_t ERR_BUILD = 8u;       // BVH construction found an inconsistent hierarchy
+constexpr uint32_t ERR_KERNEL = 16u;     // a kernel met an acceleration structure it lacks
 
 struct GeomDev {
     int32_t type;
@@ -60,6 +61,7 @@ struct GeomDev {
     float rounding_radius;  // polygon
     float bound_radius;     // polyhedron, polygon: bounding radius about the position; mesh: the
                             // largest vertex distance from the instance origin
+    const float4* face_box;  // mesh: per face its padded box in the instance frame (lo, hi)
     float color_by_face;
     float outline_width;
     Mat material;
@@ -857,20 +859,24 @@ __device__ __forceinline__ void leaf_test_mixed(const SceneDev& sc, const RayK& 
     }
 }
 
-// The references of one cell of a grid over parts: as leaf_test_mixed, but a primitive other
-// than a sphere is tested only when the ray segment (0, tmax) enters its bounding box (the
-// cylinder's, or the box about the position of the polyhedron's or polygon's bounding radius,
-// padded beyond the tree builds' padding) as a tree's box test would allow, a mesh triangle only
-// when the ray meets the bounding sphere of its instance (the mesh's largest vertex distance
-// times the squared norm of the instance's quaternion, as rotate() scales, with a margin) before
-// the closest hit, and none again right after the same primitive (last_geom, last_prim: a
-// primitive spanning several cells along the ray; its test and the acceptance are exact, so a
-// repeat could not change the hit).
+// The references of one cell of a grid over parts: the test and acceptance rule of every type
+// (mixed_prim_t, as the combined tree's leaves), with hit_prim (the primitive's index within its
+// geometry) kept instead of a leaf slot.  A cylinder, polyhedron or polygon is tested only when
+// the ray segment (0, tmax) enters its bounding box (the cylinder's, or the box about the
+// position of the bounding radius; padded beyond the tree builds' padding) as a tree's box test
+// would allow.  A mesh is referenced by instance: once the ray meets the instance's bounding
+// sphere (the mesh's largest vertex distance times the squared norm of the quaternion, as
+// rotate() scales, with a margin), the ray is taken into the instance frame once, exactly as
+// mesh_triangle takes it for each triangle, and each face whose padded local box the segment
+// enters gets mesh_triangle's two-sided test, face by face (primitive = instance * faces + face).
+// No primitive or instance is tested again right after itself (last_geom, last_prim: one
+// spanning several cells along the ray; its test and the acceptance are exact, so a repeat
+// could not change the hit).
 template <uint32_t MASK>
 __device__ __forceinline__ void parts_cell_test(const SceneDev& sc, const RayK& ray,
                                                 uint32_t first, uint32_t last, float tnear,
                                                 float& tmax, uint32_t& hit_geom,
-                                                uint32_t& hit_slot, uint32_t& last_geom,
+                                                uint32_t& hit_prim, uint32_t& last_geom,
                                                 uint32_t& last_prim, TraceCount& tc)
 {
     tc.prim += last - first;
@@ -881,14 +887,13 @@ __device__ __forceinline__ void parts_cell_test(const SceneDev& sc, const RayK& 
         const GeomDev& g = sc.geoms[gi];
         const int type = g.type;
         const float4 a = ldg4(sc.leaf_data + 2 * size_t(s));
-        if (type == FR_GEOM_MESH) {
-            // the instance's bounding sphere: its largest vertex distance, scaled as rotate()
-            // scales by the quaternion's squared norm, with a relative margin for rounding
-            // (the distance of its centre from the ray's line from a cross product, which keeps
-            // its precision when the centre is far from the ray's origin)
+        if ((MASK & (1u << FR_GEOM_MESH)) && type == FR_GEOM_MESH) {
+            // the instance's bounding sphere (the distance of its centre from the ray's line
+            // from a cross product, which keeps its precision far from the ray's origin)
             const float4 b = ldg4(sc.leaf_data + 2 * size_t(s) + 1);
             const float r = g.bound_radius * (b.x * b.x + b.y * b.y + b.z * b.z + b.w * b.w);
-            const V3 oc = v3(a.x, a.y, a.z) - ray.o;
+            const V3 pos = v3(a.x, a.y, a.z);
+            const V3 oc = pos - ray.o;
             const float scale = fmaxf(fmaxf(fabsf(oc.x), fabsf(oc.y)), fabsf(oc.z)) + r;
             const float rp = r + 1e-4f * scale + 1e-5f;
             const float dd = dot(ray.d, ray.d), bb = dot(oc, ray.d);
@@ -898,12 +903,44 @@ __device__ __forceinline__ void parts_cell_test(const SceneDev& sc, const RayK& 
             const float reach = rp * sqrtf(dd);
             if (bb + reach < 0.0f || bb - reach > tmax * dd)
                 continue;  // the sphere lies behind the origin or beyond the closest hit
-            const uint32_t prim = __ldg(sc.order + s);
-            if (gi == last_geom && prim == last_prim)
+            const uint32_t inst = __ldg(sc.order + s);
+            if (gi == last_geom && inst == last_prim)
                 continue;
             last_geom = gi;
-            last_prim = prim;
-        } else if (type != FR_GEOM_SPHERE) {
+            last_prim = inst;
+            const Qt q = Qt{b.x, v3(b.y, b.z, b.w)};
+            const V3 dl = rotate(conj(q), ray.d);
+            const V3 ol = rotate(conj(q), ray.o - pos);
+            const V3 q2 = ol + dl;
+            const RayK lr = make_rayk(ol, dl);  // t along it is t along the ray
+            const float lpad = 1e-4f * (fmaxf(fmaxf(fabsf(ol.x), fabsf(ol.y)), fabsf(ol.z)) +
+                                        g.bound_radius) + 1e-5f;
+            for (uint32_t f = 0; f < g.n_faces; ++f) {
+                float4 lo = ldg4(g.face_box + 2 * size_t(f)), hi = ldg4(g.face_box + 2 * size_t(f) + 1);
+                lo = make_float4(lo.x - lpad, lo.y - lpad, lo.z - lpad, 0.0f);
+                hi = make_float4(hi.x + lpad, hi.y + lpad, hi.z + lpad, 0.0f);
+                float tentry;
+                if (!slab(lr, lo, hi, tmax, tentry))
+                    continue;
+                const V3 v0 = load3(g.vertices, 3 * f), v1 = load3(g.vertices, 3 * f + 1),
+                         v2 = load3(g.vertices, 3 * f + 2);
+                float u, v, w, t, de;
+                V3 n;
+                const bool hit = isect_triangle(u, v, w, t, de, n, ol, q2, v0, v1, v2) ||
+                                 isect_triangle(v, u, w, t, de, n, ol, q2, v1, v0, v2);
+                const uint32_t prim = inst * g.n_faces + f;
+                if (hit && (tnear < t) &&
+                    ((t < tmax) || (t == tmax && tie_wins(
+                                                     gi, hit_geom, [&]() { return prim; },
+                                                     [&]() { return hit_prim; })))) {
+                    tmax = t;
+                    hit_geom = gi;
+                    hit_prim = prim;
+                }
+            }
+            continue;
+        }
+        if (type != FR_GEOM_SPHERE) {
             float4 lo, hi;
             if (type == FR_GEOM_CYLINDER) {
                 const float4 b = ldg4(sc.leaf_data + 2 * size_t(s) + 1);
@@ -934,15 +971,14 @@ __device__ __forceinline__ void parts_cell_test(const SceneDev& sc, const RayK& 
         }
         const auto tie = [&]() {
             return tie_wins(
-                gi, hit_geom, [&]() { return __ldg(sc.order + s); },
-                [&]() { return __ldg(sc.order + hit_slot); });
+                gi, hit_geom, [&]() { return __ldg(sc.order + s); }, [&]() { return hit_prim; });
         };
         float t;
         const bool ok = mixed_prim_t<MASK>(sc, g, type, a, s, ray, tnear, tmax, tie, t);
         if (ok && (tnear < t) && ((t < tmax) || (t == tmax && tie()))) {
             tmax = t;
             hit_geom = gi;
-            hit_slot = s;
+            hit_prim = __ldg(sc.order + s);
         }
     }
 }
@@ -1123,17 +1159,17 @@ __device__ __forceinline__ Hit trace_grid_parts(const SceneDev& sc, const RayK& 
                                                 float tmax, TraceCount& tc)
 {
     const GridDev& G = sc.grid;
-    uint32_t hg = MISS, hs = 0, last_g = MISS, last_p = 0;
+    uint32_t hg = MISS, hp = 0, last_g = MISS, last_p = 0;
     GridWalk W;
     if (grid_walk_begin(G, ray, W)) {
         while (grid_walk_visit(G, ray, tmax, W, tc, [&](uint32_t first, uint32_t last) {
-            parts_cell_test<TYPES>(sc, ray, first, last, tnear, tmax, hg, hs, last_g, last_p, tc);
+            parts_cell_test<TYPES>(sc, ray, first, last, tnear, tmax, hg, hp, last_g, last_p, tc);
         })) {
         }
     }
     Hit h;
     h.geom = hg;
-    h.prim = hg == MISS ? 0u : __ldg(sc.order + hs);
+    h.prim = hg == MISS ? 0u : hp;
     return h;
 }
 
@@ -1146,6 +1182,13 @@ constexpr uint32_t MASK_GRID = 1u << 31;
 // Kernels specialised for a scene traced through a grid over its parts (GridDev::parts = 1),
 // every geometry type compiled in, no BVH code.
 constexpr uint32_t MASK_GRID_PARTS = MASK_GRID | MASK_ALL;
+// The same without the mesh code (scenes of parts none of which is a mesh: fewer registers).
+constexpr uint32_t MASK_GRID_PARTS_NO_MESH = MASK_GRID | (MASK_ALL & ~(1u << FR_GEOM_MESH));
+// Added to a tree kernel's mask: it may also meet grids over parts (the kernels of batches whose
+// renders trace different kinds of structure).  The single-render tree kernels go without: the
+// grid-over-parts walk would raise their register count (k_path_extend: 80 -> 98, one block per
+// SM less), and those renders run the MASK_GRID_PARTS kernels.
+constexpr uint32_t MASK_MAY_PARTS = 1u << 29;
 
 // Blocks of 256 threads per SM the fused trace-and-shade kernels are compiled for.  The grid walk
 // fits 64 registers with few spills, and the fourth block hides its memory latency better (1080p
@@ -1212,14 +1255,24 @@ __device__ __forceinline__ Hit trace_closest(const SceneDev& sc, V3 o, V3 d, flo
     } else if constexpr ((MASK & MASK_GRID) != 0u) {
         return trace_grid_parts<MASK & MASK_ALL>(sc, ray, tnear, tmax, tc);
     } else {
-        // kernels for BVH scenes also serve grid scenes (a batch may mix both)
+        // kernels for BVH scenes also serve sphere grids (a batch may mix both), and grids over
+        // parts when MASK has MASK_MAY_PARTS
         if (sc.grid.n_cells != 0) {
-            if (sc.grid.parts)
-                return trace_grid_parts<MASK>(sc, ray, tnear, tmax, tc);
+            if (sc.grid.parts) {
+                if constexpr ((MASK & MASK_MAY_PARTS) != 0u) {
+                    return trace_grid_parts<MASK & MASK_ALL>(sc, ray, tnear, tmax, tc);
+                } else {
+                    atomicOr(sc.status, ERR_KERNEL);  // not launched so: reported, no hit
+                    Hit h;
+                    h.geom = MISS;
+                    h.prim = 0;
+                    return h;
+                }
+            }
             if (MASK & MASK_SPHERES)
                 return trace_grid_hit(sc.grid, ray, tnear, tmax, tc);
         }
-        return trace_closest_bvh<WIDTH, MASK>(sc, ray, tnear, tc);
+        return trace_closest_bvh<WIDTH, MASK & MASK_ALL>(sc, ray, tnear, tc);
     }
 }
 

@@ -821,10 +821,13 @@ LaunchShape path_launch_shape(int num_sms)
     s.extend_grid[3] = num_sms * blocks_per_sm(k_path_extend<4, MASK_ALL>);
     s.extend_grid_sphere_grid = num_sms * blocks_per_sm(k_path_extend<4, MASK_GRID>);
     s.refill_grid_sphere_grid = num_sms * blocks_per_sm(k_path_extend_grid_refill);
-    s.extend_grid_parts_grid = num_sms * blocks_per_sm(k_path_extend<4, MASK_GRID_PARTS>);
+    s.extend_grid_parts_grid[0] = num_sms * blocks_per_sm(k_path_extend<4, MASK_GRID_PARTS>);
+    s.extend_grid_parts_grid[1] =
+        num_sms * blocks_per_sm(k_path_extend<4, MASK_GRID_PARTS_NO_MESH>);
     s.bounce_grid[0] = num_sms * fused_blocks(MASK_ALL);
     s.bounce_grid[1] = num_sms * fused_blocks(MASK_GRID);
     s.bounce_grid[2] = num_sms * fused_blocks(MASK_GRID_PARTS);
+    s.bounce_grid[3] = num_sms * fused_blocks(MASK_GRID_PARTS_NO_MESH);
     s.persistent_grid[0] = num_sms * blocks_per_sm(k_path_extend_persistent<MASK_SPHERES>);
     s.persistent_grid[1] = num_sms * blocks_per_sm(k_path_extend_persistent<MASK_ALL>);
     s.primary_grid[0] = num_sms * blocks_per_sm(k_path_primary_persistent<MASK_SPHERES>);
@@ -832,11 +835,20 @@ LaunchShape path_launch_shape(int num_sms)
     return s;
 }
 
-// The kernels a frame runs: 0 for BVH scenes, 1 for a sphere grid, 2 for a grid over parts.
+// The kernels a frame runs: 0 for BVH scenes, 1 for a sphere grid, 2 for a grid over parts, 3
+// for a grid over parts none of which is a mesh.
 static int grid_kind(const FrameParams& P)
 {
-    return P.scene.grid.n_cells == 0 ? 0 : (P.scene.grid.parts ? 2 : 1);
+    if (P.scene.grid.n_cells == 0)
+        return 0;
+    if (!P.scene.grid.parts)
+        return 1;
+    return (P.type_mask & (1u << FR_GEOM_MESH)) ? 2 : 3;
 }
+
+// The kernel K<4, mask> for grid kind gk (1-3).
+#define FR_GRID_KERNEL(K, gk)                                                                  \
+    ((gk) == 1 ? K<4, MASK_GRID> : (gk) == 2 ? K<4, MASK_GRID_PARTS> : K<4, MASK_GRID_PARTS_NO_MESH>)
 
 void launch_path_primary(const FrameParams& P, const PathState& S, const LaunchShape& shape,
                          cudaStream_t st)
@@ -844,7 +856,9 @@ void launch_path_primary(const FrameParams& P, const PathState& S, const LaunchS
     bool spheres_only = (P.type_mask & ~MASK_SPHERES) == 0u;
     if (const int gk = grid_kind(P)) {
         const uint32_t n = primary_items(P.w, P.h, P.batch, P.tile_log2);
-        auto k = gk == 1 ? k_path_primary<4, MASK_GRID> : k_path_primary<4, MASK_GRID_PARTS>;
+        auto k = gk == 1 ? k_path_primary<4, MASK_GRID>
+                 : gk == 2 ? k_path_primary<4, MASK_GRID_PARTS>
+                           : k_path_primary<4, MASK_GRID_PARTS_NO_MESH>;
         k<<<(n + 255) / 256, 256, 0, st>>>(P, S);
         return;
     }
@@ -869,7 +883,7 @@ void launch_path_primary_shade(const FrameParams& P, const PathState& S, cudaStr
     auto k = pick(P, k_path_primary_shade<2, MASK_SPHERES>, k_path_primary_shade<2, MASK_ALL>,
                   k_path_primary_shade<4, MASK_SPHERES>, k_path_primary_shade<4, MASK_ALL>);
     if (const int gk = grid_kind(P))
-        k = gk == 1 ? k_path_primary_shade<4, MASK_GRID> : k_path_primary_shade<4, MASK_GRID_PARTS>;
+        k = FR_GRID_KERNEL(k_path_primary_shade, gk);
     k<<<(n_items + 255) / 256, 256, 0, st>>>(P, S);
 }
 
@@ -898,7 +912,10 @@ void launch_path_extend(const FrameParams& P, const PathState& S, int iteration,
     int q = iteration & 1;
     if (const int gk = grid_kind(P)) {
         if (gk == 2)
-            k_path_extend<4, MASK_GRID_PARTS><<<shape.extend_grid_parts_grid, 256, 0, st>>>(P, S, q);
+            k_path_extend<4, MASK_GRID_PARTS><<<shape.extend_grid_parts_grid[0], 256, 0, st>>>(P, S, q);
+        else if (gk == 3)
+            k_path_extend<4, MASK_GRID_PARTS_NO_MESH>
+                <<<shape.extend_grid_parts_grid[1], 256, 0, st>>>(P, S, q);
         else if (P.refill)
             k_path_extend_grid_refill<<<shape.refill_grid_sphere_grid, 256, 0, st>>>(P, S, q);
         else
@@ -933,7 +950,7 @@ void launch_path_bounce(const FrameParams& P, const PathState& S, int iteration,
                   k_path_bounce<4, MASK_SPHERES>, k_path_bounce<4, MASK_ALL>);
     const int gk = grid_kind(P);
     if (gk)
-        k = gk == 1 ? k_path_bounce<4, MASK_GRID> : k_path_bounce<4, MASK_GRID_PARTS>;
+        k = FR_GRID_KERNEL(k_path_bounce, gk);
     k<<<shape.bounce_grid[gk], 256, 0, st>>>(P, S, q);
 }
 
@@ -945,7 +962,7 @@ void launch_path_tail(const FrameParams& P, const PathState& S, int iteration,
                   k_path_tail<4, MASK_SPHERES>, k_path_tail<4, MASK_ALL>);
     const int gk = grid_kind(P);
     if (gk)
-        k = gk == 1 ? k_path_tail<4, MASK_GRID> : k_path_tail<4, MASK_GRID_PARTS>;
+        k = FR_GRID_KERNEL(k_path_tail, gk);
     k<<<shape.bounce_grid[gk], 256, 0, st>>>(P, S, q);
 }
 
@@ -964,7 +981,7 @@ void launch_preview(const FrameParams& P, uint32_t aa_n, uint2* hits, cudaStream
     auto k = pick(P, k_preview<2, MASK_SPHERES>, k_preview<2, MASK_ALL>,
                   k_preview<4, MASK_SPHERES>, k_preview<4, MASK_ALL>);
     if (const int gk = grid_kind(P))
-        k = gk == 1 ? k_preview<4, MASK_GRID> : k_preview<4, MASK_GRID_PARTS>;
+        k = FR_GRID_KERNEL(k_preview, gk);
     k<<<grid, block, 0, st>>>(P, aa_n, hits);
 }
 

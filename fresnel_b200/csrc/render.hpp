@@ -60,10 +60,10 @@ struct LaunchShape {
     int refill_grid[2];      // extension kernel with per-lane refill [spheres only|all types]
     int extend_grid[4];      // [width 2|4][spheres only|all types]
     int extend_grid_sphere_grid;  // scenes traced through a uniform sphere grid
-    int extend_grid_parts_grid;   // k_path_extend over a grid of parts
+    int extend_grid_parts_grid[2];  // k_path_extend over a grid of parts [with|without meshes]
     int refill_grid_sphere_grid;  // the same with per-lane refill
-    int bounce_grid[3];           // fused extension and shading (k_path_bounce)
-                                  // [BVH|sphere grid|parts grid]
+    int bounce_grid[4];           // fused extension and shading (k_path_bounce)
+                                  // [BVH|sphere grid|parts grid|parts grid without meshes]
     int persistent_grid[2];  // 4-wide persistent extend kernel [spheres only|all types]
     int primary_grid[2];     // 4-wide persistent primary kernel [spheres only|all types]
 };

@@ -126,7 +126,8 @@ typedef struct fr_stats {
     uint64_t primary_launches, shade_launches, extend_launches;
     uint64_t bvh_refits;    /* of bvh_builds, how many refitted an existing tree */
     uint64_t grid_builds;   /* grids built (device option "accel") */
-    uint32_t last_render_grid; /* 1 if the last render traced through a sphere grid */
+    uint32_t last_render_grid; /* the last render's grid: 0 none (BVHs), 1 sphere grid, 2 grid
+                                * over the scene's parts */
 } fr_stats;
 
 typedef struct fr_device fr_device;
@@ -183,8 +184,8 @@ FR_API fr_status fr_device_timer_stop(fr_device* dev, float* ms);
  *   "accel"         acceleration structure: 0: BVHs; 1: a uniform grid (walked cell by cell
  *                   along each ray) over the spheres of a scene whose only enabled geometry
  *                   holds spheres, else over the primitives of all its enabled geometries (at
- *                   most 8); 2 (default): the same grids, over parts only when no enabled
- *                   geometry is a mesh, and only unless the primitives are
+ *                   most 8; a mesh by instance); 2 (default): the same grids unless the
+ *                   primitives are
  *                   clustered (a cell with more than 64 of them) or a ray would cross more
  *                   than 1024 cells on average; else BVHs.  A primitive spanning more than
  *                   4096 cells leaves any scene to its BVHs.

@@ -1,5 +1,6 @@
 """Scenes of several geometries (or of one geometry that is not spheres) traced through the grid
-over their parts (device option "accel": 1 forces it, 2 chooses it when no geometry is a mesh)
+over their parts (device option "accel": 1 forces it, 2 chooses it unless the primitives are
+clustered or sparse; a mesh is referenced by instance)
 against the CPU oracle: the same closest hits (exact-t ties and rays grazing a silhouette aside,
 classified by tests/grazing.py), same-seed path images within the oracle's bar, the same images
 as the trees give, and the automatic choice.
@@ -62,9 +63,9 @@ def _mixed_without_mesh(d):
 # name: (builder, width, height, accel mode that must give the parts grid)
 SCENES = {
     "spheres_bonds": (_spheres_bonds, 160, 90, 2),
-    "mixed": (_mixed, 160, 90, 1),
+    "mixed": (_mixed, 160, 90, 2),
     "polygons_and_spheres": (_polygons_and_spheres, 128, 96, 2),
-    "icosahedra": (_icosahedra, 128, 96, 1),
+    "icosahedra": (_icosahedra, 128, 96, 2),
     "mixed_without_mesh": (_mixed_without_mesh, 160, 90, 2),
     "odd_radii": (odd_radii_scene, 120, 120, 2),
 }
@@ -92,7 +93,7 @@ def test_parts_grid_path_same_seed(name, accel, gpu_device, oracle_device):
     build, _, _, mode = SCENES[name]
     accel(mode)
     gl, g8, gt = path_render(gpu_device, build(gpu_device), 96, 54, 6, 1, seed=7)
-    assert gt._tracer.getStats()["grid"] == 1
+    assert gt._tracer.getStats()["grid"] == PARTS_GRID
     ol, o8, _ = path_render(oracle_device, build(oracle_device), 96, 54, 6, 1, seed=7)
     close = numpy.all(numpy.abs(gl - ol) <= 1e-3, axis=-1).mean()
     assert close >= 0.99, f"only {close:.4%} of pixels within 1e-3"
@@ -107,7 +108,7 @@ def test_parts_grid_and_trees_give_the_same_image(name, accel, gpu_device):
     for m in (0, mode):
         accel(m)
         lin, _, t = path_render(gpu_device, scene, 96, 64, 8, 1, seed=3)
-        assert t._tracer.getStats()["grid"] == (1 if m else 0)
+        assert t._tracer.getStats()["grid"] == (PARTS_GRID if m else 0)
         out.append(lin)
     close = numpy.all(numpy.abs(out[0] - out[1]) <= 1e-6, axis=-1).mean()
     assert close >= 0.999, f"only {close:.4%} of pixels agree"
@@ -117,10 +118,10 @@ def test_automatic_choice_over_parts(accel, gpu_device):
     accel(2)
     cases = {
         "spheres_bonds": (_spheres_bonds, PARTS_GRID),
-        "mixed": (_mixed, 0),  # a mesh keeps the trees
+        "mixed": (_mixed, PARTS_GRID),
         "mixed_without_mesh": (_mixed_without_mesh, PARTS_GRID),
         "polygons_and_spheres": (_polygons_and_spheres, PARTS_GRID),
-        "icosahedra": (_icosahedra, 0),
+        "icosahedra": (_icosahedra, PARTS_GRID),
     }
     for name, (build, kind) in cases.items():
         scene = build(gpu_device)

@@ -14,9 +14,10 @@
     classified (tests/grazing.py) and none may be non-grazing; all disagreements together at
     most 1e-4 of the samples; linear RGB within 1e-3 where every sample of a pixel agrees.
 * Mixed scene at full size (200k spheres, 50k bonds, 20k cubes, 10k icosahedra = 470k
-  primitives, one combined tree), 1280x720: Preview hit ids at 4x4 samples per pixel, and Path
-  at 128 samples per pixel: the Monte Carlo test on 2048 seeded pixels and the same-seed test
-  on 4096 (>= 99% within 1e-3).
+  primitives), 1280x720, through the engine's default (a grid over its parts) and through one
+  combined tree (accel = 0): Preview hit ids at 4x4 samples per pixel, and Path at 128 samples
+  per pixel: the Monte Carlo test on 2048 seeded pixels and the same-seed test on 4096 (>= 99%
+  within 1e-3).
 
 Every measured rate is written through parity_record.record.
 """
@@ -182,18 +183,24 @@ def test_config2_preview_anti_aliased(accel, gpu_device, oracle_device):
 C3_W, C3_H, C3_SPP = 1280, 720, 128
 
 
-def test_config3_preview(gpu_device, oracle_device):
+@pytest.mark.parametrize("accel", [2, 0], ids=["default_grid", "bvh"], indirect=True)
+def test_config3_preview(accel, gpu_device, oracle_device):
     gscene = workloads.config3(gpu_device)
     oscene = _oracle_scene(oracle_device, "config3", workloads.config3)
+    gscene._scene.build()
+    kind = gscene._scene.getAccel()[0]
+    assert kind == (2 if accel == 2 else 0), "the mixed scene should be traced as configured"
     _preview("test_config3_preview", gpu_device, oracle_device, gscene, oscene, C3_W, C3_H, 4,
-             {"scene": "config3 mixed 470k primitives", "width": C3_W, "height": C3_H, "aa": 4})
+             {"scene": "config3 mixed 470k primitives", "width": C3_W, "height": C3_H, "aa": 4,
+              "structure": "parts grid" if kind else "combined bvh"})
 
 
-def test_config3_path(gpu_device, oracle_device):
+@pytest.mark.parametrize("accel", [2, 0], ids=["default_grid", "bvh"], indirect=True)
+def test_config3_path(accel, gpu_device, oracle_device):
     gl, grid, st = _gpu_path(gpu_device, workloads.config3, C3_W, C3_H, C3_SPP, seed=7)
-    assert not grid
+    assert grid == (accel == 2)
     oscene = _oracle_scene(oracle_device, "config3", workloads.config3)
     extra = {"scene": "config3 mixed 470k primitives", "width": C3_W, "height": C3_H,
-             "structure": "combined bvh", "gpu_rays": int(st["rays"])}
+             "structure": "parts grid" if grid else "combined bvh", "gpu_rays": int(st["rays"])}
     _monte_carlo("test_config3_path", oscene, oracle_device, gl, C3_W, C3_H, C3_SPP, 8, extra)
     _same_seed("test_config3_path", oscene, oracle_device, gl, C3_W, C3_H, C3_SPP, 8, extra)

@@ -32,8 +32,9 @@ def _scene(device):
 SCENES = {  # scene, device option "accel", grid kind (0 trees, 1 sphere grid, 2 parts grid)
     "spheres_bvh": (workloads.config1, 0, 0),
     "dense_grid": (lambda d: workloads.config2(d, n=20000, box=140.0 * 0.02**(1 / 3)), 2, 1),
-    "mixed": (lambda d: workloads.config3(d, scale=0.002), 2, 0),
-    "parts_grid": (lambda d: workloads.serving_scene(d, 4000, 5), 2, 2),
+    "mixed": (lambda d: workloads.config3(d, scale=0.002), 0, 0),
+    "parts_grid": (lambda d: workloads.config3(d, scale=0.002), 2, 2),
+    "parts_grid_no_mesh": (lambda d: workloads.serving_scene(d, 4000, 5), 2, 2),
 }
 
 
