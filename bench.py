@@ -48,17 +48,20 @@ class Workload:
     uniform sphere grid (1.5 cells per sphere), measured by the oracle's restatement of the grid
     walk on the rays of an oracle render of the frame (oracle/measure_ray_costs.py --grid) and
     frozen here.  Algorithmic bytes per ray through the grid = 52 + 8 C + 16 S.
+    grid_cells / grid_refs for a scene traced through its grid over parts: cells visited and
+    references listed in them per query (oracle/measure_ray_costs.py --parts-grid); bytes per ray
+    = 52 + 8 C + 36 R (a 32 B record and a 4 B geometry index per reference).
     """
 
     def __init__(self, key, desc, scene, w, h, spp=1, light_samples=1, preview=False, aa_n=1,
                  box_tests=0.0, prim_tests=0.0, prim_bytes=16, grid_cells=None,
-                 grid_spheres=None):
+                 grid_spheres=None, grid_refs=None):
         self.key, self.desc, self.scene = key, desc, scene
         self.w, self.h, self.spp, self.light_samples = w, h, spp, light_samples
         self.full_size = (w, h)  # the frozen per-ray costs were measured on this frame
         self.preview, self.aa_n = preview, aa_n
         self.box_tests, self.prim_tests, self.prim_bytes = box_tests, prim_tests, prim_bytes
-        self.grid_cells, self.grid_spheres = grid_cells, grid_spheres
+        self.grid_cells, self.grid_spheres, self.grid_refs = grid_cells, grid_spheres, grid_refs
 
     @property
     def bytes_per_ray(self):
@@ -66,9 +69,15 @@ class Workload:
 
     @property
     def grid_bytes_per_ray(self):
-        if self.grid_cells is None:
+        if self.grid_cells is None or self.grid_spheres is None:
             return None
         return 52 + 8 * self.grid_cells + 16 * self.grid_spheres
+
+    @property
+    def parts_grid_bytes_per_ray(self):
+        if self.grid_cells is None or self.grid_refs is None:
+            return None
+        return 52 + 8 * self.grid_cells + 36 * self.grid_refs
 
     def build(self, device):
         from fresnel_b200 import workloads
@@ -89,7 +98,8 @@ WORKLOADS = {
     "c5": Workload("c5", "config5", "serving_scene_first", 1280, 720, spp=16),
     "c3": Workload("c3", "config3: 200k spheres + 50k bonds + 20k cubes + 10k icosahedra, "
                    "{w}x{h}, {spp} spp, 1 light sample", "config3", 1280, 720, spp=128,
-                   box_tests=43.51, prim_tests=1.86, prim_bytes=28),
+                   box_tests=43.51, prim_tests=1.86, prim_bytes=28, grid_cells=4.469,
+                   grid_refs=10.886),
     "tour": Workload("tour", "kernel tour", "config2", 1920, 1080),
 }
 
@@ -800,9 +810,9 @@ def main():
     # reference BVH's fixed box and primitive tests per ray (wl.bytes_per_ray).  The
     # reference-BVH figure of a grid run is kept beside it: it counts the work a BVH would do,
     # not what the kernel read.
+    frozen = wl.grid_bytes_per_ray if grid_kind == 1 else wl.parts_grid_bytes_per_ray
     if grid:
-        bpr = (wl.grid_bytes_per_ray if wl.grid_bytes_per_ray and (wl.w, wl.h) == wl.full_size
-               and grid_kind == 1 else run_bytes)
+        bpr = frozen if frozen and (wl.w, wl.h) == wl.full_size else run_bytes
     else:
         bpr = wl.bytes_per_ray
     achieved = (dom_rays * bpr) / (dom_ms / 1e3) / 1e9 if dom_ms > 0 and bpr else None
@@ -892,8 +902,11 @@ def main():
                                                   "sphere grid walked: 52 + 8 per cell + 16 "
                                                   "per sphere tested, engine counters")
                                                  if grid_kind == 1 else
-                                                 "grid over parts walked: 52 + 8 per cell + 36 "
-                                                 "per reference tested, engine counters"
+                                                 ("grid over parts walked: 52 + 8 per cell + 36 "
+                                                  "per reference, oracle counts" if
+                                                  bpr != run_bytes else
+                                                  "grid over parts walked: 52 + 8 per cell + 36 "
+                                                  "per reference, engine counters")
                                                  if grid else
                                                  "reference BVH: 52 + 32 A + S P, oracle counts"),
                          "accel": "grid" if grid else "bvh",

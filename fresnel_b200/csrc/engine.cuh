@@ -1192,10 +1192,12 @@ constexpr uint32_t MASK_MAY_PARTS = 1u << 29;
 
 // Blocks of 256 threads per SM the fused trace-and-shade kernels are compiled for.  The grid walk
 // fits 64 registers with few spills, and the fourth block hides its memory latency better (1080p
-// frame of 1M spheres: 82.8 against 85.3 ms); the BVH traversals spill heavily at 64 and keep 3.
+// frame of 1M spheres: 82.8 against 85.3 ms; spheres and bonds over parts, 2M primitives: 4.87
+// against 5.42 ms); the BVH traversals spill heavily at 64 and keep 3, and so do the grid-over-
+// parts kernels with the mesh code (mixed scene: 69.9 against 70.5 ms at 4, 79.7 at 2).
 __host__ __device__ constexpr int fused_blocks(uint32_t mask)
 {
-    return mask == MASK_GRID ? 4 : 3;
+    return (mask == MASK_GRID || mask == MASK_GRID_PARTS_NO_MESH) ? 4 : 3;
 }
 
 // Closest hit through the scene's BVHs: its combined tree, or each enabled geometry's tree.

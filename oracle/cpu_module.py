@@ -116,6 +116,8 @@ def load(kind="restated"):
     lib.or_grid_walk_stats.argtypes = [ctypes.c_void_p, ctypes.c_uint32, _fp, _fp, ctypes.c_uint32,
                                        ctypes.c_float, _fp, ctypes.c_uint64, ctypes.c_int,
                                        ctypes.POINTER(ctypes.c_double)]
+    lib.or_parts_grid_walk_stats.argtypes = [ctypes.c_void_p, ctypes.c_float, _fp, ctypes.c_uint64,
+                                             ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     _LIBS[kind] = lib
     return lib
 

@@ -115,6 +115,12 @@ uint64_t or_ray_log_count(void);
 int or_grid_walk_stats(const or_scene* s, uint32_t sphere_geom, const float* pos, const float* rad,
                        uint32_t n, float cells_per_sphere, const float* rays, uint64_t n_rays,
                        int nthreads, double out[6]);
+/* The engine's uniform grid over the scene's parts (every enabled geometry's primitives, a mesh
+   by instance), restated, walked by n_rays logged rays up to the oracle's closest hit: out =
+   {rays, cells per ray, references per ray (listed in the cells walked), cells, references}.
+   Returns 0 on success. */
+int or_parts_grid_walk_stats(const or_scene* s, float cells_per_prim, const float* rays,
+                             uint64_t n_rays, int nthreads, double out[5]);
 
 #ifdef __cplusplus
 }

@@ -65,6 +65,7 @@ struct Geom {
     float rounding_radius = 0, pg_radius = 0;
     Mat material{}, outline{};
     float outline_width = 0;
+    bool enabled = true;
     uint32_t prim_count() const { return type == FR_GEOM_MESH ? n * n_faces : n; }
 };
 
@@ -892,6 +893,164 @@ uint32_t walk_sphere_grid(const SphereGrid& G, F3 o, F3 d, float tnear, uint64_t
 }
 
 // ---------------------------------------------------------------------------------------------
+// The engine's grid over a scene's parts, restated to measure what walking it costs per ray
+// (cells visited, references listed in them) on rays the oracle's own renders trace.
+// Definition: one reference per primitive of every enabled geometry (its padded prim_box), but
+// one per mesh instance (the box of all its rotated vertices, padded by the same rule); boxes
+// that are not finite or are inverted are left out; the grid's shape follows the sphere grid's
+// rule over these boxes.  Walk: the sphere grid's DDA, ending at the first cell whose exit lies
+// at or beyond the closest hit (the oracle's own trace) or at the grid's exit.  The engine's walk
+// ends there too: the closest primitive is referenced by the cell that holds the hit point, so
+// once that cell is tested the closest hit so far is the closest hit, and no earlier cell's exit
+// reaches it.
+// ---------------------------------------------------------------------------------------------
+struct CountGrid {
+    float lo[3], cell[3], ih[3];
+    int n[3];
+    std::vector<uint32_t> count;  // references per cell
+    uint64_t refs = 0;
+};
+
+Box pad_box(Box b)
+{
+    for (int k = 0; k < 3; ++k)
+        if (!(std::isfinite(b.lo[k]) && std::isfinite(b.hi[k]) && b.lo[k] <= b.hi[k]))
+            return box_empty();
+    float scale = 0;
+    for (int k = 0; k < 3; ++k)
+        scale = std::max(scale, std::max(std::fabs(b.lo[k]), std::fabs(b.hi[k])));
+    float pad = 1e-5f * scale + 1e-6f * (b.hi[0] - b.lo[0] + b.hi[1] - b.lo[1] + b.hi[2] - b.lo[2])
+                + 1e-30f;
+    for (int k = 0; k < 3; ++k) {
+        b.lo[k] -= pad;
+        b.hi[k] += pad;
+    }
+    return b;
+}
+
+Box instance_box(const Geom& g, uint32_t inst)
+{
+    Box b = box_empty();
+    const F3 p = g.position[inst];
+    const Quat q = g.orientation[inst];
+    for (size_t k = 0; k < g.vertices.size(); ++k) {
+        F3 v = M::rotate(q, g.vertices[k]) + p;
+        box_grow(b, v.x, v.y, v.z);
+    }
+    return pad_box(b);
+}
+
+bool valid_box(const Box& b)
+{
+    return b.lo[0] <= b.hi[0] && b.lo[1] <= b.hi[1] && b.lo[2] <= b.hi[2];
+}
+
+bool build_count_grid(const std::vector<Box>& boxes, float cells_per_prim, CountGrid& G)
+{
+    float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    uint32_t valid = 0;
+    for (const Box& b : boxes) {
+        if (!valid_box(b))
+            continue;
+        for (int k = 0; k < 3; ++k) {
+            mn[k] = std::min(mn[k], b.lo[k]);
+            mx[k] = std::max(mx[k], b.hi[k]);
+        }
+        ++valid;
+    }
+    if (valid == 0)
+        return false;
+    double lo[3], ext[3], scale = 1.0;
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = mn[k];
+        ext[k] = double(mx[k]) - lo[k];
+        scale = std::max(scale, std::max(std::fabs(lo[k]), std::fabs(lo[k] + ext[k])));
+    }
+    for (int k = 0; k < 3; ++k)
+        ext[k] = std::max(ext[k], 1e-6 * scale);
+    const double volume = ext[0] * ext[1] * ext[2];
+    double h = std::cbrt(volume / (double(cells_per_prim) * valid));
+    for (int pass = 0; pass < 64; ++pass) {
+        double cells = 1.0;
+        for (int k = 0; k < 3; ++k) {
+            G.n[k] = int(std::min(1024.0, std::max(1.0, std::ceil(ext[k] / h))));
+            cells *= G.n[k];
+        }
+        if (cells <= double(1u << 26))
+            break;
+        h *= 1.25;
+    }
+    for (int k = 0; k < 3; ++k) {
+        G.lo[k] = float(lo[k]);
+        G.cell[k] = float(ext[k] / G.n[k]) * (1.0f + 4e-7f);
+        G.ih[k] = 1.0f / G.cell[k];
+    }
+    G.count.assign(size_t(G.n[0]) * G.n[1] * G.n[2], 0);
+    G.refs = 0;
+    for (const Box& b : boxes) {
+        if (!valid_box(b))
+            continue;
+        int a[3], c[3];
+        for (int k = 0; k < 3; ++k) {
+            a[k] = grid_cell_index(b.lo[k], G.lo[k], G.ih[k], G.n[k]);
+            c[k] = grid_cell_index(b.hi[k], G.lo[k], G.ih[k], G.n[k]);
+        }
+        for (int z = a[2]; z <= c[2]; ++z)
+            for (int y = a[1]; y <= c[1]; ++y)
+                for (int x = a[0]; x <= c[0]; ++x) {
+                    G.count[(size_t(z) * G.n[1] + y) * G.n[0] + x]++;
+                    G.refs++;
+                }
+    }
+    return true;
+}
+
+// Cells and references of one ray's walk up to the closest hit at t_hit (inf: none).
+void walk_count_grid(const CountGrid& G, F3 o, F3 d, float t_hit, uint64_t& cells, uint64_t& refs)
+{
+    float inv[3], oinv[3], hi[3];
+    const float of[3] = {o.x, o.y, o.z}, df[3] = {d.x, d.y, d.z};
+    for (int k = 0; k < 3; ++k) {
+        const float a = std::fabs(df[k]);
+        inv[k] = 1.0f / (a < 1e-30f ? std::copysign(1e-30f, df[k]) : df[k]);
+        oinv[k] = -of[k] * inv[k];
+        hi[k] = G.lo[k] + float(G.n[k]) * G.cell[k];
+    }
+    float t0[3], t1[3];
+    for (int k = 0; k < 3; ++k) {
+        t0[k] = std::fma(G.lo[k], inv[k], oinv[k]);
+        t1[k] = std::fma(hi[k], inv[k], oinv[k]);
+    }
+    const float t_in = std::max(std::max(std::min(t0[0], t1[0]), std::min(t0[1], t1[1])),
+                                std::max(std::min(t0[2], t1[2]), 0.0f));
+    const float t_out = std::min(std::min(std::max(t0[0], t1[0]), std::max(t0[1], t1[1])),
+                                 std::max(t0[2], t1[2]));
+    if (!(t_in <= t_out))
+        return;
+    int c[3], s[3];
+    float tn[3];
+    for (int k = 0; k < 3; ++k) {
+        const float u = (of[k] + t_in * df[k] - G.lo[k]) * G.ih[k];
+        c[k] = u >= 0.0f ? int(std::min(u, float(G.n[k] - 1))) : 0;
+        s[k] = inv[k] >= 0.0f ? 1 : -1;
+        tn[k] = std::fma(std::fma(float(c[k] + (inv[k] >= 0.0f ? 1 : 0)), G.cell[k], G.lo[k]), inv[k],
+                         oinv[k]);
+    }
+    for (int guard = G.n[0] + G.n[1] + G.n[2] + 3; guard > 0; --guard) {
+        ++cells;
+        refs += G.count[(size_t(c[2]) * G.n[1] + c[1]) * G.n[0] + c[0]];
+        const float t_cell = std::min(tn[0], std::min(tn[1], tn[2]));
+        const int axis = (tn[0] <= tn[1] && tn[0] <= tn[2]) ? 0 : (tn[1] <= tn[2] ? 1 : 2);
+        c[axis] += s[axis];
+        if (t_hit <= t_cell || !(t_cell < t_out) || c[axis] < 0 || c[axis] >= G.n[axis])
+            break;
+        tn[axis] = std::fma(std::fma(float(c[axis] + (inv[axis] >= 0.0f ? 1 : 0)), G.cell[axis],
+                                     G.lo[axis]),
+                            inv[axis], oinv[axis]);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
 // tile loops
 // ---------------------------------------------------------------------------------------------
 template <class F> void parallel_tiles(uint32_t n_items, int nthreads, F&& body)
@@ -1055,6 +1214,7 @@ or_scene* or_scene_create(const or_geometry_desc* gd, uint32_t n_geoms, int leaf
             delete s;
             return nullptr;
         }
+        g.enabled = d.enabled != 0;
         if (!d.enabled)
             continue;
         uint32_t np = g.prim_count();
@@ -1455,6 +1615,49 @@ int or_grid_walk_stats(const or_scene* s, uint32_t sphere_geom, const float* pos
     out[3] = td;
     out[4] = double(G.start.size() - 1);
     out[5] = double(G.refs.size());
+    return 0;
+}
+
+int or_parts_grid_walk_stats(const or_scene* s, float cells_per_prim, const float* rays,
+                             uint64_t n_rays, int nthreads, double out[5])
+{
+    std::vector<Box> boxes;
+    for (const Geom& g : s->geoms) {
+        if (!g.enabled || g.prim_count() == 0)
+            continue;
+        if (g.type == FR_GEOM_MESH) {
+            for (uint32_t i = 0; i < g.n; ++i)
+                boxes.push_back(instance_box(g, i));
+        } else {
+            for (uint32_t p = 0; p < g.prim_count(); ++p)
+                boxes.push_back(prim_box(g, p));
+        }
+    }
+    CountGrid G;
+    if (!build_count_grid(boxes, cells_per_prim, G))
+        return 1;
+    const uint32_t chunks = uint32_t(std::min<uint64_t>(n_rays, 4096));
+    std::vector<uint64_t> cells(chunks, 0), refs(chunks, 0);
+    parallel_tiles(chunks, nthreads, [&](uint32_t ch, int) {
+        const uint64_t a = n_rays * ch / chunks, b = n_rays * (ch + 1) / chunks;
+        for (uint64_t i = a; i < b; ++i) {
+            const float* r = rays + 7 * i;
+            const F3 o{r[0], r[1], r[2]}, d{r[3], r[4], r[5]};
+            Counters c;
+            const Hit h = trace(*s, o, d, r[6], c);
+            walk_count_grid(G, o, d, h.t, cells[ch], refs[ch]);
+        }
+    });
+    double tc = 0, tr = 0;
+    for (uint32_t ch = 0; ch < chunks; ++ch) {
+        tc += double(cells[ch]);
+        tr += double(refs[ch]);
+    }
+    out[0] = double(n_rays);
+    out[1] = n_rays ? tc / double(n_rays) : 0.0;
+    out[2] = n_rays ? tr / double(n_rays) : 0.0;
+    out[3] = double(G.count.size());
+    out[4] = double(G.refs);
     return 0;
 }
 
