@@ -68,10 +68,12 @@ struct GeomDev {
     Mat outline;
 };
 
-// Uniform grid over the spheres of one geometry (n_cells == 0: the scene has none).  Cell
-// (ix, iy, iz) spans lo + (i, i + 1) * h per axis and is numbered (iz * ny + iy) * nx + ix; its
-// sphere references are [cell_start[c], cell_start[c + 1]), each a copy of the sphere (x, y, z, r)
-// and its index.  A sphere is referenced by every cell its padded bounding box touches.
+// Uniform grid of a scene (n_cells == 0: the scene has none), over the spheres of its one
+// geometry or over the primitives of its parts (parts = 1).  Cell (ix, iy, iz) spans
+// lo + (i, i + 1) * h per axis and is numbered (iz * ny + iy) * nx + ix; its references are
+// [cell_start[c], cell_start[c + 1]): for spheres a copy of the sphere (x, y, z, r) and its index,
+// for parts a leaf-slot record (SceneDev::leaf_data, leaf_geom, order).  A primitive is referenced
+// by every cell its padded bounding box touches (a mesh by instance: the box of the instance).
 struct GridDev {
     uint32_t n_cells;
     uint32_t nx, ny, nz;
