@@ -163,6 +163,7 @@ struct fr_device {
     int combined = 1;                      // one tree per scene of several geometries
     int packet = 0;                        // warp-cooperative primary traversal
     int refill = 0;                        // extension rays with per-lane refill
+    int preview_warp = 1;                  // Preview: one warp per pixel at 32k samples/pixel
     int accel = 2;                         // sphere grid: 0 never, 1 whenever possible, 2 auto
     int fuse_shade = 1;                    // primary rays shaded in the primary pass
     int tail_after = 1;                    // fused bounce launches before the tail kernel (-1: none)
@@ -886,6 +887,7 @@ FrameParams frame_params(fr_tracer* tr, fr_scene* sc, const fr_render_params* p,
     P.shade_blocks = sc->dev->shade_blocks;
     P.packet = sc->use_grid ? 0 : sc->dev->packet;
     P.refill = sc->dev->refill;
+    P.preview_warp = sc->dev->preview_warp;
     tr->last_grid = sc->use_grid ? (sc->grid.parts ? 2u : 1u) : 0u;
     const fr_user_camera& c = p->camera;
     float f_stop = preview ? std::numeric_limits<float>::infinity() : c.f_stop;  // no depth of field in preview
@@ -1196,6 +1198,10 @@ fr_status fr_device_set_option(fr_device* d, const char* name, double value)
         if (!(value == 0.0 || value == 1.0 || value == 2.0))
             return fail(FR_ERR_INVALID, "fuse_shade must be 0, 1 or 2");
         d->fuse_shade = int(value);
+    } else if (n == "preview_warp") {
+        if (value != 0.0 && value != 1.0)
+            return fail(FR_ERR_INVALID, "preview_warp must be 0 or 1");
+        d->preview_warp = int(value);
     } else if (n == "tail") {
         if (!(value >= -1.0 && value <= 64.0 && value == double(int(value))))
             return fail(FR_ERR_INVALID, "tail must be an integer in [-1, 64]");
@@ -1240,6 +1246,8 @@ fr_status fr_device_get_option(const fr_device* d, const char* name, double* val
         *value = d->accel;
     else if (n == "tail")
         *value = d->tail_after;
+    else if (n == "preview_warp")
+        *value = d->preview_warp;
     else if (n == "fuse_shade")
         *value = d->fuse_shade;
     else if (n == "grid_density")

@@ -754,6 +754,58 @@ __global__ void __launch_bounds__(256) k_preview(FrameParams P, uint32_t aa_n, u
     }
 }
 
+// Preview with one warp per pixel (anti-aliasing with a multiple of 32 samples per pixel): lane
+// l traces samples l, l + 32, ... of its warp's pixel, so that a warp's rays are the pixel's own
+// jittered samples, which walk the same cells and nodes, where k_preview's warp holds 32 pixels
+// whose sample loops run side by side.  Each round of 32 samples is summed in sample order
+// (every lane reads the 32 colours by shuffles), so the pixel is the same float sum as
+// k_preview's; the hit ids go to the same places.
+template <int WIDTH, uint32_t MASK>
+__global__ void __launch_bounds__(256) k_preview_warp(FrameParams P, uint32_t aa_n, uint2* hits)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t p = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const bool valid = p < P.w * P.h;  // warp-uniform
+    const uint32_t ns = aa_n * aa_n;   // a multiple of 32
+    TraceCount tc;
+    if (valid) {
+        const uint32_t j = p / P.w, i = p - j * P.w;
+        float avg[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        for (uint32_t base = 0; base < ns; base += 32u) {
+            const uint32_t sample = base + lane;
+            V3 o, d;
+            camera_ray(P.cam, i, j, sample, o, d);
+            Hit h = trace_closest<WIDTH, MASK>(P.scene, o, d, 0.0f, tc);  // CPU preview: tnear 0
+            C3 c = P.bg;
+            float a = P.bg_alpha;
+            if (h.geom != MISS) {
+                const GeomDev& g = P.scene.geoms[h.geom];
+                Surface sf = hit_surface(g, h.prim, o, d, 0.0f);
+                c = preview_shade(P, g, sf, d);
+                a = 1.0f;
+            }
+            if (hits)
+                hits[size_t(p) * ns + sample] =
+                    make_uint2(h.geom == MISS ? 0u : h.geom + 1u, h.geom == MISS ? 0u : h.prim);
+            for (uint32_t k = 0; k < 32u; ++k) {
+                avg[0] += __shfl_sync(0xffffffffu, c.r, k);
+                avg[1] += __shfl_sync(0xffffffffu, c.g, k);
+                avg[2] += __shfl_sync(0xffffffffu, c.b, k);
+                avg[3] += __shfl_sync(0xffffffffu, a, k);
+            }
+        }
+        if (lane == 0u) {
+            const float q = 1.0f / float(ns);
+            write_pixel(P, p, avg[0] * q, avg[1] * q, avg[2] * q, avg[3] * q);
+        }
+    }
+    flush_counts(tc, P.stats + 3);
+    if (lane == 0u && valid) {
+        atomicAdd(P.stats + 0, (unsigned long long)ns);
+        atomicAdd(P.stats + 1, (unsigned long long)ns);
+    }
+}
+
 // Diagnostic: trace rays[i] = (o, d) with both 4-wide traversal forms (one ray per thread, and
 // the step-wise form stepped to completion by one lane); out[i] = (geom, prim, box tests) of
 // each, six words per ray.
@@ -976,6 +1028,15 @@ void launch_histogram(const float4* linear, uint32_t n, uint32_t* counts, int nu
 
 void launch_preview(const FrameParams& P, uint32_t aa_n, uint2* hits, cudaStream_t st)
 {
+    if (P.preview_warp && (aa_n * aa_n) % 32u == 0u) {  // one warp per pixel
+        const uint32_t pixels = P.w * P.h;
+        auto k = pick(P, k_preview_warp<2, MASK_SPHERES>, k_preview_warp<2, MASK_ALL>,
+                      k_preview_warp<4, MASK_SPHERES>, k_preview_warp<4, MASK_ALL>);
+        if (const int gk = grid_kind(P))
+            k = FR_GRID_KERNEL(k_preview_warp, gk);
+        k<<<(pixels + 7u) / 8u, 256, 0, st>>>(P, aa_n, hits);
+        return;
+    }
     dim3 block(16, 16);
     dim3 grid((P.w + 15) / 16, (P.h + 15) / 16);
     auto k = pick(P, k_preview<2, MASK_SPHERES>, k_preview<2, MASK_ALL>,

@@ -28,6 +28,7 @@ struct FrameParams {
     int shade_blocks;        // 0: shade kernel as compiled; 3 or 4: register-limited variants
     int packet;              // 1: primary rays traced warp-cooperatively (4-wide trees)
     int refill;              // 1: extension rays with per-lane refill where refill_geom != -1
+    int preview_warp;        // 1: Preview with 32k samples per pixel traces one pixel per warp
     int refill_geom;         // -2: the scene's combined tree; >= 0: its one enabled geometry;
                              // -1: several per-geometry trees (refill not available)
     int highlight;

@@ -1,8 +1,8 @@
-"""Shading fused into the tracing passes (device option "fuse_shade") gives the same images as
-separate passes: every slot does the same arithmetic on the same values, only in another
-kernel, so the linear outputs must be identical.  Covers several light samples per pixel sample
-(later light samples restart from the stored primary ray), the sphere grid, the BVH of one
-geometry and the combined BVH of a mixed scene."""
+"""Kernel options that change where the arithmetic runs, not what it is, give identical images:
+shading fused into the tracing passes (device option "fuse_shade"; several light samples per
+pixel sample, whose later light samples restart from the stored primary ray), per-lane refill,
+the tail kernel, and Preview with one warp per pixel; on the sphere grid, the BVH of one
+geometry and the combined BVH or grid over parts of a mixed scene."""
 
 import numpy
 import pytest
@@ -90,3 +90,29 @@ def test_tail_kernel_gives_identical_images(gpu_device):
     for img, r in out[1:]:
         assert numpy.array_equal(base, img)
         assert r == rays
+
+
+@pytest.mark.parametrize("name,accel", [("dense_grid", 2), ("dense_grid", 0), ("mixed", 2),
+                                        ("mixed", 0), ("spheres_1k_32ls", 0)])
+def test_preview_warp_per_pixel_gives_identical_output(name, accel, gpu_device):
+    """Preview with one warp per pixel (device option "preview_warp", 8x8 anti-aliasing) sums
+    each pixel's samples in the same order as one thread per pixel: identical hit ids, linear
+    and sRGB outputs, through the sphere grid, the grid over parts and the trees; 4x4
+    anti-aliasing (16 samples) keeps one thread per pixel."""
+    from parity import preview_hits
+    build, w, h, _, _ = SCENES[name]
+    dd = gpu_device._device
+    old = (dd.getOption("preview_warp"), dd.getOption("accel"))
+    try:
+        dd.setOption("accel", accel)
+        scene = build(gpu_device)
+        for aa in (8, 4):
+            out = []
+            for pw in (0, 1):
+                dd.setOption("preview_warp", pw)
+                out.append(preview_hits(gpu_device, scene, w, h, aa))
+            for a, b in zip(out[0], out[1]):
+                assert numpy.array_equal(a, b)
+    finally:
+        dd.setOption("preview_warp", old[0])
+        dd.setOption("accel", old[1])
