@@ -17,7 +17,8 @@
 // The host alternates shade/extend until the queue is empty.
 //
 // Preview (replaces direct_ray_gen/direct_closest_hit, fresnel/gpu/direct.cu, with the CPU
-// arithmetic of fresnel/cpu/TracerDirect.cc:59-220): one thread per pixel, aa_n^2 samples.
+// arithmetic of fresnel/cpu/TracerDirect.cc:59-220): aa_n^2 samples per pixel, one warp per
+// pixel when that is a multiple of 32, else one thread per pixel.
 #include "path_device.cuh"
 
 namespace fr {
