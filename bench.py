@@ -779,7 +779,9 @@ def main():
     # roofline of the traversal kernel with the most device time
     hbm, peak_kind = peaks()
     if wl.preview:
-        kern = {"k_preview": (rays, ms, args.steps)}
+        pv = ("k_preview_warp" if dd.getOption("preview_warp") and (wl.aa_n * wl.aa_n) % 32 == 0
+              else "k_preview")
+        kern = {pv: (rays, ms, args.steps)}
     else:
         primary_rays = float(wl.w * wl.h * wl.spp * args.steps)
         ext_rays = max(0.0, rays - primary_rays)
