@@ -201,6 +201,16 @@ def test_plain_trace_matches_request_counts():
         assert r.done_samples == r.samples and r.image is not None and r.rays > 0
 
 
+def test_plain_trace_waits_with_a_clock_that_passes_the_arrival():
+    """Real-time plain_trace reads the clock once per wait: a clock that crosses a request's
+    arrival between two reads must end the wait, not ask for a negative sleep."""
+    eng = FakeEngine()
+    reqs = [serving.Request(0, 8, 8, 2, seed=1, arrival=0.01, tag=0)]
+    ticks = iter([0.0, 0.0099, 0.02] + [0.02 + 1e-3 * i for i in range(100)])
+    serving.plain_trace(eng, lambda k: "scene", reqs, realtime=True, clock=lambda: next(ticks))
+    assert reqs[0].done_samples == 2 and reqs[0].t_admit >= reqs[0].t_arrive
+
+
 def test_poisson_arrivals_rate():
     rng = numpy.random.default_rng(5)
     t = serving.poisson_arrivals(200.0, 4000, rng)
