@@ -494,6 +494,8 @@ int grid_candidate(const fr_scene* sc, std::vector<uint64_t>& key, uint32_t& gi,
     }
     if (on.empty() || on.size() > size_t(MAX_PARTS))
         return 0;
+    if (sc->geoms.size() >= (size_t(1) << PART_TYPE_SHIFT))
+        return 0;  // a grid over parts keeps geometry indices below 2^24
     const int kind = (on.size() == 1 && on[0]->type == FR_GEOM_SPHERE) ? 1 : 2;
     uint32_t density_bits;
     std::memcpy(&density_bits, &dev->grid_cells_per_prim, sizeof(density_bits));

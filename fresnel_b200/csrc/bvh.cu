@@ -1333,12 +1333,29 @@ cudaError_t parts_boxes(const PartsInput& in, uint32_t n, float4* lo, float4* hi
     return cudaGetLastError();
 }
 
+namespace {
+// A reference's geometry word of a grid over parts: the geometry index with its type above it.
+__global__ void k_tag_types(PartsInput in, uint32_t n, uint32_t* geom)
+{
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n)
+        return;
+    const uint32_t gi = geom[s];
+    uint32_t type = 0;
+    for (uint32_t p = 0; p < in.n_parts; ++p)
+        if (in.geom[p] == gi)
+            type = uint32_t(in.part[p].type);
+    geom[s] = gi | (type << PART_TYPE_SHIFT);
+}
+}  // namespace
+
 cudaError_t gather_parts(const PartsInput& in, const uint32_t* prims, uint32_t total,
                          float4* data, uint32_t* order, uint32_t* geom, cudaStream_t st)
 {
     if (total == 0)
         return cudaSuccess;
     k_gather<<<(total + 255) / 256, 256, 0, st>>>(in, total, prims, data, order, geom);
+    k_tag_types<<<(total + 255) / 256, 256, 0, st>>>(in, total, geom);
     return cudaGetLastError();
 }
 

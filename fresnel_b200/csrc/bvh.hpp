@@ -137,8 +137,13 @@ cudaError_t build_bvh(const PartsInput& in, uint32_t n, const BuildParams& bp, B
 // the tree builds compute them; an empty box, lower > upper, for a primitive left out).
 cudaError_t parts_boxes(const PartsInput& in, uint32_t n, float4* lo, float4* hi, cudaStream_t st);
 
+// Geometry word of a grid-over-parts reference: the scene geometry index (below 2^24), with the
+// geometry's FR_GEOM_* type from bit PART_TYPE_SHIFT on, so that a walk learns a reference's type
+// without reading the geometry table.
+constexpr uint32_t PART_TYPE_SHIFT = 24;
+
 // For each of `total` references to primitives of `in` (combined numbering, prims[r]): its
-// leaf-slot record (2 float4 at data + 2 r), its index within its geometry and its geometry.
+// leaf-slot record (2 float4 at data + 2 r), its index within its geometry and its geometry word.
 cudaError_t gather_parts(const PartsInput& in, const uint32_t* prims, uint32_t total,
                          float4* data, uint32_t* order, uint32_t* geom, cudaStream_t st);
 

@@ -22,6 +22,7 @@
 
 #include <cstdint>
 
+#include "bvh.hpp"
 #include "fresnel_b200.h"
 #include "frmath.cuh"
 
@@ -883,11 +884,14 @@ __device__ __forceinline__ void parts_cell_test(const SceneDev& sc, const RayK& 
 {
     tc.prim += last - first;
     for (uint32_t s = first; s < last; ++s) {
-        const uint32_t gi = __ldg(sc.leaf_geom + s);
+        // geometry index and type in one word (gather_parts): a sphere needs nothing from the
+        // geometry table
+        const uint32_t gw = __ldg(sc.leaf_geom + s);
+        const uint32_t gi = gw & ((1u << PART_TYPE_SHIFT) - 1u);
         if (gi >= sc.n_geoms)
             continue;
         const GeomDev& g = sc.geoms[gi];
-        const int type = g.type;
+        const int type = int(gw >> PART_TYPE_SHIFT);
         const float4 a = ldg4(sc.leaf_data + 2 * size_t(s));
         if ((MASK & (1u << FR_GEOM_MESH)) && type == FR_GEOM_MESH) {
             // the instance's bounding sphere (the distance of its centre from the ray's line
