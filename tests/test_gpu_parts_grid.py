@@ -147,3 +147,22 @@ def test_parts_grid_follows_moving_primitives(accel, gpu_device, oracle_device):
     oh, _, _ = preview_hits(oracle_device, scenes[1], 96, 64, 1)
     check_hits("test_parts_grid_follows_moving_primitives", oracle_device, scenes[1], 96, 64, 1,
                gh, oh, scene="spheres_bonds moved", structure="parts grid")
+
+
+def test_parts_grid_follows_enabled_geometries(accel, gpu_device, oracle_device):
+    """Disabling and enabling geometries changes the grid's parts: each render's hit ids match
+    the oracle's on the same enabled set (the grid is rebuilt over the new parts each time)."""
+    accel(2)
+    scenes = [_mixed(d) for d in (gpu_device, oracle_device)]
+    for step, off in enumerate([(), (3,), (0, 2), ()]):
+        for s in scenes:
+            for i, g in enumerate(s.geometry):
+                if i in off:
+                    g.disable()
+                else:
+                    g.enable()
+        gh, _, _ = preview_hits(gpu_device, scenes[0], 96, 64, 1)
+        assert scenes[0]._scene.getAccel()[0] == PARTS_GRID
+        oh, _, _ = preview_hits(oracle_device, scenes[1], 96, 64, 1)
+        check_hits("test_parts_grid_follows_enabled_geometries", oracle_device, scenes[1], 96,
+                   64, 1, gh, oh, scene=f"mixed, disabled {off}", structure="parts grid")
