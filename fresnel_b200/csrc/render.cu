@@ -17,8 +17,8 @@
 // The host alternates shade/extend until the queue is empty.
 //
 // Preview (replaces direct_ray_gen/direct_closest_hit, fresnel/gpu/direct.cu, with the CPU
-// arithmetic of fresnel/cpu/TracerDirect.cc:59-220): aa_n^2 samples per pixel, one warp per
-// pixel when that is a multiple of 32, else one thread per pixel.
+// arithmetic of fresnel/cpu/TracerDirect.cc:59-220): aa_n^2 samples per pixel, a group of 32 or
+// 16 lanes per pixel when that count is a multiple of 16, else one thread per pixel.
 #include "path_device.cuh"
 
 namespace fr {
@@ -755,25 +755,28 @@ __global__ void __launch_bounds__(256) k_preview(FrameParams P, uint32_t aa_n, u
     }
 }
 
-// Preview with one warp per pixel (anti-aliasing with a multiple of 32 samples per pixel): lane
-// l traces samples l, l + 32, ... of its warp's pixel, so that a warp's rays are the pixel's own
-// jittered samples, which walk the same cells and nodes, where k_preview's warp holds 32 pixels
-// whose sample loops run side by side.  Each round of 32 samples is summed in sample order
-// (every lane reads the 32 colours by shuffles), so the pixel is the same float sum as
-// k_preview's; the hit ids go to the same places.
-template <int WIDTH, uint32_t MASK>
+// Preview with a group of G lanes per pixel (G = 32 or 16 dividing the samples per pixel: 4x4
+// and 8x8 anti-aliasing): lane l of a group traces samples l, l + G, ... of its pixel,
+// so that a warp's rays are a few pixels' own jittered samples, which walk the same cells and
+// nodes, where k_preview's warp holds 32 pixels whose sample loops run side by side.  Each round
+// of G samples is summed in sample order (every lane reads its group's G colours by shuffles), so
+// the pixel is the same float sum as k_preview's; the hit ids go to the same places.
+template <int WIDTH, uint32_t MASK, uint32_t G>
 __global__ void __launch_bounds__(256) k_preview_warp(FrameParams P, uint32_t aa_n, uint2* hits)
 {
     const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t p = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const bool valid = p < P.w * P.h;  // warp-uniform
-    const uint32_t ns = aa_n * aa_n;   // a multiple of 32
+    const uint32_t gl = lane & (G - 1u);  // lane within the pixel's group
+    const uint32_t first = lane - gl;     // the group's first lane
+    const uint32_t gmask = (G == 32u ? 0xffffffffu : ((1u << G) - 1u)) << first;
+    const uint32_t p = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+    const bool valid = p < P.w * P.h;  // uniform within a group
+    const uint32_t ns = aa_n * aa_n;   // a multiple of G
     TraceCount tc;
     if (valid) {
         const uint32_t j = p / P.w, i = p - j * P.w;
         float avg[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-        for (uint32_t base = 0; base < ns; base += 32u) {
-            const uint32_t sample = base + lane;
+        for (uint32_t base = 0; base < ns; base += G) {
+            const uint32_t sample = base + gl;
             V3 o, d;
             camera_ray(P.cam, i, j, sample, o, d);
             Hit h = trace_closest<WIDTH, MASK>(P.scene, o, d, 0.0f, tc);  // CPU preview: tnear 0
@@ -788,20 +791,20 @@ __global__ void __launch_bounds__(256) k_preview_warp(FrameParams P, uint32_t aa
             if (hits)
                 hits[size_t(p) * ns + sample] =
                     make_uint2(h.geom == MISS ? 0u : h.geom + 1u, h.geom == MISS ? 0u : h.prim);
-            for (uint32_t k = 0; k < 32u; ++k) {
-                avg[0] += __shfl_sync(0xffffffffu, c.r, k);
-                avg[1] += __shfl_sync(0xffffffffu, c.g, k);
-                avg[2] += __shfl_sync(0xffffffffu, c.b, k);
-                avg[3] += __shfl_sync(0xffffffffu, a, k);
+            for (uint32_t k = 0; k < G; ++k) {
+                avg[0] += __shfl_sync(gmask, c.r, first + k);
+                avg[1] += __shfl_sync(gmask, c.g, first + k);
+                avg[2] += __shfl_sync(gmask, c.b, first + k);
+                avg[3] += __shfl_sync(gmask, a, first + k);
             }
         }
-        if (lane == 0u) {
+        if (gl == 0u) {
             const float q = 1.0f / float(ns);
             write_pixel(P, p, avg[0] * q, avg[1] * q, avg[2] * q, avg[3] * q);
         }
     }
     flush_counts(tc, P.stats + 3);
-    if (lane == 0u && valid) {
+    if (valid && gl == 0u) {
         atomicAdd(P.stats + 0, (unsigned long long)ns);
         atomicAdd(P.stats + 1, (unsigned long long)ns);
     }
@@ -1029,13 +1032,24 @@ void launch_histogram(const float4* linear, uint32_t n, uint32_t* counts, int nu
 
 void launch_preview(const FrameParams& P, uint32_t aa_n, uint2* hits, cudaStream_t st)
 {
-    if (P.preview_warp && (aa_n * aa_n) % 32u == 0u) {  // one warp per pixel
-        const uint32_t pixels = P.w * P.h;
-        auto k = pick(P, k_preview_warp<2, MASK_SPHERES>, k_preview_warp<2, MASK_ALL>,
-                      k_preview_warp<4, MASK_SPHERES>, k_preview_warp<4, MASK_ALL>);
+    // a group of 32 or 16 lanes per pixel when that divides the samples per pixel (with 2x2
+    // anti-aliasing, 4 lanes per pixel were no faster than one thread on the 1M-sphere scene)
+    const uint32_t ns = aa_n * aa_n;
+    if (P.preview_warp && ns % 16u == 0u) {
+        const bool g32 = ns % 32u == 0u;
+        const uint64_t threads = uint64_t(P.w) * P.h * (g32 ? 32u : 16u);
+        auto k = g32 ? pick(P, k_preview_warp<2, MASK_SPHERES, 32>, k_preview_warp<2, MASK_ALL, 32>,
+                            k_preview_warp<4, MASK_SPHERES, 32>, k_preview_warp<4, MASK_ALL, 32>)
+                     : pick(P, k_preview_warp<2, MASK_SPHERES, 16>, k_preview_warp<2, MASK_ALL, 16>,
+                            k_preview_warp<4, MASK_SPHERES, 16>, k_preview_warp<4, MASK_ALL, 16>);
         if (const int gk = grid_kind(P))
-            k = FR_GRID_KERNEL(k_preview_warp, gk);
-        k<<<(pixels + 7u) / 8u, 256, 0, st>>>(P, aa_n, hits);
+            k = g32 ? (gk == 1   ? k_preview_warp<4, MASK_GRID, 32>
+                       : gk == 2 ? k_preview_warp<4, MASK_GRID_PARTS, 32>
+                                 : k_preview_warp<4, MASK_GRID_PARTS_NO_MESH, 32>)
+                    : (gk == 1   ? k_preview_warp<4, MASK_GRID, 16>
+                       : gk == 2 ? k_preview_warp<4, MASK_GRID_PARTS, 16>
+                                 : k_preview_warp<4, MASK_GRID_PARTS_NO_MESH, 16>);
+        k<<<uint32_t((threads + 255u) / 256u), 256, 0, st>>>(P, aa_n, hits);
         return;
     }
     dim3 block(16, 16);

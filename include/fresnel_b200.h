@@ -198,9 +198,10 @@ FR_API fr_status fr_device_timer_stop(fr_device* dev, float* ms);
  *                   launched), and for scenes traced through a sphere grid each bounce traces
  *                   and shades in one kernel; 2: bounces fused for every scene; 0: separate
  *                   passes.  The same images in every case.
- *   "preview_warp"  1 (default): Preview with a multiple of 32 samples per pixel (8x8
- *                   anti-aliasing) traces one pixel per warp, 32 of its samples at a time,
- *                   summed in sample order; 0: one pixel per thread.  The same outputs.
+ *   "preview_warp"  1 (default): Preview with a multiple of 16 samples per pixel traces each
+ *                   pixel with a group of 32 lanes (8x8 anti-aliasing) or 16 (4x4), that many
+ *                   of its samples at a time, summed in sample order; 0: one pixel per
+ *                   thread.  The same outputs.
  *   "tail"          fused sphere-grid bounces: after this many bounce launches per wavefront
  *                   (0..64, default 1), one persistent launch follows every remaining path to
  *                   its end (a lane takes the next path once its own ends), with no queue

@@ -95,10 +95,10 @@ def test_tail_kernel_gives_identical_images(gpu_device):
 @pytest.mark.parametrize("name,accel", [("dense_grid", 2), ("dense_grid", 0), ("mixed", 2),
                                         ("mixed", 0), ("spheres_1k_32ls", 0)])
 def test_preview_warp_per_pixel_gives_identical_output(name, accel, gpu_device):
-    """Preview with one warp per pixel (device option "preview_warp", 8x8 anti-aliasing) sums
-    each pixel's samples in the same order as one thread per pixel: identical hit ids, linear
-    and sRGB outputs, through the sphere grid, the grid over parts and the trees; 4x4
-    anti-aliasing (16 samples) keeps one thread per pixel."""
+    """Preview with a group of lanes per pixel (device option "preview_warp": 32 lanes at 8x8
+    anti-aliasing, 16 at 4x4) sums each pixel's samples in the same order as one thread per
+    pixel: identical hit ids, linear and sRGB outputs, through the sphere grid, the grid over
+    parts and the trees; 2x2 and 3x3 anti-aliasing keep one thread per pixel."""
     from parity import preview_hits
     build, w, h, _, _ = SCENES[name]
     dd = gpu_device._device
@@ -106,7 +106,7 @@ def test_preview_warp_per_pixel_gives_identical_output(name, accel, gpu_device):
     try:
         dd.setOption("accel", accel)
         scene = build(gpu_device)
-        for aa in (8, 4):
+        for aa in (8, 4, 2, 3):
             out = []
             for pw in (0, 1):
                 dd.setOption("preview_warp", pw)
