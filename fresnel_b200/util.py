@@ -47,14 +47,20 @@ def _parallel_ok(dst, src):
             and not numpy.may_share_memory(dst, src))
 
 
-def _copy_rows(dst, src):
+def _copy_rows(dst, src, stream_copy=None):
     """``dst[:] = src`` (same shapes) as row blocks on the copy threads.  Each block is an
-    ordinary numpy assignment, so the result equals the single assignment element for element."""
+    ordinary numpy assignment, or ``stream_copy(dst_block, src_block)`` (the backend's copy with
+    cache-bypassing stores, for a buffer uploaded next) where that takes the pair of types; either
+    way the result equals the single assignment element for element."""
     pool = _copy_pool()
     n = dst.shape[0]
     step = -(-n // _pool_workers)
-    futures = [pool.submit(dst.__setitem__, slice(i, i + step), src[i:i + step])
-               for i in range(0, n, step)]
+
+    def block(i):
+        d, s = dst[i:i + step], src[i:i + step]
+        if stream_copy is None or not stream_copy(d, s):
+            d[...] = s
+    futures = [pool.submit(block, i) for i in range(0, n, step)]
     for fut in futures:
         fut.result()
 
@@ -63,7 +69,8 @@ class Array:
     """numpy-like access to a backend buffer (fresnel/util.py:15-70).
 
     ``array[slice] = v`` maps the buffer, writes, unmaps (uploading to the device) and marks the
-    owning geometry stale; ``array[slice]`` returns a copy.
+    owning geometry stale; ``array[slice]`` returns a copy and uploads nothing (a whole tracer
+    output is downloaded straight into the returned array).
     """
 
     def __init__(self, buf, geom):
@@ -73,13 +80,13 @@ class Array:
         a = numpy.asarray(self.buf)
         self.shape = a.shape
         self.dtype = a.dtype
-        self.buf.unmap()
+        self._unmap_read()
 
     def __setitem__(self, slc, data):
         self.buf.map()
         a = numpy.asarray(self.buf)
         if _whole(slc) and _parallel_ok(a, data):
-            _copy_rows(a, data)
+            _copy_rows(a, data, getattr(self.buf, "streamCopy", None))
         else:
             a[slc] = data
         self.buf.unmap()
@@ -87,6 +94,12 @@ class Array:
             self.geom._geometry.update()
 
     def __getitem__(self, slc):
+        read_copy = getattr(self.buf, "readCopy", None)
+        if read_copy is not None and _whole(slc):
+            # a tracer output downloaded straight into the returned array's own storage
+            data = read_copy()
+            if data is not None:
+                return data
         self.buf.map()
         a = numpy.asarray(self.buf)
         if _whole(slc) and a.ndim >= 1 and a.shape[0] > 1 and a.nbytes >= PARALLEL_COPY_BYTES \
@@ -95,8 +108,13 @@ class Array:
             _copy_rows(data, a)
         else:
             data = numpy.array(a[slc], copy=True)
-        self.buf.unmap()
+        self._unmap_read()
         return data
+
+    def _unmap_read(self):
+        """Unmaps after a read: the host copy is unchanged, so nothing is uploaded again (a
+        backend without unmapRead treats every unmap as a write)."""
+        getattr(self.buf, "unmapRead", self.buf.unmap)()
 
 
 class ImageArray(Array):
@@ -108,7 +126,7 @@ class ImageArray(Array):
         self.buf.map()
         f = io.BytesIO()
         PIL_Image.fromarray(numpy.asarray(self.buf), mode='RGBA').save(f, 'png')
-        self.buf.unmap()
+        self._unmap_read()
         return f.getvalue()
 
 

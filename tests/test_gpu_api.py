@@ -174,3 +174,51 @@ def test_stats_count_rays(gpu_device):
     st = t._tracer.getStats()
     assert st["paths"] == 20 * 10 * 3 * 2
     assert st["rays"] >= 20 * 10 * 3
+
+
+def test_reading_arrays_rebuilds_nothing(gpu_device):
+    """Reading a geometry array (the whole array or a part) leaves its device copy and the
+    acceleration structure as they are; a write rebuilds."""
+    scene = workloads.hex_spheres(gpu_device)
+    t = fresnel.tracer.Preview(device=gpu_device, w=48, h=48, anti_alias=False)
+    first = t.render(scene)[:]
+    st = t._tracer.getStats()
+    built = st["bvh_builds"] + st["grid_builds"]
+    g = scene.geometry[0]
+    pos, rad, col = g.position[:], g.radius[:], g.color[:]
+    assert g.position[2:4].shape == (2, 3)
+    again = t.render(scene)[:]
+    st = t._tracer.getStats()
+    assert st["bvh_builds"] + st["grid_builds"] == built
+    assert numpy.array_equal(first, again)
+    g.position[:] = pos
+    t.render(scene)
+    st = t._tracer.getStats()
+    assert st["bvh_builds"] + st["grid_builds"] == built + 1
+    assert rad.shape == (pos.shape[0],) and col.shape == pos.shape
+
+
+def test_output_reads_are_independent_copies(gpu_device):
+    """A whole read of a tracer output (downloaded straight into the returned array) equals the
+    mapped buffer's contents, and each read is a copy of its own that later renders leave as
+    is."""
+    scene = workloads.hex_spheres(gpu_device)
+    t = fresnel.tracer.Path(device=gpu_device, w=40, h=30)
+    t.sample(scene, samples=2)
+    for arr in (t.output, t.linear_output):
+        a = arr[:]
+        arr.buf.map()
+        mapped = numpy.array(arr.buf, copy=True)
+        arr.buf.unmap()
+        assert a.dtype == mapped.dtype and a.shape == mapped.shape
+        assert numpy.array_equal(a, mapped, equal_nan=True)
+        b = arr[...]
+        assert not numpy.may_share_memory(a, b) and numpy.array_equal(a, b, equal_nan=True)
+    kept = t.output[:]
+    copy = kept.copy()
+    del a, b
+    scene.background_color = (0.9, 0.1, 0.1)
+    scene.background_alpha = 1.0
+    t.sample(scene, samples=1)
+    later = t.output[:]
+    assert numpy.array_equal(kept, copy) and not numpy.array_equal(later, kept)

@@ -140,3 +140,114 @@ def test_copy_threads_made_again_in_a_new_process(monkeypatch):
     data = numpy.arange(3 * BIG, dtype=numpy.float32).reshape(BIG, 3)
     util.Array(buf, None)[:] = data
     assert numpy.array_equal(buf.a, data)
+
+
+class TrackingBuffer(FakeBuffer):
+    """A backend buffer with the read-only unmap and the direct whole-array download: unmap()
+    marks the host copy for upload, unmapRead() does not; readCopy() returns a copy (or None, when
+    the backend has no storage to give)."""
+
+    def __init__(self, shape, dtype, copies=True):
+        super().__init__(shape, dtype)
+        self.stale = False
+        self.copies = copies
+        self.read_copies = 0
+
+    def unmap(self):
+        super().unmap()
+        self.stale = True
+
+    def unmapRead(self):
+        FakeBuffer.unmap(self)
+
+    def readCopy(self):
+        self.read_copies += 1
+        return self.a.copy() if self.copies else None
+
+
+@pytest.mark.parametrize("shape", [(BIG, 3), (40, 3)])
+def test_reads_do_not_mark_the_host_copy_for_upload(shape):
+    buf = TrackingBuffer(shape, numpy.float32, copies=False)
+    arr = util.Array(buf, FakeGeometry())
+    assert not buf.stale  # constructing the wrapper reads the shape only
+    buf.a[:] = 7.0
+    assert numpy.all(arr[:] == 7.0) and numpy.all(arr[2:5] == 7.0)
+    assert not buf.stale and not buf.mapped
+    arr[1] = (1.0, 2.0, 3.0)
+    assert buf.stale
+
+
+def test_whole_reads_take_the_direct_download():
+    buf = TrackingBuffer((12, 10, 4), numpy.uint8)
+    buf.a[:] = numpy.arange(480, dtype=numpy.uint8).reshape(12, 10, 4)
+    arr = util.ImageArray(buf, None)
+    maps = buf.maps
+    out = arr[:]
+    assert buf.read_copies == 1 and buf.maps == maps  # no map: the copy came from readCopy
+    assert numpy.array_equal(out, buf.a) and not numpy.may_share_memory(out, buf.a)
+    out = arr[...]
+    assert buf.read_copies == 2 and numpy.array_equal(out, buf.a)
+    part = arr[3:5]  # a part is read through the mapped buffer
+    assert buf.read_copies == 2 and buf.maps == maps + 1
+    assert numpy.array_equal(part, buf.a[3:5])
+    none = TrackingBuffer((12, 10, 4), numpy.uint8, copies=False)
+    none.a[:] = 5
+    assert numpy.all(util.ImageArray(none, None)[:] == 5) and none.read_copies == 1
+
+
+def _stream_copy():
+    from fresnel_b200 import _gpu
+    return _gpu.ArrayVec3f.streamCopy
+
+
+@pytest.mark.parametrize("src_dtype,dst_dtype,shape", [
+    (numpy.float32, numpy.float32, (BIG, 3)),
+    (numpy.float64, numpy.float32, (BIG, 3)),
+    (numpy.float64, numpy.float32, (5, 3)),      # shorter than one block of the conversion
+    (numpy.uint8, numpy.uint8, (97, 13, 4)),     # an odd number of bytes
+    (numpy.float32, numpy.float32, (1,)),
+])
+def test_stream_copy_equals_numpy_assignment(src_dtype, dst_dtype, shape):
+    """The backend's copy with streaming stores gives the numpy assignment's bytes, float64
+    rounding, infinities, NaN and subnormals included, at any alignment of the destination."""
+    copy = _stream_copy()
+    rng = numpy.random.default_rng(3)
+    src = rng.uniform(-1e3, 1e3, shape).astype(src_dtype)
+    if src.dtype.kind == "f":
+        flat = src.reshape(-1)
+        special = [numpy.inf, -numpy.inf, numpy.nan, 1e-45, -1e-44, 3.4028235e38, 1e39, -0.0,
+                   1.0000000596046448]  # the last rounds to even
+        with numpy.errstate(over="ignore"):
+            flat[:len(special)] = numpy.array(special[:flat.size], dtype=src_dtype)
+    for shift in (0, 4, 12):  # destination offsets of 0, 4 and 12 bytes from a 16-byte boundary
+        storage = numpy.zeros(src.size * numpy.dtype(dst_dtype).itemsize + 64, numpy.uint8)
+        base = (-storage.ctypes.data) % 16 + shift
+        dst = storage[base:base + src.size * numpy.dtype(dst_dtype).itemsize].view(dst_dtype)
+        dst = dst.reshape(shape)
+        with numpy.errstate(over="ignore"):
+            expect = numpy.zeros(shape, dst_dtype)
+            expect[...] = src
+        assert copy(dst, src) is True
+        assert dst.tobytes() == expect.tobytes()
+
+
+def test_stream_copy_declines_what_it_does_not_take():
+    copy = _stream_copy()
+    a = numpy.zeros((100, 3), numpy.float32)
+    assert copy(a, numpy.ones((100, 3), numpy.int32)) is False          # other types
+    assert copy(a, numpy.ones((99, 3), numpy.float32)) is False         # other shapes
+    assert copy(a, numpy.ones((3, 100), numpy.float32).T) is False      # not C-contiguous
+    assert copy(a[:60], a[40:]) is False                                # overlapping storage
+    assert not a.any()
+
+
+def test_large_write_through_stream_copy_equals_plain_assignment():
+    class StreamingBuffer(TrackingBuffer):
+        streamCopy = staticmethod(_stream_copy())
+    rng = numpy.random.default_rng(4)
+    for src_dtype in (numpy.float64, numpy.float32, numpy.int64):  # int64: numpy's assignment
+        data = rng.uniform(-50, 50, (BIG, 3)).astype(src_dtype)
+        buf = StreamingBuffer((BIG, 3), numpy.float32)
+        util.Array(buf, FakeGeometry())[:] = data
+        assert numpy.array_equal(buf.a, _plain_write((BIG, 3), numpy.float32, data))
+        assert buf.stale and not buf.mapped
