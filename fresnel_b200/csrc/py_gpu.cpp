@@ -7,7 +7,8 @@
 //
 // Arrays: geometry arrays keep an authoritative host copy; unmap() marks the array stale and
 // the next render uploads stale arrays (a BVH rebuild follows only when a geometric array
-// changed).  Output arrays are authoritative on the device; map() downloads them.
+// changed), unmapRead() ends a read and marks nothing.  Output arrays are authoritative on the
+// device; map() downloads them into the array's buffer, readCopy() into a new numpy array.
 #include <pybind11/numpy.h>
 #include <pybind11/pybind11.h>
 
