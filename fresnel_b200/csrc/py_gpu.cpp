@@ -186,8 +186,10 @@ bool stream_copy(const py::buffer& dst_buf, const py::buffer& src_buf)
 // Page-locked blocks that back the arrays returned by whole reads of tracer outputs: the download
 // lands in the array handed to numpy, with no copy on the host and no page faults on fresh
 // memory, and numpy's release of the array returns the block here.  A block serves requests of
-// more than half its size; at most MAX_CACHED bytes wait in the pool.  The pool is never
-// destroyed, since arrays may be released after the module is torn down.
+// more than half its size; at most MAX_CACHED bytes wait in the pool, and at most MAX_LIVE bytes
+// are held by arrays (a program that keeps many frames gets ordinary memory beyond that, so
+// that it does not lock the host's memory).  The pool is never destroyed, since arrays may be
+// released after the module is torn down.
 class PinnedPool {
 public:
     static PinnedPool& get()
@@ -205,13 +207,20 @@ public:
                 cap = it->first;
                 void* p = it->second;
                 cached_ -= cap;
+                live_ += cap;
                 free_.erase(it);
                 return p;
             }
+            if (live_ + n > MAX_LIVE)
+                return nullptr;
+            live_ += n;  // reserved before the allocation, released if it fails
         }
         void* p = nullptr;
-        if (fr_host_alloc(n, &p) != FR_OK)
+        if (fr_host_alloc(n, &p) != FR_OK) {
+            std::lock_guard<std::mutex> lock(m_);
+            live_ -= n;
             return nullptr;
+        }
         cap = n;
         return p;
     }
@@ -219,6 +228,7 @@ public:
     {
         {
             std::lock_guard<std::mutex> lock(m_);
+            live_ -= cap;
             if (cached_ + cap <= MAX_CACHED) {
                 free_.emplace(cap, p);
                 cached_ += cap;
@@ -230,9 +240,11 @@ public:
 
 private:
     static constexpr size_t MAX_CACHED = size_t(256) << 20;
+    static constexpr size_t MAX_LIVE = size_t(1) << 30;
     std::mutex m_;
     std::multimap<size_t, void*> free_;
     size_t cached_ = 0;
+    size_t live_ = 0;
 };
 
 struct ArrayBase {
