@@ -222,3 +222,42 @@ def test_output_reads_are_independent_copies(gpu_device):
     t.sample(scene, samples=1)
     later = t.output[:]
     assert numpy.array_equal(kept, copy) and not numpy.array_equal(later, kept)
+
+
+def test_whole_and_partial_array_writes_render_alike(gpu_device):
+    """Whole writes of large arrays (row blocks on the copy threads, streaming stores) give the
+    renders that the same arrays written part by part give, also when an array is written twice
+    before a render; a read between write and render sees the write."""
+    n = 400_000  # positions and colours above the 4 MB of a threaded copy, radii below
+    rng = numpy.random.default_rng(11)
+    pos = [rng.uniform(-30, 30, (n, 3)).astype(numpy.float32) for _ in range(2)]
+    col = rng.uniform(0, 1, (n, 3)).astype(numpy.float32)
+    rad = rng.uniform(0.2, 0.6, n).astype(numpy.float32)
+
+    def scene(parts):
+        s = fresnel.Scene(device=gpu_device)
+        g = fresnel.geometry.Sphere(s, N=n, material=fresnel.material.Material(
+            primitive_color_mix=1.0, roughness=0.5))
+        if parts == 1:
+            g.position[:], g.color[:], g.radius[:] = pos[0], col, rad
+        for k in range(0, n, n // parts) if parts > 1 else ():
+            g.position[k:k + n // parts] = pos[0][k:k + n // parts]
+            g.color[k:k + n // parts] = col[k:k + n // parts]
+            g.radius[k:k + n // parts] = rad[k:k + n // parts]
+        s.camera = fresnel.camera.Orthographic.fit(s)
+        return s, g
+    s_lazy, g_lazy = scene(4)  # partial writes
+    s_q, g_q = scene(1)        # whole writes
+    assert numpy.array_equal(g_q.position[:], pos[0])
+    t = fresnel.tracer.Preview(device=gpu_device, w=96, h=96, anti_alias=False)
+    a = t.render(s_lazy)[:]
+    t_q = fresnel.tracer.Preview(device=gpu_device, w=96, h=96, anti_alias=False)
+    b = t_q.render(s_q)[:]
+    assert a[..., 3].max() == 255 and numpy.array_equal(a, b)
+    g_q.position[:] = pos[1]
+    g_q.position[:] = pos[0]  # written again before the render: the last write wins
+    assert numpy.array_equal(g_q.position[:], pos[0])
+    assert numpy.array_equal(t_q.render(s_q)[:], a)
+    g_q.position[:] = pos[1]
+    g_lazy.position[0:n] = pos[1]
+    assert numpy.array_equal(t_q.render(s_q)[:], t.render(s_lazy)[:])
