@@ -8,8 +8,13 @@ CPU in double precision for the camera rays of random pixels (pinhole camera of 
 scene, fresnel's tent-filtered jitter of width 0.707 pixels, Camera.h:169-269) and reports per
 camera ray the spheres tested now (S), the spheres that survive a conservative cull against the
 pixel's ray cone (S_cull: the angle between the cone's axis and the sphere's centre at most the
-cone's half-angle plus the sphere's angular radius), and per warp the references held by the
-cells its rays visit (U_refs: the cull's work, one reference per lane).  The hit sphere of every
+cone's half-angle plus the sphere's angular radius), the tests left when only the steps of a
+warp-synchronous walk whose walking lanes all stand in one cell are culled (S_hybrid; the share
+of such steps is coop_step_frac), and per warp the references held by the cells its rays visit
+(U_refs) and the passes of one reference per lane that culling every distinct cell of every
+step would take (cull_rounds: lanes grouped by cell with __match_any_sync).  The look-ahead form
+gathers each walking lane's next BATCH cells into one batch, culls the batch's distinct cells in
+batch_passes passes and leaves S_batch exact tests per ray (S_batch_max for the warp's longest).  The hit sphere of every
 ray is checked to survive the cull.
 
 Run: python oracle/cone_cull_estimate.py [n_pixels]   (default 400)
@@ -27,6 +32,8 @@ sys.path.insert(0, REPO)
 
 AA_WIDTH = 0.707106781  # Camera.h: importanceSampleAA's tent scaled to this half-width
 TNEAR = 1e-5
+BATCH = 3  # cells per lane gathered into one cull batch (look-ahead form)
+AHEAD = BATCH - 1
 
 
 class SphereGrid:
@@ -57,15 +64,16 @@ class SphereGrid:
         self.start = numpy.searchsorted(cid[order], numpy.arange(self.dims.prod() + 1))
         self.refs_per_sphere = float(cnt.mean())
 
-    def walk(self, o, d):
-        """(cells visited, spheres tested in order, closest hit or -1) of the ray o + t d."""
+    def walk(self, o, d, ahead=0):
+        """(cells visited, spheres tested in order, closest hit or -1) of the ray o + t d, and the
+        up to `ahead` cells the DDA would reach after the stop (inside the grid)."""
         with numpy.errstate(divide="ignore"):
             inv = numpy.where(d != 0, 1.0 / numpy.where(d != 0, d, 1.0), numpy.inf)
         t0, t1 = (self.lo - o) * inv, (self.hi - o) * inv
         t_in = max(numpy.minimum(t0, t1).max(), 0.0)
         t_out = numpy.maximum(t0, t1).min()
         if not t_in <= t_out:
-            return [], [], -1
+            return [], [], -1, []
         c = numpy.clip(numpy.floor((o + t_in * d - self.lo) / self.cell).astype(numpy.int64), 0,
                        self.dims - 1)
         step = numpy.where(d >= 0, 1, -1)
@@ -93,9 +101,29 @@ class SphereGrid:
                 break
             c[a] += step[a]
             if not 0 <= c[a] < self.dims[a]:
+                return cells, tested, hit, []
+            t_next[a] += t_delta[a]
+        extra = []
+        while len(extra) < ahead:
+            a = int(numpy.argmin(t_next))
+            if t_next[a] >= t_out:
+                break
+            c[a] += step[a]
+            if not 0 <= c[a] < self.dims[a]:
                 break
             t_next[a] += t_delta[a]
-        return cells, tested, hit
+            extra.append(int((c[2] * self.dims[1] + c[1]) * self.dims[0] + c[0]))
+        return cells, tested, hit, extra
+
+
+def _kept(keep, s, pos, p, axis, half, r):
+    """Whether sphere s survives the cull against the cone (p, axis, half-angle); memoised."""
+    if s not in keep:
+        q = pos[s] - p
+        dist = numpy.linalg.norm(q)
+        ang = math.acos(max(-1.0, min(1.0, float(q @ axis) / dist)))
+        keep[s] = ang <= half + math.asin(min(1.0, r / dist)) + 1e-6
+    return keep[s]
 
 
 def _tent(u):
@@ -130,8 +158,9 @@ def estimate(n_pixels=400, seed=7):
         return d / numpy.linalg.norm(d)
 
     rng = numpy.random.default_rng(seed)
-    per_ray = {"S": [], "S_cull": [], "cells": [], "hit": []}
-    per_warp = {"U_refs": [], "U_cells": [], "S_max": [], "S_cull_max": []}
+    per_ray = {"S": [], "S_cull": [], "S_hybrid": [], "S_batch": [], "cells": [], "hit": []}
+    per_warp = {"U_refs": [], "U_cells": [], "S_max": [], "S_cull_max": [], "coop_step_frac": [],
+                "cull_rounds": [], "batch_passes": [], "S_batch_max": []}
     for _ in range(n_pixels):
         i, j = int(rng.integers(0, w)), int(rng.integers(0, h))
         dirs = numpy.array([ray(i, j, dx, dy) for dx, dy in
@@ -139,27 +168,61 @@ def estimate(n_pixels=400, seed=7):
         axis = dirs.mean(0)
         axis /= numpy.linalg.norm(axis)
         half = float(numpy.arccos(numpy.clip(dirs @ axis, -1.0, 1.0)).max())
-        walks = [grid.walk(p, d) for d in dirs]
+        walks4 = [grid.walk(p, d, AHEAD) for d in dirs]
+        walks = [x[:3] for x in walks4]
         cells = set(c for cl, _, _ in walks for c in cl)
         per_warp["U_cells"].append(len(cells))
         per_warp["U_refs"].append(sum(int(grid.start[c + 1] - grid.start[c]) for c in cells))
         keep = {}
         s_all, s_cull = [], []
         for cl, tested, hit in walks:
-            kept = 0
-            for s in tested:
-                if s not in keep:
-                    q = pos[s] - p
-                    dist = numpy.linalg.norm(q)
-                    ang = math.acos(max(-1.0, min(1.0, float(q @ axis) / dist)))
-                    keep[s] = ang <= half + math.asin(min(1.0, r / dist)) + 1e-6
-                kept += keep[s]
+            kept = sum(1 for x in tested if _kept(keep, x, pos, p, axis, half, r))
             if hit >= 0 and not keep[hit]:
                 raise AssertionError("the cull dropped a ray's hit sphere")
             s_all.append(len(tested))
             s_cull.append(kept)
             per_ray["cells"].append(len(cl))
             per_ray["hit"].append(hit >= 0)
+        # warp-synchronous walk: a step whose walking lanes all stand in one cell is culled once
+        # for the warp; any other step keeps every lane's own tests
+        steps = max(len(cl) for cl, _, _ in walks)
+        hybrid = [0] * len(walks)
+        coop = rounds = 0
+        for k in range(steps):
+            here = {cl[k] for cl, _, _ in walks if len(cl) > k}
+            for lane, (cl, _, _) in enumerate(walks):
+                if len(cl) <= k:
+                    continue
+                refs = grid.refs[grid.start[cl[k]]:grid.start[cl[k] + 1]]
+                if len(here) == 1:
+                    hybrid[lane] += sum(1 for x in refs if _kept(keep, int(x), pos, p, axis, half, r))
+                else:
+                    hybrid[lane] += len(refs)
+            coop += len(here) == 1
+            rounds += sum(-(-int(grid.start[c + 1] - grid.start[c]) // 32) for c in here)
+        # look-ahead form: every walking lane contributes its next BATCH cells (past its stop in
+        # its last batch), the batch's distinct cells are culled in passes of one reference per
+        # lane, and each lane exact-tests the survivors of its own batch cells
+        n_batches = max(-(-len(cl) // BATCH) for cl, _, _ in walks) if steps else 0
+        passes = 0
+        batch_tests = [0] * len(walks)
+        for b in range(n_batches):
+            distinct = set()
+            for lane, (cl, _, _, extra) in enumerate(walks4):
+                if len(cl) <= b * BATCH:
+                    continue
+                mine = (cl + extra)[b * BATCH:(b + 1) * BATCH]
+                distinct.update(mine)
+                batch_tests[lane] += sum(
+                    1 for c in mine for x in grid.refs[grid.start[c]:grid.start[c + 1]]
+                    if _kept(keep, int(x), pos, p, axis, half, r))
+            passes += -(-sum(int(grid.start[c + 1] - grid.start[c]) for c in distinct) // 32)
+        per_warp["batch_passes"].append(passes)
+        per_warp["S_batch_max"].append(max(batch_tests))
+        per_ray["S_batch"] += batch_tests
+        per_warp["coop_step_frac"].append(coop / steps if steps else 1.0)
+        per_warp["cull_rounds"].append(rounds)
+        per_ray["S_hybrid"] += hybrid
         per_ray["S"] += s_all
         per_ray["S_cull"] += s_cull
         per_warp["S_max"].append(max(s_all))
