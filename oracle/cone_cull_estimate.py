@@ -14,8 +14,8 @@ of such steps is coop_step_frac), and per warp the references held by the cells 
 (U_refs) and the passes of one reference per lane that culling every distinct cell of every
 step would take (cull_rounds: lanes grouped by cell with __match_any_sync).  The look-ahead form
 gathers each walking lane's next BATCH cells into one batch, culls the batch's distinct cells in
-batch_passes passes and leaves S_batch exact tests per ray (S_batch_max for the warp's longest).  The hit sphere of every
-ray is checked to survive the cull.
+batch_passes passes and leaves S_batch exact tests per ray (S_batch_max for the warp's
+longest).  The hit sphere of every ray is checked to survive the cull.
 
 Run: python oracle/cone_cull_estimate.py [n_pixels]   (default 400)
 """
